@@ -1,0 +1,393 @@
+/*
+ * av1pf.h — C ABI of the B200 (sm_100a) AV1 frame post-filter chain.
+ *
+ * The chain is the one the reference decoder runs after tile decoding
+ * (rivet-av1 src/decoder/mod.rs:747-759 `decode_frame_wrapup`, and the output
+ * process at :846-917): deblocking loop filter (7.14) -> CDEF (7.15) ->
+ * super-resolution (7.16) -> loop restoration (7.17) -> reference frame, then
+ * on output crop + film grain (7.18.3) + packing into the `Frame` layout.
+ *
+ * Every entry point is `extern "C"`, takes plain structs and pointers, and
+ * returns an `int` status (AV1PF_OK or an AV1PF_ERR_* code); nothing throws
+ * or aborts across the boundary. Sample planes and per-4x4 maps passed to the
+ * device entry points are DEVICE pointers; the `_host` entry points take host
+ * pointers and do the copies themselves. Streams are `cudaStream_t` passed as
+ * `void*` (NULL = the legacy default stream), so this header needs no CUDA
+ * include.
+ *
+ * A context is used from one host thread at a time; the serving API
+ * (av1pf_serve_*) is internally synchronised.
+ */
+#ifndef AV1PF_H
+#define AV1PF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes. The reference's post-filters are infallible (they panic on  */
+/* out-of-bounds through SharedPlane's asserts, postfilter.rs:41,48,57); its */
+/* decode-level errors are Error::{Bitstream, Unsupported, InvalidInput}     */
+/* (lib.rs:60-73). These codes map onto those, plus device-side conditions.  */
+/* ------------------------------------------------------------------------ */
+enum {
+  AV1PF_OK = 0,
+  AV1PF_ERR_INVALID_INPUT = 1, /* bad descriptor, size or parameter       */
+  AV1PF_ERR_UNSUPPORTED = 2,   /* valid AV1 but outside this build        */
+  AV1PF_ERR_OOM = 3,           /* device allocation failed                */
+  AV1PF_ERR_ADMISSION = 4,     /* refused: would exceed the HBM cap       */
+  AV1PF_ERR_TIMEOUT = 5,       /* a bounded wait ran out                  */
+  AV1PF_ERR_CUDA = 6,          /* a CUDA runtime call failed              */
+  AV1PF_ERR_NOT_FOUND = 7      /* unknown ticket / stream                 */
+};
+
+/* Restoration types (consts.rs:284-286). */
+enum { AV1PF_RESTORE_NONE = 0, AV1PF_RESTORE_WIENER = 1, AV1PF_RESTORE_SGRPROJ = 2 };
+
+#define AV1PF_MAX_PLANES 3
+
+/* One plane of samples. `data` points at sample (0,0); samples are uint8_t
+ * when the frame's sample_bytes is 1 (8-bit only) and uint16_t when it is 2.
+ * The reference keeps every plane as u16 with stride = allocated width
+ * (src/decoder/state.rs:9-42); rows are `stride` samples apart here too. */
+typedef struct av1pf_plane {
+  void* data;
+  int64_t stride; /* row pitch in samples */
+  int32_t width;  /* allocated (readable) width in samples  */
+  int32_t height; /* allocated rows */
+} av1pf_plane;
+
+/* Frame geometry and format: FrameCtx fields bit_depth, ssx, ssy, num_planes,
+ * mi_rows, mi_cols (decoder/mod.rs:44-52) plus the header's frame_width,
+ * frame_height, upscaled_width (header.rs:117-121) and the sequence's
+ * matrix_coefficients (read by film grain, grain.rs:287). */
+typedef struct av1pf_frame_info {
+  int32_t bit_depth;      /* 8, 10 or 12 */
+  int32_t sample_bytes;   /* 1 (bit_depth 8 only) or 2 */
+  int32_t subsampling_x;  /* 0/1 */
+  int32_t subsampling_y;  /* 0/1 */
+  int32_t num_planes;     /* 1 (monochrome) or 3 */
+  int32_t frame_width;    /* coded width (after superres downscaling) */
+  int32_t frame_height;
+  int32_t upscaled_width; /* == frame_width without superres */
+  int32_t mi_rows;        /* 2*((frame_height+7)>>3), header.rs:728-731 */
+  int32_t mi_cols;        /* 2*((frame_width+7)>>3) */
+  int32_t matrix_coefficients;
+} av1pf_frame_info;
+
+/* Mode info of one 4x4 luma block: the fields of the reference's `Mi`
+ * (decoder/state.rs:55-75) that the loop filter reads (postfilter.rs:133-138,
+ * 215-224) and CDEF's skip test (postfilter.rs:306-307). 8 bytes. */
+typedef struct av1pf_mi {
+  uint8_t mi_size;      /* BLOCK_4X4 (0) .. BLOCK_64X16 (21) */
+  uint8_t y_mode;       /* YMode: intra 0..12, inter NEARESTMV (14) .. */
+  int8_t ref_frame0;    /* RefFrame[0]: 0 = INTRA_FRAME, 1..7 inter */
+  uint8_t skip_segment; /* bit 7: skip; bits 0..2: segment_id */
+  int8_t delta_lf[4];   /* DeltaLF[0..3] */
+} av1pf_mi;
+
+#define AV1PF_MI_SKIP 0x80u
+
+/* One loop-restoration unit (LrType, LrWiener, LrSgrSet, LrSgrXqd of
+ * decoder/mod.rs:31-41), 12 bytes. */
+typedef struct av1pf_lr_unit {
+  uint8_t type;       /* AV1PF_RESTORE_* */
+  uint8_t sgr_set;    /* 0..15 */
+  int8_t sgr_xqd[2];
+  int8_t wiener[2][3]; /* [0] vertical, [1] horizontal coefficients */
+  uint8_t _pad[2];
+} av1pf_lr_unit;
+
+/* Per-4x4 and per-unit maps the chain reads (device pointers for the device
+ * entry points). Layouts follow the reference's FrameCtx arrays
+ * (decoder/mod.rs:547-611): `mi` is row-major with row stride `mi_stride`
+ * (the reference uses mi_cols + 32); lf_tx_size[p] is indexed
+ * (row >> ssy) * mi_stride + (col >> ssx) in every plane
+ * (postfilter.rs:135); cdef_idx is one int8 per 64x64, index
+ * (r >> 4) * cdef_stride + (c >> 4), -1 = CDEF off for that 64x64
+ * (postfilter.rs:285); lr_units[p] holds unit_rows x unit_cols units. */
+typedef struct av1pf_maps {
+  const av1pf_mi* mi;
+  int32_t mi_stride;
+  int32_t cdef_stride;
+  const uint8_t* lf_tx_size[AV1PF_MAX_PLANES];
+  const int8_t* cdef_idx;
+  const av1pf_lr_unit* lr_units[AV1PF_MAX_PLANES];
+} av1pf_maps;
+
+/* Film grain parameters (FilmGrainParams, header.rs:14-45). `apply` is
+ * film_grain_params_present && apply_grain (decoder/mod.rs:865). */
+typedef struct av1pf_film_grain {
+  int32_t apply;
+  int32_t grain_seed;
+  int32_t num_y_points;
+  int32_t point_y_value[16];
+  int32_t point_y_scaling[16];
+  int32_t chroma_scaling_from_luma;
+  int32_t num_cb_points;
+  int32_t point_cb_value[16];
+  int32_t point_cb_scaling[16];
+  int32_t num_cr_points;
+  int32_t point_cr_value[16];
+  int32_t point_cr_scaling[16];
+  int32_t grain_scaling_minus_8;
+  int32_t ar_coeff_lag;
+  int32_t ar_coeffs_y_plus_128[24];
+  int32_t ar_coeffs_cb_plus_128[25];
+  int32_t ar_coeffs_cr_plus_128[25];
+  int32_t ar_coeff_shift_minus_6;
+  int32_t grain_scale_shift;
+  int32_t cb_mult, cb_luma_mult, cb_offset;
+  int32_t cr_mult, cr_luma_mult, cr_offset;
+  int32_t overlap_flag;
+  int32_t clip_to_restricted_range;
+} av1pf_film_grain;
+
+/* The frame header's filter fields (FrameHeader, header.rs:89-177) that the
+ * chain reads, plus the derived enables. */
+typedef struct av1pf_params {
+  /* loop filter (7.14): postfilter.rs:67-264 */
+  int32_t loop_filter_level[4];
+  int32_t loop_filter_sharpness;
+  int32_t loop_filter_delta_enabled;
+  int32_t loop_filter_ref_deltas[8];
+  int32_t loop_filter_mode_deltas[2];
+  int32_t delta_lf_multi;
+  int32_t segmentation_enabled;
+  uint8_t feature_enabled[8][8];
+  int32_t feature_data[8][8];
+  /* CDEF (7.15): postfilter.rs:273-342. cdef_enabled is
+   * !coded_lossless && !allow_intrabc && enable_cdef (postfilter.rs:276). */
+  int32_t cdef_enabled;
+  int32_t cdef_damping; /* 3..6 */
+  int32_t cdef_bits;
+  int32_t cdef_y_pri_strength[8];
+  int32_t cdef_y_sec_strength[8];
+  int32_t cdef_uv_pri_strength[8];
+  int32_t cdef_uv_sec_strength[8];
+  /* super-resolution (7.16): postfilter.rs:521-566 */
+  int32_t use_superres;
+  /* loop restoration (7.17): postfilter.rs:608-1004 */
+  int32_t uses_lr;
+  int32_t frame_restoration_type[3];
+  int32_t loop_restoration_size[3];
+  int32_t lr_unit_rows[3];
+  int32_t lr_unit_cols[3];
+  /* film grain (7.18.3): grain.rs */
+  av1pf_film_grain film_grain;
+} av1pf_params;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct av1pf_ctx av1pf_ctx;
+
+/* Creates a context on CUDA device `device`. `hbm_cap_bytes` bounds the
+ * device memory the context's scratch, batches and served streams may hold
+ * (0 = no cap). Replaces the reference's Decoder::new (decoder/mod.rs:273). */
+int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out);
+int av1pf_ctx_destroy(av1pf_ctx* ctx);
+
+/* Mirrors Decoder::set_threads (decoder/mod.rs:323-329): the reference's
+ * worker-thread count for the post-filter bands. On the device the bands all
+ * run at once; here `n` is the number of frames the per-frame host entry
+ * points keep in flight on separate CUDA streams (0 = default of 2). */
+int av1pf_set_threads(av1pf_ctx* ctx, int n);
+
+/* Bytes of device memory the context currently holds. */
+int av1pf_ctx_memory(const av1pf_ctx* ctx, uint64_t* bytes);
+
+/* Validates a frame descriptor, params and plane geometry without touching
+ * the device (the reference's setup_frame limits, decoder/mod.rs:501-589). */
+int av1pf_validate(const av1pf_frame_info* info, const av1pf_params* params,
+                   const av1pf_plane* planes);
+
+/* ------------------------------------------------------------------------ */
+/* Per-stage device entry points (device pointers, stream-ordered).          */
+/* ------------------------------------------------------------------------ */
+
+/* Loop filter (7.14), in place on `planes`, both passes, every plane whose
+ * level is set. Replaces loop_filter_threads (postfilter.rs:67-104). */
+int av1pf_loop_filter(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                      const av1pf_params* params, const av1pf_maps* maps,
+                      av1pf_plane* planes, void* stream);
+
+/* CDEF (7.15) from `cur` into `out` (every sample of the MI area written:
+ * filtered, or copied where CDEF is off). Replaces cdef (postfilter.rs:273),
+ * which returns a filtered clone of `cur`. */
+int av1pf_cdef(av1pf_ctx* ctx, const av1pf_frame_info* info,
+               const av1pf_params* params, const av1pf_maps* maps,
+               const av1pf_plane* cur, av1pf_plane* out, void* stream);
+
+/* Super-resolution upscaling (7.16) of `in` (coded width) into `out`
+ * (upscaled width), rows 0..round2(frame_height, ssy). Replaces upscale
+ * (postfilter.rs:521-566). Requires params->use_superres. */
+int av1pf_superres(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                   const av1pf_params* params, const av1pf_plane* in,
+                   av1pf_plane* out, void* stream);
+
+/* Loop restoration (7.17) of the upscaled CDEF frame `cdef` into `out`, with
+ * the stripe-boundary rows taken from the upscaled pre-CDEF frame `cur`
+ * (LrCtx::sample, postfilter.rs:581-597). `out` receives the whole visible
+ * area (restored units, copies elsewhere). Replaces loop_restoration
+ * (postfilter.rs:608-636). */
+int av1pf_loop_restoration(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                           const av1pf_params* params, const av1pf_maps* maps,
+                           const av1pf_plane* cur, const av1pf_plane* cdef,
+                           av1pf_plane* out, void* stream);
+
+/* Output process (7.18): crops the reference frame `ref` to
+ * upscaled_width x frame_height, applies film grain when
+ * params->film_grain.apply, and packs the planes into `frame_out` in the
+ * reference's Frame layout (frame.rs:135-192, decoder/mod.rs:893-915): Y then
+ * U then V, each plane row-major with stride = plane width, u8 samples at
+ * 8-bit and little-endian u16 above. Replaces grain::apply (grain.rs:24) plus
+ * the packing loop of Decoder::output. */
+int av1pf_output(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                 const av1pf_params* params, const av1pf_plane* ref,
+                 uint8_t* frame_out, void* stream);
+
+/* Bytes av1pf_output writes for `info`. */
+size_t av1pf_frame_bytes(const av1pf_frame_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Whole chain                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* decode_frame_wrapup's filter chain (decoder/mod.rs:748-759) plus the
+ * output process: reads the pre-filter planes `in` (left unchanged), writes
+ * the LR frame (the reference frame, RefData.frame) into `ref_out` over the
+ * visible area, and — when `frame_out` is not NULL — the packed output frame
+ * as av1pf_output does. Scratch comes from the context. */
+int av1pf_chain(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                const av1pf_params* params, const av1pf_maps* maps,
+                const av1pf_plane* in, av1pf_plane* ref_out,
+                uint8_t* frame_out, void* stream);
+
+/* av1pf_chain from HOST memory: uploads the planes and maps, runs the chain,
+ * downloads the reference frame (when ref_out is not NULL) and the packed
+ * frame (when frame_out is not NULL), and returns when they are on the host.
+ * The host-side drop-in for decode_frame_wrapup + output. Host planes use
+ * their own strides; ref_out planes must be at least visible-area sized. */
+int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                     const av1pf_params* params, const av1pf_maps* maps,
+                     const av1pf_plane* in, av1pf_plane* ref_out,
+                     uint8_t* frame_out);
+
+/* ------------------------------------------------------------------------ */
+/* Batched path: many frames of mixed shape / bit depth / subsampling, one   */
+/* persistent launch per stage, replayed from a captured CUDA graph.         */
+/* ------------------------------------------------------------------------ */
+typedef struct av1pf_job {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_maps* maps;   /* device */
+  const av1pf_plane* in;    /* device, num_planes entries */
+  av1pf_plane* ref_out;     /* device, num_planes entries */
+  uint8_t* frame_out;       /* device, or NULL */
+} av1pf_job;
+
+typedef struct av1pf_batch av1pf_batch;
+
+/* Plans a batch: validates the jobs, allocates per-frame scratch, builds the
+ * per-stage work lists and captures the stage launches into a CUDA graph.
+ * `flags`: AV1PF_BATCH_NO_GRAPH launches the stages directly. */
+#define AV1PF_BATCH_NO_GRAPH 1u
+int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs,
+                       uint32_t flags, av1pf_batch** out);
+/* Runs the planned batch on `stream` (graph launch). */
+int av1pf_batch_run(av1pf_batch* batch, void* stream);
+int av1pf_batch_destroy(av1pf_batch* batch);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: continuous batching of post-filter jobs from many streams.       */
+/* ------------------------------------------------------------------------ */
+typedef struct av1pf_server av1pf_server;
+
+typedef struct av1pf_serve_config {
+  uint64_t hbm_cap_bytes;  /* admission cap on resident stream + batch memory */
+  int32_t max_batch_frames; /* most frames one tick takes (0 = 64) */
+  int32_t inflight_batches; /* batches on the device at once (0 = 2) */
+  int32_t tick_us;          /* longest wait for more work before a tick */
+} av1pf_serve_config;
+
+/* A submitted frame: host pointers, copied at submit time. */
+typedef struct av1pf_request {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_maps* maps;  /* host */
+  const av1pf_plane* in;   /* host */
+} av1pf_request;
+
+typedef struct av1pf_serve_stats {
+  uint64_t submitted, completed, refused, batches;
+  double p50_ms, p99_ms, mean_batch_frames;
+  uint64_t resident_bytes;
+} av1pf_serve_stats;
+
+int av1pf_serve_open(av1pf_ctx* ctx, const av1pf_serve_config* cfg,
+                     av1pf_server** out);
+/* Registers a stream: its device planes and maps stay resident until
+ * av1pf_serve_close_stream. Admission is by free HBM under the cap. */
+int av1pf_serve_open_stream(av1pf_server* s, const av1pf_frame_info* info,
+                            int32_t* stream_id);
+int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id);
+/* Queues one frame of `stream_id`; returns a ticket. Never blocks on the GPU. */
+int av1pf_serve_submit(av1pf_server* s, int32_t stream_id,
+                       const av1pf_request* req, uint64_t* ticket);
+/* Waits up to `wait_ms` for `ticket`; on completion copies the packed output
+ * frame to `frame_out` (av1pf_frame_bytes bytes; may be NULL) and returns the
+ * submit->completion latency. AV1PF_ERR_TIMEOUT if not done in time. */
+int av1pf_serve_poll(av1pf_server* s, uint64_t ticket, int32_t wait_ms,
+                     uint8_t* frame_out, double* latency_ms);
+int av1pf_serve_stats_get(av1pf_server* s, av1pf_serve_stats* out);
+int av1pf_serve_close(av1pf_server* s);
+
+/* ------------------------------------------------------------------------ */
+/* DSP entry points: the reference's src/dsp post-filter kernels over many   */
+/* independent inputs at once (device pointers), for conformance tests.     */
+/* ------------------------------------------------------------------------ */
+
+/* dsp::lf::Params (lf.rs:14-21). */
+typedef struct av1pf_lf_edge_params {
+  int32_t limit, blimit, thresh;
+  int32_t filter_size; /* 4, 6, 8 or 16 */
+  int32_t chroma;
+  int32_t bit_depth;
+} av1pf_lf_edge_params;
+
+/* dsp::lf::filter (lf.rs:25) on `n` edges: edges[e*56 + k*4 + lane] is
+ * sample k (q0 at 7) of lane `lane`, filtered in place. */
+int av1pf_dsp_lf_filter(av1pf_ctx* ctx, int32_t* edges,
+                        const av1pf_lf_edge_params* params, int n, void* stream);
+
+/* dsp::cdef::Taps (cdef.rs:13-25); offsets are in a 12-wide window. */
+typedef struct av1pf_cdef_taps {
+  int32_t pri_str, sec_str, pri_adj, sec_adj;
+  int32_t pri_taps[2], sec_taps[2];
+  int32_t pri_off[2];
+  int32_t sec_off[2][2];
+  int32_t w, h; /* block: 8x8, 4x4, 4x8 or 8x4 */
+} av1pf_cdef_taps;
+
+/* dsp::cdef::filter (cdef.rs:29) on `n` windows: win[e*144 ..] is a 12x12
+ * window (INT32_MIN = unavailable), result res[e*64 ..] with row stride w. */
+int av1pf_dsp_cdef_filter(av1pf_ctx* ctx, const int32_t* win,
+                          const av1pf_cdef_taps* taps, uint16_t* res, int n,
+                          void* stream);
+
+/* Last CUDA error string seen by this thread (diagnostics). */
+const char* av1pf_last_error(void);
+
+/* Count of device kernel launches this library has issued in this process
+ * (every stage launch, graph launches counted by the kernels they hold). */
+uint64_t av1pf_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AV1PF_H */

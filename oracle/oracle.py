@@ -1,0 +1,120 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, never by the product path. The
+oracle restates rivet-av1's post-filter chain on the CPU; see oracle.h for
+what pins it.
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(ROOT, "rivet-av1_b200"))
+import av1pf as A  # noqa: E402  (structure definitions only)
+
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle`")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        vp = C.c_void_p
+
+        def sig(name, res, *args):
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = list(args)
+
+        sig("oracle_loop_filter", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), C.c_int)
+        sig("oracle_cdef", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), P(A.Plane), C.c_int)
+        sig("oracle_superres", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Plane), P(A.Plane))
+        sig("oracle_loop_restoration", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), P(A.Plane),
+            P(A.Plane), C.c_int)
+        sig("oracle_output", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Plane), vp)
+        sig("oracle_chain", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), P(A.Plane), vp, C.c_int)
+        sig("oracle_lf_filter_lanes", None, vp, vp, C.c_int)
+        sig("oracle_lf_reference", None, vp, vp, C.c_int)
+        sig("oracle_lf_kat_cases", None, C.c_uint64, C.c_int, vp, vp)
+        sig("oracle_cdef_filter", None, vp, vp, vp, C.c_int)
+        sig("oracle_cdef_kat_cases", None, C.c_uint64, C.c_int, vp, vp)
+        _lib = L
+    return _lib
+
+
+def dtype_of(info):
+    return np.uint8 if info.sample_bytes == 1 else np.uint16
+
+
+class HostPlanes:
+    """numpy-backed planes (one per plane) exposed as an av1pf_plane array."""
+
+    def __init__(self, arrays):
+        self.arrays = [np.ascontiguousarray(a) for a in arrays]
+        self.c = (A.Plane * 3)()
+        for i, a in enumerate(self.arrays):
+            self.c[i].data = a.ctypes.data
+            self.c[i].stride = a.shape[1]
+            self.c[i].width = a.shape[1]
+            self.c[i].height = a.shape[0]
+
+    @staticmethod
+    def visible(info):
+        """Zeroed planes of the visible (upscaled) area."""
+        arrs = []
+        for p in range(info.num_planes):
+            sx = info.subsampling_x if p else 0
+            sy = info.subsampling_y if p else 0
+            arrs.append(np.zeros(((info.frame_height + sy) >> sy, (info.upscaled_width + sx) >> sx), dtype_of(info)))
+        return HostPlanes(arrs)
+
+    @staticmethod
+    def like_synth(sf):
+        """Copies of a synthetic frame's pre-filter planes (allocated layout)."""
+        f = sf.f
+        arrs = []
+        for p in range(f.info.num_planes):
+            pl = f.planes[p]
+            dt = dtype_of(f.info)
+            n = pl.height * pl.stride
+            buf = (C.c_uint8 * (n * np.dtype(dt).itemsize)).from_address(pl.data)
+            arrs.append(np.frombuffer(buf, dtype=dt).reshape(pl.height, pl.stride).copy())
+        return HostPlanes(arrs)
+
+    @staticmethod
+    def zeros_like(other):
+        return HostPlanes([np.zeros_like(a) for a in other.arrays])
+
+    @staticmethod
+    def upscaled(info):
+        """Zeroed planes of the upscaled allocation (superres output)."""
+        arrs = []
+        mh = info.mi_rows * 4
+        ah = (mh + 127) & ~127
+        for p in range(info.num_planes):
+            sx = info.subsampling_x if p else 0
+            sy = info.subsampling_y if p else 0
+            w = ((info.upscaled_width + sx) >> sx) + 32
+            arrs.append(np.zeros(((ah >> sy) + 32, w), dtype_of(info)))
+        return HostPlanes(arrs)
+
+
+def chain(sf, threads=0, want_frame=True):
+    """(ref planes, packed frame bytes) of the oracle chain on a SynthHandle."""
+    info, params, maps = sf.f.info, sf.f.params, sf.f.maps
+    inp = HostPlanes.like_synth(sf)
+    ref = HostPlanes.visible(info)
+    fb = np.zeros(A.frame_bytes(info), np.uint8) if want_frame else None
+    rc = lib().oracle_chain(C.byref(info), C.byref(params), C.byref(maps), inp.c, ref.c,
+                            fb.ctypes.data if want_frame else None, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_chain: {rc}")
+    return ref, fb
