@@ -1,0 +1,457 @@
+// api.cpp — the C ABI (include/av1pf.h): context, per-stage and whole-chain
+// entry points, the host-buffer chain, and the DSP entry points.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "av1pf.h"
+#include "ctx.h"
+#include "kernels.h"
+#include "plan.h"
+
+namespace av1pf {
+
+namespace {
+std::atomic<uint64_t> g_launches{0};
+thread_local std::string t_last_error;
+std::mutex g_tables_mu;
+bool g_tables_ready[64] = {};
+}  // namespace
+
+void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void set_error(const std::string& s) { t_last_error = s; }
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return AV1PF_OK;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? AV1PF_ERR_OOM : AV1PF_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Context resources
+// ---------------------------------------------------------------------------
+int Ctx::ensure(DevBuf& b, size_t bytes) {
+  if (b.size >= bytes) return AV1PF_OK;
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    held -= b.size;
+    b.ptr = nullptr;
+    b.size = 0;
+  }
+  if (cap && held + bytes > cap) {
+    set_error("allocation would exceed the context's HBM cap");
+    return AV1PF_ERR_ADMISSION;
+  }
+  cudaError_t e = cudaMalloc(&b.ptr, bytes);
+  if (e != cudaSuccess) {
+    b.ptr = nullptr;
+    return cuda_status(e, "cudaMalloc");
+  }
+  b.size = bytes;
+  held += bytes;
+  return AV1PF_OK;
+}
+
+int Ctx::ensure_host(HostBuf& b, size_t bytes) {
+  if (b.size >= bytes) return AV1PF_OK;
+  if (b.ptr) cudaFreeHost(b.ptr);
+  b.ptr = nullptr;
+  b.size = 0;
+  cudaError_t e = cudaMallocHost(&b.ptr, bytes);
+  if (e != cudaSuccess) return cuda_status(e, "cudaMallocHost");
+  b.size = bytes;
+  return AV1PF_OK;
+}
+
+void Ctx::release(DevBuf& b) {
+  if (b.ptr) {
+    cudaFree(b.ptr);
+    held -= b.size;
+  }
+  b.ptr = nullptr;
+  b.size = 0;
+}
+
+// Plans `jobs`, sizes scratch/meta, uploads and launches on `s`.
+int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
+  std::string why;
+  int rc = build_plan(jobs, n, nullptr, plan, &why);
+  if (rc != AV1PF_OK) return set_error(why), rc;
+  if ((rc = ensure(scratch, plan.scratch_bytes + 256)) != AV1PF_OK) return rc;
+  rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why);
+  if (rc != AV1PF_OK) return set_error(why), rc;
+  if ((rc = ensure(meta, plan.meta_bytes + 256)) != AV1PF_OK) return rc;
+  // the pinned staging buffer is reused call after call: wait for the last
+  // upload from it to finish before overwriting
+  if (staged_once) {
+    cudaError_t e = cudaEventSynchronize(staged);
+    if (e != cudaSuccess) return cuda_status(e, "staging wait");
+  }
+  if ((rc = ensure_host(meta_host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
+  pack_meta(plan, static_cast<uint8_t*>(meta_host.ptr));
+  cudaError_t e = cudaMemcpyAsync(meta.ptr, meta_host.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
+  cudaEventRecord(staged, s);
+  staged_once = true;
+  launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join);
+  e = cudaGetLastError();
+  return cuda_status(e, "kernel launch");
+}
+
+}  // namespace av1pf
+
+using namespace av1pf;
+
+namespace {
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+int check_ctx(av1pf_ctx* ctx) {
+  if (!ctx) {
+    set_error("null context");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  cudaError_t e = cudaSetDevice(ctx->device);
+  return cuda_status(e, "cudaSetDevice");
+}
+
+int validate_all(const av1pf_frame_info* info, const av1pf_params* params, const av1pf_plane* planes) {
+  std::string why;
+  const int rc = validate_frame(info, params, planes, &why);
+  if (rc != AV1PF_OK) set_error(why);
+  return rc;
+}
+
+int validate_maps(const av1pf_frame_info* info, const av1pf_params* p, const av1pf_maps* m, bool need_lf,
+                  bool need_cdef, bool need_lr) {
+  if (!m) {
+    set_error("null maps");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  if ((need_lf || need_cdef) && (!m->mi || m->mi_stride < info->mi_cols)) {
+    set_error("mi map missing or mi_stride < mi_cols");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  if (need_lf)
+    for (int k = 0; k < info->num_planes; k++)
+      if (!m->lf_tx_size[k]) {
+        set_error("lf_tx_size map missing");
+        return AV1PF_ERR_INVALID_INPUT;
+      }
+  if (need_cdef && (!m->cdef_idx || m->cdef_stride < (info->mi_cols + 15) / 16)) {
+    set_error("cdef_idx missing or cdef_stride too small");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  if (need_lr && p->uses_lr)
+    for (int k = 0; k < info->num_planes; k++)
+      if (p->frame_restoration_type[k] && !m->lr_units[k]) {
+        set_error("lr_units missing");
+        return AV1PF_ERR_INVALID_INPUT;
+      }
+  return AV1PF_OK;
+}
+
+bool lf_active(const av1pf_params* p) { return p->loop_filter_level[0] || p->loop_filter_level[1]; }
+
+}  // namespace
+
+extern "C" {
+
+int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out) {
+  if (!out) return AV1PF_ERR_INVALID_INPUT;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_status(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) {
+    set_error("no such CUDA device");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+  {
+    std::lock_guard<std::mutex> lk(g_tables_mu);
+    if (device < 64 && !g_tables_ready[device]) {
+      if ((e = upload_grain_tables()) != cudaSuccess) return cuda_status(e, "grain tables");
+      g_tables_ready[device] = true;
+    }
+  }
+  av1pf_ctx* c = new av1pf_ctx();
+  c->device = device;
+  c->cap = hbm_cap_bytes;
+  if ((e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming)) != cudaSuccess) {
+    delete c;
+    return cuda_status(e, "stream/event create");
+  }
+  *out = c;
+  return AV1PF_OK;
+}
+
+int av1pf_ctx_destroy(av1pf_ctx* ctx) {
+  if (!ctx) return AV1PF_OK;
+  cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  ctx->release(ctx->scratch);
+  ctx->release(ctx->meta);
+  for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame}) ctx->release(*b);
+  if (ctx->meta_host.ptr) cudaFreeHost(ctx->meta_host.ptr);
+  cudaStreamDestroy(ctx->side);
+  cudaStreamDestroy(ctx->own);
+  cudaEventDestroy(ctx->fork);
+  cudaEventDestroy(ctx->join);
+  cudaEventDestroy(ctx->staged);
+  delete ctx;
+  return AV1PF_OK;
+}
+
+int av1pf_set_threads(av1pf_ctx* ctx, int n) {
+  if (!ctx || n < 0) return AV1PF_ERR_INVALID_INPUT;
+  ctx->threads = n == 0 ? 2 : n;
+  return AV1PF_OK;
+}
+
+int av1pf_ctx_memory(const av1pf_ctx* ctx, uint64_t* bytes) {
+  if (!ctx || !bytes) return AV1PF_ERR_INVALID_INPUT;
+  *bytes = ctx->held;
+  return AV1PF_OK;
+}
+
+int av1pf_validate(const av1pf_frame_info* info, const av1pf_params* params, const av1pf_plane* planes) {
+  return validate_all(info, params, planes);
+}
+
+size_t av1pf_frame_bytes(const av1pf_frame_info* info) { return info ? packed_frame_bytes(info) : 0; }
+
+int av1pf_loop_filter(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                      const av1pf_maps* maps, av1pf_plane* planes, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, planes))) return rc;
+  if (!lf_active(params)) return AV1PF_OK;
+  if ((rc = validate_maps(info, params, maps, true, false, false))) return rc;
+  FrameJob j{info, params, maps, planes, nullptr, planes, nullptr, ST_LF, true};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_cdef(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params, const av1pf_maps* maps,
+               const av1pf_plane* cur, av1pf_plane* out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, cur)) || (rc = validate_all(info, params, out))) return rc;
+  if ((rc = validate_maps(info, params, maps, false, params->cdef_enabled != 0, false))) return rc;
+  FrameJob j{info, params, maps, cur, nullptr, out, nullptr, ST_CDEF, false};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_superres(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                   const av1pf_plane* in, av1pf_plane* out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, in))) return rc;
+  if (!params->use_superres || !out) {
+    set_error("superres is off for this frame");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  for (int k = 0; k < info->num_planes; k++) {
+    if (!out[k].data || out[k].width < plane_w(info, k, info->upscaled_width) || out[k].height < plane_h(info, k)) {
+      set_error("superres output plane too small");
+      return AV1PF_ERR_INVALID_INPUT;
+    }
+  }
+  FrameJob j{info, params, nullptr, in, nullptr, out, nullptr, ST_SR, false};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_loop_restoration(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                           const av1pf_maps* maps, const av1pf_plane* cur, const av1pf_plane* cdef,
+                           av1pf_plane* out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, nullptr))) return rc;
+  if (!cur || !cdef || !out) {
+    set_error("null planes");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  for (int k = 0; k < info->num_planes; k++) {
+    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
+    if (!cur[k].data || !cdef[k].data || !out[k].data || cur[k].width < pw || cdef[k].width < pw ||
+        out[k].width < pw || cur[k].height < ph || cdef[k].height < ph || out[k].height < ph) {
+      set_error("loop restoration planes smaller than the visible area");
+      return AV1PF_ERR_INVALID_INPUT;
+    }
+  }
+  if ((rc = validate_maps(info, params, maps, false, false, true))) return rc;
+  FrameJob j{info, params, maps, cdef, cur, out, nullptr, ST_LR, false};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_output(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params, const av1pf_plane* ref,
+                 uint8_t* frame_out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, nullptr))) return rc;
+  if (!ref || !frame_out) {
+    set_error("null planes / output");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  FrameJob j{info, params, nullptr, ref, nullptr, nullptr, frame_out, ST_OUT, false};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_chain(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params, const av1pf_maps* maps,
+                const av1pf_plane* in, av1pf_plane* ref_out, uint8_t* frame_out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, in))) return rc;
+  if (!ref_out) {
+    set_error("null ref_out");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  for (int k = 0; k < info->num_planes; k++) {
+    if (!ref_out[k].data || ref_out[k].width < plane_w(info, k, info->upscaled_width) ||
+        ref_out[k].height < plane_h(info, k)) {
+      set_error("ref_out plane smaller than the visible area");
+      return AV1PF_ERR_INVALID_INPUT;
+    }
+  }
+  if ((rc = validate_maps(info, params, maps, lf_active(params), params->cdef_enabled != 0, true))) return rc;
+  FrameJob j{info, params, maps, in, nullptr, ref_out, frame_out, ST_CHAIN, false};
+  return ctx->run(&j, 1, as_stream(stream));
+}
+
+int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                     const av1pf_maps* maps, const av1pf_plane* in, av1pf_plane* ref_out, uint8_t* frame_out) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if ((rc = validate_all(info, params, nullptr))) return rc;
+  if (!in || !maps) {
+    set_error("null input");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  const int np = info->num_planes, sb = info->sample_bytes;
+  cudaStream_t s = ctx->own;
+  // device layout: input planes with 64-sample-aligned strides, visible-size
+  // reference planes, maps, packed frame
+  size_t in_off[3], ref_off[3], total_in = 0, total_ref = 0;
+  av1pf_plane din[3], dref[3];
+  for (int k = 0; k < np; k++) {
+    const int64_t stride = (int64_t(in[k].width) + 63) / 64 * 64;
+    in_off[k] = total_in;
+    total_in += (size_t(stride) * size_t(in[k].height) * size_t(sb) + 255) / 256 * 256;
+    din[k] = av1pf_plane{nullptr, stride, in[k].width, in[k].height};
+    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
+    const int64_t rstride = (int64_t(pw) + 63) / 64 * 64;
+    ref_off[k] = total_ref;
+    total_ref += (size_t(rstride) * size_t(ph) * size_t(sb) + 255) / 256 * 256;
+    dref[k] = av1pf_plane{nullptr, rstride, pw, ph};
+  }
+  const int sy_c = np > 1 ? info->subsampling_y : 0;
+  const size_t mi_n = size_t(info->mi_rows) * size_t(maps->mi_stride);
+  const size_t tx_rows[3] = {size_t(info->mi_rows), size_t((info->mi_rows + (1 << sy_c) - 1) >> sy_c),
+                             size_t((info->mi_rows + (1 << sy_c) - 1) >> sy_c)};
+  const size_t cdef_n = size_t((info->mi_rows + 15) / 16) * size_t(maps->cdef_stride);
+  size_t lr_n[3] = {0, 0, 0};
+  for (int k = 0; k < np; k++)
+    if (params->uses_lr && params->frame_restoration_type[k] && maps->lr_units[k])
+      lr_n[k] = size_t(params->lr_unit_rows[k]) * size_t(params->lr_unit_cols[k]);
+  size_t map_off[8], total_maps = 0;
+  auto put = [&](int slot, size_t bytes) {
+    map_off[slot] = total_maps;
+    total_maps += (bytes + 255) / 256 * 256;
+  };
+  put(0, mi_n * sizeof(av1pf_mi));
+  for (int k = 0; k < 3; k++) put(1 + k, k < np ? tx_rows[k] * size_t(maps->mi_stride) : 0);
+  put(4, cdef_n);
+  for (int k = 0; k < 3; k++) put(5 + k, lr_n[k] * sizeof(av1pf_lr_unit));
+  const size_t fbytes = packed_frame_bytes(info);
+  if ((rc = ctx->ensure(ctx->h_in, total_in)) || (rc = ctx->ensure(ctx->h_ref, total_ref)) ||
+      (rc = ctx->ensure(ctx->h_maps, total_maps)) || (rc = ctx->ensure(ctx->h_frame, fbytes + 16)))
+    return rc;
+  uint8_t* bin = static_cast<uint8_t*>(ctx->h_in.ptr);
+  uint8_t* bref = static_cast<uint8_t*>(ctx->h_ref.ptr);
+  uint8_t* bmap = static_cast<uint8_t*>(ctx->h_maps.ptr);
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < np && e == cudaSuccess; k++) {
+    din[k].data = bin + in_off[k];
+    dref[k].data = bref + ref_off[k];
+    e = cudaMemcpy2DAsync(din[k].data, size_t(din[k].stride) * sb, in[k].data, size_t(in[k].stride) * sb,
+                          size_t(in[k].width) * sb, size_t(in[k].height), cudaMemcpyHostToDevice, s);
+  }
+  av1pf_maps dm = *maps;
+  dm.mi = reinterpret_cast<const av1pf_mi*>(bmap + map_off[0]);
+  if (e == cudaSuccess && mi_n && maps->mi)
+    e = cudaMemcpyAsync(bmap + map_off[0], maps->mi, mi_n * sizeof(av1pf_mi), cudaMemcpyHostToDevice, s);
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+    dm.lf_tx_size[k] = nullptr;
+    if (k < np && maps->lf_tx_size[k]) {
+      dm.lf_tx_size[k] = bmap + map_off[1 + k];
+      e = cudaMemcpyAsync(bmap + map_off[1 + k], maps->lf_tx_size[k], tx_rows[k] * size_t(maps->mi_stride),
+                          cudaMemcpyHostToDevice, s);
+    }
+  }
+  dm.cdef_idx = nullptr;
+  if (e == cudaSuccess && maps->cdef_idx) {
+    dm.cdef_idx = reinterpret_cast<const int8_t*>(bmap + map_off[4]);
+    e = cudaMemcpyAsync(bmap + map_off[4], maps->cdef_idx, cdef_n, cudaMemcpyHostToDevice, s);
+  }
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+    dm.lr_units[k] = nullptr;
+    if (lr_n[k]) {
+      dm.lr_units[k] = reinterpret_cast<const av1pf_lr_unit*>(bmap + map_off[5 + k]);
+      e = cudaMemcpyAsync(bmap + map_off[5 + k], maps->lr_units[k], lr_n[k] * sizeof(av1pf_lr_unit),
+                          cudaMemcpyHostToDevice, s);
+    }
+  }
+  if (e != cudaSuccess) return cuda_status(e, "host-to-device copy");
+  uint8_t* dframe = frame_out ? static_cast<uint8_t*>(ctx->h_frame.ptr) : nullptr;
+  rc = av1pf_chain(ctx, info, params, &dm, din, dref, dframe, s);
+  if (rc != AV1PF_OK) return rc;
+  for (int k = 0; ref_out && k < np && e == cudaSuccess; k++) {
+    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
+    e = cudaMemcpy2DAsync(ref_out[k].data, size_t(ref_out[k].stride) * sb, dref[k].data, size_t(dref[k].stride) * sb,
+                          size_t(pw) * sb, size_t(ph), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess && frame_out) e = cudaMemcpyAsync(frame_out, dframe, fbytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "chain_host");
+  uint32_t flags = 0;
+  e = read_error_flags(&flags, s);
+  if (e != cudaSuccess) return cuda_status(e, "error flags");
+  if (flags) {
+    set_error("the maps broke a conformance requirement (bad block / transform size or edge position)");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  return AV1PF_OK;
+}
+
+int av1pf_dsp_lf_filter(av1pf_ctx* ctx, int32_t* edges, const av1pf_lf_edge_params* params, int n, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!edges || !params || n < 0) return AV1PF_ERR_INVALID_INPUT;
+  launch_dsp_lf(edges, params, n, as_stream(stream));
+  return cuda_status(cudaGetLastError(), "dsp_lf launch");
+}
+
+int av1pf_dsp_cdef_filter(av1pf_ctx* ctx, const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n,
+                          void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!win || !taps || !res || n < 0) return AV1PF_ERR_INVALID_INPUT;
+  launch_dsp_cdef(win, taps, res, n, as_stream(stream));
+  return cuda_status(cudaGetLastError(), "dsp_cdef launch");
+}
+
+const char* av1pf_last_error(void) { return t_last_error.c_str(); }
+
+uint64_t av1pf_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// desc.h — the per-frame descriptor and work-item format shared by the host
+// planner and the stage kernels (plain structs, host-safe).
+#pragma once
+
+#include <cstdint>
+
+#include "av1pf.h"
+
+namespace av1pf {
+
+// Sample planes on the device: `p` points at sample (0,0), rows `stride`
+// samples apart; samples are u8 when the frame's sample_bytes is 1, else u16.
+struct DPlane {
+  uint8_t* p;
+  int64_t stride;
+  int32_t w, h;
+};
+
+// Film-grain scratch of one frame (filled by the template kernel).
+struct GrainScratch {
+  int16_t tmpl[3][73][82];  // luma, cb, cr grain templates (7.18.3.3)
+  uint8_t lut[3][256];      // scaling lookup (7.18.3.4)
+};
+
+// Everything a stage kernel needs about one frame. Built on the host,
+// copied to device memory once per call (or once per captured batch).
+struct FrameDesc {
+  // geometry (av1pf_frame_info)
+  int32_t bd, sb, ssx, ssy, np;
+  int32_t fw, fh, uw, mi_rows, mi_cols, mc;
+  // stage buffers, per plane
+  DPlane in[3];     // pre-filter planes
+  DPlane cur[3];    // loop-filtered in place (CDEF source, pre-CDEF rows for LR)
+  DPlane cdef[3];   // after CDEF
+  DPlane up[3];     // after superres (LR source)
+  DPlane lines[3];  // upscaled pre-CDEF stripe-boundary rows (superres only)
+  DPlane ref[3];    // LR output = reference frame
+  uint8_t* frame_out;
+  int64_t out_off[3];
+  // maps (av1pf_maps)
+  const av1pf_mi* mi;
+  const uint8_t* tx[3];
+  const int8_t* cdef_idx;
+  const av1pf_lr_unit* lru[3];
+  int32_t mi_stride, cdef_stride;
+  // loop filter (7.14.4-5)
+  int32_t lf_level[4];
+  int32_t sharpness, delta_enabled, delta_lf_multi;
+  int32_t ref_deltas[8], mode_deltas[2];
+  int32_t seg_enabled;
+  int32_t seg_lf_on[8][4];
+  int32_t seg_lf_data[8][4];
+  // CDEF
+  int32_t cdef_damping;
+  int32_t cdef_y_pri[8], cdef_y_sec[8], cdef_uv_pri[8], cdef_uv_sec[8];
+  // superres (7.16): per plane step, initial position, last source column
+  int32_t sr_on;
+  int32_t sr_step[3], sr_init[3], sr_maxx[3], sr_w[3];
+  // LR
+  int32_t lr_on;
+  int32_t lr_type[3], lr_unit_size[3], lr_unit_rows[3], lr_unit_cols[3];
+  int32_t stripes;
+  // film grain
+  int32_t grain_on;
+  GrainScratch* grain;
+  uint8_t* grain_off;      // [stripe][block] random offsets (7.18.3.5)
+  int32_t grain_nb;        // blocks per stripe
+  int32_t grain_ns;        // stripes
+  av1pf_film_grain g;
+};
+
+// One unit of work of a stage: a tile of one plane of one frame.
+struct Item {
+  uint16_t frame;
+  uint8_t plane;
+  uint8_t kind;
+  uint16_t x0, y0;  // tile origin (plane samples, or stage-specific units)
+  uint16_t x1, y1;  // tile end (exclusive)
+  uint16_t a, b;    // stage-specific (LR: stripe, unit column)
+};
+static_assert(sizeof(Item) == 16, "Item is 16 bytes");
+
+}  // namespace av1pf

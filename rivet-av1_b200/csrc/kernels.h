@@ -1,0 +1,50 @@
+// kernels.h — host-side launchers of the stage kernels (internal interface
+// between the C ABI implementation and the .cu files).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "av1pf.h"
+
+namespace av1pf {
+
+struct FrameDesc;
+struct Item;
+
+// Grid cap of the grid-stride stage kernels: 8 resident CTAs on each of the
+// B200's 148 SMs.
+constexpr int kNumSMs = 148;
+constexpr int kMaxGrid = kNumSMs * 8;
+
+// Counts every kernel launch this library issues (av1pf_launch_count).
+void note_launch(uint64_t n = 1);
+
+// Loop filter (lf.cu)
+void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_v, uint64_t* list_h,
+                    uint32_t* counts, uint32_t cap, cudaStream_t s);
+void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,
+                     cudaStream_t s);
+void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s);
+
+// CDEF (cdef.cu)
+void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
+
+// Super-resolution (superres.cu)
+void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+
+// Loop restoration (lr.cu)
+void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+
+// Film grain + output packing (grain.cu)
+void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// Uploads the LFSR jump-ahead tables (once per device).
+cudaError_t upload_grain_tables();
+
+// Device error flags (g_error_flags): read and clear.
+cudaError_t read_error_flags(uint32_t* flags, cudaStream_t s);
+
+}  // namespace av1pf

@@ -1,0 +1,83 @@
+// plan.h — host-side planning of the post-filter chain: validation, the
+// per-frame scratch layout, the device descriptors and the per-stage work
+// lists. Shared by the per-frame entry points, the batched path and the
+// serving loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "av1pf.h"
+#include "desc.h"
+
+namespace av1pf {
+
+// Which stages a plan runs and where their buffers come from.
+enum StageMask : uint32_t {
+  ST_LF = 1u,
+  ST_CDEF = 2u,
+  ST_SR = 4u,
+  ST_LR = 8u,
+  ST_OUT = 16u,
+  ST_CHAIN = ST_LF | ST_CDEF | ST_SR | ST_LR | ST_OUT,
+};
+
+// One frame to plan. Planes are device pointers.
+struct FrameJob {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_maps* maps;   // device
+  const av1pf_plane* in;    // chain input / per-stage input
+  const av1pf_plane* cur;   // per-stage: LR's pre-CDEF source (may be null)
+  av1pf_plane* out;         // chain: reference frame; per-stage: the stage's output
+  uint8_t* frame_out;       // packed output or null
+  uint32_t stages;          // StageMask
+  bool in_place_lf;         // av1pf_loop_filter: filter `in` in place
+};
+
+// Work lists of every stage for a set of frames.
+struct Plan {
+  std::vector<FrameDesc> frames;
+  std::vector<Item> lf_items, cdef_items, sr_items, lr_items, grain_items, out_items, copy_items;
+  uint32_t edge_cap = 0;
+  size_t scratch_bytes = 0;   // bytes of per-frame scratch (planes, grain)
+  bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
+  // byte offsets of each list in the device meta buffer
+  size_t off_frames = 0, off_lf = 0, off_cdef = 0, off_sr = 0, off_lr = 0, off_grain = 0, off_out = 0,
+         off_copy = 0, off_edges_v = 0, off_edges_h = 0, off_counts = 0, meta_bytes = 0, upload_bytes = 0;
+};
+
+// Validation shared by av1pf_validate and every entry point.
+int validate_frame(const av1pf_frame_info* info, const av1pf_params* params, const av1pf_plane* planes,
+                   std::string* why);
+int validate_params(const av1pf_frame_info* info, const av1pf_params* p, std::string* why);
+
+// Builds the plan of `jobs`. Scratch pointers are laid out from
+// `scratch_base` (pass nullptr first to learn plan.scratch_bytes, then again
+// with the allocation). Returns AV1PF_OK or an error code.
+int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, std::string* why);
+
+// Serialises the plan's descriptors and items into `host` (plan.upload_bytes
+// long) in the layout of the device meta buffer.
+void pack_meta(const Plan& plan, uint8_t* host);
+
+// Enqueues the plan's kernels on `s`; `meta` is the device meta buffer.
+// `side`/`fork`/`join` run the grain templates concurrently when present.
+void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                 cudaEvent_t join);
+
+// Plane helpers.
+inline int plane_w(const av1pf_frame_info* i, int p, int width) {
+  const int sx = p ? i->subsampling_x : 0;
+  return (width + sx) >> sx;
+}
+inline int plane_h(const av1pf_frame_info* i, int p) {
+  const int sy = p ? i->subsampling_y : 0;
+  return (i->frame_height + sy) >> sy;
+}
+size_t packed_frame_bytes(const av1pf_frame_info* info);
+
+}  // namespace av1pf
