@@ -1,0 +1,510 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 AV1 post-filter chain (loop filter -> CDEF ->
+superres -> loop restoration -> film grain / output packing).
+
+Metric: bit-exact post-filtered Mpx/s (luma pixels upscaled_width x
+frame_height per frame, the reference's decbench convention,
+examples/av1_decbench.rs:38-50).
+
+Headline workload (one step = one frame through the chain): a single
+1920x1080 10-bit 4:2:0 frame of seeded synthetic filter-stage input (low-
+frequency field + steps on the transform grid + noise sigma 8; random
+partitions, transform sizes, loop-filter levels U[0,63], sharpness U[0,7],
+8 CDEF presets, 64x64 LR units of Wiener / self-guided). Steps rotate over
+a pool of distinct frames whose inputs total more than twice the 126 MB L2,
+so no step starts with its input in L2.
+
+The same run reports, beside the headline:
+  e2e          the same metric through av1pf_chain_host from pinned host
+               memory (input planes + maps up, packed frame down, per step);
+  stages       per-stage device time (CUDA events on the chain's stream);
+  roofline     the dominant stage's algorithmic bytes / its event time;
+  mix          the batched path (one launch per stage for 64 mixed frames,
+               replayed from a CUDA graph) against the per-frame GPU path
+               on the same frames, outputs compared bit for bit;
+  c3_4k        4K chains with superres + film grain (10-bit 4:2:0, 12-bit 4:4:4);
+  cpu_baseline the CPU oracle (this repo's C++ restatement of the reference's
+               filters, all host threads) on a bounded sample.
+
+Multi-GPU (torchrun): replicas only — each rank runs its own frames, no
+collective on the data path; value = all ranks' pixels / max-over-ranks time.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "rivet-av1_b200"), os.path.join(ROOT, "tests")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+import av1pf as A  # noqa: E402
+
+METRIC = "bit-exact post-filtered Mpx/s"
+HEADLINE = dict(width=1920, height=1080, bit_depth=10)
+L2_BYTES = 126 * 2**20
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def plane_set_bytes(info, upscaled=True):
+    """S: visible plane-set bytes at the native sample width."""
+    w = info.upscaled_width if upscaled else info.frame_width
+    n = 0
+    for p in range(info.num_planes):
+        sx = info.subsampling_x if p else 0
+        sy = info.subsampling_y if p else 0
+        n += ((w + sx) >> sx) * ((info.frame_height + sy) >> sy)
+    return n * (2 if info.bit_depth > 8 else 1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU implementation of the path (the oracle port)
+# ---------------------------------------------------------------------------
+def cpu_rate(cfgs, budget_s, threads=0):
+    """Mpx/s of the CPU oracle over the frames of `cfgs` (cycled) for about
+    budget_s seconds of work; returns (Mpx/s, frames, seconds, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sfs = [A.SynthHandle(**c) for c in cfgs]
+    cores = os.cpu_count() if threads == 0 else threads
+    t0 = time.perf_counter()
+    px = 0
+    n = 0
+    while True:
+        sf = sfs[n % len(sfs)]
+        O.chain(sf, threads=threads)
+        px += sf.info.upscaled_width * sf.info.frame_height
+        n += 1
+        el = time.perf_counter() - t0
+        if (el >= budget_s and n >= 2) or el > 3 * budget_s:
+            break
+    return px / el / 1e6, n, el, cores
+
+
+def reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    cfg = dict(HEADLINE, seed=1)
+    steps, warm = args.steps, args.warmup
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sf = A.SynthHandle(**cfg)
+    for _ in range(warm):
+        O.chain(sf, threads=0)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.chain(sf, threads=0)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    mpx = 1920 * 1080 * steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(mpx, 3), "unit": "Mpx/s", "n_gpus": world,
+        "steps": steps, "warmup": warm, "ms_per_step": round(1e3 * total / steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+CDEF+LR)",
+                   "frames_per_step": 1},
+        "cpu_baseline": {"value": round(mpx, 3), "unit": "Mpx/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{steps} timed frames of the workload after {warm} warm-up, all host threads"},
+        "e2e": {"value": round(mpx, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main_gpu(args):
+    import torch
+    import gpu_util as G
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as D
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = D
+    L = A.lib()
+    ctx = G.Ctx(local)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- headline pool: distinct frames whose inputs exceed 2x L2 ----
+    probe = A.SynthHandle(**HEADLINE, seed=1)
+    in_bytes = sum(probe.f.plane_bytes[p] for p in range(3))
+    pool_n = max(8, int(2 * L2_BYTES / in_bytes) + 1)
+    del probe
+    sfs = [A.SynthHandle(**HEADLINE, seed=1000 * (rank + 1) + i) for i in range(pool_n)]
+    dfs = [G.DevFrame(s) for s in sfs]
+    outs = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
+
+    def step(i):
+        d = dfs[i % pool_n]
+        r, fb = outs[i % pool_n]
+        rc = L.av1pf_chain(ctx.p, C.byref(d.info), C.byref(d.params), C.byref(d.maps), d.inp.c, r.c,
+                           fb.data_ptr(), None)
+        if rc:
+            A.check(rc, "av1pf_chain")
+
+    # bit-exactness of the measured path: one pool frame against the oracle
+    exact = None
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        ref_cpu, fb_cpu = O.chain(sfs[0], threads=0)
+        step(0)
+        torch.cuda.synchronize()
+        exact = bool(np.array_equal(outs[0][1][: A.frame_bytes(dfs[0].info)].cpu().numpy(), fb_cpu) and all(
+            np.array_equal(outs[0][0].host(p), ref_cpu.arrays[p]) for p in range(3)))
+
+    for i in range(args.warmup):
+        step(i)
+    L.av1pf_set_profiling(ctx.p, 1)
+    ms5 = (C.c_float * 5)()
+    calls = C.c_uint32()
+    L.av1pf_stage_times(ctx.p, ms5, C.byref(calls))  # reset
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.5)  # let nvidia-smi start sampling before the timed region
+    barrier()
+    launches0 = L.av1pf_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    e1.record()
+    barrier()
+    launches = L.av1pf_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    L.av1pf_stage_times(ctx.p, ms5, C.byref(calls))
+    L.av1pf_set_profiling(ctx.p, 0)
+    ms_max = max_over_ranks(ms)
+    px_frame = 1920 * 1080
+    value = world * args.steps * px_frame / (ms_max / 1e3) / 1e6
+    stage_names = ["loop_filter", "cdef", "superres", "loop_restoration", "output"]
+    stage_ms = {n: float(ms5[k]) / max(1, calls.value) for k, n in enumerate(stage_names)}
+
+    # ---- roofline of the dominant stage ----
+    info = dfs[0].info
+    S = plane_set_bytes(info)
+    algo = {"loop_filter": 2 * S, "cdef": 2 * S, "superres": 2 * S, "loop_restoration": 2 * S,
+            "output": 2 * S}
+    dom = max(stage_ms, key=stage_ms.get)
+    peak, peak_kind = peaks()
+    achieved = algo[dom] / (stage_ms[dom] / 1e3) / 1e9
+    chain_bytes = S + S + plane_set_bytes(info)  # input + reference frame + packed output
+    result = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+CDEF+LR+pack)",
+                   "frames_per_step": 1, "pool_frames": pool_n,
+                   "l2": f"inputs rotate over {pool_n} distinct frames ({pool_n * in_bytes / 2**20:.0f} MiB > 2x L2)",
+                   "parallelism": f"replicas x{world}"},
+        "bit_exact_vs_oracle": exact,
+        "gpu_launches": int(launches),
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "algorithmic_bytes": int(algo[dom]), "traffic": None,
+                     "chain_frac": round(chain_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak, 4)},
+        "clocks": clocks,
+    }
+
+    # ---- e2e through the host-buffer entry point (pinned host memory) ----
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    hosts = []
+    for s in sfs[: min(pool_n, 8)]:
+        hp = O.HostPlanes.like_synth(s)
+        pinned = [torch.from_numpy(a.view(np.uint8).reshape(-1)).pin_memory() for a in hp.arrays]
+        planes = (A.Plane * 3)()
+        for p, (a, t) in enumerate(zip(hp.arrays, pinned)):
+            planes[p].data = t.data_ptr()
+            planes[p].stride = a.shape[1]
+            planes[p].width = a.shape[1]
+            planes[p].height = a.shape[0]
+        f = s.f
+        m = A.Maps()
+        m.mi_stride, m.cdef_stride = f.maps.mi_stride, f.maps.cdef_stride
+        keep = []
+
+        def pin(ptr, n):
+            t = torch.from_numpy(np.frombuffer((C.c_uint8 * n).from_address(ptr), np.uint8).copy()).pin_memory()
+            keep.append(t)
+            return t.data_ptr()
+        m.mi = pin(f.maps.mi, f.mi_count * 8)
+        for p in range(3):
+            if f.maps.lf_tx_size[p]:
+                m.lf_tx_size[p] = pin(f.maps.lf_tx_size[p], f.tx_count[p])
+            if f.maps.lr_units[p] and f.lr_count[p]:
+                m.lr_units[p] = pin(f.maps.lr_units[p], f.lr_count[p] * 12)
+        m.cdef_idx = pin(f.maps.cdef_idx, f.cdef_count)
+        fb = torch.empty(A.frame_bytes(f.info), dtype=torch.uint8).pin_memory()
+        hosts.append((s, pinned, planes, m, keep, fb))
+    mi_rows = info.mi_rows
+    h2d = sum(hosts[0][0].f.plane_bytes[p] for p in range(3)) + mi_rows * hosts[0][3].mi_stride * 8 + \
+        sum((mi_rows >> (1 if p else 0)) * hosts[0][3].mi_stride for p in range(3)) + \
+        ((mi_rows + 15) // 16) * hosts[0][3].cdef_stride + sum(hosts[0][0].f.lr_count[p] * 12 for p in range(3))
+    d2h = A.frame_bytes(info)
+
+    def e2e_step(i):
+        s, pinned, planes, m, keep, fb = hosts[i % len(hosts)]
+        A.check(L.av1pf_chain_host(ctx.p, C.byref(s.f.info), C.byref(s.f.params), C.byref(m), planes, None,
+                                   fb.data_ptr()), "chain_host")
+
+    e2e_steps = min(args.steps, 1000)
+    for i in range(args.warmup):
+        e2e_step(i)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        e2e_step(i)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    # the host path returns the same bytes as the device path
+    e2e_exact = bool(np.array_equal(hosts[0][5].numpy(), outs[0][1][: A.frame_bytes(info)].cpu().numpy()))
+    result["e2e"] = {"value": round(world * e2e_steps * px_frame / e2e_s / 1e6, 2), "unit": "Mpx/s",
+                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                     "ms_per_step": round(1e3 * e2e_s / e2e_steps, 3), "bit_exact_vs_device_path": e2e_exact}
+    del hosts
+
+    # ---- batched vs per-frame on the mixed-resolution batch ----
+    if not args.skip_extras:
+        result["mix"] = bench_mix(args, ctx, rank, barrier, max_over_ranks)
+        result["c3_4k"] = bench_4k(args, ctx, barrier, max_over_ranks)
+
+    # ---- CPU baseline (rank 0, N = 1) ----
+    if rank == 0 and world == 1:
+        rate, n, el, cores = cpu_rate([dict(HEADLINE, seed=1000 + i) for i in range(4)], args.cpu_seconds)
+        result["cpu_baseline"] = {"value": round(rate, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
+                                  "sample": f"{n} frames of the headline workload in {el:.1f} s, "
+                                            f"CPU oracle on all host threads"}
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    return 0
+
+
+MIX = [(16, dict(width=640, height=360, bit_depth=8, sample_bytes=1)),
+       (16, dict(width=960, height=540, bit_depth=8, sample_bytes=1)),
+       (16, dict(width=1280, height=720, bit_depth=8, sample_bytes=1)),
+       (12, dict(width=1920, height=1080, bit_depth=10)),
+       (4, dict(width=3840, height=2160, bit_depth=10, subsampling_x=0, subsampling_y=0))]
+
+
+def bench_mix(args, ctx, rank, barrier, max_over_ranks):
+    """64 mixed frames: per-frame chain calls vs one batch replayed from a graph."""
+    import torch
+    import gpu_util as G
+    L = A.lib()
+    sfs = []
+    k = 0
+    for count, cfg in MIX:
+        for _ in range(count):
+            sfs.append(A.SynthHandle(**cfg, seed=5000 + 100 * rank + k, frame_index=k))
+            k += 1
+    dfs = [G.DevFrame(s) for s in sfs]
+    out_a = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
+    out_b = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
+    px = sum(s.info.upscaled_width * s.info.frame_height for s in sfs)
+
+    def per_frame():
+        for d, (r, fb) in zip(dfs, out_a):
+            A.check(L.av1pf_chain(ctx.p, C.byref(d.info), C.byref(d.params), C.byref(d.maps), d.inp.c, r.c,
+                                  fb.data_ptr(), None))
+
+    jobs = (A.Job * len(dfs))()
+    for i, (d, (r, fb)) in enumerate(zip(dfs, out_b)):
+        jobs[i].info = C.pointer(d.info)
+        jobs[i].params = C.pointer(d.params)
+        jobs[i].maps = C.pointer(d.maps)
+        jobs[i].inp = C.cast(d.inp.c, C.POINTER(A.Plane))
+        jobs[i].ref_out = C.cast(r.c, C.POINTER(A.Plane))
+        jobs[i].frame_out = fb.data_ptr()
+    b = C.c_void_p()
+    A.check(L.av1pf_batch_create(ctx.p, jobs, len(dfs), 0, C.byref(b)), "batch_create")
+
+    def timed(fn, reps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)) / reps
+
+    reps = max(3, min(20, args.steps // 4))
+    t_pf = timed(per_frame, reps)
+    t_b = timed(lambda: A.check(L.av1pf_batch_run(b, None)), reps)
+    exact = all(np.array_equal(ra.host(p), rb.host(p)) and bool(torch.equal(fa, fb))
+                for (ra, fa), (rb, fb), d in zip(out_a, out_b, dfs) for p in range(d.info.num_planes))
+    A.lib().av1pf_batch_destroy(b)
+    return {"frames": len(dfs), "mpx_per_batch": round(px / 1e6, 3),
+            "per_frame_mpx_s": round(px / (t_pf / 1e3) / 1e6, 1), "batched_mpx_s": round(px / (t_b / 1e3) / 1e6, 1),
+            "speedup": round(t_pf / t_b, 3), "per_frame_ms": round(t_pf, 3), "batched_ms": round(t_b, 3),
+            "bit_exact_batched_vs_per_frame": bool(exact)}
+
+
+def bench_4k(args, ctx, barrier, max_over_ranks):
+    """4K chains with superres (denominator 13 / 10) and film grain."""
+    import torch
+    import gpu_util as G
+    L = A.lib()
+    res = {}
+    for name, cfg in [("10bit_420_superres_grain", dict(width=3840, height=2160, bit_depth=10, superres_denom=13,
+                                                         enable_grain=1, seed=77, frame_index=3)),
+                      ("12bit_444_superres_grain", dict(width=3840, height=2160, bit_depth=12, subsampling_x=0,
+                                                         subsampling_y=0, superres_denom=10, enable_grain=1,
+                                                         seed=78, frame_index=4))]:
+        sfs = [A.SynthHandle(**dict(cfg, seed=cfg["seed"] + i)) for i in range(3)]
+        dfs = [G.DevFrame(s) for s in sfs]
+        outs = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
+
+        def run(i):
+            d = dfs[i % 3]
+            r, fb = outs[i % 3]
+            A.check(L.av1pf_chain(ctx.p, C.byref(d.info), C.byref(d.params), C.byref(d.maps), d.inp.c, r.c,
+                                  fb.data_ptr(), None))
+        for i in range(args.warmup):
+            run(i)
+        L.av1pf_set_profiling(ctx.p, 1)
+        ms5 = (C.c_float * 5)()
+        calls = C.c_uint32()
+        L.av1pf_stage_times(ctx.p, ms5, C.byref(calls))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(3, min(60, args.steps // 2))
+        e0.record()
+        for i in range(reps):
+            run(i)
+        e1.record()
+        barrier()
+        L.av1pf_stage_times(ctx.p, ms5, C.byref(calls))
+        L.av1pf_set_profiling(ctx.p, 0)
+        ms = max_over_ranks(e0.elapsed_time(e1)) / reps
+        info = dfs[0].info
+        chain_bytes = plane_set_bytes(info, upscaled=False) + 2 * plane_set_bytes(info)
+        peak, _ = peaks()
+        res[name] = {"ms_per_frame": round(ms, 4), "mpx_s": round(3840 * 2160 / (ms / 1e3) / 1e6, 1),
+                     "chain_hbm_frac": round(chain_bytes / (ms / 1e3) / 1e9 / peak, 4),
+                     "stages_ms": {n: round(float(ms5[k]) / max(1, calls.value), 4)
+                                   for k, n in enumerate(["loop_filter", "cdef", "superres", "loop_restoration",
+                                                          "output"])}}
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-extras", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return main_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

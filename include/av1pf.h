@@ -380,6 +380,16 @@ int av1pf_dsp_cdef_filter(av1pf_ctx* ctx, const int32_t* win,
                           const av1pf_cdef_taps* taps, uint16_t* res, int n,
                           void* stream);
 
+/* Per-stage device timing of the per-frame entry points (diagnostics). When
+ * on, every av1pf_chain / per-stage call records CUDA events on its stream
+ * between stages. */
+int av1pf_set_profiling(av1pf_ctx* ctx, int on);
+/* Sums, in milliseconds, of the stage times of every profiled call since the
+ * last read: [0] loop filter, [1] CDEF, [2] superres, [3] loop restoration,
+ * [4] output (film grain + packing); *calls = number of calls summed. Waits
+ * for those calls to finish, then resets the sums. */
+int av1pf_stage_times(av1pf_ctx* ctx, float ms[5], uint32_t* calls);
+
 /* Last CUDA error string seen by this thread (diagnostics). */
 const char* av1pf_last_error(void);
 

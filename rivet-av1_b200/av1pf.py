@@ -178,6 +178,8 @@ def lib():
         _sig(L, "av1pf_serve_close", C.c_int, vp)
         _sig(L, "av1pf_dsp_lf_filter", C.c_int, vp, vp, vp, C.c_int, vp)
         _sig(L, "av1pf_dsp_cdef_filter", C.c_int, vp, vp, vp, vp, C.c_int, vp)
+        _sig(L, "av1pf_set_profiling", C.c_int, vp, C.c_int)
+        _sig(L, "av1pf_stage_times", C.c_int, vp, P(C.c_float), P(C.c_uint32))
         _sig(L, "av1pf_last_error", C.c_char_p)
         _sig(L, "av1pf_launch_count", C.c_uint64)
         _lib = L

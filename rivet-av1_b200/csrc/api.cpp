@@ -99,9 +99,29 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
   cudaEventRecord(staged, s);
   staged_once = true;
-  launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join);
+  const cudaEvent_t* ev = nullptr;
+  if (prof) {
+    const int slot = prof_next;
+    prof_next = (prof_next + 1) % kProfSlots;
+    if (prof_used[slot]) prof_collect(slot);
+    if (!prof_ev[slot][0])
+      for (int k = 0; k < 6; k++) cudaEventCreate(&prof_ev[slot][k]);
+    prof_used[slot] = true;
+    ev = prof_ev[slot];
+  }
+  launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join, ev);
   e = cudaGetLastError();
   return cuda_status(e, "kernel launch");
+}
+
+void Ctx::prof_collect(int slot) {
+  cudaEventSynchronize(prof_ev[slot][5]);
+  for (int k = 0; k < 5; k++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, prof_ev[slot][k], prof_ev[slot][k + 1]) == cudaSuccess) prof_ms[k] += ms;
+  }
+  prof_calls++;
+  prof_used[slot] = false;
 }
 
 }  // namespace av1pf
@@ -209,6 +229,9 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   cudaEventDestroy(ctx->fork);
   cudaEventDestroy(ctx->join);
   cudaEventDestroy(ctx->staged);
+  for (auto& slot : ctx->prof_ev)
+    for (auto& e : slot)
+      if (e) cudaEventDestroy(e);
   delete ctx;
   return AV1PF_OK;
 }
@@ -448,6 +471,26 @@ int av1pf_dsp_cdef_filter(av1pf_ctx* ctx, const int32_t* win, const av1pf_cdef_t
   if (!win || !taps || !res || n < 0) return AV1PF_ERR_INVALID_INPUT;
   launch_dsp_cdef(win, taps, res, n, as_stream(stream));
   return cuda_status(cudaGetLastError(), "dsp_cdef launch");
+}
+
+int av1pf_set_profiling(av1pf_ctx* ctx, int on) {
+  if (!ctx) return AV1PF_ERR_INVALID_INPUT;
+  ctx->prof = on != 0;
+  return AV1PF_OK;
+}
+
+int av1pf_stage_times(av1pf_ctx* ctx, float ms[5], uint32_t* calls) {
+  if (!ctx || !ms) return AV1PF_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  for (int k = 0; k < Ctx::kProfSlots; k++)
+    if (ctx->prof_used[k]) ctx->prof_collect(k);
+  for (int k = 0; k < 5; k++) {
+    ms[k] = float(ctx->prof_ms[k]);
+    ctx->prof_ms[k] = 0;
+  }
+  if (calls) *calls = ctx->prof_calls;
+  ctx->prof_calls = 0;
+  return AV1PF_OK;
 }
 
 const char* av1pf_last_error(void) { return t_last_error.c_str(); }

@@ -33,7 +33,7 @@ extern __device__ int16_t g_gaussian[2048];
 // LFSR jump-ahead (7.18.3.2): column b of M^(82r) / M^(44r) is the state
 // reached from state 1<<b after 82r / 44r steps.
 extern __device__ uint16_t g_rng_jump82[73][16];
-extern __device__ uint16_t g_rng_jump44[38][16];
+extern __device__ uint16_t g_rng_jump44[73][16];
 // Sticky device-side error bits (bad map values met by a kernel).
 extern __device__ uint32_t g_error_flags;
 enum : uint32_t { ERRF_BAD_MAP = 1u, ERRF_BAD_ITEM = 2u };

@@ -34,6 +34,15 @@ struct Ctx {
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
   HostBuf meta_host;
   Plan plan;
+  // profiling: a ring of event sets, one per profiled call
+  static constexpr int kProfSlots = 64;
+  bool prof = false;
+  cudaEvent_t prof_ev[kProfSlots][6] = {};
+  bool prof_used[kProfSlots] = {};
+  int prof_next = 0;
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  uint32_t prof_calls = 0;
+  void prof_collect(int slot);
 
   int ensure(DevBuf& b, size_t bytes);
   int ensure_host(HostBuf& b, size_t bytes);

@@ -440,7 +440,10 @@ void pack_meta(const Plan& plan, uint8_t* host) {
 }
 
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join) {
+                 cudaEvent_t join, const cudaEvent_t* stage_ev) {
+  auto mark = [&](int k) {
+    if (stage_ev) cudaEventRecord(stage_ev[k], s);
+  };
   const FrameDesc* frames = reinterpret_cast<const FrameDesc*>(meta + plan.off_frames);
   auto items = [&](size_t off) { return reinterpret_cast<const Item*>(meta + off); };
   uint64_t* ev = reinterpret_cast<uint64_t*>(meta + plan.off_edges_v);
@@ -453,6 +456,7 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     launch_grain_prep(frames, items(plan.off_grain), int(plan.grain_items.size()), side);
     cudaEventRecord(join, side);
   }
+  mark(0);
   if (!plan.copy_items.empty()) {
     cudaMemsetAsync(counts, 0, 16, s);
     launch_lf_prep(frames, items(plan.off_copy), int(plan.copy_items.size()), ev, eh, counts, 0, s);
@@ -463,13 +467,18 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     launch_lf_edges(0, frames, ev, counts + 0, plan.edge_cap, s);
     launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
+  mark(1);
   if (plan.any_cdef) launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), s);
+  mark(2);
   if (plan.any_sr) launch_superres(frames, items(plan.off_sr), int(plan.sr_items.size()), s);
+  mark(3);
   if (plan.any_lr) launch_lr(frames, items(plan.off_lr), int(plan.lr_items.size()), s);
+  mark(4);
   if (plan.any_out) {
     if (plan.any_grain) cudaStreamWaitEvent(s, join, 0);
     launch_output(frames, items(plan.off_out), int(plan.out_items.size()), s);
   }
+  mark(5);
 }
 
 }  // namespace av1pf

@@ -66,8 +66,10 @@ void pack_meta(const Plan& plan, uint8_t* host);
 
 // Enqueues the plan's kernels on `s`; `meta` is the device meta buffer.
 // `side`/`fork`/`join` run the grain templates concurrently when present.
+// `stage_ev`, when not null, holds 6 events recorded before the loop
+// filter and after each of the 5 stages (for av1pf_stage_times).
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join);
+                 cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr);
 
 // Plane helpers.
 inline int plane_w(const av1pf_frame_info* i, int p, int width) {

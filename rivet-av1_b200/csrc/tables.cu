@@ -18,7 +18,7 @@ __constant__ int32_t c_sgr_params[16][4] = AV1T_SGR_PARAMS;
 __device__ int16_t g_upscale_filter[64][8] = AV1T_UPSCALE_FILTER;
 __device__ int16_t g_gaussian[2048] = AV1T_GAUSSIAN_SEQUENCE;
 __device__ uint16_t g_rng_jump82[73][16];
-__device__ uint16_t g_rng_jump44[38][16];
+__device__ uint16_t g_rng_jump44[73][16];
 __device__ uint32_t g_error_flags;
 
 // LFSR of 7.18.3.2 as a GF(2) matrix: column b of M^n is the state reached
@@ -28,7 +28,7 @@ cudaError_t upload_grain_tables() {
     const uint32_t bit = (r ^ (r >> 1) ^ (r >> 3) ^ (r >> 12)) & 1u;
     return (r >> 1) | (bit << 15);
   };
-  uint16_t j82[73][16], j44[38][16];
+  uint16_t j82[73][16], j44[73][16];
   for (int b = 0; b < 16; b++) {
     uint32_t s = 1u << b;
     for (int r = 0; r < 73; r++) {
@@ -36,7 +36,7 @@ cudaError_t upload_grain_tables() {
       for (int k = 0; k < 82; k++) s = step(s);
     }
     s = 1u << b;
-    for (int r = 0; r < 38; r++) {
+    for (int r = 0; r < 73; r++) {
       j44[r][b] = uint16_t(s);
       for (int k = 0; k < 44; k++) s = step(s);
     }
