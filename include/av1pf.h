@@ -254,6 +254,27 @@ int av1pf_output(av1pf_ctx* ctx, const av1pf_frame_info* info,
 /* Bytes av1pf_output writes for `info`. */
 size_t av1pf_frame_bytes(const av1pf_frame_info* info);
 
+/* av1pf_output for callers that cannot allocate device memory — a decoder
+ * embedded in a host whose device memory belongs to another allocator, or a
+ * real-time output path that cannot take an allocation's latency or an
+ * out-of-memory failure mid-stream. No counterpart in the reference (its
+ * output process allocates freely on the host).
+ *
+ * It takes no context and allocates nothing: its scratch (descriptor, work
+ * list, film-grain templates and block offsets) is one fixed device array of
+ * about 260 KB inside libav1pf, which every GPU that loads the library holds
+ * until the process exits. Limit: with film grain on, frames up to
+ * ceil(upscaled_width/32) * ceil(frame_height/32) <= 65536 (e.g. 8192x8192);
+ * larger frames are refused with AV1PF_ERR_UNSUPPORTED. Runs on the current
+ * device. The first call on a device does a one-time set-up there (looks up
+ * the array's device address, uploads the grain RNG tables); make that first
+ * call before any stream capture. Every call shares the one array, and each
+ * call rewrites all of it that it reads, so nothing depends on earlier
+ * contents; calls that overlap on the GPU (different streams, or several
+ * host threads at once) race on it — issue them on one stream. */
+int av1pf_output_noalloc(const av1pf_frame_info* info, const av1pf_params* params,
+                         const av1pf_plane* ref, uint8_t* frame_out, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Whole chain                                                               */
 /* ------------------------------------------------------------------------ */

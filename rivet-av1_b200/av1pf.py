@@ -164,6 +164,7 @@ def lib():
              P(Plane), vp)
         _sig(L, "av1pf_output", C.c_int, vp, P(FrameInfo), P(Params), P(Plane), vp, vp)
         _sig(L, "av1pf_frame_bytes", C.c_size_t, P(FrameInfo))
+        _sig(L, "av1pf_output_noalloc", C.c_int, P(FrameInfo), P(Params), P(Plane), vp, vp)
         _sig(L, "av1pf_chain", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp, vp)
         _sig(L, "av1pf_chain_host", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp)
         _sig(L, "av1pf_batch_create", C.c_int, vp, P(Job), C.c_int, C.c_uint32, P(vp))
