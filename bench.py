@@ -363,6 +363,7 @@ def main_gpu(args):
     if not args.skip_extras:
         result["mix"] = bench_mix(args, ctx, rank, barrier, max_over_ranks)
         result["c3_4k"] = bench_4k(args, ctx, barrier, max_over_ranks)
+        result["serve"] = bench_serve(args, ctx, rank)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     if rank == 0 and world == 1:
@@ -488,6 +489,168 @@ def bench_4k(args, ctx, barrier, max_over_ranks):
                                    for k, n in enumerate(["loop_filter", "cdef", "superres", "loop_restoration",
                                                           "output"])}}
     return res
+
+
+SERVE_MIX = [(8, dict(width=640, height=360, bit_depth=8, sample_bytes=1)),
+             (8, dict(width=960, height=540, bit_depth=8, sample_bytes=1)),
+             (8, dict(width=1280, height=720, bit_depth=8, sample_bytes=1)),
+             (6, dict(width=1920, height=1080, bit_depth=10)),
+             (2, dict(width=3840, height=2160, bit_depth=10, subsampling_x=0, subsampling_y=0))]
+
+
+def bench_serve(args, ctx, rank, duration_s=1.0):
+    """Config 5: 32 streams (config 4's resolution mix) at 24-60 fps each,
+    seeded Poisson arrivals over `duration_s`. Two feeds are measured through
+    the serving loop: frames arriving in host memory (uploaded by the server)
+    and frames already resident on the device (as a GPU decoder leaves them).
+    Each is compared with the plain per-frame path on the same frame sequence
+    (av1pf_chain_host / av1pf_chain, one call per frame), and the serving loop
+    is also run saturated (every frame of the sequence submitted at once).
+    Latency is submit -> completion of the batch that carried the frame."""
+    import threading
+    import torch
+    import gpu_util as G
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    L = A.lib()
+    rng = np.random.default_rng(2024 + rank)
+    streams = []
+    k = 0
+    for count, cfg in SERVE_MIX:
+        for _ in range(count):
+            frames = [A.SynthHandle(**cfg, seed=9000 + 100 * rank + 10 * k + j, frame_index=j) for j in range(2)]
+            host = [O.HostPlanes.like_synth(sf) for sf in frames]
+            dev = [G.DevFrame(sf) for sf in frames]
+            outs = [(G.DevPlanes.visible(sf.f.info), G.dev_bytes(A.frame_bytes(sf.f.info))) for sf in frames]
+            hreq, dreq = [], []
+            for sf, hp, df, (r_out, f_out) in zip(frames, host, dev, outs):
+                r = A.Request()
+                r.info, r.params, r.maps = C.pointer(sf.f.info), C.pointer(sf.f.params), C.pointer(sf.f.maps)
+                r.inp = C.cast(hp.c, C.POINTER(A.Plane))
+                hreq.append(r)
+                d = A.Request()
+                d.info, d.params, d.maps = C.pointer(df.info), C.pointer(df.params), C.pointer(df.maps)
+                d.inp = C.cast(df.inp.c, C.POINTER(A.Plane))
+                d.device = 1
+                d.ref_out = C.cast(r_out.c, C.POINTER(A.Plane))
+                d.frame_out = f_out.data_ptr()
+                dreq.append(d)
+            streams.append({"frames": frames, "host": host, "dev": dev, "outs": outs, "hreq": hreq, "dreq": dreq,
+                            "fps": float(rng.uniform(24, 60))})
+            k += 1
+    arrivals = []
+    for si, st in enumerate(streams):
+        t, j = float(rng.exponential(1.0 / st["fps"])), 0
+        while t < duration_s:
+            arrivals.append((t, si, j % 2))
+            t += float(rng.exponential(1.0 / st["fps"]))
+            j += 1
+    arrivals.sort()
+    n = len(arrivals)
+    px = sum(streams[si]["frames"][j].info.upscaled_width * streams[si]["frames"][j].info.frame_height
+             for (_, si, j) in arrivals)
+    cfg = A.ServeConfig(40 << 30, 64, 2, 50)
+    srv = C.c_void_p()
+    A.check(L.av1pf_serve_open(ctx.p, C.byref(cfg), C.byref(srv)), "serve_open")
+    for st in streams:
+        sid = C.c_int32()
+        A.check(L.av1pf_serve_open_stream(srv, C.byref(st["frames"][0].f.info), C.byref(sid)), "open_stream")
+        st["sid"] = sid.value
+
+    def run(kind, paced, keep_out=None):
+        """Submits the arrival sequence (paced by arrival time or all at once)
+        while a second thread polls completions in order."""
+        import queue as Q
+        pending = Q.Queue()
+        lats = []
+
+        def poller():
+            while True:
+                item = pending.get()
+                if item is None:
+                    return
+                tk, si, j = item
+                fb = None
+                if kind == "hreq":
+                    fb = np.empty(A.frame_bytes(streams[si]["frames"][j].f.info), np.uint8)
+                lat = C.c_double()
+                A.check(L.av1pf_serve_poll(srv, tk, 120000, fb.ctypes.data if fb is not None else None,
+                                           C.byref(lat)), "poll")
+                lats.append(lat.value)
+                if keep_out is not None and fb is not None:
+                    keep_out.setdefault((si, j), fb)
+        th = threading.Thread(target=poller)
+        th.start()
+        t0 = time.perf_counter()
+        for (ta, si, j) in arrivals:
+            if paced:
+                while time.perf_counter() - t0 < ta:
+                    time.sleep(0.0001)
+            tk = C.c_uint64()
+            A.check(L.av1pf_serve_submit(srv, streams[si]["sid"], C.byref(streams[si][kind][j]), C.byref(tk)),
+                    "submit")
+            pending.put((tk.value, si, j))
+        pending.put(None)
+        th.join()
+        wall = time.perf_counter() - t0
+        return wall, lats
+
+    run("hreq", False)  # warm-up: pinned pools, scratch
+    run("dreq", False)
+    b0 = A.ServeStats()
+    A.check(L.av1pf_serve_stats_get(srv, C.byref(b0)))
+    outs = {}
+    w_h, lat_h = run("hreq", True, outs)
+    b1 = A.ServeStats()
+    A.check(L.av1pf_serve_stats_get(srv, C.byref(b1)))
+    w_d, lat_d = run("dreq", True)
+    s_h, _ = run("hreq", False)
+    s_d, _ = run("dreq", False)
+    b2 = A.ServeStats()
+    A.check(L.av1pf_serve_stats_get(srv, C.byref(b2)))
+    A.check(L.av1pf_serve_close(srv))
+    # the plain per-frame paths on the same sequence
+    pf_h, pf_d, exact = [], [], True
+    t0 = time.perf_counter()
+    for (ta, si, j) in arrivals:
+        sf = streams[si]["frames"][j]
+        fb = np.empty(A.frame_bytes(sf.f.info), np.uint8)
+        a = time.perf_counter()
+        A.check(L.av1pf_chain_host(ctx.p, C.byref(sf.f.info), C.byref(sf.f.params), C.byref(sf.f.maps),
+                                   streams[si]["host"][j].c, None, fb.ctypes.data), "chain_host")
+        pf_h.append(1e3 * (time.perf_counter() - a))
+        if exact and (si, j) in outs:
+            exact = bool(np.array_equal(fb, outs[(si, j)]))
+    t_pfh = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for (ta, si, j) in arrivals:
+        df = streams[si]["dev"][j]
+        r_out, f_out = streams[si]["outs"][j]
+        a = time.perf_counter()
+        A.check(L.av1pf_chain(ctx.p, C.byref(df.info), C.byref(df.params), C.byref(df.maps), df.inp.c, r_out.c,
+                              f_out.data_ptr(), None), "chain")
+        torch.cuda.synchronize()
+        pf_d.append(1e3 * (time.perf_counter() - a))
+    t_pfd = time.perf_counter() - t0
+
+    def pct(v, q):
+        return round(float(np.percentile(v, q)), 3)
+    return {"streams": len(streams), "frames": n, "mpx": round(px / 1e6, 2), "duration_s": duration_s,
+            "offered_fps": round(n / duration_s, 1),
+            "host_feed": {"served_fps": round(n / w_h, 1), "p50_ms": pct(lat_h, 50), "p99_ms": pct(lat_h, 99),
+                          "mean_batch_frames": round((b1.completed - b0.completed) / max(1, b1.batches - b0.batches), 2),
+                          "saturated_fps": round(n / s_h, 1), "saturated_mpx_s": round(px / s_h / 1e6, 1),
+                          "per_frame_fps": round(n / t_pfh, 1), "per_frame_mpx_s": round(px / t_pfh / 1e6, 1),
+                          "per_frame_p50_ms": pct(pf_h, 50), "per_frame_p99_ms": pct(pf_h, 99),
+                          "saturated_vs_per_frame": round(t_pfh / s_h, 3)},
+            "device_feed": {"served_fps": round(n / w_d, 1), "p50_ms": pct(lat_d, 50), "p99_ms": pct(lat_d, 99),
+                            "saturated_fps": round(n / s_d, 1), "saturated_mpx_s": round(px / s_d / 1e6, 1),
+                            "per_frame_fps": round(n / t_pfd, 1), "per_frame_mpx_s": round(px / t_pfd / 1e6, 1),
+                            "per_frame_p50_ms": pct(pf_d, 50), "per_frame_p99_ms": pct(pf_d, 99),
+                            "saturated_vs_per_frame": round(t_pfd / s_d, 3)},
+            "mean_batch_frames_all": round(b2.mean_batch_frames, 2),
+            "bit_exact_serve_vs_per_frame": exact}
 
 
 def main():

@@ -336,12 +336,20 @@ typedef struct av1pf_serve_config {
   int32_t tick_us;          /* longest wait for more work before a tick */
 } av1pf_serve_config;
 
-/* A submitted frame: host pointers, copied at submit time. */
+/* A submitted frame. With device == 0, `maps` and `in` are host pointers,
+ * copied at submit time, and av1pf_serve_poll returns the packed frame. With
+ * device != 0 they are device pointers (a decoder that produced the planes
+ * on the GPU), which must stay valid until the frame completes; the server
+ * reads them in place and writes the reference frame to `ref_out` and the
+ * packed frame to `frame_out` (device pointers; either may be NULL). */
 typedef struct av1pf_request {
   const av1pf_frame_info* info;
   const av1pf_params* params;
-  const av1pf_maps* maps;  /* host */
-  const av1pf_plane* in;   /* host */
+  const av1pf_maps* maps;
+  const av1pf_plane* in;
+  int32_t device;
+  av1pf_plane* ref_out;    /* device requests only */
+  uint8_t* frame_out;      /* device requests only */
 } av1pf_request;
 
 typedef struct av1pf_serve_stats {

@@ -92,7 +92,8 @@ class ServeConfig(C.Structure):
 
 class Request(C.Structure):
     _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("maps", C.POINTER(Maps)),
-                ("inp", C.POINTER(Plane))]
+                ("inp", C.POINTER(Plane)), ("device", C.c_int32), ("ref_out", C.POINTER(Plane)),
+                ("frame_out", C.c_void_p)]
 
 
 class ServeStats(C.Structure):

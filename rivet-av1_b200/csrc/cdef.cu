@@ -10,9 +10,9 @@
 // 421-422, 464-488) stored as -32768. That value needs no special case:
 // constrain() of a difference that large is 0 for every strength/damping
 // pair the format allows (|d| >= 2^(damping+1) >= str << adj), a signed max
-// never picks it, and an unsigned min never picks it. The direction search
-// gives each warp one of the 8 directions and each lane one 8x8 block, so
-// the partial-sum bins are compile-time register indices.
+// never picks it, and an unsigned min never picks it. In the direction
+// search each thread takes one 8x8 block and two of the 8 directions (one
+// pair per warp), so the partial-sum bins are compile-time register indices.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -20,16 +20,21 @@ namespace av1pf {
 
 namespace {
 
-constexpr int kWin = 72;         // smem row stride (int16) of a plane window
-constexpr int kWinRows = 68;     // 64 + 2*2 rows
+// Shared-memory window of one plane: 68 rows (64 + 2*2) x 80 columns
+// (64 + 8 on each side, so global loads stay 8-sample aligned), row stride
+// 82 int16 = 41 words: a warp's 4 rows x 8 blocks of centre loads then hit
+// 32 different banks.
+constexpr int kS = 82;
+constexpr int kRows = 68;
+constexpr int kColOff = 8;       // window column of plane x = px0
 constexpr int16_t kNA = -32768;  // unavailable sample
 
-struct CdefBlk {
-  int16_t pri, sec;  // strengths (after the luma variance adjustment)
-  int8_t dir;        // filter direction
-  int8_t damping;    // damping (+coeff_shift, -1 for chroma)
-  int8_t copy;       // 1: skipped / CDEF off: output = input
-  int8_t pad;
+// Per 8x8 block and plane: strengths, tap weights and window offsets.
+struct BlkTaps {
+  int16_t pri, sec;
+  int16_t po0, po1, so00, so01, so10, so11;
+  int8_t pri_adj, sec_adj, pt0, pt1;
+  int8_t copy, pad0, pad1, pad2;
 };
 
 }  // namespace
@@ -71,48 +76,60 @@ __device__ __forceinline__ int cdef_px(const int16_t* c, const TapsDev& t) {
 
 // The Taps of cdef_filter_block (postfilter.rs:489-511) for a window of row
 // stride `st`. CDEF_SEC_TAPS is [2, 1] for both primary-tap parities.
-__device__ __forceinline__ TapsDev make_taps(int pri, int sec, int damping, int dir, int coeff_shift, int st) {
-  TapsDev t;
-  t.pri = pri;
-  t.sec = sec;
-  t.pri_adj = pri ? max(damping - floor_log2(uint32_t(pri)), 0) : 0;
-  t.sec_adj = sec ? max(damping - floor_log2(uint32_t(sec)), 0) : 0;
+__device__ __forceinline__ BlkTaps make_blk_taps(int pri, int sec, int damping, int dir, int coeff_shift, int st) {
+  BlkTaps t;
+  t.pri = int16_t(pri);
+  t.sec = int16_t(sec);
+  t.pri_adj = int8_t(pri ? max(damping - floor_log2(uint32_t(pri)), 0) : 0);
+  t.sec_adj = int8_t(sec ? max(damping - floor_log2(uint32_t(sec)), 0) : 0);
   const bool odd = (pri >> coeff_shift) & 1;  // CDEF_PRI_TAPS[(pri >> cs) & 1]: [4,2] / [3,3]
-  t.pt0 = odd ? 3 : 4;
-  t.pt1 = odd ? 3 : 2;
+  t.pt0 = int8_t(odd ? 3 : 4);
+  t.pt1 = int8_t(odd ? 3 : 2);
   const int dlo = (dir + 6) & 7, dhi = (dir + 2) & 7;
-  t.po0 = c_cdef_dirs[dir][0][0] * st + c_cdef_dirs[dir][0][1];
-  t.po1 = c_cdef_dirs[dir][1][0] * st + c_cdef_dirs[dir][1][1];
-  t.so00 = c_cdef_dirs[dlo][0][0] * st + c_cdef_dirs[dlo][0][1];
-  t.so01 = c_cdef_dirs[dhi][0][0] * st + c_cdef_dirs[dhi][0][1];
-  t.so10 = c_cdef_dirs[dlo][1][0] * st + c_cdef_dirs[dlo][1][1];
-  t.so11 = c_cdef_dirs[dhi][1][0] * st + c_cdef_dirs[dhi][1][1];
+  t.po0 = int16_t(c_cdef_dirs[dir][0][0] * st + c_cdef_dirs[dir][0][1]);
+  t.po1 = int16_t(c_cdef_dirs[dir][1][0] * st + c_cdef_dirs[dir][1][1]);
+  t.so00 = int16_t(c_cdef_dirs[dlo][0][0] * st + c_cdef_dirs[dlo][0][1]);
+  t.so01 = int16_t(c_cdef_dirs[dhi][0][0] * st + c_cdef_dirs[dhi][0][1]);
+  t.so10 = int16_t(c_cdef_dirs[dlo][1][0] * st + c_cdef_dirs[dlo][1][1]);
+  t.so11 = int16_t(c_cdef_dirs[dhi][1][0] * st + c_cdef_dirs[dhi][1][1]);
+  t.copy = (pri == 0 && sec == 0) ? 1 : 0;  // a zero-strength filter is the identity
+  t.pad0 = t.pad1 = t.pad2 = 0;
   return t;
 }
 
-// cdef_direction's cost of direction D (postfilter.rs:345-390) for the 8x8
-// block at `s` (row stride st); samples are >> sh then - 128.
+__device__ __forceinline__ TapsDev taps_of(const BlkTaps& b) {
+  TapsDev t;
+  t.pri = b.pri;
+  t.sec = b.sec;
+  t.pri_adj = b.pri_adj;
+  t.sec_adj = b.sec_adj;
+  t.pt0 = b.pt0;
+  t.pt1 = b.pt1;
+  t.po0 = b.po0;
+  t.po1 = b.po1;
+  t.so00 = b.so00;
+  t.so01 = b.so01;
+  t.so10 = b.so10;
+  t.so11 = b.so11;
+  return t;
+}
+
+// Partial-sum bin of direction D for pixel (i, j) (postfilter.rs:352-363).
 template <int D>
-__device__ __forceinline__ int32_t cdef_cost(const int16_t* s, int st, int sh) {
-  int32_t p[15];
-#pragma unroll
-  for (int k = 0; k < 15; k++) p[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int x = (int(s[i * st + j]) >> sh) - 128;
-      const int k = D == 0 ? i + j
-                  : D == 1 ? i + j / 2
-                  : D == 2 ? i
-                  : D == 3 ? 3 + i - j / 2
-                  : D == 4 ? 7 + i - j
-                  : D == 5 ? 3 - i / 2 + j
-                  : D == 6 ? j
-                           : i / 2 + j;
-      p[k] += x;
-    }
-  }
+__device__ __forceinline__ constexpr int cdef_bin(int i, int j) {
+  return D == 0 ? i + j
+       : D == 1 ? i + j / 2
+       : D == 2 ? i
+       : D == 3 ? 3 + i - j / 2
+       : D == 4 ? 7 + i - j
+       : D == 5 ? 3 - i / 2 + j
+       : D == 6 ? j
+                : i / 2 + j;
+}
+
+// The cost of direction D from its partial sums (postfilter.rs:365-390).
+template <int D>
+__device__ __forceinline__ int32_t cdef_cost_of(const int32_t* p) {
   int32_t cost = 0;
   if (D == 2 || D == 6) {
 #pragma unroll
@@ -132,27 +149,41 @@ __device__ __forceinline__ int32_t cdef_cost(const int16_t* s, int st, int sh) {
   return cost;
 }
 
-__device__ __forceinline__ int32_t cdef_cost_dir(int d, const int16_t* s, int st, int sh) {
-  switch (d) {
-    case 0: return cdef_cost<0>(s, st, sh);
-    case 1: return cdef_cost<1>(s, st, sh);
-    case 2: return cdef_cost<2>(s, st, sh);
-    case 3: return cdef_cost<3>(s, st, sh);
-    case 4: return cdef_cost<4>(s, st, sh);
-    case 5: return cdef_cost<5>(s, st, sh);
-    case 6: return cdef_cost<6>(s, st, sh);
-    default: return cdef_cost<7>(s, st, sh);
+// Costs of directions P and P + 4 of the 8x8 block whose top-left sample is
+// window word `w0` (4-byte aligned); samples are >> sh then - 128.
+template <int P>
+__device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int32_t& c1, int32_t& c2) {
+  int32_t a[15], b[15];
+#pragma unroll
+  for (int k = 0; k < 15; k++) a[k] = b[k] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t* row = reinterpret_cast<const uint32_t*>(s + i * kS);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint32_t w = row[q];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = 2 * q + h;
+        const int x = ((int(int16_t(h ? (w >> 16) : (w & 0xffffu)))) >> sh) - 128;
+        a[cdef_bin<P>(i, j)] += x;
+        b[cdef_bin<P + 4>(i, j)] += x;
+      }
+    }
   }
+  c1 = cdef_cost_of<P>(a);
+  c2 = cdef_cost_of<P + 4>(b);
 }
 
 // Item: superblock (x0 = SB column, y0 = SB row). 256 threads.
-__global__ void __launch_bounds__(256) cdef_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDesc* __restrict__ frames,
                                                    const Item* __restrict__ items, int n_items) {
-  __shared__ int16_t win[3][kWinRows * kWin];
+  __shared__ __align__(16) int16_t win[3][kRows * kS];
   __shared__ int32_t cost[64][8];
-  __shared__ CdefBlk blk[3][64];
+  __shared__ BlkTaps taps[3][64];
   __shared__ uint8_t bstate[64];  // 0 = outside the MI area, 1 = copy, 2 = filter
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -160,19 +191,52 @@ __global__ void __launch_bounds__(256) cdef_kernel(const FrameDesc* __restrict__
     const int np = f.np, sb = f.sb;
     const int cs = f.bd - 8;
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
-    // --- stage the windows (postfilter.rs:464-488) ---
+    // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
     for (int p = 0; p < np; p++) {
       const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-      const int bw = (64 >> sx) + 4, bh = (64 >> sy) + 4;
-      const int px0 = ((sc * 64) >> sx) - 2, py0 = ((sr * 64) >> sy) - 2;
+      const int bh = (64 >> sy) + 4;
+      const int nch = ((64 >> sx) + 16) / 8;  // chunks per window row
+      const int px0 = (sc * 64) >> sx, py0 = ((sr * 64) >> sy) - 2;
       const int xlim = (f.mi_cols * 4) >> sx, ylim = (f.mi_rows * 4) >> sy;
       const DPlane src = f.cur[p];
-      for (int k = tid; k < bw * bh; k += 256) {
-        const int r = k / bw, c = k - r * bw;
-        const int gx = px0 + c, gy = py0 + r;
-        int16_t v = kNA;
-        if (gx >= 0 && gx < xlim && gy >= 0 && gy < ylim) v = int16_t(ld_sample(src, sb, gx, gy));
-        win[p][r * kWin + c] = v;
+      int16_t* wp = win[p];
+      for (int k = tid; k < bh * 16; k += 256) {
+        const int r = k >> 4, ch = k & 15;
+        if (ch >= nch) continue;
+        const int gy = py0 + r;
+        const int gx0 = px0 - kColOff + ch * 8;
+        int16_t v[8];
+        if (gy < 0 || gy >= ylim || gx0 + 8 <= 0 || gx0 >= xlim) {
+#pragma unroll
+          for (int e = 0; e < 8; e++) v[e] = kNA;
+        } else if (gx0 >= 0 && gx0 + 8 <= xlim) {
+          const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
+          if (sb == 2) {
+            const uint4 q = *reinterpret_cast<const uint4*>(rowp + int64_t(gx0) * 2);
+            const uint32_t ws[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              v[2 * e] = int16_t(ws[e] & 0xffffu);
+              v[2 * e + 1] = int16_t(ws[e] >> 16);
+            }
+          } else {
+            const uint2 q = *reinterpret_cast<const uint2*>(rowp + gx0);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              v[e] = int16_t((q.x >> (8 * e)) & 0xffu);
+              v[4 + e] = int16_t((q.y >> (8 * e)) & 0xffu);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            const int gx = gx0 + e;
+            v[e] = (gx >= 0 && gx < xlim) ? int16_t(ld_sample(src, sb, gx, gy)) : kNA;
+          }
+        }
+        uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
+#pragma unroll
+        for (int e = 0; e < 4; e++) dst[e] = uint32_t(uint16_t(v[2 * e])) | (uint32_t(uint16_t(v[2 * e + 1])) << 16);
       }
     }
     // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
@@ -193,27 +257,34 @@ __global__ void __launch_bounds__(256) cdef_kernel(const FrameDesc* __restrict__
       bstate[tid] = st;
     }
     __syncthreads();
-    // --- direction search (postfilter.rs:345-401): warp = direction, lane = block ---
+    // --- direction search (postfilter.rs:345-401): each thread two directions of one block ---
     {
-      const int d = tid >> 5, lane = tid & 31;
-#pragma unroll
-      for (int half = 0; half < 2; half++) {
-        const int b = lane + 32 * half;
-        if (bstate[b] == 2) {
-          const int by = b >> 3, bx = b & 7;
-          const int16_t* s = &win[0][(2 + by * 8) * kWin + 2 + bx * 8];
-          cost[b][d] = cdef_cost_dir(d, s, kWin, cs);
+      const int pair = warp & 3;
+      const int b = (warp >> 2) * 32 + lane;
+      if (bstate[b] == 2) {
+        const int by = b >> 3, bx = b & 7;
+        const int16_t* s = &win[0][(2 + by * 8) * kS + kColOff + bx * 8];
+        int32_t c1, c2;
+        switch (pair) {
+          case 0: cdef_cost_pair<0>(s, cs, c1, c2); break;
+          case 1: cdef_cost_pair<1>(s, cs, c1, c2); break;
+          case 2: cdef_cost_pair<2>(s, cs, c1, c2); break;
+          default: cdef_cost_pair<3>(s, cs, c1, c2); break;
         }
+        cost[b][pair] = c1;
+        cost[b][pair + 4] = c2;
       }
     }
     __syncthreads();
-    // --- per-block strengths (postfilter.rs:311-341) ---
+    // --- per-block strengths and taps (postfilter.rs:311-341) ---
     if (tid < 64) {
       const int b = tid;
-      CdefBlk L{0, 0, 0, 0, 1, 0}, U{0, 0, 0, 0, 1, 0};
-      if (bstate[b] == 2) {
+      int lp = 0, ls = 0, ld = 0, up = 0, us = 0, ud = 0;
+      bool filt = bstate[b] == 2;
+      if (filt) {
         int32_t best = 0;
         int y_dir = 0;
+#pragma unroll
         for (int d = 0; d < 8; d++) {
           if (cost[b][d] > best) {
             best = cost[b][d];
@@ -222,65 +293,43 @@ __global__ void __launch_bounds__(256) cdef_kernel(const FrameDesc* __restrict__
         }
         const int32_t var = (best - cost[b][(y_dir + 4) & 7]) >> 10;
         int pri = f.cdef_y_pri[idx] << cs;
-        const int sec = f.cdef_y_sec[idx] << cs;
-        const int dir = pri == 0 ? 0 : y_dir;
+        ls = f.cdef_y_sec[idx] << cs;
+        ld = pri == 0 ? 0 : y_dir;
         const int var_str = (var >> 6) != 0 ? min(floor_log2(uint32_t(var >> 6)), 12) : 0;
-        pri = var != 0 ? (pri * (4 + var_str) + 8) >> 4 : 0;
-        L.pri = int16_t(pri);
-        L.sec = int16_t(sec);
-        L.dir = int8_t(dir);
-        L.damping = int8_t(f.cdef_damping + cs);
-        L.copy = (pri == 0 && sec == 0) ? 1 : 0;  // a zero-strength filter is the identity
-        const int upri = f.cdef_uv_pri[idx] << cs;
-        const int usec = f.cdef_uv_sec[idx] << cs;
-        U.pri = int16_t(upri);
-        U.sec = int16_t(usec);
-        U.dir = int8_t(upri == 0 ? 0 : c_cdef_uv_dir[f.ssx][f.ssy][y_dir]);
-        U.damping = int8_t(f.cdef_damping + cs - 1);
-        U.copy = (upri == 0 && usec == 0) ? 1 : 0;
+        lp = var != 0 ? (pri * (4 + var_str) + 8) >> 4 : 0;
+        up = f.cdef_uv_pri[idx] << cs;
+        us = f.cdef_uv_sec[idx] << cs;
+        ud = up == 0 ? 0 : c_cdef_uv_dir[f.ssx][f.ssy][y_dir];
       }
-      blk[0][b] = L;
-      blk[1][b] = U;
-      blk[2][b] = U;
+      BlkTaps L = make_blk_taps(lp, ls, f.cdef_damping + cs, ld, cs, kS);
+      BlkTaps U = make_blk_taps(up, us, f.cdef_damping + cs - 1, ud, cs, kS);
+      if (!filt) L.copy = U.copy = 1;
+      taps[0][b] = L;
+      taps[1][b] = U;
+      taps[2][b] = U;
     }
     __syncthreads();
-    // --- filter + write: one block row per step (postfilter.rs:405-442) ---
-    {
-      const int csx = f.ssx, csy = f.ssy;
-      const int rows_l = 64 * 8;
-      const int ch_h = 8 >> csy;
-      const int rows_c = np > 1 ? 64 * ch_h : 0;
-      const int total = rows_l + 2 * rows_c;
-      for (int k = tid; k < total; k += 256) {
-        int p, b, rr;
-        if (k < rows_l) {
-          p = 0;
-          b = k >> 3;
-          rr = k & 7;
-        } else {
-          const int kk = k - rows_l;
-          p = 1 + kk / rows_c;
-          const int q = kk % rows_c;
-          b = q / ch_h;
-          rr = q - b * ch_h;
-        }
+    // --- filter + write (postfilter.rs:405-442): warp = block row, lane = (row, block) ---
+    for (int p = 0; p < np; p++) {
+      const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+      const int w = 8 >> sx, bhp = 8 >> sy;
+      const DPlane dst = f.cdef[p];
+      for (int q = 0; q < bhp / 4; q++) {
+        const int by = warp, bx = lane & 7, rr = q * 4 + (lane >> 3);
+        const int b = by * 8 + bx;
         if (bstate[b] == 0) continue;
-        const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-        const int w = 8 >> sx;
-        const int by = b >> 3, bx = b & 7;
-        const int lx = bx * w, ly = by * (8 >> sy) + rr;  // position within the plane's SB
-        const int16_t* c = &win[p][(2 + ly) * kWin + 2 + lx];
+        const int lx = bx * w, ly = by * bhp + rr;
+        const int16_t* c = &win[p][(2 + ly) * kS + kColOff + lx];
         int out[8];
-        const CdefBlk pb = blk[p][b];
-        if (pb.copy) {
+        const BlkTaps bt = taps[p][b];
+        if (bt.copy) {
 #pragma unroll
           for (int j = 0; j < 8; j++) out[j] = j < w ? c[j] : 0;
         } else {
-          const TapsDev t = make_taps(pb.pri, pb.sec, pb.damping, pb.dir, cs, kWin);
+          const TapsDev t = taps_of(bt);
 #pragma unroll
           for (int j = 0; j < 8; j++) out[j] = j < w ? cdef_px(c + j, t) : 0;
         }
-        const DPlane dst = f.cdef[p];
         const int gx = ((sc * 64) >> sx) + lx, gy = ((sr * 64) >> sy) + ly;
         uint8_t* row = dst.p + int64_t(gy) * dst.stride * sb;
         if (sb == 2) {

@@ -252,10 +252,12 @@ __global__ void __launch_bounds__(256) output_kernel(const FrameDesc* __restrict
       grain = p == 0 ? g.num_y_points > 0
                      : ((p == 1 ? g.num_cb_points : g.num_cr_points) > 0 || g.chroma_scaling_from_luma);
     }
+    // tiles are at most 64 columns wide: 64 fixed slots per row
     const int tw = int(item.x1) - int(item.x0);
-    const int n = tw * (int(item.y1) - int(item.y0));
+    const int n = 64 * (int(item.y1) - int(item.y0));
     for (int k = threadIdx.x; k < n; k += 256) {
-      const int yy = item.y0 + k / tw, xx = item.x0 + k % tw;
+      if ((k & 63) >= tw) continue;
+      const int yy = item.y0 + (k >> 6), xx = item.x0 + (k & 63);
       const int orig = ld_sample(src, sb, xx, yy);
       int v = orig;
       if (grain) {

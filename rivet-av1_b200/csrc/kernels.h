@@ -37,6 +37,8 @@ void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cu
 
 // Loop restoration (lr.cu)
 void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// Sets lr_kernel's dynamic shared-memory limit on the current device.
+cudaError_t lr_init();
 
 // Film grain + output packing (grain.cu)
 void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);

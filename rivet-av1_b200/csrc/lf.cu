@@ -139,18 +139,22 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
       const int sb = f.sb;
       const int x0 = item.x0, x1 = min(int(item.x1), src.w);
       const int y0 = item.y0, y1 = min(int(item.y1), src.h);
-      const int bx0 = x0 * sb, bx1 = x1 * sb;  // byte columns
+      const int bx0 = x0 * sb, bx1 = x1 * sb;  // byte columns (a tile row is at most 128 bytes)
       const int nvec = (bx1 - bx0) >> 4;
       const int rows = y1 - y0;
-      for (int k = threadIdx.x; k < nvec * rows; k += blockDim.x) {
-        const int r = y0 + k / nvec, c = bx0 + (k % nvec) * 16;
-        const uint4 v = *reinterpret_cast<const uint4*>(src.p + int64_t(r) * src.stride * sb + c);
-        *reinterpret_cast<uint4*>(dst.p + int64_t(r) * dst.stride * sb + c) = v;
+      for (int k = threadIdx.x; k < rows * 8; k += blockDim.x) {
+        const int v = k & 7;
+        if (v >= nvec) continue;
+        const int r = y0 + (k >> 3), c = bx0 + v * 16;
+        const uint4 q = *reinterpret_cast<const uint4*>(src.p + int64_t(r) * src.stride * sb + c);
+        *reinterpret_cast<uint4*>(dst.p + int64_t(r) * dst.stride * sb + c) = q;
       }
       const int tail = (bx1 - bx0) & 15;
       if (tail) {
-        for (int k = threadIdx.x; k < tail * rows; k += blockDim.x) {
-          const int r = y0 + k / tail, c = bx0 + nvec * 16 + (k % tail);
+        for (int k = threadIdx.x; k < rows * 16; k += blockDim.x) {
+          const int e = k & 15;
+          if (e >= tail) continue;
+          const int r = y0 + (k >> 4), c = bx0 + nvec * 16 + e;
           dst.p[int64_t(r) * dst.stride * sb + c] = src.p[int64_t(r) * src.stride * sb + c];
         }
       }
@@ -159,11 +163,11 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
       const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
       const int gw = f.mi_cols >> sx, gh = f.mi_rows >> sy;  // 4x4 grid of the plane
       const int cx0 = item.x0 >> 2, cy0 = item.y0 >> 2;
-      const int tw = (int(item.x1) - int(item.x0) + 3) >> 2;
+      const int tw = (int(item.x1) - int(item.x0) + 3) >> 2;  // <= 16 (64-sample tiles)
       const int th = (int(item.y1) - int(item.y0) + 3) >> 2;
-      for (int k = threadIdx.x; k < ((tw * th + 31) & ~31); k += blockDim.x) {
-        const int cx = cx0 + (k % tw), cy = cy0 + (k / tw);
-        const bool in = k < tw * th && cx < gw && cy < gh;
+      for (int k = threadIdx.x; k < th * 16; k += blockDim.x) {
+        const int cx = cx0 + (k & 15), cy = cy0 + (k >> 4);
+        const bool in = (k & 15) < tw && cx < gw && cy < gh;
         int dv = 0, dh = 0;
         if (in) {
           dv = lf_decide(f, plane, 0, cx, cy);
