@@ -197,6 +197,14 @@ def main_gpu(args):
     import gpu_util as G
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
+    if args.only:
+        ctx = G.Ctx(local)
+        fn = {"mix": lambda: bench_mix(args, ctx, rank, torch.cuda.synchronize, lambda v: v),
+              "c3": lambda: bench_4k(args, ctx, torch.cuda.synchronize, lambda v: v),
+              "serve": lambda: bench_serve(args, ctx, rank)}[args.only]
+        print(json.dumps({args.only: fn()}), flush=True)
+        ctx.close()
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -661,6 +669,8 @@ def main():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-extras", action="store_true")
+    ap.add_argument("--only", choices=["mix", "c3", "serve"], default=None,
+                    help="run one extra section alone (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -199,6 +199,7 @@ int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out) {
     if (device < 64 && !g_tables_ready[device]) {
       if ((e = upload_grain_tables()) != cudaSuccess) return cuda_status(e, "grain tables");
       if ((e = lr_init()) != cudaSuccess) return cuda_status(e, "loop restoration kernel attributes");
+      if ((e = superres_init()) != cudaSuccess) return cuda_status(e, "superres kernel attributes");
       g_tables_ready[device] = true;
     }
   }

@@ -15,7 +15,7 @@
 //     most 3 columns left and 3 rows up (3 columns right on earlier rows),
 //     so cells with equal (x - 3) + 4 (y - 3) are independent: one thread
 //     per template row walks the anti-diagonal wavefront.
-// output_kernel: per tile of a plane's visible area, reads the reference
+// output_kernel: per 256-column tile of a plane's visible area, reads the reference
 // frame, adds grain (noise assembled from the templates, the 32x32 block
 // offsets and the overlap blends of grain.rs:179-283, evaluated per sample
 // instead of through the reference's noise-stripe and noise-image buffers),
@@ -40,14 +40,89 @@ __device__ __forceinline__ uint32_t rng_jump(uint32_t seed, const uint16_t* cols
 }
 
 constexpr int kTH = 73, kTW = 82;
+// Staged block offsets per output item: 256 columns span at most 16 grain
+// blocks (16 columns wide in subsampled chroma), plus the block to the left.
+constexpr int kOutOffs = 18;
 }  // namespace
+
+// Luma auto-regression (grain.rs:55-73) with lag LAG: thread `rr` owns
+// template row 3 + rr and walks the wavefront (x - 3) + 4 * rr = t, so every
+// cell's earlier neighbours (left in its row, up to LAG right in the rows
+// above) are done one step earlier. Coefficients live in registers.
+template <int LAG>
+__device__ __forceinline__ void ar_luma(int16_t (*T)[kTW], const int32_t* coef_s, int ar_shift, int gmin, int gmax) {
+  constexpr int NC = 2 * LAG * (LAG + 1);
+  int c[NC > 0 ? NC : 1];
+#pragma unroll
+  for (int k = 0; k < NC; k++) c[k] = coef_s[k];
+  const int rr = threadIdx.x;
+  const int y = 3 + rr;
+  const int steps = (kTW - 3 - 3 - 1) + 4 * (kTH - 3 - 1) + 1;
+  for (int t = 0; t < steps; t++) {
+    const int x = 3 + t - 4 * rr;
+    if (y < kTH && x >= 3 && x < kTW - 3) {
+      int s = 0, pos = 0;
+#pragma unroll
+      for (int dr = -LAG; dr <= 0; dr++)
+#pragma unroll
+        for (int dc = -LAG; dc <= LAG; dc++) {
+          if (dr == 0 && dc >= 0) continue;
+          s += T[y + dr][x + dc] * c[pos];
+          pos++;
+        }
+      T[y][x] = int16_t(clip3(gmin, gmax, T[y][x] + round2(s, ar_shift)));
+    }
+    __syncthreads();
+  }
+}
+
+// Chroma auto-regression with the luma term (grain.rs:101-134): threads
+// 0..127 take Cb rows, 128..255 Cr rows, same wavefront as the luma one.
+template <int LAG>
+__device__ __forceinline__ void ar_chroma(int16_t (*T)[kTH][kTW], const int32_t (*coef_s)[25], int ar_shift, int gmin,
+                                          int gmax, int chroma_w, int chroma_h, int sub_x, int sub_y, bool luma_on) {
+  constexpr int NC = 2 * LAG * (LAG + 1);
+  const int plane = threadIdx.x < 128 ? 1 : 2;
+  int c[NC + 1];
+#pragma unroll
+  for (int k = 0; k <= NC; k++) c[k] = coef_s[plane][k];
+  const int rr = threadIdx.x & 127;
+  const int y = 3 + rr;
+  const int steps = (chroma_w - 3 - 3 - 1) + 4 * (chroma_h - 3 - 1) + 1;
+  for (int t = 0; t < steps; t++) {
+    const int x = 3 + t - 4 * rr;
+    if (y < chroma_h && x >= 3 && x < chroma_w - 3) {
+      int s = 0, pos = 0;
+#pragma unroll
+      for (int dr = -LAG; dr <= 0; dr++)
+#pragma unroll
+        for (int dc = -LAG; dc <= LAG; dc++) {
+          if (dr == 0 && dc >= 0) continue;
+          s += T[plane][y + dr][x + dc] * c[pos];
+          pos++;
+        }
+      if (luma_on) {
+        int luma = 0;
+        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
+        for (int i = 0; i <= sub_y; i++)
+          for (int j = 0; j <= sub_x; j++) luma += T[0][ly + i][lx + j];
+        luma = round2(luma, sub_x + sub_y);
+        s += luma * c[NC];
+      }
+      T[plane][y][x] = int16_t(clip3(gmin, gmax, T[plane][y][x] + round2(s, ar_shift)));
+    }
+    __syncthreads();
+  }
+}
 
 __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __restrict__ frames,
                                                          const Item* __restrict__ items, int n_items) {
   __shared__ int16_t T[3][kTH][kTW];
   __shared__ int32_t coef[3][25];
   __shared__ int32_t lut[3][256];
+  __shared__ int16_t gauss[2048];
   const int tid = threadIdx.x;
+  for (int k = tid; k < 2048; k += 256) gauss[k] = g_gaussian[k];
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -89,68 +164,28 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
           uint32_t r = rng_jump(s0, width == 82 ? g_rng_jump82[row] : g_rng_jump44[row]);
           for (int c = 0; c < width; c++) {
             r = rng_step(r);
-            T[plane][row][c] = int16_t(round2(g_gaussian[(r >> 5) & 2047u], shift));
+            T[plane][row][c] = int16_t(round2(gauss[(r >> 5) & 2047u], shift));
           }
         }
       }
     }
     __syncthreads();
-    // --- luma auto-regression (grain.rs:55-73): wavefront over (x-3) + 4(y-3) ---
+    // --- auto-regression (grain.rs:55-134) ---
     const int lag = g.ar_coeff_lag;
     const int ar_shift = g.ar_coeff_shift_minus_6 + 6;
-    {
-      const int y = 3 + tid;
-      const int steps = (kTW - 3 - 3 - 1) + 4 * (kTH - 3 - 1) + 1;
-      for (int t = 0; t < steps; t++) {
-        const int x = 3 + t - 4 * tid;
-        if (y < kTH && x >= 3 && x < kTW - 3) {
-          int s = 0, pos = 0;
-          for (int dr = -lag; dr <= 0; dr++) {
-            for (int dc = -lag; dc <= lag; dc++) {
-              if (dr == 0 && dc == 0) break;
-              s += T[0][y + dr][x + dc] * coef[0][pos];
-              pos++;
-            }
-          }
-          T[0][y][x] = int16_t(clip3(grain_min, grain_max, T[0][y][x] + round2(s, ar_shift)));
-        }
-        __syncthreads();
-      }
+    switch (lag) {
+      case 0: ar_luma<0>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
+      case 1: ar_luma<1>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
+      case 2: ar_luma<2>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
+      default: ar_luma<3>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
     }
-    // --- chroma auto-regression with the luma term (grain.rs:101-134) ---
     if (!mono) {
-      const int plane = tid < 128 ? 1 : 2;
-      const int rr = tid & 127;
-      const int y = 3 + rr;
-      const int steps = (chroma_w - 3 - 3 - 1) + 4 * (chroma_h - 3 - 1) + 1;
-      for (int t = 0; t < steps; t++) {
-        const int x = 3 + t - 4 * rr;
-        if (y < chroma_h && x >= 3 && x < chroma_w - 3) {
-          int s = 0, pos = 0;
-          for (int dr = -lag; dr <= 0; dr++) {
-            bool done = false;
-            for (int dc = -lag; dc <= lag; dc++) {
-              const int c = coef[plane][pos];
-              if (dr == 0 && dc == 0) {
-                if (g.num_y_points > 0) {
-                  int luma = 0;
-                  const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
-                  for (int i = 0; i <= sub_y; i++)
-                    for (int j = 0; j <= sub_x; j++) luma += T[0][ly + i][lx + j];
-                  luma = round2(luma, sub_x + sub_y);
-                  s += luma * c;
-                }
-                done = true;
-                break;
-              }
-              s += T[plane][y + dr][x + dc] * c;
-              pos++;
-            }
-            if (done) break;
-          }
-          T[plane][y][x] = int16_t(clip3(grain_min, grain_max, T[plane][y][x] + round2(s, ar_shift)));
-        }
-        __syncthreads();
+      const bool luma_on = g.num_y_points > 0;
+      switch (lag) {
+        case 0: ar_chroma<0>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
+        case 1: ar_chroma<1>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
+        case 2: ar_chroma<2>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
+        default: ar_chroma<3>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
       }
     }
     // --- scaling lookup (grain.rs:137-165): one thread per plane, as written ---
@@ -198,123 +233,242 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
   }
 }
 
-// The noise of stripe `s`, stripe row `row`, plane column x after the
-// horizontal overlap of 32x32 (luma) blocks (grain.rs:200-243).
-__device__ __forceinline__ int grain_hval(const int16_t* T, const uint8_t* off, int nb, int psx, int psy, int s,
-                                          int row, int x, bool overlap, int gmin, int gmax) {
-  const int bw = 32 >> psx;
-  const int b = x >> (5 - psx);
-  const int j = x - b * bw;
-  const int rnd = off[s * nb + b];
+// scale_lut of grain.rs:166-177 (`lut` in shared memory).
+__device__ __forceinline__ int grain_scale(const int16_t* lut, int index, int sh) {
+  const int x = index >> sh;
+  const int rem = index - (x << sh);
+  if (sh == 0 || x == 255) return lut[x];
+  const int start = lut[x], end = lut[x + 1];
+  return start + round2((end - start) * rem, sh);
+}
+
+// Per-item constants of the output stage, held in registers: the stores to
+// the packed frame are byte stores, which the compiler must otherwise assume
+// alias the frame descriptor.
+struct OutParams {
+  const uint8_t* src;
+  int64_t src_pitch;  // bytes
+  const uint8_t* luma;
+  int64_t luma_pitch;
+  uint8_t* out;
+  int pw, w, sb, bd, psx, psy, ssx, ssy;
+  bool wide, grain, overlap, csfl;
+  const uint8_t* off;
+  int nb, gmin, gmax, min_value, max_v, maxpix, scaling_shift;
+  int mult, lmult, offs;
+};
+
+// One noise sample from the template in shared memory (grain.rs:200-243 for
+// the horizontal overlap): stripe offsets `rnd` (this block) and `rnd_prev`
+// (the block to its left).
+__device__ __forceinline__ int noise_at(const int16_t* T, int psx, int psy, int row, int j, int rnd, int rnd_prev,
+                                        bool blend, int gmin, int gmax) {
   const int ox = rnd >> 4, oy = rnd & 15;
   const int pox = psx ? 6 + ox : 9 + 2 * ox;
   const int poy = psy ? 6 + oy : 9 + 2 * oy;
   int gv = T[(poy + row) * kTW + pox + j];
-  if (overlap && b > 0 && j < (psx ? 1 : 2)) {
-    const int rp = off[s * nb + b - 1];
-    const int oxp = rp >> 4, oyp = rp & 15;
+  if (blend) {
+    const int oxp = rnd_prev >> 4, oyp = rnd_prev & 15;
     const int poxp = psx ? 6 + oxp : 9 + 2 * oxp;
     const int poyp = psy ? 6 + oyp : 9 + 2 * oyp;
-    const int old = T[(poyp + row) * kTW + poxp + j + bw];
+    const int old = T[(poyp + row) * kTW + poxp + j + (32 >> psx)];
     gv = psx ? old * 23 + gv * 22 : (j == 0 ? old * 27 + gv * 17 : old * 17 + gv * 27);
     gv = clip3(gmin, gmax, round2(gv, 5));
   }
   return gv;
 }
 
-// scale_lut of grain.rs:166-177.
-__device__ __forceinline__ int grain_scale(const uint8_t* lut, int index, int bd) {
-  const int sh = bd - 8;
-  const int x = index >> sh;
-  const int rem = index - (x << sh);
-  if (bd == 8 || x == 255) return lut[x];
-  const int start = lut[x], end = lut[x + 1];
-  return start + round2((end - start) * rem, sh);
-}
-
-// Item: plane tile [x0,x1) x [y0,y1) of the visible area. 256 threads.
-__global__ void __launch_bounds__(256) output_kernel(const FrameDesc* __restrict__ frames,
+// Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
+// 256 (so of the grain block width). The rows are taken one noise stripe
+// (32 rows, 16 for vertically subsampled chroma) at a time, with the
+// stripe's block offsets staged in shared memory; 256 threads, 8 consecutive
+// samples (one grain block) per thread per step.
+__global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restrict__ frames,
                                                      const Item* __restrict__ items, int n_items) {
+  __shared__ __align__(16) int16_t T[kTH * kTW];
+  __shared__ int16_t lut[256];
+  // block offsets of stripes s and s-1, blocks b0-1 .. b0+16
+  __shared__ uint8_t offs_cur[kOutOffs], offs_prev[kOutOffs];
+  int loaded = -1;  // frame * 4 + plane whose template is in T
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
-    const FrameDesc& f = frames[item.frame];
-    const int p = item.plane;
-    const int bd = f.bd, sb = f.sb;
-    const int psx = plane_ssx(f, p), psy = plane_ssy(f, p);
-    const int w = f.uw, h = f.fh;
-    const int pw = (w + psx) >> psx;
-    const bool wide = bd > 8;
-    uint8_t* out = f.frame_out + f.out_off[p];
-    const DPlane src = f.ref[p];
-    const av1pf_film_grain& g = f.g;
-    bool grain = f.grain_on != 0;
-    if (grain) {
-      grain = p == 0 ? g.num_y_points > 0
-                     : ((p == 1 ? g.num_cb_points : g.num_cr_points) > 0 || g.chroma_scaling_from_luma);
-    }
-    // tiles are at most 64 columns wide: 64 fixed slots per row
-    const int tw = int(item.x1) - int(item.x0);
-    const int n = 64 * (int(item.y1) - int(item.y0));
-    for (int k = threadIdx.x; k < n; k += 256) {
-      if ((k & 63) >= tw) continue;
-      const int yy = item.y0 + (k >> 6), xx = item.x0 + (k & 63);
-      const int orig = ld_sample(src, sb, xx, yy);
-      int v = orig;
-      if (grain) {
+    OutParams P;
+    {
+      const FrameDesc& f = frames[item.frame];
+      const int p = item.plane;
+      P.bd = f.bd;
+      P.sb = f.sb;
+      P.psx = plane_ssx(f, p);
+      P.psy = plane_ssy(f, p);
+      P.ssx = f.ssx;
+      P.ssy = f.ssy;
+      P.w = f.uw;
+      P.pw = (f.uw + P.psx) >> P.psx;
+      P.wide = P.bd > 8;
+      P.out = f.frame_out + f.out_off[p];
+      P.src = f.ref[p].p;
+      P.src_pitch = f.ref[p].stride * P.sb;
+      P.luma = f.ref[0].p;
+      P.luma_pitch = f.ref[0].stride * P.sb;
+      const av1pf_film_grain& g = f.g;
+      P.grain = f.grain_on != 0 &&
+                (p == 0 ? g.num_y_points > 0
+                        : ((p == 1 ? g.num_cb_points : g.num_cr_points) > 0 || g.chroma_scaling_from_luma));
+      if (P.grain) {
+        const int bd = P.bd;
         const int grain_center = 128 << (bd - 8);
-        const int gmin = -grain_center, gmax = (256 << (bd - 8)) - 1 - grain_center;
-        const int16_t* T = &f.grain->tmpl[p][0][0];
-        const uint8_t* lut = f.grain->lut[p];
-        const bool overlap = g.overlap_flag != 0;
-        // noise image (grain.rs:251-283)
-        const int stripe = yy >> (5 - psy);
-        const int i = yy - (stripe << (5 - psy));
-        int noise = grain_hval(T, f.grain_off, f.grain_nb, psx, psy, stripe, i, xx, overlap, gmin, gmax);
-        if (overlap && stripe > 0 && i < (psy ? 1 : 2)) {
-          const int old = grain_hval(T, f.grain_off, f.grain_nb, psx, psy, stripe - 1, i + (32 >> psy), xx, overlap,
-                                     gmin, gmax);
-          noise = psy ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
-          noise = clip3(gmin, gmax, round2(noise, 5));
-        }
-        int min_value, max_luma, max_chroma;
+        P.gmin = -grain_center;
+        P.gmax = (256 << (bd - 8)) - 1 - grain_center;
+        P.off = f.grain_off;
+        P.nb = f.grain_nb;
+        P.overlap = g.overlap_flag != 0;
+        P.csfl = g.chroma_scaling_from_luma != 0;
         if (g.clip_to_restricted_range) {
-          min_value = 16 << (bd - 8);
-          max_luma = 235 << (bd - 8);
-          max_chroma = f.mc == 0 ? max_luma : (240 << (bd - 8));  // MC_IDENTITY
+          P.min_value = 16 << (bd - 8);
+          const int max_luma = 235 << (bd - 8);
+          P.max_v = p == 0 ? max_luma : (f.mc == 0 ? max_luma : (240 << (bd - 8)));  // MC_IDENTITY
         } else {
-          min_value = 0;
-          max_luma = max_chroma = (256 << (bd - 8)) - 1;
+          P.min_value = 0;
+          P.max_v = (256 << (bd - 8)) - 1;
         }
-        const int scaling_shift = g.grain_scaling_minus_8 + 8;
-        if (p == 0) {
-          noise = round2(grain_scale(lut, orig, bd) * noise, scaling_shift);
-          v = clip3(min_value, max_luma, orig + noise);
-        } else {
-          // grain.rs:301-343
-          const int lx = xx << f.ssx, ly = yy << f.ssy;
-          const int lnx = min(lx + 1, w - 1);
-          const DPlane L = f.ref[0];
-          const int avg = f.ssx ? round2(ld_sample(L, sb, lx, ly) + ld_sample(L, sb, lnx, ly), 1)
-                                : ld_sample(L, sb, lx, ly);
-          int merged;
-          if (g.chroma_scaling_from_luma) {
-            merged = avg;
-          } else {
-            const int mult = p == 1 ? g.cb_mult : g.cr_mult;
-            const int lmult = p == 1 ? g.cb_luma_mult : g.cr_luma_mult;
-            const int offs = p == 1 ? g.cb_offset : g.cr_offset;
-            const int combined = avg * (lmult - 128) + orig * (mult - 128);
-            merged = clip3(0, (1 << bd) - 1, (combined >> 6) + ((offs - 256) * (1 << (bd - 8))));
-          }
-          noise = round2(grain_scale(lut, merged, bd) * noise, scaling_shift);
-          v = clip3(min_value, max_chroma, orig + noise);
+        P.maxpix = (1 << bd) - 1;
+        P.scaling_shift = g.grain_scaling_minus_8 + 8;
+        P.mult = p == 1 ? g.cb_mult : g.cr_mult;
+        P.lmult = p == 1 ? g.cb_luma_mult : g.cr_luma_mult;
+        P.offs = p == 1 ? g.cb_offset : g.cr_offset;
+        const int key = int(item.frame) * 4 + p;
+        if (key != loaded) {  // the plane's template and scaling table
+          __syncthreads();
+          const int16_t* tg = &f.grain->tmpl[p][0][0];
+          for (int k = threadIdx.x; k < kTH * kTW / 2; k += 256)
+            reinterpret_cast<uint32_t*>(T)[k] = reinterpret_cast<const uint32_t*>(tg)[k];
+          for (int k = threadIdx.x; k < 256; k += 256) lut[k] = f.grain->lut[p][k];
+          loaded = key;
         }
       }
-      const int64_t o = int64_t(yy) * pw + xx;
-      if (wide)
-        reinterpret_cast<uint16_t*>(out)[o] = uint16_t(v);  // little-endian u16 (frame.rs:153-158)
-      else
-        out[o] = uint8_t(v);
+    }
+    const int x0 = item.x0, x1 = item.x1;
+    const int ngroups = (x1 - x0 + 7) >> 3;  // 8-sample groups per row (<= 32)
+    const int sh = P.bd - 8;
+    const int bshift = 5 - P.psx;  // grain block width 32 >> psx
+    const int sshift = 5 - P.psy;  // noise stripe height 32 >> psy
+    const int b0 = x0 >> bshift;
+    for (int ys = item.y0; ys < int(item.y1);) {
+      const int stripe = ys >> sshift;
+      const int ye = min(int(item.y1), (stripe + 1) << sshift);
+      if (P.grain && threadIdx.x < kOutOffs) {
+        const int b = b0 - 1 + int(threadIdx.x);
+        const bool ok = b >= 0 && b < P.nb;
+        offs_cur[threadIdx.x] = ok ? P.off[int64_t(stripe) * P.nb + b] : 0;
+        offs_prev[threadIdx.x] = ok && stripe > 0 ? P.off[int64_t(stripe - 1) * P.nb + b] : 0;
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
+        const int gx = k & 31, r = k >> 5;
+        if (gx >= ngroups) continue;
+        const int yy = ys + r;
+        const int xs = x0 + gx * 8;
+        const int n = min(8, x1 - xs);
+        int v[8];
+        const uint8_t* sp = P.src + int64_t(yy) * P.src_pitch + int64_t(xs) * P.sb;
+        const bool vec = n == 8 && (reinterpret_cast<uintptr_t>(sp) & (8 * P.sb - 1)) == 0;
+        if (vec && P.sb == 2) {
+          const uint4 q = *reinterpret_cast<const uint4*>(sp);
+          v[0] = q.x & 0xffff; v[1] = q.x >> 16; v[2] = q.y & 0xffff; v[3] = q.y >> 16;
+          v[4] = q.z & 0xffff; v[5] = q.z >> 16; v[6] = q.w & 0xffff; v[7] = q.w >> 16;
+        } else if (vec) {
+          const uint2 q = *reinterpret_cast<const uint2*>(sp);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            v[e] = (q.x >> (8 * e)) & 0xff;
+            v[4 + e] = (q.y >> (8 * e)) & 0xff;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; e++)
+            v[e] = e < n ? (P.sb == 1 ? int(sp[e]) : int(reinterpret_cast<const uint16_t*>(sp)[e])) : 0;
+        }
+        if (P.grain) {
+          // noise image (grain.rs:251-283); the 8 samples share one grain block
+          const int i = yy - (stripe << sshift);
+          const int b = xs >> bshift;
+          const int jb = xs - (b << bshift);
+          const int li = b - b0 + 1;  // index into the staged offsets
+          const bool vblend = P.overlap && stripe > 0 && i < (P.psy ? 1 : 2);
+          int lum[8];
+          if (item.plane != 0) {
+            // un-grained luma under each chroma sample (grain.rs:303-314)
+            const int ly = yy << P.ssy;
+            const uint8_t* lrow = P.luma + int64_t(ly) * P.luma_pitch;
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              if (e < n) {
+                const int lx = (xs + e) << P.ssx;
+                const int lnx = min(lx + 1, P.w - 1);
+                const int l0 = P.sb == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
+                const int l1 = P.sb == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
+                lum[e] = P.ssx ? round2(l0 + l1, 1) : l0;
+              }
+            }
+          }
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            if (e >= n) continue;
+            const int j = jb + e;
+            const bool hblend = P.overlap && b > 0 && j < (P.psx ? 1 : 2);
+            int noise = noise_at(T, P.psx, P.psy, i, j, offs_cur[li], offs_cur[li - 1], hblend, P.gmin, P.gmax);
+            if (vblend) {
+              const int old = noise_at(T, P.psx, P.psy, i + (32 >> P.psy), j, offs_prev[li], offs_prev[li - 1],
+                                       hblend, P.gmin, P.gmax);
+              noise = P.psy ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
+              noise = clip3(P.gmin, P.gmax, round2(noise, 5));
+            }
+            const int orig = v[e];
+            int idx = orig;
+            if (item.plane != 0) {
+              if (P.csfl) {
+                idx = lum[e];
+              } else {
+                const int combined = lum[e] * (P.lmult - 128) + orig * (P.mult - 128);
+                idx = clip3(0, P.maxpix, (combined >> 6) + ((P.offs - 256) * (1 << sh)));
+              }
+            }
+            noise = round2(grain_scale(lut, idx, sh) * noise, P.scaling_shift);
+            v[e] = clip3(P.min_value, P.max_v, orig + noise);
+          }
+        }
+        // pack (frame.rs:153-158): u8 at 8-bit, little-endian u16 above
+        const int64_t o = int64_t(yy) * P.pw + xs;
+        if (P.wide) {
+          uint16_t* op = reinterpret_cast<uint16_t*>(P.out) + o;
+          if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 15) == 0) {
+            uint4 q;
+            q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 16);
+            q.y = uint32_t(v[2]) | (uint32_t(v[3]) << 16);
+            q.z = uint32_t(v[4]) | (uint32_t(v[5]) << 16);
+            q.w = uint32_t(v[6]) | (uint32_t(v[7]) << 16);
+            *reinterpret_cast<uint4*>(op) = q;
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; e++)
+              if (e < n) op[e] = uint16_t(v[e]);
+          }
+        } else {
+          uint8_t* op = P.out + o;
+          if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 7) == 0) {
+            uint2 q;
+            q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 8) | (uint32_t(v[2]) << 16) | (uint32_t(v[3]) << 24);
+            q.y = uint32_t(v[4]) | (uint32_t(v[5]) << 8) | (uint32_t(v[6]) << 16) | (uint32_t(v[7]) << 24);
+            *reinterpret_cast<uint2*>(op) = q;
+          } else {
+#pragma unroll
+            for (int e = 0; e < 8; e++)
+              if (e < n) op[e] = uint8_t(v[e]);
+          }
+        }
+      }
+      __syncthreads();
+      ys = ye;
     }
   }
 }

@@ -34,6 +34,8 @@ void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* 
 
 // Super-resolution (superres.cu)
 void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// Sets superres_kernel's dynamic shared-memory limit on the current device.
+cudaError_t superres_init();
 
 // Loop restoration (lr.cu)
 void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);

@@ -48,10 +48,34 @@ __device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, in
   return lvl;
 }
 
+// Small tables the decisions index with per-lane values, copied to shared
+// memory (constant memory serialises divergent indices).
+struct LfTables {
+  uint8_t subsampled[22][2][2];
+  uint8_t bw_log2[23], bh_log2[23];  // log2 of block width/height in samples (22 = invalid)
+  uint8_t txw_log2[19], txh_log2[19];
+  uint8_t txw[19], txh[19];
+};
+
+__device__ __forceinline__ void load_lf_tables(LfTables& t) {
+  for (int k = threadIdx.x; k < 22 * 4; k += blockDim.x) (&t.subsampled[0][0][0])[k] = (&c_subsampled_size[0][0][0])[k];
+  for (int k = threadIdx.x; k < 23; k += blockDim.x) {
+    t.bw_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4w[k]))) : 0;
+    t.bh_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4h[k]))) : 0;
+  }
+  for (int k = threadIdx.x; k < 19; k += blockDim.x) {
+    t.txw[k] = c_tx_w[k];
+    t.txh[k] = c_tx_h[k];
+    t.txw_log2[k] = uint8_t(31 - __clz(c_tx_w[k]));
+    t.txh_log2[k] = uint8_t(31 - __clz(c_tx_h[k]));
+  }
+}
+
 // edge_loop_filter's decision (postfilter.rs:107-172) for the 4x4 at plane
 // position (cx, cy): 0 = not filtered, else (size code << 6) | lvl with size
-// code 1 = 4, 2 = 8, 3 = 16.
-__device__ int lf_decide(const FrameDesc& f, int plane, int pass, int cx, int cy) {
+// code 1 = 4, 2 = 8, 3 = 16. Block and transform sizes are powers of two, so
+// the edge tests are masks.
+__device__ int lf_decide(const FrameDesc& f, const LfTables& tb, int plane, int pass, int cx, int cy) {
   const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
   int row = cy << sy, col = cx << sx;
   const int x = col * 4, y = row * 4;
@@ -74,7 +98,7 @@ __device__ int lf_decide(const FrameDesc& f, int plane, int pass, int cx, int cy
     atomicOr(&g_error_flags, ERRF_BAD_MAP);
     return 0;
   }
-  const int plane_size = c_subsampled_size[mi_size][sx][sy];
+  const int plane_size = tb.subsampled[mi_size][sx][sy];
   if (plane_size >= 22) {
     atomicOr(&g_error_flags, ERRF_BAD_MAP);
     return 0;
@@ -82,13 +106,13 @@ __device__ int lf_decide(const FrameDesc& f, int plane, int pass, int cx, int cy
   bool is_block_edge, is_tx_edge;
   int base;
   if (pass == 0) {
-    is_block_edge = (xp % (4 * c_n4w[plane_size])) == 0;
-    is_tx_edge = (xp % c_tx_w[tx_sz]) == 0;
-    base = min(c_tx_w[prev_tx], c_tx_w[tx_sz]);
+    is_block_edge = (xp & ((1 << tb.bw_log2[plane_size]) - 1)) == 0;
+    is_tx_edge = (xp & ((1 << tb.txw_log2[tx_sz]) - 1)) == 0;
+    base = min(tb.txw[prev_tx], tb.txw[tx_sz]);
   } else {
-    is_block_edge = (yp % (4 * c_n4h[plane_size])) == 0;
-    is_tx_edge = (yp % c_tx_h[tx_sz]) == 0;
-    base = min(c_tx_h[prev_tx], c_tx_h[tx_sz]);
+    is_block_edge = (yp & ((1 << tb.bh_log2[plane_size]) - 1)) == 0;
+    is_tx_edge = (yp & ((1 << tb.txh_log2[tx_sz]) - 1)) == 0;
+    base = min(tb.txh[prev_tx], tb.txh[tx_sz]);
   }
   if (!(is_tx_edge && (is_block_edge || !skip || is_intra))) return 0;
   const int size = plane == 0 ? min(16, base) : min(8, base);
@@ -129,6 +153,9 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
                                                       const Item* __restrict__ items, int n_items,
                                                       uint64_t* __restrict__ list_v, uint64_t* __restrict__ list_h,
                                                       uint32_t* __restrict__ counts, uint32_t cap) {
+  __shared__ LfTables tb;
+  load_lf_tables(tb);
+  __syncthreads();
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -170,13 +197,32 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
         const bool in = (k & 15) < tw && cx < gw && cy < gh;
         int dv = 0, dh = 0;
         if (in) {
-          dv = lf_decide(f, plane, 0, cx, cy);
-          dh = lf_decide(f, plane, 1, cx, cy);
+          dv = lf_decide(f, tb, plane, 0, cx, cy);
+          dh = lf_decide(f, tb, plane, 1, cx, cy);
         }
         append_edge(list_v, &counts[0], cap, dv != 0, pack_edge(item.frame, plane, dv, cx, cy));
         append_edge(list_h, &counts[1], cap, dh != 0, pack_edge(item.frame, plane, dh, cx, cy));
       }
     }
+  }
+}
+
+// The wide filter of 7.14.6.4 with N taps each side (inner weight-2 taps
+// |j| <= N2), output positions 7-N .. 7+N-1, all indices compile-time.
+template <int N, int N2, int LOG2>
+__device__ __forceinline__ void lf_wide(int32_t v[14]) {
+  int32_t o[14];
+#pragma unroll
+  for (int k = 0; k < 14; k++) o[k] = v[k];
+#pragma unroll
+  for (int i = -N; i < N; i++) {
+    int32_t acc = 0;
+#pragma unroll
+    for (int j = -N; j <= N; j++) {
+      const int pp = (i + j) < -(N + 1) ? -(N + 1) : ((i + j) > N ? N : (i + j));
+      acc += o[7 + pp] * ((j <= N2 && j >= -N2) ? 2 : 1);
+    }
+    v[7 + i] = (acc + (1 << (LOG2 - 1))) >> LOG2;
   }
 }
 
@@ -231,23 +277,21 @@ __device__ __forceinline__ void lf_filter_one(int32_t v[14], int filter_size, bo
     return;
   }
   // wide filters (7.14.6.4)
-  const int log2_size = (filter_size == 8 || !flat2) ? 3 : 4;
-  const int n = log2_size == 4 ? 6 : (!chroma ? 3 : 2);
-  const int n2 = (log2_size == 3 && !chroma) ? 0 : 1;
-  int32_t orig[14];
-#pragma unroll
-  for (int k = 0; k < 14; k++) orig[k] = v[k];
-  for (int i = -n; i < n; i++) {
-    int32_t acc = 0;
-    for (int j = -n; j <= n; j++) {
-      const int pp = clip3(-(n + 1), n, i + j);
-      const int tap = abs(j) <= n2 ? 2 : 1;
-      acc += orig[7 + pp] * tap;
+  if (filter_size == 8 || !flat2) {
+    if (chroma) {
+      lf_wide<2, 1, 3>(v);
+      lo = 5;
+      hi = 9;
+    } else {
+      lf_wide<3, 0, 3>(v);
+      lo = 4;
+      hi = 10;
     }
-    v[7 + i] = (acc + (1 << (log2_size - 1))) >> log2_size;
+  } else {
+    lf_wide<6, 1, 4>(v);
+    lo = 1;
+    hi = 13;
   }
-  lo = 7 - n;
-  hi = 7 + n;
 }
 
 __device__ __forceinline__ void lf_limits(int lvl, int sharp, int& limit, int& blimit, int& thresh) {
@@ -331,7 +375,9 @@ __global__ void __launch_bounds__(256) lf_edge_kernel(const FrameDesc* __restric
     }
     int lo, hi;
     lf_filter_one(v, filter_size, plane != 0, bd, limit, blimit, thresh, lo, hi);
-    for (int k = lo; k < hi; k++) {
+#pragma unroll
+    for (int k = 1; k < 13; k++) {
+      if (k < lo || k >= hi) continue;
       const int pos = epos + k - 7;
       if (PASS == 0)
         st_sample(p, sb, pos, lanepos, v[k]);
@@ -348,10 +394,13 @@ __global__ void dsp_lf_kernel(int32_t* __restrict__ edges, const av1pf_lf_edge_p
   const int e = i >> 2, lane = i & 3;
   const av1pf_lf_edge_params p = prm[e];
   int32_t v[14];
+#pragma unroll
   for (int k = 0; k < 14; k++) v[k] = edges[int64_t(e) * 56 + k * 4 + lane];
   int lo, hi;
   lf_filter_one(v, p.filter_size, p.chroma != 0, p.bit_depth, p.limit, p.blimit, p.thresh, lo, hi);
-  for (int k = lo; k < hi; k++) edges[int64_t(e) * 56 + k * 4 + lane] = v[k];
+#pragma unroll
+  for (int k = 0; k < 14; k++)
+    if (k >= lo && k < hi) edges[int64_t(e) * 56 + k * 4 + lane] = v[k];
 }
 
 // ---------------------------------------------------------------------------

@@ -150,12 +150,13 @@ extern "C" int av1pf_output_noalloc(const av1pf_frame_info* info, const av1pf_pa
     ph[k] = plane_h(info, k);
     off += int64_t(pw[k]) * ph[k] * bps;
   }
-  // Work list: 64-column tiles, as tall as needed to fit the fixed list.
+  // Work list: 256-column tiles (the kernel wants x0 a multiple of 256), as
+  // tall as needed to fit the fixed list.
   Item* items = reinterpret_cast<Item*>(g_staging.bytes + kDescBytes);
   int th = 32;
   auto count = [&](int t) {
     size_t n = 0;
-    for (int k = 0; k < np; k++) n += size_t((pw[k] + 63) / 64) * size_t((ph[k] + t - 1) / t);
+    for (int k = 0; k < np; k++) n += size_t((pw[k] + 255) / 256) * size_t((ph[k] + t - 1) / t);
     return n;
   };
   while (count(th) + 1 > kMaxItems) th *= 2;
@@ -167,12 +168,12 @@ extern "C" int av1pf_output_noalloc(const av1pf_frame_info* info, const av1pf_pa
   const int first_out = n;
   for (int k = 0; k < np; k++)
     for (int y = 0; y < ph[k]; y += th)
-      for (int x = 0; x < pw[k]; x += 64) {
+      for (int x = 0; x < pw[k]; x += 256) {
         Item it{};
         it.plane = uint8_t(k);
         it.x0 = uint16_t(x);
         it.y0 = uint16_t(y);
-        it.x1 = uint16_t(x + 64 < pw[k] ? x + 64 : pw[k]);
+        it.x1 = uint16_t(x + 256 < pw[k] ? x + 256 : pw[k]);
         it.y1 = uint16_t(y + th < ph[k] ? y + th : ph[k]);
         items[n++] = it;
       }

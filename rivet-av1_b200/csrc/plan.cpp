@@ -382,7 +382,8 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         d.out_off[k] = off;
         const int pw = plane_w(i, k, i->upscaled_width), ph = plane_h(i, k);
         off += int64_t(pw) * ph * bps;
-        add_tiles(plan.out_items, fi, k, 0, pw, ph, 64, 32);
+        // 256 columns by one noise stripe (32 rows, 16 in vertically subsampled chroma)
+        add_tiles(plan.out_items, fi, k, 0, pw, ph, 256, k ? 32 >> i->subsampling_y : 32);
       }
       if (p->film_grain.apply) {
         plan.any_grain = true;

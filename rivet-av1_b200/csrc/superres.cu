@@ -8,55 +8,101 @@
 // frame is upscaled only at those rows, into a small line buffer.
 // Item kind 0: rows [y0, y1) of cdef -> up. Kind 1: line rows [y0, y1) of the
 // line buffer (4 per stripe boundary: rows B-2 .. B+1 of the boundary at B).
+// Each source row is staged once in shared memory (16-byte loads), then every
+// output sample reads its 8 taps from there.
 #include "common.cuh"
 #include "kernels.h"
 
 namespace av1pf {
 
+namespace {
+constexpr int kMaxRow = 16384 + 16;  // source samples staged per row
+}
+
 __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restrict__ frames,
                                                        const Item* __restrict__ items, int n_items) {
-  __shared__ int16_t filt[64][8];
-  for (int k = threadIdx.x; k < 64 * 8; k += blockDim.x) filt[k >> 3][k & 7] = g_upscale_filter[k >> 3][k & 7];
+  extern __shared__ __align__(16) uint8_t sr_smem[];
+  int16_t* filt = reinterpret_cast<int16_t*>(sr_smem);               // [64][8]
+  uint16_t* row = reinterpret_cast<uint16_t*>(sr_smem + 64 * 8 * 2);  // staged source row
+  for (int k = threadIdx.x; k < 64 * 8; k += blockDim.x) filt[k] = g_upscale_filter[k >> 3][k & 7];
   __syncthreads();
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
-    const FrameDesc& f = frames[item.frame];
-    const int p = item.plane;
-    const int sy = plane_ssy(f, p);
-    const int sb = f.sb;
-    const int maxv = (1 << f.bd) - 1;
-    const int step = f.sr_step[p], init = f.sr_init[p], max_x = f.sr_maxx[p], w = f.sr_w[p];
-    const int plane_h = (f.fh + sy) >> sy;
-    const DPlane src = item.kind == 0 ? f.cdef[p] : f.cur[p];
-    const DPlane dst = item.kind == 0 ? f.up[p] : f.lines[p];
+    int p, sy, sb, maxv, step, init, max_x, w, plane_h, kind;
+    DPlane src, dst;
+    {
+      const FrameDesc& f = frames[item.frame];
+      p = item.plane;
+      kind = item.kind;
+      sy = plane_ssy(f, p);
+      sb = f.sb;
+      maxv = (1 << f.bd) - 1;
+      step = f.sr_step[p];
+      init = f.sr_init[p];
+      max_x = f.sr_maxx[p];
+      w = f.sr_w[p];
+      plane_h = (f.fh + sy) >> sy;
+      src = kind == 0 ? f.cdef[p] : f.cur[p];
+      dst = kind == 0 ? f.up[p] : f.lines[p];
+    }
+    const int n_src = max_x + 1;
     for (int r = item.y0; r < item.y1; r++) {
-      int sy_row = r;
-      if (item.kind == 1) {
+      int src_row = r;
+      if (kind == 1) {
         const int s = r / 4 + 1, j = r % 4;
         const int B = (64 * s - 8) >> sy;
-        sy_row = B - 2 + j;
-        if (sy_row < 0 || sy_row >= plane_h) continue;
+        src_row = B - 2 + j;
       }
-      for (int x = threadIdx.x; x < w; x += blockDim.x) {
-        // postfilter.rs:547-561
-        const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
-        const int px = int(src_x >> 14);
-        const int phase = int((src_x & 0x3fff) >> 8);
-        int sum = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const int sx = min(max(px + k - 3, 0), max_x);
-          sum += ld_sample(src, sb, sx, sy_row) * filt[phase][k];
+      const bool live = src_row >= 0 && src_row < plane_h;  // uniform across the CTA
+      if (live) {
+        const uint8_t* sp = src.p + int64_t(src_row) * src.stride * sb;
+        if (sb == 2) {
+          const int nv = n_src >> 3;
+          for (int k = threadIdx.x; k < nv; k += blockDim.x)
+            reinterpret_cast<uint4*>(row)[k] = reinterpret_cast<const uint4*>(sp)[k];
+          for (int k = nv * 8 + threadIdx.x; k < n_src; k += blockDim.x)
+            row[k] = reinterpret_cast<const uint16_t*>(sp)[k];
+        } else {
+          for (int k = threadIdx.x; k < n_src; k += blockDim.x) row[k] = sp[k];
         }
-        st_sample(dst, sb, x, r, min(max(round2(sum, 7), 0), maxv));
       }
+      __syncthreads();
+      if (live) {
+        uint8_t* dp = dst.p + int64_t(r) * dst.stride * sb;
+        for (int x = threadIdx.x; x < w; x += blockDim.x) {
+          // postfilter.rs:547-561
+          const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
+          const int px = int(src_x >> 14);
+          const int phase = int((src_x & 0x3fff) >> 8);
+          const int16_t* fk = &filt[phase * 8];
+          int sum = 0;
+          if (px - 3 >= 0 && px + 4 <= max_x) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) sum += int(row[px - 3 + k]) * fk[k];
+          } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) sum += int(row[min(max(px + k - 3, 0), max_x)]) * fk[k];
+          }
+          const int v = min(max(round2(sum, 7), 0), maxv);
+          if (sb == 2)
+            reinterpret_cast<uint16_t*>(dp)[x] = uint16_t(v);
+          else
+            dp[x] = uint8_t(v);
+        }
+      }
+      __syncthreads();
     }
   }
 }
 
+cudaError_t superres_init() {
+  return cudaFuncSetAttribute(superres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              64 * 8 * 2 + kMaxRow * 2);
+}
+
 void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  superres_kernel<<<min(n_items, kMaxGrid), 256, 0, s>>>(frames, items, n_items);
+  superres_kernel<<<min(n_items, kMaxGrid), 256, 64 * 8 * 2 + kMaxRow * 2, s>>>(frames, items, n_items);
   note_launch();
 }
 
