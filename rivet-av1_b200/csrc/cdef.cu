@@ -54,24 +54,35 @@ __device__ __forceinline__ void cdef_tap(int p, int x, int str, int adj, int w, 
   mn = min(mn, unsigned(p));
 }
 
+// MODE 0: primary and secondary taps, result clamped to the available taps'
+// [min, max]. MODE 1 (secondary strength 0) and MODE 2 (primary strength
+// 0) leave out the zero-strength taps, whose constrain() is 0, and the
+// clamp: with one kind of tap the weights sum to 12 < 16, so
+// x + round(sum / 16) already lies within [x - D, x + D'] where D, D' are the
+// largest negative and positive differences of the taps in use.
+template <int MODE>
 __device__ __forceinline__ int cdef_px(const int16_t* c, const TapsDev& t) {
   const int x = c[0];
   int sum = 0, mx = x;
   unsigned mn = unsigned(x);
-  cdef_tap(c[t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-  cdef_tap(c[-t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-  cdef_tap(c[t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-  cdef_tap(c[-t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-  cdef_tap(c[t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-  cdef_tap(c[-t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-  cdef_tap(c[t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
-  cdef_tap(c[-t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
-  cdef_tap(c[t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-  cdef_tap(c[-t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-  cdef_tap(c[t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-  cdef_tap(c[-t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+  if (MODE != 2) {
+    cdef_tap(c[t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+    cdef_tap(c[-t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+    cdef_tap(c[t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+    cdef_tap(c[-t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+  }
+  if (MODE != 1) {
+    cdef_tap(c[t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[-t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[-t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[-t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[-t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+  }
   const int v = x + ((8 + sum - (sum < 0 ? 1 : 0)) >> 4);
-  return min(max(v, int(mn)), mx);
+  return MODE == 0 ? min(max(v, int(mn)), mx) : v;
 }
 
 // The Taps of cdef_filter_block (postfilter.rs:489-511) for a window of row
@@ -175,8 +186,77 @@ __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int32_t
   c2 = cdef_cost_of<P + 4>(b);
 }
 
+// Stages plane p of superblock (sc, sr) with its 2-sample border into the
+// window `wp` as int16, unavailable samples as kNA. Window rows are NCH
+// chunks of 8 samples (the first chunk starts 8 samples left of the
+// superblock, so loads stay 8-sample aligned); a thread's loads all issue
+// before its stores.
+template <int SX>
+__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int sr, int16_t* wp, int tid) {
+  constexpr int NCH = ((64 >> SX) + 16) / 8;
+  constexpr int kSlots = (kRows * NCH + 255) / 256;
+  const int sy = plane_ssy(f, p), sb = f.sb;
+  const int bh = (64 >> sy) + 4;
+  const int px0 = (sc * 64) >> SX, py0 = ((sr * 64) >> sy) - 2;
+  const int xlim = (f.mi_cols * 4) >> SX, ylim = (f.mi_rows * 4) >> sy;
+  const DPlane src = f.cur[p];
+  // chunk class: 0 none, 1 unavailable, 2 inside (vector load), 3 straddles the edge
+  auto kind_of = [&](int r, int gy, int gx0) {
+    if (r >= bh) return 0;
+    if (gy < 0 || gy >= ylim || gx0 + 8 <= 0 || gx0 >= xlim) return 1;
+    return (gx0 >= 0 && gx0 + 8 <= xlim) ? 2 : 3;
+  };
+  uint4 q[kSlots];
+#pragma unroll
+  for (int m = 0; m < kSlots; m++) {
+    const int k = tid + 256 * m, r = k / NCH, ch = k - r * NCH;
+    const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
+    if (kind_of(r, gy, gx0) == 2) {
+      const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
+      if (sb == 2) {
+        q[m] = *reinterpret_cast<const uint4*>(rowp + int64_t(gx0) * 2);
+      } else {
+        const uint2 h2 = *reinterpret_cast<const uint2*>(rowp + gx0);
+        q[m] = make_uint4(h2.x, h2.y, 0, 0);
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < kSlots; m++) {
+    const int k = tid + 256 * m, r = k / NCH, ch = k - r * NCH;
+    const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
+    const int kind = kind_of(r, gy, gx0);
+    if (kind == 0) continue;
+    uint32_t o[4];
+    if (kind == 2 && sb == 2) {
+      o[0] = q[m].x;
+      o[1] = q[m].y;
+      o[2] = q[m].z;
+      o[3] = q[m].w;
+    } else if (kind == 2) {
+      // bytes b0..b3 -> int16 pairs
+      o[0] = __byte_perm(q[m].x, 0, 0x4140);
+      o[1] = __byte_perm(q[m].x, 0, 0x4342);
+      o[2] = __byte_perm(q[m].y, 0, 0x4140);
+      o[3] = __byte_perm(q[m].y, 0, 0x4342);
+    } else {
+      int16_t v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int gx = gx0 + e;
+        v[e] = (kind == 3 && gx >= 0 && gx < xlim) ? int16_t(ld_sample(src, sb, gx, gy)) : kNA;
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) o[e] = uint32_t(uint16_t(v[2 * e])) | (uint32_t(uint16_t(v[2 * e + 1])) << 16);
+    }
+    uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
+#pragma unroll
+    for (int e = 0; e < 4; e++) dst[e] = o[e];
+  }
+}
+
 // Item: superblock (x0 = SB column, y0 = SB row). 256 threads.
-__global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restrict__ frames,
                                                    const Item* __restrict__ items, int n_items) {
   __shared__ __align__(16) int16_t win[3][kRows * kS];
   __shared__ int32_t cost[64][8];
@@ -193,51 +273,10 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDesc* __restric
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
     // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
     for (int p = 0; p < np; p++) {
-      const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-      const int bh = (64 >> sy) + 4;
-      const int nch = ((64 >> sx) + 16) / 8;  // chunks per window row
-      const int px0 = (sc * 64) >> sx, py0 = ((sr * 64) >> sy) - 2;
-      const int xlim = (f.mi_cols * 4) >> sx, ylim = (f.mi_rows * 4) >> sy;
-      const DPlane src = f.cur[p];
-      int16_t* wp = win[p];
-      for (int k = tid; k < bh * 16; k += 256) {
-        const int r = k >> 4, ch = k & 15;
-        if (ch >= nch) continue;
-        const int gy = py0 + r;
-        const int gx0 = px0 - kColOff + ch * 8;
-        int16_t v[8];
-        if (gy < 0 || gy >= ylim || gx0 + 8 <= 0 || gx0 >= xlim) {
-#pragma unroll
-          for (int e = 0; e < 8; e++) v[e] = kNA;
-        } else if (gx0 >= 0 && gx0 + 8 <= xlim) {
-          const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
-          if (sb == 2) {
-            const uint4 q = *reinterpret_cast<const uint4*>(rowp + int64_t(gx0) * 2);
-            const uint32_t ws[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              v[2 * e] = int16_t(ws[e] & 0xffffu);
-              v[2 * e + 1] = int16_t(ws[e] >> 16);
-            }
-          } else {
-            const uint2 q = *reinterpret_cast<const uint2*>(rowp + gx0);
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-              v[e] = int16_t((q.x >> (8 * e)) & 0xffu);
-              v[4 + e] = int16_t((q.y >> (8 * e)) & 0xffu);
-            }
-          }
-        } else {
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            const int gx = gx0 + e;
-            v[e] = (gx >= 0 && gx < xlim) ? int16_t(ld_sample(src, sb, gx, gy)) : kNA;
-          }
-        }
-        uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
-#pragma unroll
-        for (int e = 0; e < 4; e++) dst[e] = uint32_t(uint16_t(v[2 * e])) | (uint32_t(uint16_t(v[2 * e + 1])) << 16);
-      }
+      if (plane_ssx(f, p))
+        stage_plane<1>(f, p, sc, sr, win[p], tid);
+      else
+        stage_plane<0>(f, p, sc, sr, win[p], tid);
     }
     // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
     if (tid < 64) {
@@ -320,44 +359,41 @@ __global__ void __launch_bounds__(256, 3) cdef_kernel(const FrameDesc* __restric
         if (bstate[b] == 0) continue;
         const int lx = bx * w, ly = by * bhp + rr;
         const int16_t* c = &win[p][(2 + ly) * kS + kColOff + lx];
-        int out[8];
+        // results packed two int16 per word as they are produced
+        uint32_t o[4] = {0, 0, 0, 0};
         const BlkTaps bt = taps[p][b];
+#define CDEF_ROW(EXPR)                                                   \
+  _Pragma("unroll") for (int j = 0; j < 8; j++) if (j < w) {             \
+    const uint32_t v_ = uint32_t(EXPR);                                   \
+    o[j >> 1] = (j & 1) ? (o[j >> 1] | (v_ << 16)) : v_;                  \
+  }
         if (bt.copy) {
-#pragma unroll
-          for (int j = 0; j < 8; j++) out[j] = j < w ? c[j] : 0;
+          CDEF_ROW(uint16_t(c[j]))
         } else {
           const TapsDev t = taps_of(bt);
-#pragma unroll
-          for (int j = 0; j < 8; j++) out[j] = j < w ? cdef_px(c + j, t) : 0;
+          if (t.pri != 0 && t.sec != 0) {
+            CDEF_ROW(cdef_px<0>(c + j, t))
+          } else if (t.pri != 0) {
+            CDEF_ROW(cdef_px<1>(c + j, t))
+          } else {
+            CDEF_ROW(cdef_px<2>(c + j, t))
+          }
         }
+#undef CDEF_ROW
         const int gx = ((sc * 64) >> sx) + lx, gy = ((sr * 64) >> sy) + ly;
         uint8_t* row = dst.p + int64_t(gy) * dst.stride * sb;
         if (sb == 2) {
           uint16_t* r16 = reinterpret_cast<uint16_t*>(row) + gx;
-          if (w == 8) {
-            uint4 v;
-            v.x = uint32_t(out[0]) | (uint32_t(out[1]) << 16);
-            v.y = uint32_t(out[2]) | (uint32_t(out[3]) << 16);
-            v.z = uint32_t(out[4]) | (uint32_t(out[5]) << 16);
-            v.w = uint32_t(out[6]) | (uint32_t(out[7]) << 16);
-            *reinterpret_cast<uint4*>(r16) = v;
-          } else {
-            uint2 v;
-            v.x = uint32_t(out[0]) | (uint32_t(out[1]) << 16);
-            v.y = uint32_t(out[2]) | (uint32_t(out[3]) << 16);
-            *reinterpret_cast<uint2*>(r16) = v;
-          }
+          if (w == 8)
+            *reinterpret_cast<uint4*>(r16) = make_uint4(o[0], o[1], o[2], o[3]);
+          else
+            *reinterpret_cast<uint2*>(r16) = make_uint2(o[0], o[1]);
         } else {
           uint8_t* r8 = row + gx;
-          if (w == 8) {
-            uint2 v;
-            v.x = uint32_t(out[0]) | (uint32_t(out[1]) << 8) | (uint32_t(out[2]) << 16) | (uint32_t(out[3]) << 24);
-            v.y = uint32_t(out[4]) | (uint32_t(out[5]) << 8) | (uint32_t(out[6]) << 16) | (uint32_t(out[7]) << 24);
-            *reinterpret_cast<uint2*>(r8) = v;
-          } else {
-            *reinterpret_cast<uint32_t*>(r8) =
-                uint32_t(out[0]) | (uint32_t(out[1]) << 8) | (uint32_t(out[2]) << 16) | (uint32_t(out[3]) << 24);
-          }
+          if (w == 8)
+            *reinterpret_cast<uint2*>(r8) = make_uint2(__byte_perm(o[0], o[1], 0x6420), __byte_perm(o[2], o[3], 0x6420));
+          else
+            *reinterpret_cast<uint32_t*>(r8) = __byte_perm(o[0], o[1], 0x6420);
         }
       }
     }

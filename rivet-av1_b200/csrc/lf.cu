@@ -24,9 +24,9 @@
 
 namespace av1pf {
 
-// 7.14.4-5 filter_strength (postfilter.rs:207-246): the level of one 4x4.
-__device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, int plane, int pass) {
-  const uint2 raw = *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * f.mi_stride + col);
+// 7.14.4-5 filter_strength (postfilter.rs:207-246): the level of one 4x4
+// from its mode-info words.
+__device__ __forceinline__ int lf_level_raw(const FrameDesc& f, uint2 raw, int plane, int pass) {
   const int mi_segment = int((raw.x >> 24) & 7u);
   const int rf = int(int8_t((raw.x >> 16) & 0xffu));
   const int mode = int((raw.x >> 8) & 0xffu);
@@ -46,6 +46,10 @@ __device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, in
     lvl = clip3(0, 63, lvl);
   }
   return lvl;
+}
+
+__device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, int plane, int pass) {
+  return lf_level_raw(f, *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * f.mi_stride + col), plane, pass);
 }
 
 // Small tables the decisions index with per-lane values, copied to shared
@@ -71,56 +75,62 @@ __device__ __forceinline__ void load_lf_tables(LfTables& t) {
   }
 }
 
-// edge_loop_filter's decision (postfilter.rs:107-172) for the 4x4 at plane
-// position (cx, cy): 0 = not filtered, else (size code << 6) | lvl with size
-// code 1 = 4, 2 = 8, 3 = 16. Block and transform sizes are powers of two, so
-// the edge tests are masks.
-__device__ int lf_decide(const FrameDesc& f, const LfTables& tb, int plane, int pass, int cx, int cy) {
+// edge_loop_filter's decisions (postfilter.rs:107-172) for the 4x4 at plane
+// position (cx, cy), both passes: 0 = not filtered, else (size code << 6) |
+// lvl with size code 1 = 4, 2 = 8, 3 = 16. Block and transform sizes are
+// powers of two, so the edge tests are masks. The mode-info word and the
+// three transform sizes (this 4x4, its left and upper neighbours) are all
+// loaded before any is used.
+__device__ __forceinline__ void lf_decide2(const FrameDesc& f, const LfTables& tb, int plane, int cx, int cy,
+                                           int& dv, int& dh) {
+  dv = dh = 0;
   const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
   int row = cy << sy, col = cx << sx;
   const int x = col * 4, y = row * 4;
-  if (x >= f.fw || y >= f.fh || (pass == 0 && x == 0) || (pass == 1 && y == 0)) return 0;
+  if (x >= f.fw || y >= f.fh) return;
   const int xp = x >> sx, yp = y >> sy;
   row |= sy;
   col |= sx;
-  const int prev_row = row - (pass == 1 ? (1 << sy) : 0);
-  const int prev_col = col - (pass == 0 ? (1 << sx) : 0);
   const int ms = f.mi_stride;
-  const av1pf_mi* mp = f.mi + int64_t(row) * ms + col;
-  const uint32_t w0 = *reinterpret_cast<const uint32_t*>(mp);
-  const int mi_size = int(w0 & 0xffu);
-  const bool skip = (w0 >> 24) & AV1PF_MI_SKIP;
-  const bool is_intra = int(int8_t((w0 >> 16) & 0xffu)) <= 0;
   const uint8_t* txm = f.tx[plane];
+  const bool has_v = x != 0, has_h = y != 0;
+  const uint2 raw = *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * ms + col);
   const int tx_sz = txm[int64_t(row >> sy) * ms + (col >> sx)];
-  const int prev_tx = txm[int64_t(prev_row >> sy) * ms + (prev_col >> sx)];
-  if (mi_size >= 22 || tx_sz >= 19 || prev_tx >= 19) {
+  const int tx_v = has_v ? txm[int64_t(row >> sy) * ms + ((col - (1 << sx)) >> sx)] : 0;
+  const int tx_h = has_h ? txm[int64_t((row - (1 << sy)) >> sy) * ms + (col >> sx)] : 0;
+  const int mi_size = int(raw.x & 0xffu);
+  const bool skip = (raw.x >> 24) & AV1PF_MI_SKIP;
+  const bool is_intra = int(int8_t((raw.x >> 16) & 0xffu)) <= 0;
+  if (mi_size >= 22 || tx_sz >= 19 || tx_v >= 19 || tx_h >= 19) {
     atomicOr(&g_error_flags, ERRF_BAD_MAP);
-    return 0;
+    return;
   }
   const int plane_size = tb.subsampled[mi_size][sx][sy];
   if (plane_size >= 22) {
     atomicOr(&g_error_flags, ERRF_BAD_MAP);
-    return 0;
+    return;
   }
-  bool is_block_edge, is_tx_edge;
-  int base;
-  if (pass == 0) {
-    is_block_edge = (xp & ((1 << tb.bw_log2[plane_size]) - 1)) == 0;
-    is_tx_edge = (xp & ((1 << tb.txw_log2[tx_sz]) - 1)) == 0;
-    base = min(tb.txw[prev_tx], tb.txw[tx_sz]);
-  } else {
-    is_block_edge = (yp & ((1 << tb.bh_log2[plane_size]) - 1)) == 0;
-    is_tx_edge = (yp & ((1 << tb.txh_log2[tx_sz]) - 1)) == 0;
-    base = min(tb.txh[prev_tx], tb.txh[tx_sz]);
+  const int cap = plane == 0 ? 16 : 8;
+  if (has_v) {
+    const bool is_block_edge = (xp & ((1 << tb.bw_log2[plane_size]) - 1)) == 0;
+    const bool is_tx_edge = (xp & ((1 << tb.txw_log2[tx_sz]) - 1)) == 0;
+    if (is_tx_edge && (is_block_edge || !skip || is_intra)) {
+      const int size = min(cap, min(int(tb.txw[tx_v]), int(tb.txw[tx_sz])));
+      int lvl = lf_level_raw(f, raw, plane, 0);
+      if (lvl == 0) lvl = lf_level(f, row, col - (1 << sx), plane, 0);
+      if (lvl) dv = ((size >= 16 ? 3 : (size >= 8 ? 2 : 1)) << 6) | lvl;
+    }
   }
-  if (!(is_tx_edge && (is_block_edge || !skip || is_intra))) return 0;
-  const int size = plane == 0 ? min(16, base) : min(8, base);
-  int lvl = lf_level(f, row, col, plane, pass);
-  if (lvl == 0) lvl = lf_level(f, prev_row, prev_col, plane, pass);
-  if (lvl == 0) return 0;
-  const int code = size >= 16 ? 3 : (size >= 8 ? 2 : 1);
-  return (code << 6) | lvl;
+  if (has_h) {
+    const bool is_block_edge = (yp & ((1 << tb.bh_log2[plane_size]) - 1)) == 0;
+    const bool is_tx_edge = (yp & ((1 << tb.txh_log2[tx_sz]) - 1)) == 0;
+    if (is_tx_edge && (is_block_edge || !skip || is_intra)) {
+      const int size = min(cap, min(int(tb.txh[tx_h]), int(tb.txh[tx_sz])));
+      int lvl = lf_level_raw(f, raw, plane, 1);
+      if (lvl == 0) lvl = lf_level(f, row - (1 << sy), col, plane, 1);
+      if (lvl) dh = ((size >= 16 ? 3 : (size >= 8 ? 2 : 1)) << 6) | lvl;
+    }
+  }
 }
 
 // Edge list entry: frame:16 | plane:2 | code:2 | lvl:6 | cx:14 | cy:14.
@@ -169,12 +179,23 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
       const int bx0 = x0 * sb, bx1 = x1 * sb;  // byte columns (a tile row is at most 128 bytes)
       const int nvec = (bx1 - bx0) >> 4;
       const int rows = y1 - y0;
-      for (int k = threadIdx.x; k < rows * 8; k += blockDim.x) {
-        const int v = k & 7;
-        if (v >= nvec) continue;
-        const int r = y0 + (k >> 3), c = bx0 + v * 16;
-        const uint4 q = *reinterpret_cast<const uint4*>(src.p + int64_t(r) * src.stride * sb + c);
-        *reinterpret_cast<uint4*>(dst.p + int64_t(r) * dst.stride * sb + c) = q;
+      // 64 rows x 8 chunk slots = 2 per thread: both loads issue before the stores
+      for (int k0 = threadIdx.x; k0 < rows * 8; k0 += 2 * blockDim.x) {
+        uint4 q[2];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          const int k = k0 + m * blockDim.x;
+          const int r = y0 + (k >> 3), c = bx0 + (k & 7) * 16;
+          if (k < rows * 8 && (k & 7) < nvec)
+            q[m] = *reinterpret_cast<const uint4*>(src.p + int64_t(r) * src.stride * sb + c);
+        }
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          const int k = k0 + m * blockDim.x;
+          const int r = y0 + (k >> 3), c = bx0 + (k & 7) * 16;
+          if (k < rows * 8 && (k & 7) < nvec)
+            *reinterpret_cast<uint4*>(dst.p + int64_t(r) * dst.stride * sb + c) = q[m];
+        }
       }
       const int tail = (bx1 - bx0) & 15;
       if (tail) {
@@ -196,10 +217,7 @@ __global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restric
         const int cx = cx0 + (k & 15), cy = cy0 + (k >> 4);
         const bool in = (k & 15) < tw && cx < gw && cy < gh;
         int dv = 0, dh = 0;
-        if (in) {
-          dv = lf_decide(f, tb, plane, 0, cx, cy);
-          dh = lf_decide(f, tb, plane, 1, cx, cy);
-        }
+        if (in) lf_decide2(f, tb, plane, cx, cy, dv, dh);
         append_edge(list_v, &counts[0], cap, dv != 0, pack_edge(item.frame, plane, dv, cx, cy));
         append_edge(list_h, &counts[1], cap, dh != 0, pack_edge(item.frame, plane, dh, cx, cy));
       }
@@ -333,7 +351,7 @@ __device__ __forceinline__ void lf_load(const DPlane& p, int sb, int e, int lane
 }
 
 template <int PASS>
-__global__ void __launch_bounds__(256) lf_edge_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 4) lf_edge_kernel(const FrameDesc* __restrict__ frames,
                                                       const uint64_t* __restrict__ list,
                                                       const uint32_t* __restrict__ count_ptr, uint32_t cap) {
   const uint32_t n = min(*count_ptr, cap) * 4u;

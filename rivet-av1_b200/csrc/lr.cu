@@ -32,7 +32,8 @@ constexpr int kWS = 72;                  // window row stride (u16): w + 6 <= 70
 constexpr int kAS = 72;                  // A/B row stride (int32): w + 2 <= 66
 constexpr int kWinBytes = (kMaxH + 6) * kWS * 2;
 constexpr int kABytes = (kMaxH + 2) * kAS * 4;
-constexpr int kSmemBytes = kWinBytes + 2 * kABytes + 256 * 4;
+constexpr int kF0Bytes = kMaxH * kMaxW * 4;  // the first self-guided filter's output
+constexpr int kSmemBytes = kWinBytes + 2 * kABytes + 256 * 4 + kF0Bytes;
 constexpr int kRowsPerThread = kMaxH / kGroups;  // 16
 static_assert((kMaxH + 6) * kWS * 2 <= kABytes, "Wiener intermediate must fit the A area");
 }  // namespace
@@ -41,38 +42,57 @@ struct LrGeom {
   int ss, se, y0, y1, pex, pey;
 };
 
-// The row LrCtx::sample (postfilter.rs:584-596) reads for window row y of
-// stripe `s`: the source plane and row. With superres the pre-CDEF rows come
-// from the line buffer, 4 rows per stripe boundary: boundary b (the first row
-// B of stripe b) holds rows B-2 .. B+1 at line rows (b-1)*4 ...
-__device__ __forceinline__ const uint8_t* lr_row(const FrameDesc& f, int p, const LrGeom& g, int s, int y) {
+// The three sources LrCtx::sample (postfilter.rs:584-596) draws rows from,
+// read once per rectangle: the upscaled CDEF plane, the loop-filtered plane
+// and (with superres) the line buffer of upscaled pre-CDEF rows.
+struct LrSrc {
+  const uint8_t* up;
+  const uint8_t* cur;
+  const uint8_t* lines;
+  int64_t up_pitch, cur_pitch, lines_pitch;  // bytes
+  bool sr;
+};
+
+// The row LrCtx::sample reads for window row y of stripe `s`. With superres
+// the pre-CDEF rows come from the line buffer, 4 rows per stripe boundary:
+// boundary b (the first row B of stripe b) holds rows B-2 .. B+1 at line
+// rows (b-1)*4 ...
+__device__ __forceinline__ const uint8_t* lr_row(const LrSrc& src, const LrGeom& g, int s, int y) {
   y = max(min(y, g.pey), 0);
-  const int sb = f.sb;
-  DPlane src;
-  int row;
   if (y < g.ss) {
     const int yy = max(g.ss - 2, y);
-    if (f.sr_on) {
-      src = f.lines[p];
-      row = (s - 1) * 4 + (yy - (g.ss - 2));
-    } else {
-      src = f.cur[p];
-      row = yy;
-    }
-  } else if (y > g.se) {
-    const int yy = min(g.se + 2, y);
-    if (f.sr_on) {
-      src = f.lines[p];
-      row = s * 4 + (yy - (g.se - 1));
-    } else {
-      src = f.cur[p];
-      row = yy;
-    }
-  } else {
-    src = f.up[p];
-    row = y;
+    return src.sr ? src.lines + int64_t((s - 1) * 4 + (yy - (g.ss - 2))) * src.lines_pitch
+                  : src.cur + int64_t(yy) * src.cur_pitch;
   }
-  return src.p + int64_t(row) * src.stride * sb;
+  if (y > g.se) {
+    const int yy = min(g.se + 2, y);
+    return src.sr ? src.lines + int64_t(s * 4 + (yy - (g.se - 1))) * src.lines_pitch
+                  : src.cur + int64_t(yy) * src.cur_pitch;
+  }
+  return src.up + int64_t(y) * src.up_pitch;
+}
+
+// Copies a w x h rectangle (w <= 64) between planes of sample width sb:
+// 16-byte chunks when both rows are 16-byte aligned there, else samples.
+__device__ __forceinline__ void copy_rect(const DPlane& src, const DPlane& dst, int sb, int x0, int y0, int w, int h,
+                                          int tid) {
+  const int bytes = w * sb;
+  const uint8_t* s0 = src.p + (int64_t(y0) * src.stride + x0) * sb;
+  uint8_t* d0 = dst.p + (int64_t(y0) * dst.stride + x0) * sb;
+  const int64_t sp = src.stride * sb, dp = dst.stride * sb;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(d0) | uintptr_t(sp) |
+                         uintptr_t(dp)) & 15) == 0;
+  // 8 chunk slots per row (w * sb <= 128 bytes); a ragged last chunk goes bytewise
+  for (int k = tid; k < h * 8; k += kThreads) {
+    const int r = k >> 3, ch = k & 7;
+    const uint8_t* sr = s0 + r * sp + ch * 16;
+    uint8_t* dr = d0 + r * dp + ch * 16;
+    if (aligned && ch * 16 + 16 <= bytes) {
+      *reinterpret_cast<uint4*>(dr) = *reinterpret_cast<const uint4*>(sr);
+    } else {
+      for (int b = 0; b < min(16, bytes - ch * 16); b++) dr[b] = sr[b];
+    }
+  }
 }
 
 __device__ __forceinline__ int ld_row(const uint8_t* row, int sb, int x) {
@@ -177,6 +197,7 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
   int32_t* A = reinterpret_cast<int32_t*>(smem + kWinBytes);
   int32_t* B = reinterpret_cast<int32_t*>(smem + kWinBytes + kABytes);
   int32_t* a2tab = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
+  int32_t* F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes + 256 * 4);
   int16_t* inter = reinterpret_cast<int16_t*>(A);  // Wiener reuses the A area
   const int tid = threadIdx.x;
   const int g = tid / kCols, c = tid - g * kCols;
@@ -214,19 +235,36 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     }
     const DPlane dst = f.ref[p];
     if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
-      const DPlane src = f.up[p];
-      if (c < w)
-        for (int r = g; r < h; r += kGroups)
-          st_sample(dst, sb, x0 + c, geo.y0 + r, ld_sample(src, sb, x0 + c, geo.y0 + r));
+      copy_rect(f.up[p], dst, sb, x0, geo.y0, w, h, tid);
       continue;
     }
-    // lr_window (postfilter.rs:765-777)
+    // lr_window (postfilter.rs:765-777): a thread's loads all issue before its stores
     const int ww = w + 6, wh = h + 6;
     {
+      LrSrc src;
+      src.up = f.up[p].p;
+      src.cur = f.cur[p].p;
+      src.lines = f.lines[p].p;
+      src.up_pitch = f.up[p].stride * sb;
+      src.cur_pitch = f.cur[p].stride * sb;
+      src.lines_pitch = f.lines[p].stride * sb;
+      src.sr = f.sr_on != 0;
       const int x = max(min(x0 + c - 3, geo.pex), 0);
-      for (int r = g; r < wh; r += kGroups) {
-        const uint8_t* row = lr_row(f, p, geo, s, geo.y0 + r - 3);
-        if (c < ww) win[r * kWS + c] = uint16_t(ld_row(row, sb, x));
+      constexpr int kWinRows = (kMaxH + 6 + kGroups - 1) / kGroups;  // 18 window rows per thread
+      constexpr int kBatch = 6;
+#pragma unroll
+      for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
+        int v[kBatch];
+#pragma unroll
+        for (int m = 0; m < kBatch; m++) {
+          const int r = g + kGroups * (m0 + m);
+          if (r < wh && c < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
+        }
+#pragma unroll
+        for (int m = 0; m < kBatch; m++) {
+          const int r = g + kGroups * (m0 + m);
+          if (r < wh && c < ww) win[r * kWS + c] = uint16_t(v[m]);
+        }
       }
     }
     __syncthreads();
@@ -259,14 +297,13 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       // postfilter.rs:823-851 with box_filter_rect (postfilter.rs:901-991)
       const int set = unit.sgr_set & 15;
       const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][2];
-      int32_t f0[kRowsPerThread];
       if (r0) {
         sgr_ab<0>(win, A, B, a2tab, c_sgr_params[set][1], bd, geo.y0, h, w, c, g);
         __syncthreads();
 #pragma unroll
         for (int m = 0; m < kRowsPerThread; m++) {
           const int i = g + kGroups * m;
-          if (i < h && c < w) f0[m] = sgr_flt<0>(A, B, i, c, geo.y0 + i, win[(i + 3) * kWS + c + 3]);
+          if (i < h && c < w) F0[i * kMaxW + c] = sgr_flt<0>(A, B, i, c, geo.y0 + i, win[(i + 3) * kWS + c + 3]);
         }
         __syncthreads();
       }
@@ -283,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
           const int cd = win[(i + 3) * kWS + c + 3];
           const int u = cd << 4;
           int v = w1 * u;
-          v += r0 != 0 ? w0 * f0[m] : w0 * u;
+          v += r0 != 0 ? w0 * F0[i * kMaxW + c] : w0 * u;
           v += r1 != 0 ? w2 * sgr_flt<1>(A, B, i, c, geo.y0 + i, cd) : w2 * u;
           st_sample(dst, sb, x0 + c, geo.y0 + i, clip3(0, maxv, round2(v, 11)));
         }
@@ -299,7 +336,9 @@ cudaError_t lr_init() {
 
 void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  lr_kernel<<<min(n_items, kNumSMs * 3), kThreads, kSmemBytes, s>>>(frames, items, n_items);
+  // one CTA per rectangle: the block scheduler hands rectangles of uneven
+  // cost (copy, Wiener, self-guided) to SMs as they free up
+  lr_kernel<<<min(n_items, 1 << 20), kThreads, kSmemBytes, s>>>(frames, items, n_items);
   note_launch();
 }
 
