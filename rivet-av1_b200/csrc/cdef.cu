@@ -452,7 +452,7 @@ __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cde
 
 void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  cdef_kernel<<<min(n_items, kNumSMs * 4), 256, 0, s>>>(frames, items, n_items);
+  cdef_kernel<<<min(n_items, kItemGrid), 256, 0, s>>>(frames, items, n_items);
   note_launch();
 }
 

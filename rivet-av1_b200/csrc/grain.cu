@@ -481,7 +481,7 @@ void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, 
 
 void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  output_kernel<<<min(n_items, kMaxGrid), 256, 0, s>>>(frames, items, n_items);
+  output_kernel<<<min(n_items, kItemGrid), 256, 0, s>>>(frames, items, n_items);
   note_launch();
 }
 

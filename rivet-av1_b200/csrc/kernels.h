@@ -17,6 +17,9 @@ struct Item;
 // B200's 148 SMs.
 constexpr int kNumSMs = 148;
 constexpr int kMaxGrid = kNumSMs * 8;
+// Grid cap of the item kernels, which launch one CTA per item: the block
+// scheduler then hands items of uneven cost to SMs as slots free up.
+constexpr int kItemGrid = 1 << 20;
 
 // Counts every kernel launch this library issues (av1pf_launch_count).
 void note_launch(uint64_t n = 1);

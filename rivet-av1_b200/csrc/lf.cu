@@ -159,7 +159,7 @@ __device__ __forceinline__ void append_edge(uint64_t* list, uint32_t* count, uin
 
 // Item: tile [x0,x1) x [y0,y1) of plane `plane` (samples). kind bit 0: copy
 // in -> cur over the tile; bit 1: decide the tile's 4x4 edges. 256 threads.
-__global__ void __launch_bounds__(256) lf_prep_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __restrict__ frames,
                                                       const Item* __restrict__ items, int n_items,
                                                       uint64_t* __restrict__ list_v, uint64_t* __restrict__ list_h,
                                                       uint32_t* __restrict__ counts, uint32_t cap) {
@@ -427,7 +427,7 @@ __global__ void dsp_lf_kernel(int32_t* __restrict__ edges, const av1pf_lf_edge_p
 void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_v, uint64_t* list_h,
                     uint32_t* counts, uint32_t cap, cudaStream_t s) {
   if (n_items <= 0) return;
-  const int grid = min(n_items, kMaxGrid);
+  const int grid = min(n_items, kItemGrid);
   lf_prep_kernel<<<grid, 256, 0, s>>>(frames, items, n_items, list_v, list_h, counts, cap);
   note_launch();
 }

@@ -338,7 +338,7 @@ void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStre
   if (n_items <= 0) return;
   // one CTA per rectangle: the block scheduler hands rectangles of uneven
   // cost (copy, Wiener, self-guided) to SMs as they free up
-  lr_kernel<<<min(n_items, 1 << 20), kThreads, kSmemBytes, s>>>(frames, items, n_items);
+  lr_kernel<<<min(n_items, kItemGrid), kThreads, kSmemBytes, s>>>(frames, items, n_items);
   note_launch();
 }
 

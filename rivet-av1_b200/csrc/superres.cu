@@ -102,7 +102,7 @@ cudaError_t superres_init() {
 
 void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  superres_kernel<<<min(n_items, kMaxGrid), 256, 64 * 8 * 2 + kMaxRow * 2, s>>>(frames, items, n_items);
+  superres_kernel<<<min(n_items, kItemGrid), 256, 64 * 8 * 2 + kMaxRow * 2, s>>>(frames, items, n_items);
   note_launch();
 }
 
