@@ -318,11 +318,51 @@ typedef struct av1pf_batch av1pf_batch;
  * per-stage work lists and captures the stage launches into a CUDA graph.
  * `flags`: AV1PF_BATCH_NO_GRAPH launches the stages directly. */
 #define AV1PF_BATCH_NO_GRAPH 1u
+/* AV1PF_BATCH_AUTOTUNE: first run av1pf_autotune on the jobs' shapes that
+ * the context has not measured (the jobs' outputs are overwritten). */
+#define AV1PF_BATCH_AUTOTUNE 2u
 int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs,
                        uint32_t flags, av1pf_batch** out);
 /* Runs the planned batch on `stream` (graph launch). */
 int av1pf_batch_run(av1pf_batch* batch, void* stream);
 int av1pf_batch_destroy(av1pf_batch* batch);
+
+/* ------------------------------------------------------------------------ */
+/* Kernel variants and the autotuner. No counterpart in the reference, whose  */
+/* filters each have one code path; the variants compute the same samples.    */
+/* ------------------------------------------------------------------------ */
+typedef struct av1pf_tuning {
+  /* How the loop filter runs in chain calls. -1: per frame shape, the mode
+   * av1pf_autotune measured fastest (mode 0 while a shape is unmeasured).
+   * 0: one kernel decides every 4x4 edge into a compact list per direction,
+   *    then one kernel per direction filters the listed edges in place;
+   * 1: vertical edges filtered per 64x64 tile in shared memory (the tile
+   *    staged with 16 columns of halo), horizontal edges from a list;
+   * 2: as 1, with the horizontal edges filtered inside the CDEF kernel on
+   *    its staged superblock window (frames with CDEF enabled; others use
+   *    mode 1). */
+  int32_t lf_mode;
+  /* 0: per frame shape, as measured (64 while unmeasured); 32 or 64: the
+   *    width of the loop-restoration rectangles one CTA restores. */
+  int32_t lr_rect_cols;
+} av1pf_tuning;
+
+/* Sets / reads the context's variant choices (chain, chain_host, batches
+ * created afterwards, and servers created from the context). */
+int av1pf_set_tuning(av1pf_ctx* ctx, const av1pf_tuning* tuning);
+int av1pf_get_tuning(av1pf_ctx* ctx, av1pf_tuning* tuning);
+
+/* Times every variant on the first job of each frame shape (frame and
+ * upscaled width, height, bit depth, subsampling, planes) among `jobs`, as
+ * a one-frame batch replayed `reps` times, and records the fastest per
+ * shape in the context. The jobs' outputs are overwritten. Shapes already
+ * recorded are measured again. *n_shapes (may be NULL) = shapes measured. */
+int av1pf_autotune(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, int32_t reps, int32_t* n_shapes);
+
+/* The recorded choice for the shape of `info` (lf_mode 0-2 and
+ * lr_rect_cols) and its measured device time per frame in ms;
+ * AV1PF_ERR_NOT_FOUND when the shape has not been measured. */
+int av1pf_tuned_choice(av1pf_ctx* ctx, const av1pf_frame_info* info, av1pf_tuning* choice, float* ms);
 
 /* ------------------------------------------------------------------------ */
 /* Serving: continuous batching of post-filter jobs from many streams.       */

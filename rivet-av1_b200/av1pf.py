@@ -23,6 +23,7 @@ ERR_NOT_FOUND = 7
 MI_SKIP = 0x80
 RESTORE_NONE, RESTORE_WIENER, RESTORE_SGRPROJ = 0, 1, 2
 BATCH_NO_GRAPH = 1
+BATCH_AUTOTUNE = 2
 
 
 class Plane(C.Structure):
@@ -83,6 +84,10 @@ class Params(C.Structure):
 class Job(C.Structure):
     _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("maps", C.POINTER(Maps)),
                 ("inp", C.POINTER(Plane)), ("ref_out", C.POINTER(Plane)), ("frame_out", C.c_void_p)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("lf_mode", C.c_int32), ("lr_rect_cols", C.c_int32)]
 
 
 class ServeConfig(C.Structure):
@@ -171,6 +176,10 @@ def lib():
         _sig(L, "av1pf_batch_create", C.c_int, vp, P(Job), C.c_int, C.c_uint32, P(vp))
         _sig(L, "av1pf_batch_run", C.c_int, vp, vp)
         _sig(L, "av1pf_batch_destroy", C.c_int, vp)
+        _sig(L, "av1pf_set_tuning", C.c_int, vp, P(Tuning))
+        _sig(L, "av1pf_get_tuning", C.c_int, vp, P(Tuning))
+        _sig(L, "av1pf_autotune", C.c_int, vp, P(Job), C.c_int, C.c_int32, P(C.c_int32))
+        _sig(L, "av1pf_tuned_choice", C.c_int, vp, P(FrameInfo), P(Tuning), P(C.c_float))
         _sig(L, "av1pf_serve_open", C.c_int, vp, P(ServeConfig), P(vp))
         _sig(L, "av1pf_serve_open_stream", C.c_int, vp, P(FrameInfo), P(C.c_int32))
         _sig(L, "av1pf_serve_close_stream", C.c_int, vp, C.c_int32)

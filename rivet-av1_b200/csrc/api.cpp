@@ -23,7 +23,22 @@ std::mutex g_tables_mu;
 bool g_tables_ready[64] = {};
 }  // namespace
 
-void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+namespace {
+// launches enqueued while capturing a graph are counted when it runs
+thread_local int t_capturing = 0;
+thread_local uint64_t t_captured = 0;
+}  // namespace
+
+void note_launch(uint64_t n) {
+  if (t_capturing)
+    t_captured += n;
+  else
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+CaptureScope::CaptureScope() : start(t_captured) { ++t_capturing; }
+CaptureScope::~CaptureScope() { --t_capturing; }
+uint64_t CaptureScope::launches() const { return t_captured - start; }
 
 void set_error(const std::string& s) { t_last_error = s; }
 
@@ -109,9 +124,55 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
     prof_used[slot] = true;
     ev = prof_ev[slot];
   }
-  launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join, ev);
-  e = cudaGetLastError();
-  return cuda_status(e, "kernel launch");
+  if (ev) {
+    // profiled calls launch directly, with the stage events between stages
+    launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join, ev);
+    e = cudaGetLastError();
+    return cuda_status(e, "kernel launch");
+  }
+  // Calls whose plan has the same launch structure (list sizes, offsets,
+  // flags, meta buffer) replay one captured graph: the descriptors and work
+  // lists it reads were just uploaded to the same addresses.
+  std::vector<uint64_t> key;
+  launch_key(plan, meta.ptr, key);
+  GraphEntry* g = nullptr;
+  for (GraphEntry& c : graphs)
+    if (c.exec && c.key == key) g = &c;
+  if (!g) {
+    GraphEntry* slot = &graphs[0];
+    for (GraphEntry& c : graphs)
+      if (!c.exec || c.last_use < slot->last_use) slot = &c;
+    if (slot->exec) cudaGraphExecDestroy(slot->exec);
+    slot->exec = nullptr;
+    if (!capture) {
+      e = cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_status(e, "capture stream");
+    }
+    cudaGraph_t graph = nullptr;
+    uint64_t kernels = 0;
+    {
+      CaptureScope cs;
+      e = cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        launch_plan(plan, static_cast<uint8_t*>(meta.ptr), capture, side, fork, join, nullptr);
+        e = cudaStreamEndCapture(capture, &graph);
+      }
+      kernels = cs.launches();
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&slot->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      slot->exec = nullptr;
+      return cuda_status(e, "graph capture");
+    }
+    slot->key = key;
+    slot->kernels = kernels;
+    g = slot;
+  }
+  g->last_use = ++graph_clock;
+  e = cudaGraphLaunch(g->exec, s);
+  note_launch(g->kernels);
+  return cuda_status(e, "graph launch");
 }
 
 void Ctx::prof_collect(int slot) {
@@ -200,6 +261,7 @@ int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out) {
       if ((e = upload_grain_tables()) != cudaSuccess) return cuda_status(e, "grain tables");
       if ((e = lr_init()) != cudaSuccess) return cuda_status(e, "loop restoration kernel attributes");
       if ((e = superres_init()) != cudaSuccess) return cuda_status(e, "superres kernel attributes");
+      if ((e = cdef_init()) != cudaSuccess) return cuda_status(e, "CDEF kernel attributes");
       g_tables_ready[device] = true;
     }
   }
@@ -226,6 +288,9 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   ctx->release(ctx->meta);
   for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame}) ctx->release(*b);
   if (ctx->meta_host.ptr) cudaFreeHost(ctx->meta_host.ptr);
+  for (GraphEntry& g : ctx->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (ctx->capture) cudaStreamDestroy(ctx->capture);
   cudaStreamDestroy(ctx->side);
   cudaStreamDestroy(ctx->own);
   cudaEventDestroy(ctx->fork);
@@ -350,6 +415,7 @@ int av1pf_chain(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params
   }
   if ((rc = validate_maps(info, params, maps, lf_active(params), params->cdef_enabled != 0, true))) return rc;
   FrameJob j{info, params, maps, in, nullptr, ref_out, frame_out, ST_CHAIN, false};
+  ctx->apply_tuning(j);
   return ctx->run(&j, 1, as_stream(stream));
 }
 

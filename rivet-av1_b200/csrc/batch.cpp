@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "av1pf.h"
+#include "batch.h"
 #include "ctx.h"
 #include "kernels.h"
 #include "plan.h"
@@ -28,36 +29,32 @@ struct Batch {
 
 struct av1pf_batch : av1pf::Batch {};
 
-using namespace av1pf;
+namespace av1pf {
 
-extern "C" {
+int validate_job(const av1pf_job& j, int i) {
+  std::string why;
+  int rc = validate_frame(j.info, j.params, j.in, &why);
+  if (rc != AV1PF_OK) {
+    set_error("job " + std::to_string(i) + ": " + why);
+    return rc;
+  }
+  if (!j.maps || !j.ref_out) {
+    set_error("job " + std::to_string(i) + ": null maps or ref_out");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  return AV1PF_OK;
+}
 
-int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, uint32_t flags, av1pf_batch** out) {
-  if (!ctx || !jobs || n_jobs <= 0 || !out) return AV1PF_ERR_INVALID_INPUT;
+int create_batch(Ctx* ctx, const FrameJob* fj, int n_jobs, uint32_t flags, av1pf_batch** out) {
   *out = nullptr;
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
-  std::vector<FrameJob> fj(static_cast<size_t>(n_jobs));
-  for (int i = 0; i < n_jobs; i++) {
-    const av1pf_job& j = jobs[i];
-    std::string why;
-    int rc = validate_frame(j.info, j.params, j.in, &why);
-    if (rc != AV1PF_OK) {
-      set_error("job " + std::to_string(i) + ": " + why);
-      return rc;
-    }
-    if (!j.maps || !j.ref_out) {
-      set_error("job " + std::to_string(i) + ": null maps or ref_out");
-      return AV1PF_ERR_INVALID_INPUT;
-    }
-    fj[size_t(i)] = FrameJob{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
-  }
   av1pf_batch* b = new av1pf_batch();
   b->ctx = ctx;
   std::string why;
-  int rc = build_plan(fj.data(), n_jobs, nullptr, b->plan, &why);
+  int rc = build_plan(fj, n_jobs, nullptr, b->plan, &why);
   if (rc == AV1PF_OK) rc = ctx->ensure(b->scratch, b->plan.scratch_bytes + 256);
-  if (rc == AV1PF_OK) rc = build_plan(fj.data(), n_jobs, static_cast<uint8_t*>(b->scratch.ptr), b->plan, &why);
+  if (rc == AV1PF_OK) rc = build_plan(fj, n_jobs, static_cast<uint8_t*>(b->scratch.ptr), b->plan, &why);
   if (rc == AV1PF_OK) rc = ctx->ensure(b->meta, b->plan.meta_bytes + 256);
   if (rc != AV1PF_OK) {
     if (!why.empty()) set_error(why);
@@ -71,15 +68,15 @@ int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, uint32
   pack_meta(b->plan, host.data());
   e = cudaMemcpy(b->meta.ptr, host.data(), b->plan.upload_bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
-  const uint64_t before = av1pf_launch_count();
   if (e == cudaSuccess && !(flags & AV1PF_BATCH_NO_GRAPH)) {
+    CaptureScope cs;
     e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       launch_plan(b->plan, static_cast<uint8_t*>(b->meta.ptr), b->cap_stream, ctx->side, ctx->fork, ctx->join);
       e = cudaStreamEndCapture(b->cap_stream, &b->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-    b->kernels_per_run = av1pf_launch_count() - before;
+    b->kernels_per_run = cs.launches();
   }
   if (e != cudaSuccess) {
     rc = cuda_status(e, "batch create");
@@ -88,6 +85,34 @@ int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, uint32
   }
   *out = b;
   return AV1PF_OK;
+}
+
+}  // namespace av1pf
+
+using namespace av1pf;
+
+extern "C" {
+
+int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, uint32_t flags, av1pf_batch** out) {
+  if (!ctx || !jobs || n_jobs <= 0 || !out) return AV1PF_ERR_INVALID_INPUT;
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+  for (int i = 0; i < n_jobs; i++) {
+    const int rc = validate_job(jobs[i], i);
+    if (rc != AV1PF_OK) return rc;
+  }
+  if (flags & AV1PF_BATCH_AUTOTUNE) {
+    const int rc = tune_shapes(ctx, jobs, n_jobs, 10, true, nullptr);
+    if (rc != AV1PF_OK) return rc;
+  }
+  std::vector<FrameJob> fj(static_cast<size_t>(n_jobs));
+  for (int i = 0; i < n_jobs; i++) {
+    const av1pf_job& j = jobs[i];
+    fj[size_t(i)] = FrameJob{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
+    ctx->apply_tuning(fj[size_t(i)]);
+  }
+  return create_batch(ctx, fj.data(), n_jobs, flags, out);
 }
 
 int av1pf_batch_run(av1pf_batch* b, void* stream) {

@@ -1,0 +1,24 @@
+// batch.h — internal interface of the batched path, shared with the
+// autotuner (tune.cpp).
+#pragma once
+
+#include <cstdint>
+
+#include "av1pf.h"
+#include "ctx.h"
+#include "plan.h"
+
+namespace av1pf {
+
+// Checks one av1pf_job (index i names it in the error text).
+int validate_job(const av1pf_job& j, int i);
+
+// Plans `fj` (variants already chosen), uploads the work lists and, unless
+// AV1PF_BATCH_NO_GRAPH, captures the launches into a graph.
+int create_batch(Ctx* ctx, const FrameJob* fj, int n_jobs, uint32_t flags, av1pf_batch** out);
+
+// av1pf_autotune over `jobs` (validated by the caller); only_new skips the
+// shapes the context has recorded.
+int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only_new, int* n_shapes);
+
+}  // namespace av1pf

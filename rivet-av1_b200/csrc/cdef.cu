@@ -15,19 +15,23 @@
 // pair per warp), so the partial-sum bins are compile-time register indices.
 #include "common.cuh"
 #include "kernels.h"
+#include "lf_core.cuh"
 
 namespace av1pf {
 
 namespace {
 
-// Shared-memory window of one plane: 68 rows (64 + 2*2) x 80 columns
+// Shared-memory window of one plane: up to 86 rows (64 + 2*2, or 64 + 2*11
+// with the horizontal loop-filter pass fused in) x 80 columns
 // (64 + 8 on each side, so global loads stay 8-sample aligned), row stride
 // 82 int16 = 41 words: a warp's 4 rows x 8 blocks of centre loads then hit
 // 32 different banks.
 constexpr int kS = 82;
-constexpr int kRows = 68;
+constexpr int kTopLfh = 11;  // rows above (and below) the superblock with the horizontal LF pass fused
+constexpr int kRows = 64 + 2 * kTopLfh;  // 86 (68 used without the fused pass)
 constexpr int kColOff = 8;       // window column of plane x = px0
 constexpr int16_t kNA = -32768;  // unavailable sample
+constexpr int kCdefSmem = 3 * kRows * kS * 2;  // dynamic shared memory: the three windows
 
 // Per 8x8 block and plane: strengths, tap weights and window offsets.
 struct BlkTaps {
@@ -186,18 +190,19 @@ __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int32_t
   c2 = cdef_cost_of<P + 4>(b);
 }
 
-// Stages plane p of superblock (sc, sr) with its 2-sample border into the
-// window `wp` as int16, unavailable samples as kNA. Window rows are NCH
-// chunks of 8 samples (the first chunk starts 8 samples left of the
-// superblock, so loads stay 8-sample aligned); a thread's loads all issue
-// before its stores.
+// Stages plane p of superblock (sc, sr) with `top` rows above and below
+// (the 2-sample CDEF border, or 11 with the horizontal loop-filter pass) into
+// the window `wp` as int16, samples outside the mode-info area as kNA.
+// Window rows are NCH chunks of 8 samples (the first chunk starts 8 samples
+// left of the superblock, so loads stay 8-sample aligned); loads issue two
+// at a time before their stores.
 template <int SX>
-__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int sr, int16_t* wp, int tid) {
+__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int sr, int top, int16_t* wp, int tid) {
   constexpr int NCH = ((64 >> SX) + 16) / 8;
   constexpr int kSlots = (kRows * NCH + 255) / 256;
   const int sy = plane_ssy(f, p), sb = f.sb;
-  const int bh = (64 >> sy) + 4;
-  const int px0 = (sc * 64) >> SX, py0 = ((sr * 64) >> sy) - 2;
+  const int bh = (64 >> sy) + 2 * top;
+  const int px0 = (sc * 64) >> SX, py0 = ((sr * 64) >> sy) - top;
   const int xlim = (f.mi_cols * 4) >> SX, ylim = (f.mi_rows * 4) >> sy;
   const DPlane src = f.cur[p];
   // chunk class: 0 none, 1 unavailable, 2 inside (vector load), 3 straddles the edge
@@ -206,64 +211,142 @@ __device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, i
     if (gy < 0 || gy >= ylim || gx0 + 8 <= 0 || gx0 >= xlim) return 1;
     return (gx0 >= 0 && gx0 + 8 <= xlim) ? 2 : 3;
   };
-  uint4 q[kSlots];
 #pragma unroll
-  for (int m = 0; m < kSlots; m++) {
-    const int k = tid + 256 * m, r = k / NCH, ch = k - r * NCH;
-    const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
-    if (kind_of(r, gy, gx0) == 2) {
-      const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
-      if (sb == 2) {
-        q[m] = *reinterpret_cast<const uint4*>(rowp + int64_t(gx0) * 2);
+  for (int m0 = 0; m0 < kSlots; m0 += 2) {
+    uint4 q[2];
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int k = tid + 256 * (m0 + m), r = k / NCH, ch = k - r * NCH;
+      const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
+      if (m0 + m < kSlots && kind_of(r, gy, gx0) == 2) {
+        const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
+        if (sb == 2) {
+          q[m] = *reinterpret_cast<const uint4*>(rowp + int64_t(gx0) * 2);
+        } else {
+          const uint2 h2 = *reinterpret_cast<const uint2*>(rowp + gx0);
+          q[m] = make_uint4(h2.x, h2.y, 0, 0);
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      if (m0 + m >= kSlots) continue;
+      const int k = tid + 256 * (m0 + m), r = k / NCH, ch = k - r * NCH;
+      const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
+      const int kind = kind_of(r, gy, gx0);
+      if (kind == 0) continue;
+      uint32_t o[4];
+      if (kind == 2 && sb == 2) {
+        o[0] = q[m].x;
+        o[1] = q[m].y;
+        o[2] = q[m].z;
+        o[3] = q[m].w;
+      } else if (kind == 2) {
+        // bytes b0..b3 -> int16 pairs
+        o[0] = __byte_perm(q[m].x, 0, 0x4140);
+        o[1] = __byte_perm(q[m].x, 0, 0x4342);
+        o[2] = __byte_perm(q[m].y, 0, 0x4140);
+        o[3] = __byte_perm(q[m].y, 0, 0x4342);
       } else {
-        const uint2 h2 = *reinterpret_cast<const uint2*>(rowp + gx0);
-        q[m] = make_uint4(h2.x, h2.y, 0, 0);
+        int16_t v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          const int gx = gx0 + e;
+          v[e] = (kind == 3 && gx >= 0 && gx < xlim) ? int16_t(ld_sample(src, sb, gx, gy)) : kNA;
+        }
+#pragma unroll
+        for (int e = 0; e < 4; e++) o[e] = uint32_t(uint16_t(v[2 * e])) | (uint32_t(uint16_t(v[2 * e + 1])) << 16);
       }
+      uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
+#pragma unroll
+      for (int e = 0; e < 4; e++) dst[e] = o[e];
     }
-  }
-#pragma unroll
-  for (int m = 0; m < kSlots; m++) {
-    const int k = tid + 256 * m, r = k / NCH, ch = k - r * NCH;
-    const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
-    const int kind = kind_of(r, gy, gx0);
-    if (kind == 0) continue;
-    uint32_t o[4];
-    if (kind == 2 && sb == 2) {
-      o[0] = q[m].x;
-      o[1] = q[m].y;
-      o[2] = q[m].z;
-      o[3] = q[m].w;
-    } else if (kind == 2) {
-      // bytes b0..b3 -> int16 pairs
-      o[0] = __byte_perm(q[m].x, 0, 0x4140);
-      o[1] = __byte_perm(q[m].x, 0, 0x4342);
-      o[2] = __byte_perm(q[m].y, 0, 0x4140);
-      o[3] = __byte_perm(q[m].y, 0, 0x4342);
-    } else {
-      int16_t v[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int gx = gx0 + e;
-        v[e] = (kind == 3 && gx >= 0 && gx < xlim) ? int16_t(ld_sample(src, sb, gx, gy)) : kNA;
-      }
-#pragma unroll
-      for (int e = 0; e < 4; e++) o[e] = uint32_t(uint16_t(v[2 * e])) | (uint32_t(uint16_t(v[2 * e + 1])) << 16);
-    }
-    uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
-#pragma unroll
-    for (int e = 0; e < 4; e++) dst[e] = o[e];
   }
 }
 
+// One horizontal-edge lane on the window (kept out of line: the CDEF
+// kernel's register budget is sized for the CDEF phases).
+__device__ __noinline__ void lfh_lane(int16_t* q0p, int code, bool chroma, int bd, int lvl, int sharp) {
+  lf_filter_smem(q0p, kS, code, chroma, bd, lvl, sharp);
+}
+
+// The horizontal loop-filter edges (postfilter.rs:67-104 pass 1) of plane p
+// that change rows of the staged window: edges at plane rows py0-4 ..
+// py0+bh+4 across the superblock's columns and one 4x4 column on each side.
+// Every edge reads at most 7 rows on either side, which the 11-row halo
+// holds, so the window ends up holding the loop filter's output on the
+// rows CDEF reads. Edges of a pass never touch each other's samples in a
+// conformant frame, so they run in parallel in place.
+__device__ __forceinline__ void lfh_window(const FrameDesc& f, const LfTables& tb, int p, int sc, int sr,
+                                           int16_t* wp, uint16_t* hdec, int tid) {
+  const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+  const int bhs = 64 >> sy;
+  const int px0 = (sc * 64) >> sx, py0 = (sr * 64) >> sy;
+  const int cx0 = (px0 >> 2) - 1, cy0 = (py0 >> 2) - 1;
+  const int ncx = ((64 >> sx) >> 2) + 2;  // 18 or 10
+  const int ncy = (bhs >> 2) + 3;         // 19 or 11
+  const int gw = f.mi_cols >> sx, gh = f.mi_rows >> sy;
+  for (int k = tid; k < ncy * 18; k += 256) {
+    const int cyi = k / 18, cxi = k - cyi * 18;
+    const int cx = cx0 + cxi, cy = cy0 + cyi;
+    int dv = 0, dh = 0;
+    if (cxi < ncx && cx >= 0 && cy >= 0 && cx < gw && cy < gh) lf_decide2(f, tb, p, cx, cy, dv, dh);
+    hdec[k] = uint16_t(dh);
+  }
+  __syncthreads();
+  const int bd = f.bd, sharp = f.sharpness;
+  for (int k = tid; k < ncy * 18 * 4; k += 256) {
+    const int lane = k & 3, cell = k >> 2;
+    const int d = hdec[cell];
+    if (!d) continue;
+    const int cyi = cell / 18, cxi = cell - cyi * 18;
+    const int code = d >> 6, lvl = d & 63;
+    const int e = (cy0 + cyi) * 4;  // plane row of q0
+    if (e < (code == 3 ? 8 : 4)) {  // a conformant map keeps wide edges off the plane start
+      atomicOr(&g_error_flags, ERRF_BAD_MAP);
+      continue;
+    }
+    const int col = (cx0 + cxi) * 4 + lane;
+    lfh_lane(&wp[(e - py0 + kTopLfh) * kS + (col - px0 + kColOff)], code, p != 0, bd, lvl, sharp);
+  }
+  __syncthreads();
+}
+
+// Rows B-2 .. B+1 of the stripe boundary B inside superblock row sr (the
+// loop filter's output, which loop restoration reads across the boundary)
+// from the window to f.prelf[p], over the superblock's columns.
+__device__ __forceinline__ void write_prelf(const FrameDesc& f, int p, int sc, int sr, const int16_t* wp, int tid) {
+  const DPlane dst = f.prelf[p];
+  const int b = sr + 1;  // the boundary inside superblock row sr
+  if (!dst.p || b >= f.stripes) return;
+  const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+  const int px0 = (sc * 64) >> sx, py0 = (sr * 64) >> sy;
+  const int B = (64 * b - 8) >> sy;
+  const int xlim = (f.mi_cols * 4) >> sx, ylim = (f.mi_rows * 4) >> sy;
+  const int w = 64 >> sx;
+  const int j = tid / w, c = tid - j * w;  // 4 rows x w columns
+  if (j >= 4) return;
+  const int y = B - 2 + j, x = px0 + c;
+  if (y >= ylim || x >= xlim) return;
+  st_sample(dst, f.sb, x, (b - 1) * 4 + j, wp[(y - py0 + kTopLfh) * kS + c + kColOff]);
+}
+
 // Item: superblock (x0 = SB column, y0 = SB row). 256 threads.
+// Item kind 1: the frame's horizontal loop-filter edges (planes in
+// f.lfh_mask) are filtered here, on the staged window, before CDEF.
 __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restrict__ frames,
                                                    const Item* __restrict__ items, int n_items) {
-  __shared__ __align__(16) int16_t win[3][kRows * kS];
+  extern __shared__ __align__(16) int16_t cdef_win[];  // [3][kRows * kS]
+  auto win = [&](int p) { return cdef_win + p * kRows * kS; };  // plane p's window
   __shared__ int32_t cost[64][8];
   __shared__ BlkTaps taps[3][64];
   __shared__ uint8_t bstate[64];  // 0 = outside the MI area, 1 = copy, 2 = filter
+  __shared__ LfTables tb;
+  __shared__ uint16_t hdec[19 * 18];  // horizontal-edge decisions of one plane
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
+  load_lf_tables(tb);
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -271,12 +354,22 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     const int np = f.np, sb = f.sb;
     const int cs = f.bd - 8;
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
+    const bool lfh = item.kind != 0;
+    const int top = lfh ? kTopLfh : 2;  // window row of the superblock's first row
+    __syncthreads();  // the previous item is done with the windows
     // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
     for (int p = 0; p < np; p++) {
       if (plane_ssx(f, p))
-        stage_plane<1>(f, p, sc, sr, win[p], tid);
+        stage_plane<1>(f, p, sc, sr, top, win(p), tid);
       else
-        stage_plane<0>(f, p, sc, sr, win[p], tid);
+        stage_plane<0>(f, p, sc, sr, top, win(p), tid);
+    }
+    if (lfh) {
+      __syncthreads();
+      for (int p = 0; p < np; p++)
+        if ((f.lfh_mask >> p) & 1) lfh_window(f, tb, p, sc, sr, win(p), hdec, tid);
+      for (int p = 0; p < np; p++)
+        if ((f.lfh_mask >> p) & 1) write_prelf(f, p, sc, sr, win(p), tid);
     }
     // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
     if (tid < 64) {
@@ -302,7 +395,7 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
       const int b = (warp >> 2) * 32 + lane;
       if (bstate[b] == 2) {
         const int by = b >> 3, bx = b & 7;
-        const int16_t* s = &win[0][(2 + by * 8) * kS + kColOff + bx * 8];
+        const int16_t* s = &win(0)[(top + by * 8) * kS + kColOff + bx * 8];
         int32_t c1, c2;
         switch (pair) {
           case 0: cdef_cost_pair<0>(s, cs, c1, c2); break;
@@ -358,7 +451,7 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
         const int b = by * 8 + bx;
         if (bstate[b] == 0) continue;
         const int lx = bx * w, ly = by * bhp + rr;
-        const int16_t* c = &win[p][(2 + ly) * kS + kColOff + lx];
+        const int16_t* c = &win(p)[(top + ly) * kS + kColOff + lx];
         // results packed two int16 per word as they are produced
         uint32_t o[4] = {0, 0, 0, 0};
         const BlkTaps bt = taps[p][b];
@@ -450,10 +543,13 @@ __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cde
   res[int64_t(e) * 64 + i * a.w + j] = uint16_t(min(max(v, int(mn)), mx));
 }
 
+cudaError_t cdef_init() {
+  return cudaFuncSetAttribute(cdef_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCdefSmem);
+}
+
 void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  cdef_kernel<<<min(n_items, kItemGrid), 256, 0, s>>>(frames, items, n_items);
-  note_launch();
+  launch_pdl(cdef_kernel, min(n_items, kItemGrid), 256, kCdefSmem, s, frames, items, n_items);
 }
 
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s) {

@@ -69,6 +69,17 @@ __device__ __forceinline__ void st_sample(const DPlane& p, int sb, int x, int y,
 __device__ __forceinline__ int plane_ssx(const FrameDesc& f, int plane) { return plane ? f.ssx : 0; }
 __device__ __forceinline__ int plane_ssy(const FrameDesc& f, int plane) { return plane ? f.ssy : 0; }
 
+// Programmatic dependent launch (sm_90 and later). The stage kernels are
+// launched with programmatic stream serialization (launch_pdl): a kernel may
+// be scheduled while its predecessor on the stream drains, so every stage
+// kernel starts with pdl_wait(), which returns once the predecessor has
+// completed and its writes are visible, and then lets its own successor
+// start launching.
+__device__ __forceinline__ void pdl_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Grid-stride loop over the items of a launch.
 #define FOR_EACH_ITEM(it, n)                                   \
   for (int it = blockIdx.x; it < (n); it += gridDim.x)

@@ -5,7 +5,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "av1pf.h"
 #include "plan.h"
@@ -21,6 +25,39 @@ struct HostBuf {
   size_t size = 0;
 };
 
+// The frame shape the autotuner keys its choices by.
+struct ShapeKey {
+  int32_t fw, uw, fh, bd, ssx, ssy, np;
+  bool operator<(const ShapeKey& o) const {
+    return std::tie(fw, uw, fh, bd, ssx, ssy, np) < std::tie(o.fw, o.uw, o.fh, o.bd, o.ssx, o.ssy, o.np);
+  }
+};
+ShapeKey shape_of(const av1pf_frame_info* info);
+
+struct ShapeChoice {
+  int lf_mode;
+  int lr_cols;
+  float ms;  // measured device time per frame
+};
+
+// A captured per-frame launch sequence and the launch structure it was
+// captured for (launch_key).
+struct GraphEntry {
+  std::vector<uint64_t> key;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t kernels = 0;   // kernels per replay
+  uint64_t last_use = 0;
+};
+
+// While alive, kernel launches on this thread are not counted (they are
+// being captured into a graph, and count when the graph runs).
+struct CaptureScope {
+  CaptureScope();
+  ~CaptureScope();
+  uint64_t launches() const;  // launches enqueued in this scope so far
+  uint64_t start;
+};
+
 struct Ctx {
   int device = 0;
   uint64_t cap = 0;   // 0 = no cap
@@ -34,6 +71,11 @@ struct Ctx {
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
   HostBuf meta_host;
   Plan plan;
+  // per-frame graphs, by launch structure (least recently used replaced)
+  static constexpr int kGraphs = 8;
+  GraphEntry graphs[kGraphs];
+  uint64_t graph_clock = 0;
+  cudaStream_t capture = nullptr;
   // profiling: a ring of event sets, one per profiled call
   static constexpr int kProfSlots = 64;
   bool prof = false;
@@ -43,6 +85,13 @@ struct Ctx {
   double prof_ms[5] = {0, 0, 0, 0, 0};
   uint32_t prof_calls = 0;
   void prof_collect(int slot);
+
+  // kernel variants (av1pf_tuning) and the autotuner's record per shape
+  av1pf_tuning tuning{-1, 0};
+  std::map<ShapeKey, ShapeChoice> tuned;
+  mutable std::mutex tune_mu;
+  // Sets j.lf_mode and j.lr_cols from the tuning and the record.
+  void apply_tuning(FrameJob& j) const;
 
   int ensure(DevBuf& b, size_t bytes);
   int ensure_host(HostBuf& b, size_t bytes);

@@ -35,6 +35,12 @@ struct FrameDesc {
   DPlane up[3];     // after superres (LR source)
   DPlane lines[3];  // upscaled pre-CDEF stripe-boundary rows (superres only)
   DPlane ref[3];    // LR output = reference frame
+  // Post-loop-filter rows at the stripe boundaries (rows B-2 .. B+1 of each
+  // boundary B, 4 rows per boundary, boundary b at rows (b-1)*4) for planes
+  // whose horizontal loop-filter edges the CDEF kernel filters (lfh_mask);
+  // loop restoration and superres read the pre-CDEF rows from here then.
+  DPlane prelf[3];
+  int32_t lfh_mask;
   uint8_t* frame_out;
   int64_t out_off[3];
   // maps (av1pf_maps)

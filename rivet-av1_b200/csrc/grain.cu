@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
   __shared__ int16_t gauss[2048];
   const int tid = threadIdx.x;
   for (int k = tid; k < 2048; k += 256) gauss[k] = g_gaussian[k];
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -290,6 +291,7 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
   // block offsets of stripes s and s-1, blocks b0-1 .. b0+16
   __shared__ uint8_t offs_cur[kOutOffs], offs_prev[kOutOffs];
   int loaded = -1;  // frame * 4 + plane whose template is in T
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     OutParams P;
@@ -475,14 +477,12 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
 
 void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  grain_prep_kernel<<<n_items, 256, 0, s>>>(frames, items, n_items);
-  note_launch();
+  launch_pdl(grain_prep_kernel, n_items, 256, 0, s, frames, items, n_items);
 }
 
 void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  output_kernel<<<min(n_items, kItemGrid), 256, 0, s>>>(frames, items, n_items);
-  note_launch();
+  launch_pdl(output_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items);
 }
 
 }  // namespace av1pf

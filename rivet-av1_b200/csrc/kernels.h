@@ -24,15 +24,40 @@ constexpr int kItemGrid = 1 << 20;
 // Counts every kernel launch this library issues (av1pf_launch_count).
 void note_launch(uint64_t n = 1);
 
+// Launches a stage kernel with programmatic stream serialization: it may be
+// scheduled while the previous kernel on `s` drains (the kernel waits for
+// it in pdl_wait() before reading its output). Counts the launch.
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid));
+  cfg.blockDim = dim3(unsigned(block));
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  note_launch();
+}
+
 // Loop filter (lf.cu)
 void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_v, uint64_t* list_h,
                     uint32_t* counts, uint32_t cap, cudaStream_t s);
+// Vertical edges filtered per 64x64 tile in shared memory (copy in -> cur
+// included); horizontal decisions appended to list_h when item kind bit 2.
+void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_h, uint32_t* counts,
+                     uint32_t cap, cudaStream_t s);
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,
                      cudaStream_t s);
 void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s);
 
 // CDEF (cdef.cu)
 void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// Sets cdef_kernel's dynamic shared-memory limit on the current device.
+cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
 
 // Super-resolution (superres.cu)

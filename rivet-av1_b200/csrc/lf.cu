@@ -21,117 +21,9 @@
 // it read, so the results are the same.
 #include "common.cuh"
 #include "kernels.h"
+#include "lf_core.cuh"
 
 namespace av1pf {
-
-// 7.14.4-5 filter_strength (postfilter.rs:207-246): the level of one 4x4
-// from its mode-info words.
-__device__ __forceinline__ int lf_level_raw(const FrameDesc& f, uint2 raw, int plane, int pass) {
-  const int mi_segment = int((raw.x >> 24) & 7u);
-  const int rf = int(int8_t((raw.x >> 16) & 0xffu));
-  const int mode = int((raw.x >> 8) & 0xffu);
-  const int mode_type = (mode >= 14 && mode != 16 && mode != 24) ? 1 : 0;  // NEARESTMV.., !GLOBALMV, !GLOBAL_GLOBALMV
-  const int i = plane == 0 ? pass : plane + 1;
-  const int didx = f.delta_lf_multi ? i : 0;
-  const int delta_lf = int(int8_t((raw.y >> (8 * didx)) & 0xffu));
-  int lvl = clip3(0, 63, delta_lf + f.lf_level[i]);
-  if (f.seg_enabled && f.seg_lf_on[mi_segment][i]) lvl = clip3(0, 63, f.seg_lf_data[mi_segment][i] + lvl);
-  if (f.delta_enabled) {
-    const int n_shift = lvl >> 5;
-    if (rf == 0) {
-      lvl += f.ref_deltas[0] * (1 << n_shift);
-    } else if (rf > 0) {
-      lvl += f.ref_deltas[rf & 7] * (1 << n_shift) + f.mode_deltas[mode_type] * (1 << n_shift);
-    }
-    lvl = clip3(0, 63, lvl);
-  }
-  return lvl;
-}
-
-__device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, int plane, int pass) {
-  return lf_level_raw(f, *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * f.mi_stride + col), plane, pass);
-}
-
-// Small tables the decisions index with per-lane values, copied to shared
-// memory (constant memory serialises divergent indices).
-struct LfTables {
-  uint8_t subsampled[22][2][2];
-  uint8_t bw_log2[23], bh_log2[23];  // log2 of block width/height in samples (22 = invalid)
-  uint8_t txw_log2[19], txh_log2[19];
-  uint8_t txw[19], txh[19];
-};
-
-__device__ __forceinline__ void load_lf_tables(LfTables& t) {
-  for (int k = threadIdx.x; k < 22 * 4; k += blockDim.x) (&t.subsampled[0][0][0])[k] = (&c_subsampled_size[0][0][0])[k];
-  for (int k = threadIdx.x; k < 23; k += blockDim.x) {
-    t.bw_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4w[k]))) : 0;
-    t.bh_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4h[k]))) : 0;
-  }
-  for (int k = threadIdx.x; k < 19; k += blockDim.x) {
-    t.txw[k] = c_tx_w[k];
-    t.txh[k] = c_tx_h[k];
-    t.txw_log2[k] = uint8_t(31 - __clz(c_tx_w[k]));
-    t.txh_log2[k] = uint8_t(31 - __clz(c_tx_h[k]));
-  }
-}
-
-// edge_loop_filter's decisions (postfilter.rs:107-172) for the 4x4 at plane
-// position (cx, cy), both passes: 0 = not filtered, else (size code << 6) |
-// lvl with size code 1 = 4, 2 = 8, 3 = 16. Block and transform sizes are
-// powers of two, so the edge tests are masks. The mode-info word and the
-// three transform sizes (this 4x4, its left and upper neighbours) are all
-// loaded before any is used.
-__device__ __forceinline__ void lf_decide2(const FrameDesc& f, const LfTables& tb, int plane, int cx, int cy,
-                                           int& dv, int& dh) {
-  dv = dh = 0;
-  const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
-  int row = cy << sy, col = cx << sx;
-  const int x = col * 4, y = row * 4;
-  if (x >= f.fw || y >= f.fh) return;
-  const int xp = x >> sx, yp = y >> sy;
-  row |= sy;
-  col |= sx;
-  const int ms = f.mi_stride;
-  const uint8_t* txm = f.tx[plane];
-  const bool has_v = x != 0, has_h = y != 0;
-  const uint2 raw = *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * ms + col);
-  const int tx_sz = txm[int64_t(row >> sy) * ms + (col >> sx)];
-  const int tx_v = has_v ? txm[int64_t(row >> sy) * ms + ((col - (1 << sx)) >> sx)] : 0;
-  const int tx_h = has_h ? txm[int64_t((row - (1 << sy)) >> sy) * ms + (col >> sx)] : 0;
-  const int mi_size = int(raw.x & 0xffu);
-  const bool skip = (raw.x >> 24) & AV1PF_MI_SKIP;
-  const bool is_intra = int(int8_t((raw.x >> 16) & 0xffu)) <= 0;
-  if (mi_size >= 22 || tx_sz >= 19 || tx_v >= 19 || tx_h >= 19) {
-    atomicOr(&g_error_flags, ERRF_BAD_MAP);
-    return;
-  }
-  const int plane_size = tb.subsampled[mi_size][sx][sy];
-  if (plane_size >= 22) {
-    atomicOr(&g_error_flags, ERRF_BAD_MAP);
-    return;
-  }
-  const int cap = plane == 0 ? 16 : 8;
-  if (has_v) {
-    const bool is_block_edge = (xp & ((1 << tb.bw_log2[plane_size]) - 1)) == 0;
-    const bool is_tx_edge = (xp & ((1 << tb.txw_log2[tx_sz]) - 1)) == 0;
-    if (is_tx_edge && (is_block_edge || !skip || is_intra)) {
-      const int size = min(cap, min(int(tb.txw[tx_v]), int(tb.txw[tx_sz])));
-      int lvl = lf_level_raw(f, raw, plane, 0);
-      if (lvl == 0) lvl = lf_level(f, row, col - (1 << sx), plane, 0);
-      if (lvl) dv = ((size >= 16 ? 3 : (size >= 8 ? 2 : 1)) << 6) | lvl;
-    }
-  }
-  if (has_h) {
-    const bool is_block_edge = (yp & ((1 << tb.bh_log2[plane_size]) - 1)) == 0;
-    const bool is_tx_edge = (yp & ((1 << tb.txh_log2[tx_sz]) - 1)) == 0;
-    if (is_tx_edge && (is_block_edge || !skip || is_intra)) {
-      const int size = min(cap, min(int(tb.txh[tx_h]), int(tb.txh[tx_sz])));
-      int lvl = lf_level_raw(f, raw, plane, 1);
-      if (lvl == 0) lvl = lf_level(f, row - (1 << sy), col, plane, 1);
-      if (lvl) dh = ((size >= 16 ? 3 : (size >= 8 ? 2 : 1)) << 6) | lvl;
-    }
-  }
-}
 
 // Edge list entry: frame:16 | plane:2 | code:2 | lvl:6 | cx:14 | cy:14.
 __device__ __forceinline__ uint64_t pack_edge(int frame, int plane, int dec, int cx, int cy) {
@@ -166,6 +58,7 @@ __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __rest
   __shared__ LfTables tb;
   load_lf_tables(tb);
   __syncthreads();
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -225,101 +118,6 @@ __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __rest
   }
 }
 
-// The wide filter of 7.14.6.4 with N taps each side (inner weight-2 taps
-// |j| <= N2), output positions 7-N .. 7+N-1, all indices compile-time.
-template <int N, int N2, int LOG2>
-__device__ __forceinline__ void lf_wide(int32_t v[14]) {
-  int32_t o[14];
-#pragma unroll
-  for (int k = 0; k < 14; k++) o[k] = v[k];
-#pragma unroll
-  for (int i = -N; i < N; i++) {
-    int32_t acc = 0;
-#pragma unroll
-    for (int j = -N; j <= N; j++) {
-      const int pp = (i + j) < -(N + 1) ? -(N + 1) : ((i + j) > N ? N : (i + j));
-      acc += o[7 + pp] * ((j <= N2 && j >= -N2) ? 2 : 1);
-    }
-    v[7 + i] = (acc + (1 << (LOG2 - 1))) >> LOG2;
-  }
-}
-
-// One lane of one edge (the one-sample process of 7.14.6, as lf.rs:218-306
-// states it; lf.rs:58-211 computes the same per lane). v[7] is q0. Returns the
-// first and one-past-last index of the samples the chosen filter changes
-// (lo == hi: none).
-__device__ __forceinline__ void lf_filter_one(int32_t v[14], int filter_size, bool chroma, int bd, int limit,
-                                              int blimit, int thresh, int& lo, int& hi) {
-  lo = hi = 0;
-  const int sh = bd - 8;
-  const int32_t q0 = v[7], q1 = v[8], q2 = v[9], q3 = v[10];
-  const int32_t p0 = v[6], p1 = v[5], p2 = v[4], p3 = v[3];
-  const int32_t thresh_bd = thresh << sh, limit_bd = limit << sh, blimit_bd = blimit << sh;
-  const bool hev = abs(p1 - p0) > thresh_bd || abs(q1 - q0) > thresh_bd;
-  const int filter_len = filter_size == 4 ? 4 : (chroma ? 6 : (filter_size == 8 ? 8 : 16));
-  bool mask = abs(p1 - p0) > limit_bd || abs(q1 - q0) > limit_bd || abs(p0 - q0) * 2 + abs(p1 - q1) / 2 > blimit_bd;
-  if (filter_len >= 6) mask = mask || abs(p2 - p1) > limit_bd || abs(q2 - q1) > limit_bd;
-  if (filter_len >= 8) mask = mask || abs(p3 - p2) > limit_bd || abs(q3 - q2) > limit_bd;
-  if (mask) return;
-  const int32_t t = 1 << sh;
-  bool flat = false;
-  if (filter_size >= 8) {
-    bool m = abs(p1 - p0) > t || abs(q1 - q0) > t || abs(p2 - p0) > t || abs(q2 - q0) > t;
-    if (filter_len >= 8) m = m || abs(p3 - p0) > t || abs(q3 - q0) > t;
-    flat = !m;
-  }
-  bool flat2 = false;
-  if (filter_size >= 16) {
-    const bool m = abs(v[0] - p0) > t || abs(v[13] - q0) > t || abs(v[1] - p0) > t || abs(v[12] - q0) > t ||
-                   abs(v[2] - p0) > t || abs(v[11] - q0) > t;
-    flat2 = !m;
-  }
-  if (filter_size == 4 || !flat) {
-    // narrow filter (7.14.6.3)
-    const int32_t clo = -(1 << (bd - 1)), chi = (1 << (bd - 1)) - 1;
-    const int32_t off = 0x80 << sh;
-    const int32_t ps1 = p1 - off, ps0 = p0 - off, qs0 = q0 - off, qs1 = q1 - off;
-    int32_t fl = hev ? clip3(clo, chi, ps1 - qs1) : 0;
-    fl = clip3(clo, chi, fl + 3 * (qs0 - ps0));
-    const int32_t filter1 = clip3(clo, chi, fl + 4) >> 3;
-    const int32_t filter2 = clip3(clo, chi, fl + 3) >> 3;
-    v[7] = clip3(clo, chi, qs0 - filter1) + off;
-    v[6] = clip3(clo, chi, ps0 + filter2) + off;
-    if (!hev) {
-      const int32_t fr = (filter1 + 1) >> 1;
-      v[8] = clip3(clo, chi, qs1 - fr) + off;
-      v[5] = clip3(clo, chi, ps1 + fr) + off;
-    }
-    lo = 5;
-    hi = 9;
-    return;
-  }
-  // wide filters (7.14.6.4)
-  if (filter_size == 8 || !flat2) {
-    if (chroma) {
-      lf_wide<2, 1, 3>(v);
-      lo = 5;
-      hi = 9;
-    } else {
-      lf_wide<3, 0, 3>(v);
-      lo = 4;
-      hi = 10;
-    }
-  } else {
-    lf_wide<6, 1, 4>(v);
-    lo = 1;
-    hi = 13;
-  }
-}
-
-__device__ __forceinline__ void lf_limits(int lvl, int sharp, int& limit, int& blimit, int& thresh) {
-  // postfilter.rs:248-262
-  const int shift = sharp > 4 ? 2 : (sharp > 0 ? 1 : 0);
-  limit = sharp > 0 ? clip3(1, 9 - sharp, lvl >> shift) : max(lvl >> shift, 1);
-  blimit = 2 * (lvl + 2) + limit;
-  thresh = lvl >> 4;
-}
-
 // Loads samples s[e+k], k in [k0, k0+n), along the filter direction.
 template <int PASS>
 __device__ __forceinline__ void lf_load(const DPlane& p, int sb, int e, int lanepos, int k0, int n, int32_t* out) {
@@ -354,6 +152,7 @@ template <int PASS>
 __global__ void __launch_bounds__(256, 4) lf_edge_kernel(const FrameDesc* __restrict__ frames,
                                                       const uint64_t* __restrict__ list,
                                                       const uint32_t* __restrict__ count_ptr, uint32_t cap) {
+  pdl_wait();  // the edge list and count are complete past this point
   const uint32_t n = min(*count_ptr, cap) * 4u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint64_t e = list[i >> 2];
@@ -405,6 +204,142 @@ __global__ void __launch_bounds__(256, 4) lf_edge_kernel(const FrameDesc* __rest
   }
 }
 
+namespace {
+constexpr int kLfTile = 64;                  // tile side (samples)
+constexpr int kLfHalo = 16;                  // columns staged on each side
+constexpr int kLfTS = 104;                   // tile row stride (u16): >= 64 + 2 * 16, rows 16-byte aligned
+constexpr int kLfCells = kLfTile / 4 + 2;    // 4x4 columns decided: the tile's 16 plus one each side
+}  // namespace
+
+// Loop filter, vertical edges, one 64x64 tile per CTA (kind bit 0: the tile
+// is copied in -> cur; bit 1: it overlaps the mode-info area and its
+// vertical edges are filtered; bit 2: its horizontal edges are appended to
+// list_h for lf_edge_kernel<1>). The tile and 16 columns on each side are
+// staged from the unfiltered input, so edges of neighbouring tiles that
+// reach into this one (at most 6 samples) are filtered here too, from the
+// same input, and no tile reads what another writes. Each tile writes only
+// its own samples of cur. 256 threads.
+__global__ void __launch_bounds__(256, 4) lf_tile_kernel(const FrameDesc* __restrict__ frames,
+                                                      const Item* __restrict__ items, int n_items,
+                                                      uint64_t* __restrict__ list_h, uint32_t* __restrict__ counts,
+                                                      uint32_t cap) {
+  __shared__ LfTables tb;
+  __shared__ __align__(16) uint16_t T[kLfTile * kLfTS];
+  __shared__ uint16_t dec[kLfTile / 4][kLfCells];  // vertical-edge decisions
+  load_lf_tables(tb);
+  const int tid = threadIdx.x;
+  pdl_wait();  // the previous stage's output is complete past this point
+  FOR_EACH_ITEM(it, n_items) {
+    const Item item = items[it];
+    const FrameDesc& f = frames[item.frame];
+    const int plane = item.plane;
+    const DPlane src = f.in[plane], dst = f.cur[plane];
+    const int sb = f.sb;
+    const int x0 = item.x0, y0 = item.y0;
+    const int x1 = min(int(item.x1), src.w), y1 = min(int(item.y1), src.h);
+    const int rows = y1 - y0;
+    const bool filt = (item.kind & 2) != 0;
+    __syncthreads();  // the previous item's tile is written out
+    // --- stage columns [x0 - 16, x0 + 80) of rows [y0, y1): 16-byte chunks ---
+    {
+      const int cw = 16 / sb;                    // samples per chunk
+      const int nch = (kLfTile + 2 * kLfHalo) / cw;  // 6 or 12 chunks per row
+      const int c_lo = filt ? 0 : kLfHalo / cw;  // a copy-only tile needs no halo
+      const int c_hi = filt ? nch : (kLfHalo + kLfTile) / cw;
+      for (int k = tid; k < rows * 12; k += 256) {
+        const int r = k / 12, ch = k - r * 12;
+        if (ch < c_lo || ch >= c_hi) continue;
+        const int gx = x0 - kLfHalo + ch * cw;  // first sample of the chunk
+        const uint8_t* rp = src.p + int64_t(y0 + r) * src.stride * sb;
+        uint16_t* tp = &T[r * kLfTS + ch * cw];
+        if (gx >= 0 && gx + cw <= src.w) {
+          const uint4 q = *reinterpret_cast<const uint4*>(rp + int64_t(gx) * sb);
+          if (sb == 2) {
+            *reinterpret_cast<uint4*>(tp) = q;
+          } else {
+            const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+              reinterpret_cast<uint32_t*>(tp)[2 * e] = __byte_perm(w4[e], 0, 0x4140);
+              reinterpret_cast<uint32_t*>(tp)[2 * e + 1] = __byte_perm(w4[e], 0, 0x4342);
+            }
+          }
+        } else {
+          for (int e = 0; e < cw; e++) {
+            const int x = gx + e;
+            tp[e] = (x >= 0 && x < src.w) ? uint16_t(sb == 1 ? rp[x] : reinterpret_cast<const uint16_t*>(rp)[x]) : 0;
+          }
+        }
+      }
+    }
+    if (filt) {
+      // --- decisions: the tile's 4x4 rows x (its 16 columns + one each side) ---
+      const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
+      const int gw = f.mi_cols >> sx, gh = f.mi_rows >> sy;
+      const int cx0 = (x0 >> 2) - 1, cy0 = y0 >> 2;
+      const int th = (rows + 3) >> 2;
+      const int tw_end = (x1 - x0 + 3) >> 2;  // tile columns (cells 1 .. tw_end)
+      for (int k = tid; k < (kLfTile / 4) * 32; k += 256) {
+        const int cyi = k >> 5, cxi = k & 31;
+        const int cx = cx0 + cxi, cy = cy0 + cyi;
+        const bool in = cxi < kLfCells && cyi < th && cx >= 0 && cx < gw && cy < gh;
+        int dv = 0, dh = 0;
+        if (in) lf_decide2(f, tb, plane, cx, cy, dv, dh);
+        if (cxi < kLfCells && cyi < kLfTile / 4) dec[cyi][cxi] = uint16_t(dv);
+        if (item.kind & 4) {
+          const bool own = in && cxi >= 1 && cxi <= tw_end && dh != 0;
+          append_edge(list_h, &counts[1], cap, own, pack_edge(item.frame, plane, dh, cx, cy));
+        }
+      }
+      __syncthreads();
+      // --- vertical edges in shared memory: (cell, row lane) per thread ---
+      const int bd = f.bd, sharp = f.sharpness;
+      for (int k = tid; k < th * kLfCells * 4; k += 256) {
+        const int lane = k & 3, cell = k >> 2;
+        const int cyi = cell / kLfCells, cxi = cell - cyi * kLfCells;
+        const int d = dec[cyi][cxi];
+        if (!d) continue;
+        const int code = d >> 6, lvl = d & 63;
+        const int r = cyi * 4 + lane;
+        if (r >= rows) continue;
+        const int e = (cx0 + cxi) * 4;  // plane column of q0
+        if (e < (code == 3 ? 8 : 4)) {  // a conformant map keeps wide edges off the plane start
+          atomicOr(&g_error_flags, ERRF_BAD_MAP);
+          continue;
+        }
+        lf_filter_smem(&T[r * kLfTS + (e - x0 + kLfHalo)], 1, code, plane != 0, bd, lvl, sharp);
+      }
+    }
+    __syncthreads();
+    // --- write the tile's own samples [x0, x1) x [y0, y1) ---
+    {
+      const int w = x1 - x0;
+      const int nv = w >> 3;  // 8-sample groups
+      for (int k = tid; k < rows * 8; k += 256) {
+        const int r = k >> 3, g = k & 7;
+        uint8_t* rp = dst.p + int64_t(y0 + r) * dst.stride * sb;
+        const uint16_t* tp = &T[r * kLfTS + kLfHalo + g * 8];
+        if (g < nv) {
+          const uint4 q = *reinterpret_cast<const uint4*>(tp);
+          if (sb == 2) {
+            *reinterpret_cast<uint4*>(rp + int64_t(x0 + g * 8) * 2) = q;
+          } else {
+            *reinterpret_cast<uint2*>(rp + x0 + g * 8) =
+                make_uint2(__byte_perm(q.x, q.y, 0x6420), __byte_perm(q.z, q.w, 0x6420));
+          }
+        } else if (g == nv) {
+          for (int e = 0; e < w - nv * 8; e++) {
+            if (sb == 2)
+              reinterpret_cast<uint16_t*>(rp)[x0 + g * 8 + e] = tp[e];
+            else
+              rp[x0 + g * 8 + e] = uint8_t(tp[e]);
+          }
+        }
+      }
+    }
+  }
+}
+
 // dsp::lf::filter (lf.rs:25) on independent edges: one thread per lane.
 __global__ void dsp_lf_kernel(int32_t* __restrict__ edges, const av1pf_lf_edge_params* __restrict__ prm, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -428,8 +363,13 @@ void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uin
                     uint32_t* counts, uint32_t cap, cudaStream_t s) {
   if (n_items <= 0) return;
   const int grid = min(n_items, kItemGrid);
-  lf_prep_kernel<<<grid, 256, 0, s>>>(frames, items, n_items, list_v, list_h, counts, cap);
-  note_launch();
+  launch_pdl(lf_prep_kernel, grid, 256, 0, s, frames, items, n_items, list_v, list_h, counts, cap);
+}
+
+void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_h, uint32_t* counts,
+                     uint32_t cap, cudaStream_t s) {
+  if (n_items <= 0) return;
+  launch_pdl(lf_tile_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items, list_h, counts, cap);
 }
 
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,
@@ -437,10 +377,9 @@ void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, co
   // The edge count is only known on the device: a fixed grid strides over it.
   const int grid = kMaxGrid;
   if (pass == 0)
-    lf_edge_kernel<0><<<grid, 256, 0, s>>>(frames, list, count, cap);
+    launch_pdl(lf_edge_kernel<0>, grid, 256, 0, s, frames, list, count, cap);
   else
-    lf_edge_kernel<1><<<grid, 256, 0, s>>>(frames, list, count, cap);
-  note_launch();
+    launch_pdl(lf_edge_kernel<1>, grid, 256, 0, s, frames, list, count, cap);
 }
 
 void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s) {

@@ -50,11 +50,12 @@ struct LrSrc {
   const uint8_t* cur;
   const uint8_t* lines;
   int64_t up_pitch, cur_pitch, lines_pitch;  // bytes
-  bool sr;
+  bool sr;  // the pre-CDEF rows come from `lines` (4 per stripe boundary), not `cur`
 };
 
 // The row LrCtx::sample reads for window row y of stripe `s`. With superres
-// the pre-CDEF rows come from the line buffer, 4 rows per stripe boundary:
+// (or with the loop filter's horizontal pass run inside the CDEF kernel) the
+// pre-CDEF rows come from a line buffer, 4 rows per stripe boundary:
 // boundary b (the first row B of stripe b) holds rows B-2 .. B+1 at line
 // rows (b-1)*4 ...
 __device__ __forceinline__ const uint8_t* lr_row(const LrSrc& src, const LrGeom& g, int s, int y) {
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
   for (int z = tid; z < 256; z += kThreads) a2tab[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
   __syncthreads();
 
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -244,11 +246,14 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       LrSrc src;
       src.up = f.up[p].p;
       src.cur = f.cur[p].p;
-      src.lines = f.lines[p].p;
+      // superres: upscaled boundary rows; fused horizontal LF pass: the
+      // loop filter's boundary rows; else the loop-filtered plane itself
+      const DPlane lines = f.sr_on ? f.lines[p] : f.prelf[p];
+      src.lines = lines.p;
       src.up_pitch = f.up[p].stride * sb;
       src.cur_pitch = f.cur[p].stride * sb;
-      src.lines_pitch = f.lines[p].stride * sb;
-      src.sr = f.sr_on != 0;
+      src.lines_pitch = lines.stride * sb;
+      src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
       const int x = max(min(x0 + c - 3, geo.pex), 0);
       constexpr int kWinRows = (kMaxH + 6 + kGroups - 1) / kGroups;  // 18 window rows per thread
       constexpr int kBatch = 6;
@@ -338,8 +343,7 @@ void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStre
   if (n_items <= 0) return;
   // one CTA per rectangle: the block scheduler hands rectangles of uneven
   // cost (copy, Wiener, self-guided) to SMs as they free up
-  lr_kernel<<<min(n_items, kItemGrid), kThreads, kSmemBytes, s>>>(frames, items, n_items);
-  note_launch();
+  launch_pdl(lr_kernel, min(n_items, kItemGrid), kThreads, size_t(kSmemBytes), s, frames, items, n_items);
 }
 
 }  // namespace av1pf

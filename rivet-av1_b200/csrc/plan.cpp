@@ -234,6 +234,10 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     const bool chain = (j.stages & ST_CHAIN) == ST_CHAIN;
     // --- loop filter: postfilter.rs:67-70, decoder/mod.rs:748 ---
     const bool lf_frame = (j.stages & ST_LF) && (p->loop_filter_level[0] || p->loop_filter_level[1]);
+    // horizontal edges inside the CDEF kernel: needs the chain's copy of the
+    // input (cur is not the caller's) and a CDEF pass to carry them
+    const bool tiles = !j.in_place_lf && j.lf_mode >= 1;
+    const bool fuse_h = lf_frame && chain && tiles && j.lf_mode == 2 && (j.stages & ST_CDEF) && p->cdef_enabled;
     for (int k = 0; k < np; k++) {
       d.in[k] = from_abi(j.in[k]);
       const bool lf_plane = lf_frame && (k == 0 || p->loop_filter_level[1 + k] != 0);
@@ -247,7 +251,8 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       if (j.in_place_lf) {
         d.cur[k] = d.in[k];
         add_tiles(plan.lf_items, fi, k, 2, gw * 4, gh * 4, kTile, kTile);
-      } else {
+      } else if (!tiles) {
+        // copy in -> cur and decide every 4x4 edge into the two edge lists
         d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
         const int W = d.in[k].w, H = d.in[k].h;
         for (int y = 0; y < H; y += kTile)
@@ -262,7 +267,32 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
             it.y1 = uint16_t(std::min(y + kTile, H));
             plan.lf_items.push_back(it);
           }
+        plan.any_hlist = true;
+      } else {
+        // copy in -> cur with the vertical edges filtered per tile; the
+        // horizontal edges go to the edge list
+        d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
+        const int W = d.in[k].w, H = d.in[k].h;
+        for (int y = 0; y < H; y += kTile)
+          for (int x = 0; x < W; x += kTile) {
+            Item it{};
+            it.frame = uint16_t(fi);
+            it.plane = uint8_t(k);
+            it.kind = uint8_t(1 | ((x < gw * 4 && y < gh * 4) ? (fuse_h ? 2 : 2 | 4) : 0));
+            it.x0 = uint16_t(x);
+            it.y0 = uint16_t(y);
+            it.x1 = uint16_t(std::min(x + kTile, W));
+            it.y1 = uint16_t(std::min(y + kTile, H));
+            plan.lft_items.push_back(it);
+          }
+        if (fuse_h) {
+          d.lfh_mask |= 1 << k;
+          if (d.stripes > 1) d.prelf[k] = bump.plane(d.in[k].w, (d.stripes - 1) * 4, sb);
+        } else {
+          plan.any_hlist = true;
+        }
       }
+      if (j.in_place_lf) plan.any_hlist = true;
       cap += uint32_t(gw) * uint32_t(gh);
     }
     // --- CDEF: postfilter.rs:273-301 ---
@@ -285,6 +315,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         for (int c = 0; c < sbc; c++) {
           Item it{};
           it.frame = uint16_t(fi);
+          it.kind = uint8_t(d.lfh_mask ? 1 : 0);
           it.x0 = uint16_t(c);
           it.y0 = uint16_t(r);
           plan.cdef_items.push_back(it);
@@ -346,6 +377,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         const bool has_lr = p->uses_lr && p->frame_restoration_type[k] != 0;
         const int us = has_lr ? p->loop_restoration_size[k] : 1 << 30;
         const int ucols = has_lr ? p->lr_unit_cols[k] : 1;
+        const int rw = j.lr_cols == 32 ? 32 : kTile;  // rectangle width (the kernel takes <= 64)
         for (int s = 0; s < d.stripes; s++) {
           const int sy = k ? d.ssy : 0;
           const int ss = (-8 + s * 64) >> sy;
@@ -356,12 +388,12 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
             const int x0 = uc * std::min(us, 1 << 20);
             const int x1 = uc + 1 == ucols ? pex : std::min((uc + 1) * us - 1, pex);
             if (x0 > pex) continue;
-            for (int cx = x0; cx <= x1; cx += kTile) {
+            for (int cx = x0; cx <= x1; cx += rw) {
               Item it{};
               it.frame = uint16_t(fi);
               it.plane = uint8_t(k);
               it.x0 = uint16_t(cx);
-              it.x1 = uint16_t(std::min(cx + kTile, x1 + 1));
+              it.x1 = uint16_t(std::min(cx + rw, x1 + 1));
               it.a = uint16_t(s);
               it.b = uint16_t(uc);
               plan.lr_items.push_back(it);
@@ -411,6 +443,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   };
   plan.off_frames = place(plan.frames.size() * sizeof(FrameDesc));
   plan.off_lf = place(plan.lf_items.size() * sizeof(Item));
+  plan.off_lft = place(plan.lft_items.size() * sizeof(Item));
   plan.off_cdef = place(plan.cdef_items.size() * sizeof(Item));
   plan.off_sr = place(plan.sr_items.size() * sizeof(Item));
   plan.off_lr = place(plan.lr_items.size() * sizeof(Item));
@@ -432,12 +465,25 @@ void pack_meta(const Plan& plan, uint8_t* host) {
   };
   put(plan.off_frames, plan.frames.data(), plan.frames.size() * sizeof(FrameDesc));
   put(plan.off_lf, plan.lf_items.data(), plan.lf_items.size() * sizeof(Item));
+  put(plan.off_lft, plan.lft_items.data(), plan.lft_items.size() * sizeof(Item));
   put(plan.off_cdef, plan.cdef_items.data(), plan.cdef_items.size() * sizeof(Item));
   put(plan.off_sr, plan.sr_items.data(), plan.sr_items.size() * sizeof(Item));
   put(plan.off_lr, plan.lr_items.data(), plan.lr_items.size() * sizeof(Item));
   put(plan.off_grain, plan.grain_items.data(), plan.grain_items.size() * sizeof(Item));
   put(plan.off_out, plan.out_items.data(), plan.out_items.size() * sizeof(Item));
   put(plan.off_copy, plan.copy_items.data(), plan.copy_items.size() * sizeof(Item));
+}
+
+void launch_key(const Plan& plan, const void* meta, std::vector<uint64_t>& key) {
+  key.assign({reinterpret_cast<uint64_t>(meta),
+              plan.frames.size(), plan.lf_items.size(), plan.lft_items.size(), plan.cdef_items.size(),
+              plan.sr_items.size(), plan.lr_items.size(), plan.grain_items.size(), plan.out_items.size(),
+              plan.copy_items.size(), plan.edge_cap,
+              plan.off_frames, plan.off_lf, plan.off_lft, plan.off_cdef, plan.off_sr, plan.off_lr, plan.off_grain,
+              plan.off_out, plan.off_copy, plan.off_edges_v, plan.off_edges_h, plan.off_counts,
+              uint64_t(plan.any_lf) | uint64_t(plan.any_cdef) << 1 | uint64_t(plan.any_sr) << 2 |
+                  uint64_t(plan.any_lr) << 3 | uint64_t(plan.any_grain) << 4 | uint64_t(plan.any_out) << 5 |
+                  uint64_t(plan.any_hlist) << 6});
 }
 
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
@@ -462,11 +508,18 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     cudaMemsetAsync(counts, 0, 16, s);
     launch_lf_prep(frames, items(plan.off_copy), int(plan.copy_items.size()), ev, eh, counts, 0, s);
   }
-  if (plan.any_lf) {
+  if (plan.any_lf && !plan.lf_items.empty()) {
+    // in place: decisions into both edge lists, then one pass per direction
     cudaMemsetAsync(counts, 0, 16, s);
     launch_lf_prep(frames, items(plan.off_lf), int(plan.lf_items.size()), ev, eh, counts, plan.edge_cap, s);
     launch_lf_edges(0, frames, ev, counts + 0, plan.edge_cap, s);
     launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
+  }
+  if (plan.any_lf && !plan.lft_items.empty()) {
+    // copy + vertical edges per tile, then the horizontal edge list
+    cudaMemsetAsync(counts, 0, 16, s);
+    launch_lf_tiles(frames, items(plan.off_lft), int(plan.lft_items.size()), eh, counts, plan.edge_cap, s);
+    if (plan.any_hlist) launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
   mark(1);
   if (plan.any_cdef) launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), s);

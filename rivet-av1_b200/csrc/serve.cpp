@@ -272,6 +272,7 @@ int Server::start_batch(InFlight& b, std::vector<Request*>& reqs) {
                                  plane_h(&st->info, p)};
     jobs.push_back(FrameJob{&st->info, &r->params, &r->dmaps, r->din, nullptr, r->dref, r->dframe_out, ST_CHAIN,
                             false});
+    ctx->apply_tuning(jobs.back());
   }
   std::string why;
   int rc = build_plan(jobs.data(), int(jobs.size()), nullptr, b.plan, &why);

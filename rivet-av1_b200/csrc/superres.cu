@@ -26,9 +26,11 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
   uint16_t* row = reinterpret_cast<uint16_t*>(sr_smem + 64 * 8 * 2);  // staged source row
   for (int k = threadIdx.x; k < 64 * 8; k += blockDim.x) filt[k] = g_upscale_filter[k >> 3][k & 7];
   __syncthreads();
+  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     int p, sy, sb, maxv, step, init, max_x, w, plane_h, kind;
+    bool prelf;
     DPlane src, dst;
     {
       const FrameDesc& f = frames[item.frame];
@@ -42,7 +44,10 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
       max_x = f.sr_maxx[p];
       w = f.sr_w[p];
       plane_h = (f.fh + sy) >> sy;
-      src = kind == 0 ? f.cdef[p] : f.cur[p];
+      // kind 1 reads the loop filter's boundary rows: from the plane, or
+      // from f.prelf when the CDEF kernel ran the horizontal LF pass
+      prelf = kind == 1 && f.prelf[p].p != nullptr;
+      src = kind == 0 ? f.cdef[p] : (prelf ? f.prelf[p] : f.cur[p]);
       dst = kind == 0 ? f.up[p] : f.lines[p];
     }
     const int n_src = max_x + 1;
@@ -55,7 +60,7 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
       }
       const bool live = src_row >= 0 && src_row < plane_h;  // uniform across the CTA
       if (live) {
-        const uint8_t* sp = src.p + int64_t(src_row) * src.stride * sb;
+        const uint8_t* sp = src.p + int64_t(prelf ? r : src_row) * src.stride * sb;
         if (sb == 2) {
           const int nv = n_src >> 3;
           for (int k = threadIdx.x; k < nv; k += blockDim.x)
@@ -102,8 +107,8 @@ cudaError_t superres_init() {
 
 void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  superres_kernel<<<min(n_items, kItemGrid), 256, 64 * 8 * 2 + kMaxRow * 2, s>>>(frames, items, n_items);
-  note_launch();
+  launch_pdl(superres_kernel, min(n_items, kItemGrid), 256, size_t(64 * 8 * 2 + kMaxRow * 2), s, frames, items,
+             n_items);
 }
 
 }  // namespace av1pf
