@@ -128,34 +128,43 @@ __device__ __forceinline__ void sgr_ab(const uint16_t* win, int32_t* A, int32_t*
       s2 += v * v;
     }
   };
+  // ring of the horizontal sums of the 2R+1 rows in the box: the row that
+  // enters at step i goes to slot (i - i0 + 2R) mod N, the row that leaves
+  // is in slot (i - i0) mod N; unrolling by N makes the slots constants
+  constexpr int N = 2 * R + 1;
+  int r1[N], r2[N];
   int bsum = 0, bsq = 0;
 #pragma unroll
-  for (int dy = -R; dy < R; dy++) {
-    int s1, s2;
-    hs(i0 + 2 + dy, s1, s2);
-    bsum += s1;
-    bsq += s2;
+  for (int m = 0; m < 2 * R; m++) {
+    hs(i0 + 2 - R + m, r1[m], r2[m]);
+    bsum += r1[m];
+    bsq += r2[m];
   }
-  for (int i = i0; i < i1; i++) {
-    int s1, s2;
-    hs(i + 2 + R, s1, s2);
-    bsum += s1;
-    bsq += s2;
-    // the first filter weighs only the odd rows' A and B (postfilter.rs:937)
-    if (PASS == 1 || ((y0 + i - 1) & 1) != 0) {
-      const int a = round2(bsq, 2 * (bd - 8));
-      const int d = round2(bsum, bd - 8);
-      const int pp = max(a * n - d * d, 0);
-      const uint64_t z = (uint64_t(uint32_t(pp)) * sc + (1u << 19)) >> 20;
-      const int a2 = a2tab[z > 255 ? 255 : int(z)];
-      const uint32_t k = uint32_t(256 - a2) * uint32_t(one_over_n);
-      const uint64_t b2 = uint64_t(k) * uint32_t(bsum);
-      A[i * kAS + c] = a2;
-      B[i * kAS + c] = int32_t((b2 + (1u << 11)) >> 12);
+  for (int ib = i0; ib < i1; ib += N) {
+#pragma unroll
+    for (int u = 0; u < N; u++) {
+      const int i = ib + u;
+      if (i < i1) {
+        const int sn = (u + 2 * R) % N;
+        hs(i + 2 + R, r1[sn], r2[sn]);
+        bsum += r1[sn];
+        bsq += r2[sn];
+        // the first filter weighs only the odd rows' A and B (postfilter.rs:937)
+        if (PASS == 1 || ((y0 + i - 1) & 1) != 0) {
+          const int a = round2(bsq, 2 * (bd - 8));
+          const int d = round2(bsum, bd - 8);
+          const int pp = max(a * n - d * d, 0);
+          const uint64_t z = (uint64_t(uint32_t(pp)) * sc + (1u << 19)) >> 20;
+          const int a2 = a2tab[z > 255 ? 255 : int(z)];
+          const uint32_t k = uint32_t(256 - a2) * uint32_t(one_over_n);
+          const uint64_t b2 = uint64_t(k) * uint32_t(bsum);
+          A[i * kAS + c] = a2;
+          B[i * kAS + c] = int32_t((b2 + (1u << 11)) >> 12);
+        }
+        bsum -= r1[u];
+        bsq -= r2[u];
+      }
     }
-    hs(i + 2 - R, s1, s2);
-    bsum -= s1;
-    bsq -= s2;
   }
 }
 
@@ -281,21 +290,40 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       const int h0 = unit.wiener[1][0], h1 = unit.wiener[1][1], h2 = unit.wiener[1][2];
       const int v0 = unit.wiener[0][0], v1 = unit.wiener[0][1], v2 = unit.wiener[0][2];
       const int h3 = 128 - 2 * (h0 + h1 + h2), v3 = 128 - 2 * (v0 + v1 + v2);
-      if (c < w) {
-        for (int r = g; r < wh; r += kGroups) {
-          const uint16_t* sp = &win[r * kWS + c];
-          const int acc = h0 * (int(sp[0]) + int(sp[6])) + h1 * (int(sp[1]) + int(sp[5])) +
-                          h2 * (int(sp[2]) + int(sp[4])) + h3 * int(sp[3]);
-          inter[r * kWS + c] = int16_t(clip3(-offset, limit - offset, round2(acc, round0)));
-        }
+      // horizontal pass: two adjacent outputs per task from 8 window samples
+      // (four aligned 32-bit loads), packed into one 32-bit store
+      for (int k = tid; k < wh * 32; k += kThreads) {
+        const int r = k >> 5, c2 = (k & 31) * 2;
+        if (c2 >= w) continue;
+        const uint32_t* sp = reinterpret_cast<const uint32_t*>(&win[r * kWS + c2]);
+        const uint32_t q0 = sp[0], q1 = sp[1], q2 = sp[2], q3 = sp[3];
+        const int s0 = int(q0 & 0xffffu), s1 = int(q0 >> 16), s2 = int(q1 & 0xffffu), s3 = int(q1 >> 16);
+        const int s4 = int(q2 & 0xffffu), s5 = int(q2 >> 16), s6 = int(q3 & 0xffffu), s7 = int(q3 >> 16);
+        const int a0 = h0 * (s0 + s6) + h1 * (s1 + s5) + h2 * (s2 + s4) + h3 * s3;
+        const int a1 = h0 * (s1 + s7) + h1 * (s2 + s6) + h2 * (s3 + s5) + h3 * s4;
+        const int o0 = clip3(-offset, limit - offset, round2(a0, round0));
+        const int o1 = clip3(-offset, limit - offset, round2(a1, round0));
+        *reinterpret_cast<uint32_t*>(&inter[r * kWS + c2]) = uint32_t(uint16_t(o0)) | (uint32_t(uint16_t(o1)) << 16);
       }
       __syncthreads();
+      // vertical pass: each row group slides a 7-row window down its column
       if (c < w) {
-        for (int i = g; i < h; i += kGroups) {
-          const int16_t* ip = &inter[i * kWS + c];
-          const int acc = v0 * (int(ip[0]) + int(ip[6 * kWS])) + v1 * (int(ip[kWS]) + int(ip[5 * kWS])) +
-                          v2 * (int(ip[2 * kWS]) + int(ip[4 * kWS])) + v3 * int(ip[3 * kWS]);
-          st_sample(dst, sb, x0 + c, geo.y0 + i, clip3(0, maxv, round2(acc, round1)));
+        const int per = (h + kGroups - 1) / kGroups;
+        const int i0 = g * per, i1 = min(h, i0 + per);
+        if (i0 < i1) {
+          const int16_t* ip = &inter[i0 * kWS + c];
+          int t0 = ip[0], t1 = ip[kWS], t2 = ip[2 * kWS], t3 = ip[3 * kWS], t4 = ip[4 * kWS], t5 = ip[5 * kWS];
+          for (int i = i0; i < i1; i++) {
+            const int t6 = inter[(i + 6) * kWS + c];
+            const int acc = v0 * (t0 + t6) + v1 * (t1 + t5) + v2 * (t2 + t4) + v3 * t3;
+            st_sample(dst, sb, x0 + c, geo.y0 + i, clip3(0, maxv, round2(acc, round1)));
+            t0 = t1;
+            t1 = t2;
+            t2 = t3;
+            t3 = t4;
+            t4 = t5;
+            t5 = t6;
+          }
         }
       }
     } else {
