@@ -53,6 +53,11 @@ HEADLINE = dict(width=1920, height=1080, bit_depth=10)
 L2_BYTES = 126 * 2**20
 HEADLINE_WORKLOAD = "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+CDEF+LR+pack)"
 REF_ARM_BUDGET_S = 120.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each stage's kernels on the
+# headline workload, from one `ncu --set full` capture (cold cache; the outputs stay in the 126 MB
+# L2, so the writes read 0). The loop filter's is its three kernels together.
+NCU_TRAFFIC_HEADLINE = {"loop_filter": 8314624 + 6636032 + 4793600, "cdef": 7042048, "loop_restoration": 6813952,
+                        "output": 6269184}
 
 
 def peaks():
@@ -297,7 +302,7 @@ def main_gpu(args):
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "algorithmic_bytes": int(algo[dom]), "traffic": None,
+                     "algorithmic_bytes": int(algo[dom]), "traffic": NCU_TRAFFIC_HEADLINE.get(dom),
                      "chain_frac": round(chain_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak, 4)},
         "clocks": clocks,
     }
@@ -415,6 +420,22 @@ def bench_mix(args, ctx, rank, barrier, max_over_ranks):
         jobs[i].inp = C.cast(d.inp.c, C.POINTER(A.Plane))
         jobs[i].ref_out = C.cast(r.c, C.POINTER(A.Plane))
         jobs[i].frame_out = fb.data_ptr()
+    # the autotuner picks the loop-filter mode and LR rectangle width per shape;
+    # the per-frame calls and the batch both run on its choices
+    n_shapes = C.c_int32()
+    A.check(L.av1pf_autotune(ctx.p, jobs, len(dfs), 5, C.byref(n_shapes)), "autotune")
+    tuned, seen = [], set()
+    for d in dfs:
+        i = d.info
+        key = (i.upscaled_width, i.frame_height, i.bit_depth, i.subsampling_x, i.subsampling_y)
+        if key in seen:
+            continue
+        seen.add(key)
+        t, ms = A.Tuning(), C.c_float()
+        A.check(L.av1pf_tuned_choice(ctx.p, C.byref(i), C.byref(t), C.byref(ms)), "tuned_choice")
+        sub = "4:4:4" if not i.subsampling_x else ("4:2:2" if not i.subsampling_y else "4:2:0")
+        tuned.append({"shape": f"{i.upscaled_width}x{i.frame_height} {i.bit_depth}-bit {sub}",
+                      "lf_mode": t.lf_mode, "lr_rect_cols": t.lr_rect_cols, "frame_ms": round(ms.value, 4)})
     b = C.c_void_p()
     A.check(L.av1pf_batch_create(ctx.p, jobs, len(dfs), 0, C.byref(b)), "batch_create")
 
@@ -439,7 +460,7 @@ def bench_mix(args, ctx, rank, barrier, max_over_ranks):
     return {"frames": len(dfs), "mpx_per_batch": round(px / 1e6, 3),
             "per_frame_mpx_s": round(px / (t_pf / 1e3) / 1e6, 1), "batched_mpx_s": round(px / (t_b / 1e3) / 1e6, 1),
             "speedup": round(t_pf / t_b, 3), "per_frame_ms": round(t_pf, 3), "batched_ms": round(t_b, 3),
-            "bit_exact_batched_vs_per_frame": bool(exact)}
+            "bit_exact_batched_vs_per_frame": bool(exact), "autotune": tuned}
 
 
 def bench_4k(args, ctx, barrier, max_over_ranks):
