@@ -436,8 +436,9 @@ def bench_mix(args, ctx, rank, barrier, max_over_ranks):
         sub = "4:4:4" if not i.subsampling_x else ("4:2:2" if not i.subsampling_y else "4:2:0")
         tuned.append({"shape": f"{i.upscaled_width}x{i.frame_height} {i.bit_depth}-bit {sub}",
                       "lf_mode": t.lf_mode, "lr_rect_cols": t.lr_rect_cols, "frame_ms": round(ms.value, 4)})
+    # the batch is tuned as a whole: each variant on every frame, and the per-shape choices
     b = C.c_void_p()
-    A.check(L.av1pf_batch_create(ctx.p, jobs, len(dfs), 0, C.byref(b)), "batch_create")
+    A.check(L.av1pf_batch_create(ctx.p, jobs, len(dfs), A.BATCH_AUTOTUNE, C.byref(b)), "batch_create")
 
     def timed(fn, reps):
         for _ in range(max(1, args.warmup)):

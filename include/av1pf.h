@@ -319,7 +319,9 @@ typedef struct av1pf_batch av1pf_batch;
  * `flags`: AV1PF_BATCH_NO_GRAPH launches the stages directly. */
 #define AV1PF_BATCH_NO_GRAPH 1u
 /* AV1PF_BATCH_AUTOTUNE: first run av1pf_autotune on the jobs' shapes that
- * the context has not measured (the jobs' outputs are overwritten). */
+ * the context has not measured, then time each kernel variant applied to the
+ * whole batch (and the per-shape choices) on the batch itself and plan the
+ * fastest. The jobs' outputs are overwritten while timing. */
 #define AV1PF_BATCH_AUTOTUNE 2u
 int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs,
                        uint32_t flags, av1pf_batch** out);

@@ -102,15 +102,17 @@ int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, uint32
     const int rc = validate_job(jobs[i], i);
     if (rc != AV1PF_OK) return rc;
   }
-  if (flags & AV1PF_BATCH_AUTOTUNE) {
-    const int rc = tune_shapes(ctx, jobs, n_jobs, 10, true, nullptr);
-    if (rc != AV1PF_OK) return rc;
-  }
   std::vector<FrameJob> fj(static_cast<size_t>(n_jobs));
-  for (int i = 0; i < n_jobs; i++) {
-    const av1pf_job& j = jobs[i];
-    fj[size_t(i)] = FrameJob{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
-    ctx->apply_tuning(fj[size_t(i)]);
+  if (flags & AV1PF_BATCH_AUTOTUNE) {
+    int rc = tune_shapes(ctx, jobs, n_jobs, 10, true, nullptr);
+    if (rc == AV1PF_OK) rc = tune_batch(ctx, jobs, n_jobs, 5, fj);
+    if (rc != AV1PF_OK) return rc;
+  } else {
+    for (int i = 0; i < n_jobs; i++) {
+      const av1pf_job& j = jobs[i];
+      fj[size_t(i)] = FrameJob{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
+      ctx->apply_tuning(fj[size_t(i)]);
+    }
   }
   return create_batch(ctx, fj.data(), n_jobs, flags, out);
 }

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 
 #include "av1pf.h"
 #include "ctx.h"
@@ -20,5 +21,9 @@ int create_batch(Ctx* ctx, const FrameJob* fj, int n_jobs, uint32_t flags, av1pf
 // av1pf_autotune over `jobs` (validated by the caller); only_new skips the
 // shapes the context has recorded.
 int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only_new, int* n_shapes);
+
+// Times every variant applied to the whole batch, and the per-shape choices,
+// and returns the fastest set of frame jobs in `best`.
+int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vector<FrameJob>& best);
 
 }  // namespace av1pf

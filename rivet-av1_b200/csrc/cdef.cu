@@ -346,7 +346,6 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   load_lf_tables(tb);
-  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -356,7 +355,26 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
     const bool lfh = item.kind != 0;
     const int top = lfh ? kTopLfh : 2;  // window row of the superblock's first row
-    __syncthreads();  // the previous item is done with the windows
+    // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
+    // (the maps are inputs of the chain: read before waiting for the loop filter)
+    uint8_t st = 0;
+    if (tid < 64) {
+      const int by = tid >> 3, bx = tid & 7;
+      const int r = sr * 16 + 2 * by, c = sc * 16 + 2 * bx;
+      if (r < f.mi_rows && c < f.mi_cols) {
+        st = 1;
+        if (idx >= 0) {
+          const av1pf_mi* m = f.mi + int64_t(r) * f.mi_stride + c;
+          const int ms = f.mi_stride;
+          const bool skip = (m[0].skip_segment & AV1PF_MI_SKIP) && (m[ms].skip_segment & AV1PF_MI_SKIP) &&
+                            (m[1].skip_segment & AV1PF_MI_SKIP) && (m[ms + 1].skip_segment & AV1PF_MI_SKIP);
+          if (!skip) st = 2;
+        }
+      }
+    }
+    pdl_wait();       // the loop filter's output is complete past this point
+    __syncthreads();  // the previous item is done with the windows and block states
+    if (tid < 64) bstate[tid] = st;
     // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
     for (int p = 0; p < np; p++) {
       if (plane_ssx(f, p))
@@ -370,23 +388,6 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
         if ((f.lfh_mask >> p) & 1) lfh_window(f, tb, p, sc, sr, win(p), hdec, tid);
       for (int p = 0; p < np; p++)
         if ((f.lfh_mask >> p) & 1) write_prelf(f, p, sc, sr, win(p), tid);
-    }
-    // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
-    if (tid < 64) {
-      const int by = tid >> 3, bx = tid & 7;
-      const int r = sr * 16 + 2 * by, c = sc * 16 + 2 * bx;
-      uint8_t st = 0;
-      if (r < f.mi_rows && c < f.mi_cols) {
-        st = 1;
-        if (idx >= 0) {
-          const av1pf_mi* m = f.mi + int64_t(r) * f.mi_stride + c;
-          const int ms = f.mi_stride;
-          const bool skip = (m[0].skip_segment & AV1PF_MI_SKIP) && (m[ms].skip_segment & AV1PF_MI_SKIP) &&
-                            (m[1].skip_segment & AV1PF_MI_SKIP) && (m[ms + 1].skip_segment & AV1PF_MI_SKIP);
-          if (!skip) st = 2;
-        }
-      }
-      bstate[tid] = st;
     }
     __syncthreads();
     // --- direction search (postfilter.rs:345-401): each thread two directions of one block ---

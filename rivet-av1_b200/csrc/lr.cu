@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
   for (int z = tid; z < 256; z += kThreads) a2tab[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
   __syncthreads();
 
-  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -234,7 +233,10 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     geo.y1 = min(geo.se, geo.pey);
     const int x0 = item.x0, w = int(item.x1) - int(item.x0);
     const int h = geo.y1 - geo.y0 + 1;
-    if (h <= 0 || w <= 0) continue;
+    if (h <= 0 || w <= 0) {
+      pdl_wait();  // every CTA waits, so the kernel never completes before its predecessor
+      continue;
+    }
     int type = AV1PF_RESTORE_NONE;
     av1pf_lr_unit unit{};
     if (f.lr_on && f.lr_type[p] != AV1PF_RESTORE_NONE) {
@@ -244,6 +246,9 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       unit = f.lru[p][unit_row * f.lr_unit_cols[p] + item.b];
       type = unit.type;
     }
+    // the descriptor and the unit are inputs of the chain; the planes below
+    // are the previous stage's output
+    pdl_wait();
     const DPlane dst = f.ref[p];
     if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
       copy_rect(f.up[p], dst, sb, x0, geo.y0, w, h, tid);

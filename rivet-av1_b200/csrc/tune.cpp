@@ -11,7 +11,11 @@
 //     halo).
 // The autotuner times each variant per frame shape as a one-frame batch
 // replayed from a CUDA graph (device time only), keeps the fastest in the
-// context, and the chain, batch and serving paths read it from there.
+// context, and the chain and serving paths read it from there. A batch
+// created with AV1PF_BATCH_AUTOTUNE is tuned as a whole instead: each variant
+// applied to every frame, and the per-shape choices, timed on the batch
+// itself (a batch's throughput and a single frame's latency can favour
+// different cuts).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,10 +52,10 @@ void Ctx::apply_tuning(FrameJob& j) const {
 
 namespace {
 
-// Median device time (ms) of `reps` replays of a one-frame batch.
-int time_variant(Ctx* ctx, const FrameJob& fj, int reps, float* ms) {
+// Median device time (ms) of `reps` replays of the batch of `fj`.
+int time_variant(Ctx* ctx, const FrameJob* fj, int n, int reps, float* ms) {
   av1pf_batch* b = nullptr;
-  int rc = create_batch(ctx, &fj, 1, 0, &b);
+  int rc = create_batch(ctx, fj, n, 0, &b);
   if (rc != AV1PF_OK) return rc;
   cudaStream_t s = ctx->own;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -110,7 +114,7 @@ int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only
         fj.lf_mode = mode;
         fj.lr_cols = cols;
         float ms = 0;
-        const int rc = time_variant(ctx, fj, reps, &ms);
+        const int rc = time_variant(ctx, &fj, 1, reps, &ms);
         if (rc != AV1PF_OK) return rc;
         if (!have || ms < best.ms) {
           best = ShapeChoice{mode, cols, ms};
@@ -122,6 +126,51 @@ int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only
       ctx->tuned[kv.first] = best;
     }
     if (n_shapes) ++*n_shapes;
+  }
+  return AV1PF_OK;
+}
+
+int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vector<FrameJob>& best) {
+  reps = std::max(1, std::min(reps, 1000));
+  auto base = [&](int i) {
+    const av1pf_job& j = jobs[i];
+    return FrameJob{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
+  };
+  bool any_cdef = false;
+  for (int i = 0; i < n_jobs; i++) any_cdef = any_cdef || jobs[i].params->cdef_enabled;
+  // candidates: each variant for every frame, and the per-shape record
+  std::vector<std::vector<FrameJob>> cands;
+  for (int mode = 0; mode < (any_cdef ? 3 : 2); mode++)
+    for (int cols : {64, 32}) {
+      std::vector<FrameJob> v;
+      for (int i = 0; i < n_jobs; i++) {
+        FrameJob fj = base(i);
+        fj.lf_mode = mode;
+        fj.lr_cols = cols;
+        v.push_back(fj);
+      }
+      cands.push_back(std::move(v));
+    }
+  {
+    std::vector<FrameJob> v;
+    for (int i = 0; i < n_jobs; i++) {
+      FrameJob fj = base(i);
+      ctx->apply_tuning(fj);
+      v.push_back(fj);
+    }
+    cands.push_back(std::move(v));
+  }
+  float best_ms = 0;
+  bool have = false;
+  for (auto& v : cands) {
+    float ms = 0;
+    const int rc = time_variant(ctx, v.data(), n_jobs, reps, &ms);
+    if (rc != AV1PF_OK) return rc;
+    if (!have || ms < best_ms) {
+      best_ms = ms;
+      best = v;
+      have = true;
+    }
   }
   return AV1PF_OK;
 }
