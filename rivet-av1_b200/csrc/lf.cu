@@ -49,6 +49,56 @@ __device__ __forceinline__ void append_edge(uint64_t* list, uint32_t* count, uin
   }
 }
 
+// Shared state of append_edges_cta.
+struct EdgeAgg {
+  uint32_t warp_off[2][8];  // per list: the warps' counts, then their offsets
+  uint32_t base[2];         // per list: the CTA's first slot
+};
+
+// Appends the active edges of all 256 threads of the CTA (every thread
+// calls) to two lists with one global atomic per list: each warp counts its
+// edges with a ballot, one thread sums the counts in shared memory and
+// reserves the CTA's range, and each edge goes to base + warp offset + rank.
+// (Every warp of every tile adding to the same two counters serialises on
+// them.)
+__device__ __forceinline__ void append_edges_cta(EdgeAgg& agg, uint64_t* list_a, uint64_t* list_b, uint32_t* counts,
+                                                 uint32_t cap, bool act_a, uint64_t ea, bool act_b, uint64_t eb) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned ma = __ballot_sync(0xffffffffu, act_a), mb = __ballot_sync(0xffffffffu, act_b);
+  if (lane == 0) {
+    agg.warp_off[0][warp] = uint32_t(__popc(ma));
+    agg.warp_off[1][warp] = uint32_t(__popc(mb));
+  }
+  __syncthreads();
+  if (threadIdx.x < 2) {
+    const int l = threadIdx.x;
+    uint32_t run = 0;
+    for (int w = 0; w < 8; w++) {
+      const uint32_t n = agg.warp_off[l][w];
+      agg.warp_off[l][w] = run;
+      run += n;
+    }
+    agg.base[l] = run ? atomicAdd(&counts[l], run) : 0u;
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  if (act_a) {
+    const uint32_t pos = agg.base[0] + agg.warp_off[0][warp] + uint32_t(__popc(ma & lt));
+    if (pos < cap)
+      list_a[pos] = ea;
+    else
+      atomicOr(&g_error_flags, ERRF_BAD_ITEM);
+  }
+  if (act_b) {
+    const uint32_t pos = agg.base[1] + agg.warp_off[1][warp] + uint32_t(__popc(mb & lt));
+    if (pos < cap)
+      list_b[pos] = eb;
+    else
+      atomicOr(&g_error_flags, ERRF_BAD_ITEM);
+  }
+  __syncthreads();  // agg is free for the next call
+}
+
 // Item: tile [x0,x1) x [y0,y1) of plane `plane` (samples). kind bit 0: copy
 // in -> cur over the tile; bit 1: decide the tile's 4x4 edges. 256 threads.
 __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __restrict__ frames,
@@ -56,6 +106,7 @@ __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __rest
                                                       uint64_t* __restrict__ list_v, uint64_t* __restrict__ list_h,
                                                       uint32_t* __restrict__ counts, uint32_t cap) {
   __shared__ LfTables tb;
+  __shared__ EdgeAgg agg;
   load_lf_tables(tb);
   __syncthreads();
   pdl_wait();  // the previous stage's output is complete past this point
@@ -106,14 +157,14 @@ __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __rest
       const int cx0 = item.x0 >> 2, cy0 = item.y0 >> 2;
       const int tw = (int(item.x1) - int(item.x0) + 3) >> 2;  // <= 16 (64-sample tiles)
       const int th = (int(item.y1) - int(item.y0) + 3) >> 2;
-      for (int k = threadIdx.x; k < th * 16; k += blockDim.x) {
-        const int cx = cx0 + (k & 15), cy = cy0 + (k >> 4);
-        const bool in = (k & 15) < tw && cx < gw && cy < gh;
-        int dv = 0, dh = 0;
-        if (in) lf_decide2(f, tb, plane, cx, cy, dv, dh);
-        append_edge(list_v, &counts[0], cap, dv != 0, pack_edge(item.frame, plane, dv, cx, cy));
-        append_edge(list_h, &counts[1], cap, dh != 0, pack_edge(item.frame, plane, dh, cx, cy));
-      }
+      // one 4x4 per thread (a 64x64 tile has 16 x 16 of them)
+      const int k = threadIdx.x;
+      const int cx = cx0 + (k & 15), cy = cy0 + (k >> 4);
+      const bool in = k < th * 16 && (k & 15) < tw && cx < gw && cy < gh;
+      int dv = 0, dh = 0;
+      if (in) lf_decide2(f, tb, plane, cx, cy, dv, dh);
+      append_edges_cta(agg, list_v, list_h, counts, cap, dv != 0, pack_edge(item.frame, plane, dv, cx, cy), dh != 0,
+                       pack_edge(item.frame, plane, dh, cx, cy));
     }
   }
 }
