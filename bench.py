@@ -530,7 +530,10 @@ def bench_serve(args, ctx, rank, duration_s=1.0):
     and frames already resident on the device (as a GPU decoder leaves them).
     Each is compared with the plain per-frame path on the same frame sequence
     (av1pf_chain_host / av1pf_chain, one call per frame), and the serving loop
-    is also run saturated (every frame of the sequence submitted at once).
+    is also run saturated (every frame of the sequence queued as one
+    av1pf_serve_submit_many group). The per-frame device path's throughput is
+    timed with its calls queued back to back, its latency with a synchronize
+    after each call.
     Latency is submit -> completion of the batch that carried the frame."""
     import threading
     import torch
@@ -574,7 +577,7 @@ def bench_serve(args, ctx, rank, duration_s=1.0):
     n = len(arrivals)
     px = sum(streams[si]["frames"][j].info.upscaled_width * streams[si]["frames"][j].info.frame_height
              for (_, si, j) in arrivals)
-    cfg = A.ServeConfig(40 << 30, 64, 2, 50)
+    cfg = A.ServeConfig(40 << 30, 64, 2, 50, 4)  # 40 GB cap, <= 64 frames a batch, 2 in flight, 4 slots a stream
     srv = C.c_void_p()
     A.check(L.av1pf_serve_open(ctx.p, C.byref(cfg), C.byref(srv)), "serve_open")
     for st in streams:
@@ -605,12 +608,20 @@ def bench_serve(args, ctx, rank, duration_s=1.0):
                 if keep_out is not None and fb is not None:
                     keep_out.setdefault((si, j), fb)
         th = threading.Thread(target=poller)
+        if not paced:
+            # saturated: the whole sequence in one group, queued at once
+            ids = (C.c_int32 * n)(*[streams[si]["sid"] for (_, si, _) in arrivals])
+            reqs = (A.Request * n)(*[streams[si][kind][j] for (_, si, j) in arrivals])
+            tks = (C.c_uint64 * n)()
         th.start()
         t0 = time.perf_counter()
-        for (ta, si, j) in arrivals:
-            if paced:
-                while time.perf_counter() - t0 < ta:
-                    time.sleep(0.0001)
+        if not paced:
+            A.check(L.av1pf_serve_submit_many(srv, n, ids, reqs, tks), "submit_many")
+            for k, (_, si, j) in enumerate(arrivals):
+                pending.put((tks[k], si, j))
+        for (ta, si, j) in (arrivals if paced else []):
+            while time.perf_counter() - t0 < ta:
+                time.sleep(0.0001)
             tk = C.c_uint64()
             A.check(L.av1pf_serve_submit(srv, streams[si]["sid"], C.byref(streams[si][kind][j]), C.byref(tk)),
                     "submit")
@@ -648,7 +659,16 @@ def bench_serve(args, ctx, rank, duration_s=1.0):
             exact = bool(np.array_equal(fb, outs[(si, j)]))
     t_pfh = time.perf_counter() - t0
     torch.cuda.synchronize()
+    # per-frame device path: throughput with the calls queued back to back
+    # (one synchronize at the end), then latency with a synchronize per call
     t0 = time.perf_counter()
+    for (ta, si, j) in arrivals:
+        df = streams[si]["dev"][j]
+        r_out, f_out = streams[si]["outs"][j]
+        A.check(L.av1pf_chain(ctx.p, C.byref(df.info), C.byref(df.params), C.byref(df.maps), df.inp.c, r_out.c,
+                              f_out.data_ptr(), None), "chain")
+    torch.cuda.synchronize()
+    t_pfd = time.perf_counter() - t0
     for (ta, si, j) in arrivals:
         df = streams[si]["dev"][j]
         r_out, f_out = streams[si]["outs"][j]
@@ -657,7 +677,6 @@ def bench_serve(args, ctx, rank, duration_s=1.0):
                               f_out.data_ptr(), None), "chain")
         torch.cuda.synchronize()
         pf_d.append(1e3 * (time.perf_counter() - a))
-    t_pfd = time.perf_counter() - t0
 
     def pct(v, q):
         return round(float(np.percentile(v, q)), 3)

@@ -376,6 +376,9 @@ typedef struct av1pf_serve_config {
   int32_t max_batch_frames; /* most frames one tick takes (0 = 64) */
   int32_t inflight_batches; /* batches on the device at once (0 = 2) */
   int32_t tick_us;          /* longest wait for more work before a tick */
+  int32_t slots_per_stream; /* frames of one stream resident at once (0 = 2);
+                               more slots let one batch take more of a
+                               stream's queued frames */
 } av1pf_serve_config;
 
 /* A submitted frame. With device == 0, `maps` and `in` are host pointers,
@@ -410,6 +413,11 @@ int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id);
 /* Queues one frame of `stream_id`; returns a ticket. Never blocks on the GPU. */
 int av1pf_serve_submit(av1pf_server* s, int32_t stream_id,
                        const av1pf_request* req, uint64_t* ticket);
+/* Queues n frames (frame k of stream stream_ids[k]) under one lock, in
+ * order, so one tick can batch them together; tickets[k] receives frame k's
+ * ticket. All or nothing: if one request is refused, none is queued. */
+int av1pf_serve_submit_many(av1pf_server* s, int32_t n, const int32_t* stream_ids,
+                            const av1pf_request* reqs, uint64_t* tickets);
 /* Waits up to `wait_ms` for `ticket`; on completion copies the packed output
  * frame to `frame_out` (av1pf_frame_bytes bytes; may be NULL) and returns the
  * submit->completion latency. AV1PF_ERR_TIMEOUT if not done in time. */

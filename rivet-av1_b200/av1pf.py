@@ -92,7 +92,7 @@ class Tuning(C.Structure):
 
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_cap_bytes", C.c_uint64), ("max_batch_frames", C.c_int32),
-                ("inflight_batches", C.c_int32), ("tick_us", C.c_int32)]
+                ("inflight_batches", C.c_int32), ("tick_us", C.c_int32), ("slots_per_stream", C.c_int32)]
 
 
 class Request(C.Structure):
@@ -184,6 +184,7 @@ def lib():
         _sig(L, "av1pf_serve_open_stream", C.c_int, vp, P(FrameInfo), P(C.c_int32))
         _sig(L, "av1pf_serve_close_stream", C.c_int, vp, C.c_int32)
         _sig(L, "av1pf_serve_submit", C.c_int, vp, C.c_int32, P(Request), P(C.c_uint64))
+        _sig(L, "av1pf_serve_submit_many", C.c_int, vp, C.c_int32, P(C.c_int32), P(Request), P(C.c_uint64))
         _sig(L, "av1pf_serve_poll", C.c_int, vp, C.c_uint64, C.c_int32, vp, P(C.c_double))
         _sig(L, "av1pf_serve_stats_get", C.c_int, vp, P(ServeStats))
         _sig(L, "av1pf_serve_close", C.c_int, vp)

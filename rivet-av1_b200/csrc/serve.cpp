@@ -414,104 +414,13 @@ bool same_geometry(const av1pf_frame_info& a, const av1pf_frame_info& b) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-int av1pf_serve_open(av1pf_ctx* ctx, const av1pf_serve_config* cfg, av1pf_server** out) {
-  if (!ctx || !out) return AV1PF_ERR_INVALID_INPUT;
+// Checks one request and, for a host request, packs its input into a pinned
+// buffer of its stream's pool; the request is not queued yet.
+int prepare_request(av1pf_server* s, int32_t stream_id, const av1pf_request* req, Request** out) {
   *out = nullptr;
-  cudaError_t e = cudaSetDevice(ctx->device);
-  if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
-  av1pf_server* s = new av1pf_server();
-  s->ctx = ctx;
-  if (cfg) s->cfg = *cfg;
-  const int nb = s->cfg.inflight_batches > 0 ? s->cfg.inflight_batches : 2;
-  for (int i = 0; i < nb; i++) {
-    InFlight* b = new InFlight();
-    b->wake = &s->cv;
-    if ((e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming)) != cudaSuccess) {
-      delete b;
-      av1pf_serve_close(s);
-      return cuda_status(e, "serving: stream create");
-    }
-    s->inflight.push_back(b);
-  }
-  s->worker = std::thread([s] { s->run(); });
-  *out = s;
-  return AV1PF_OK;
-}
-
-int av1pf_serve_open_stream(av1pf_server* s, const av1pf_frame_info* info, int32_t* stream_id) {
-  if (!s || !info || !stream_id) return AV1PF_ERR_INVALID_INPUT;
-  std::string why;
-  int rc = validate_frame(info, nullptr, nullptr, &why);
-  if (rc != AV1PF_OK) {
-    set_error(why);
-    return rc;
-  }
-  cudaSetDevice(s->ctx->device);
-  Stream* st = new Stream();
-  st->info = *info;
-  st->lay.build(*info);
-  const int nslots = 2;
-  std::lock_guard<std::mutex> lk(s->mu);
-  const size_t need = nslots * (st->lay.bytes + st->lay.ref_bytes + align256(st->lay.frame_bytes)) + 3 * 256;
-  if (s->cfg.hbm_cap_bytes && s->held + need > s->cfg.hbm_cap_bytes) {
-    delete st;
-    s->refused++;
-    set_error("serving: stream refused, its frame slots would exceed the HBM cap");
-    return AV1PF_ERR_ADMISSION;
-  }
-  st->slots.resize(nslots);
-  for (Slot& sl : st->slots) {
-    if ((rc = s->dev_alloc(&sl.dblob, st->lay.bytes)) || (rc = s->dev_alloc(&sl.dref, st->lay.ref_bytes)) ||
-        (rc = s->dev_alloc(&sl.dframe, align256(st->lay.frame_bytes)))) {
-      for (Slot& x : st->slots) {
-        s->dev_free(x.dblob, st->lay.bytes);
-        s->dev_free(x.dref, st->lay.ref_bytes);
-        s->dev_free(x.dframe, align256(st->lay.frame_bytes));
-      }
-      delete st;
-      return rc;
-    }
-  }
-  st->id = s->next_stream++;
-  s->streams[st->id] = st;
-  *stream_id = st->id;
-  return AV1PF_OK;
-}
-
-int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id) {
-  if (!s) return AV1PF_ERR_INVALID_INPUT;
-  std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->streams.find(stream_id);
-  if (it == s->streams.end()) return AV1PF_ERR_NOT_FOUND;
-  Stream* st = it->second;
-  st->closing = true;
-  // wait for the stream's queued and running frames
-  auto busy = [&] {
-    if (st->running) return true;
-    for (Request* r : s->queue)
-      if (r->stream == stream_id) return true;
-    return false;
-  };
-  while (busy()) s->cv_done.wait_for(lk, std::chrono::milliseconds(5));
-  cudaSetDevice(s->ctx->device);
-  for (Slot& x : st->slots) {
-    s->dev_free(x.dblob, st->lay.bytes);
-    s->dev_free(x.dref, st->lay.ref_bytes);
-    s->dev_free(x.dframe, align256(st->lay.frame_bytes));
-  }
-  for (void* p : st->all_pinned) cudaFreeHost(p);
-  s->streams.erase(it);
-  delete st;
-  return AV1PF_OK;
-}
-
-int av1pf_serve_submit(av1pf_server* s, int32_t stream_id, const av1pf_request* req, uint64_t* ticket) {
-  if (!s || !req || !ticket || !req->info || !req->params || !req->maps || !req->in) return AV1PF_ERR_INVALID_INPUT;
+  if (!s || !req || !req->info || !req->params || !req->maps || !req->in) return AV1PF_ERR_INVALID_INPUT;
   Stream* st = nullptr;
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -593,16 +502,159 @@ int av1pf_serve_submit(av1pf_server* s, int32_t stream_id, const av1pf_request* 
       std::memcpy(b + L.lr_off[p], m.lr_units[p], n * sizeof(av1pf_lr_unit));
     }
   }
+  *out = r;
+  return AV1PF_OK;
+}
+
+// Gives back what prepare_request took for a request that will not run.
+void discard_request(av1pf_server* s, Request* r) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (r->hin) r->st->pool_in.push_back(r->hin);
+  delete r;
+}
+
+// Queues prepared requests in order under one lock, so the worker sees them
+// together.
+void enqueue(av1pf_server* s, Request* const* rs, int n, uint64_t* tickets) {
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    r->ticket = s->next_ticket++;
-    r->t_submit = now_ms();
-    s->tickets[r->ticket] = r;
-    s->queue.push_back(r);
-    s->submitted++;
-    *ticket = r->ticket;
+    const double t = now_ms();
+    for (int k = 0; k < n; k++) {
+      Request* r = rs[k];
+      r->ticket = s->next_ticket++;
+      r->t_submit = t;
+      s->tickets[r->ticket] = r;
+      s->queue.push_back(r);
+      s->submitted++;
+      tickets[k] = r->ticket;
+    }
   }
   s->cv.notify_one();
+}
+
+}  // namespace
+
+extern "C" {
+
+int av1pf_serve_open(av1pf_ctx* ctx, const av1pf_serve_config* cfg, av1pf_server** out) {
+  if (!ctx || !out) return AV1PF_ERR_INVALID_INPUT;
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_status(e, "cudaSetDevice");
+  av1pf_server* s = new av1pf_server();
+  s->ctx = ctx;
+  if (cfg) s->cfg = *cfg;
+  const int nb = s->cfg.inflight_batches > 0 ? s->cfg.inflight_batches : 2;
+  for (int i = 0; i < nb; i++) {
+    InFlight* b = new InFlight();
+    b->wake = &s->cv;
+    if ((e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming)) != cudaSuccess) {
+      delete b;
+      av1pf_serve_close(s);
+      return cuda_status(e, "serving: stream create");
+    }
+    s->inflight.push_back(b);
+  }
+  s->worker = std::thread([s] { s->run(); });
+  *out = s;
+  return AV1PF_OK;
+}
+
+int av1pf_serve_open_stream(av1pf_server* s, const av1pf_frame_info* info, int32_t* stream_id) {
+  if (!s || !info || !stream_id) return AV1PF_ERR_INVALID_INPUT;
+  std::string why;
+  int rc = validate_frame(info, nullptr, nullptr, &why);
+  if (rc != AV1PF_OK) {
+    set_error(why);
+    return rc;
+  }
+  cudaSetDevice(s->ctx->device);
+  Stream* st = new Stream();
+  st->info = *info;
+  st->lay.build(*info);
+  const int nslots = s->cfg.slots_per_stream > 0 ? std::min(s->cfg.slots_per_stream, 64) : 2;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const size_t need = nslots * (st->lay.bytes + st->lay.ref_bytes + align256(st->lay.frame_bytes)) + 3 * 256;
+  if (s->cfg.hbm_cap_bytes && s->held + need > s->cfg.hbm_cap_bytes) {
+    delete st;
+    s->refused++;
+    set_error("serving: stream refused, its frame slots would exceed the HBM cap");
+    return AV1PF_ERR_ADMISSION;
+  }
+  st->slots.resize(nslots);
+  for (Slot& sl : st->slots) {
+    if ((rc = s->dev_alloc(&sl.dblob, st->lay.bytes)) || (rc = s->dev_alloc(&sl.dref, st->lay.ref_bytes)) ||
+        (rc = s->dev_alloc(&sl.dframe, align256(st->lay.frame_bytes)))) {
+      for (Slot& x : st->slots) {
+        s->dev_free(x.dblob, st->lay.bytes);
+        s->dev_free(x.dref, st->lay.ref_bytes);
+        s->dev_free(x.dframe, align256(st->lay.frame_bytes));
+      }
+      delete st;
+      return rc;
+    }
+  }
+  st->id = s->next_stream++;
+  s->streams[st->id] = st;
+  *stream_id = st->id;
+  return AV1PF_OK;
+}
+
+int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id) {
+  if (!s) return AV1PF_ERR_INVALID_INPUT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->streams.find(stream_id);
+  if (it == s->streams.end()) return AV1PF_ERR_NOT_FOUND;
+  Stream* st = it->second;
+  st->closing = true;
+  // wait for the stream's queued and running frames
+  auto busy = [&] {
+    if (st->running) return true;
+    for (Request* r : s->queue)
+      if (r->stream == stream_id) return true;
+    return false;
+  };
+  while (busy()) s->cv_done.wait_for(lk, std::chrono::milliseconds(5));
+  cudaSetDevice(s->ctx->device);
+  for (Slot& x : st->slots) {
+    s->dev_free(x.dblob, st->lay.bytes);
+    s->dev_free(x.dref, st->lay.ref_bytes);
+    s->dev_free(x.dframe, align256(st->lay.frame_bytes));
+  }
+  for (void* p : st->all_pinned) cudaFreeHost(p);
+  s->streams.erase(it);
+  delete st;
+  return AV1PF_OK;
+}
+
+int av1pf_serve_submit(av1pf_server* s, int32_t stream_id, const av1pf_request* req, uint64_t* ticket) {
+  if (!ticket) return AV1PF_ERR_INVALID_INPUT;
+  Request* r = nullptr;
+  const int rc = prepare_request(s, stream_id, req, &r);
+  if (rc != AV1PF_OK) return rc;
+  enqueue(s, &r, 1, ticket);
+  return AV1PF_OK;
+}
+
+int av1pf_serve_submit_many(av1pf_server* s, int32_t n, const int32_t* stream_ids, const av1pf_request* reqs,
+                            uint64_t* tickets) {
+  if (!s || n < 0 || (n > 0 && (!stream_ids || !reqs || !tickets))) return AV1PF_ERR_INVALID_INPUT;
+  std::vector<Request*> rs;
+  rs.reserve(size_t(n));
+  for (int k = 0; k < n; k++) {
+    Request* r = nullptr;
+    const int rc = prepare_request(s, stream_ids[k], &reqs[k], &r);
+    if (rc != AV1PF_OK) {
+      for (Request* q : rs) discard_request(s, q);
+      set_error("serving: request " + std::to_string(k) + " of the group refused (none queued)");
+      return rc;
+    }
+    rs.push_back(r);
+  }
+  if (n > 0) enqueue(s, rs.data(), n, tickets);
   return AV1PF_OK;
 }
 

@@ -165,3 +165,45 @@ def test_serve_device_resident_requests():
             assert np.array_equal(ref.host(p), ref_cpu.arrays[p])
     A.check(L().av1pf_serve_close(srv))
     ctx.close()
+
+
+def test_serve_submit_many_group():
+    """A group of frames queued at once (av1pf_serve_submit_many) comes back
+    equal to the oracle, with 4 slots per stream letting ticks batch several
+    frames of one stream; a group with one bad request queues nothing."""
+    ctx = G.Ctx()
+    frames = {i: [A.SynthHandle(**cfg, seed=300 + 10 * i + k, frame_index=k) for k in range(3)]
+              for i, cfg in enumerate(STREAMS)}
+    want = {(i, k): O.chain(sf, threads=0)[1] for i in frames for k, sf in enumerate(frames[i])}
+    keep = []
+    cfg = A.ServeConfig(40 << 30, 32, 2, 100, 4)
+    srv = C.c_void_p()
+    A.check(L().av1pf_serve_open(ctx.p, C.byref(cfg), C.byref(srv)), "serve_open")
+    sids = {}
+    for i in frames:
+        s = C.c_int32()
+        A.check(L().av1pf_serve_open_stream(srv, C.byref(frames[i][0].f.info), C.byref(s)))
+        sids[i] = s.value
+    order = [(i, k) for rep in range(2) for k in range(3) for i in frames]
+    n = len(order)
+    ids = (C.c_int32 * n)(*[sids[i] for i, _ in order])
+    reqs = (A.Request * n)(*[request(frames[i][k], keep) for i, k in order])
+    tks = (C.c_uint64 * n)()
+    A.check(L().av1pf_serve_submit_many(srv, n, ids, reqs, tks), "submit_many")
+    assert len(set(tks)) == n
+    for t, (i, k) in zip(tks, order):
+        out = np.zeros(A.frame_bytes(frames[i][k].f.info), np.uint8)
+        A.check(L().av1pf_serve_poll(srv, t, 20000, out.ctypes.data, None), "poll")
+        assert np.array_equal(out, want[(i, k)]), (i, k)
+    st = A.ServeStats()
+    A.check(L().av1pf_serve_stats_get(srv, C.byref(st)))
+    assert st.completed == st.submitted == n
+    # all or nothing: an unknown stream in the group refuses the whole group
+    bad = (C.c_int32 * 2)(sids[0], 999)
+    reqs2 = (A.Request * 2)(request(frames[0][0], keep), request(frames[0][1], keep))
+    tks2 = (C.c_uint64 * 2)()
+    assert L().av1pf_serve_submit_many(srv, 2, bad, reqs2, tks2) == A.ERR_NOT_FOUND
+    A.check(L().av1pf_serve_stats_get(srv, C.byref(st)))
+    assert st.submitted == n
+    A.check(L().av1pf_serve_close(srv))
+    ctx.close()
