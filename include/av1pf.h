@@ -323,6 +323,12 @@ typedef struct av1pf_batch av1pf_batch;
  * whole batch (and the per-shape choices) on the batch itself and plan the
  * fastest. The jobs' outputs are overwritten while timing. */
 #define AV1PF_BATCH_AUTOTUNE 2u
+/* Frame groups: (n << AV1PF_BATCH_GROUPS_SHIFT), n in 1..15, splits the
+ * frames into n groups of about equal samples whose stage chains run as
+ * parallel branches of the graph, so stages of different groups overlap on
+ * the device. 0 (the default): 2 groups from 8 frames up, else 1. With
+ * AV1PF_BATCH_AUTOTUNE the tuned count replaces it. */
+#define AV1PF_BATCH_GROUPS_SHIFT 8
 int av1pf_batch_create(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs,
                        uint32_t flags, av1pf_batch** out);
 /* Runs the planned batch on `stream` (graph launch). */

@@ -24,6 +24,7 @@ MI_SKIP = 0x80
 RESTORE_NONE, RESTORE_WIENER, RESTORE_SGRPROJ = 0, 1, 2
 BATCH_NO_GRAPH = 1
 BATCH_AUTOTUNE = 2
+BATCH_GROUPS_SHIFT = 8
 
 
 class Plane(C.Structure):

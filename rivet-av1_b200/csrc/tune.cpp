@@ -52,10 +52,11 @@ void Ctx::apply_tuning(FrameJob& j) const {
 
 namespace {
 
-// Median device time (ms) of `reps` replays of the batch of `fj`.
-int time_variant(Ctx* ctx, const FrameJob* fj, int n, int reps, float* ms) {
+// Median device time (ms) of `reps` replays of the batch of `fj` in
+// `groups` frame groups.
+int time_variant(Ctx* ctx, const FrameJob* fj, int n, int reps, float* ms, int groups = 1) {
   av1pf_batch* b = nullptr;
-  int rc = create_batch(ctx, fj, n, 0, &b);
+  int rc = create_batch(ctx, fj, n, uint32_t(groups) << AV1PF_BATCH_GROUPS_SHIFT, &b);
   if (rc != AV1PF_OK) return rc;
   cudaStream_t s = ctx->own;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -130,7 +131,8 @@ int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only
   return AV1PF_OK;
 }
 
-int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vector<FrameJob>& best) {
+int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vector<FrameJob>& best,
+               int* best_groups) {
   reps = std::max(1, std::min(reps, 1000));
   auto base = [&](int i) {
     const av1pf_job& j = jobs[i];
@@ -162,16 +164,19 @@ int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vecto
   }
   float best_ms = 0;
   bool have = false;
-  for (auto& v : cands) {
-    float ms = 0;
-    const int rc = time_variant(ctx, v.data(), n_jobs, reps, &ms);
-    if (rc != AV1PF_OK) return rc;
-    if (!have || ms < best_ms) {
-      best_ms = ms;
-      best = v;
-      have = true;
+  *best_groups = 1;
+  for (int groups = 1; groups <= std::min(3, n_jobs); groups++)
+    for (auto& v : cands) {
+      float ms = 0;
+      const int rc = time_variant(ctx, v.data(), n_jobs, reps, &ms, groups);
+      if (rc != AV1PF_OK) return rc;
+      if (!have || ms < best_ms) {
+        best_ms = ms;
+        best = v;
+        *best_groups = groups;
+        have = true;
+      }
     }
-  }
   return AV1PF_OK;
 }
 

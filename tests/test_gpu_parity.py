@@ -264,7 +264,8 @@ def test_batch_matches_per_frame(ctx):
         jobs[i].inp = C.cast(d.inp.c, C.POINTER(A.Plane))
         jobs[i].ref_out = C.cast(r.c, C.POINTER(A.Plane))
         jobs[i].frame_out = fb.data_ptr()
-    for flags in (0, A.BATCH_NO_GRAPH):
+    # graph and direct launches; frame groups on parallel branches (2 and 3)
+    for flags in (0, A.BATCH_NO_GRAPH, 3 << A.BATCH_GROUPS_SHIFT, A.BATCH_NO_GRAPH | (2 << A.BATCH_GROUPS_SHIFT)):
         for r, fb in outs:
             for t in r.t:
                 t.zero_()
