@@ -38,7 +38,7 @@ struct BlkTaps {
   int16_t pri, sec;
   int16_t po0, po1, so00, so01, so10, so11;
   int8_t pri_adj, sec_adj, pt0, pt1;
-  int8_t copy, pad0, pad1, pad2;
+  int8_t copy, one, pad1, pad2;  // one: always 1 (see cdef_tap)
 };
 
 }  // namespace
@@ -48,12 +48,18 @@ struct BlkTaps {
 struct TapsDev {
   int pri, sec, pri_adj, sec_adj, pt0, pt1;
   int po0, po1, so00, so01, so10, so11;
+  int one, mone;  // 1 and -1, read from shared memory (see cdef_tap)
 };
 
-__device__ __forceinline__ void cdef_tap(int p, int x, int str, int adj, int w, int& sum, int& mx, unsigned& mn) {
-  const int d = p - x;
-  const int lim = max(0, str - (abs(d) >> adj));
-  sum += w * min(max(d, -lim), lim);
+// `one` is 1 and `mone` -1 at run time but opaque to the compiler, so the
+// differences below are integer multiply-adds: the kernel is bound by the
+// integer ALU pipe, and these move three of a tap's operations to the
+// multiply-add pipe, which is otherwise mostly idle. nx = -x.
+__device__ __forceinline__ void cdef_tap(int p, int nx, int one, int mone, int str, int adj, int w, int& sum, int& mx,
+                                         unsigned& mn) {
+  const int d = p * one + nx;                              // p - x
+  const int lim = max(0, (abs(d) >> adj) * mone + str);    // max(0, str - (|d| >> adj))
+  sum += w * min(max(d, lim * mone), lim);                 // constrain(d)
   mx = max(mx, p);
   mn = min(mn, unsigned(p));
 }
@@ -67,23 +73,24 @@ __device__ __forceinline__ void cdef_tap(int p, int x, int str, int adj, int w, 
 template <int MODE>
 __device__ __forceinline__ int cdef_px(const int16_t* c, const TapsDev& t) {
   const int x = c[0];
+  const int nx = x * t.mone;
   int sum = 0, mx = x;
   unsigned mn = unsigned(x);
   if (MODE != 2) {
-    cdef_tap(c[t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-    cdef_tap(c[-t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-    cdef_tap(c[t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
-    cdef_tap(c[-t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+    cdef_tap(c[t.po0], nx, t.one, t.mone, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+    cdef_tap(c[-t.po0], nx, t.one, t.mone, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+    cdef_tap(c[t.po1], nx, t.one, t.mone, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+    cdef_tap(c[-t.po1], nx, t.one, t.mone, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
   }
   if (MODE != 1) {
-    cdef_tap(c[t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-    cdef_tap(c[-t.so00], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-    cdef_tap(c[t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-    cdef_tap(c[-t.so01], x, t.sec, t.sec_adj, 2, sum, mx, mn);
-    cdef_tap(c[t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-    cdef_tap(c[-t.so10], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-    cdef_tap(c[t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
-    cdef_tap(c[-t.so11], x, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[t.so00], nx, t.one, t.mone, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[-t.so00], nx, t.one, t.mone, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[t.so01], nx, t.one, t.mone, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[-t.so01], nx, t.one, t.mone, t.sec, t.sec_adj, 2, sum, mx, mn);
+    cdef_tap(c[t.so10], nx, t.one, t.mone, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[-t.so10], nx, t.one, t.mone, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[t.so11], nx, t.one, t.mone, t.sec, t.sec_adj, 1, sum, mx, mn);
+    cdef_tap(c[-t.so11], nx, t.one, t.mone, t.sec, t.sec_adj, 1, sum, mx, mn);
   }
   const int v = x + ((8 + sum - (sum < 0 ? 1 : 0)) >> 4);
   return MODE == 0 ? min(max(v, int(mn)), mx) : v;
@@ -108,7 +115,8 @@ __device__ __forceinline__ BlkTaps make_blk_taps(int pri, int sec, int damping, 
   t.so10 = int16_t(c_cdef_dirs[dlo][1][0] * st + c_cdef_dirs[dlo][1][1]);
   t.so11 = int16_t(c_cdef_dirs[dhi][1][0] * st + c_cdef_dirs[dhi][1][1]);
   t.copy = (pri == 0 && sec == 0) ? 1 : 0;  // a zero-strength filter is the identity
-  t.pad0 = t.pad1 = t.pad2 = 0;
+  t.one = 1;
+  t.pad1 = t.pad2 = 0;
   return t;
 }
 
@@ -126,6 +134,8 @@ __device__ __forceinline__ TapsDev taps_of(const BlkTaps& b) {
   t.so01 = b.so01;
   t.so10 = b.so10;
   t.so11 = b.so11;
+  t.one = b.one;
+  t.mone = -t.one;
   return t;
 }
 
@@ -528,18 +538,18 @@ __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cde
   const int x = c[0];
   int sum = 0, mx = x;
   unsigned mn = unsigned(x);
-  cdef_tap(c[t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-  cdef_tap(c[-t.po0], x, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
-  cdef_tap(c[t.so00], x, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
-  cdef_tap(c[-t.so00], x, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
-  cdef_tap(c[t.so01], x, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
-  cdef_tap(c[-t.so01], x, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
-  cdef_tap(c[t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
-  cdef_tap(c[-t.po1], x, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
-  cdef_tap(c[t.so10], x, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
-  cdef_tap(c[-t.so10], x, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
-  cdef_tap(c[t.so11], x, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
-  cdef_tap(c[-t.so11], x, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
+  cdef_tap(c[t.po0], -x, 1, -1, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+  cdef_tap(c[-t.po0], -x, 1, -1, t.pri, t.pri_adj, t.pt0, sum, mx, mn);
+  cdef_tap(c[t.so00], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
+  cdef_tap(c[-t.so00], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
+  cdef_tap(c[t.so01], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
+  cdef_tap(c[-t.so01], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[0], sum, mx, mn);
+  cdef_tap(c[t.po1], -x, 1, -1, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+  cdef_tap(c[-t.po1], -x, 1, -1, t.pri, t.pri_adj, t.pt1, sum, mx, mn);
+  cdef_tap(c[t.so10], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
+  cdef_tap(c[-t.so10], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
+  cdef_tap(c[t.so11], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
+  cdef_tap(c[-t.so11], -x, 1, -1, t.sec, t.sec_adj, a.sec_taps[1], sum, mx, mn);
   const int v = x + ((8 + sum - (sum < 0 ? 1 : 0)) >> 4);
   res[int64_t(e) * 64 + i * a.w + j] = uint16_t(min(max(v, int(mn)), mx));
 }
