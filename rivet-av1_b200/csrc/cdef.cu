@@ -96,9 +96,12 @@ __device__ __forceinline__ int cdef_px(const int16_t* c, const TapsDev& t) {
   return MODE == 0 ? min(max(v, int(mn)), mx) : v;
 }
 
-// The Taps of cdef_filter_block (postfilter.rs:489-511) for a window of row
-// stride `st`. CDEF_SEC_TAPS is [2, 1] for both primary-tap parities.
-__device__ __forceinline__ BlkTaps make_blk_taps(int pri, int sec, int damping, int dir, int coeff_shift, int st) {
+// The Taps of cdef_filter_block (postfilter.rs:489-511); doff[d][k] is the
+// window offset of CDEF_DIRECTIONS[d][k] (shared memory: the threads index
+// it by their blocks' directions). CDEF_SEC_TAPS is [2, 1] for both
+// primary-tap parities.
+__device__ __forceinline__ BlkTaps make_blk_taps(int pri, int sec, int damping, int dir, int coeff_shift,
+                                                 const int16_t (*doff)[2]) {
   BlkTaps t;
   t.pri = int16_t(pri);
   t.sec = int16_t(sec);
@@ -108,12 +111,12 @@ __device__ __forceinline__ BlkTaps make_blk_taps(int pri, int sec, int damping, 
   t.pt0 = int8_t(odd ? 3 : 4);
   t.pt1 = int8_t(odd ? 3 : 2);
   const int dlo = (dir + 6) & 7, dhi = (dir + 2) & 7;
-  t.po0 = int16_t(c_cdef_dirs[dir][0][0] * st + c_cdef_dirs[dir][0][1]);
-  t.po1 = int16_t(c_cdef_dirs[dir][1][0] * st + c_cdef_dirs[dir][1][1]);
-  t.so00 = int16_t(c_cdef_dirs[dlo][0][0] * st + c_cdef_dirs[dlo][0][1]);
-  t.so01 = int16_t(c_cdef_dirs[dhi][0][0] * st + c_cdef_dirs[dhi][0][1]);
-  t.so10 = int16_t(c_cdef_dirs[dlo][1][0] * st + c_cdef_dirs[dlo][1][1]);
-  t.so11 = int16_t(c_cdef_dirs[dhi][1][0] * st + c_cdef_dirs[dhi][1][1]);
+  t.po0 = doff[dir][0];
+  t.po1 = doff[dir][1];
+  t.so00 = doff[dlo][0];
+  t.so01 = doff[dhi][0];
+  t.so10 = doff[dlo][1];
+  t.so11 = doff[dhi][1];
   t.copy = (pri == 0 && sec == 0) ? 1 : 0;  // a zero-strength filter is the identity
   t.one = 1;
   t.pad1 = t.pad2 = 0;
@@ -177,7 +180,7 @@ __device__ __forceinline__ int32_t cdef_cost_of(const int32_t* p) {
 // Costs of directions P and P + 4 of the 8x8 block whose top-left sample is
 // window word `w0` (4-byte aligned); samples are >> sh then - 128.
 template <int P>
-__device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int32_t& c1, int32_t& c2) {
+__device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int one, int32_t& c1, int32_t& c2) {
   int32_t a[15], b[15];
 #pragma unroll
   for (int k = 0; k < 15; k++) a[k] = b[k] = 0;
@@ -191,8 +194,9 @@ __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int32_t
       for (int h = 0; h < 2; h++) {
         const int j = 2 * q + h;
         const int x = ((int(int16_t(h ? (w >> 16) : (w & 0xffffu)))) >> sh) - 128;
-        a[cdef_bin<P>(i, j)] += x;
-        b[cdef_bin<P + 4>(i, j)] += x;
+        // multiply-adds by an opaque 1: the bins accumulate on the multiply-add pipe
+        a[cdef_bin<P>(i, j)] = x * one + a[cdef_bin<P>(i, j)];
+        b[cdef_bin<P + 4>(i, j)] = x * one + b[cdef_bin<P + 4>(i, j)];
       }
     }
   }
@@ -353,9 +357,15 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
   __shared__ uint8_t bstate[64];  // 0 = outside the MI area, 1 = copy, 2 = filter
   __shared__ LfTables tb;
   __shared__ uint16_t hdec[19 * 18];  // horizontal-edge decisions of one plane
+  __shared__ int16_t doff[8][2];      // window offsets of CDEF_DIRECTIONS
+  __shared__ uint8_t uvdir[2][2][8];  // CDEF_UV_DIR
+  __shared__ int s_one;               // 1, opaque to the compiler (see cdef_tap)
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   load_lf_tables(tb);
+  if (tid < 16) doff[tid >> 1][tid & 1] = int16_t(c_cdef_dirs[tid >> 1][tid & 1][0] * kS + c_cdef_dirs[tid >> 1][tid & 1][1]);
+  if (tid < 32) (&uvdir[0][0][0])[tid] = (&c_cdef_uv_dir[0][0][0])[tid];
+  if (tid == 0) s_one = 1;
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -409,10 +419,10 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
         const int16_t* s = &win(0)[(top + by * 8) * kS + kColOff + bx * 8];
         int32_t c1, c2;
         switch (pair) {
-          case 0: cdef_cost_pair<0>(s, cs, c1, c2); break;
-          case 1: cdef_cost_pair<1>(s, cs, c1, c2); break;
-          case 2: cdef_cost_pair<2>(s, cs, c1, c2); break;
-          default: cdef_cost_pair<3>(s, cs, c1, c2); break;
+          case 0: cdef_cost_pair<0>(s, cs, s_one, c1, c2); break;
+          case 1: cdef_cost_pair<1>(s, cs, s_one, c1, c2); break;
+          case 2: cdef_cost_pair<2>(s, cs, s_one, c1, c2); break;
+          default: cdef_cost_pair<3>(s, cs, s_one, c1, c2); break;
         }
         cost[b][pair] = c1;
         cost[b][pair + 4] = c2;
@@ -442,10 +452,10 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
         lp = var != 0 ? (pri * (4 + var_str) + 8) >> 4 : 0;
         up = f.cdef_uv_pri[idx] << cs;
         us = f.cdef_uv_sec[idx] << cs;
-        ud = up == 0 ? 0 : c_cdef_uv_dir[f.ssx][f.ssy][y_dir];
+        ud = up == 0 ? 0 : uvdir[f.ssx][f.ssy][y_dir];
       }
-      BlkTaps L = make_blk_taps(lp, ls, f.cdef_damping + cs, ld, cs, kS);
-      BlkTaps U = make_blk_taps(up, us, f.cdef_damping + cs - 1, ud, cs, kS);
+      BlkTaps L = make_blk_taps(lp, ls, f.cdef_damping + cs, ld, cs, doff);
+      BlkTaps U = make_blk_taps(up, us, f.cdef_damping + cs - 1, ud, cs, doff);
       if (!filt) L.copy = U.copy = 1;
       taps[0][b] = L;
       taps[1][b] = U;
