@@ -283,8 +283,10 @@ def main_gpu(args):
     # ---- roofline of the dominant stage ----
     info = dfs[0].info
     S = plane_set_bytes(info)
-    algo = {"loop_filter": 2 * S, "cdef": 2 * S, "superres": 2 * S, "loop_restoration": 2 * S,
-            "output": 2 * S}
+    # loop restoration reads the CDEF output and writes the reference frame
+    # and (no film grain here) the packed frame
+    algo = {"loop_filter": 2 * S, "cdef": 2 * S, "superres": 2 * S,
+            "loop_restoration": 2 * S + A.frame_bytes(info), "output": 2 * S}
     dom = max(stage_ms, key=stage_ms.get)
     peak, peak_kind = peaks()
     achieved = algo[dom] / (stage_ms[dom] / 1e3) / 1e9

@@ -43,6 +43,10 @@ struct FrameDesc {
   int32_t lfh_mask;
   uint8_t* frame_out;
   int64_t out_off[3];
+  // Without film grain the packed frame holds the reference frame's samples
+  // unchanged: the loop-restoration kernel then writes both and the frame
+  // has no output items.
+  int32_t lr_pack;
   // maps (av1pf_maps)
   const av1pf_mi* mi;
   const uint8_t* tx[3];

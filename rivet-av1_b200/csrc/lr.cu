@@ -15,8 +15,12 @@
 // and one old row of horizontal sums per step), which is exact in 32 bits for
 // <= 12-bit samples (25 * 4095^2 < 2^31); the products the reference forms in
 // 64 bits (p * s and the B term) are 32x32->64 multiplies here. Rectangles of
-// units without restoration (and planes or frames without it) are copied, so
-// the kernel writes the whole visible area of the reference frame.
+// units without restoration (and planes or frames without it) pass their
+// samples through, so the kernel writes the whole visible area of the
+// reference frame. Every rectangle's output gathers in a shared-memory tile
+// and leaves in 16-byte row chunks: to the reference frame and, for a frame
+// without film grain, to the packed output frame too, so such a frame needs
+// no output pass.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -49,7 +53,7 @@ struct LrSrc {
   const uint8_t* up;
   const uint8_t* cur;
   const uint8_t* lines;
-  int64_t up_pitch, cur_pitch, lines_pitch;  // bytes
+  int32_t up_pitch, cur_pitch, lines_pitch;  // bytes
   bool sr;  // the pre-CDEF rows come from `lines` (4 per stripe boundary), not `cur`
 };
 
@@ -73,31 +77,81 @@ __device__ __forceinline__ const uint8_t* lr_row(const LrSrc& src, const LrGeom&
   return src.up + int64_t(y) * src.up_pitch;
 }
 
-// Copies a w x h rectangle (w <= 64) between planes of sample width sb:
-// 16-byte chunks when both rows are 16-byte aligned there, else samples.
-__device__ __forceinline__ void copy_rect(const DPlane& src, const DPlane& dst, int sb, int x0, int y0, int w, int h,
+__device__ __forceinline__ int ld_row(const uint8_t* row, int sb, int x) {
+  return sb == 1 ? int(row[x]) : int(reinterpret_cast<const uint16_t*>(row)[x]);
+}
+
+// Reads the w x h samples at (x0, y0) of `src` (sample width sb) into `tile`
+// (int32, row stride kMaxW): 16-byte chunks where the rows allow them, else
+// single samples.
+__device__ __forceinline__ void load_tile(const DPlane& src, int sb, int x0, int y0, int w, int h, int32_t* tile,
                                           int tid) {
-  const int bytes = w * sb;
   const uint8_t* s0 = src.p + (int64_t(y0) * src.stride + x0) * sb;
-  uint8_t* d0 = dst.p + (int64_t(y0) * dst.stride + x0) * sb;
-  const int64_t sp = src.stride * sb, dp = dst.stride * sb;
-  const bool aligned = ((reinterpret_cast<uintptr_t>(s0) | reinterpret_cast<uintptr_t>(d0) | uintptr_t(sp) |
-                         uintptr_t(dp)) & 15) == 0;
-  // 8 chunk slots per row (w * sb <= 128 bytes); a ragged last chunk goes bytewise
+  const int64_t sp = src.stride * sb;
+  const bool vec = ((reinterpret_cast<uintptr_t>(s0) | uintptr_t(sp)) & 15) == 0;
+  const int cs = sb == 2 ? 3 : 4;  // log2 samples per chunk
   for (int k = tid; k < h * 8; k += kThreads) {
-    const int r = k >> 3, ch = k & 7;
-    const uint8_t* sr = s0 + r * sp + ch * 16;
-    uint8_t* dr = d0 + r * dp + ch * 16;
-    if (aligned && ch * 16 + 16 <= bytes) {
-      *reinterpret_cast<uint4*>(dr) = *reinterpret_cast<const uint4*>(sr);
+    const int r = k >> 3, e0 = (k & 7) << cs;
+    if (e0 >= w) continue;
+    const uint8_t* row = s0 + int64_t(r) * sp;
+    int32_t* t = tile + r * kMaxW + e0;
+    if (vec && e0 + (1 << cs) <= w) {
+      const uint4 q = *reinterpret_cast<const uint4*>(row + e0 * sb);
+      if (sb == 2) {
+        reinterpret_cast<int4*>(t)[0] = make_int4(q.x & 0xffff, q.x >> 16, q.y & 0xffff, q.y >> 16);
+        reinterpret_cast<int4*>(t)[1] = make_int4(q.z & 0xffff, q.z >> 16, q.w & 0xffff, q.w >> 16);
+      } else {
+        const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          reinterpret_cast<int4*>(t)[j] =
+              make_int4(wd[j] & 0xff, (wd[j] >> 8) & 0xff, (wd[j] >> 16) & 0xff, wd[j] >> 24);
+      }
     } else {
-      for (int b = 0; b < min(16, bytes - ch * 16); b++) dr[b] = sr[b];
+      for (int e = e0; e < min(w, e0 + (1 << cs)); e++) t[e - e0] = ld_row(row, sb, e);
     }
   }
 }
 
-__device__ __forceinline__ int ld_row(const uint8_t* row, int sb, int x) {
-  return sb == 1 ? int(row[x]) : int(reinterpret_cast<const uint16_t*>(row)[x]);
+// Writes the w x h output samples of `tile` (int32, row stride kMaxW) to
+// rows of `width`-byte samples from `base`, `pitch` bytes apart: 16-byte
+// chunks (8 or 16 samples) where `vec` says the rows allow them, else single
+// samples.
+__device__ __forceinline__ void store_tile(const int32_t* tile, uint8_t* base, int64_t pitch, int width, bool vec,
+                                           int w, int h, int tid) {
+  const int cs = width == 2 ? 3 : 4;  // log2 samples per chunk
+  for (int k = tid; k < h * 8; k += kThreads) {
+    const int r = k >> 3, e0 = (k & 7) << cs;
+    if (e0 >= w) continue;
+    const int32_t* t = tile + r * kMaxW + e0;
+    uint8_t* row = base + int64_t(r) * pitch;
+    if (vec && e0 + (1 << cs) <= w) {
+      const int4 a = *reinterpret_cast<const int4*>(t);
+      const int4 b = *reinterpret_cast<const int4*>(t + 4);
+      uint4 q;
+      if (width == 2) {
+        q.x = uint32_t(a.x) | (uint32_t(a.y) << 16);
+        q.y = uint32_t(a.z) | (uint32_t(a.w) << 16);
+        q.z = uint32_t(b.x) | (uint32_t(b.y) << 16);
+        q.w = uint32_t(b.z) | (uint32_t(b.w) << 16);
+      } else {
+        const int4 c = *reinterpret_cast<const int4*>(t + 8);
+        const int4 d = *reinterpret_cast<const int4*>(t + 12);
+        q.x = uint32_t(a.x) | (uint32_t(a.y) << 8) | (uint32_t(a.z) << 16) | (uint32_t(a.w) << 24);
+        q.y = uint32_t(b.x) | (uint32_t(b.y) << 8) | (uint32_t(b.z) << 16) | (uint32_t(b.w) << 24);
+        q.z = uint32_t(c.x) | (uint32_t(c.y) << 8) | (uint32_t(c.z) << 16) | (uint32_t(c.w) << 24);
+        q.w = uint32_t(d.x) | (uint32_t(d.y) << 8) | (uint32_t(d.z) << 16) | (uint32_t(d.w) << 24);
+      }
+      *reinterpret_cast<uint4*>(row + e0 * width) = q;
+    } else {
+      for (int e = e0; e < min(w, e0 + (1 << cs)); e++) {
+        if (width == 2)
+          reinterpret_cast<uint16_t*>(row)[e] = uint16_t(t[e - e0]);
+        else
+          row[e] = uint8_t(t[e - e0]);
+      }
+    }
+  }
 }
 
 // Box sums of radius R over the window and the A / B of box_filter_rect
@@ -208,6 +262,7 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
   int32_t* B = reinterpret_cast<int32_t*>(smem + kWinBytes + kABytes);
   int32_t* a2tab = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
   int32_t* F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes + 256 * 4);
+  __shared__ av1pf_lr_unit s_unit;
   int16_t* inter = reinterpret_cast<int16_t*>(A);  // Wiener reuses the A area
   const int tid = threadIdx.x;
   const int g = tid / kCols, c = tid - g * kCols;
@@ -238,130 +293,150 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       continue;
     }
     int type = AV1PF_RESTORE_NONE;
-    av1pf_lr_unit unit{};
+    const av1pf_lr_unit* unit_p = nullptr;
     if (f.lr_on && f.lr_type[p] != AV1PF_RESTORE_NONE) {
       const int unit_size = f.lr_unit_size[p];
       const int luma_row = max(s * 64 - 8, 0);
       const int unit_row = min(f.lr_unit_rows[p] - 1, ((luma_row + 8) >> sy) / unit_size);
-      unit = f.lru[p][unit_row * f.lr_unit_cols[p] + item.b];
-      type = unit.type;
+      unit_p = &f.lru[p][unit_row * f.lr_unit_cols[p] + item.b];
+      type = unit_p->type;
     }
     // the descriptor and the unit are inputs of the chain; the planes below
     // are the previous stage's output
     pdl_wait();
-    const DPlane dst = f.ref[p];
     if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
-      copy_rect(f.up[p], dst, sb, x0, geo.y0, w, h, tid);
-      continue;
-    }
-    // lr_window (postfilter.rs:765-777): a thread's loads all issue before its stores
-    const int ww = w + 6, wh = h + 6;
-    {
-      LrSrc src;
-      src.up = f.up[p].p;
-      src.cur = f.cur[p].p;
-      // superres: upscaled boundary rows; fused horizontal LF pass: the
-      // loop filter's boundary rows; else the loop-filtered plane itself
-      const DPlane lines = f.sr_on ? f.lines[p] : f.prelf[p];
-      src.lines = lines.p;
-      src.up_pitch = f.up[p].stride * sb;
-      src.cur_pitch = f.cur[p].stride * sb;
-      src.lines_pitch = lines.stride * sb;
-      src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
-      const int x = max(min(x0 + c - 3, geo.pex), 0);
-      constexpr int kWinRows = (kMaxH + 6 + kGroups - 1) / kGroups;  // 18 window rows per thread
-      constexpr int kBatch = 6;
+      // a unit without restoration passes its samples through
+      load_tile(f.up[p], sb, x0, geo.y0, w, h, F0, tid);
+    } else {
+      // the unit's coefficients wait in shared memory while the window loads
+      if (tid == 0) s_unit = *unit_p;
+      // lr_window (postfilter.rs:765-777): a thread's loads all issue before its stores
+      const int ww = w + 6, wh = h + 6;
+      {
+        LrSrc src;
+        src.up = f.up[p].p;
+        src.cur = f.cur[p].p;
+        // superres: upscaled boundary rows; fused horizontal LF pass: the
+        // loop filter's boundary rows; else the loop-filtered plane itself
+        const DPlane lines = f.sr_on ? f.lines[p] : f.prelf[p];
+        src.lines = lines.p;
+        src.up_pitch = int32_t(f.up[p].stride * sb);
+        src.cur_pitch = int32_t(f.cur[p].stride * sb);
+        src.lines_pitch = int32_t(lines.stride * sb);
+        src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
+        const int x = max(min(x0 + c - 3, geo.pex), 0);
+        constexpr int kWinRows = (kMaxH + 6 + kGroups - 1) / kGroups;  // 18 window rows per thread
+        constexpr int kBatch = 6;
 #pragma unroll
-      for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
-        int v[kBatch];
+        for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
+          int v[kBatch];
 #pragma unroll
-        for (int m = 0; m < kBatch; m++) {
-          const int r = g + kGroups * (m0 + m);
-          if (r < wh && c < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
+          for (int m = 0; m < kBatch; m++) {
+            const int r = g + kGroups * (m0 + m);
+            if (r < wh && c < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
+          }
+#pragma unroll
+          for (int m = 0; m < kBatch; m++) {
+            const int r = g + kGroups * (m0 + m);
+            if (r < wh && c < ww) win[r * kWS + c] = uint16_t(v[m]);
+          }
         }
+      }
+      __syncthreads();
+      const av1pf_lr_unit& unit = s_unit;
+      if (type == AV1PF_RESTORE_WIENER) {
+        // postfilter.rs:795-822
+        const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
+        const int offset = 1 << (bd + 7 - round0 - 1);
+        const int limit = (1 << (bd + 1 + 7 - round0)) - 1;
+        const int h0 = unit.wiener[1][0], h1 = unit.wiener[1][1], h2 = unit.wiener[1][2];
+        const int v0 = unit.wiener[0][0], v1 = unit.wiener[0][1], v2 = unit.wiener[0][2];
+        const int h3 = 128 - 2 * (h0 + h1 + h2), v3 = 128 - 2 * (v0 + v1 + v2);
+        // horizontal pass: two adjacent outputs per task from 8 window samples
+        // (four aligned 32-bit loads), packed into one 32-bit store
+        for (int k = tid; k < wh * 32; k += kThreads) {
+          const int r = k >> 5, c2 = (k & 31) * 2;
+          if (c2 >= w) continue;
+          const uint32_t* sp = reinterpret_cast<const uint32_t*>(&win[r * kWS + c2]);
+          const uint32_t q0 = sp[0], q1 = sp[1], q2 = sp[2], q3 = sp[3];
+          const int s0 = int(q0 & 0xffffu), s1 = int(q0 >> 16), s2 = int(q1 & 0xffffu), s3 = int(q1 >> 16);
+          const int s4 = int(q2 & 0xffffu), s5 = int(q2 >> 16), s6 = int(q3 & 0xffffu), s7 = int(q3 >> 16);
+          const int a0 = h0 * (s0 + s6) + h1 * (s1 + s5) + h2 * (s2 + s4) + h3 * s3;
+          const int a1 = h0 * (s1 + s7) + h1 * (s2 + s6) + h2 * (s3 + s5) + h3 * s4;
+          const int o0 = clip3(-offset, limit - offset, round2(a0, round0));
+          const int o1 = clip3(-offset, limit - offset, round2(a1, round0));
+          *reinterpret_cast<uint32_t*>(&inter[r * kWS + c2]) = uint32_t(uint16_t(o0)) | (uint32_t(uint16_t(o1)) << 16);
+        }
+        __syncthreads();
+        // vertical pass: each row group slides a 7-row window down its column
+        if (c < w) {
+          const int per = (h + kGroups - 1) / kGroups;
+          const int i0 = g * per, i1 = min(h, i0 + per);
+          if (i0 < i1) {
+            const int16_t* ip = &inter[i0 * kWS + c];
+            int t0 = ip[0], t1 = ip[kWS], t2 = ip[2 * kWS], t3 = ip[3 * kWS], t4 = ip[4 * kWS], t5 = ip[5 * kWS];
+            for (int i = i0; i < i1; i++) {
+              const int t6 = inter[(i + 6) * kWS + c];
+              const int acc = v0 * (t0 + t6) + v1 * (t1 + t5) + v2 * (t2 + t4) + v3 * t3;
+              F0[i * kMaxW + c] = clip3(0, maxv, round2(acc, round1));
+              t0 = t1;
+              t1 = t2;
+              t2 = t3;
+              t3 = t4;
+              t4 = t5;
+              t5 = t6;
+            }
+          }
+        }
+      } else {
+        // postfilter.rs:823-851 with box_filter_rect (postfilter.rs:901-991)
+        const int set = unit.sgr_set & 15;
+        const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][2];
+        if (r0) {
+          sgr_ab<0>(win, A, B, a2tab, c_sgr_params[set][1], bd, geo.y0, h, w, c, g);
+          __syncthreads();
 #pragma unroll
-        for (int m = 0; m < kBatch; m++) {
-          const int r = g + kGroups * (m0 + m);
-          if (r < wh && c < ww) win[r * kWS + c] = uint16_t(v[m]);
+          for (int m = 0; m < kRowsPerThread; m++) {
+            const int i = g + kGroups * m;
+            if (i < h && c < w) F0[i * kMaxW + c] = sgr_flt<0>(A, B, i, c, geo.y0 + i, win[(i + 3) * kWS + c + 3]);
+          }
+          __syncthreads();
+        }
+        if (r1) {
+          sgr_ab<1>(win, A, B, a2tab, c_sgr_params[set][3], bd, geo.y0, h, w, c, g);
+          __syncthreads();
+        }
+        const int w0 = unit.sgr_xqd[0], w1 = unit.sgr_xqd[1];
+        const int w2 = (1 << 7) - w0 - w1;
+#pragma unroll
+        for (int m = 0; m < kRowsPerThread; m++) {
+          const int i = g + kGroups * m;
+          if (i < h && c < w) {
+            const int cd = win[(i + 3) * kWS + c + 3];
+            const int u = cd << 4;
+            int v = w1 * u;
+            v += r0 != 0 ? w0 * F0[i * kMaxW + c] : w0 * u;
+            v += r1 != 0 ? w2 * sgr_flt<1>(A, B, i, c, geo.y0 + i, cd) : w2 * u;
+            F0[i * kMaxW + c] = clip3(0, maxv, round2(v, 11));  // this thread's own slot
+          }
         }
       }
     }
     __syncthreads();
-    if (type == AV1PF_RESTORE_WIENER) {
-      // postfilter.rs:795-822
-      const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
-      const int offset = 1 << (bd + 7 - round0 - 1);
-      const int limit = (1 << (bd + 1 + 7 - round0)) - 1;
-      const int h0 = unit.wiener[1][0], h1 = unit.wiener[1][1], h2 = unit.wiener[1][2];
-      const int v0 = unit.wiener[0][0], v1 = unit.wiener[0][1], v2 = unit.wiener[0][2];
-      const int h3 = 128 - 2 * (h0 + h1 + h2), v3 = 128 - 2 * (v0 + v1 + v2);
-      // horizontal pass: two adjacent outputs per task from 8 window samples
-      // (four aligned 32-bit loads), packed into one 32-bit store
-      for (int k = tid; k < wh * 32; k += kThreads) {
-        const int r = k >> 5, c2 = (k & 31) * 2;
-        if (c2 >= w) continue;
-        const uint32_t* sp = reinterpret_cast<const uint32_t*>(&win[r * kWS + c2]);
-        const uint32_t q0 = sp[0], q1 = sp[1], q2 = sp[2], q3 = sp[3];
-        const int s0 = int(q0 & 0xffffu), s1 = int(q0 >> 16), s2 = int(q1 & 0xffffu), s3 = int(q1 >> 16);
-        const int s4 = int(q2 & 0xffffu), s5 = int(q2 >> 16), s6 = int(q3 & 0xffffu), s7 = int(q3 >> 16);
-        const int a0 = h0 * (s0 + s6) + h1 * (s1 + s5) + h2 * (s2 + s4) + h3 * s3;
-        const int a1 = h0 * (s1 + s7) + h1 * (s2 + s6) + h2 * (s3 + s5) + h3 * s4;
-        const int o0 = clip3(-offset, limit - offset, round2(a0, round0));
-        const int o1 = clip3(-offset, limit - offset, round2(a1, round0));
-        *reinterpret_cast<uint32_t*>(&inter[r * kWS + c2]) = uint32_t(uint16_t(o0)) | (uint32_t(uint16_t(o1)) << 16);
-      }
-      __syncthreads();
-      // vertical pass: each row group slides a 7-row window down its column
-      if (c < w) {
-        const int per = (h + kGroups - 1) / kGroups;
-        const int i0 = g * per, i1 = min(h, i0 + per);
-        if (i0 < i1) {
-          const int16_t* ip = &inter[i0 * kWS + c];
-          int t0 = ip[0], t1 = ip[kWS], t2 = ip[2 * kWS], t3 = ip[3 * kWS], t4 = ip[4 * kWS], t5 = ip[5 * kWS];
-          for (int i = i0; i < i1; i++) {
-            const int t6 = inter[(i + 6) * kWS + c];
-            const int acc = v0 * (t0 + t6) + v1 * (t1 + t5) + v2 * (t2 + t4) + v3 * t3;
-            st_sample(dst, sb, x0 + c, geo.y0 + i, clip3(0, maxv, round2(acc, round1)));
-            t0 = t1;
-            t1 = t2;
-            t2 = t3;
-            t3 = t4;
-            t4 = t5;
-            t5 = t6;
-          }
-        }
-      }
-    } else {
-      // postfilter.rs:823-851 with box_filter_rect (postfilter.rs:901-991)
-      const int set = unit.sgr_set & 15;
-      const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][2];
-      if (r0) {
-        sgr_ab<0>(win, A, B, a2tab, c_sgr_params[set][1], bd, geo.y0, h, w, c, g);
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < kRowsPerThread; m++) {
-          const int i = g + kGroups * m;
-          if (i < h && c < w) F0[i * kMaxW + c] = sgr_flt<0>(A, B, i, c, geo.y0 + i, win[(i + 3) * kWS + c + 3]);
-        }
-        __syncthreads();
-      }
-      if (r1) {
-        sgr_ab<1>(win, A, B, a2tab, c_sgr_params[set][3], bd, geo.y0, h, w, c, g);
-        __syncthreads();
-      }
-      const int w0 = unit.sgr_xqd[0], w1 = unit.sgr_xqd[1];
-      const int w2 = (1 << 7) - w0 - w1;
-#pragma unroll
-      for (int m = 0; m < kRowsPerThread; m++) {
-        const int i = g + kGroups * m;
-        if (i < h && c < w) {
-          const int cd = win[(i + 3) * kWS + c + 3];
-          const int u = cd << 4;
-          int v = w1 * u;
-          v += r0 != 0 ? w0 * F0[i * kMaxW + c] : w0 * u;
-          v += r1 != 0 ? w2 * sgr_flt<1>(A, B, i, c, geo.y0 + i, cd) : w2 * u;
-          st_sample(dst, sb, x0 + c, geo.y0 + i, clip3(0, maxv, round2(v, 11)));
-        }
+    // the rectangle's output samples, from shared memory to the reference
+    // frame and (frames without film grain) the packed frame: u8 samples at
+    // 8 bits, little-endian u16 above (frame.rs:153-158), rows of the plane's
+    // width (decoder/mod.rs:846-917)
+    {
+      const DPlane dst = f.ref[p];
+      uint8_t* d0 = dst.p + (int64_t(geo.y0) * dst.stride + x0) * sb;
+      const int64_t dp = dst.stride * sb;
+      store_tile(F0, d0, dp, sb, ((reinterpret_cast<uintptr_t>(d0) | uintptr_t(dp)) & 15) == 0, w, h, tid);
+      if (f.lr_pack) {
+        const int bps = bd > 8 ? 2 : 1;
+        const int64_t op = int64_t(geo.pex + 1) * bps;
+        uint8_t* o0 = f.frame_out + f.out_off[p] + int64_t(geo.y0) * op + int64_t(x0) * bps;
+        store_tile(F0, o0, op, bps, ((reinterpret_cast<uintptr_t>(o0) | uintptr_t(op)) & 15) == 0, w, h, tid);
       }
     }
     __syncthreads();

@@ -404,10 +404,12 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     }
     // --- output: decoder/mod.rs:846-917 ---
     if ((j.stages & ST_OUT) && j.frame_out) {
-      plan.any_out = true;
       if (!chain)
         for (int k = 0; k < np; k++) d.ref[k] = from_abi(j.in[k]);
       d.frame_out = j.frame_out;
+      // a whole chain without film grain packs inside the loop-restoration
+      // kernel, which writes every visible sample of the reference frame
+      d.lr_pack = chain && !p->film_grain.apply ? 1 : 0;
       const int64_t bps = i->bit_depth > 8 ? 2 : 1;
       int64_t off = 0;
       for (int k = 0; k < np; k++) {
@@ -415,7 +417,10 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         const int pw = plane_w(i, k, i->upscaled_width), ph = plane_h(i, k);
         off += int64_t(pw) * ph * bps;
         // 256 columns by one noise stripe (32 rows, 16 in vertically subsampled chroma)
-        add_tiles(plan.out_items, fi, k, 0, pw, ph, 256, k ? 32 >> i->subsampling_y : 32);
+        if (!d.lr_pack) {
+          plan.any_out = true;
+          add_tiles(plan.out_items, fi, k, 0, pw, ph, 256, k ? 32 >> i->subsampling_y : 32);
+        }
       }
       if (p->film_grain.apply) {
         plan.any_grain = true;
