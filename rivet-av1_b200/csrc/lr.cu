@@ -6,15 +6,18 @@
 //
 // One CTA restores one rectangle: the rows of one stripe (64 luma rows,
 // offset by 8) and up to 64 columns of one restoration unit. 288 threads are
-// 4 row groups x 72 columns, so every thread owns a column and no loop
+// 4 row groups x 72 columns (8 x 36 for rectangles of up to 32 columns, as
+// 4:2:0 chroma units are), so every thread owns a column and no loop
 // divides by a runtime width. The window the rectangle reads (3-sample
 // border, the stripe-boundary rule of LrCtx::sample) is staged in shared
 // memory with one row-uniform source choice per row. Wiener runs its
 // horizontal pass into an int16 intermediate, then the vertical pass. The
 // self-guided filter slides each column's box sums down its rows (one new
-// and one old row of horizontal sums per step), which is exact in 32 bits for
-// <= 12-bit samples (25 * 4095^2 < 2^31); the products the reference forms in
-// 64 bits (p * s and the B term) are 32x32->64 multiplies here. Rectangles of
+// and one old row of horizontal sums per step), then walks each column's
+// output rows with three rows of A and B in registers. The sums are exact in
+// 32 bits for <= 12-bit samples (25 * 4095^2 < 2^31); the products the
+// reference forms in 64 bits (p * s and the B term) are 32x32->64 multiplies
+// here. Rectangles of
 // units without restoration (and planes or frames without it) pass their
 // samples through, so the kernel writes the whole visible area of the
 // reference frame. Every rectangle's output gathers in a shared-memory tile
@@ -28,8 +31,6 @@ namespace av1pf {
 
 namespace {
 constexpr int kThreads = 288;
-constexpr int kCols = 72;                // threads per row group
-constexpr int kGroups = kThreads / kCols;  // 4
 constexpr int kMaxW = 64;                // columns per rectangle
 constexpr int kMaxH = 64;                // rows per stripe
 constexpr int kWS = 72;                  // window row stride (u16): w + 6 <= 70
@@ -38,7 +39,6 @@ constexpr int kWinBytes = (kMaxH + 6) * kWS * 2;
 constexpr int kABytes = (kMaxH + 2) * kAS * 4;
 constexpr int kF0Bytes = kMaxH * kMaxW * 4;  // the first self-guided filter's output
 constexpr int kSmemBytes = kWinBytes + 2 * kABytes + 256 * 4 + kF0Bytes;
-constexpr int kRowsPerThread = kMaxH / kGroups;  // 16
 static_assert((kMaxH + 6) * kWS * 2 <= kABytes, "Wiener intermediate must fit the A area");
 }  // namespace
 
@@ -83,15 +83,17 @@ __device__ __forceinline__ int ld_row(const uint8_t* row, int sb, int x) {
 
 // Reads the w x h samples at (x0, y0) of `src` (sample width sb) into `tile`
 // (int32, row stride kMaxW): 16-byte chunks where the rows allow them, else
-// single samples.
+// single samples. Rows hold MW >> cs chunk slots (w <= MW).
+template <int MW>
 __device__ __forceinline__ void load_tile(const DPlane& src, int sb, int x0, int y0, int w, int h, int32_t* tile,
                                           int tid) {
   const uint8_t* s0 = src.p + (int64_t(y0) * src.stride + x0) * sb;
   const int64_t sp = src.stride * sb;
   const bool vec = ((reinterpret_cast<uintptr_t>(s0) | uintptr_t(sp)) & 15) == 0;
-  const int cs = sb == 2 ? 3 : 4;  // log2 samples per chunk
-  for (int k = tid; k < h * 8; k += kThreads) {
-    const int r = k >> 3, e0 = (k & 7) << cs;
+  const int cs = sb == 2 ? 3 : 4;                  // log2 samples per chunk
+  const int ls = (MW == 64 ? 6 : 5) - cs;          // log2 chunk slots per row
+  for (int k = tid; k < (h << ls); k += kThreads) {
+    const int r = k >> ls, e0 = (k & ((1 << ls) - 1)) << cs;
     if (e0 >= w) continue;
     const uint8_t* row = s0 + int64_t(r) * sp;
     int32_t* t = tile + r * kMaxW + e0;
@@ -116,12 +118,14 @@ __device__ __forceinline__ void load_tile(const DPlane& src, int sb, int x0, int
 // Writes the w x h output samples of `tile` (int32, row stride kMaxW) to
 // rows of `width`-byte samples from `base`, `pitch` bytes apart: 16-byte
 // chunks (8 or 16 samples) where `vec` says the rows allow them, else single
-// samples.
+// samples. Rows hold MW >> cs chunk slots (w <= MW).
+template <int MW>
 __device__ __forceinline__ void store_tile(const int32_t* tile, uint8_t* base, int64_t pitch, int width, bool vec,
                                            int w, int h, int tid) {
-  const int cs = width == 2 ? 3 : 4;  // log2 samples per chunk
-  for (int k = tid; k < h * 8; k += kThreads) {
-    const int r = k >> 3, e0 = (k & 7) << cs;
+  const int cs = width == 2 ? 3 : 4;      // log2 samples per chunk
+  const int ls = (MW == 64 ? 6 : 5) - cs;  // log2 chunk slots per row
+  for (int k = tid; k < (h << ls); k += kThreads) {
+    const int r = k >> ls, e0 = (k & ((1 << ls) - 1)) << cs;
     if (e0 >= w) continue;
     const int32_t* t = tile + r * kMaxW + e0;
     uint8_t* row = base + int64_t(r) * pitch;
@@ -155,9 +159,10 @@ __device__ __forceinline__ void store_tile(const int32_t* tile, uint8_t* base, i
 }
 
 // Box sums of radius R over the window and the A / B of box_filter_rect
-// (postfilter.rs:935-959) for positions (i, j), i in [0, h+2), j = column.
-// Each row group owns a contiguous run of rows and slides down it.
-template <int PASS>
+// (postfilter.rs:935-959) for positions (i, j), i in [0, h+2), j = c - 1,
+// stored at [i][c]. Each of the G row groups owns a contiguous run of rows
+// and slides down it.
+template <int PASS, int G>
 __device__ __forceinline__ void sgr_ab(const uint16_t* win, int32_t* A, int32_t* B, const int32_t* a2tab, int eps,
                                        int bd, int y0, int h, int w, int c, int g) {
   constexpr int R = PASS == 0 ? 2 : 1;  // SGR_PARAMS radii: first 0 or 2, second 0 or 1
@@ -167,7 +172,7 @@ __device__ __forceinline__ void sgr_ab(const uint16_t* win, int32_t* A, int32_t*
   constexpr int one_over_n = ((1 << 12) + n / 2) / n;
   if (c >= w + 2) return;
   const int rows = h + 2;
-  const int rpg = (rows + kGroups - 1) / kGroups;
+  const int rpg = (rows + G - 1) / G;
   const int i0 = g * rpg, i1 = min(i0 + rpg, rows);
   if (i0 >= i1) return;
   // horizontal sums of window row wr around column c + 2
@@ -222,50 +227,226 @@ __device__ __forceinline__ void sgr_ab(const uint16_t* win, int32_t* A, int32_t*
   }
 }
 
-// The filtered value of pixel (i, j) from A and B (postfilter.rs:960-989).
-template <int PASS>
-__device__ __forceinline__ int sgr_flt(const int32_t* A, const int32_t* B, int i, int j, int yabs, int cdef) {
-  const int32_t* Ar = &A[(i + 1) * kAS + j + 1];
-  const int32_t* Br = &B[(i + 1) * kAS + j + 1];
-  int a, b, shift;
-  if (PASS == 0) {
-    if (yabs & 1) {
-      a = 6 * Ar[0] + 5 * (Ar[-1] + Ar[1]);
-      b = 6 * Br[0] + 5 * (Br[-1] + Br[1]);
-      shift = 4;
+// The self-guided filter's value at rows [i0, i1) of column c
+// (postfilter.rs:960-989), handed to emit(i, window sample, value). The walk
+// down the column keeps the three A and B rows around row i in registers,
+// each as its centre value and the sum of its left and right neighbours, so
+// a row costs three loads of A and three of B.
+template <int PASS, typename Emit>
+__device__ __forceinline__ void sgr_flt_col(const int32_t* A, const int32_t* B, const uint16_t* win, int c, int i0,
+                                            int i1, int y0, Emit emit) {
+  const int32_t* pa = A + c + 1;
+  const int32_t* pb = B + c + 1;
+  auto row = [&](const int32_t* q, int& m, int& sum) {
+    m = q[0];
+    sum = q[-1] + q[1];
+  };
+  int am0, as0, am1, as1, bm0, bs0, bm1, bs1;
+  row(pa + i0 * kAS, am0, as0);
+  row(pb + i0 * kAS, bm0, bs0);
+  row(pa + (i0 + 1) * kAS, am1, as1);
+  row(pb + (i0 + 1) * kAS, bm1, bs1);
+  for (int i = i0; i < i1; i++) {
+    int am2, as2, bm2, bs2;
+    row(pa + (i + 2) * kAS, am2, as2);
+    row(pb + (i + 2) * kAS, bm2, bs2);
+    const int cd = win[(i + 3) * kWS + c + 3];
+    int a, b, shift;
+    if (PASS == 0) {
+      if ((y0 + i) & 1) {
+        a = 6 * am1 + 5 * as1;
+        b = 6 * bm1 + 5 * bs1;
+        shift = 4;
+      } else {
+        a = 6 * (am0 + am2) + 5 * (as0 + as2);
+        b = 6 * (bm0 + bm2) + 5 * (bs0 + bs2);
+        shift = 5;
+      }
     } else {
-      const int32_t* Au = Ar - kAS;
-      const int32_t* Ad = Ar + kAS;
-      const int32_t* Bu = Br - kAS;
-      const int32_t* Bd = Br + kAS;
-      a = 6 * (Au[0] + Ad[0]) + 5 * (Au[-1] + Au[1] + Ad[-1] + Ad[1]);
-      b = 6 * (Bu[0] + Bd[0]) + 5 * (Bu[-1] + Bu[1] + Bd[-1] + Bd[1]);
+      a = 4 * (am1 + as1 + am0 + am2) + 3 * (as0 + as2);
+      b = 4 * (bm1 + bs1 + bm0 + bm2) + 3 * (bs0 + bs2);
       shift = 5;
     }
-  } else {
-    const int32_t* Au = Ar - kAS;
-    const int32_t* Ad = Ar + kAS;
-    const int32_t* Bu = Br - kAS;
-    const int32_t* Bd = Br + kAS;
-    a = 4 * (Ar[0] + Ar[-1] + Ar[1] + Au[0] + Ad[0]) + 3 * (Au[-1] + Au[1] + Ad[-1] + Ad[1]);
-    b = 4 * (Br[0] + Br[-1] + Br[1] + Bu[0] + Bd[0]) + 3 * (Bu[-1] + Bu[1] + Bd[-1] + Bd[1]);
-    shift = 5;
+    emit(i, cd, round2(a * cd + b, 8 + shift - 4));
+    am0 = am1;
+    as0 = as1;
+    bm0 = bm1;
+    bs0 = bs1;
+    am1 = am2;
+    as1 = as2;
+    bm1 = bm2;
+    bs1 = bs2;
   }
-  return round2(a * cdef + b, 8 + shift - 4);
+}
+
+// The shared-memory areas of one CTA.
+struct LrSmem {
+  uint16_t* win;    // the window, rows kWS apart
+  int32_t* A;       // self-guided A (Wiener: the int16 intermediate)
+  int32_t* B;       // self-guided B
+  const int32_t* a2tab;
+  int32_t* F0;      // first self-guided output, then every rectangle's output
+  av1pf_lr_unit* unit;
+};
+
+// Restores one rectangle of w <= MW columns into the output tile. CW is the
+// width of a row group (threads per group: 72 for rectangles up to 64
+// columns, 36 for those up to 32, so narrow rectangles keep most threads
+// busy); the window is staged by groups SW threads wide.
+template <int CW>
+__device__ __forceinline__ void restore_rect(const FrameDesc& f, const LrSmem& sm, const LrGeom& geo, int p, int s,
+                                             int x0, int w, int h, int type, const av1pf_lr_unit* unit_p, int tid) {
+  constexpr int G = kThreads / CW;          // row groups
+  constexpr int MW = CW == 72 ? 64 : 32;    // widest rectangle
+  constexpr int SW = CW == 72 ? 72 : 48;    // staging group width (>= MW + 6)
+  constexpr int SG = kThreads / SW;         // staging groups
+  static_assert(G * CW == kThreads && SG * SW == kThreads, "layouts cover the CTA");
+  const int g = tid / CW, c = tid - g * CW;
+  const int sb = f.sb, bd = f.bd;
+  const int maxv = (1 << bd) - 1;
+  int32_t* F0 = sm.F0;
+  if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
+    // a unit without restoration passes its samples through
+    load_tile<MW>(f.up[p], sb, x0, geo.y0, w, h, F0, tid);
+    return;
+  }
+  uint16_t* win = sm.win;
+  // the unit's coefficients wait in shared memory while the window loads
+  if (tid == 0) *sm.unit = *unit_p;
+  // lr_window (postfilter.rs:765-777): a thread's loads all issue before its stores
+  const int ww = w + 6, wh = h + 6;
+  {
+    LrSrc src;
+    src.up = f.up[p].p;
+    src.cur = f.cur[p].p;
+    // superres: upscaled boundary rows; fused horizontal LF pass: the
+    // loop filter's boundary rows; else the loop-filtered plane itself
+    const DPlane lines = f.sr_on ? f.lines[p] : f.prelf[p];
+    src.lines = lines.p;
+    src.up_pitch = int32_t(f.up[p].stride * sb);
+    src.cur_pitch = int32_t(f.cur[p].stride * sb);
+    src.lines_pitch = int32_t(lines.stride * sb);
+    src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
+    const int sg = tid / SW, sc = tid - sg * SW;
+    const int x = max(min(x0 + sc - 3, geo.pex), 0);
+    constexpr int kWinRows = (kMaxH + 6 + SG - 1) / SG;  // window rows per thread
+    constexpr int kBatch = (kWinRows + 1) / 2;               // loads in flight per thread
+#pragma unroll
+    for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
+      int v[kBatch];
+#pragma unroll
+      for (int m = 0; m < kBatch; m++) {
+        const int r = sg + SG * (m0 + m);
+        if (r < wh && sc < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
+      }
+#pragma unroll
+      for (int m = 0; m < kBatch; m++) {
+        const int r = sg + SG * (m0 + m);
+        if (r < wh && sc < ww) win[r * kWS + sc] = uint16_t(v[m]);
+      }
+    }
+  }
+  __syncthreads();
+  const av1pf_lr_unit& unit = *sm.unit;
+  // each row group's contiguous run of output rows
+  const int per = (h + G - 1) / G;
+  const int i0 = g * per, i1 = min(h, i0 + per);
+  const bool col = c < w && i0 < i1;
+  if (type == AV1PF_RESTORE_WIENER) {
+    // postfilter.rs:795-822
+    int16_t* inter = reinterpret_cast<int16_t*>(sm.A);
+    const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
+    const int offset = 1 << (bd + 7 - round0 - 1);
+    const int limit = (1 << (bd + 1 + 7 - round0)) - 1;
+    const int h0 = unit.wiener[1][0], h1 = unit.wiener[1][1], h2 = unit.wiener[1][2];
+    const int v0 = unit.wiener[0][0], v1 = unit.wiener[0][1], v2 = unit.wiener[0][2];
+    const int h3 = 128 - 2 * (h0 + h1 + h2), v3 = 128 - 2 * (v0 + v1 + v2);
+    // horizontal pass: two adjacent outputs per task from 8 window samples
+    // (four aligned 32-bit loads), packed into one 32-bit store
+    constexpr int LP = MW == 64 ? 5 : 4;  // log2 column pairs per row
+    for (int k = tid; k < (wh << LP); k += kThreads) {
+      const int r = k >> LP, c2 = (k & ((1 << LP) - 1)) * 2;
+      if (c2 >= w) continue;
+      const uint32_t* sp = reinterpret_cast<const uint32_t*>(&win[r * kWS + c2]);
+      const uint32_t q0 = sp[0], q1 = sp[1], q2 = sp[2], q3 = sp[3];
+      const int s0 = int(q0 & 0xffffu), s1 = int(q0 >> 16), s2 = int(q1 & 0xffffu), s3 = int(q1 >> 16);
+      const int s4 = int(q2 & 0xffffu), s5 = int(q2 >> 16), s6 = int(q3 & 0xffffu), s7 = int(q3 >> 16);
+      const int a0 = h0 * (s0 + s6) + h1 * (s1 + s5) + h2 * (s2 + s4) + h3 * s3;
+      const int a1 = h0 * (s1 + s7) + h1 * (s2 + s6) + h2 * (s3 + s5) + h3 * s4;
+      const int o0 = clip3(-offset, limit - offset, round2(a0, round0));
+      const int o1 = clip3(-offset, limit - offset, round2(a1, round0));
+      *reinterpret_cast<uint32_t*>(&inter[r * kWS + c2]) = uint32_t(uint16_t(o0)) | (uint32_t(uint16_t(o1)) << 16);
+    }
+    __syncthreads();
+    // vertical pass: each row group slides a 7-row window down its column
+    if (col) {
+      const int16_t* ip = &inter[i0 * kWS + c];
+      int t0 = ip[0], t1 = ip[kWS], t2 = ip[2 * kWS], t3 = ip[3 * kWS], t4 = ip[4 * kWS], t5 = ip[5 * kWS];
+      for (int i = i0; i < i1; i++) {
+        const int t6 = inter[(i + 6) * kWS + c];
+        const int acc = v0 * (t0 + t6) + v1 * (t1 + t5) + v2 * (t2 + t4) + v3 * t3;
+        F0[i * kMaxW + c] = clip3(0, maxv, round2(acc, round1));
+        t0 = t1;
+        t1 = t2;
+        t2 = t3;
+        t3 = t4;
+        t4 = t5;
+        t5 = t6;
+      }
+    }
+    return;
+  }
+  // postfilter.rs:823-851 with box_filter_rect (postfilter.rs:901-991)
+  int32_t* A = sm.A;
+  int32_t* B = sm.B;
+  const int set = unit.sgr_set & 15;
+  const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][2];
+  if (r0) {
+    sgr_ab<0, G>(win, A, B, sm.a2tab, c_sgr_params[set][1], bd, geo.y0, h, w, c, g);
+    __syncthreads();
+    if (col) sgr_flt_col<0>(A, B, win, c, i0, i1, geo.y0, [&](int i, int, int v) { F0[i * kMaxW + c] = v; });
+    __syncthreads();
+  }
+  if (r1) {
+    sgr_ab<1, G>(win, A, B, sm.a2tab, c_sgr_params[set][3], bd, geo.y0, h, w, c, g);
+    __syncthreads();
+  }
+  const int w0 = unit.sgr_xqd[0], w1 = unit.sgr_xqd[1];
+  const int w2 = (1 << 7) - w0 - w1;
+  if (col) {
+    // the weighted sum of the two filters and the sample itself; this
+    // thread's own slot of the output tile
+    auto combine = [&](int i, int cd, int flt1) {
+      const int u = cd << 4;
+      int v = w1 * u;
+      v += r0 != 0 ? w0 * F0[i * kMaxW + c] : w0 * u;
+      v += w2 * flt1;
+      F0[i * kMaxW + c] = clip3(0, maxv, round2(v, 11));
+    };
+    if (r1) {
+      sgr_flt_col<1>(A, B, win, c, i0, i1, geo.y0, combine);
+    } else {
+      for (int i = i0; i < i1; i++) {
+        const int cd = win[(i + 3) * kWS + c + 3];
+        combine(i, cd, cd << 4);
+      }
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __restrict__ frames,
                                                          const Item* __restrict__ items, int n_items) {
   extern __shared__ __align__(16) uint8_t smem[];
-  uint16_t* win = reinterpret_cast<uint16_t*>(smem);
-  int32_t* A = reinterpret_cast<int32_t*>(smem + kWinBytes);
-  int32_t* B = reinterpret_cast<int32_t*>(smem + kWinBytes + kABytes);
-  int32_t* a2tab = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
-  int32_t* F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes + 256 * 4);
   __shared__ av1pf_lr_unit s_unit;
-  int16_t* inter = reinterpret_cast<int16_t*>(A);  // Wiener reuses the A area
+  LrSmem sm;
+  sm.win = reinterpret_cast<uint16_t*>(smem);
+  sm.A = reinterpret_cast<int32_t*>(smem + kWinBytes);
+  sm.B = reinterpret_cast<int32_t*>(smem + kWinBytes + kABytes);
+  int32_t* a2tab = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
+  sm.a2tab = a2tab;
+  sm.F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes + 256 * 4);
+  sm.unit = &s_unit;
   const int tid = threadIdx.x;
-  const int g = tid / kCols, c = tid - g * kCols;
   // SGR_A2 (postfilter.rs:884-898)
   for (int z = tid; z < 256; z += kThreads) a2tab[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
   __syncthreads();
@@ -275,8 +456,6 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     const FrameDesc& f = frames[item.frame];
     const int p = item.plane;
     const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-    const int sb = f.sb, bd = f.bd;
-    const int maxv = (1 << bd) - 1;
     // lr_stripe (postfilter.rs:640-661)
     LrGeom geo;
     const int s = item.a;
@@ -304,139 +483,31 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     // the descriptor and the unit are inputs of the chain; the planes below
     // are the previous stage's output
     pdl_wait();
-    if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
-      // a unit without restoration passes its samples through
-      load_tile(f.up[p], sb, x0, geo.y0, w, h, F0, tid);
-    } else {
-      // the unit's coefficients wait in shared memory while the window loads
-      if (tid == 0) s_unit = *unit_p;
-      // lr_window (postfilter.rs:765-777): a thread's loads all issue before its stores
-      const int ww = w + 6, wh = h + 6;
-      {
-        LrSrc src;
-        src.up = f.up[p].p;
-        src.cur = f.cur[p].p;
-        // superres: upscaled boundary rows; fused horizontal LF pass: the
-        // loop filter's boundary rows; else the loop-filtered plane itself
-        const DPlane lines = f.sr_on ? f.lines[p] : f.prelf[p];
-        src.lines = lines.p;
-        src.up_pitch = int32_t(f.up[p].stride * sb);
-        src.cur_pitch = int32_t(f.cur[p].stride * sb);
-        src.lines_pitch = int32_t(lines.stride * sb);
-        src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
-        const int x = max(min(x0 + c - 3, geo.pex), 0);
-        constexpr int kWinRows = (kMaxH + 6 + kGroups - 1) / kGroups;  // 18 window rows per thread
-        constexpr int kBatch = 6;
-#pragma unroll
-        for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
-          int v[kBatch];
-#pragma unroll
-          for (int m = 0; m < kBatch; m++) {
-            const int r = g + kGroups * (m0 + m);
-            if (r < wh && c < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
-          }
-#pragma unroll
-          for (int m = 0; m < kBatch; m++) {
-            const int r = g + kGroups * (m0 + m);
-            if (r < wh && c < ww) win[r * kWS + c] = uint16_t(v[m]);
-          }
-        }
-      }
-      __syncthreads();
-      const av1pf_lr_unit& unit = s_unit;
-      if (type == AV1PF_RESTORE_WIENER) {
-        // postfilter.rs:795-822
-        const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
-        const int offset = 1 << (bd + 7 - round0 - 1);
-        const int limit = (1 << (bd + 1 + 7 - round0)) - 1;
-        const int h0 = unit.wiener[1][0], h1 = unit.wiener[1][1], h2 = unit.wiener[1][2];
-        const int v0 = unit.wiener[0][0], v1 = unit.wiener[0][1], v2 = unit.wiener[0][2];
-        const int h3 = 128 - 2 * (h0 + h1 + h2), v3 = 128 - 2 * (v0 + v1 + v2);
-        // horizontal pass: two adjacent outputs per task from 8 window samples
-        // (four aligned 32-bit loads), packed into one 32-bit store
-        for (int k = tid; k < wh * 32; k += kThreads) {
-          const int r = k >> 5, c2 = (k & 31) * 2;
-          if (c2 >= w) continue;
-          const uint32_t* sp = reinterpret_cast<const uint32_t*>(&win[r * kWS + c2]);
-          const uint32_t q0 = sp[0], q1 = sp[1], q2 = sp[2], q3 = sp[3];
-          const int s0 = int(q0 & 0xffffu), s1 = int(q0 >> 16), s2 = int(q1 & 0xffffu), s3 = int(q1 >> 16);
-          const int s4 = int(q2 & 0xffffu), s5 = int(q2 >> 16), s6 = int(q3 & 0xffffu), s7 = int(q3 >> 16);
-          const int a0 = h0 * (s0 + s6) + h1 * (s1 + s5) + h2 * (s2 + s4) + h3 * s3;
-          const int a1 = h0 * (s1 + s7) + h1 * (s2 + s6) + h2 * (s3 + s5) + h3 * s4;
-          const int o0 = clip3(-offset, limit - offset, round2(a0, round0));
-          const int o1 = clip3(-offset, limit - offset, round2(a1, round0));
-          *reinterpret_cast<uint32_t*>(&inter[r * kWS + c2]) = uint32_t(uint16_t(o0)) | (uint32_t(uint16_t(o1)) << 16);
-        }
-        __syncthreads();
-        // vertical pass: each row group slides a 7-row window down its column
-        if (c < w) {
-          const int per = (h + kGroups - 1) / kGroups;
-          const int i0 = g * per, i1 = min(h, i0 + per);
-          if (i0 < i1) {
-            const int16_t* ip = &inter[i0 * kWS + c];
-            int t0 = ip[0], t1 = ip[kWS], t2 = ip[2 * kWS], t3 = ip[3 * kWS], t4 = ip[4 * kWS], t5 = ip[5 * kWS];
-            for (int i = i0; i < i1; i++) {
-              const int t6 = inter[(i + 6) * kWS + c];
-              const int acc = v0 * (t0 + t6) + v1 * (t1 + t5) + v2 * (t2 + t4) + v3 * t3;
-              F0[i * kMaxW + c] = clip3(0, maxv, round2(acc, round1));
-              t0 = t1;
-              t1 = t2;
-              t2 = t3;
-              t3 = t4;
-              t4 = t5;
-              t5 = t6;
-            }
-          }
-        }
-      } else {
-        // postfilter.rs:823-851 with box_filter_rect (postfilter.rs:901-991)
-        const int set = unit.sgr_set & 15;
-        const int r0 = c_sgr_params[set][0], r1 = c_sgr_params[set][2];
-        if (r0) {
-          sgr_ab<0>(win, A, B, a2tab, c_sgr_params[set][1], bd, geo.y0, h, w, c, g);
-          __syncthreads();
-#pragma unroll
-          for (int m = 0; m < kRowsPerThread; m++) {
-            const int i = g + kGroups * m;
-            if (i < h && c < w) F0[i * kMaxW + c] = sgr_flt<0>(A, B, i, c, geo.y0 + i, win[(i + 3) * kWS + c + 3]);
-          }
-          __syncthreads();
-        }
-        if (r1) {
-          sgr_ab<1>(win, A, B, a2tab, c_sgr_params[set][3], bd, geo.y0, h, w, c, g);
-          __syncthreads();
-        }
-        const int w0 = unit.sgr_xqd[0], w1 = unit.sgr_xqd[1];
-        const int w2 = (1 << 7) - w0 - w1;
-#pragma unroll
-        for (int m = 0; m < kRowsPerThread; m++) {
-          const int i = g + kGroups * m;
-          if (i < h && c < w) {
-            const int cd = win[(i + 3) * kWS + c + 3];
-            const int u = cd << 4;
-            int v = w1 * u;
-            v += r0 != 0 ? w0 * F0[i * kMaxW + c] : w0 * u;
-            v += r1 != 0 ? w2 * sgr_flt<1>(A, B, i, c, geo.y0 + i, cd) : w2 * u;
-            F0[i * kMaxW + c] = clip3(0, maxv, round2(v, 11));  // this thread's own slot
-          }
-        }
-      }
-    }
+    if (w > 32)
+      restore_rect<72>(f, sm, geo, p, s, x0, w, h, type, unit_p, tid);
+    else
+      restore_rect<36>(f, sm, geo, p, s, x0, w, h, type, unit_p, tid);
     __syncthreads();
     // the rectangle's output samples, from shared memory to the reference
     // frame and (frames without film grain) the packed frame: u8 samples at
     // 8 bits, little-endian u16 above (frame.rs:153-158), rows of the plane's
     // width (decoder/mod.rs:846-917)
     {
+      const int sb = f.sb, bd = f.bd;
       const DPlane dst = f.ref[p];
       uint8_t* d0 = dst.p + (int64_t(geo.y0) * dst.stride + x0) * sb;
       const int64_t dp = dst.stride * sb;
-      store_tile(F0, d0, dp, sb, ((reinterpret_cast<uintptr_t>(d0) | uintptr_t(dp)) & 15) == 0, w, h, tid);
-      if (f.lr_pack) {
-        const int bps = bd > 8 ? 2 : 1;
-        const int64_t op = int64_t(geo.pex + 1) * bps;
-        uint8_t* o0 = f.frame_out + f.out_off[p] + int64_t(geo.y0) * op + int64_t(x0) * bps;
-        store_tile(F0, o0, op, bps, ((reinterpret_cast<uintptr_t>(o0) | uintptr_t(op)) & 15) == 0, w, h, tid);
+      const bool d_vec = ((reinterpret_cast<uintptr_t>(d0) | uintptr_t(dp)) & 15) == 0;
+      const int bps = bd > 8 ? 2 : 1;
+      const int64_t op = int64_t(geo.pex + 1) * bps;
+      uint8_t* o0 = f.lr_pack ? f.frame_out + f.out_off[p] + int64_t(geo.y0) * op + int64_t(x0) * bps : nullptr;
+      const bool o_vec = ((reinterpret_cast<uintptr_t>(o0) | uintptr_t(op)) & 15) == 0;
+      if (w > 32) {
+        store_tile<64>(sm.F0, d0, dp, sb, d_vec, w, h, tid);
+        if (o0) store_tile<64>(sm.F0, o0, op, bps, o_vec, w, h, tid);
+      } else {
+        store_tile<32>(sm.F0, d0, dp, sb, d_vec, w, h, tid);
+        if (o0) store_tile<32>(sm.F0, o0, op, bps, o_vec, w, h, tid);
       }
     }
     __syncthreads();
