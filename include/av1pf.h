@@ -299,6 +299,26 @@ int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info,
                      const av1pf_plane* in, av1pf_plane* ref_out,
                      uint8_t* frame_out);
 
+/* One frame of av1pf_chain_host_many: the arguments of av1pf_chain_host. */
+typedef struct av1pf_host_job {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_maps* maps;
+  const av1pf_plane* in;
+  av1pf_plane* ref_out;  /* NULL: no reference-frame download */
+  uint8_t* frame_out;    /* NULL: no packed-frame download */
+} av1pf_host_job;
+
+/* n av1pf_chain_host calls in one, for a decoder that holds several decoded
+ * frames (a sequence's frames, or several streams'): the frames' uploads,
+ * filter chains and downloads overlap on separate streams, over 3 device
+ * frame slots used in turn, so the copies in both directions and the
+ * kernels run at the same time. Returns when every job's outputs are on the
+ * host; the results equal n av1pf_chain_host calls. Every job is validated
+ * before anything is queued. Host buffers should be pinned (page-locked),
+ * or the copies do not overlap. */
+int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs);
+
 /* ------------------------------------------------------------------------ */
 /* Batched path: many frames of mixed shape / bit depth / subsampling, one   */
 /* persistent launch per stage, replayed from a captured CUDA graph.         */

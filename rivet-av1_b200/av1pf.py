@@ -87,6 +87,12 @@ class Job(C.Structure):
                 ("inp", C.POINTER(Plane)), ("ref_out", C.POINTER(Plane)), ("frame_out", C.c_void_p)]
 
 
+class HostJob(C.Structure):
+    """av1pf_host_job: one frame of av1pf_chain_host_many (host pointers)."""
+    _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("maps", C.POINTER(Maps)),
+                ("inp", C.POINTER(Plane)), ("ref_out", C.POINTER(Plane)), ("frame_out", C.c_void_p)]
+
+
 class Tuning(C.Structure):
     _fields_ = [("lf_mode", C.c_int32), ("lr_rect_cols", C.c_int32)]
 
@@ -174,6 +180,7 @@ def lib():
         _sig(L, "av1pf_output_noalloc", C.c_int, P(FrameInfo), P(Params), P(Plane), vp, vp)
         _sig(L, "av1pf_chain", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp, vp)
         _sig(L, "av1pf_chain_host", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp)
+        _sig(L, "av1pf_chain_host_many", C.c_int, vp, C.c_int, P(HostJob))
         _sig(L, "av1pf_batch_create", C.c_int, vp, P(Job), C.c_int, C.c_uint32, P(vp))
         _sig(L, "av1pf_batch_run", C.c_int, vp, vp)
         _sig(L, "av1pf_batch_destroy", C.c_int, vp)

@@ -2,6 +2,7 @@
 // entry points, the host-buffer chain, and the DSP entry points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -82,6 +83,17 @@ int Ctx::ensure_host(HostBuf& b, size_t bytes) {
   if (e != cudaSuccess) return cuda_status(e, "cudaMallocHost");
   b.size = bytes;
   return AV1PF_OK;
+}
+
+cudaError_t Ctx::pipe_streams() {
+  cudaError_t e = cudaSuccess;
+  if (!pipe_up) e = cudaStreamCreateWithFlags(&pipe_up, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !pipe_down) e = cudaStreamCreateWithFlags(&pipe_down, cudaStreamNonBlocking);
+  for (PipeSlot& ps : pipe) {
+    for (cudaEvent_t* ev : {&ps.uploaded, &ps.computed, &ps.downloaded})
+      if (e == cudaSuccess && !*ev) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  }
+  return e;
 }
 
 void Ctx::release(DevBuf& b) {
@@ -287,6 +299,13 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   ctx->release(ctx->scratch);
   ctx->release(ctx->meta);
   for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame}) ctx->release(*b);
+  for (Ctx::PipeSlot& ps : ctx->pipe) {
+    for (auto* b : {&ps.in, &ps.ref, &ps.maps, &ps.frame}) ctx->release(*b);
+    for (cudaEvent_t ev : {ps.uploaded, ps.computed, ps.downloaded})
+      if (ev) cudaEventDestroy(ev);
+  }
+  if (ctx->pipe_up) cudaStreamDestroy(ctx->pipe_up);
+  if (ctx->pipe_down) cudaStreamDestroy(ctx->pipe_down);
   if (ctx->meta_host.ptr) cudaFreeHost(ctx->meta_host.ptr);
   for (GraphEntry& g : ctx->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -419,6 +438,140 @@ int av1pf_chain(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params
   return ctx->run(&j, 1, as_stream(stream));
 }
 
+namespace {
+
+// Device layout of one host-buffer job: input planes with 64-sample-aligned
+// strides, visible-size reference planes, the maps, the packed frame.
+struct HostLayout {
+  size_t in_off[3] = {0, 0, 0}, ref_off[3] = {0, 0, 0}, map_off[8] = {};
+  size_t total_in = 0, total_ref = 0, total_maps = 0, fbytes = 0;
+  size_t mi_n = 0, tx_rows[3] = {0, 0, 0}, cdef_n = 0, lr_n[3] = {0, 0, 0};
+  av1pf_plane din[3] = {}, dref[3] = {};
+};
+
+void host_layout(const av1pf_frame_info* info, const av1pf_params* params, const av1pf_maps* maps,
+                 const av1pf_plane* in, HostLayout& L) {
+  const int np = info->num_planes, sb = info->sample_bytes;
+  for (int k = 0; k < np; k++) {
+    // host rows 16-byte aligned: the device plane keeps their stride and the
+    // upload is one contiguous copy; else 64-sample rows and a 2D copy
+    const bool flat = ((in[k].stride * sb) & 15) == 0 && in[k].stride >= in[k].width;
+    const int64_t stride = flat ? in[k].stride : (int64_t(in[k].width) + 63) / 64 * 64;
+    L.in_off[k] = L.total_in;
+    L.total_in += (size_t(stride) * size_t(in[k].height) * size_t(sb) + 255) / 256 * 256;
+    L.din[k] = av1pf_plane{nullptr, stride, in[k].width, in[k].height};
+    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
+    const int64_t rstride = (int64_t(pw) + 63) / 64 * 64;
+    L.ref_off[k] = L.total_ref;
+    L.total_ref += (size_t(rstride) * size_t(ph) * size_t(sb) + 255) / 256 * 256;
+    L.dref[k] = av1pf_plane{nullptr, rstride, pw, ph};
+  }
+  const int sy_c = np > 1 ? info->subsampling_y : 0;
+  L.mi_n = size_t(info->mi_rows) * size_t(maps->mi_stride);
+  L.tx_rows[0] = size_t(info->mi_rows);
+  L.tx_rows[1] = L.tx_rows[2] = size_t((info->mi_rows + (1 << sy_c) - 1) >> sy_c);
+  L.cdef_n = size_t((info->mi_rows + 15) / 16) * size_t(maps->cdef_stride);
+  for (int k = 0; k < np; k++)
+    if (params->uses_lr && params->frame_restoration_type[k] && maps->lr_units[k])
+      L.lr_n[k] = size_t(params->lr_unit_rows[k]) * size_t(params->lr_unit_cols[k]);
+  auto put = [&](int slot, size_t bytes) {
+    L.map_off[slot] = L.total_maps;
+    L.total_maps += (bytes + 255) / 256 * 256;
+  };
+  put(0, L.mi_n * sizeof(av1pf_mi));
+  for (int k = 0; k < 3; k++) put(1 + k, k < np ? L.tx_rows[k] * size_t(maps->mi_stride) : 0);
+  put(4, L.cdef_n);
+  for (int k = 0; k < 3; k++) put(5 + k, L.lr_n[k] * sizeof(av1pf_lr_unit));
+  L.fbytes = packed_frame_bytes(info);
+}
+
+// Enqueues the uploads of a job's planes and maps into device buffers laid
+// out by `L`; fills din / dref / dm with the device-side descriptions.
+cudaError_t upload_job(const HostLayout& L, const av1pf_frame_info* info, const av1pf_maps* maps,
+                       const av1pf_plane* in, uint8_t* bin, uint8_t* bref, uint8_t* bmap, av1pf_plane* din,
+                       av1pf_plane* dref, av1pf_maps& dm, cudaStream_t s) {
+  const int np = info->num_planes, sb = info->sample_bytes;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < np && e == cudaSuccess; k++) {
+    din[k] = L.din[k];
+    dref[k] = L.dref[k];
+    din[k].data = bin + L.in_off[k];
+    dref[k].data = bref + L.ref_off[k];
+    if (din[k].stride == in[k].stride) {
+      const size_t bytes = (size_t(in[k].stride) * size_t(in[k].height - 1) + size_t(in[k].width)) * size_t(sb);
+      e = cudaMemcpyAsync(din[k].data, in[k].data, bytes, cudaMemcpyHostToDevice, s);
+    } else {
+      e = cudaMemcpy2DAsync(din[k].data, size_t(din[k].stride) * sb, in[k].data, size_t(in[k].stride) * sb,
+                            size_t(in[k].width) * sb, size_t(in[k].height), cudaMemcpyHostToDevice, s);
+    }
+  }
+  dm = *maps;
+  dm.mi = reinterpret_cast<const av1pf_mi*>(bmap + L.map_off[0]);
+  if (e == cudaSuccess && L.mi_n && maps->mi)
+    e = cudaMemcpyAsync(bmap + L.map_off[0], maps->mi, L.mi_n * sizeof(av1pf_mi), cudaMemcpyHostToDevice, s);
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+    dm.lf_tx_size[k] = nullptr;
+    if (k < np && maps->lf_tx_size[k]) {
+      dm.lf_tx_size[k] = bmap + L.map_off[1 + k];
+      e = cudaMemcpyAsync(bmap + L.map_off[1 + k], maps->lf_tx_size[k], L.tx_rows[k] * size_t(maps->mi_stride),
+                          cudaMemcpyHostToDevice, s);
+    }
+  }
+  dm.cdef_idx = nullptr;
+  if (e == cudaSuccess && maps->cdef_idx) {
+    dm.cdef_idx = reinterpret_cast<const int8_t*>(bmap + L.map_off[4]);
+    e = cudaMemcpyAsync(bmap + L.map_off[4], maps->cdef_idx, L.cdef_n, cudaMemcpyHostToDevice, s);
+  }
+  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+    dm.lr_units[k] = nullptr;
+    if (L.lr_n[k]) {
+      dm.lr_units[k] = reinterpret_cast<const av1pf_lr_unit*>(bmap + L.map_off[5 + k]);
+      e = cudaMemcpyAsync(bmap + L.map_off[5 + k], maps->lr_units[k], L.lr_n[k] * sizeof(av1pf_lr_unit),
+                          cudaMemcpyHostToDevice, s);
+    }
+  }
+  return e;
+}
+
+// Enqueues the downloads of the reference planes (when ref_out is set) and
+// the packed frame (when frame_out is set).
+cudaError_t download_job(const HostLayout& L, const av1pf_frame_info* info, const av1pf_plane* dref,
+                         av1pf_plane* ref_out, const uint8_t* dframe, uint8_t* frame_out, cudaStream_t s) {
+  const int np = info->num_planes, sb = info->sample_bytes;
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; ref_out && k < np && e == cudaSuccess; k++) {
+    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
+    e = cudaMemcpy2DAsync(ref_out[k].data, size_t(ref_out[k].stride) * sb, dref[k].data, size_t(dref[k].stride) * sb,
+                          size_t(pw) * sb, size_t(ph), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess && frame_out) e = cudaMemcpyAsync(frame_out, dframe, L.fbytes, cudaMemcpyDeviceToHost, s);
+  return e;
+}
+
+// The host planes' own geometry (their size against the frame is checked
+// on the device copies by av1pf_chain).
+int check_host_planes(const av1pf_frame_info* info, const av1pf_plane* in) {
+  for (int k = 0; k < info->num_planes; k++)
+    if (!in[k].data || in[k].width <= 0 || in[k].height <= 0 || in[k].stride < in[k].width) {
+      set_error("host plane: null data, empty, or stride < width");
+      return AV1PF_ERR_INVALID_INPUT;
+    }
+  return AV1PF_OK;
+}
+
+int check_error_flags(cudaStream_t s) {
+  uint32_t flags = 0;
+  cudaError_t e = read_error_flags(&flags, s);
+  if (e != cudaSuccess) return cuda_status(e, "error flags");
+  if (flags) {
+    set_error("the maps broke a conformance requirement (bad block / transform size or edge position)");
+    return AV1PF_ERR_INVALID_INPUT;
+  }
+  return AV1PF_OK;
+}
+
+}  // namespace
+
 int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
                      const av1pf_maps* maps, const av1pf_plane* in, av1pf_plane* ref_out, uint8_t* frame_out) {
   int rc = check_ctx(ctx);
@@ -428,100 +581,101 @@ int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_p
     set_error("null input");
     return AV1PF_ERR_INVALID_INPUT;
   }
-  const int np = info->num_planes, sb = info->sample_bytes;
+  if ((rc = check_host_planes(info, in))) return rc;
   cudaStream_t s = ctx->own;
-  // device layout: input planes with 64-sample-aligned strides, visible-size
-  // reference planes, maps, packed frame
-  size_t in_off[3], ref_off[3], total_in = 0, total_ref = 0;
-  av1pf_plane din[3], dref[3];
-  for (int k = 0; k < np; k++) {
-    const int64_t stride = (int64_t(in[k].width) + 63) / 64 * 64;
-    in_off[k] = total_in;
-    total_in += (size_t(stride) * size_t(in[k].height) * size_t(sb) + 255) / 256 * 256;
-    din[k] = av1pf_plane{nullptr, stride, in[k].width, in[k].height};
-    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
-    const int64_t rstride = (int64_t(pw) + 63) / 64 * 64;
-    ref_off[k] = total_ref;
-    total_ref += (size_t(rstride) * size_t(ph) * size_t(sb) + 255) / 256 * 256;
-    dref[k] = av1pf_plane{nullptr, rstride, pw, ph};
-  }
-  const int sy_c = np > 1 ? info->subsampling_y : 0;
-  const size_t mi_n = size_t(info->mi_rows) * size_t(maps->mi_stride);
-  const size_t tx_rows[3] = {size_t(info->mi_rows), size_t((info->mi_rows + (1 << sy_c) - 1) >> sy_c),
-                             size_t((info->mi_rows + (1 << sy_c) - 1) >> sy_c)};
-  const size_t cdef_n = size_t((info->mi_rows + 15) / 16) * size_t(maps->cdef_stride);
-  size_t lr_n[3] = {0, 0, 0};
-  for (int k = 0; k < np; k++)
-    if (params->uses_lr && params->frame_restoration_type[k] && maps->lr_units[k])
-      lr_n[k] = size_t(params->lr_unit_rows[k]) * size_t(params->lr_unit_cols[k]);
-  size_t map_off[8], total_maps = 0;
-  auto put = [&](int slot, size_t bytes) {
-    map_off[slot] = total_maps;
-    total_maps += (bytes + 255) / 256 * 256;
-  };
-  put(0, mi_n * sizeof(av1pf_mi));
-  for (int k = 0; k < 3; k++) put(1 + k, k < np ? tx_rows[k] * size_t(maps->mi_stride) : 0);
-  put(4, cdef_n);
-  for (int k = 0; k < 3; k++) put(5 + k, lr_n[k] * sizeof(av1pf_lr_unit));
-  const size_t fbytes = packed_frame_bytes(info);
-  if ((rc = ctx->ensure(ctx->h_in, total_in)) || (rc = ctx->ensure(ctx->h_ref, total_ref)) ||
-      (rc = ctx->ensure(ctx->h_maps, total_maps)) || (rc = ctx->ensure(ctx->h_frame, fbytes + 16)))
+  HostLayout L;
+  host_layout(info, params, maps, in, L);
+  if ((rc = ctx->ensure(ctx->h_in, L.total_in)) || (rc = ctx->ensure(ctx->h_ref, L.total_ref)) ||
+      (rc = ctx->ensure(ctx->h_maps, L.total_maps)) || (rc = ctx->ensure(ctx->h_frame, L.fbytes + 16)))
     return rc;
-  uint8_t* bin = static_cast<uint8_t*>(ctx->h_in.ptr);
-  uint8_t* bref = static_cast<uint8_t*>(ctx->h_ref.ptr);
-  uint8_t* bmap = static_cast<uint8_t*>(ctx->h_maps.ptr);
-  cudaError_t e = cudaSuccess;
-  for (int k = 0; k < np && e == cudaSuccess; k++) {
-    din[k].data = bin + in_off[k];
-    dref[k].data = bref + ref_off[k];
-    e = cudaMemcpy2DAsync(din[k].data, size_t(din[k].stride) * sb, in[k].data, size_t(in[k].stride) * sb,
-                          size_t(in[k].width) * sb, size_t(in[k].height), cudaMemcpyHostToDevice, s);
-  }
-  av1pf_maps dm = *maps;
-  dm.mi = reinterpret_cast<const av1pf_mi*>(bmap + map_off[0]);
-  if (e == cudaSuccess && mi_n && maps->mi)
-    e = cudaMemcpyAsync(bmap + map_off[0], maps->mi, mi_n * sizeof(av1pf_mi), cudaMemcpyHostToDevice, s);
-  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
-    dm.lf_tx_size[k] = nullptr;
-    if (k < np && maps->lf_tx_size[k]) {
-      dm.lf_tx_size[k] = bmap + map_off[1 + k];
-      e = cudaMemcpyAsync(bmap + map_off[1 + k], maps->lf_tx_size[k], tx_rows[k] * size_t(maps->mi_stride),
-                          cudaMemcpyHostToDevice, s);
-    }
-  }
-  dm.cdef_idx = nullptr;
-  if (e == cudaSuccess && maps->cdef_idx) {
-    dm.cdef_idx = reinterpret_cast<const int8_t*>(bmap + map_off[4]);
-    e = cudaMemcpyAsync(bmap + map_off[4], maps->cdef_idx, cdef_n, cudaMemcpyHostToDevice, s);
-  }
-  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
-    dm.lr_units[k] = nullptr;
-    if (lr_n[k]) {
-      dm.lr_units[k] = reinterpret_cast<const av1pf_lr_unit*>(bmap + map_off[5 + k]);
-      e = cudaMemcpyAsync(bmap + map_off[5 + k], maps->lr_units[k], lr_n[k] * sizeof(av1pf_lr_unit),
-                          cudaMemcpyHostToDevice, s);
-    }
-  }
+  av1pf_plane din[3], dref[3];
+  av1pf_maps dm;
+  cudaError_t e = upload_job(L, info, maps, in, static_cast<uint8_t*>(ctx->h_in.ptr),
+                             static_cast<uint8_t*>(ctx->h_ref.ptr), static_cast<uint8_t*>(ctx->h_maps.ptr), din, dref,
+                             dm, s);
   if (e != cudaSuccess) return cuda_status(e, "host-to-device copy");
   uint8_t* dframe = frame_out ? static_cast<uint8_t*>(ctx->h_frame.ptr) : nullptr;
   rc = av1pf_chain(ctx, info, params, &dm, din, dref, dframe, s);
   if (rc != AV1PF_OK) return rc;
-  for (int k = 0; ref_out && k < np && e == cudaSuccess; k++) {
-    const int pw = plane_w(info, k, info->upscaled_width), ph = plane_h(info, k);
-    e = cudaMemcpy2DAsync(ref_out[k].data, size_t(ref_out[k].stride) * sb, dref[k].data, size_t(dref[k].stride) * sb,
-                          size_t(pw) * sb, size_t(ph), cudaMemcpyDeviceToHost, s);
-  }
-  if (e == cudaSuccess && frame_out) e = cudaMemcpyAsync(frame_out, dframe, fbytes, cudaMemcpyDeviceToHost, s);
+  e = download_job(L, info, dref, ref_out, dframe, frame_out, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_status(e, "chain_host");
-  uint32_t flags = 0;
-  e = read_error_flags(&flags, s);
-  if (e != cudaSuccess) return cuda_status(e, "error flags");
-  if (flags) {
-    set_error("the maps broke a conformance requirement (bad block / transform size or edge position)");
+  return check_error_flags(s);
+}
+
+int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && !jobs)) {
+    set_error("bad job list");
     return AV1PF_ERR_INVALID_INPUT;
   }
-  return AV1PF_OK;
+  if (n == 0) return AV1PF_OK;
+  // every job is checked, and the slots sized for the largest, before
+  // anything is queued
+  std::vector<HostLayout> lay(static_cast<size_t>(n));
+  size_t need_in = 0, need_ref = 0, need_maps = 0, need_frame = 0;
+  for (int k = 0; k < n; k++) {
+    const av1pf_host_job& j = jobs[k];
+    if ((rc = validate_all(j.info, j.params, nullptr))) return rc;
+    if (!j.in || !j.maps) {
+      set_error("null input");
+      return AV1PF_ERR_INVALID_INPUT;
+    }
+    if ((rc = check_host_planes(j.info, j.in))) return rc;
+    host_layout(j.info, j.params, j.maps, j.in, lay[size_t(k)]);
+    need_in = std::max(need_in, lay[size_t(k)].total_in);
+    need_ref = std::max(need_ref, lay[size_t(k)].total_ref);
+    need_maps = std::max(need_maps, lay[size_t(k)].total_maps);
+    need_frame = std::max(need_frame, lay[size_t(k)].fbytes + 16);
+  }
+  const int slots = std::min(n, Ctx::kPipeSlots);
+  for (int q = 0; q < slots; q++) {
+    Ctx::PipeSlot& ps = ctx->pipe[q];
+    if ((rc = ctx->ensure(ps.in, need_in)) || (rc = ctx->ensure(ps.ref, need_ref)) ||
+        (rc = ctx->ensure(ps.maps, need_maps)) || (rc = ctx->ensure(ps.frame, need_frame)))
+      return rc;
+  }
+  cudaError_t e = ctx->pipe_streams();
+  if (e != cudaSuccess) return cuda_status(e, "pipeline streams");
+  cudaStream_t up = ctx->pipe_up, comp = ctx->own, down = ctx->pipe_down;
+  // frame k uses slot k % slots: its upload waits for the chain that last
+  // read the slot's inputs, its chain for its upload and for the download
+  // that last read the slot's outputs
+  for (int k = 0; k < n && e == cudaSuccess; k++) {
+    const av1pf_host_job& j = jobs[k];
+    Ctx::PipeSlot& ps = ctx->pipe[k % slots];
+    const bool reused = k >= slots;
+    if (reused) e = cudaStreamWaitEvent(up, ps.computed, 0);
+    av1pf_plane din[3], dref[3];
+    av1pf_maps dm;
+    if (e == cudaSuccess)
+      e = upload_job(lay[size_t(k)], j.info, j.maps, j.in, static_cast<uint8_t*>(ps.in.ptr),
+                     static_cast<uint8_t*>(ps.ref.ptr), static_cast<uint8_t*>(ps.maps.ptr), din, dref, dm, up);
+    if (e == cudaSuccess) e = cudaEventRecord(ps.uploaded, up);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ps.uploaded, 0);
+    if (e == cudaSuccess && reused) e = cudaStreamWaitEvent(comp, ps.downloaded, 0);
+    if (e != cudaSuccess) break;
+    uint8_t* dframe = j.frame_out ? static_cast<uint8_t*>(ps.frame.ptr) : nullptr;
+    rc = av1pf_chain(ctx, j.info, j.params, &dm, din, dref, dframe, comp);
+    if (rc != AV1PF_OK) {
+      cudaStreamSynchronize(up);
+      cudaStreamSynchronize(comp);
+      cudaStreamSynchronize(down);
+      return rc;
+    }
+    e = cudaEventRecord(ps.computed, comp);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(down, ps.computed, 0);
+    if (e == cudaSuccess) e = download_job(lay[size_t(k)], j.info, dref, j.ref_out, dframe, j.frame_out, down);
+    if (e == cudaSuccess) e = cudaEventRecord(ps.downloaded, down);
+  }
+  // every download waits for its chain, which waits for its upload
+  const cudaError_t e_up = cudaStreamSynchronize(up);
+  const cudaError_t e_comp = cudaStreamSynchronize(comp);
+  const cudaError_t e_down = cudaStreamSynchronize(down);
+  if (e == cudaSuccess) e = e_up != cudaSuccess ? e_up : (e_comp != cudaSuccess ? e_comp : e_down);
+  if (e != cudaSuccess) return cuda_status(e, "chain_host_many");
+  return check_error_flags(comp);
 }
 
 int av1pf_dsp_lf_filter(av1pf_ctx* ctx, int32_t* edges, const av1pf_lf_edge_params* params, int n, void* stream) {

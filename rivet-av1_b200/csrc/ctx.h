@@ -69,6 +69,17 @@ struct Ctx {
   bool staged_once = false;
   DevBuf scratch, meta;
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
+  // av1pf_chain_host_many: device frame slots used in turn, with the events
+  // that order a slot's upload (pipe_up), chain (own) and download
+  // (pipe_down) against its next use
+  static constexpr int kPipeSlots = 3;
+  struct PipeSlot {
+    DevBuf in, ref, maps, frame;
+    cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
+  };
+  PipeSlot pipe[kPipeSlots];
+  cudaStream_t pipe_up = nullptr, pipe_down = nullptr;
+  cudaError_t pipe_streams();  // creates the streams and events on first use
   HostBuf meta_host;
   Plan plan;
   // per-frame graphs, by launch structure (least recently used replaced)

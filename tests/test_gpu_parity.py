@@ -250,6 +250,50 @@ def test_chain_host_matches_oracle(ctx, name):
     assert_same(ref.arrays, fb, ref_cpu, fb_cpu, name)
 
 
+def test_chain_host_many_matches_oracle(ctx):
+    """Frames of different shapes through the pipelined host entry point (more
+    frames than device slots, so slots are reused across shapes), some with
+    pinned and some with pageable buffers, some without a reference download:
+    every output equals the oracle's."""
+    import torch
+    names = ["c1_352x288_8bit_u8", "b12_444_superres_grain", "b10_420", "b10_422_grain", "tiny_17x9",
+             "b10_420", "b8_mono_grain"]
+    sfs = [A.SynthHandle(**dict(CHAIN_CASES[n], seed=CHAIN_CASES[n]["seed"] + 7 * i)) for i, n in enumerate(names)]
+    want = [O.chain(sf, threads=0) for sf in sfs]
+    jobs = (A.HostJob * len(sfs))()
+    keep = []
+    for i, sf in enumerate(sfs):
+        info = sf.f.info
+        inp = O.HostPlanes.like_synth(sf)
+        ref = O.HostPlanes.visible(info) if i % 3 != 1 else None
+        if i % 2 == 0:
+            fb_t = torch.zeros(A.frame_bytes(info), dtype=torch.uint8).pin_memory()
+            fb, fb_ptr = fb_t, fb_t.data_ptr()
+        else:
+            fb = np.zeros(A.frame_bytes(info), np.uint8)
+            fb_ptr = fb.ctypes.data
+        keep.append((inp, ref, fb))
+        jobs[i].info = C.pointer(info)
+        jobs[i].params = C.pointer(sf.f.params)
+        jobs[i].maps = C.pointer(sf.f.maps)
+        jobs[i].inp = C.cast(inp.c, C.POINTER(A.Plane))
+        jobs[i].ref_out = C.cast(ref.c, C.POINTER(A.Plane)) if ref is not None else None
+        jobs[i].frame_out = fb_ptr
+    A.check(A.lib().av1pf_chain_host_many(ctx.p, len(sfs), jobs), "chain_host_many")
+    for i, ((inp, ref, fb), (ref_cpu, fb_cpu)) in enumerate(zip(keep, want)):
+        fb_np = fb.numpy() if hasattr(fb, "numpy") else fb
+        assert np.array_equal(fb_np, fb_cpu), f"frame {i} ({names[i]}): packed frame"
+        if ref is not None:
+            for p in range(sfs[i].info.num_planes):
+                assert np.array_equal(ref.arrays[p], ref_cpu.arrays[p]), f"frame {i} plane {p}"
+    # an invalid job refuses the whole call before anything is queued
+    bad = (A.HostJob * 1)()
+    bad[0] = jobs[0]
+    bad[0].inp = None
+    assert A.lib().av1pf_chain_host_many(ctx.p, 1, bad) == A.ERR_INVALID_INPUT
+    A.check(A.lib().av1pf_chain_host_many(ctx.p, 0, None))
+
+
 def test_batch_matches_per_frame(ctx):
     names = ["c1_352x288_8bit_u8", "b10_420", "b12_444_superres_grain", "b10_422_grain", "b8_mono_grain",
              "tiny_17x9", "lr_unit128", "b10_superres_d16"]
