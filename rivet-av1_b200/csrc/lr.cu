@@ -38,9 +38,22 @@ constexpr int kAS = 72;                  // A/B row stride (int32): w + 2 <= 66
 constexpr int kWinBytes = (kMaxH + 6) * kWS * 2;
 constexpr int kABytes = (kMaxH + 2) * kAS * 4;
 constexpr int kF0Bytes = kMaxH * kMaxW * 4;  // the first self-guided filter's output
-constexpr int kSmemBytes = kWinBytes + 2 * kABytes + 256 * 4 + kF0Bytes;
+constexpr int kSmemBytes = kWinBytes + 2 * kABytes + kF0Bytes;
 static_assert((kMaxH + 6) * kWS * 2 <= kABytes, "Wiener intermediate must fit the A area");
+
+// SGR_A2 (postfilter.rs:884-898), built at compile time into global memory:
+// the self-guided passes read it through the L1, so no CTA sets it up.
+struct A2Table {
+  int32_t v[256];
+};
+constexpr A2Table make_a2() {
+  A2Table t{};
+  for (int z = 0; z < 256; z++) t.v[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
+  return t;
+}
 }  // namespace
+
+__device__ const A2Table g_sgr_a2 = make_a2();
 
 struct LrGeom {
   int ss, se, y0, y1, pex, pey;
@@ -214,7 +227,7 @@ __device__ __forceinline__ void sgr_ab(const uint16_t* win, int32_t* A, int32_t*
           const int d = round2(bsum, bd - 8);
           const int pp = max(a * n - d * d, 0);
           const uint64_t z = (uint64_t(uint32_t(pp)) * sc + (1u << 19)) >> 20;
-          const int a2 = a2tab[z > 255 ? 255 : int(z)];
+          const int a2 = __ldg(a2tab + (z > 255 ? 255 : int(z)));
           const uint32_t k = uint32_t(256 - a2) * uint32_t(one_over_n);
           const uint64_t b2 = uint64_t(k) * uint32_t(bsum);
           A[i * kAS + c] = a2;
@@ -284,7 +297,7 @@ struct LrSmem {
   uint16_t* win;    // the window, rows kWS apart
   int32_t* A;       // self-guided A (Wiener: the int16 intermediate)
   int32_t* B;       // self-guided B
-  const int32_t* a2tab;
+  const int32_t* a2tab;  // SGR_A2 (global memory)
   int32_t* F0;      // first self-guided output, then every rectangle's output
   av1pf_lr_unit* unit;
 };
@@ -442,14 +455,10 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
   sm.win = reinterpret_cast<uint16_t*>(smem);
   sm.A = reinterpret_cast<int32_t*>(smem + kWinBytes);
   sm.B = reinterpret_cast<int32_t*>(smem + kWinBytes + kABytes);
-  int32_t* a2tab = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
-  sm.a2tab = a2tab;
-  sm.F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes + 256 * 4);
+  sm.a2tab = g_sgr_a2.v;
+  sm.F0 = reinterpret_cast<int32_t*>(smem + kWinBytes + 2 * kABytes);
   sm.unit = &s_unit;
   const int tid = threadIdx.x;
-  // SGR_A2 (postfilter.rs:884-898)
-  for (int z = tid; z < 256; z += kThreads) a2tab[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
-  __syncthreads();
 
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
