@@ -435,13 +435,17 @@ int av1pf_serve_open(av1pf_ctx* ctx, const av1pf_serve_config* cfg,
  * av1pf_serve_close_stream. Admission is by free HBM under the cap. */
 int av1pf_serve_open_stream(av1pf_server* s, const av1pf_frame_info* info,
                             int32_t* stream_id);
+/* Waits for the stream's queued and running frames, then frees its slots.
+ * Results of host requests not polled yet go with them: polling such a
+ * ticket afterwards returns AV1PF_ERR_NOT_FOUND. */
 int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id);
 /* Queues one frame of `stream_id`; returns a ticket. Never blocks on the GPU. */
 int av1pf_serve_submit(av1pf_server* s, int32_t stream_id,
                        const av1pf_request* req, uint64_t* ticket);
 /* Queues n frames (frame k of stream stream_ids[k]) under one lock, in
  * order, so one tick can batch them together; tickets[k] receives frame k's
- * ticket. All or nothing: if one request is refused, none is queued. */
+ * ticket. All or nothing: if one request is refused, none is queued. A
+ * group of host requests is copied into staging by up to 8 threads. */
 int av1pf_serve_submit_many(av1pf_server* s, int32_t n, const int32_t* stream_ids,
                             const av1pf_request* reqs, uint64_t* tickets);
 /* Waits up to `wait_ms` for `ticket`; on completion copies the packed output

@@ -142,6 +142,7 @@ struct Stream {
   std::vector<void*> pool_in, pool_out;  // free pinned buffers
   std::vector<void*> all_pinned;         // every pinned buffer (freed at close)
   int running = 0;
+  int copying = 0;  // polls copying a result out of this stream's pinned buffers
   bool closing = false;
 };
 
@@ -612,12 +613,23 @@ int av1pf_serve_close_stream(av1pf_server* s, int32_t stream_id) {
   st->closing = true;
   // wait for the stream's queued and running frames
   auto busy = [&] {
-    if (st->running) return true;
+    if (st->running || st->copying) return true;
     for (Request* r : s->queue)
       if (r->stream == stream_id) return true;
     return false;
   };
   while (busy()) s->cv_done.wait_for(lk, std::chrono::milliseconds(5));
+  // results not polled yet lose their buffers with the stream: a later poll
+  // of such a ticket reports the loss instead of reading freed memory
+  for (auto& tr : s->tickets) {
+    Request* r = tr.second;
+    if (r->stream != stream_id || !r->hres) continue;
+    r->hres = nullptr;
+    if (r->state == 2) {
+      r->state = 3;
+      r->status = AV1PF_ERR_NOT_FOUND;
+    }
+  }
   cudaSetDevice(s->ctx->device);
   for (Slot& x : st->slots) {
     s->dev_free(x.dblob, st->lay.bytes);
@@ -642,17 +654,36 @@ int av1pf_serve_submit(av1pf_server* s, int32_t stream_id, const av1pf_request* 
 int av1pf_serve_submit_many(av1pf_server* s, int32_t n, const int32_t* stream_ids, const av1pf_request* reqs,
                             uint64_t* tickets) {
   if (!s || n < 0 || (n > 0 && (!stream_ids || !reqs || !tickets))) return AV1PF_ERR_INVALID_INPUT;
-  std::vector<Request*> rs;
-  rs.reserve(size_t(n));
-  for (int k = 0; k < n; k++) {
-    Request* r = nullptr;
-    const int rc = prepare_request(s, stream_ids[k], &reqs[k], &r);
-    if (rc != AV1PF_OK) {
-      for (Request* q : rs) discard_request(s, q);
-      set_error("serving: request " + std::to_string(k) + " of the group refused (none queued)");
-      return rc;
+  std::vector<Request*> rs(size_t(n), nullptr);
+  std::vector<int> rcs(size_t(n), AV1PF_OK);
+  std::vector<std::string> why(static_cast<size_t>(n));
+  // Host requests are copied into pinned staging at submit time; a large
+  // group spreads those copies over a few threads (host memory bandwidth,
+  // not one core, then bounds them). Each thread takes every nt-th request.
+  int host_reqs = 0;
+  for (int k = 0; k < n; k++) host_reqs += reqs[k].device ? 0 : 1;
+  const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
+  const int nt = std::max(1, std::min({8, hw / 2, host_reqs / 4}));
+  auto prep = [&](int t) {
+    for (int k = t; k < n; k += nt) {
+      rcs[size_t(k)] = prepare_request(s, stream_ids[k], &reqs[k], &rs[size_t(k)]);
+      if (rcs[size_t(k)] != AV1PF_OK) why[size_t(k)] = av1pf_last_error();
     }
-    rs.push_back(r);
+  };
+  if (nt == 1) {
+    prep(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(prep, t);
+    prep(0);
+    for (std::thread& x : th) x.join();
+  }
+  for (int k = 0; k < n; k++) {
+    if (rcs[size_t(k)] == AV1PF_OK) continue;
+    for (Request* q : rs)
+      if (q) discard_request(s, q);
+    set_error("serving: request " + std::to_string(k) + " of the group refused (none queued): " + why[size_t(k)]);
+    return rcs[size_t(k)];
   }
   if (n > 0) enqueue(s, rs.data(), n, tickets);
   return AV1PF_OK;
@@ -669,12 +700,23 @@ int av1pf_serve_poll(av1pf_server* s, uint64_t ticket, int32_t wait_ms, uint8_t*
     if (s->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && r->state < 2) return AV1PF_ERR_TIMEOUT;
   }
   const int status = r->state == 2 ? AV1PF_OK : r->status;
+  s->tickets.erase(it);
+  // the result copy runs without the lock, so the worker and other callers
+  // are not held up by it; the request is this caller's alone now, and the
+  // stream's pinned buffers stay allocated while `copying` counts it
+  if (r->hres) r->st->copying++;
+  lk.unlock();
   if (status == AV1PF_OK) {
     if (frame_out && r->hres) std::memcpy(frame_out, r->hres, r->st->lay.frame_bytes);
     if (latency_ms) *latency_ms = r->t_done - r->t_submit;
   }
-  if (r->hres) r->st->pool_out.push_back(r->hres);
-  s->tickets.erase(it);
+  if (r->hres) {
+    lk.lock();
+    r->st->pool_out.push_back(r->hres);
+    r->st->copying--;
+    lk.unlock();
+    s->cv_done.notify_all();
+  }
   delete r;
   return status;
 }

@@ -125,6 +125,38 @@ def test_serve_admission_and_errors():
     ctx.close()
 
 
+def test_serve_close_stream_drops_unpolled_results():
+    """A host request that completed but was not polled when its stream
+    closed reports ERR_NOT_FOUND at poll instead of reading freed buffers;
+    polls before the close still return the frame."""
+    import time
+    ctx = G.Ctx()
+    srv = open_server(ctx)
+    sf = A.SynthHandle(**STREAMS[0], seed=41)
+    want = O.chain(sf, threads=0)[1]
+    sid = C.c_int32()
+    A.check(L().av1pf_serve_open_stream(srv, C.byref(sf.f.info), C.byref(sid)))
+    keep = []
+    t1, t2 = C.c_uint64(), C.c_uint64()
+    A.check(L().av1pf_serve_submit(srv, sid.value, C.byref(request(sf, keep)), C.byref(t1)))
+    A.check(L().av1pf_serve_submit(srv, sid.value, C.byref(request(sf, keep)), C.byref(t2)))
+    out = np.zeros(A.frame_bytes(sf.f.info), np.uint8)
+    A.check(L().av1pf_serve_poll(srv, t1.value, 10000, out.ctypes.data, None))
+    assert np.array_equal(out, want)
+    st = A.ServeStats()
+    deadline = time.time() + 10
+    while time.time() < deadline:
+        A.check(L().av1pf_serve_stats_get(srv, C.byref(st)))
+        if st.completed == 2:
+            break
+        time.sleep(0.01)
+    assert st.completed == 2
+    A.check(L().av1pf_serve_close_stream(srv, sid.value))
+    assert L().av1pf_serve_poll(srv, t2.value, 0, out.ctypes.data, None) == A.ERR_NOT_FOUND
+    A.check(L().av1pf_serve_close(srv))
+    ctx.close()
+
+
 def test_serve_device_resident_requests():
     """Frames already on the device (as a GPU decoder leaves them) are served
     in place into the caller's device outputs, bit-exact with the oracle."""
