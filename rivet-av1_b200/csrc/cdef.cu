@@ -355,14 +355,13 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
   __shared__ int32_t cost[64][8];
   __shared__ BlkTaps taps[3][64];
   __shared__ uint8_t bstate[64];  // 0 = outside the MI area, 1 = copy, 2 = filter
-  __shared__ LfTables tb;
+  const LfTables& tb = g_lf_tables;
   __shared__ uint16_t hdec[19 * 18];  // horizontal-edge decisions of one plane
   __shared__ int16_t doff[8][2];      // window offsets of CDEF_DIRECTIONS
   __shared__ uint8_t uvdir[2][2][8];  // CDEF_UV_DIR
   __shared__ int s_one;               // 1, opaque to the compiler (see cdef_tap)
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  load_lf_tables(tb);
   if (tid < 16) doff[tid >> 1][tid & 1] = int16_t(c_cdef_dirs[tid >> 1][tid & 1][0] * kS + c_cdef_dirs[tid >> 1][tid & 1][1]);
   if (tid < 32) (&uvdir[0][0][0])[tid] = (&c_cdef_uv_dir[0][0][0])[tid];
   if (tid == 0) s_one = 1;

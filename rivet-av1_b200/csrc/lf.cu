@@ -25,6 +25,8 @@
 
 namespace av1pf {
 
+__device__ const LfTables g_lf_tables = make_lf_tables();
+
 // Edge list entry: frame:16 | plane:2 | code:2 | lvl:6 | cx:14 | cy:14.
 __device__ __forceinline__ uint64_t pack_edge(int frame, int plane, int dec, int cx, int cy) {
   return uint64_t(frame) | (uint64_t(plane) << 16) | (uint64_t(dec) << 18) | (uint64_t(cx) << 26) |
@@ -105,10 +107,8 @@ __global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __rest
                                                       const Item* __restrict__ items, int n_items,
                                                       uint64_t* __restrict__ list_v, uint64_t* __restrict__ list_h,
                                                       uint32_t* __restrict__ counts, uint32_t cap) {
-  __shared__ LfTables tb;
+  const LfTables& tb = g_lf_tables;
   __shared__ EdgeAgg agg;
-  load_lf_tables(tb);
-  __syncthreads();
   pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
@@ -274,10 +274,9 @@ __global__ void __launch_bounds__(256, 4) lf_tile_kernel(const FrameDesc* __rest
                                                       const Item* __restrict__ items, int n_items,
                                                       uint64_t* __restrict__ list_h, uint32_t* __restrict__ counts,
                                                       uint32_t cap) {
-  __shared__ LfTables tb;
+  const LfTables& tb = g_lf_tables;
   __shared__ __align__(16) uint16_t T[kLfTile * kLfTS];
   __shared__ uint16_t dec[kLfTile / 4][kLfCells];  // vertical-edge decisions
-  load_lf_tables(tb);
   const int tid = threadIdx.x;
   pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {

@@ -6,6 +6,7 @@
 // filter_strength) and src/dsp/lf.rs:58-306 (the sample filters).
 #pragma once
 
+#include "av1_tables.h"
 #include "common.cuh"
 
 namespace av1pf {
@@ -38,8 +39,9 @@ __device__ __forceinline__ int lf_level(const FrameDesc& f, int row, int col, in
   return lf_level_raw(f, *reinterpret_cast<const uint2*>(f.mi + int64_t(row) * f.mi_stride + col), plane, pass);
 }
 
-// Small tables the decisions index with per-lane values, copied to shared
-// memory (constant memory serialises divergent indices).
+// Small tables the decisions index with per-lane values (constant memory
+// serialises divergent indices), built at compile time into global memory
+// and read through the L1, so no CTA sets them up.
 struct LfTables {
   uint8_t subsampled[22][2][2];
   uint8_t bw_log2[23], bh_log2[23];  // log2 of block width/height in samples (22 = invalid)
@@ -47,19 +49,39 @@ struct LfTables {
   uint8_t txw[19], txh[19];
 };
 
-__device__ __forceinline__ void load_lf_tables(LfTables& t) {
-  for (int k = threadIdx.x; k < 22 * 4; k += blockDim.x) (&t.subsampled[0][0][0])[k] = (&c_subsampled_size[0][0][0])[k];
-  for (int k = threadIdx.x; k < 23; k += blockDim.x) {
-    t.bw_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4w[k]))) : 0;
-    t.bh_log2[k] = k < 22 ? uint8_t(2 + (31 - __clz(c_n4h[k]))) : 0;
+constexpr int lf_ilog2(int v) {
+  int r = 0;
+  while (v > 1) {
+    v >>= 1;
+    r++;
   }
-  for (int k = threadIdx.x; k < 19; k += blockDim.x) {
-    t.txw[k] = c_tx_w[k];
-    t.txh[k] = c_tx_h[k];
-    t.txw_log2[k] = uint8_t(31 - __clz(c_tx_w[k]));
-    t.txh_log2[k] = uint8_t(31 - __clz(c_tx_h[k]));
-  }
+  return r;
 }
+
+constexpr LfTables make_lf_tables() {
+  LfTables t{};
+  constexpr uint8_t sub[22][2][2] = AV1T_SUBSAMPLED_SIZE;
+  constexpr uint8_t n4w[22] = AV1T_NUM_4X4_BLOCKS_WIDE;
+  constexpr uint8_t n4h[22] = AV1T_NUM_4X4_BLOCKS_HIGH;
+  constexpr uint8_t txw[19] = AV1T_TX_WIDTH;
+  constexpr uint8_t txh[19] = AV1T_TX_HEIGHT;
+  for (int i = 0; i < 22; i++)
+    for (int j = 0; j < 2; j++)
+      for (int k = 0; k < 2; k++) t.subsampled[i][j][k] = sub[i][j][k];
+  for (int k = 0; k < 23; k++) {
+    t.bw_log2[k] = uint8_t(k < 22 ? 2 + lf_ilog2(n4w[k]) : 0);
+    t.bh_log2[k] = uint8_t(k < 22 ? 2 + lf_ilog2(n4h[k]) : 0);
+  }
+  for (int k = 0; k < 19; k++) {
+    t.txw[k] = txw[k];
+    t.txh[k] = txh[k];
+    t.txw_log2[k] = uint8_t(lf_ilog2(txw[k]));
+    t.txh_log2[k] = uint8_t(lf_ilog2(txh[k]));
+  }
+  return t;
+}
+
+extern __device__ const LfTables g_lf_tables;  // lf.cu
 
 // edge_loop_filter's decisions (postfilter.rs:107-172) for the 4x4 at plane
 // position (cx, cy), both passes: 0 = not filtered, else (size code << 6) |
