@@ -28,7 +28,7 @@ extern __constant__ uint8_t c_tx_h[19];
 extern __constant__ uint8_t c_n4w[22];
 extern __constant__ uint8_t c_n4h[22];
 extern __constant__ int32_t c_sgr_params[16][4];
-extern __device__ int16_t g_upscale_filter[64][8];
+extern __device__ const int16_t g_upscale_filter[64][8];  // 16-byte aligned rows
 extern __device__ int16_t g_gaussian[2048];
 // LFSR jump-ahead (7.18.3.2): column b of M^(82r) / M^(44r) is the state
 // reached from state 1<<b after 82r / 44r steps.

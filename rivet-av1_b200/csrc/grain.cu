@@ -341,10 +341,17 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
         const int key = int(item.frame) * 4 + p;
         if (key != loaded) {  // the plane's template and scaling table
           __syncthreads();
-          const int16_t* tg = &f.grain->tmpl[p][0][0];
+          // the template goes to shared memory as asynchronous copies, all
+          // in flight at once (a thread's 12 words would otherwise wait
+          // for each other's loads); the barrier before the stripe's
+          // samples follows the wait
+          const uint32_t* tg = reinterpret_cast<const uint32_t*>(&f.grain->tmpl[p][0][0]);
+          const uint32_t tbase = static_cast<uint32_t>(__cvta_generic_to_shared(T));
           for (int k = threadIdx.x; k < kTH * kTW / 2; k += 256)
-            reinterpret_cast<uint32_t*>(T)[k] = reinterpret_cast<const uint32_t*>(tg)[k];
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tbase + 4u * uint32_t(k)), "l"(tg + k)
+                         : "memory");
           for (int k = threadIdx.x; k < 256; k += 256) lut[k] = f.grain->lut[p][k];
+          asm volatile("cp.async.wait_all;" ::: "memory");
           loaded = key;
         }
       }

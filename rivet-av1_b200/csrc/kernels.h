@@ -61,7 +61,8 @@ cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
 
 // Super-resolution (superres.cu)
-void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// `row_max`: the most source samples in a row among the launch's frames.
+void launch_superres(const FrameDesc* frames, const Item* items, int n_items, int row_max, cudaStream_t s);
 // Sets superres_kernel's dynamic shared-memory limit on the current device.
 cudaError_t superres_init();
 

@@ -353,6 +353,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         plan.any_sr = true;
         d.up[k] = chain ? bump.plane(d.sr_w[k], ph, sb) : from_abi(j.out[k]);
         add_tiles(plan.sr_items, fi, k, 0, 1, ph, 1, 4);
+        plan.sr_row_max = std::max(plan.sr_row_max, d.sr_maxx[k] + 1);
         if (chain && d.stripes > 1) {
           const int lines = (d.stripes - 1) * 4;
           d.lines[k] = bump.plane(d.sr_w[k], lines, sb);
@@ -488,7 +489,8 @@ void launch_key(const Plan& plan, const void* meta, std::vector<uint64_t>& key) 
               plan.off_out, plan.off_copy, plan.off_edges_v, plan.off_edges_h, plan.off_counts,
               uint64_t(plan.any_lf) | uint64_t(plan.any_cdef) << 1 | uint64_t(plan.any_sr) << 2 |
                   uint64_t(plan.any_lr) << 3 | uint64_t(plan.any_grain) << 4 | uint64_t(plan.any_out) << 5 |
-                  uint64_t(plan.any_hlist) << 6});
+                  uint64_t(plan.any_hlist) << 6,
+              uint64_t(plan.sr_row_max)});
 }
 
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
@@ -529,7 +531,7 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
   mark(1);
   if (plan.any_cdef) launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), s);
   mark(2);
-  if (plan.any_sr) launch_superres(frames, items(plan.off_sr), int(plan.sr_items.size()), s);
+  if (plan.any_sr) launch_superres(frames, items(plan.off_sr), int(plan.sr_items.size()), plan.sr_row_max, s);
   mark(3);
   if (plan.any_lr) launch_lr(frames, items(plan.off_lr), int(plan.lr_items.size()), s);
   mark(4);

@@ -49,6 +49,7 @@ struct Plan {
   uint32_t edge_cap = 0;
   size_t scratch_bytes = 0;   // bytes of per-frame scratch (planes, grain)
   bool any_hlist = false;  // some plane's horizontal loop-filter edges run as their own pass
+  int sr_row_max = 0;      // superres: the most source samples in a row (sr_maxx + 1)
   bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
   // byte offsets of each list in the device meta buffer
   size_t off_frames = 0, off_lf = 0, off_lft = 0, off_cdef = 0, off_sr = 0, off_lr = 0, off_grain = 0, off_out = 0,

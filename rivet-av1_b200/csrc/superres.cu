@@ -9,23 +9,23 @@
 // Item kind 0: rows [y0, y1) of cdef -> up. Kind 1: line rows [y0, y1) of the
 // line buffer (4 per stripe boundary: rows B-2 .. B+1 of the boundary at B).
 // Each source row is staged once in shared memory (16-byte loads), then every
-// output sample reads its 8 taps from there.
+// output sample reads its 8 taps from there and its filter phase's 8
+// coefficients with one 16-byte load from global memory (through the L1),
+// so CTAs start without staging the filter table. The row buffer is sized
+// per launch to the widest source row among the launch's frames.
 #include "common.cuh"
 #include "kernels.h"
 
 namespace av1pf {
 
 namespace {
-constexpr int kMaxRow = 16384 + 16;  // source samples staged per row
+constexpr int kMaxRow = 16384 + 16;  // source samples staged per row, at most
 }
 
 __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restrict__ frames,
                                                        const Item* __restrict__ items, int n_items) {
   extern __shared__ __align__(16) uint8_t sr_smem[];
-  int16_t* filt = reinterpret_cast<int16_t*>(sr_smem);               // [64][8]
-  uint16_t* row = reinterpret_cast<uint16_t*>(sr_smem + 64 * 8 * 2);  // staged source row
-  for (int k = threadIdx.x; k < 64 * 8; k += blockDim.x) filt[k] = g_upscale_filter[k >> 3][k & 7];
-  __syncthreads();
+  uint16_t* row = reinterpret_cast<uint16_t*>(sr_smem);  // staged source row
   pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
@@ -79,7 +79,14 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
           const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
           const int px = int(src_x >> 14);
           const int phase = int((src_x & 0x3fff) >> 8);
-          const int16_t* fk = &filt[phase * 8];
+          const int4 fq = __ldg(reinterpret_cast<const int4*>(g_upscale_filter[phase]));
+          const uint32_t fw[4] = {uint32_t(fq.x), uint32_t(fq.y), uint32_t(fq.z), uint32_t(fq.w)};
+          int fk[8];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            fk[2 * k] = int(int16_t(uint16_t(fw[k] & 0xffffu)));
+            fk[2 * k + 1] = int(int16_t(uint16_t(fw[k] >> 16)));
+          }
           int sum = 0;
           if (px - 3 >= 0 && px + 4 <= max_x) {
 #pragma unroll
@@ -101,13 +108,13 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
 }
 
 cudaError_t superres_init() {
-  return cudaFuncSetAttribute(superres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              64 * 8 * 2 + kMaxRow * 2);
+  return cudaFuncSetAttribute(superres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxRow * 2);
 }
 
-void launch_superres(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
+void launch_superres(const FrameDesc* frames, const Item* items, int n_items, int row_max, cudaStream_t s) {
   if (n_items <= 0) return;
-  launch_pdl(superres_kernel, min(n_items, kItemGrid), 256, size_t(64 * 8 * 2 + kMaxRow * 2), s, frames, items,
+  const int row = min(max(row_max, 8), kMaxRow);
+  launch_pdl(superres_kernel, min(n_items, kItemGrid), 256, size_t((row * 2 + 15) / 16 * 16), s, frames, items,
              n_items);
 }
 

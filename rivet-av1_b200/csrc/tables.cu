@@ -15,7 +15,7 @@ __constant__ uint8_t c_tx_h[19] = AV1T_TX_HEIGHT;
 __constant__ uint8_t c_n4w[22] = AV1T_NUM_4X4_BLOCKS_WIDE;
 __constant__ uint8_t c_n4h[22] = AV1T_NUM_4X4_BLOCKS_HIGH;
 __constant__ int32_t c_sgr_params[16][4] = AV1T_SGR_PARAMS;
-__device__ int16_t g_upscale_filter[64][8] = AV1T_UPSCALE_FILTER;
+__device__ __align__(16) const int16_t g_upscale_filter[64][8] = AV1T_UPSCALE_FILTER;
 __device__ int16_t g_gaussian[2048] = AV1T_GAUSSIAN_SEQUENCE;
 __device__ uint16_t g_rng_jump82[73][16];
 __device__ uint16_t g_rng_jump44[73][16];
