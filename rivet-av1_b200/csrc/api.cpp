@@ -108,12 +108,25 @@ void Ctx::release(DevBuf& b) {
 // Plans `jobs`, sizes scratch/meta, uploads and launches on `s`.
 int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   std::string why;
-  int rc = build_plan(jobs, n, nullptr, plan, &why);
-  if (rc != AV1PF_OK) return set_error(why), rc;
-  if ((rc = ensure(scratch, plan.scratch_bytes + 256)) != AV1PF_OK) return rc;
-  rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why);
-  if (rc != AV1PF_OK) return set_error(why), rc;
-  if ((rc = ensure(meta, plan.meta_bytes + 256)) != AV1PF_OK) return rc;
+  int rc = AV1PF_OK;
+  // Jobs with the structure of the previous call (a decoder filtering frame
+  // after frame of one stream) get the same work lists: only the frame
+  // descriptors are rebuilt and uploaded, the lists already on the device
+  // stay. Anything else is planned in full.
+  structure_key(jobs, n, key_scratch);
+  const bool reuse = plan_ready && key_scratch == plan_key && plan_meta == meta.ptr && plan_scratch == scratch.ptr;
+  if (reuse) {
+    rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why, false);
+    if (rc != AV1PF_OK) return set_error(why), rc;
+  } else {
+    plan_ready = false;
+    rc = build_plan(jobs, n, nullptr, plan, &why);
+    if (rc != AV1PF_OK) return set_error(why), rc;
+    if ((rc = ensure(scratch, plan.scratch_bytes + 256)) != AV1PF_OK) return rc;
+    rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why);
+    if (rc != AV1PF_OK) return set_error(why), rc;
+    if ((rc = ensure(meta, plan.meta_bytes + 256)) != AV1PF_OK) return rc;
+  }
   // the pinned staging buffer is reused call after call: wait for the last
   // upload from it to finish before overwriting
   if (staged_once) {
@@ -121,8 +134,22 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
     if (e != cudaSuccess) return cuda_status(e, "staging wait");
   }
   if ((rc = ensure_host(meta_host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
-  pack_meta(plan, static_cast<uint8_t*>(meta_host.ptr));
-  cudaError_t e = cudaMemcpyAsync(meta.ptr, meta_host.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e;
+  if (reuse) {
+    const size_t fbytes = plan.frames.size() * sizeof(FrameDesc);
+    std::memcpy(static_cast<uint8_t*>(meta_host.ptr) + plan.off_frames, plan.frames.data(), fbytes);
+    e = cudaMemcpyAsync(static_cast<uint8_t*>(meta.ptr) + plan.off_frames,
+                        static_cast<uint8_t*>(meta_host.ptr) + plan.off_frames, fbytes, cudaMemcpyHostToDevice, s);
+  } else {
+    pack_meta(plan, static_cast<uint8_t*>(meta_host.ptr));
+    e = cudaMemcpyAsync(meta.ptr, meta_host.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+      plan_key = key_scratch;
+      plan_meta = meta.ptr;
+      plan_scratch = scratch.ptr;
+      plan_ready = true;
+    }
+  }
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
   cudaEventRecord(staged, s);
   staged_once = true;

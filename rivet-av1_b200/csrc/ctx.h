@@ -82,6 +82,12 @@ struct Ctx {
   cudaError_t pipe_streams();  // creates the streams and events on first use
   HostBuf meta_host;
   Plan plan;
+  // the structure the device's work lists in `meta` were uploaded for
+  // (structure_key), and the buffers they were laid out in
+  std::vector<int64_t> plan_key, key_scratch;
+  const void* plan_meta = nullptr;
+  const void* plan_scratch = nullptr;
+  bool plan_ready = false;
   // per-frame graphs, by launch structure (least recently used replaced)
   static constexpr int kGraphs = 8;
   GraphEntry graphs[kGraphs];

@@ -168,8 +168,23 @@ int validate_params(const av1pf_frame_info* i, const av1pf_params* p, std::strin
   return AV1PF_OK;
 }
 
-int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, std::string* why) {
-  plan = Plan{};
+int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, std::string* why, bool items) {
+  plan.frames.clear();
+  plan.scratch_bytes = 0;
+  if (items) {
+    // the lists keep their capacity from call to call (a chain call plans
+    // one frame of the same shape again and again)
+    for (auto* v : {&plan.lf_items, &plan.lft_items, &plan.cdef_items, &plan.sr_items, &plan.lr_items,
+                    &plan.grain_items, &plan.out_items, &plan.copy_items})
+      v->clear();
+    plan.edge_cap = 0;
+    plan.any_hlist = false;
+    plan.sr_row_max = 0;
+    plan.any_lf = plan.any_cdef = plan.any_sr = plan.any_lr = plan.any_grain = plan.any_out = false;
+    plan.off_frames = plan.off_lf = plan.off_lft = plan.off_cdef = plan.off_sr = plan.off_lr = plan.off_grain =
+        plan.off_out = plan.off_copy = plan.off_edges_v = plan.off_edges_h = plan.off_counts = plan.meta_bytes =
+            plan.upload_bytes = 0;
+  }
   if (n <= 0 || n > 65535) return fail(why, "bad job count"), AV1PF_ERR_INVALID_INPUT;
   Bump bump{scratch_base};
   uint32_t cap = 0;
@@ -250,12 +265,12 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       const int gw = i->mi_cols >> sx, gh = i->mi_rows >> sy;
       if (j.in_place_lf) {
         d.cur[k] = d.in[k];
-        add_tiles(plan.lf_items, fi, k, 2, gw * 4, gh * 4, kTile, kTile);
+        if (items) add_tiles(plan.lf_items, fi, k, 2, gw * 4, gh * 4, kTile, kTile);
       } else if (!tiles) {
         // copy in -> cur and decide every 4x4 edge into the two edge lists
         d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
         const int W = d.in[k].w, H = d.in[k].h;
-        for (int y = 0; y < H; y += kTile)
+        for (int y = 0; items && y < H; y += kTile)
           for (int x = 0; x < W; x += kTile) {
             Item it{};
             it.frame = uint16_t(fi);
@@ -265,7 +280,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
             it.y0 = uint16_t(y);
             it.x1 = uint16_t(std::min(x + kTile, W));
             it.y1 = uint16_t(std::min(y + kTile, H));
-            plan.lf_items.push_back(it);
+            if (items) plan.lf_items.push_back(it);
           }
         plan.any_hlist = true;
       } else {
@@ -273,7 +288,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         // horizontal edges go to the edge list
         d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
         const int W = d.in[k].w, H = d.in[k].h;
-        for (int y = 0; y < H; y += kTile)
+        for (int y = 0; items && y < H; y += kTile)
           for (int x = 0; x < W; x += kTile) {
             Item it{};
             it.frame = uint16_t(fi);
@@ -283,7 +298,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
             it.y0 = uint16_t(y);
             it.x1 = uint16_t(std::min(x + kTile, W));
             it.y1 = uint16_t(std::min(y + kTile, H));
-            plan.lft_items.push_back(it);
+            if (items) plan.lft_items.push_back(it);
           }
         if (fuse_h) {
           d.lfh_mask |= 1 << k;
@@ -311,14 +326,14 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     if (cdef_on) {
       plan.any_cdef = true;
       const int sbr = (i->mi_rows + 15) / 16, sbc = (i->mi_cols + 15) / 16;
-      for (int r = 0; r < sbr; r++)
+      for (int r = 0; items && r < sbr; r++)
         for (int c = 0; c < sbc; c++) {
           Item it{};
           it.frame = uint16_t(fi);
           it.kind = uint8_t(d.lfh_mask ? 1 : 0);
           it.x0 = uint16_t(c);
           it.y0 = uint16_t(r);
-          plan.cdef_items.push_back(it);
+          if (items) plan.cdef_items.push_back(it);
         }
     } else if (cdef_stage && !chain) {
       // the reference returns a clone of cur when CDEF is off: copy the MI area
@@ -326,7 +341,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         d.in[k] = d.cur[k];
         d.cur[k] = from_abi(j.out[k]);
         const int sx = k ? d.ssx : 0, sy = k ? d.ssy : 0;
-        add_tiles(plan.copy_items, fi, k, 1, (i->mi_cols * 4) >> sx, (i->mi_rows * 4) >> sy, kTile, kTile);
+        if (items) add_tiles(plan.copy_items, fi, k, 1, (i->mi_cols * 4) >> sx, (i->mi_rows * 4) >> sy, kTile, kTile);
       }
     }
     // --- superres: postfilter.rs:521-566, decoder/mod.rs:752-757 ---
@@ -352,12 +367,12 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       if (sr_stage) {
         plan.any_sr = true;
         d.up[k] = chain ? bump.plane(d.sr_w[k], ph, sb) : from_abi(j.out[k]);
-        add_tiles(plan.sr_items, fi, k, 0, 1, ph, 1, 4);
+        if (items) add_tiles(plan.sr_items, fi, k, 0, 1, ph, 1, 4);
         plan.sr_row_max = std::max(plan.sr_row_max, d.sr_maxx[k] + 1);
         if (chain && d.stripes > 1) {
           const int lines = (d.stripes - 1) * 4;
           d.lines[k] = bump.plane(d.sr_w[k], lines, sb);
-          add_tiles(plan.sr_items, fi, k, 1, 1, lines, 1, 4);
+          if (items) add_tiles(plan.sr_items, fi, k, 1, 1, lines, 1, 4);
         }
       } else {
         d.up[k] = d.cdef[k];
@@ -379,7 +394,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         const int us = has_lr ? p->loop_restoration_size[k] : 1 << 30;
         const int ucols = has_lr ? p->lr_unit_cols[k] : 1;
         const int rw = j.lr_cols == 32 ? 32 : kTile;  // rectangle width (the kernel takes <= 64)
-        for (int s = 0; s < d.stripes; s++) {
+        for (int s = 0; items && s < d.stripes; s++) {
           const int sy = k ? d.ssy : 0;
           const int ss = (-8 + s * 64) >> sy;
           const int y0 = std::max(ss, 0), y1 = std::min(ss + (64 >> sy) - 1, plane_h(i, k) - 1);
@@ -397,7 +412,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
               it.x1 = uint16_t(std::min(cx + rw, x1 + 1));
               it.a = uint16_t(s);
               it.b = uint16_t(uc);
-              plan.lr_items.push_back(it);
+              if (items) plan.lr_items.push_back(it);
             }
           }
         }
@@ -420,7 +435,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         // 256 columns by one noise stripe (32 rows, 16 in vertically subsampled chroma)
         if (!d.lr_pack) {
           plan.any_out = true;
-          add_tiles(plan.out_items, fi, k, 0, pw, ph, 256, k ? 32 >> i->subsampling_y : 32);
+          if (items) add_tiles(plan.out_items, fi, k, 0, pw, ph, 256, k ? 32 >> i->subsampling_y : 32);
         }
       }
       if (p->film_grain.apply) {
@@ -432,13 +447,14 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
         d.grain_off = bump.take(size_t(d.grain_ns) * size_t(d.grain_nb));
         Item it{};
         it.frame = uint16_t(fi);
-        plan.grain_items.push_back(it);
+        if (items) plan.grain_items.push_back(it);
       }
     }
     plan.frames.push_back(d);
   }
-  plan.edge_cap = cap;
   plan.scratch_bytes = align_up(bump.used, 256);
+  if (!items) return AV1PF_OK;  // the lists and their layout are the previous call's
+  plan.edge_cap = cap;
   // meta layout: [frames][items...] uploaded, then [edges v][edges h][counts] device-only
   size_t off = 0;
   auto place = [&](size_t bytes) {
@@ -462,6 +478,28 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   plan.off_counts = place(16);
   plan.meta_bytes = align_up(off, 256);
   return AV1PF_OK;
+}
+
+void structure_key(const FrameJob* jobs, int n, std::vector<int64_t>& key) {
+  key.clear();
+  key.push_back(n);
+  for (int fi = 0; fi < n; fi++) {
+    const FrameJob& j = jobs[fi];
+    const av1pf_frame_info* i = j.info;
+    const av1pf_params* p = j.params;
+    key.insert(key.end(), {i->bit_depth, i->sample_bytes, i->subsampling_x, i->subsampling_y, i->num_planes,
+                           i->frame_width, i->frame_height, i->upscaled_width, i->mi_rows, i->mi_cols,
+                           int64_t(j.stages), int64_t(j.in_place_lf), j.lf_mode, j.lr_cols,
+                           int64_t(j.frame_out != nullptr), int64_t(j.maps != nullptr),
+                           int64_t(p->loop_filter_level[0] != 0 || p->loop_filter_level[1] != 0),
+                           int64_t(p->loop_filter_level[2] != 0), int64_t(p->loop_filter_level[3] != 0),
+                           p->cdef_enabled, p->use_superres, p->uses_lr, p->film_grain.apply});
+    for (int k = 0; k < 3; k++) {
+      key.insert(key.end(), {p->frame_restoration_type[k], p->loop_restoration_size[k], p->lr_unit_rows[k],
+                             p->lr_unit_cols[k]});
+      if (k < i->num_planes && j.in) key.insert(key.end(), {j.in[k].width, j.in[k].height});
+    }
+  }
 }
 
 void pack_meta(const Plan& plan, uint8_t* host) {

@@ -63,8 +63,14 @@ int validate_params(const av1pf_frame_info* info, const av1pf_params* p, std::st
 
 // Builds the plan of `jobs`. Scratch pointers are laid out from
 // `scratch_base` (pass nullptr first to learn plan.scratch_bytes, then again
-// with the allocation). Returns AV1PF_OK or an error code.
-int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, std::string* why);
+// with the allocation). With items == false only the descriptors are built:
+// the work lists, flags and layout stay those of the previous call, for jobs
+// with the same structure (structure_key). Returns AV1PF_OK or an error code.
+int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, std::string* why, bool items = true);
+
+// Everything build_plan's work lists, flags, layout and scratch layout
+// depend on: jobs with equal keys get equal lists (their descriptors differ).
+void structure_key(const FrameJob* jobs, int n, std::vector<int64_t>& key);
 
 // Serialises the plan's descriptors and items into `host` (plan.upload_bytes
 // long) in the layout of the device meta buffer.
