@@ -105,54 +105,80 @@ void Ctx::release(DevBuf& b) {
   b.size = 0;
 }
 
-// Plans `jobs`, sizes scratch/meta, uploads and launches on `s`.
+// Plans `jobs`, sizes scratch and a descriptor buffer, uploads and launches
+// on `s`.
 int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   std::string why;
   int rc = AV1PF_OK;
   // Jobs with the structure of the previous call (a decoder filtering frame
   // after frame of one stream) get the same work lists: only the frame
-  // descriptors are rebuilt and uploaded, the lists already on the device
-  // stay. Anything else is planned in full.
+  // descriptors are rebuilt, and uploaded where the buffer already holds
+  // the lists. Anything else is planned in full.
   structure_key(jobs, n, key_scratch);
-  const bool reuse = plan_ready && key_scratch == plan_key && plan_meta == meta.ptr && plan_scratch == scratch.ptr;
-  if (reuse) {
+  if (host_ready && key_scratch == host_key) {
     rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why, false);
     if (rc != AV1PF_OK) return set_error(why), rc;
   } else {
-    plan_ready = false;
+    host_ready = false;
     rc = build_plan(jobs, n, nullptr, plan, &why);
     if (rc != AV1PF_OK) return set_error(why), rc;
     if ((rc = ensure(scratch, plan.scratch_bytes + 256)) != AV1PF_OK) return rc;
     rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why);
     if (rc != AV1PF_OK) return set_error(why), rc;
-    if ((rc = ensure(meta, plan.meta_bytes + 256)) != AV1PF_OK) return rc;
+    host_key = key_scratch;
+    host_ready = true;
   }
-  // the pinned staging buffer is reused call after call: wait for the last
-  // upload from it to finish before overwriting
-  if (staged_once) {
-    cudaError_t e = cudaEventSynchronize(staged);
-    if (e != cudaSuccess) return cuda_status(e, "staging wait");
+  // Two descriptor buffers in turn: call k's upload runs on its own stream
+  // while call k-1's kernels read the other buffer, and a buffer is
+  // rewritten only after the launches that read it are done.
+  cudaError_t e = cudaSuccess;
+  if (!upload) {
+    e = cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking);
+    for (MetaSlot& q : metas)
+      for (cudaEvent_t* ev : {&q.uploaded, &q.done})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_status(e, "descriptor stream");
   }
-  if ((rc = ensure_host(meta_host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
-  cudaError_t e;
-  if (reuse) {
+  MetaSlot& m = metas[meta_next];
+  meta_next ^= 1;
+  if (m.dev.size < plan.meta_bytes + 256) {
+    if (m.used && (e = cudaEventSynchronize(m.done)) != cudaSuccess) return cuda_status(e, "descriptor wait");
+    m.ready = false;
+    if ((rc = ensure(m.dev, plan.meta_bytes + 256)) != AV1PF_OK) return rc;
+  }
+  // the pinned staging buffer: its last upload must be done before it is
+  // overwritten
+  if (m.used && (e = cudaEventSynchronize(m.uploaded)) != cudaSuccess) return cuda_status(e, "staging wait");
+  if ((rc = ensure_host(m.host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
+  if (m.used) cudaStreamWaitEvent(upload, m.done, 0);
+  uint8_t* dmeta = static_cast<uint8_t*>(m.dev.ptr);
+  uint8_t* hmeta = static_cast<uint8_t*>(m.host.ptr);
+  if (m.ready && m.key == key_scratch) {
     const size_t fbytes = plan.frames.size() * sizeof(FrameDesc);
-    std::memcpy(static_cast<uint8_t*>(meta_host.ptr) + plan.off_frames, plan.frames.data(), fbytes);
-    e = cudaMemcpyAsync(static_cast<uint8_t*>(meta.ptr) + plan.off_frames,
-                        static_cast<uint8_t*>(meta_host.ptr) + plan.off_frames, fbytes, cudaMemcpyHostToDevice, s);
+    std::memcpy(hmeta + plan.off_frames, plan.frames.data(), fbytes);
+    e = cudaMemcpyAsync(dmeta + plan.off_frames, hmeta + plan.off_frames, fbytes, cudaMemcpyHostToDevice, upload);
   } else {
-    pack_meta(plan, static_cast<uint8_t*>(meta_host.ptr));
-    e = cudaMemcpyAsync(meta.ptr, meta_host.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, s);
+    m.ready = false;
+    pack_meta(plan, hmeta);
+    e = cudaMemcpyAsync(dmeta, hmeta, plan.upload_bytes, cudaMemcpyHostToDevice, upload);
     if (e == cudaSuccess) {
-      plan_key = key_scratch;
-      plan_meta = meta.ptr;
-      plan_scratch = scratch.ptr;
-      plan_ready = true;
+      m.key = key_scratch;
+      m.ready = true;
     }
   }
+  if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, upload);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, m.uploaded, 0);
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
-  cudaEventRecord(staged, s);
-  staged_once = true;
+  m.used = true;
+  rc = launch_on(dmeta, s);
+  cudaEventRecord(m.done, s);
+  return rc;
+}
+
+// Launches the planned stages reading descriptor buffer `dmeta`: directly
+// with stage events when profiling, else by replaying a captured graph.
+int Ctx::launch_on(uint8_t* dmeta, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
   const cudaEvent_t* ev = nullptr;
   if (prof) {
     const int slot = prof_next;
@@ -165,7 +191,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   }
   if (ev) {
     // profiled calls launch directly, with the stage events between stages
-    launch_plan(plan, static_cast<uint8_t*>(meta.ptr), s, side, fork, join, ev);
+    launch_plan(plan, dmeta, s, side, fork, join, ev);
     e = cudaGetLastError();
     return cuda_status(e, "kernel launch");
   }
@@ -173,7 +199,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // flags, meta buffer) replay one captured graph: the descriptors and work
   // lists it reads were just uploaded to the same addresses.
   std::vector<uint64_t> key;
-  launch_key(plan, meta.ptr, key);
+  launch_key(plan, dmeta, key);
   GraphEntry* g = nullptr;
   for (GraphEntry& c : graphs)
     if (c.exec && c.key == key) g = &c;
@@ -193,7 +219,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
       CaptureScope cs;
       e = cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
-        launch_plan(plan, static_cast<uint8_t*>(meta.ptr), capture, side, fork, join, nullptr);
+        launch_plan(plan, dmeta, capture, side, fork, join, nullptr);
         e = cudaStreamEndCapture(capture, &graph);
       }
       kernels = cs.launches();
@@ -310,8 +336,7 @@ int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out) {
   if ((e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaEventCreateWithFlags(&c->staged, cudaEventDisableTiming)) != cudaSuccess) {
+      (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) != cudaSuccess) {
     delete c;
     return cuda_status(e, "stream/event create");
   }
@@ -324,7 +349,13 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
   ctx->release(ctx->scratch);
-  ctx->release(ctx->meta);
+  for (Ctx::MetaSlot& m : ctx->metas) {
+    ctx->release(m.dev);
+    if (m.host.ptr) cudaFreeHost(m.host.ptr);
+    for (cudaEvent_t ev : {m.uploaded, m.done})
+      if (ev) cudaEventDestroy(ev);
+  }
+  if (ctx->upload) cudaStreamDestroy(ctx->upload);
   for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame}) ctx->release(*b);
   for (Ctx::PipeSlot& ps : ctx->pipe) {
     for (auto* b : {&ps.in, &ps.ref, &ps.maps, &ps.frame}) ctx->release(*b);
@@ -333,7 +364,6 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   }
   if (ctx->pipe_up) cudaStreamDestroy(ctx->pipe_up);
   if (ctx->pipe_down) cudaStreamDestroy(ctx->pipe_down);
-  if (ctx->meta_host.ptr) cudaFreeHost(ctx->meta_host.ptr);
   for (GraphEntry& g : ctx->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (ctx->capture) cudaStreamDestroy(ctx->capture);
@@ -341,7 +371,6 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   cudaStreamDestroy(ctx->own);
   cudaEventDestroy(ctx->fork);
   cudaEventDestroy(ctx->join);
-  cudaEventDestroy(ctx->staged);
   for (auto& slot : ctx->prof_ev)
     for (auto& e : slot)
       if (e) cudaEventDestroy(e);

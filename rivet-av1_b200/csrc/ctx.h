@@ -65,9 +65,8 @@ struct Ctx {
   int threads = 2;
   cudaStream_t side = nullptr;  // grain templates beside the chain
   cudaStream_t own = nullptr;   // the host-buffer entry points
-  cudaEvent_t fork = nullptr, join = nullptr, staged = nullptr;
-  bool staged_once = false;
-  DevBuf scratch, meta;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  DevBuf scratch;
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
   // av1pf_chain_host_many: device frame slots used in turn, with the events
   // that order a slot's upload (pipe_up), chain (own) and download
@@ -80,14 +79,23 @@ struct Ctx {
   PipeSlot pipe[kPipeSlots];
   cudaStream_t pipe_up = nullptr, pipe_down = nullptr;
   cudaError_t pipe_streams();  // creates the streams and events on first use
-  HostBuf meta_host;
   Plan plan;
-  // the structure the device's work lists in `meta` were uploaded for
-  // (structure_key), and the buffers they were laid out in
-  std::vector<int64_t> plan_key, key_scratch;
-  const void* plan_meta = nullptr;
-  const void* plan_scratch = nullptr;
-  bool plan_ready = false;
+  // the structure `plan`'s work lists were built for (structure_key)
+  std::vector<int64_t> host_key, key_scratch;
+  bool host_ready = false;
+  // descriptor buffers used in turn: device copy, pinned staging, the
+  // upload's and the reading launches' events, and the structure whose work
+  // lists the device copy holds
+  struct MetaSlot {
+    DevBuf dev;
+    HostBuf host;
+    cudaEvent_t uploaded = nullptr, done = nullptr;
+    bool used = false, ready = false;
+    std::vector<int64_t> key;
+  };
+  MetaSlot metas[2];
+  int meta_next = 0;
+  cudaStream_t upload = nullptr;  // descriptor uploads
   // per-frame graphs, by launch structure (least recently used replaced)
   static constexpr int kGraphs = 8;
   GraphEntry graphs[kGraphs];
@@ -114,6 +122,7 @@ struct Ctx {
   int ensure_host(HostBuf& b, size_t bytes);
   void release(DevBuf& b);
   int run(const FrameJob* jobs, int n, cudaStream_t s);
+  int launch_on(uint8_t* dmeta, cudaStream_t s);
 };
 
 void set_error(const std::string& s);
