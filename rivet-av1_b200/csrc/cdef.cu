@@ -4,8 +4,12 @@
 // cdef_direction, cdef_filter, cdef_filter_block) and src/dsp/cdef.rs:13-90
 // (Taps, constrain, filter_scalar).
 //
-// One CTA per 64x64 luma superblock (and its chroma): the superblock plus a
-// 2-sample border of every plane is staged in shared memory as int16 with
+// One CTA per superblock (64x64 luma and its chroma; R = 64 rows, 256
+// threads), or per half superblock (R = 32 rows, 128 threads) when a launch
+// has at most one wave of superblocks: 510 superblocks of a 1080p frame
+// would leave 66 SMs with 4 and 82 with 3, 1020 halves spread within 2%.
+// The rows plus a 2-sample border of every plane are staged in shared
+// memory as int16 with
 // unavailable samples (outside the frame's mode-info area, postfilter.rs:
 // 421-422, 464-488) stored as -32768. That value needs no special case:
 // constrain() of a difference that large is 0 for every strength/damping
@@ -21,17 +25,18 @@ namespace av1pf {
 
 namespace {
 
-// Shared-memory window of one plane: up to 86 rows (64 + 2*2, or 64 + 2*11
+// Shared-memory window of one plane: up to 54 rows (32 + 2*2, or 32 + 2*11
 // with the horizontal loop-filter pass fused in) x 80 columns
 // (64 + 8 on each side, so global loads stay 8-sample aligned), row stride
 // 82 int16 = 41 words: a warp's 4 rows x 8 blocks of centre loads then hit
 // 32 different banks.
 constexpr int kS = 82;
-constexpr int kTopLfh = 11;  // rows above (and below) the superblock with the horizontal LF pass fused
-constexpr int kRows = 64 + 2 * kTopLfh;  // 86 (68 used without the fused pass)
+constexpr int kTopLfh = 11;     // rows above (and below) with the horizontal LF pass fused
 constexpr int kColOff = 8;       // window column of plane x = px0
 constexpr int16_t kNA = -32768;  // unavailable sample
-constexpr int kCdefSmem = 3 * kRows * kS * 2;  // dynamic shared memory: the three windows
+// dynamic shared memory of the three windows: R + 2*2 rows, or R + 2*11 with
+// the horizontal loop-filter pass fused in
+constexpr int cdef_smem(int R, bool lfh) { return 3 * (R + 2 * (lfh ? kTopLfh : 2)) * kS * 2; }
 
 // Per 8x8 block and plane: strengths, tap weights and window offsets.
 struct BlkTaps {
@@ -204,19 +209,20 @@ __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int one
   c2 = cdef_cost_of<P + 4>(b);
 }
 
-// Stages plane p of superblock (sc, sr) with `top` rows above and below
-// (the 2-sample CDEF border, or 11 with the horizontal loop-filter pass) into
-// the window `wp` as int16, samples outside the mode-info area as kNA.
-// Window rows are NCH chunks of 8 samples (the first chunk starts 8 samples
-// left of the superblock, so loads stay 8-sample aligned); loads issue two
-// at a time before their stores.
-template <int SX>
-__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int sr, int top, int16_t* wp, int tid) {
+// Stages plane p of the half superblock at superblock column sc and luma
+// row y0 with `top` rows above and below (the 2-sample CDEF border, or 11
+// with the horizontal loop-filter pass) into the window `wp` as int16,
+// samples outside the mode-info area as kNA. Window rows are NCH chunks of 8
+// samples (the first chunk starts 8 samples left of the superblock, so loads
+// stay 8-sample aligned); loads issue two at a time before their stores.
+template <int R, int SX>
+__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int y0, int top, int16_t* wp, int tid) {
+  constexpr int NT = 4 * R;
   constexpr int NCH = ((64 >> SX) + 16) / 8;
-  constexpr int kSlots = (kRows * NCH + 255) / 256;
+  constexpr int kSlots = ((R + 2 * kTopLfh) * NCH + NT - 1) / NT;
   const int sy = plane_ssy(f, p), sb = f.sb;
-  const int bh = (64 >> sy) + 2 * top;
-  const int px0 = (sc * 64) >> SX, py0 = ((sr * 64) >> sy) - top;
+  const int bh = (R >> sy) + 2 * top;
+  const int px0 = (sc * 64) >> SX, py0 = (y0 >> sy) - top;
   const int xlim = (f.mi_cols * 4) >> SX, ylim = (f.mi_rows * 4) >> sy;
   const DPlane src = f.cur[p];
   // chunk class: 0 none, 1 unavailable, 2 inside (vector load), 3 straddles the edge
@@ -230,7 +236,7 @@ __device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, i
     uint4 q[2];
 #pragma unroll
     for (int m = 0; m < 2; m++) {
-      const int k = tid + 256 * (m0 + m), r = k / NCH, ch = k - r * NCH;
+      const int k = tid + NT * (m0 + m), r = k / NCH, ch = k - r * NCH;
       const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
       if (m0 + m < kSlots && kind_of(r, gy, gx0) == 2) {
         const uint8_t* rowp = src.p + int64_t(gy) * src.stride * sb;
@@ -245,7 +251,7 @@ __device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, i
 #pragma unroll
     for (int m = 0; m < 2; m++) {
       if (m0 + m >= kSlots) continue;
-      const int k = tid + 256 * (m0 + m), r = k / NCH, ch = k - r * NCH;
+      const int k = tid + NT * (m0 + m), r = k / NCH, ch = k - r * NCH;
       const int gy = py0 + r, gx0 = px0 - kColOff + ch * 8;
       const int kind = kind_of(r, gy, gx0);
       if (kind == 0) continue;
@@ -286,21 +292,24 @@ __device__ __noinline__ void lfh_lane(int16_t* q0p, int code, bool chroma, int b
 
 // The horizontal loop-filter edges (postfilter.rs:67-104 pass 1) of plane p
 // that change rows of the staged window: edges at plane rows py0-4 ..
-// py0+bh+4 across the superblock's columns and one 4x4 column on each side.
+// py0+bh+4 (py0 the half's first row) across the superblock's columns and
+// one 4x4 column on each side.
 // Every edge reads at most 7 rows on either side, which the 11-row halo
 // holds, so the window ends up holding the loop filter's output on the
 // rows CDEF reads. Edges of a pass never touch each other's samples in a
 // conformant frame, so they run in parallel in place.
-__device__ __forceinline__ void lfh_window(const FrameDesc& f, const LfTables& tb, int p, int sc, int sr,
+template <int R>
+__device__ __forceinline__ void lfh_window(const FrameDesc& f, const LfTables& tb, int p, int sc, int y0,
                                            int16_t* wp, uint16_t* hdec, int tid) {
+  constexpr int NT = 4 * R;
   const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-  const int bhs = 64 >> sy;
-  const int px0 = (sc * 64) >> sx, py0 = (sr * 64) >> sy;
+  const int bhs = R >> sy;
+  const int px0 = (sc * 64) >> sx, py0 = y0 >> sy;
   const int cx0 = (px0 >> 2) - 1, cy0 = (py0 >> 2) - 1;
   const int ncx = ((64 >> sx) >> 2) + 2;  // 18 or 10
-  const int ncy = (bhs >> 2) + 3;         // 19 or 11
+  const int ncy = (bhs >> 2) + 3;         // 19, 11 or 7
   const int gw = f.mi_cols >> sx, gh = f.mi_rows >> sy;
-  for (int k = tid; k < ncy * 18; k += 256) {
+  for (int k = tid; k < ncy * 18; k += NT) {
     const int cyi = k / 18, cxi = k - cyi * 18;
     const int cx = cx0 + cxi, cy = cy0 + cyi;
     int dv = 0, dh = 0;
@@ -309,7 +318,7 @@ __device__ __forceinline__ void lfh_window(const FrameDesc& f, const LfTables& t
   }
   __syncthreads();
   const int bd = f.bd, sharp = f.sharpness;
-  for (int k = tid; k < ncy * 18 * 4; k += 256) {
+  for (int k = tid; k < ncy * 18 * 4; k += NT) {
     const int lane = k & 3, cell = k >> 2;
     const int d = hdec[cell];
     if (!d) continue;
@@ -328,35 +337,43 @@ __device__ __forceinline__ void lfh_window(const FrameDesc& f, const LfTables& t
 
 // Rows B-2 .. B+1 of the stripe boundary B inside superblock row sr (the
 // loop filter's output, which loop restoration reads across the boundary)
-// from the window to f.prelf[p], over the superblock's columns.
+// from the window to f.prelf[p], over the superblock's columns. B is 8 luma
+// rows above the superblock row's end: a half superblock CTA writes them
+// from the bottom half (the window starting R rows above the row's end).
+template <int R>
 __device__ __forceinline__ void write_prelf(const FrameDesc& f, int p, int sc, int sr, const int16_t* wp, int tid) {
+  constexpr int NT = 4 * R;
   const DPlane dst = f.prelf[p];
   const int b = sr + 1;  // the boundary inside superblock row sr
   if (!dst.p || b >= f.stripes) return;
   const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
-  const int px0 = (sc * 64) >> sx, py0 = (sr * 64) >> sy;
+  const int px0 = (sc * 64) >> sx, py0 = (sr * 64 + 64 - R) >> sy;  // the window's first plane row
   const int B = (64 * b - 8) >> sy;
   const int xlim = (f.mi_cols * 4) >> sx, ylim = (f.mi_rows * 4) >> sy;
-  const int w = 64 >> sx;
-  const int j = tid / w, c = tid - j * w;  // 4 rows x w columns
-  if (j >= 4) return;
-  const int y = B - 2 + j, x = px0 + c;
-  if (y >= ylim || x >= xlim) return;
-  st_sample(dst, f.sb, x, (b - 1) * 4 + j, wp[(y - py0 + kTopLfh) * kS + c + kColOff]);
+  const int ws = 6 - sx;  // log2 of the superblock's width in the plane
+  for (int k = tid; k < (4 << ws); k += NT) {
+    const int j = k >> ws, c = k & ((1 << ws) - 1);  // 4 rows x 64 >> sx columns
+    const int y = B - 2 + j, x = px0 + c;
+    if (y < ylim && x < xlim)
+      st_sample(dst, f.sb, x, (b - 1) * 4 + j, wp[(y - py0 + kTopLfh) * kS + c + kColOff]);
+  }
 }
 
-// Item: superblock (x0 = SB column, y0 = SB row). 256 threads.
-// Item kind 1: the frame's horizontal loop-filter edges (planes in
-// f.lfh_mask) are filtered here, on the staged window, before CDEF.
-__global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restrict__ frames,
-                                                   const Item* __restrict__ items, int n_items) {
-  extern __shared__ __align__(16) int16_t cdef_win[];  // [3][kRows * kS]
-  auto win = [&](int p) { return cdef_win + p * kRows * kS; };  // plane p's window
-  __shared__ int32_t cost[64][8];
-  __shared__ BlkTaps taps[3][64];
-  __shared__ uint8_t bstate[64];  // 0 = outside the MI area, 1 = copy, 2 = filter
+// Item: R luma rows of a superblock (x0 = SB column, y0 = SB row, a = which
+// R rows). 4R threads, one warp per 8x8 block row. Item kind 1: the frame's
+// horizontal loop-filter edges (planes in f.lfh_mask) are filtered here, on
+// the staged window, before CDEF. `wrows` is the rows of one plane's window
+// (R + 22 when the launch has kind-1 items, else R + 4).
+template <int R>
+__global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* __restrict__ frames,
+                                                           const Item* __restrict__ items, int n_items, int wrows) {
+  extern __shared__ __align__(16) int16_t cdef_win[];  // [3][wrows * kS]
+  auto win = [&](int p) { return cdef_win + p * wrows * kS; };  // plane p's window
+  __shared__ int32_t cost[R][8];
+  __shared__ BlkTaps taps[3][R];
+  __shared__ uint8_t bstate[R];  // 0 = outside the MI area, 1 = copy, 2 = filter
   const LfTables& tb = g_lf_tables;
-  __shared__ uint16_t hdec[19 * 18];  // horizontal-edge decisions of one plane
+  __shared__ uint16_t hdec[(R / 4 + 3) * 18];  // horizontal-edge decisions of one plane
   __shared__ int16_t doff[8][2];      // window offsets of CDEF_DIRECTIONS
   __shared__ uint8_t uvdir[2][2][8];  // CDEF_UV_DIR
   __shared__ int s_one;               // 1, opaque to the compiler (see cdef_tap)
@@ -369,6 +386,7 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
     const int sc = item.x0, sr = item.y0;
+    const int y0 = sr * 64 + item.a * R;  // luma row of the CTA's first row
     const int np = f.np, sb = f.sb;
     const int cs = f.bd - 8;
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
@@ -377,9 +395,9 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
     // (the maps are inputs of the chain: read before waiting for the loop filter)
     uint8_t st = 0;
-    if (tid < 64) {
+    if (tid < R) {
       const int by = tid >> 3, bx = tid & 7;
-      const int r = sr * 16 + 2 * by, c = sc * 16 + 2 * bx;
+      const int r = (y0 >> 2) + 2 * by, c = sc * 16 + 2 * bx;
       if (r < f.mi_rows && c < f.mi_cols) {
         st = 1;
         if (idx >= 0) {
@@ -393,20 +411,21 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     }
     pdl_wait();       // the loop filter's output is complete past this point
     __syncthreads();  // the previous item is done with the windows and block states
-    if (tid < 64) bstate[tid] = st;
+    if (tid < R) bstate[tid] = st;
     // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
     for (int p = 0; p < np; p++) {
       if (plane_ssx(f, p))
-        stage_plane<1>(f, p, sc, sr, top, win(p), tid);
+        stage_plane<R, 1>(f, p, sc, y0, top, win(p), tid);
       else
-        stage_plane<0>(f, p, sc, sr, top, win(p), tid);
+        stage_plane<R, 0>(f, p, sc, y0, top, win(p), tid);
     }
     if (lfh) {
       __syncthreads();
       for (int p = 0; p < np; p++)
-        if ((f.lfh_mask >> p) & 1) lfh_window(f, tb, p, sc, sr, win(p), hdec, tid);
-      for (int p = 0; p < np; p++)
-        if ((f.lfh_mask >> p) & 1) write_prelf(f, p, sc, sr, win(p), tid);
+        if ((f.lfh_mask >> p) & 1) lfh_window<R>(f, tb, p, sc, y0, win(p), hdec, tid);
+      if (y0 + R == sr * 64 + 64)  // the rows that end the superblock row
+        for (int p = 0; p < np; p++)
+          if ((f.lfh_mask >> p) & 1) write_prelf<R>(f, p, sc, sr, win(p), tid);
     }
     __syncthreads();
     // --- direction search (postfilter.rs:345-401): each thread two directions of one block ---
@@ -429,7 +448,7 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
     }
     __syncthreads();
     // --- per-block strengths and taps (postfilter.rs:311-341) ---
-    if (tid < 64) {
+    if (tid < R) {
       const int b = tid;
       int lp = 0, ls = 0, ld = 0, up = 0, us = 0, ud = 0;
       bool filt = bstate[b] == 2;
@@ -493,7 +512,7 @@ __global__ void __launch_bounds__(256, 4) cdef_kernel(const FrameDesc* __restric
           }
         }
 #undef CDEF_ROW
-        const int gx = ((sc * 64) >> sx) + lx, gy = ((sr * 64) >> sy) + ly;
+        const int gx = ((sc * 64) >> sx) + lx, gy = (y0 >> sy) + ly;
         uint8_t* row = dst.p + int64_t(gy) * dst.stride * sb;
         if (sb == 2) {
           uint16_t* r16 = reinterpret_cast<uint16_t*>(row) + gx;
@@ -564,12 +583,25 @@ __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cde
 }
 
 cudaError_t cdef_init() {
-  return cudaFuncSetAttribute(cdef_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kCdefSmem);
+  cudaError_t e = cudaFuncSetAttribute(cdef_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       cdef_smem(64, true));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cdef_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, cdef_smem(32, true));
+  return e;
 }
 
-void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
+void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, cudaStream_t s) {
   if (n_items <= 0) return;
-  launch_pdl(cdef_kernel, min(n_items, kItemGrid), 256, kCdefSmem, s, frames, items, n_items);
+  // without the fused horizontal pass the windows hold 2 border rows each
+  // side: smaller windows, more CTAs per SM
+  const int R = half ? 32 : 64;
+  const int wrows = R + 2 * (lfh ? kTopLfh : 2);
+  if (half)
+    launch_pdl(cdef_kernel<32>, min(n_items, kItemGrid), 128, size_t(cdef_smem(32, lfh)), s, frames, items, n_items,
+               wrows);
+  else
+    launch_pdl(cdef_kernel<64>, min(n_items, kItemGrid), 256, size_t(cdef_smem(64, lfh)), s, frames, items, n_items,
+               wrows);
 }
 
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s) {

@@ -55,7 +55,9 @@ void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, co
 void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s);
 
 // CDEF (cdef.cu)
-void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// `lfh`: some item has the horizontal loop-filter pass fused (item kind 1).
+// `half`: the items are half superblocks (Item::a = 0 top, 1 bottom).
+void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, cudaStream_t s);
 // Sets cdef_kernel's dynamic shared-memory limit on the current device.
 cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);

@@ -179,6 +179,8 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       v->clear();
     plan.edge_cap = 0;
     plan.any_hlist = false;
+    plan.any_lfh = false;
+    plan.cdef_half = false;
     plan.sr_row_max = 0;
     plan.any_lf = plan.any_cdef = plan.any_sr = plan.any_lr = plan.any_grain = plan.any_out = false;
     plan.off_frames = plan.off_lf = plan.off_lft = plan.off_cdef = plan.off_sr = plan.off_lr = plan.off_grain =
@@ -326,6 +328,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     if (cdef_on) {
       plan.any_cdef = true;
       const int sbr = (i->mi_rows + 15) / 16, sbc = (i->mi_cols + 15) / 16;
+      if (d.lfh_mask) plan.any_lfh = true;
       for (int r = 0; items && r < sbr; r++)
         for (int c = 0; c < sbc; c++) {
           Item it{};
@@ -333,7 +336,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
           it.kind = uint8_t(d.lfh_mask ? 1 : 0);
           it.x0 = uint16_t(c);
           it.y0 = uint16_t(r);
-          if (items) plan.cdef_items.push_back(it);
+          plan.cdef_items.push_back(it);
         }
     } else if (cdef_stage && !chain) {
       // the reference returns a clone of cur when CDEF is off: copy the MI area
@@ -454,6 +457,23 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   }
   plan.scratch_bytes = align_up(bump.used, 256);
   if (!items) return AV1PF_OK;  // the lists and their layout are the previous call's
+  // At most one wave of superblocks (4 CTAs on each SM): CDEF runs a CTA per
+  // half superblock instead, so the SMs end up with equal shares.
+  plan.cdef_half = !plan.cdef_items.empty() && plan.cdef_items.size() <= size_t(kNumSMs) * 4;
+  if (plan.cdef_half) {
+    std::vector<Item> halves;
+    halves.reserve(plan.cdef_items.size() * 2);
+    for (const Item& it : plan.cdef_items) {
+      for (int half = 0; half < 2; half++) {
+        // the bottom half of a superblock row past the mode-info area is empty
+        if (it.y0 * 16 + half * 8 >= jobs[it.frame].info->mi_rows) continue;
+        Item h = it;
+        h.a = uint16_t(half);
+        halves.push_back(h);
+      }
+    }
+    plan.cdef_items.swap(halves);
+  }
   plan.edge_cap = cap;
   // meta layout: [frames][items...] uploaded, then [edges v][edges h][counts] device-only
   size_t off = 0;
@@ -527,7 +547,7 @@ void launch_key(const Plan& plan, const void* meta, std::vector<uint64_t>& key) 
               plan.off_out, plan.off_copy, plan.off_edges_v, plan.off_edges_h, plan.off_counts,
               uint64_t(plan.any_lf) | uint64_t(plan.any_cdef) << 1 | uint64_t(plan.any_sr) << 2 |
                   uint64_t(plan.any_lr) << 3 | uint64_t(plan.any_grain) << 4 | uint64_t(plan.any_out) << 5 |
-                  uint64_t(plan.any_hlist) << 6,
+                  uint64_t(plan.any_hlist) << 6 | uint64_t(plan.any_lfh) << 7 | uint64_t(plan.cdef_half) << 8,
               uint64_t(plan.sr_row_max)});
 }
 
@@ -567,7 +587,8 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     if (plan.any_hlist) launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
   mark(1);
-  if (plan.any_cdef) launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), s);
+  if (plan.any_cdef)
+    launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), plan.any_lfh, plan.cdef_half, s);
   mark(2);
   if (plan.any_sr) launch_superres(frames, items(plan.off_sr), int(plan.sr_items.size()), plan.sr_row_max, s);
   mark(3);

@@ -49,6 +49,8 @@ struct Plan {
   uint32_t edge_cap = 0;
   size_t scratch_bytes = 0;   // bytes of per-frame scratch (planes, grain)
   bool any_hlist = false;  // some plane's horizontal loop-filter edges run as their own pass
+  bool any_lfh = false;    // some frame's horizontal loop-filter edges run inside the CDEF kernel
+  bool cdef_half = false;  // CDEF items are half superblocks (Item::a: 0 top, 1 bottom)
   int sr_row_max = 0;      // superres: the most source samples in a row (sr_maxx + 1)
   bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
   // byte offsets of each list in the device meta buffer

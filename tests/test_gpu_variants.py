@@ -65,6 +65,21 @@ def test_full_hd_variant(ctx, variant):
         set_tuning(ctx, -1, 0)
 
 
+def test_full_superblock_ctas_with_fused_lf(ctx):
+    """A 4K frame has more than one wave of CDEF superblocks, so CDEF runs a
+    CTA per whole superblock (1080p and smaller frames run halves); with
+    loop-filter mode 2 that path also filters the horizontal edges and writes
+    the stripe-boundary rows."""
+    set_tuning(ctx, 2, 64)
+    try:
+        sf = A.SynthHandle(width=3840, height=2160, bit_depth=10, seed=113)
+        ref_cpu, fb_cpu = O.chain(sf, threads=0)
+        ref_gpu, fb_gpu = G.gpu_chain(ctx, G.DevFrame(sf))
+        assert_same(ref_gpu, fb_gpu, ref_cpu, fb_cpu, "4K lf_mode 2")
+    finally:
+        set_tuning(ctx, -1, 0)
+
+
 def test_tuning_rejects_bad_values(ctx):
     for bad in [(3, 0), (-2, 0), (0, 48), (1, 128)]:
         t = A.Tuning(*bad)
