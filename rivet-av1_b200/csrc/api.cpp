@@ -166,6 +166,9 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
       m.ready = true;
     }
   }
+  // the loop filter's edge-list counters start at zero: cleared here, in the
+  // upload's stream order, so the chain's stream holds kernels only
+  if (e == cudaSuccess) e = cudaMemsetAsync(dmeta + plan.off_counts, 0, 16, upload);
   if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, upload);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(s, m.uploaded, 0);
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
@@ -175,10 +178,12 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   return rc;
 }
 
-// Launches the planned stages reading descriptor buffer `dmeta`: directly
-// with stage events when profiling, else by replaying a captured graph.
+// Launches the planned stages reading descriptor buffer `dmeta` as stream
+// launches with programmatic dependent launch, so consecutive calls' kernels
+// chain without a gap at the call boundary (the first loop-filter kernel of
+// a call starts its launch while the previous call's last kernel drains);
+// profiled calls record stage events between the stages.
 int Ctx::launch_on(uint8_t* dmeta, cudaStream_t s) {
-  cudaError_t e = cudaSuccess;
   const cudaEvent_t* ev = nullptr;
   if (prof) {
     const int slot = prof_next;
@@ -189,55 +194,8 @@ int Ctx::launch_on(uint8_t* dmeta, cudaStream_t s) {
     prof_used[slot] = true;
     ev = prof_ev[slot];
   }
-  if (ev) {
-    // profiled calls launch directly, with the stage events between stages
-    launch_plan(plan, dmeta, s, side, fork, join, ev);
-    e = cudaGetLastError();
-    return cuda_status(e, "kernel launch");
-  }
-  // Calls whose plan has the same launch structure (list sizes, offsets,
-  // flags, meta buffer) replay one captured graph: the descriptors and work
-  // lists it reads were just uploaded to the same addresses.
-  std::vector<uint64_t> key;
-  launch_key(plan, dmeta, key);
-  GraphEntry* g = nullptr;
-  for (GraphEntry& c : graphs)
-    if (c.exec && c.key == key) g = &c;
-  if (!g) {
-    GraphEntry* slot = &graphs[0];
-    for (GraphEntry& c : graphs)
-      if (!c.exec || c.last_use < slot->last_use) slot = &c;
-    if (slot->exec) cudaGraphExecDestroy(slot->exec);
-    slot->exec = nullptr;
-    if (!capture) {
-      e = cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking);
-      if (e != cudaSuccess) return cuda_status(e, "capture stream");
-    }
-    cudaGraph_t graph = nullptr;
-    uint64_t kernels = 0;
-    {
-      CaptureScope cs;
-      e = cudaStreamBeginCapture(capture, cudaStreamCaptureModeThreadLocal);
-      if (e == cudaSuccess) {
-        launch_plan(plan, dmeta, capture, side, fork, join, nullptr);
-        e = cudaStreamEndCapture(capture, &graph);
-      }
-      kernels = cs.launches();
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&slot->exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      slot->exec = nullptr;
-      return cuda_status(e, "graph capture");
-    }
-    slot->key = key;
-    slot->kernels = kernels;
-    g = slot;
-  }
-  g->last_use = ++graph_clock;
-  e = cudaGraphLaunch(g->exec, s);
-  note_launch(g->kernels);
-  return cuda_status(e, "graph launch");
+  launch_plan(plan, dmeta, s, side, fork, join, ev, true);
+  return cuda_status(cudaGetLastError(), "kernel launch");
 }
 
 void Ctx::prof_collect(int slot) {
@@ -364,9 +322,6 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   }
   if (ctx->pipe_up) cudaStreamDestroy(ctx->pipe_up);
   if (ctx->pipe_down) cudaStreamDestroy(ctx->pipe_down);
-  for (GraphEntry& g : ctx->graphs)
-    if (g.exec) cudaGraphExecDestroy(g.exec);
-  if (ctx->capture) cudaStreamDestroy(ctx->capture);
   cudaStreamDestroy(ctx->side);
   cudaStreamDestroy(ctx->own);
   cudaEventDestroy(ctx->fork);

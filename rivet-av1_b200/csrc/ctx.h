@@ -40,15 +40,6 @@ struct ShapeChoice {
   float ms;  // measured device time per frame
 };
 
-// A captured per-frame launch sequence and the launch structure it was
-// captured for (launch_key).
-struct GraphEntry {
-  std::vector<uint64_t> key;
-  cudaGraphExec_t exec = nullptr;
-  uint64_t kernels = 0;   // kernels per replay
-  uint64_t last_use = 0;
-};
-
 // While alive, kernel launches on this thread are not counted (they are
 // being captured into a graph, and count when the graph runs).
 struct CaptureScope {
@@ -96,11 +87,6 @@ struct Ctx {
   MetaSlot metas[2];
   int meta_next = 0;
   cudaStream_t upload = nullptr;  // descriptor uploads
-  // per-frame graphs, by launch structure (least recently used replaced)
-  static constexpr int kGraphs = 8;
-  GraphEntry graphs[kGraphs];
-  uint64_t graph_clock = 0;
-  cudaStream_t capture = nullptr;
   // profiling: a ring of event sets, one per profiled call
   static constexpr int kProfSlots = 64;
   bool prof = false;

@@ -538,21 +538,8 @@ void pack_meta(const Plan& plan, uint8_t* host) {
   put(plan.off_copy, plan.copy_items.data(), plan.copy_items.size() * sizeof(Item));
 }
 
-void launch_key(const Plan& plan, const void* meta, std::vector<uint64_t>& key) {
-  key.assign({reinterpret_cast<uint64_t>(meta),
-              plan.frames.size(), plan.lf_items.size(), plan.lft_items.size(), plan.cdef_items.size(),
-              plan.sr_items.size(), plan.lr_items.size(), plan.grain_items.size(), plan.out_items.size(),
-              plan.copy_items.size(), plan.edge_cap,
-              plan.off_frames, plan.off_lf, plan.off_lft, plan.off_cdef, plan.off_sr, plan.off_lr, plan.off_grain,
-              plan.off_out, plan.off_copy, plan.off_edges_v, plan.off_edges_h, plan.off_counts,
-              uint64_t(plan.any_lf) | uint64_t(plan.any_cdef) << 1 | uint64_t(plan.any_sr) << 2 |
-                  uint64_t(plan.any_lr) << 3 | uint64_t(plan.any_grain) << 4 | uint64_t(plan.any_out) << 5 |
-                  uint64_t(plan.any_hlist) << 6 | uint64_t(plan.any_lfh) << 7 | uint64_t(plan.cdef_half) << 8,
-              uint64_t(plan.sr_row_max)});
-}
-
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join, const cudaEvent_t* stage_ev) {
+                 cudaEvent_t join, const cudaEvent_t* stage_ev, bool counts_zeroed) {
   auto mark = [&](int k) {
     if (stage_ev) cudaEventRecord(stage_ev[k], s);
   };
@@ -570,19 +557,22 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
   }
   mark(0);
   if (!plan.copy_items.empty()) {
-    cudaMemsetAsync(counts, 0, 16, s);
+    if (!counts_zeroed) cudaMemsetAsync(counts, 0, 16, s);
+    counts_zeroed = false;
     launch_lf_prep(frames, items(plan.off_copy), int(plan.copy_items.size()), ev, eh, counts, 0, s);
   }
   if (plan.any_lf && !plan.lf_items.empty()) {
     // in place: decisions into both edge lists, then one pass per direction
-    cudaMemsetAsync(counts, 0, 16, s);
+    if (!counts_zeroed) cudaMemsetAsync(counts, 0, 16, s);
+    counts_zeroed = false;
     launch_lf_prep(frames, items(plan.off_lf), int(plan.lf_items.size()), ev, eh, counts, plan.edge_cap, s);
     launch_lf_edges(0, frames, ev, counts + 0, plan.edge_cap, s);
     launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
   if (plan.any_lf && !plan.lft_items.empty()) {
     // copy + vertical edges per tile, then the horizontal edge list
-    cudaMemsetAsync(counts, 0, 16, s);
+    if (!counts_zeroed) cudaMemsetAsync(counts, 0, 16, s);
+    counts_zeroed = false;
     launch_lf_tiles(frames, items(plan.off_lft), int(plan.lft_items.size()), eh, counts, plan.edge_cap, s);
     if (plan.any_hlist) launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }

@@ -78,17 +78,15 @@ void structure_key(const FrameJob* jobs, int n, std::vector<int64_t>& key);
 // long) in the layout of the device meta buffer.
 void pack_meta(const Plan& plan, uint8_t* host);
 
-// The launch structure of a plan on meta buffer `meta` (list sizes,
-// offsets, flags): two plans with the same key enqueue the same launches
-// with the same arguments, so one captured graph serves both.
-void launch_key(const Plan& plan, const void* meta, std::vector<uint64_t>& key);
-
 // Enqueues the plan's kernels on `s`; `meta` is the device meta buffer.
 // `side`/`fork`/`join` run the grain templates concurrently when present.
 // `stage_ev`, when not null, holds 6 events recorded before the loop
 // filter and after each of the 5 stages (for av1pf_stage_times).
+// `counts_zeroed`: the edge-list counters in `meta` are already zero (the
+// caller cleared them in stream order), so the first loop-filter pass needs
+// no memset on `s`.
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr);
+                 cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr, bool counts_zeroed = false);
 
 // Plane helpers.
 inline int plane_w(const av1pf_frame_info* i, int p, int width) {

@@ -167,10 +167,10 @@ def test_batch_mixing_fused_and_separate_frames(ctx):
         set_tuning(ctx, -1, 0)
 
 
-def test_per_frame_graph_cache_many_shapes(ctx):
-    """av1pf_chain replays a captured graph per launch structure (8 kept,
-    least recently used replaced): cycle 11 shapes twice, interleaved, and
-    check every result."""
+def test_per_frame_many_shapes(ctx):
+    """av1pf_chain replans only the descriptors while the structure repeats
+    and uploads them into two buffers in turn: cycle 11 shapes twice,
+    interleaved (every call a new structure), and check every result."""
     cfgs = [dict(width=64 + 24 * k, height=48 + 16 * k, bit_depth=(8, 10, 12)[k % 3],
                  sample_bytes=1 if k % 3 == 0 else 2, enable_grain=k % 2, superres_denom=9 + k % 8 if k % 4 == 1 else 8,
                  seed=500 + k) for k in range(11)]
@@ -182,5 +182,5 @@ def test_per_frame_graph_cache_many_shapes(ctx):
         for k in list(range(11)) + list(range(10, -1, -1)):
             ref_gpu, fb_gpu = G.gpu_chain(ctx, dfs[k])
             assert_same(ref_gpu, fb_gpu, want[k][0], want[k][1], f"shape {k} round {rnd}")
-    # every call launched its kernels (graph replays count their kernels)
+    # every call launched its kernels
     assert A.lib().av1pf_launch_count() - launches0 >= 2 * 22 * 4
