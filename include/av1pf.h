@@ -457,6 +457,68 @@ int av1pf_serve_stats_get(av1pf_server* s, av1pf_serve_stats* out);
 int av1pf_serve_close(av1pf_server* s);
 
 /* ------------------------------------------------------------------------ */
+/* Encoder filter searches: the encoder's choice of loop-filter levels and   */
+/* CDEF strengths, every candidate filtered and scored on the device.        */
+/* ------------------------------------------------------------------------ */
+
+/* Candidate (primary, secondary) strength pairs of the CDEF search
+ * (encoder/cdef.rs:60-80): luma primaries {0,1,2,4,6,9,12} (thorough:
+ * {0,1,2,3,4,5,6,8,10,12,15}) x coded secondaries {0,1,2,3}; chroma
+ * primaries {0,1,2,4,7} (thorough: {0,1,2,3,4,6,8,11}) x {0,1,2}; pairs
+ * ordered primary-major. */
+#define AV1PF_CDEF_SEARCH_NY 28
+#define AV1PF_CDEF_SEARCH_NUV 15
+#define AV1PF_CDEF_SEARCH_NY_THOROUGH 44
+#define AV1PF_CDEF_SEARCH_NUV_THOROUGH 24
+
+/* CdefParams (encoder/cdef.rs:18-29): 1 << bits index entries; secondary
+ * strengths as coded (3 means 4, 6.10.14). */
+typedef struct av1pf_cdef_search_result {
+  int32_t damping_minus_3;
+  int32_t bits;
+  int32_t y_pri[8], y_sec[8];
+  int32_t uv_pri[8], uv_sec[8];
+} av1pf_cdef_search_result;
+
+/* cdef::search (encoder/cdef.rs:52-251). `cur` holds the deblocked frame and
+ * `src` the source planes (device planes in the frame's sample format, at
+ * least mi_cols*4 x mi_rows*4 luma samples readable in `cur`, the frame area
+ * in `src`); `maps` (device) gives the mode info (skip flags) and the
+ * first pass's cdef_idx table, whose entries >= 0 mark the 64x64 blocks that
+ * code an index. Every candidate strength pair filters every 8x8 block CDEF
+ * would filter, with the decoder's direction search and filter, and its
+ * squared error against the source inside the frame is summed per 64x64
+ * block, luma and chroma apart; then up to eight (luma, chroma) pairs are
+ * chosen greedily to minimise the error plus lambda * bits per block, and
+ * each block takes its best.
+ * Writes the result to `result` (host) and the table to `cdef_idx_out`
+ * (host, cdef_stride * ceil(mi_rows/16) entries: the input table with each
+ * coding block's chosen index). `block_sse` (host, may be NULL) receives the
+ * per-block errors: ceil(mi_rows/16) * ceil(mi_cols/16) blocks in raster
+ * order, each NY luma then NUV chroma u64 sums (zero for blocks that code no
+ * index). Returns once the outputs are on the host. */
+int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                      const av1pf_maps* maps, const av1pf_plane* cur,
+                      const av1pf_plane* src, int32_t base_q_idx,
+                      double lambda, int32_t thorough,
+                      av1pf_cdef_search_result* result, int8_t* cdef_idx_out,
+                      uint64_t* block_sse, void* stream);
+
+/* search_lf (encoder/mod.rs:1457-1506): the loop-filter levels with the
+ * least error. `params` carries the starting levels (loop_filter_level) and
+ * the other loop-filter fields the filter reads; `cur` (device, left
+ * unchanged) is the unfiltered reconstruction and `src` the source planes.
+ * The six scales {0, 0.5, 0.75, 1, 1.25, 1.5} of the starting levels are
+ * filtered as one batch, and each plane's squared error against the source
+ * inside the frame picks that plane's level. Writes the chosen levels to
+ * `levels_out` (host) and, when `sse_out` is not NULL, the 6 x 3 errors
+ * (scale-major; zero for absent planes). Returns once they are on the host. */
+int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                    const av1pf_params* params, const av1pf_maps* maps,
+                    const av1pf_plane* cur, const av1pf_plane* src,
+                    int32_t levels_out[4], uint64_t* sse_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* DSP entry points: the reference's src/dsp post-filter kernels over many   */
 /* independent inputs at once (device pointers), for conformance tests.     */
 /* ------------------------------------------------------------------------ */

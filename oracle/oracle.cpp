@@ -16,6 +16,8 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <cfloat>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -1530,6 +1532,227 @@ LfParams lf_params_from(const av1pf_lf_edge_params& p) {
   return LfParams{p.limit, p.blimit, p.thresh, size_t(p.filter_size), p.chroma != 0, uint32_t(p.bit_depth)};
 }
 
+// ---------------------------------------------------------------------------
+// Encoder filter searches (encoder/cdef.rs, encoder/mod.rs:1457-1506)
+// ---------------------------------------------------------------------------
+using Pair = std::pair<uint32_t, uint32_t>;
+
+// encoder/cdef.rs:43-46 `sec`
+int32_t coded_sec(uint32_t coded) { return coded == 3 ? 4 : int32_t(coded); }
+
+// encoder/cdef.rs:255-258 `damping_for`
+uint32_t damping_for(uint32_t qidx) { return std::min(qidx >> 6, 3u); }
+
+// encoder/cdef.rs:60-80: the candidate (primary, coded secondary) pairs
+void cdef_candidates(bool thorough, std::vector<Pair>& y, std::vector<Pair>& uv) {
+  const std::vector<uint32_t> y_pri = thorough ? std::vector<uint32_t>{0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15}
+                                               : std::vector<uint32_t>{0, 1, 2, 4, 6, 9, 12};
+  const std::vector<uint32_t> uv_pri = thorough ? std::vector<uint32_t>{0, 1, 2, 3, 4, 6, 8, 11}
+                                                : std::vector<uint32_t>{0, 1, 2, 4, 7};
+  y.clear();
+  uv.clear();
+  for (uint32_t p : y_pri)
+    for (uint32_t s : {0u, 1u, 2u, 3u}) y.emplace_back(p, s);
+  for (uint32_t p : uv_pri)
+    for (uint32_t s : {0u, 1u, 2u}) uv.emplace_back(p, s);
+}
+
+// encoder/cdef.rs:261-285 `block_sse`
+uint64_t block_sse(const uint16_t* res, size_t w, size_t h, const PlaneBuf& src, size_t x0, size_t y0,
+                   const FrameCtx& f, size_t plane) {
+  auto ss = f.plane_ss(plane);
+  size_t fw = (size_t(f.hdr.frame_width) + ss.first) >> ss.first;
+  size_t fh = (size_t(f.hdr.frame_height) + ss.second) >> ss.second;
+  size_t hh = std::min(h, fh > y0 ? fh - y0 : 0), ww = std::min(w, fw > x0 ? fw - x0 : 0);
+  uint64_t s = 0;
+  for (size_t i = 0; i < hh; i++)
+    for (size_t j = 0; j < ww; j++) {
+      int64_t d = int64_t(res[i * w + j]) - int64_t(src.get(x0 + j, y0 + i));
+      s += uint64_t(d * d);
+    }
+  return s;
+}
+
+struct CdefSearch {
+  uint32_t damping_minus_3 = 0, bits = 0;
+  std::vector<Pair> y, uv;           // the chosen pairs, one per index
+  std::vector<int8_t> table;         // cdef_idx with each coding block's index
+  std::vector<std::pair<size_t, size_t>> blocks;  // (fb row, fb col) of the coding blocks
+  std::vector<uint64_t> ysse, uvsse;  // [block][candidate]
+  size_t ny = 0, nuv = 0;
+};
+
+// encoder/cdef.rs:52-251 `search`. `f.cur` holds the deblocked frame.
+CdefSearch cdef_search(const FrameCtx& f, const FrameBuf& src, uint32_t qidx, double lambda, bool thorough,
+                       size_t threads) {
+  CdefSearch out;
+  std::vector<Pair> ycands, uvcands;
+  cdef_candidates(thorough, ycands, uvcands);
+  const uint32_t damping_minus_3 = damping_for(qidx);
+  const uint32_t coeff_shift = f.bit_depth - 8;
+  const int32_t damping = int32_t(damping_minus_3) + 3;
+  const size_t fb_rows = (f.mi_rows + 15) / 16, fb_cols = (f.mi_cols + 15) / 16;
+  for (size_t fr = 0; fr < fb_rows; fr++)
+    for (size_t fc = 0; fc < fb_cols; fc++)
+      if (f.cdef_idx[fr * f.cdef_stride + fc] >= 0) out.blocks.emplace_back(fr, fc);
+  out.table = f.cdef_idx;
+  out.ny = ycands.size();
+  out.nuv = uvcands.size();
+  if (out.blocks.empty()) {  // CdefParams::off()
+    out.y = {Pair(0, 0)};
+    out.uv = {Pair(0, 0)};
+    return out;
+  }
+  const size_t ny = out.ny, nuv = out.nuv, nb = out.blocks.size();
+  out.ysse.assign(nb * ny, 0);
+  out.uvsse.assign(nb * nuv, 0);
+  const size_t cols = f.ms;
+  auto per_block = [&](size_t bi) {
+    size_t fr = out.blocks[bi].first, fc = out.blocks[bi].second;
+    uint64_t* ysse = &out.ysse[bi * ny];
+    uint64_t* uvsse = &out.uvsse[bi * nuv];
+    uint16_t res[64];
+    for (size_t r = fr * 16; r < std::min(fr * 16 + 16, f.mi_rows); r += 2) {
+      for (size_t c = fc * 16; c < std::min(fc * 16 + 16, f.mi_cols); c += 2) {
+        auto sk = [&](size_t rr, size_t cc) { return f.mi[rr * cols + cc].skip; };
+        if (sk(r, c) && sk(r + 1, c) && sk(r, c + 1) && sk(r + 1, c + 1)) continue;
+        auto dv = cdef_direction(f, r, c);
+        size_t y_dir = dv.first;
+        int32_t var = dv.second;
+        size_t x0 = c * MI_SIZE, y0 = r * MI_SIZE;
+        size_t xlim = f.mi_cols * MI_SIZE, ylim = f.mi_rows * MI_SIZE;
+        for (size_t k = 0; k < ny; k++) {
+          int32_t pri_str = int32_t(ycands[k].first) << coeff_shift;
+          int32_t sec_str = coded_sec(ycands[k].second) << coeff_shift;
+          size_t dir = pri_str == 0 ? 0 : y_dir;
+          int32_t var_str = (var >> 6) != 0 ? std::min(int32_t(floor_log2(uint32_t(var >> 6))), 12) : 0;
+          pri_str = var != 0 ? (pri_str * (4 + var_str) + 8) >> 4 : 0;
+          int32_t d = damping + int32_t(coeff_shift);
+          cdef_filter_block(f.cur.planes[0], x0, y0, 8, 8, xlim, ylim, pri_str, sec_str, d, dir, coeff_shift, res);
+          ysse[k] += block_sse(res, 8, 8, src.planes[0], x0, y0, f, 0);
+        }
+        if (f.num_planes > 1) {
+          size_t w = 8 >> f.ssx, h = 8 >> f.ssy;
+          size_t cx0 = x0 >> f.ssx, cy0 = y0 >> f.ssy;
+          size_t cxlim = xlim >> f.ssx, cylim = ylim >> f.ssy;
+          for (size_t k = 0; k < nuv; k++) {
+            int32_t pri_str = int32_t(uvcands[k].first) << coeff_shift;
+            int32_t sec_str = coded_sec(uvcands[k].second) << coeff_shift;
+            size_t dir = pri_str == 0 ? 0 : CDEF_UV_DIR[f.ssx][f.ssy][y_dir];
+            int32_t d = damping + int32_t(coeff_shift) - 1;
+            uint64_t total = 0;
+            for (size_t p = 1; p < 3; p++) {
+              cdef_filter_block(f.cur.planes[p], cx0, cy0, w, h, cxlim, cylim, pri_str, sec_str, d, dir,
+                                coeff_shift, res);
+              total += block_sse(res, w, h, src.planes[p], cx0, cy0, f, p);
+            }
+            uvsse[k] += total;
+          }
+        }
+      }
+    }
+  };
+  run_bands(nb, threads, per_block);
+  // Greedy choice of up to 2^bits (luma, chroma) pairs, for each bits
+  // (encoder/cdef.rs:195-240).
+  auto best_for = [&](const std::vector<std::pair<size_t, size_t>>& set, std::vector<size_t>* pick) {
+    double total = 0;
+    for (size_t b = 0; b < nb; b++) {
+      uint64_t best = UINT64_MAX;
+      for (size_t i = 0; i < set.size(); i++) {
+        uint64_t v = out.ysse[b * ny + set[i].first] + out.uvsse[b * nuv + set[i].second];
+        if (v < best) {
+          best = v;
+          if (pick) (*pick)[b] = i;
+        }
+      }
+      total += double(best);
+    }
+    return total;
+  };
+  double best_cost = DBL_MAX;
+  std::vector<std::pair<size_t, size_t>> set, best_set;
+  std::vector<size_t> best_pick;
+  for (uint32_t bits = 0; bits <= 3; bits++) {
+    while (set.size() < (size_t(1) << bits)) {
+      double add_t = DBL_MAX;
+      std::pair<size_t, size_t> add(0, 0);
+      for (size_t yk = 0; yk < ny; yk++) {
+        for (size_t uk = 0; uk < nuv; uk++) {
+          if (std::find(set.begin(), set.end(), std::make_pair(yk, uk)) != set.end()) continue;
+          set.emplace_back(yk, uk);
+          double t = best_for(set, nullptr);
+          set.pop_back();
+          if (t < add_t) {
+            add_t = t;
+            add = {yk, uk};
+          }
+        }
+      }
+      set.push_back(add);
+    }
+    std::vector<size_t> pick(nb, 0);
+    double t = best_for(set, &pick);
+    // lambda * (bits as f64) * nb as f64, evaluated left to right
+    double cost = t + lambda * double(bits) * double(nb);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_set = set;
+      best_pick = pick;
+    }
+  }
+  out.damping_minus_3 = damping_minus_3;
+  out.bits = uint32_t(__builtin_ctz(unsigned(best_set.size())));
+  for (size_t b = 0; b < nb; b++)
+    out.table[out.blocks[b].first * f.cdef_stride + out.blocks[b].second] = int8_t(best_pick[b]);
+  for (auto& s : best_set) {
+    out.y.push_back(ycands[s.first]);
+    out.uv.push_back(uvcands[s.second]);
+  }
+  return out;
+}
+
+// encoder/mod.rs:1494-1506 `plane_sse`
+uint64_t plane_sse(const FrameCtx& f, const FrameBuf& src, size_t p) {
+  auto ss = f.plane_ss(p);
+  size_t w = (size_t(f.hdr.frame_width) + ss.first) >> ss.first;
+  size_t h = (size_t(f.hdr.frame_height) + ss.second) >> ss.second;
+  uint64_t s = 0;
+  for (size_t y = 0; y < h; y++) {
+    const uint16_t* a = src.planes[p].row(y);
+    const uint16_t* b = f.cur.planes[p].row(y);
+    for (size_t x = 0; x < w; x++) {
+      int64_t d = int64_t(a[x]) - int64_t(b[x]);
+      s += uint64_t(d * d);
+    }
+  }
+  return s;
+}
+
+// encoder/mod.rs:1457-1493 `search_lf`: f.cur is left unfiltered.
+std::array<uint32_t, 4> search_lf(FrameCtx& f, const FrameBuf& src, const std::array<uint32_t, 4>& start,
+                                  size_t threads, uint64_t* sse_out) {
+  const FrameBuf saved = f.cur;
+  std::pair<uint64_t, uint32_t> best[3] = {{UINT64_MAX, 0}, {UINT64_MAX, 0}, {UINT64_MAX, 0}};
+  const size_t planes = f.num_planes;
+  const double scales[6] = {0.0, 0.5, 0.75, 1.0, 1.25, 1.5};
+  for (size_t si = 0; si < 6; si++) {
+    auto lv = [&](uint32_t l) { return std::min(uint32_t(std::round(double(l) * scales[si])), 63u); };
+    uint32_t levels[4] = {lv(start[0]), lv(start[1]), lv(start[2]), lv(start[3])};
+    for (int i = 0; i < 4; i++) f.hdr.loop_filter_level[i] = int32_t(levels[i]);
+    if (levels[0] != 0 || levels[1] != 0) loop_filter_threads(f, threads);
+    for (size_t p = 0; p < planes; p++) {
+      uint64_t e = plane_sse(f, src, p);
+      if (sse_out) sse_out[si * 3 + p] = e;
+      if (e < best[p].first) best[p] = {e, p == 0 ? levels[0] : levels[1 + p]};
+    }
+    f.cur.planes = saved.planes;
+  }
+  // Chroma is filtered only when luma is.
+  if (best[0].second == 0) return {0, 0, 0, 0};
+  return {best[0].second, best[0].second, best[1].second, best[2].second};
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1732,6 +1955,56 @@ void oracle_cdef_kat_cases(uint64_t seed, int cases, int32_t* win, av1pf_cdef_ta
       taps[e] = t;
     }
   }
+}
+
+int oracle_cdef_search(const av1pf_frame_info* info, const av1pf_maps* maps, const av1pf_plane* cur,
+                       const av1pf_plane* src, int32_t base_q_idx, double lambda, int32_t thorough,
+                       av1pf_cdef_search_result* result, int8_t* cdef_idx_out, uint64_t* block_sse, int threads) {
+  if (!info_ok(info) || !maps || !maps->mi || !maps->cdef_idx || !cur || !src || !result || base_q_idx < 0)
+    return AV1PF_ERR_INVALID_INPUT;
+  FrameCtx f;
+  ctx_from(f, info, nullptr, maps, cur);
+  FrameBuf s = frame_from(info, src);
+  CdefSearch o = cdef_search(f, s, uint32_t(base_q_idx), lambda, thorough != 0, resolve_threads(threads));
+  std::memset(result, 0, sizeof(*result));
+  result->damping_minus_3 = int32_t(o.damping_minus_3);
+  result->bits = int32_t(o.bits);
+  for (size_t i = 0; i < o.y.size(); i++) {
+    result->y_pri[i] = int32_t(o.y[i].first);
+    result->y_sec[i] = int32_t(o.y[i].second);
+    result->uv_pri[i] = int32_t(o.uv[i].first);
+    result->uv_sec[i] = int32_t(o.uv[i].second);
+  }
+  const size_t fb_rows = (f.mi_rows + 15) / 16, fb_cols = (f.mi_cols + 15) / 16;
+  if (cdef_idx_out) std::memcpy(cdef_idx_out, o.table.data(), fb_rows * f.cdef_stride);
+  if (block_sse) {
+    const size_t nc = o.ny + o.nuv;
+    std::memset(block_sse, 0, fb_rows * fb_cols * nc * sizeof(uint64_t));
+    for (size_t b = 0; b < o.blocks.size(); b++) {
+      uint64_t* row = block_sse + (o.blocks[b].first * fb_cols + o.blocks[b].second) * nc;
+      std::memcpy(row, &o.ysse[b * o.ny], o.ny * sizeof(uint64_t));
+      std::memcpy(row + o.ny, &o.uvsse[b * o.nuv], o.nuv * sizeof(uint64_t));
+    }
+  }
+  return AV1PF_OK;
+}
+
+int oracle_lf_search(const av1pf_frame_info* info, const av1pf_params* p, const av1pf_maps* maps,
+                     const av1pf_plane* cur, const av1pf_plane* src, int32_t levels_out[4], uint64_t* sse_out,
+                     int threads) {
+  if (!info_ok(info) || !p || !maps || !cur || !src || !levels_out) return AV1PF_ERR_INVALID_INPUT;
+  std::array<uint32_t, 4> start;
+  for (int i = 0; i < 4; i++) {
+    if (p->loop_filter_level[i] < 0 || p->loop_filter_level[i] > 63) return AV1PF_ERR_INVALID_INPUT;
+    start[size_t(i)] = uint32_t(p->loop_filter_level[i]);
+  }
+  FrameCtx f;
+  ctx_from(f, info, p, maps, cur);
+  FrameBuf s = frame_from(info, src);
+  if (sse_out) std::memset(sse_out, 0, 6 * 3 * sizeof(uint64_t));
+  std::array<uint32_t, 4> lv = search_lf(f, s, start, resolve_threads(threads), sse_out);
+  for (int i = 0; i < 4; i++) levels_out[i] = int32_t(lv[size_t(i)]);
+  return AV1PF_OK;
 }
 
 }  // extern "C"

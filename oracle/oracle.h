@@ -67,6 +67,19 @@ void oracle_cdef_filter(const int32_t* win, const av1pf_cdef_taps* taps,
 void oracle_cdef_kat_cases(uint64_t seed, int cases, int32_t* win,
                            av1pf_cdef_taps* taps);
 
+/* cdef::search (encoder/cdef.rs:52-251): outputs as av1pf_cdef_search
+ * (host pointers; block_sse and cdef_idx_out may be NULL). */
+int oracle_cdef_search(const av1pf_frame_info* info, const av1pf_maps* maps,
+                       const av1pf_plane* cur, const av1pf_plane* src,
+                       int32_t base_q_idx, double lambda, int32_t thorough,
+                       av1pf_cdef_search_result* result, int8_t* cdef_idx_out,
+                       uint64_t* block_sse, int threads);
+/* search_lf (encoder/mod.rs:1457-1506): outputs as av1pf_lf_search. */
+int oracle_lf_search(const av1pf_frame_info* info, const av1pf_params* p,
+                     const av1pf_maps* maps, const av1pf_plane* cur,
+                     const av1pf_plane* src, int32_t levels_out[4],
+                     uint64_t* sse_out, int threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,10 @@ def lib():
         sig("oracle_lf_kat_cases", None, C.c_uint64, C.c_int, vp, vp)
         sig("oracle_cdef_filter", None, vp, vp, vp, C.c_int)
         sig("oracle_cdef_kat_cases", None, C.c_uint64, C.c_int, vp, vp)
+        sig("oracle_cdef_search", C.c_int, P(A.FrameInfo), P(A.Maps), P(A.Plane), P(A.Plane), C.c_int32, C.c_double,
+            C.c_int32, P(A.CdefSearchResult), vp, vp, C.c_int)
+        sig("oracle_lf_search", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), P(A.Plane),
+            P(C.c_int32), vp, C.c_int)
         _lib = L
     return _lib
 
@@ -118,3 +122,51 @@ def chain(sf, threads=0, want_frame=True):
     if rc != 0:
         raise RuntimeError(f"oracle_chain: {rc}")
     return ref, fb
+
+
+def search_inputs(sf, seed, amp=None):
+    """(cur, src) HostPlanes for the encoder searches on a SynthHandle: the
+    source is the synthetic frame's planes, the reconstruction the source
+    plus seeded noise of +-amp (default 3 << (bit_depth - 8)) in blocks of
+    4x4, clipped to the sample range."""
+    info = sf.f.info
+    src = HostPlanes.like_synth(sf)
+    rng = np.random.default_rng(seed)
+    a = (3 << (info.bit_depth - 8)) if amp is None else amp
+    hi = (1 << info.bit_depth) - 1
+    cur = []
+    for arr in src.arrays:
+        h, w = arr.shape
+        blk = rng.integers(-a, a + 1, size=((h + 3) // 4, (w + 3) // 4))
+        fine = rng.integers(-(a // 2), a // 2 + 1, size=(h, w))
+        noise = np.kron(blk, np.ones((4, 4), np.int64))[:h, :w] + fine
+        cur.append(np.clip(arr.astype(np.int64) + noise, 0, hi).astype(arr.dtype))
+    return HostPlanes(cur), src
+
+
+def cdef_search(sf, cur, src, q, lam, thorough, threads=0):
+    """(result, cdef_idx table, block_sse [blocks, ny + nuv]) of the oracle's
+    CDEF search."""
+    info, maps = sf.f.info, sf.f.maps
+    fbr, fbc = (info.mi_rows + 15) // 16, (info.mi_cols + 15) // 16
+    ny, nuv = A.CDEF_SEARCH_N[bool(thorough)]
+    res = A.CdefSearchResult()
+    table = np.zeros(fbr * maps.cdef_stride, np.int8)
+    sse = np.zeros((fbr * fbc, ny + nuv), np.uint64)
+    rc = lib().oracle_cdef_search(C.byref(info), C.byref(maps), cur.c, src.c, q, lam, int(thorough), C.byref(res),
+                                  table.ctypes.data, sse.ctypes.data, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_cdef_search: {rc}")
+    return res, table, sse
+
+
+def lf_search(sf, cur, src, threads=0, params=None):
+    """(levels[4], sse[6, 3]) of the oracle's loop-filter level search."""
+    info, maps = sf.f.info, sf.f.maps
+    levels = (C.c_int32 * 4)()
+    sse = np.zeros((6, 3), np.uint64)
+    rc = lib().oracle_lf_search(C.byref(info), C.byref(params if params is not None else sf.f.params),
+                                C.byref(maps), cur.c, src.c, levels, sse.ctypes.data, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_lf_search: {rc}")
+    return list(levels), sse

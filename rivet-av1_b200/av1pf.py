@@ -114,6 +114,18 @@ class ServeStats(C.Structure):
                 ("mean_batch_frames", C.c_double), ("resident_bytes", C.c_uint64)]
 
 
+class CdefSearchResult(C.Structure):
+    _fields_ = [("damping_minus_3", C.c_int32), ("bits", C.c_int32), ("y_pri", C.c_int32 * 8),
+                ("y_sec", C.c_int32 * 8), ("uv_pri", C.c_int32 * 8), ("uv_sec", C.c_int32 * 8)]
+
+    def pairs(self):
+        """[(y_pri, y_sec, uv_pri, uv_sec)] per index (secondaries as coded)."""
+        return [(self.y_pri[i], self.y_sec[i], self.uv_pri[i], self.uv_sec[i]) for i in range(1 << self.bits)]
+
+
+CDEF_SEARCH_N = {False: (28, 15), True: (44, 24)}  # (luma, chroma) candidate pairs
+
+
 class LfEdgeParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("limit", "blimit", "thresh", "filter_size", "chroma", "bit_depth")]
 
@@ -196,6 +208,10 @@ def lib():
         _sig(L, "av1pf_serve_poll", C.c_int, vp, C.c_uint64, C.c_int32, vp, P(C.c_double))
         _sig(L, "av1pf_serve_stats_get", C.c_int, vp, P(ServeStats))
         _sig(L, "av1pf_serve_close", C.c_int, vp)
+        _sig(L, "av1pf_cdef_search", C.c_int, vp, P(FrameInfo), P(Maps), P(Plane), P(Plane), C.c_int32, C.c_double,
+             C.c_int32, P(CdefSearchResult), vp, vp, vp)
+        _sig(L, "av1pf_lf_search", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane),
+             P(C.c_int32), vp, vp)
         _sig(L, "av1pf_dsp_lf_filter", C.c_int, vp, vp, vp, C.c_int, vp)
         _sig(L, "av1pf_dsp_cdef_filter", C.c_int, vp, vp, vp, vp, C.c_int, vp)
         _sig(L, "av1pf_set_profiling", C.c_int, vp, C.c_int)

@@ -314,7 +314,9 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
       if (ev) cudaEventDestroy(ev);
   }
   if (ctx->upload) cudaStreamDestroy(ctx->upload);
-  for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame}) ctx->release(*b);
+  for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame, &ctx->search_dev, &ctx->search_planes})
+    ctx->release(*b);
+  if (ctx->search_host.ptr) cudaFreeHost(ctx->search_host.ptr);
   for (Ctx::PipeSlot& ps : ctx->pipe) {
     for (auto* b : {&ps.in, &ps.ref, &ps.maps, &ps.frame}) ctx->release(*b);
     for (cudaEvent_t ev : {ps.uploaded, ps.computed, ps.downloaded})

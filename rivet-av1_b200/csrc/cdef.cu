@@ -533,6 +533,212 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
   }
 }
 
+// Sum of a u32 over the warp, exactly (two 16-bit halves, so no lane sum
+// overflows).
+__device__ __forceinline__ uint64_t warp_sum_u32(uint32_t v) {
+  const uint32_t lo = __reduce_add_sync(0xffffffffu, v & 0xffffu);
+  const uint32_t hi = __reduce_add_sync(0xffffffffu, v >> 16);
+  return (uint64_t(hi) << 16) + lo;
+}
+
+// Squared errors against the source window `s` (kNA outside the frame) of
+// one row of n samples filtered with `t` (MODE as cdef_px; 3 = unfiltered).
+template <int MODE>
+__device__ __forceinline__ uint32_t row_sse(const int16_t* c, const int16_t* s, int n, const TapsDev& t) {
+  uint32_t acc = 0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    if (j < n && s[j] != kNA) {
+      const int v = MODE == 3 ? int(c[j]) : cdef_px<MODE>(c + j, t);
+      const int d = v - s[j];
+      acc += uint32_t(d * d);
+    }
+  }
+  return acc;
+}
+
+// The rows of one thread's share of an 8x8 block (rows rr and rr+4 of the
+// block's h rows, w samples each) under candidate taps, as squared error.
+__device__ __forceinline__ uint32_t block_rows_sse(const int16_t* c, const int16_t* s, int w, int h, int mode,
+                                                   const TapsDev& t) {
+  uint32_t acc = 0;
+  for (int q = 0; q < h / 4; q++) {
+    const int16_t* cq = c + q * 4 * kS;
+    const int16_t* sq = s + q * 4 * kS;
+    switch (mode) {
+      case 0: acc += row_sse<0>(cq, sq, w, t); break;
+      case 1: acc += row_sse<1>(cq, sq, w, t); break;
+      case 2: acc += row_sse<2>(cq, sq, w, t); break;
+      default: acc += row_sse<3>(cq, sq, w, t); break;
+    }
+  }
+  return acc;
+}
+
+// The encoder's CDEF search, error tables (encoder/cdef.rs:103-190): one CTA
+// per 64x64 block, 256 threads. The block's planes are staged as in the
+// decoder's kernel (2-sample border, kNA outside the mode-info area) with
+// the source beside them (kNA outside the frame, so block_sse's crop,
+// encoder/cdef.rs:261-285, is a test per sample); the direction search is
+// the decoder's. Then every candidate pair filters every 8x8 block CDEF
+// would filter (a warp per row of 8x8 blocks, lanes = (block, row pair)),
+// and its squared error is summed over the CTA per candidate: the filter
+// and the error of a sample never leave registers. The filter mode is
+// chosen per candidate (uniform over the CTA): zero strengths drop their
+// taps exactly as in the decoder's kernel.
+__global__ void __launch_bounds__(256, 3) cdef_search_kernel(const FrameDesc* __restrict__ frames,
+                                                           const CdefSearchDesc d, CdefGreedy* __restrict__ g) {
+  constexpr int R = 64, top = 2, wrows = R + 2 * top;
+  extern __shared__ __align__(16) int16_t cs_smem[];
+  auto win = [&](int p) { return cs_smem + p * wrows * kS; };           // cur windows
+  auto srcw = [&](int p) { return cs_smem + 3 * wrows * kS + p * R * kS; };  // source
+  __shared__ int32_t cost[R][8];
+  __shared__ uint8_t bstate[R];
+  __shared__ uint8_t bdir[R];
+  __shared__ int32_t bvar[R];
+  __shared__ int16_t doff[8][2];
+  __shared__ uint8_t uvdir[2][2][8];
+  __shared__ int s_one;
+  __shared__ uint64_t red[8][kSearchMaxY + kSearchMaxUV];
+  const FrameDesc& f = frames[0];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int fb = blockIdx.x, nfb = d.fb_rows * d.fb_cols;
+  const int fr = fb / d.fb_cols, fc = fb - fr * d.fb_cols;
+  const int nc = d.ny + d.nuv;
+  const int idx = f.cdef_idx[int64_t(fr) * f.cdef_stride + fc];
+  if (idx < 0) {  // codes no index: zero errors, and no part in the greedy's sums
+    for (int k = tid; k < nc; k += blockDim.x) d.sse[int64_t(k) * nfb + fb] = 0;
+    if (tid == 0) d.best[fb] = 0;
+    return;
+  }
+  if (tid == 0) {
+    d.best[fb] = ~uint64_t(0);
+    atomicAdd(&g->nb, 1u);
+  }
+  if (tid < 16) doff[tid >> 1][tid & 1] = int16_t(c_cdef_dirs[tid >> 1][tid & 1][0] * kS + c_cdef_dirs[tid >> 1][tid & 1][1]);
+  if (tid < 32) (&uvdir[0][0][0])[tid] = (&c_cdef_uv_dir[0][0][0])[tid];
+  if (tid == 0) s_one = 1;
+  const int np = f.np, sb = f.sb, cs = f.bd - 8;
+  // --- the 8x8 blocks CDEF filters (encoder/cdef.rs:106-112) ---
+  if (tid < R) {
+    const int by = tid >> 3, bx = tid & 7;
+    const int r = fr * 16 + 2 * by, c = fc * 16 + 2 * bx;
+    uint8_t st = 0;
+    if (r < f.mi_rows && c < f.mi_cols) {
+      const av1pf_mi* m = f.mi + int64_t(r) * f.mi_stride + c;
+      const int ms = f.mi_stride;
+      const bool skip = (m[0].skip_segment & AV1PF_MI_SKIP) && (m[ms].skip_segment & AV1PF_MI_SKIP) &&
+                        (m[1].skip_segment & AV1PF_MI_SKIP) && (m[ms + 1].skip_segment & AV1PF_MI_SKIP);
+      st = skip ? 0 : 2;
+    }
+    bstate[tid] = st;
+  }
+  // --- stage the reconstruction and the source ---
+  for (int p = 0; p < np; p++) {
+    if (plane_ssx(f, p))
+      stage_plane<R, 1>(f, p, fc, fr * 64, top, win(p), tid);
+    else
+      stage_plane<R, 0>(f, p, fc, fr * 64, top, win(p), tid);
+    const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+    const int pw = R >> sx, ph = R >> sy;
+    const int fw = (f.fw + sx) >> sx, fh = (f.fh + sy) >> sy;
+    const int x0 = (fc * 64) >> sx, y0 = (fr * 64) >> sy;
+    int16_t* sp = srcw(p);
+    for (int k = tid; k < pw * ph; k += blockDim.x) {
+      const int r = k / pw, c = k - r * pw;
+      const int gx = x0 + c, gy = y0 + r;
+      sp[r * kS + c] = (gx < fw && gy < fh) ? int16_t(ld_sample(d.src[p], sb, gx, gy)) : kNA;
+    }
+  }
+  __syncthreads();
+  // --- direction search (postfilter.rs:345-401), as in the decoder's kernel ---
+  {
+    const int pair = warp & 3;
+    const int b = (warp >> 2) * 32 + lane;
+    if (bstate[b] == 2) {
+      const int by = b >> 3, bx = b & 7;
+      const int16_t* s = &win(0)[(top + by * 8) * kS + kColOff + bx * 8];
+      int32_t c1, c2;
+      switch (pair) {
+        case 0: cdef_cost_pair<0>(s, cs, s_one, c1, c2); break;
+        case 1: cdef_cost_pair<1>(s, cs, s_one, c1, c2); break;
+        case 2: cdef_cost_pair<2>(s, cs, s_one, c1, c2); break;
+        default: cdef_cost_pair<3>(s, cs, s_one, c1, c2); break;
+      }
+      cost[b][pair] = c1;
+      cost[b][pair + 4] = c2;
+    }
+  }
+  __syncthreads();
+  if (tid < R && bstate[tid] == 2) {
+    int32_t best = 0;
+    int y_dir = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      if (cost[tid][k] > best) {
+        best = cost[tid][k];
+        y_dir = k;
+      }
+    }
+    bdir[tid] = uint8_t(y_dir);
+    bvar[tid] = (best - cost[tid][(y_dir + 4) & 7]) >> 10;
+  }
+  __syncthreads();
+  // --- every candidate on every filtered block (encoder/cdef.rs:113-188) ---
+  const int by = warp, bx = lane & 7, rr = lane >> 3;
+  const int b = by * 8 + bx;
+  const bool act = bstate[b] == 2;
+  const int y_dir = act ? bdir[b] : 0;
+  const int32_t var = act ? bvar[b] : 0;
+  const int var_str = (var >> 6) != 0 ? min(floor_log2(uint32_t(var >> 6)), 12) : 0;
+  {
+    const int16_t* c = &win(0)[(top + by * 8 + rr) * kS + kColOff + bx * 8];
+    const int16_t* s = &srcw(0)[(by * 8 + rr) * kS + bx * 8];
+    for (int k = 0; k < d.ny; k++) {
+      const int pri0 = int(d.y_pri[k]) << cs, sec = int(d.y_sec[k]) << cs;
+      uint32_t acc = 0;
+      if (act) {
+        const int dir = pri0 == 0 ? 0 : y_dir;
+        const int pri = var != 0 ? (pri0 * (4 + var_str) + 8) >> 4 : 0;
+        const TapsDev t = taps_of(make_blk_taps(pri, sec, d.damping + cs, dir, cs, doff));
+        const int mode = pri0 == 0 ? (sec == 0 ? 3 : 2) : (sec == 0 ? 1 : 0);
+        acc = block_rows_sse(c, s, 8, 8, mode, t);
+      }
+      const uint64_t ws = warp_sum_u32(acc);
+      if (lane == 0) red[warp][k] = ws;
+    }
+  }
+  if (np > 1) {
+    const int sx = f.ssx, sy = f.ssy;
+    const int w = 8 >> sx, h = 8 >> sy;  // h is 4 or 8: rows rr (and rr + 4)
+    for (int k = 0; k < d.nuv; k++) {
+      const int pri = int(d.uv_pri[k]) << cs, sec = int(d.uv_sec[k]) << cs;
+      uint32_t acc = 0;
+      if (act) {
+        const int dir = pri == 0 ? 0 : uvdir[sx][sy][y_dir];
+        const TapsDev t = taps_of(make_blk_taps(pri, sec, d.damping + cs - 1, dir, cs, doff));
+        const int mode = pri == 0 ? (sec == 0 ? 3 : 2) : (sec == 0 ? 1 : 0);
+        for (int p = 1; p < 3; p++) {
+          const int16_t* c = &win(p)[(top + by * h + rr) * kS + kColOff + bx * w];
+          const int16_t* s = &srcw(p)[(by * h + rr) * kS + bx * w];
+          acc += block_rows_sse(c, s, w, h, mode, t);
+        }
+      }
+      const uint64_t ws = warp_sum_u32(acc);
+      if (lane == 0) red[warp][d.ny + k] = ws;
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < nc; k += blockDim.x) {
+    uint64_t s = 0;
+    if (k < d.ny || np > 1)
+      for (int w8 = 0; w8 < 8; w8++) s += red[w8][k];
+    d.sse[int64_t(k) * nfb + fb] = s;
+  }
+}
+
+constexpr int kSearchSmem = 3 * (64 + 4) * kS * 2 + 3 * 64 * kS * 2;
+
 // dsp::cdef::filter (cdef.rs:29) on independent 12x12 windows: one CTA per
 // window, one thread per output sample.
 __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cdef_taps* __restrict__ taps,
@@ -587,6 +793,8 @@ cudaError_t cdef_init() {
                                        cdef_smem(64, true));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(cdef_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, cdef_smem(32, true));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cdef_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSearchSmem);
   return e;
 }
 
@@ -602,6 +810,13 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
   else
     launch_pdl(cdef_kernel<64>, min(n_items, kItemGrid), 256, size_t(cdef_smem(64, lfh)), s, frames, items, n_items,
                wrows);
+}
+
+void launch_cdef_search(const FrameDesc* frames, const CdefSearchDesc& d, CdefGreedy* g, cudaStream_t s) {
+  const int nfb = d.fb_rows * d.fb_cols;
+  if (nfb <= 0) return;
+  cdef_search_kernel<<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
+  note_launch();
 }
 
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s) {

@@ -59,6 +59,10 @@ struct Ctx {
   cudaEvent_t fork = nullptr, join = nullptr;
   DevBuf scratch;
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
+  // encoder searches: descriptors, error tables and greedy state; the
+  // loop-filter search's filtered copies; pinned staging of both
+  DevBuf search_dev, search_planes;
+  HostBuf search_host;
   // av1pf_chain_host_many: device frame slots used in turn, with the events
   // that order a slot's upload (pipe_up), chain (own) and download
   // (pipe_down) against its next use

@@ -90,4 +90,28 @@ struct Item {
 };
 static_assert(sizeof(Item) == 16, "Item is 16 bytes");
 
+// The encoder's CDEF search (encoder/cdef.rs:52-251): candidate strength
+// pairs and the per-block error table.
+constexpr int kSearchMaxY = 48, kSearchMaxUV = 32;
+struct CdefSearchDesc {
+  DPlane src[3];           // source planes (frame area)
+  int32_t ny, nuv;         // candidate pairs
+  int32_t damping;         // cdef_damping (damping_minus_3 + 3)
+  int32_t fb_rows, fb_cols;
+  int8_t y_pri[kSearchMaxY], y_sec[kSearchMaxY];     // secondary decoded (coded 3 -> 4)
+  int8_t uv_pri[kSearchMaxUV], uv_sec[kSearchMaxUV];
+  uint64_t* sse;           // [ny + nuv][fb_rows * fb_cols], candidate-major
+  uint64_t* best;          // [fb_rows * fb_cols]: the greedy's per-block minimum
+};
+
+// State of the greedy choice of (luma, chroma) pairs (encoder/cdef.rs:195-240).
+struct CdefGreedy {
+  uint32_t arrived;        // CTAs of the current step done (the last one picks)
+  int32_t n;               // pairs chosen so far
+  int32_t set_y[8], set_uv[8];
+  uint32_t nb;             // blocks that code an index
+  int32_t best_bits;
+  double best_cost;
+};
+
 }  // namespace av1pf

@@ -12,6 +12,8 @@ namespace av1pf {
 
 struct FrameDesc;
 struct Item;
+struct CdefSearchDesc;
+struct CdefGreedy;
 
 // Grid cap of the grid-stride stage kernels: 8 resident CTAs on each of the
 // B200's 148 SMs.
@@ -61,6 +63,28 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
 // Sets cdef_kernel's dynamic shared-memory limit on the current device.
 cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
+// The encoder's CDEF search: per-block squared errors of every candidate
+// (one CTA per 64x64 block of frames[0]); counts the coding blocks into g->nb.
+void launch_cdef_search(const FrameDesc* frames, const CdefSearchDesc& d, CdefGreedy* g, cudaStream_t s);
+
+// Encoder searches (search.cu)
+// One greedy step of the CDEF search: every pair not yet chosen is scored
+// and the best is added (the last CTA to finish picks); `tot` holds
+// ny * nuv totals.
+void launch_cdef_greedy_step(const CdefSearchDesc& d, CdefGreedy* g, uint64_t* tot, double lambda, cudaStream_t s);
+// The CDEF search's outcome: each coding block's index into `table` (a copy
+// of cdef_idx, rows x stride) and the chosen pairs into `res`.
+void launch_cdef_greedy_finish(const CdefSearchDesc& d, const CdefGreedy* g, const int8_t* cdef_idx, int stride,
+                               int8_t* table, int32_t* res, cudaStream_t s);
+// Squared error of planes against the source over each plane's frame area:
+// sse[i] += sum over plane job i (a[i], b[i]: plane pointers, strides).
+struct SsePlane {
+  const uint8_t* a;
+  const uint8_t* b;
+  int64_t sa, sb_;  // strides in samples
+  int32_t w, h;
+};
+void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s);
 
 // Super-resolution (superres.cu)
 // `row_max`: the most source samples in a row among the launch's frames.

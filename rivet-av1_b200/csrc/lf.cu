@@ -103,7 +103,7 @@ __device__ __forceinline__ void append_edges_cta(EdgeAgg& agg, uint64_t* list_a,
 
 // Item: tile [x0,x1) x [y0,y1) of plane `plane` (samples). kind bit 0: copy
 // in -> cur over the tile; bit 1: decide the tile's 4x4 edges. 256 threads.
-__global__ void __launch_bounds__(256, 4) lf_prep_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 5) lf_prep_kernel(const FrameDesc* __restrict__ frames,
                                                       const Item* __restrict__ items, int n_items,
                                                       uint64_t* __restrict__ list_v, uint64_t* __restrict__ list_h,
                                                       uint32_t* __restrict__ counts, uint32_t cap) {

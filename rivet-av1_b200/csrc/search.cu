@@ -1,0 +1,276 @@
+// search.cu — the encoder's filter searches on the device: the greedy choice
+// of CDEF strength pairs (encoder/cdef.rs:195-250) over the error table that
+// cdef_search_kernel (cdef.cu) fills, and the plane errors of the
+// loop-filter level search (encoder/mod.rs:1494-1506).
+//
+// The reference sums block errors into an f64 in block order
+// (`total += best as f64`). Every block error is an integer far below 2^53,
+// so while a total stays below 2^53 each of those additions is exact and the
+// f64 total equals the exact integer sum: the kernels sum in u64 (in any
+// order) and convert. A total at or above 2^53 (frames of more than ~45,000
+// 64x64 blocks at 12 bits) is summed again in f64, in block order, as the
+// reference does. The cost of a choice, t + lambda * bits * nb, is evaluated
+// with round-to-nearest multiplies and adds in the reference's order (no
+// fused multiply-add).
+#include <cfloat>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace av1pf {
+
+namespace {
+
+constexpr uint64_t kExact = uint64_t(1) << 53;
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// The reference's f64 total of per-block minima, in block order (blocks that
+// code no index hold 0 everywhere and add nothing); Y == nullptr: of best[]
+// alone.
+__device__ double ordered_total(const uint64_t* best, const uint64_t* Y, const uint64_t* U, int nfb) {
+  double t = 0.0;
+  for (int b = 0; b < nfb; b++) {
+    const uint64_t v = Y ? min(__ldcg(&best[b]), Y[b] + U[b]) : __ldcg(&best[b]);
+    t = __dadd_rn(t, double(v));
+  }
+  return t;
+}
+
+// Step k of the greedy (encoder/cdef.rs:215-232): a warp per candidate pair
+// scores sum_b min(best[b], Y[yk][b] + UV[uk][b]) — the reference's
+// best_for(set + pair), since best[b] is the minimum over the set so far —
+// lanes striding over the blocks (candidate-major table: coalesced). The
+// last CTA to finish (a fenced arrival count; no CTA waits) takes the
+// smallest total, first in (yk, uk) order on ties, adds it to the set,
+// lowers best[], and at set sizes 1, 2, 4 and 8 prices the set.
+__global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchDesc d, CdefGreedy* g, double lambda,
+                                                             uint64_t* __restrict__ tot) {
+  const int nfb = d.fb_rows * d.fb_cols, ncand = d.ny * d.nuv;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int n = g->n;
+  const int c = blockIdx.x * 8 + warp;
+  if (c < ncand) {
+    const int yk = c / d.nuv, uk = c - yk * d.nuv;
+    bool in_set = false;
+    for (int i = 0; i < n; i++) in_set |= g->set_y[i] == yk && g->set_uv[i] == uk;
+    uint64_t acc = 0;
+    if (!in_set) {
+      const uint64_t* Y = d.sse + int64_t(yk) * nfb;
+      const uint64_t* U = d.sse + int64_t(d.ny + uk) * nfb;
+      for (int b = lane; b < nfb; b += 32) acc += min(d.best[b], Y[b] + U[b]);
+      acc = warp_sum_u64(acc);
+    }
+    if (lane == 0) tot[c] = in_set ? ~uint64_t(0) : acc;
+  }
+  __shared__ bool s_last;
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    s_last = atomicAdd(&g->arrived, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // --- argmin over (total, candidate) ---
+  __shared__ double s_t[256];
+  __shared__ int s_c[256];
+  double bt = DBL_MAX;
+  int bc = -1;
+  for (int k = tid; k < ncand; k += blockDim.x) {
+    const uint64_t u = __ldcg(&tot[k]);
+    if (u == ~uint64_t(0)) continue;  // in the set
+    const double t = u < kExact ? double(u)
+                                 : ordered_total(d.best, d.sse + int64_t(k / d.nuv) * nfb,
+                                                 d.sse + int64_t(d.ny + k % d.nuv) * nfb, nfb);
+    if (t < bt) {  // k ascends within a thread: the first of equals stays
+      bt = t;
+      bc = k;
+    }
+  }
+  s_t[tid] = bt;
+  s_c[tid] = bc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w; w >>= 1) {
+    if (tid < w) {
+      const double t2 = s_t[tid + w];
+      const int c2 = s_c[tid + w];
+      if (c2 >= 0 && (s_c[tid] < 0 || t2 < s_t[tid] || (t2 == s_t[tid] && c2 < s_c[tid]))) {
+        s_t[tid] = t2;
+        s_c[tid] = c2;
+      }
+    }
+    __syncthreads();
+  }
+  // no pair left (fewer than 8 candidates): the reference adds (0, 0)
+  const int pick = s_c[0] < 0 ? 0 : s_c[0];
+  const int py = pick / d.nuv, pu = pick - py * d.nuv;
+  if (tid == 0) {
+    g->set_y[n] = py;
+    g->set_uv[n] = pu;
+    g->n = n + 1;
+    g->arrived = 0;
+  }
+  // --- lower the per-block minima by the new pair ---
+  __shared__ uint64_t s_sum[8];
+  uint64_t part = 0;
+  {
+    const uint64_t* Y = d.sse + int64_t(py) * nfb;
+    const uint64_t* U = d.sse + int64_t(d.ny + pu) * nfb;
+    for (int b = tid; b < nfb; b += blockDim.x) {
+      const uint64_t m = min(__ldcg(&d.best[b]), Y[b] + U[b]);
+      d.best[b] = m;
+      part += m;
+    }
+  }
+  const int size = n + 1;
+  if ((size & (size - 1)) != 0) return;  // not a power of two: the level is not complete
+  // --- price the set of 1 << bits pairs (encoder/cdef.rs:233-239) ---
+  part = warp_sum_u64(part);
+  if (lane == 0) s_sum[warp] = part;
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t total = 0;
+    for (int w = 0; w < 8; w++) total += s_sum[w];
+    const int bits = __ffs(size) - 1;
+    double t;
+    if (total < kExact) {
+      t = double(total);
+    } else {
+      t = ordered_total(d.best, nullptr, nullptr, nfb);
+    }
+    const double pen = __dmul_rn(__dmul_rn(lambda, double(bits)), double(g->nb));
+    const double cost = __dadd_rn(t, pen);
+    const double prev = bits == 0 ? DBL_MAX : g->best_cost;
+    if (cost < prev) {
+      g->best_cost = cost;
+      g->best_bits = bits;
+    } else if (bits == 0) {
+      g->best_cost = DBL_MAX;
+    }
+  }
+}
+
+// The outcome (encoder/cdef.rs:241-250): each coding block's index is the
+// first of the chosen 1 << best_bits pairs with its least error; the other
+// table entries are copied.
+__global__ void cdef_greedy_finish_kernel(const CdefSearchDesc d, const CdefGreedy* __restrict__ g,
+                                          const int8_t* __restrict__ cdef_idx, int stride, int8_t* __restrict__ table,
+                                          int32_t* __restrict__ res) {
+  const int nfb = d.fb_rows * d.fb_cols;
+  const int m = 1 << g->best_bits;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e == 0) {
+    res[0] = int32_t(g->nb);
+    res[1] = g->best_bits;
+    for (int i = 0; i < 8; i++) {
+      res[2 + i] = i < m ? g->set_y[i] : 0;
+      res[10 + i] = i < m ? g->set_uv[i] : 0;
+    }
+  }
+  if (e >= d.fb_rows * stride) return;
+  const int r = e / stride, c = e - r * stride;
+  int8_t v = cdef_idx[e];
+  if (c < d.fb_cols && v >= 0) {
+    const int b = r * d.fb_cols + c;
+    uint64_t best = ~uint64_t(0);
+    int pick = 0;
+    for (int i = 0; i < m; i++) {
+      const uint64_t x = d.sse[int64_t(g->set_y[i]) * nfb + b] + d.sse[int64_t(d.ny + g->set_uv[i]) * nfb + b];
+      if (x < best) {
+        best = x;
+        pick = i;
+      }
+    }
+    v = int8_t(pick);
+  }
+  table[e] = v;
+}
+
+// Squared error of one plane pair over rows [4*blockIdx.x, +4) of job
+// blockIdx.y: 16-byte loads (planes and rows are 16-byte aligned), the
+// ragged end of a row sample by sample.
+struct SseJobs {
+  SsePlane p[18];
+};
+
+__global__ void __launch_bounds__(256) plane_sse_kernel(const SseJobs jobs, int sb, uint64_t* __restrict__ sse) {
+  const SsePlane j = jobs.p[blockIdx.y];
+  const int y0 = blockIdx.x * 4;
+  uint64_t acc = 0;
+  if (y0 < j.h) {
+    const int per = 16 / sb;  // samples per 16 bytes
+    const int nv = j.w / per;
+    const int rows = min(4, j.h - y0);
+    for (int k = threadIdx.x; k < rows * nv; k += blockDim.x) {
+      const int r = y0 + k / nv, v = k % nv;
+      const uint4 qa = *reinterpret_cast<const uint4*>(j.a + (int64_t(r) * j.sa + int64_t(v) * per) * sb);
+      const uint4 qb = *reinterpret_cast<const uint4*>(j.b + (int64_t(r) * j.sb_ + int64_t(v) * per) * sb);
+      const uint32_t wa[4] = {qa.x, qa.y, qa.z, qa.w}, wb[4] = {qb.x, qb.y, qb.z, qb.w};
+      uint32_t s = 0;  // 8 squares below 4096^2, or 16 below 256^2: fits
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (sb == 2) {
+          const int d0 = int(wa[q] & 0xffffu) - int(wb[q] & 0xffffu), d1 = int(wa[q] >> 16) - int(wb[q] >> 16);
+          s += uint32_t(d0 * d0) + uint32_t(d1 * d1);
+        } else {
+#pragma unroll
+          for (int h = 0; h < 4; h++) {
+            const int dd = int((wa[q] >> (8 * h)) & 0xffu) - int((wb[q] >> (8 * h)) & 0xffu);
+            s += uint32_t(dd * dd);
+          }
+        }
+      }
+      acc += s;
+    }
+    const int tail = j.w - nv * per;
+    for (int k = threadIdx.x; k < rows * tail; k += blockDim.x) {
+      const int r = y0 + k / tail, x = nv * per + k % tail;
+      int dd;
+      if (sb == 2)
+        dd = int(reinterpret_cast<const uint16_t*>(j.a)[int64_t(r) * j.sa + x]) -
+             int(reinterpret_cast<const uint16_t*>(j.b)[int64_t(r) * j.sb_ + x]);
+      else
+        dd = int(j.a[int64_t(r) * j.sa + x]) - int(j.b[int64_t(r) * j.sb_ + x]);
+      acc += uint64_t(dd * dd);
+    }
+  }
+  __shared__ uint64_t s_sum[8];
+  acc = warp_sum_u64(acc);
+  if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < 8; w++) t += s_sum[w];
+    if (t) atomicAdd(reinterpret_cast<unsigned long long*>(&sse[blockIdx.y]), static_cast<unsigned long long>(t));
+  }
+}
+
+}  // namespace
+
+void launch_cdef_greedy_step(const CdefSearchDesc& d, CdefGreedy* g, uint64_t* tot, double lambda, cudaStream_t s) {
+  const int ncand = d.ny * d.nuv;
+  cdef_greedy_step_kernel<<<(ncand + 7) / 8, 256, 0, s>>>(d, g, lambda, tot);
+  note_launch();
+}
+
+void launch_cdef_greedy_finish(const CdefSearchDesc& d, const CdefGreedy* g, const int8_t* cdef_idx, int stride,
+                               int8_t* table, int32_t* res, cudaStream_t s) {
+  const int n = d.fb_rows * stride;
+  cdef_greedy_finish_kernel<<<(n + 255) / 256, 256, 0, s>>>(d, g, cdef_idx, stride, table, res);
+  note_launch();
+}
+
+void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s) {
+  if (n <= 0 || rows_max <= 0) return;
+  SseJobs j{};
+  for (int i = 0; i < n && i < 18; i++) j.p[i] = jobs[i];
+  plane_sse_kernel<<<dim3(unsigned((rows_max + 3) / 4), unsigned(n)), 256, 0, s>>>(j, sample_bytes, sse);
+  note_launch();
+}
+
+}  // namespace av1pf

@@ -1,0 +1,154 @@
+"""The encoder's filter searches on the GPU (av1pf_cdef_search,
+av1pf_lf_search) against the oracle, bit for bit: the chosen CDEF strengths,
+bits and damping, the per-block index table and every candidate's per-block
+error; the loop-filter levels and every scale's plane errors. Shapes cover
+8/10/12-bit, one- and two-byte samples, 4:2:0, 4:2:2, 4:4:4 and monochrome,
+ragged frame edges, full HD, frames with no coding block, and both
+candidate lists."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import av1pf as A
+import oracle as O
+from conftest import cuda_available
+from test_search import CASES, coding_blocks
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")]
+
+if cuda_available():
+    import gpu_util as G
+    import torch
+
+GPU_CASES = dict(CASES)
+GPU_CASES["1920x1080_10b"] = dict(width=1920, height=1080, bit_depth=10, seed=21)
+GPU_CASES["1000x600_12b_444"] = dict(width=1000, height=600, bit_depth=12, subsampling_x=0, subsampling_y=0,
+                                     seed=22)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.Ctx()
+    yield c
+    c.close()
+
+
+def gpu_cdef_search(ctx, sf, df, cur, src, q, lam, thorough):
+    info = sf.f.info
+    fbr, fbc = (info.mi_rows + 15) // 16, (info.mi_cols + 15) // 16
+    ny, nuv = A.CDEF_SEARCH_N[bool(thorough)]
+    dcur, dsrc = G.DevPlanes.from_host(info, cur), G.DevPlanes.from_host(info, src)
+    res = A.CdefSearchResult()
+    table = np.zeros(fbr * df.maps.cdef_stride, np.int8)
+    sse = np.zeros((fbr * fbc, ny + nuv), np.uint64)
+    A.check(A.lib().av1pf_cdef_search(ctx.p, C.byref(info), C.byref(df.maps), dcur.c, dsrc.c, q, lam,
+                                      int(thorough), C.byref(res), table.ctypes.data, sse.ctypes.data, None),
+            "av1pf_cdef_search")
+    return res, table, sse
+
+
+def assert_cdef_same(g, o, what):
+    (rg, tg, sg), (ro, to, so) = g, o
+    assert (rg.damping_minus_3, rg.bits) == (ro.damping_minus_3, ro.bits), what
+    assert rg.pairs() == ro.pairs(), what
+    assert np.array_equal(sg, so), f"{what}: block errors differ at {np.argwhere(sg != so)[:5]}"
+    assert np.array_equal(tg, to), what
+
+
+@pytest.mark.parametrize("thorough", [False, True], ids=["fast", "thorough"])
+@pytest.mark.parametrize("name", sorted(GPU_CASES))
+def test_cdef_search_matches_oracle(ctx, name, thorough):
+    sf = A.SynthHandle(**GPU_CASES[name])
+    cur, src = O.search_inputs(sf, 31)
+    df = G.DevFrame(sf)
+    for q, lam in ((30, 0.0), (140, 40.0), (250, 900.0)):
+        o = O.cdef_search(sf, cur, src, q, lam, thorough)
+        g = gpu_cdef_search(ctx, sf, df, cur, src, q, lam, thorough)
+        assert_cdef_same(g, o, f"{name} q{q} lambda{lam}")
+
+
+def test_cdef_search_picks_filters_on_noisy_reconstruction(ctx):
+    """A reconstruction with strong block noise: the search chooses several
+    nonzero strengths, and GPU and oracle agree on them."""
+    sf = A.SynthHandle(**GPU_CASES["1920x1080_10b"])
+    cur, src = O.search_inputs(sf, 32, amp=24)
+    o = O.cdef_search(sf, cur, src, 120, 1.0, False)
+    g = gpu_cdef_search(ctx, sf, G.DevFrame(sf), cur, src, 120, 1.0, False)
+    assert_cdef_same(g, o, "noisy 1080p")
+    assert o[0].bits >= 1 and any(p != (0, 0, 0, 0) for p in o[0].pairs())
+
+
+def test_cdef_search_without_coding_blocks(ctx):
+    sf = A.SynthHandle(**GPU_CASES["200x120_8b"])
+    idx, _, _ = coding_blocks(sf)
+    idx[:] = -1
+    cur, src = O.search_inputs(sf, 33)
+    o = O.cdef_search(sf, cur, src, 200, 5.0, True)
+    g = gpu_cdef_search(ctx, sf, G.DevFrame(sf), cur, src, 200, 5.0, True)
+    assert_cdef_same(g, o, "no coding blocks")
+    assert g[0].bits == 0 and g[0].damping_minus_3 == 0
+
+
+def test_cdef_search_rejects_bad_arguments(ctx):
+    sf = A.SynthHandle(**GPU_CASES["256x144_10b"])
+    cur, src = O.search_inputs(sf, 34)
+    df = G.DevFrame(sf)
+    info = sf.f.info
+    dcur, dsrc = G.DevPlanes.from_host(info, cur), G.DevPlanes.from_host(info, src)
+    res = A.CdefSearchResult()
+    L = A.lib()
+    for q, lam in ((-1, 1.0), (256, 1.0), (10, float("nan")), (10, -1.0), (10, float("inf"))):
+        rc = L.av1pf_cdef_search(ctx.p, C.byref(info), C.byref(df.maps), dcur.c, dsrc.c, q, lam, 0, C.byref(res),
+                                 None, None, None)
+        assert rc == A.ERR_INVALID_INPUT, (q, lam)
+    assert L.av1pf_cdef_search(ctx.p, C.byref(info), C.byref(df.maps), dcur.c, None, 10, 1.0, 0, C.byref(res),
+                               None, None, None) == A.ERR_INVALID_INPUT
+
+
+def gpu_lf_search(ctx, sf, cur, src, params=None):
+    info = sf.f.info
+    df = G.DevFrame(sf)
+    dcur, dsrc = G.DevPlanes.from_host(info, cur), G.DevPlanes.from_host(info, src)
+    levels = (C.c_int32 * 4)()
+    sse = np.zeros((6, 3), np.uint64)
+    A.check(A.lib().av1pf_lf_search(ctx.p, C.byref(info), C.byref(params if params is not None else sf.f.params),
+                                    C.byref(df.maps), dcur.c, dsrc.c, levels, sse.ctypes.data, None),
+            "av1pf_lf_search")
+    torch.cuda.synchronize()
+    # the reconstruction is left unfiltered
+    for p in range(info.num_planes):
+        a = dcur.host(p)
+        assert np.array_equal(a, cur.arrays[p]), "av1pf_lf_search changed its input"
+    return list(levels), sse
+
+
+@pytest.mark.parametrize("name", sorted(GPU_CASES))
+def test_lf_search_matches_oracle(ctx, name):
+    sf = A.SynthHandle(**GPU_CASES[name])
+    cur, src = O.search_inputs(sf, 35)
+    lv_o, sse_o = O.lf_search(sf, cur, src)
+    lv_g, sse_g = gpu_lf_search(ctx, sf, cur, src)
+    assert np.array_equal(sse_g, sse_o), name
+    assert lv_g == lv_o, name
+
+
+def test_lf_search_picks_levels_on_blocky_reconstruction(ctx):
+    """Starting levels with blocking artefacts to remove: a nonzero level is
+    chosen and GPU and oracle agree on every scale's errors."""
+    sf = A.SynthHandle(**GPU_CASES["256x144_10b"])
+    src = O.HostPlanes.like_synth(sf)
+    rng = np.random.default_rng(36)
+    cur = []
+    for a in src.arrays:
+        h, w = a.shape
+        steps = np.kron(rng.integers(-40, 41, size=((h + 7) // 8, (w + 7) // 8)), np.ones((8, 8), np.int64))[:h, :w]
+        cur.append(np.clip(a.astype(np.int64) + steps, 0, 1023).astype(a.dtype))
+    cur = O.HostPlanes(cur)
+    p = A.Params.from_buffer_copy(sf.f.params)
+    for k, v in enumerate((30, 30, 20, 20)):
+        p.loop_filter_level[k] = v
+    lv_o, sse_o = O.lf_search(sf, cur, src, params=p)
+    lv_g, sse_g = gpu_lf_search(ctx, sf, cur, src, params=p)
+    assert np.array_equal(sse_g, sse_o) and lv_g == lv_o
+    assert lv_o[0] > 0
