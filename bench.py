@@ -26,6 +26,10 @@ The same run reports, beside the headline:
                replayed from a CUDA graph) against the per-frame GPU path
                on the same frames, outputs compared bit for bit;
   c3_4k        4K chains with superres + film grain (10-bit 4:2:0, 12-bit 4:4:4);
+  serve        continuous-batching server: 32 streams, p50/p99 latency;
+  search       the encoder's filter searches (CDEF strengths, fast and
+               thorough lists; loop-filter levels) per 1080p / 4K frame,
+               against the oracle's time for the same call;
   cpu_baseline the CPU oracle (this repo's C++ restatement of the reference's
                filters, all host threads) on a bounded sample.
 
@@ -212,7 +216,8 @@ def main_gpu(args):
         ctx = G.Ctx(local)
         fn = {"mix": lambda: bench_mix(args, ctx, rank, torch.cuda.synchronize, lambda v: v),
               "c3": lambda: bench_4k(args, ctx, torch.cuda.synchronize, lambda v: v),
-              "serve": lambda: bench_serve(args, ctx, rank)}[args.only]
+              "serve": lambda: bench_serve(args, ctx, rank),
+              "search": lambda: bench_search(args, ctx, rank, world)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
         ctx.close()
         ranks.close()
@@ -404,6 +409,7 @@ def main_gpu(args):
         result["mix"] = bench_mix(args, ctx, rank, barrier, max_over_ranks)
         result["c3_4k"] = bench_4k(args, ctx, barrier, max_over_ranks)
         result["serve"] = bench_serve(args, ctx, rank)
+        result["search"] = bench_search(args, ctx, rank, world)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     if rank == 0 and world == 1:
@@ -547,6 +553,94 @@ def bench_4k(args, ctx, barrier, max_over_ranks):
                      "stages_ms": {n: round(float(ms5[k]) / max(1, calls.value), 4)
                                    for k, n in enumerate(["loop_filter", "cdef", "superres", "loop_restoration",
                                                           "output"])}}
+    return res
+
+
+def search_cpu(sf, cur, src, thorough, q, lam):
+    """The oracle's CDEF and loop-filter searches on all host threads: the
+    CPU leg of the search section (one call each; returns their ms and
+    results)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    hc, hs = O.HostPlanes(cur), O.HostPlanes(src)
+    t = time.perf_counter()
+    res, table, _ = O.cdef_search(sf, hc, hs, q, lam, thorough)
+    cdef_ms = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    levels, _ = O.lf_search(sf, hc, hs)
+    lf_ms = (time.perf_counter() - t) * 1e3
+    return cdef_ms, lf_ms, (res.pairs(), res.bits, table), levels
+
+
+def bench_search(args, ctx, rank, world):
+    """The encoder's filter searches (encoder/cdef.rs:52-251,
+    encoder/mod.rs:1457-1506) on one frame per call: CDEF strength search
+    with the fast and thorough candidate lists and the loop-filter level
+    search, device-resident planes, host clock around each synchronous
+    call; the oracle's time for the same call beside it (rank 0, N = 1)."""
+    import gpu_util as G
+    L = A.lib()
+    res = {}
+    q, lam = 120, 40.0
+    for name, cfg in [("1080p_10bit", dict(width=1920, height=1080, bit_depth=10, seed=501)),
+                      ("4k_10bit", dict(width=3840, height=2160, bit_depth=10, seed=502))]:
+        sf = A.SynthHandle(**cfg)
+        cur, src = A.synth_search_planes(sf, 7, amp=24)
+        info = sf.f.info
+        df = G.DevFrame(sf)
+        dcur, dsrc = G.DevPlanes(info, [(a.shape[1], a.shape[0]) for a in cur], [a.shape[1] for a in cur]), \
+            G.DevPlanes(info, [(a.shape[1], a.shape[0]) for a in src], [a.shape[1] for a in src])
+        import torch
+        for p in range(info.num_planes):
+            dcur.t[p].copy_(torch.from_numpy(cur[p].view(np.uint8).reshape(-1)))
+            dsrc.t[p].copy_(torch.from_numpy(src[p].view(np.uint8).reshape(-1)))
+        fbr = (info.mi_rows + 15) // 16
+        out = {}
+        choice = {}
+        for th in (0, 1):
+            r = A.CdefSearchResult()
+            table = np.zeros(fbr * df.maps.cdef_stride, np.int8)
+
+            def run():
+                A.check(L.av1pf_cdef_search(ctx.p, C.byref(info), C.byref(df.maps), dcur.c, dsrc.c, q, lam, th,
+                                            C.byref(r), table.ctypes.data, None, None), "av1pf_cdef_search")
+            for _ in range(max(3, args.warmup)):
+                run()
+            reps = 30
+            t = time.perf_counter()
+            for _ in range(reps):
+                run()
+            out["cdef_thorough_ms" if th else "cdef_fast_ms"] = round((time.perf_counter() - t) / reps * 1e3, 4)
+            choice[th] = (r.pairs(), r.bits, table.copy())
+        lv = (C.c_int32 * 4)()
+
+        def runl():
+            A.check(L.av1pf_lf_search(ctx.p, C.byref(info), C.byref(sf.f.params), C.byref(df.maps), dcur.c, dsrc.c,
+                                      lv, None, None), "av1pf_lf_search")
+        for _ in range(max(3, args.warmup)):
+            runl()
+        reps = 30
+        t = time.perf_counter()
+        for _ in range(reps):
+            runl()
+        out["lf_ms"] = round((time.perf_counter() - t) / reps * 1e3, 4)
+        out["chosen"] = {"cdef_fast": {"bits": choice[0][1], "pairs": choice[0][0]}, "lf_levels": list(lv)}
+        if rank == 0 and world == 1 and args.cpu_seconds > 0:
+            exact = True
+            for th in (0, 1):
+                cms, lms, (pairs, bits, table), levels = search_cpu(sf, cur, src, bool(th), q, lam)
+                exact &= pairs == choice[th][0] and bits == choice[th][1] and np.array_equal(table, choice[th][2])
+                exact &= levels == list(lv)
+                key = "cdef_thorough" if th else "cdef_fast"
+                out.setdefault("cpu_oracle_ms", {})[key] = round(cms, 1)
+                out["cpu_oracle_ms"]["lf"] = round(lms, 1)
+            out["cpu_threads"] = os.cpu_count()
+            out["same_choice_as_oracle"] = bool(exact)
+            out["speedup_vs_oracle"] = {k: round(out["cpu_oracle_ms"][k] / out[k + "_ms"], 1)
+                                        for k in ("cdef_fast", "cdef_thorough", "lf")}
+        res[name] = out
+    res["inputs"] = (f"seeded synthetic frames; reconstruction = source + seeded 4x4-block noise (+-24) and "
+                     f"per-sample noise; base_q_idx {q}, lambda {lam}")
     return res
 
 
@@ -739,7 +833,7 @@ def main():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-extras", action="store_true")
-    ap.add_argument("--only", choices=["mix", "c3", "serve"], default=None,
+    ap.add_argument("--only", choices=["mix", "c3", "serve", "search"], default=None,
                     help="run one extra section alone (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -125,23 +125,9 @@ def chain(sf, threads=0, want_frame=True):
 
 
 def search_inputs(sf, seed, amp=None):
-    """(cur, src) HostPlanes for the encoder searches on a SynthHandle: the
-    source is the synthetic frame's planes, the reconstruction the source
-    plus seeded noise of +-amp (default 3 << (bit_depth - 8)) in blocks of
-    4x4, clipped to the sample range."""
-    info = sf.f.info
-    src = HostPlanes.like_synth(sf)
-    rng = np.random.default_rng(seed)
-    a = (3 << (info.bit_depth - 8)) if amp is None else amp
-    hi = (1 << info.bit_depth) - 1
-    cur = []
-    for arr in src.arrays:
-        h, w = arr.shape
-        blk = rng.integers(-a, a + 1, size=((h + 3) // 4, (w + 3) // 4))
-        fine = rng.integers(-(a // 2), a // 2 + 1, size=(h, w))
-        noise = np.kron(blk, np.ones((4, 4), np.int64))[:h, :w] + fine
-        cur.append(np.clip(arr.astype(np.int64) + noise, 0, hi).astype(arr.dtype))
-    return HostPlanes(cur), src
+    """(cur, src) HostPlanes of av1pf.synth_search_planes."""
+    cur, src = A.synth_search_planes(sf, seed, amp)
+    return HostPlanes(cur), HostPlanes(src)
 
 
 def cdef_search(sf, cur, src, q, lam, thorough, threads=0):

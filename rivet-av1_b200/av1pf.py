@@ -277,6 +277,42 @@ class SynthHandle:
         return ((i.upscaled_width + sx) >> sx, (i.frame_height + sy) >> sy)
 
 
+def synth_planes(sf):
+    """Copies of a synthetic frame's planes (allocated layout) as numpy arrays."""
+    import numpy as np
+    f = sf.f
+    dt = np.uint8 if f.info.sample_bytes == 1 else np.uint16
+    out = []
+    for p in range(f.info.num_planes):
+        pl = f.planes[p]
+        n = pl.height * pl.stride
+        buf = (C.c_uint8 * (n * np.dtype(dt).itemsize)).from_address(pl.data)
+        out.append(np.frombuffer(buf, dtype=dt).reshape(pl.height, pl.stride).copy())
+    return out
+
+
+def synth_search_planes(sf, seed, amp=None):
+    """(reconstruction, source) plane lists for the encoder searches on a
+    SynthHandle: the source is the synthetic frame's planes, the
+    reconstruction the source plus seeded noise of +-amp (default
+    3 << (bit_depth - 8)) in 4x4 blocks and +-amp/2 per sample, clipped to
+    the sample range."""
+    import numpy as np
+    info = sf.f.info
+    src = synth_planes(sf)
+    rng = np.random.default_rng(seed)
+    a = (3 << (info.bit_depth - 8)) if amp is None else amp
+    hi = (1 << info.bit_depth) - 1
+    cur = []
+    for arr in src:
+        h, w = arr.shape
+        blk = rng.integers(-a, a + 1, size=((h + 3) // 4, (w + 3) // 4))
+        fine = rng.integers(-(a // 2), a // 2 + 1, size=(h, w))
+        noise = np.kron(blk, np.ones((4, 4), np.int64))[:h, :w] + fine
+        cur.append(np.clip(arr.astype(np.int64) + noise, 0, hi).astype(arr.dtype))
+    return cur, src
+
+
 def frame_bytes(info):
     """Bytes of the packed output Frame (frame.rs:135-158) — computed here
     without the library so CPU-only code can size buffers."""

@@ -17,6 +17,7 @@
 // never picks it, and an unsigned min never picks it. In the direction
 // search each thread takes one 8x8 block and two of the 8 directions (one
 // pair per warp), so the partial-sum bins are compile-time register indices.
+#include "av1_tables.h"
 #include "common.cuh"
 #include "kernels.h"
 #include "lf_core.cuh"
@@ -541,38 +542,171 @@ __device__ __forceinline__ uint64_t warp_sum_u32(uint32_t v) {
   return (uint64_t(hi) << 16) + lo;
 }
 
-// Squared errors against the source window `s` (kNA outside the frame) of
-// one row of n samples filtered with `t` (MODE as cdef_px; 3 = unfiltered).
-template <int MODE>
-__device__ __forceinline__ uint32_t row_sse(const int16_t* c, const int16_t* s, int n, const TapsDev& t) {
-  uint32_t acc = 0;
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    if (j < n && s[j] != kNA) {
-      const int v = MODE == 3 ? int(c[j]) : cdef_px<MODE>(c + j, t);
-      const int d = v - s[j];
-      acc += uint32_t(d * d);
-    }
-  }
-  return acc;
+// The search's candidate strengths (encoder/cdef.rs:60-80): primaries of
+// the fast and thorough lists, secondaries decoded (coded 3 is 4).
+__host__ __device__ constexpr int search_y_pri(bool th, int i) {
+  constexpr int f[7] = {0, 1, 2, 4, 6, 9, 12}, t[11] = {0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15};
+  return th ? t[i] : f[i];
+}
+__host__ __device__ constexpr int search_uv_pri(bool th, int i) {
+  constexpr int f[5] = {0, 1, 2, 4, 7}, t[8] = {0, 1, 2, 3, 4, 6, 8, 11};
+  return th ? t[i] : f[i];
+}
+__host__ __device__ constexpr int search_sec(int j) { return j == 3 ? 4 : j; }
+
+// |constrain(d)| (cdef.rs:48-51) from |d|: min(|d|, max(0, str - (|d| >> adj))).
+// `mone` is -1 at run time but opaque to the compiler, so the subtraction
+// is a multiply-add (the integer ALU pipe is this kernel's bound).
+__device__ __forceinline__ int cmag(int ad, int str, int adj, int mone) {
+  return min(ad, max((ad >> adj) * mone + str, 0));
 }
 
-// The rows of one thread's share of an 8x8 block (rows rr and rr+4 of the
-// block's h rows, w samples each) under candidate taps, as squared error.
-__device__ __forceinline__ uint32_t block_rows_sse(const int16_t* c, const int16_t* s, int w, int h, int mode,
-                                                   const TapsDev& t) {
-  uint32_t acc = 0;
-  for (int q = 0; q < h / 4; q++) {
-    const int16_t* cq = c + q * 4 * kS;
-    const int16_t* sq = s + q * 4 * kS;
-    switch (mode) {
-      case 0: acc += row_sse<0>(cq, sq, w, t); break;
-      case 1: acc += row_sse<1>(cq, sq, w, t); break;
-      case 2: acc += row_sse<2>(cq, sq, w, t); break;
-      default: acc += row_sse<3>(cq, sq, w, t); break;
+// Window offsets of the secondary taps of direction 0 (the taps of the
+// candidates with primary strength 0, whose direction is 0): directions 6
+// and 2 (postfilter.rs:489-511).
+constexpr int8_t kSearchDirs[8][2][2] = AV1T_CDEF_DIRECTIONS;
+constexpr int kA0 = kSearchDirs[6][0][0] * kS + kSearchDirs[6][0][1];  // weight 2
+constexpr int kA1 = kSearchDirs[2][0][0] * kS + kSearchDirs[2][0][1];  // weight 2
+constexpr int kA2 = kSearchDirs[6][1][0] * kS + kSearchDirs[6][1][1];  // weight 1
+constexpr int kA3 = kSearchDirs[2][1][0] * kS + kSearchDirs[2][1][1];  // weight 1
+
+// The squared error of one sample under every (primary, secondary) pair of
+// a plane's list, added to acc[i * NS + j] (encoder/cdef.rs:113-188).
+// A pair's filter sum is P(primary) + S(secondary): the primary taps'
+// constrained sum depends on the primary strength alone and the secondary
+// taps' on the secondary strength alone, so each distinct P and S is
+// computed once per sample and every pair costs a few adds. A tap's
+// constrained difference is sign(d) * cmag(|d|): |d| and the signed weight
+// are set once per sample. Pairs with primary strength 0 filter in
+// direction 0 (secondary taps at directions 6 and 2); the others in the
+// block's direction (offsets `o`: primary k0, k1, secondary lo k0, hi k0,
+// lo k1, hi k1). The result is clamped to the block direction's available
+// taps (cdef.rs:54-90); with one kind of tap (a zero primary or secondary
+// strength) the weights sum to 12 < 16 and the result already lies within
+// the taps' range, so those pairs skip the clamp.
+template <int NP, int NS>
+__device__ __forceinline__ void sample_pairs(const int16_t* c, int s, const int (&o)[6], const int (&pstr)[NP],
+                                             const int (&padj)[NP], const int (&pw0)[NP], const int (&pw1)[NP],
+                                             const int (&sstr)[NS], const int (&sadj)[NS], int one, int mone,
+                                             uint32_t (&acc)[NP * NS]) {
+  const int x = c[0];
+  const int nx = x * mone, ns = s * mone;
+  int aB[12], gB[12];  // |d|, and sign(d) (primary) or the signed weight (secondary)
+  int mx = x;
+  unsigned mn = unsigned(x);
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    const int p0 = c[o[k]], p1 = c[-o[k]];
+    mx = max(mx, max(p0, p1));
+    mn = min(mn, min(unsigned(p0), unsigned(p1)));
+    const int d0 = p0 * one + nx, d1 = p1 * one + nx;
+    const int w = k < 2 ? 1 : (k < 4 ? 2 : 1);
+    aB[2 * k] = abs(d0);
+    aB[2 * k + 1] = abs(d1);
+    gB[2 * k] = (d0 >> 31) * (2 * w) + w;
+    gB[2 * k + 1] = (d1 >> 31) * (2 * w) + w;
+  }
+  int aA[8], gA[8];
+  {
+    const int offs[4] = {kA0, kA1, kA2, kA3};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int d0 = c[offs[k]] * one + nx, d1 = c[-offs[k]] * one + nx;
+      const int w = k < 2 ? 2 : 1;
+      aA[2 * k] = abs(d0);
+      aA[2 * k + 1] = abs(d1);
+      gA[2 * k] = (d0 >> 31) * (2 * w) + w;
+      gA[2 * k + 1] = (d1 >> 31) * (2 * w) + w;
     }
   }
-  return acc;
+  // secondary sums per nonzero secondary strength, both directions
+  int SA[NS], SB[NS];
+  SA[0] = SB[0] = 0;
+#pragma unroll
+  for (int j = 1; j < NS; j++) {
+    int sa = 0, sb = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      sa = gA[k] * cmag(aA[k], sstr[j], sadj[j], mone) + sa;
+      sb = gB[4 + k] * cmag(aB[4 + k], sstr[j], sadj[j], mone) + sb;
+    }
+    SA[j] = sa;
+    SB[j] = sb;
+  }
+  const int x16 = x * 16 + 8;  // x + round(sum / 16) = (x16 + sum - (sum < 0)) >> 4
+#pragma unroll
+  for (int j = 0; j < NS; j++) {  // primary strength 0: secondary taps alone
+    const int v = (x16 + SA[j] + (SA[j] >> 31)) >> 4;
+    const int e = v * one + ns;
+    acc[j] = uint32_t(e * e) + acc[j];
+  }
+#pragma unroll
+  for (int i = 1; i < NP; i++) {
+    const int q0 = gB[0] * cmag(aB[0], pstr[i], padj[i], mone) + gB[1] * cmag(aB[1], pstr[i], padj[i], mone);
+    const int q1 = gB[2] * cmag(aB[2], pstr[i], padj[i], mone) + gB[3] * cmag(aB[3], pstr[i], padj[i], mone);
+    const int P = pw0[i] * q0 + pw1[i] * q1;
+    {  // secondary strength 0: primary taps alone
+      const int v = (x16 + P + (P >> 31)) >> 4;
+      const int e = v * one + ns;
+      acc[i * NS] = uint32_t(e * e) + acc[i * NS];
+    }
+#pragma unroll
+    for (int j = 1; j < NS; j++) {
+      const int sum = P * one + SB[j];
+      const int v = min(max((x16 + sum + (sum >> 31)) >> 4, int(mn)), mx);
+      const int e = v * one + ns;
+      acc[i * NS + j] = uint32_t(e * e) + acc[i * NS + j];
+    }
+  }
+}
+
+// Strengths, damping adjustments and primary tap weights of one plane's
+// list (postfilter.rs:489-511): pstr[i] is the primary strength after the
+// block's variance adjustment (luma, postfilter.rs:318-323; `var` < 0 for
+// chroma, which has none).
+template <int NP, int NS, bool TH, bool LUMA>
+__device__ __forceinline__ void pair_taps(int cs, int damping, int32_t var, int (&pstr)[NP], int (&padj)[NP],
+                                          int (&pw0)[NP], int (&pw1)[NP], int (&sstr)[NS], int (&sadj)[NS]) {
+  const int var_str = (var >> 6) != 0 ? min(floor_log2(uint32_t(var >> 6)), 12) : 0;
+#pragma unroll
+  for (int i = 0; i < NP; i++) {
+    const int p0 = (LUMA ? search_y_pri(TH, i) : search_uv_pri(TH, i)) << cs;
+    const int p = LUMA ? (var != 0 ? (p0 * (4 + var_str) + 8) >> 4 : 0) : p0;
+    pstr[i] = p;
+    padj[i] = p ? max(damping - floor_log2(uint32_t(p)), 0) : 0;
+    const bool odd = (p >> cs) & 1;
+    pw0[i] = odd ? 3 : 4;
+    pw1[i] = odd ? 3 : 2;
+  }
+#pragma unroll
+  for (int j = 0; j < NS; j++) {
+    const int q = search_sec(j) << cs;
+    sstr[j] = q;
+    sadj[j] = q ? max(damping - floor_log2(uint32_t(q)), 0) : 0;
+  }
+}
+
+// Block-direction offsets of the taps (primary k0, k1, secondary lo k0,
+// hi k0, lo k1, hi k1) in window samples.
+__device__ __forceinline__ void dir_offsets(const int16_t (*doff)[2], int dir, int (&o)[6]) {
+  const int dlo = (dir + 6) & 7, dhi = (dir + 2) & 7;
+  o[0] = doff[dir][0];
+  o[1] = doff[dir][1];
+  o[2] = doff[dlo][0];
+  o[3] = doff[dhi][0];
+  o[4] = doff[dlo][1];
+  o[5] = doff[dhi][1];
+}
+
+// Adds warp sums of acc[] to red[warp][base + k].
+template <int N>
+__device__ __forceinline__ void warp_reduce_pairs(const uint32_t (&acc)[N], uint64_t (*red)[kSearchMaxY + kSearchMaxUV],
+                                                  int warp, int lane, int base) {
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    const uint64_t ws = warp_sum_u32(acc[k]);
+    if (lane == 0) red[warp][base + k] = ws;
+  }
 }
 
 // The encoder's CDEF search, error tables (encoder/cdef.rs:103-190): one CTA
@@ -580,17 +714,18 @@ __device__ __forceinline__ uint32_t block_rows_sse(const int16_t* c, const int16
 // decoder's kernel (2-sample border, kNA outside the mode-info area) with
 // the source beside them (kNA outside the frame, so block_sse's crop,
 // encoder/cdef.rs:261-285, is a test per sample); the direction search is
-// the decoder's. Then every candidate pair filters every 8x8 block CDEF
-// would filter (a warp per row of 8x8 blocks, lanes = (block, row pair)),
-// and its squared error is summed over the CTA per candidate: the filter
-// and the error of a sample never leave registers. The filter mode is
-// chosen per candidate (uniform over the CTA): zero strengths drop their
-// taps exactly as in the decoder's kernel.
-__global__ void __launch_bounds__(256, 3) cdef_search_kernel(const FrameDesc* __restrict__ frames,
-                                                           const CdefSearchDesc d, CdefGreedy* __restrict__ g) {
+// the decoder's. Then each thread takes 16 luma samples of one 8x8 block
+// (rows r and r + 4; a warp per row of blocks) and scores every pair on
+// each (sample_pairs), the errors of each pair accumulating in a register;
+// the chroma samples of the same block follow. TH: the thorough lists.
+template <bool TH>
+__global__ void __launch_bounds__(256, 2) cdef_search_kernel(const FrameDesc* __restrict__ frames,
+                                                                    const CdefSearchDesc d, CdefGreedy* __restrict__ g) {
+  constexpr int NYP = TH ? 11 : 7, NUVP = TH ? 8 : 5, NYS = 4, NUVS = 3;
+  constexpr int NY = NYP * NYS, NUV = NUVP * NUVS;
   constexpr int R = 64, top = 2, wrows = R + 2 * top;
   extern __shared__ __align__(16) int16_t cs_smem[];
-  auto win = [&](int p) { return cs_smem + p * wrows * kS; };           // cur windows
+  auto win = [&](int p) { return cs_smem + p * wrows * kS; };                // reconstruction windows
   auto srcw = [&](int p) { return cs_smem + 3 * wrows * kS + p * R * kS; };  // source
   __shared__ int32_t cost[R][8];
   __shared__ uint8_t bstate[R];
@@ -604,10 +739,9 @@ __global__ void __launch_bounds__(256, 3) cdef_search_kernel(const FrameDesc* __
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int fb = blockIdx.x, nfb = d.fb_rows * d.fb_cols;
   const int fr = fb / d.fb_cols, fc = fb - fr * d.fb_cols;
-  const int nc = d.ny + d.nuv;
   const int idx = f.cdef_idx[int64_t(fr) * f.cdef_stride + fc];
   if (idx < 0) {  // codes no index: zero errors, and no part in the greedy's sums
-    for (int k = tid; k < nc; k += blockDim.x) d.sse[int64_t(k) * nfb + fb] = 0;
+    for (int k = tid; k < NY + NUV; k += blockDim.x) d.sse[int64_t(k) * nfb + fb] = 0;
     if (tid == 0) d.best[fb] = 0;
     return;
   }
@@ -684,60 +818,66 @@ __global__ void __launch_bounds__(256, 3) cdef_search_kernel(const FrameDesc* __
     bvar[tid] = (best - cost[tid][(y_dir + 4) & 7]) >> 10;
   }
   __syncthreads();
-  // --- every candidate on every filtered block (encoder/cdef.rs:113-188) ---
+  // --- every pair on every filtered sample (encoder/cdef.rs:113-188) ---
   const int by = warp, bx = lane & 7, rr = lane >> 3;
   const int b = by * 8 + bx;
   const bool act = bstate[b] == 2;
   const int y_dir = act ? bdir[b] : 0;
-  const int32_t var = act ? bvar[b] : 0;
-  const int var_str = (var >> 6) != 0 ? min(floor_log2(uint32_t(var >> 6)), 12) : 0;
+  const int one = s_one;
   {
-    const int16_t* c = &win(0)[(top + by * 8 + rr) * kS + kColOff + bx * 8];
-    const int16_t* s = &srcw(0)[(by * 8 + rr) * kS + bx * 8];
-    for (int k = 0; k < d.ny; k++) {
-      const int pri0 = int(d.y_pri[k]) << cs, sec = int(d.y_sec[k]) << cs;
-      uint32_t acc = 0;
-      if (act) {
-        const int dir = pri0 == 0 ? 0 : y_dir;
-        const int pri = var != 0 ? (pri0 * (4 + var_str) + 8) >> 4 : 0;
-        const TapsDev t = taps_of(make_blk_taps(pri, sec, d.damping + cs, dir, cs, doff));
-        const int mode = pri0 == 0 ? (sec == 0 ? 3 : 2) : (sec == 0 ? 1 : 0);
-        acc = block_rows_sse(c, s, 8, 8, mode, t);
-      }
-      const uint64_t ws = warp_sum_u32(acc);
-      if (lane == 0) red[warp][k] = ws;
+    int pstr[NYP], padj[NYP], pw0[NYP], pw1[NYP], sstr[NYS], sadj[NYS], o[6];
+    pair_taps<NYP, NYS, TH, true>(cs, d.damping + cs, act ? bvar[b] : 0, pstr, padj, pw0, pw1, sstr, sadj);
+    dir_offsets(doff, y_dir, o);
+    uint32_t acc[NY];
+#pragma unroll
+    for (int k = 0; k < NY; k++) acc[k] = 0;
+    if (act) {
+      const int16_t* c = &win(0)[(top + by * 8 + rr) * kS + kColOff + bx * 8];
+      const int16_t* sv = &srcw(0)[(by * 8 + rr) * kS + bx * 8];
+      for (int q = 0; q < 2; q++)
+        for (int j = 0; j < 8; j++) {
+          const int sval = sv[q * 4 * kS + j];
+          if (sval != kNA)
+            sample_pairs<NYP, NYS>(c + q * 4 * kS + j, sval, o, pstr, padj, pw0, pw1, sstr, sadj, one, -one, acc);
+        }
     }
+    warp_reduce_pairs<NY>(acc, red, warp, lane, 0);
   }
   if (np > 1) {
     const int sx = f.ssx, sy = f.ssy;
     const int w = 8 >> sx, h = 8 >> sy;  // h is 4 or 8: rows rr (and rr + 4)
-    for (int k = 0; k < d.nuv; k++) {
-      const int pri = int(d.uv_pri[k]) << cs, sec = int(d.uv_sec[k]) << cs;
-      uint32_t acc = 0;
-      if (act) {
-        const int dir = pri == 0 ? 0 : uvdir[sx][sy][y_dir];
-        const TapsDev t = taps_of(make_blk_taps(pri, sec, d.damping + cs - 1, dir, cs, doff));
-        const int mode = pri == 0 ? (sec == 0 ? 3 : 2) : (sec == 0 ? 1 : 0);
-        for (int p = 1; p < 3; p++) {
-          const int16_t* c = &win(p)[(top + by * h + rr) * kS + kColOff + bx * w];
-          const int16_t* s = &srcw(p)[(by * h + rr) * kS + bx * w];
-          acc += block_rows_sse(c, s, w, h, mode, t);
-        }
+    int pstr[NUVP], padj[NUVP], pw0[NUVP], pw1[NUVP], sstr[NUVS], sadj[NUVS], o[6];
+    pair_taps<NUVP, NUVS, TH, false>(cs, d.damping + cs - 1, 0, pstr, padj, pw0, pw1, sstr, sadj);
+    dir_offsets(doff, uvdir[sx][sy][y_dir], o);
+    uint32_t acc[NUV];
+#pragma unroll
+    for (int k = 0; k < NUV; k++) acc[k] = 0;
+    if (act) {
+      for (int p = 1; p < 3; p++) {
+        const int16_t* c = &win(p)[(top + by * h + rr) * kS + kColOff + bx * w];
+        const int16_t* sv = &srcw(p)[(by * h + rr) * kS + bx * w];
+        for (int q = 0; q < h / 4; q++)
+          for (int j = 0; j < w; j++) {
+            const int sval = sv[q * 4 * kS + j];
+            if (sval != kNA)
+              sample_pairs<NUVP, NUVS>(c + q * 4 * kS + j, sval, o, pstr, padj, pw0, pw1, sstr, sadj, one, -one,
+                                       acc);
+          }
       }
-      const uint64_t ws = warp_sum_u32(acc);
-      if (lane == 0) red[warp][d.ny + k] = ws;
     }
+    warp_reduce_pairs<NUV>(acc, red, warp, lane, NY);
   }
   __syncthreads();
-  for (int k = tid; k < nc; k += blockDim.x) {
+  for (int k = tid; k < NY + NUV; k += blockDim.x) {
     uint64_t s = 0;
-    if (k < d.ny || np > 1)
+    if (k < NY || np > 1)
       for (int w8 = 0; w8 < 8; w8++) s += red[w8][k];
     d.sse[int64_t(k) * nfb + fb] = s;
   }
 }
 
 constexpr int kSearchSmem = 3 * (64 + 4) * kS * 2 + 3 * 64 * kS * 2;
+constexpr int search_lists_ny(bool th) { return th ? 44 : 28; }
 
 // dsp::cdef::filter (cdef.rs:29) on independent 12x12 windows: one CTA per
 // window, one thread per output sample.
@@ -794,7 +934,9 @@ cudaError_t cdef_init() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(cdef_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, cdef_smem(32, true));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(cdef_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSearchSmem);
+    e = cudaFuncSetAttribute(cdef_search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSearchSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cdef_search_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSearchSmem);
   return e;
 }
 
@@ -815,7 +957,10 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
 void launch_cdef_search(const FrameDesc* frames, const CdefSearchDesc& d, CdefGreedy* g, cudaStream_t s) {
   const int nfb = d.fb_rows * d.fb_cols;
   if (nfb <= 0) return;
-  cdef_search_kernel<<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
+  if (d.ny == search_lists_ny(true))
+    cdef_search_kernel<true><<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
+  else
+    cdef_search_kernel<false><<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
   note_launch();
 }
 

@@ -41,17 +41,29 @@ __device__ double ordered_total(const uint64_t* best, const uint64_t* Y, const u
   return t;
 }
 
+// (total, candidate) of the smaller, the first candidate on equal totals;
+// candidate -1 is none.
+__device__ __forceinline__ void argmin_pair(double& t, int& c, double t2, int c2) {
+  if (c2 >= 0 && (c < 0 || t2 < t || (t2 == t && c2 < c))) {
+    t = t2;
+    c = c2;
+  }
+}
+
 // Step k of the greedy (encoder/cdef.rs:215-232): a warp per candidate pair
 // scores sum_b min(best[b], Y[yk][b] + UV[uk][b]) — the reference's
 // best_for(set + pair), since best[b] is the minimum over the set so far —
-// lanes striding over the blocks (candidate-major table: coalesced). The
-// last CTA to finish (a fenced arrival count; no CTA waits) takes the
-// smallest total, first in (yk, uk) order on ties, adds it to the set,
-// lowers best[], and at set sizes 1, 2, 4 and 8 prices the set.
+// lanes striding over the blocks (candidate-major table: coalesced, four
+// blocks in flight per lane). The last CTA to finish (a fenced arrival
+// count; no CTA waits) takes the smallest total, first in (yk, uk) order
+// on ties, adds it to the set, lowers best[], and at set sizes 1, 2, 4 and
+// 8 prices the set. Launched with programmatic dependent launch: the state
+// is read after pdl_wait().
 __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchDesc d, CdefGreedy* g, double lambda,
                                                              uint64_t* __restrict__ tot) {
   const int nfb = d.fb_rows * d.fb_cols, ncand = d.ny * d.nuv;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  pdl_wait();
   const int n = g->n;
   const int c = blockIdx.x * 8 + warp;
   if (c < ncand) {
@@ -62,8 +74,17 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
     if (!in_set) {
       const uint64_t* Y = d.sse + int64_t(yk) * nfb;
       const uint64_t* U = d.sse + int64_t(d.ny + uk) * nfb;
-      for (int b = lane; b < nfb; b += 32) acc += min(d.best[b], Y[b] + U[b]);
-      acc = warp_sum_u64(acc);
+      const uint64_t* B = d.best;
+      uint64_t a1 = 0, a2 = 0, a3 = 0;
+      int b = lane;
+      for (; b + 96 < nfb; b += 128) {
+        acc += min(B[b], Y[b] + U[b]);
+        a1 += min(B[b + 32], Y[b + 32] + U[b + 32]);
+        a2 += min(B[b + 64], Y[b + 64] + U[b + 64]);
+        a3 += min(B[b + 96], Y[b + 96] + U[b + 96]);
+      }
+      for (; b < nfb; b += 32) acc += min(B[b], Y[b] + U[b]);
+      acc = warp_sum_u64(acc + a1 + a2 + a3);
     }
     if (lane == 0) tot[c] = in_set ? ~uint64_t(0) : acc;
   }
@@ -76,9 +97,9 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  // --- argmin over (total, candidate) ---
-  __shared__ double s_t[256];
-  __shared__ int s_c[256];
+  // --- argmin over (total, candidate): per thread, per warp, then warp 0 ---
+  __shared__ double s_t[8];
+  __shared__ int s_c[8];
   double bt = DBL_MAX;
   int bc = -1;
   for (int k = tid; k < ncand; k += blockDim.x) {
@@ -87,27 +108,24 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
     const double t = u < kExact ? double(u)
                                  : ordered_total(d.best, d.sse + int64_t(k / d.nuv) * nfb,
                                                  d.sse + int64_t(d.ny + k % d.nuv) * nfb, nfb);
-    if (t < bt) {  // k ascends within a thread: the first of equals stays
-      bt = t;
-      bc = k;
-    }
+    argmin_pair(bt, bc, t, k);
   }
-  s_t[tid] = bt;
-  s_c[tid] = bc;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    const double t2 = __shfl_xor_sync(0xffffffffu, bt, o);
+    const int c2 = __shfl_xor_sync(0xffffffffu, bc, o);
+    argmin_pair(bt, bc, t2, c2);
+  }
+  if (lane == 0) {
+    s_t[warp] = bt;
+    s_c[warp] = bc;
+  }
   __syncthreads();
-  for (int w = blockDim.x / 2; w; w >>= 1) {
-    if (tid < w) {
-      const double t2 = s_t[tid + w];
-      const int c2 = s_c[tid + w];
-      if (c2 >= 0 && (s_c[tid] < 0 || t2 < s_t[tid] || (t2 == s_t[tid] && c2 < s_c[tid]))) {
-        s_t[tid] = t2;
-        s_c[tid] = c2;
-      }
-    }
-    __syncthreads();
-  }
+  bt = s_t[0];
+  bc = s_c[0];
+  for (int w = 1; w < 8; w++) argmin_pair(bt, bc, s_t[w], s_c[w]);
   // no pair left (fewer than 8 candidates): the reference adds (0, 0)
-  const int pick = s_c[0] < 0 ? 0 : s_c[0];
+  const int pick = bc < 0 ? 0 : bc;
   const int py = pick / d.nuv, pu = pick - py * d.nuv;
   if (tid == 0) {
     g->set_y[n] = py;
@@ -162,6 +180,7 @@ __global__ void cdef_greedy_finish_kernel(const CdefSearchDesc d, const CdefGree
                                           const int8_t* __restrict__ cdef_idx, int stride, int8_t* __restrict__ table,
                                           int32_t* __restrict__ res) {
   const int nfb = d.fb_rows * d.fb_cols;
+  pdl_wait();
   const int m = 1 << g->best_bits;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e == 0) {
@@ -254,15 +273,13 @@ __global__ void __launch_bounds__(256) plane_sse_kernel(const SseJobs jobs, int 
 
 void launch_cdef_greedy_step(const CdefSearchDesc& d, CdefGreedy* g, uint64_t* tot, double lambda, cudaStream_t s) {
   const int ncand = d.ny * d.nuv;
-  cdef_greedy_step_kernel<<<(ncand + 7) / 8, 256, 0, s>>>(d, g, lambda, tot);
-  note_launch();
+  launch_pdl(cdef_greedy_step_kernel, (ncand + 7) / 8, 256, 0, s, d, g, lambda, tot);
 }
 
 void launch_cdef_greedy_finish(const CdefSearchDesc& d, const CdefGreedy* g, const int8_t* cdef_idx, int stride,
                                int8_t* table, int32_t* res, cudaStream_t s) {
   const int n = d.fb_rows * stride;
-  cdef_greedy_finish_kernel<<<(n + 255) / 256, 256, 0, s>>>(d, g, cdef_idx, stride, table, res);
-  note_launch();
+  launch_pdl(cdef_greedy_finish_kernel, (n + 255) / 256, 256, 0, s, d, g, cdef_idx, stride, table, res);
 }
 
 void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s) {
