@@ -504,6 +504,31 @@ int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
                       av1pf_cdef_search_result* result, int8_t* cdef_idx_out,
                       uint64_t* block_sse, void* stream);
 
+/* Effort of the loop-restoration search (encoder/lr.rs:47-58): fast fits
+ * on every other row and column and tries 2 self-guided parameter sets,
+ * normal 6, thorough all 16. */
+enum { AV1PF_LR_FAST = 0, AV1PF_LR_NORMAL = 1, AV1PF_LR_THOROUGH = 2 };
+
+/* lr::search (encoder/lr.rs:64-210): each restoration unit's filter — none,
+ * a Wiener filter fitted to the source by least squares, or a self-guided
+ * filter with fitted projection weights for each parameter set tried — the
+ * cheapest of error + lambda * (1, 40 or 28 for a luma or chroma Wiener
+ * filter, 20), measured with the decoder's own restoration over the samples
+ * it reads; and each plane's frame restoration type (0 none, 1 Wiener,
+ * 2 self-guided, 3 switchable). `params` gives the unit grid
+ * (loop_restoration_size, lr_unit_rows, lr_unit_cols; the restoration
+ * types are ignored); `cur` (deblocked frame, read at stripe boundaries),
+ * `cdef` (CDEF output) and `src` are device planes covering the visible
+ * frame. Writes units_out[p] (host, lr_unit_rows[p] * lr_unit_cols[p]
+ * entries, NULL to skip a plane) and frame_type_out. Any finite lambda.
+ * Returns once the outputs are on the host. */
+int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
+                    const av1pf_params* params, const av1pf_plane* cur,
+                    const av1pf_plane* cdef, const av1pf_plane* src,
+                    double lambda, int32_t effort,
+                    av1pf_lr_unit* const units_out[3],
+                    int32_t frame_type_out[3], void* stream);
+
 /* search_lf (encoder/mod.rs:1457-1506): the loop-filter levels with the
  * least error. `params` carries the starting levels (loop_filter_level) and
  * the other loop-filter fields the filter reads; `cur` (device, left

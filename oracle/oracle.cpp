@@ -1753,6 +1753,300 @@ std::array<uint32_t, 4> search_lf(FrameCtx& f, const FrameBuf& src, const std::a
   return {best[0].second, best[0].second, best[1].second, best[2].second};
 }
 
+// encoder/lr.rs:212-233 `solve`: m x = v by Gaussian elimination with
+// partial pivoting (the last row of equal magnitude wins, as Iterator::max_by
+// keeps the last maximum); zeros when singular.
+template <size_t N>
+std::array<double, N> lr_solve(std::array<std::array<double, N>, N> m, std::array<double, N> v) {
+  for (size_t i = 0; i < N; i++) {
+    size_t piv = i;
+    for (size_t a = i + 1; a < N; a++)
+      if (!(std::fabs(m[a][i]) < std::fabs(m[piv][i]))) piv = a;  // >=: the last maximum
+    std::swap(m[i], m[piv]);
+    std::swap(v[i], v[piv]);
+    if (std::fabs(m[i][i]) < 1e-9) return {};
+    for (size_t r = 0; r < N; r++) {
+      if (r != i) {
+        double fct = m[r][i] / m[i][i];
+        for (size_t c = i; c < N; c++) m[r][c] -= fct * m[i][c];
+        v[r] -= fct * v[i];
+      }
+    }
+  }
+  std::array<double, N> x{};
+  for (size_t i = 0; i < N; i++) x[i] = v[i] / m[i][i];
+  return x;
+}
+
+// f64 -> i32 as Rust's `as` converts (saturating, NaN to 0).
+int32_t f64_to_i32(double x) {
+  if (std::isnan(x)) return 0;
+  if (x <= -2147483648.0) return INT32_MIN;
+  if (x >= 2147483647.0) return INT32_MAX;
+  return int32_t(x);
+}
+
+const int32_t WIENER_TAPS_MIN_T[3] = AV1T_WIENER_TAPS_MIN, WIENER_TAPS_MAX_T[3] = AV1T_WIENER_TAPS_MAX;
+const int32_t SGRPROJ_XQD_MIN_T[2] = AV1T_SGRPROJ_XQD_MIN, SGRPROJ_XQD_MAX_T[2] = AV1T_SGRPROJ_XQD_MAX;
+
+struct LrRect {
+  LrCtx ctx;
+  int32_t y0;
+  size_t h;
+};
+
+// encoder/lr.rs:235-328 `fit_wiener`: [vertical, horizontal] coefficients.
+std::array<std::array<int32_t, 3>, 2> fit_wiener(size_t plane, const std::vector<LrRect>& rects, int32_t x0, size_t w,
+                                                 const PlaneBuf& src, size_t step, LrBuffers& buf) {
+  const size_t first = plane == 0 ? 0 : 1;
+  const size_t ww = w + 2 * LRB;
+  std::array<double, 3> hc{}, vc{};
+  for (int iter = 0; iter < 3; iter++) {
+    const bool vertical = iter % 2 == 0;
+    std::array<std::array<double, 3>, 3> m{};
+    std::array<double, 3> v{};
+    for (const LrRect& rc : rects) {
+      lr_window(rc.ctx, x0, rc.y0, w, rc.h, buf);
+      auto at = [&](size_t r, size_t c) { return double(buf.win[r * ww + c]); };
+      for (size_t i = 0; i < rc.h; i += step) {
+        const uint16_t* srow = src.row(size_t(rc.y0) + i) + x0;
+        for (size_t j = 0; j < w; j += step) {
+          double line[7];
+          for (size_t t = 0; t < 7; t++) {
+            size_t r = vertical ? i + t : i + LRB, c = vertical ? j + LRB : j + t;
+            const std::array<double, 3>& other = vertical ? hc : vc;
+            double center = at(r, c);
+            double sum = center;
+            for (size_t k = 0; k < 3; k++) {
+              size_t d = 3 - k;
+              double a = vertical ? at(r, c - d) : at(r - d, c);
+              double b = vertical ? at(r, c + d) : at(r + d, c);
+              sum += other[k] * (a + b - 2.0 * center);
+            }
+            line[t] = sum;
+          }
+          double target = double(srow[j]) - line[3];
+          double d[3];
+          for (size_t k = 0; k < 3; k++) d[k] = line[k] + line[6 - k] - 2.0 * line[3];
+          for (size_t a = first; a < 3; a++) {
+            for (size_t b = first; b < 3; b++) m[a][b] += d[a] * d[b];
+            v[a] += d[a] * target;
+          }
+        }
+      }
+    }
+    std::array<double, 3> sol{};
+    if (first == 0) {
+      sol = lr_solve<3>(m, v);
+    } else {
+      std::array<double, 2> s2 = lr_solve<2>({{{m[1][1], m[1][2]}, {m[2][1], m[2][2]}}}, {v[1], v[2]});
+      sol = {0.0, s2[0], s2[1]};
+    }
+    if (vertical)
+      vc = sol;
+    else
+      hc = sol;
+  }
+  auto q = [&](const std::array<double, 3>& c) {
+    std::array<int32_t, 3> o{};
+    for (size_t k = 0; k < 3; k++)
+      o[k] = k < first ? 0 : iclamp(f64_to_i32(std::round(c[k] * 128.0)), WIENER_TAPS_MIN_T[k], WIENER_TAPS_MAX_T[k]);
+    return o;
+  };
+  return {q(vc), q(hc)};
+}
+
+// encoder/lr.rs:330-430 `fit_sgr`: the projection weights of set `set` and
+// their error.
+std::pair<std::array<int32_t, 2>, uint64_t> fit_sgr(const FrameCtx& f, size_t set, const std::vector<LrRect>& rects,
+                                                    int32_t x0, size_t w, const PlaneBuf& src, size_t step,
+                                                    LrBuffers& buf) {
+  const int32_t r0 = SGR_PARAMS[set][0], r1 = SGR_PARAMS[set][2];
+  double m[2][2] = {{0, 0}, {0, 0}}, v[2] = {0, 0};
+  std::vector<std::array<std::vector<int32_t>, 2>> flts;
+  for (const LrRect& rc : rects) {
+    lr_window(rc.ctx, x0, rc.y0, w, rc.h, buf);
+    for (size_t pass = 0; pass < 2; pass++) box_filter_rect(f, rc.ctx, x0, rc.y0, w, rc.h, set, pass, buf);
+    flts.push_back({buf.flt[0], buf.flt[1]});
+    for (size_t i = 0; i < rc.h; i += step) {
+      const uint16_t* srow = src.row(size_t(rc.y0) + i) + x0;
+      for (size_t j = 0; j < w; j += step) {
+        double u = double(int32_t(rc.ctx.cdef->get(size_t(x0) + j, size_t(rc.y0) + i)) << SGRPROJ_RST_BITS);
+        double a = r0 != 0 ? double(buf.flt[0][i * w + j]) - u : 0.0;
+        double b = r1 != 0 ? double(buf.flt[1][i * w + j]) - u : 0.0;
+        double t = 128.0 * (double(int32_t(srow[j]) << SGRPROJ_RST_BITS) - u);
+        m[0][0] += a * a;
+        m[0][1] += a * b;
+        m[1][1] += b * b;
+        v[0] += a * t;
+        v[1] += b * t;
+      }
+    }
+  }
+  m[1][0] = m[0][1];
+  double w0, w2;
+  if (r0 != 0 && r1 != 0) {
+    std::array<double, 2> s2 = lr_solve<2>({{{m[0][0], m[0][1]}, {m[1][0], m[1][1]}}}, {v[0], v[1]});
+    w0 = s2[0];
+    w2 = s2[1];
+  } else if (r0 != 0) {
+    w0 = m[0][0] > 0.0 ? v[0] / m[0][0] : 0.0;
+    w2 = 0.0;
+  } else {
+    w0 = 0.0;
+    w2 = m[1][1] > 0.0 ? v[1] / m[1][1] : 0.0;
+  }
+  int32_t x0q = r0 != 0 ? iclamp(f64_to_i32(std::round(w0)), SGRPROJ_XQD_MIN_T[0], SGRPROJ_XQD_MAX_T[0]) : 0;
+  int32_t x1q;
+  if (r1 != 0) {
+    // i32 arithmetic wraps as the reference's release build does
+    int32_t diff = int32_t(uint32_t(1 << SGRPROJ_PRJ_BITS) - uint32_t(x0q) - uint32_t(f64_to_i32(std::round(w2))));
+    x1q = iclamp(diff, SGRPROJ_XQD_MIN_T[1], SGRPROJ_XQD_MAX_T[1]);
+  } else {
+    x1q = iclamp((1 << SGRPROJ_PRJ_BITS) - x0q, SGRPROJ_XQD_MIN_T[1], SGRPROJ_XQD_MAX_T[1]);
+  }
+  const int32_t pw0 = x0q, pw1 = x1q, pw2 = (1 << SGRPROJ_PRJ_BITS) - pw0 - pw1;
+  const int32_t maxv = (1 << f.bit_depth) - 1;
+  uint64_t sse = 0;
+  for (size_t ri = 0; ri < rects.size(); ri++) {
+    const LrRect& rc = rects[ri];
+    for (size_t i = 0; i < rc.h; i++) {
+      const uint16_t* srow = src.row(size_t(rc.y0) + i) + x0;
+      for (size_t j = 0; j < w; j++) {
+        int32_t u = int32_t(rc.ctx.cdef->get(size_t(x0) + j, size_t(rc.y0) + i)) << SGRPROJ_RST_BITS;
+        int32_t val = pw1 * u;
+        val += r0 != 0 ? pw0 * flts[ri][0][i * w + j] : pw0 * u;
+        val += r1 != 0 ? pw2 * flts[ri][1][i * w + j] : pw2 * u;
+        int32_t out = iclamp(round2(val, unsigned(SGRPROJ_RST_BITS + SGRPROJ_PRJ_BITS)), 0, maxv);
+        int64_t d = int64_t(out) - int64_t(srow[j]);
+        sse += uint64_t(d * d);
+      }
+    }
+  }
+  return {{x0q, x1q}, sse};
+}
+
+struct LrChoice {  // encoder/lr.rs:22-29
+  uint8_t t = RESTORE_NONE;
+  std::array<std::array<int32_t, 3>, 2> wiener{};
+  uint8_t set = 0;
+  std::array<int32_t, 2> xqd{};
+};
+
+// encoder/lr.rs:64-210 `search`: each unit's restoration and each plane's
+// frame restoration type. `f.lr` holds the unit grid, `cur` the deblocked
+// frame, `cdefb` the CDEF output.
+void lr_search(const FrameCtx& f, const FrameBuf& cur, const FrameBuf& cdefb, const FrameBuf& src, double lambda,
+               int effort, size_t threads, std::vector<LrChoice> units[3], uint8_t frame_type[3]) {
+  static const size_t kNormal[6] = {0, 3, 6, 10, 13, 14}, kFast[2] = {3, 10};
+  std::vector<size_t> sets;
+  if (effort == 2)
+    for (size_t k = 0; k < 16; k++) sets.push_back(k);
+  else if (effort == 1)
+    sets.assign(kNormal, kNormal + 6);
+  else
+    sets.assign(kFast, kFast + 2);
+  const size_t step = effort == 0 ? 2 : 1;
+  const size_t stripes = (size_t(f.hdr.frame_height) + 8 + 63) / 64;
+  struct Stripe {
+    int32_t ss, se, y0, y1;
+  };
+  std::vector<std::vector<Stripe>> rows[3];
+  struct Job {
+    size_t plane, ur, uc;
+  };
+  std::vector<Job> jobs;
+  for (size_t plane = 0; plane < f.num_planes; plane++) {
+    const LrPlane& lp = f.lr[plane];
+    rows[plane].assign(lp.unit_rows, {});
+    for (size_t s = 0; s < stripes; s++) {
+      int32_t ss, se, y0, y1;
+      size_t ur;
+      if (lr_stripe(f, plane, s, ss, se, y0, y1, ur)) rows[plane][ur].push_back({ss, se, y0, y1});
+    }
+    for (size_t ur = 0; ur < lp.unit_rows; ur++)
+      for (size_t uc = 0; uc < lp.unit_cols; uc++) jobs.push_back({plane, ur, uc});
+  }
+  std::vector<LrChoice> results(jobs.size());
+  std::vector<uint8_t> present(jobs.size(), 0);
+  auto unit = [&](size_t ji) {
+    const Job& jb = jobs[ji];
+    const size_t plane = jb.plane;
+    auto ssv = f.plane_ss(plane);
+    const int32_t plane_end_x = round2(f.hdr.upscaled_width, unsigned(ssv.first)) - 1;
+    const int32_t plane_end_y = round2(f.hdr.frame_height, unsigned(ssv.second)) - 1;
+    auto xr = lr_unit_cols(f, plane, jb.uc);
+    const int32_t x0 = xr.first, x1 = xr.second;
+    if (x0 > plane_end_x || rows[plane][jb.ur].empty()) return;
+    LrBuffers buf;
+    const size_t w = size_t(x1 - x0 + 1);
+    std::vector<LrRect> rects;
+    for (const Stripe& st : rows[plane][jb.ur])
+      rects.push_back({LrCtx{&cur.planes[plane], &cdefb.planes[plane], st.ss, st.se, plane_end_x, plane_end_y}, st.y0,
+                       size_t(st.y1 - st.y0 + 1)});
+    const PlaneBuf& sp = src.planes[plane];
+    auto sse_of = [&](const LrParams* prm) {
+      uint64_t total = 0;
+      for (const LrRect& rc : rects) {
+        if (prm) {
+          lr_window(rc.ctx, x0, rc.y0, w, rc.h, buf);
+          restore_rect_from_window(f, rc.ctx, x0, rc.y0, w, rc.h, *prm, buf);
+        }
+        for (size_t i = 0; i < rc.h; i++) {
+          const size_t y = size_t(rc.y0) + i;
+          const uint16_t* srow = sp.row(y) + x0;
+          for (size_t j = 0; j < w; j++) {
+            int64_t val = prm ? int64_t(buf.out[i * w + j]) : int64_t(rc.ctx.cdef->get(size_t(x0) + j, y));
+            int64_t d = val - int64_t(srow[j]);
+            total += uint64_t(d * d);
+          }
+        }
+      }
+      return total;
+    };
+    const uint64_t none = sse_of(nullptr);
+    double best_cost = double(none) + lambda;
+    LrChoice best{};
+    auto coef = fit_wiener(plane, rects, x0, w, sp, step, buf);
+    LrParams pw{};
+    pw.wiener = true;
+    pw.coef = coef;
+    double cost = double(sse_of(&pw)) + lambda * (plane == 0 ? 40.0 : 28.0);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = LrChoice{};
+      best.t = RESTORE_WIENER;
+      best.wiener = coef;
+    }
+    for (size_t set : sets) {
+      auto fit = fit_sgr(f, set, rects, x0, w, sp, step, buf);
+      cost = double(fit.second) + lambda * 20.0;
+      if (cost < best_cost) {
+        best_cost = cost;
+        best = LrChoice{};
+        best.t = RESTORE_SGRPROJ;
+        best.set = uint8_t(set);
+        best.xqd = fit.first;
+      }
+    }
+    results[ji] = best;
+    present[ji] = 1;
+  };
+  run_bands(jobs.size(), threads, unit);
+  for (size_t plane = 0; plane < f.num_planes; plane++)
+    units[plane].assign(f.lr[plane].unit_rows * f.lr[plane].unit_cols, LrChoice{});
+  for (size_t ji = 0; ji < jobs.size(); ji++)
+    if (present[ji]) units[jobs[ji].plane][jobs[ji].ur * f.lr[jobs[ji].plane].unit_cols + jobs[ji].uc] = results[ji];
+  for (size_t plane = 0; plane < f.num_planes; plane++) {
+    bool wu = false, su = false;
+    for (const LrChoice& c : units[plane]) {
+      wu |= c.t == RESTORE_WIENER;
+      su |= c.t == RESTORE_SGRPROJ;
+    }
+    frame_type[plane] = wu ? (su ? 3 : RESTORE_WIENER) : (su ? RESTORE_SGRPROJ : RESTORE_NONE);
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -2004,6 +2298,39 @@ int oracle_lf_search(const av1pf_frame_info* info, const av1pf_params* p, const 
   if (sse_out) std::memset(sse_out, 0, 6 * 3 * sizeof(uint64_t));
   std::array<uint32_t, 4> lv = search_lf(f, s, start, resolve_threads(threads), sse_out);
   for (int i = 0; i < 4; i++) levels_out[i] = int32_t(lv[size_t(i)]);
+  return AV1PF_OK;
+}
+
+int oracle_lr_search(const av1pf_frame_info* info, const av1pf_params* p, const av1pf_plane* cur,
+                     const av1pf_plane* cdefp, const av1pf_plane* src, double lambda, int32_t effort,
+                     av1pf_lr_unit* const units_out[3], int32_t frame_type_out[3], int threads) {
+  if (!info_ok(info) || !p || !cur || !cdefp || !src || !units_out || !frame_type_out || effort < 0 || effort > 2)
+    return AV1PF_ERR_INVALID_INPUT;
+  av1pf_params q = *p;
+  q.uses_lr = 1;
+  for (int k = 0; k < 3; k++) q.frame_restoration_type[k] = 3;
+  av1pf_maps none{};
+  FrameCtx f;
+  ctx_from(f, info, &q, &none, nullptr);
+  FrameBuf c = frame_from(info, cur), d = frame_from(info, cdefp), s = frame_from(info, src);
+  std::vector<LrChoice> units[3];
+  uint8_t ft[3] = {0, 0, 0};
+  lr_search(f, c, d, s, lambda, effort, resolve_threads(threads), units, ft);
+  for (size_t pl = 0; pl < 3; pl++) {
+    frame_type_out[pl] = pl < f.num_planes ? ft[pl] : 0;
+    if (pl >= f.num_planes || !units_out[pl]) continue;
+    for (size_t i = 0; i < units[pl].size(); i++) {
+      const LrChoice& ch = units[pl][i];
+      av1pf_lr_unit& u = units_out[pl][i];
+      std::memset(&u, 0, sizeof(u));
+      u.type = ch.t;
+      u.sgr_set = ch.set;
+      u.sgr_xqd[0] = int8_t(ch.xqd[0]);
+      u.sgr_xqd[1] = int8_t(ch.xqd[1]);
+      for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 3; b++) u.wiener[a][b] = int8_t(ch.wiener[size_t(a)][size_t(b)]);
+    }
+  }
   return AV1PF_OK;
 }
 

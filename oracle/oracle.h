@@ -79,6 +79,13 @@ int oracle_lf_search(const av1pf_frame_info* info, const av1pf_params* p,
                      const av1pf_maps* maps, const av1pf_plane* cur,
                      const av1pf_plane* src, int32_t levels_out[4],
                      uint64_t* sse_out, int threads);
+/* lr::search (encoder/lr.rs:64-210): outputs as av1pf_lr_search (host
+ * pointers; units_out[p] may be NULL). */
+int oracle_lr_search(const av1pf_frame_info* info, const av1pf_params* p,
+                     const av1pf_plane* cur, const av1pf_plane* cdef,
+                     const av1pf_plane* src, double lambda, int32_t effort,
+                     av1pf_lr_unit* const units_out[3], int32_t frame_type_out[3],
+                     int threads);
 
 #ifdef __cplusplus
 }

@@ -48,6 +48,8 @@ def lib():
         sig("oracle_cdef_kat_cases", None, C.c_uint64, C.c_int, vp, vp)
         sig("oracle_cdef_search", C.c_int, P(A.FrameInfo), P(A.Maps), P(A.Plane), P(A.Plane), C.c_int32, C.c_double,
             C.c_int32, P(A.CdefSearchResult), vp, vp, C.c_int)
+        sig("oracle_lr_search", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Plane), P(A.Plane), P(A.Plane),
+            C.c_double, C.c_int32, P(C.POINTER(A.LrUnit)), P(C.c_int32), C.c_int)
         sig("oracle_lf_search", C.c_int, P(A.FrameInfo), P(A.Params), P(A.Maps), P(A.Plane), P(A.Plane),
             P(C.c_int32), vp, C.c_int)
         _lib = L
@@ -156,3 +158,37 @@ def lf_search(sf, cur, src, threads=0, params=None):
     if rc != 0:
         raise RuntimeError(f"oracle_lf_search: {rc}")
     return list(levels), sse
+
+
+def lr_unit_tuple(u):
+    """(type, wiener ((v0, v1, v2), (h0, h1, h2)), set, xqd) of an av1pf_lr_unit."""
+    return (u.type, (tuple(u.wiener[0]), tuple(u.wiener[1])), u.sgr_set, tuple(u.sgr_xqd))
+
+
+def lr_unit_arrays(params, num_planes):
+    return [(A.LrUnit * max(1, params.lr_unit_rows[p] * params.lr_unit_cols[p]))() if p < num_planes else None
+            for p in range(3)]
+
+
+def lr_search(sf, cur, cdef, src, lam, effort, threads=0):
+    """(frame types[3], per-plane lists of unit tuples) of the oracle's LR search."""
+    info, params = sf.f.info, sf.f.params
+    arrs = lr_unit_arrays(params, info.num_planes)
+    ptrs = (C.POINTER(A.LrUnit) * 3)(*[C.cast(a, C.POINTER(A.LrUnit)) if a is not None else None for a in arrs])
+    ft = (C.c_int32 * 3)()
+    rc = lib().oracle_lr_search(C.byref(info), C.byref(params), cur.c, cdef.c, src.c, lam, effort, ptrs, ft, threads)
+    if rc != 0:
+        raise RuntimeError(f"oracle_lr_search: {rc}")
+    units = [[lr_unit_tuple(u) for u in arrs[p][:params.lr_unit_rows[p] * params.lr_unit_cols[p]]]
+             if arrs[p] is not None else [] for p in range(3)]
+    return list(ft), units
+
+
+def lr_search_inputs(sf, seed, amp=None):
+    """(cur, cdef, src) HostPlanes for the LR search: the source is the
+    synthetic frame's planes, the CDEF output the source plus seeded noise,
+    and the deblocked frame (read at stripe boundaries) the source plus other
+    noise."""
+    cdef, src = A.synth_search_planes(sf, seed, amp)
+    cur, _ = A.synth_search_planes(sf, seed + 1000, amp)
+    return HostPlanes(cur), HostPlanes(cdef), HostPlanes(src)

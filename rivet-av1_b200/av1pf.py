@@ -210,6 +210,8 @@ def lib():
         _sig(L, "av1pf_serve_close", C.c_int, vp)
         _sig(L, "av1pf_cdef_search", C.c_int, vp, P(FrameInfo), P(Maps), P(Plane), P(Plane), C.c_int32, C.c_double,
              C.c_int32, P(CdefSearchResult), vp, vp, vp)
+        _sig(L, "av1pf_lr_search", C.c_int, vp, P(FrameInfo), P(Params), P(Plane), P(Plane), P(Plane), C.c_double,
+             C.c_int32, P(P(LrUnit)), P(C.c_int32), vp)
         _sig(L, "av1pf_lf_search", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane),
              P(C.c_int32), vp, vp)
         _sig(L, "av1pf_dsp_lf_filter", C.c_int, vp, vp, vp, C.c_int, vp)

@@ -104,6 +104,29 @@ struct CdefSearchDesc {
   uint64_t* best;          // [fb_rows * fb_cols]: the greedy's per-block minimum
 };
 
+// The encoder's loop-restoration search (encoder/lr.rs:64-430): one job
+// per restoration unit, its stripe rectangles, and the chosen filter.
+struct LrSearchJob {
+  int32_t plane, x0, w;  // unit columns x0 .. x0 + w - 1
+  int32_t r0, nr;        // rectangles r0 .. r0 + nr - 1 (one per stripe)
+};
+struct LrSearchRect {
+  int32_t ss, se;  // StripeStartY, StripeEndY
+  int32_t y0, h;   // rows restored
+};
+struct LrSearchDesc {
+  DPlane cur[3], cdef[3], src[3];  // deblocked frame, CDEF output, source
+  int32_t bd, sb;
+  int32_t pex[3], pey[3];  // last column / row of each plane
+  int32_t wmax, hmax;      // the widest unit and tallest rectangle
+  int32_t step;            // fit on every step-th row and column
+  int32_t nsets, sets[16];
+  double lambda;
+  const LrSearchJob* jobs;
+  const LrSearchRect* rects;
+  av1pf_lr_unit* out;  // one per job
+};
+
 // State of the greedy choice of (luma, chroma) pairs (encoder/cdef.rs:195-240).
 struct CdefGreedy {
   uint32_t arrived;        // CTAs of the current step done (the last one picks)

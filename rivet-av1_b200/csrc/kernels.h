@@ -14,6 +14,7 @@ struct FrameDesc;
 struct Item;
 struct CdefSearchDesc;
 struct CdefGreedy;
+struct LrSearchDesc;
 
 // Grid cap of the grid-stride stage kernels: 8 resident CTAs on each of the
 // B200's 148 SMs.
@@ -84,6 +85,10 @@ struct SsePlane {
   int64_t sa, sb_;  // strides in samples
   int32_t w, h;
 };
+// The loop-restoration search (lr_search.cu): one CTA per unit job.
+size_t lr_search_smem(int wmax, int hmax);
+cudaError_t lr_search_init(size_t smem);  // raises the kernel's shared-memory limit
+void launch_lr_search(const LrSearchDesc& d, int njobs, size_t smem, cudaStream_t s);
 void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s);
 
 // Super-resolution (superres.cu)

@@ -1,0 +1,640 @@
+// lr_search.cu — the encoder's loop-restoration search on the device
+// (encoder/lr.rs:64-430): per restoration unit, the error of no filter, of
+// a Wiener filter fitted to the source and of a self-guided filter fitted
+// for each parameter set, priced with lambda; the cheapest is the unit's
+// choice.
+//
+// One CTA per unit, 256 threads. Each of the unit's stripe rectangles is
+// staged as the decoder's restoration window (postfilter.rs:765-777:
+// clamped to the plane, rows beyond the stripe from the deblocked frame)
+// in shared memory, once per phase.
+//
+// Exactness. The reference fits in f64, summing over the unit's samples in
+// row-major order. Sums whose terms are integers (the first Wiener pass,
+// whose lines are plain samples, and the self-guided fit, whose terms are
+// products of filter outputs and samples) are exact in any order while the
+// sum of the terms' magnitudes stays below 2^53: they are summed in int64
+// in parallel (the self-guided sums check that bound and otherwise redo the
+// sum in order on one thread). The second and third Wiener passes have
+// real-valued terms, so their sums run in the reference's order: warps 1-7
+// produce a row's terms into shared memory while lanes of warp 0 each add
+// one accumulator's terms in sample order. Every f64 operation is a
+// round-to-nearest multiply, add or divide in the reference's order (this
+// file is compiled without floating-point contraction, and the sums use
+// the explicit _rn intrinsics).
+#include <cfloat>
+
+#include "av1_tables.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace av1pf {
+
+namespace {
+
+constexpr int kB = 3;            // window border (postfilter.rs:744 LRB)
+constexpr int kBand = 8;         // self-guided output rows per band
+constexpr int kThreads = 256;
+__constant__ int32_t kSgrParams[16][4] = AV1T_SGR_PARAMS;
+__constant__ int32_t kWienerMin[3] = AV1T_WIENER_TAPS_MIN, kWienerMax[3] = AV1T_WIENER_TAPS_MAX;
+__constant__ int32_t kXqdMin[2] = AV1T_SGRPROJ_XQD_MIN, kXqdMax[2] = AV1T_SGRPROJ_XQD_MAX;
+constexpr uint64_t kExact = uint64_t(1) << 53;
+
+__device__ __forceinline__ int ld(const DPlane& p, int sb, int x, int y) { return ld_sample(p, sb, x, y); }
+
+// f64 -> i32 as Rust's `as` converts: saturating, NaN to 0.
+__device__ __forceinline__ int32_t f64_to_i32(double x) {
+  if (isnan(x)) return 0;
+  if (x <= -2147483648.0) return INT32_MIN;
+  if (x >= 2147483647.0) return INT32_MAX;
+  return int32_t(x);
+}
+
+struct Win {
+  const int16_t* w;
+  int ws;  // row stride
+  __device__ __forceinline__ int at(int r, int c) const { return w[r * ws + c]; }
+};
+
+// lr_window (postfilter.rs:765-777) of rectangle `rc` into shared memory.
+__device__ void stage_window(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int w, int16_t* win,
+                             int ws) {
+  const int pex = d.pex[p], pey = d.pey[p];
+  const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
+  for (int k = threadIdx.x; k < ww * wh; k += blockDim.x) {
+    const int r = k / ww, c = k - r * ww;
+    const int x = max(min(x0 + c - kB, pex), 0);
+    const int y = max(min(rc.y0 + r - kB, pey), 0);
+    int v;
+    if (y < rc.ss)
+      v = ld(d.cur[p], d.sb, x, max(rc.ss - 2, y));
+    else if (y > rc.se)
+      v = ld(d.cur[p], d.sb, x, min(rc.se + 2, y));
+    else
+      v = ld(d.cdef[p], d.sb, x, y);
+    win[r * ws + c] = int16_t(v);
+  }
+}
+
+// Block sum of 64-bit values (every thread gets the result).
+__device__ int64_t block_sum_i64(int64_t v, int64_t* red) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int64_t t = 0;
+  for (int w = 0; w < kThreads / 32; w++) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Gaussian elimination with partial pivoting (encoder/lr.rs:212-233): the
+// last row of largest magnitude is the pivot (Iterator::max_by); zeros when
+// singular.
+template <int N>
+__device__ void solve(double (&m)[N][N], double (&v)[N], double (&x)[N]) {
+  for (int i = 0; i < N; i++) {
+    int piv = i;
+    for (int a = i + 1; a < N; a++)
+      if (!(fabs(m[a][i]) < fabs(m[piv][i]))) piv = a;
+    for (int c = 0; c < N; c++) {
+      const double t = m[i][c];
+      m[i][c] = m[piv][c];
+      m[piv][c] = t;
+    }
+    const double tv = v[i];
+    v[i] = v[piv];
+    v[piv] = tv;
+    if (fabs(m[i][i]) < 1e-9) {
+      for (int k = 0; k < N; k++) x[k] = 0.0;
+      return;
+    }
+    for (int r = 0; r < N; r++) {
+      if (r != i) {
+        const double f = __ddiv_rn(m[r][i], m[i][i]);
+        for (int c = i; c < N; c++) m[r][c] = __dsub_rn(m[r][c], __dmul_rn(f, m[i][c]));
+        v[r] = __dsub_rn(v[r], __dmul_rn(f, v[i]));
+      }
+    }
+  }
+  for (int i = 0; i < N; i++) x[i] = __ddiv_rn(v[i], m[i][i]);
+}
+
+// The 7 samples of a Wiener line at (i, j) with the other direction's
+// filter applied first (encoder/lr.rs:265-285); the line's taps run along
+// columns (vertical) or rows.
+__device__ __forceinline__ void wiener_line(const Win& W, bool vertical, int i, int j, const double* other,
+                                            double (&line)[7]) {
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    const int r = vertical ? i + t : i + kB, c = vertical ? j + kB : j + t;
+    const double center = double(W.at(r, c));
+    double s = center;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int dd = 3 - k;
+      const double a = double(vertical ? W.at(r, c - dd) : W.at(r - dd, c));
+      const double b = double(vertical ? W.at(r, c + dd) : W.at(r + dd, c));
+      s = __dadd_rn(s, __dmul_rn(other[k], __dsub_rn(__dadd_rn(a, b), __dmul_rn(2.0, center))));
+    }
+    line[t] = s;
+  }
+}
+
+// One restored Wiener sample (postfilter.rs:781-822) at (i, j) of the window.
+__device__ __forceinline__ int wiener_px(const Win& W, int i, int j, const int (&hf)[7], const int (&vf)[7], int round0,
+                                         int round1, int off, int lim, int maxv) {
+  int s = 0;
+#pragma unroll
+  for (int t = 0; t < 7; t++) {
+    int h = 0;
+#pragma unroll
+    for (int u = 0; u < 7; u++) h += hf[u] * W.at(i + t, j + u);
+    s += vf[t] * clip3(-off, lim - off, round2(h, round0));
+  }
+  return min(max(round2(s, round1), 0), maxv);
+}
+
+// One self-guided A/B pair (postfilter.rs:918-948) at A/B position (ai, aj)
+// of the rectangle (window position ai + 2, aj + 2).
+__device__ __forceinline__ void sgr_ab(const Win& W, int ai, int aj, int r, int n, int s, int one_over_n, int bd,
+                                       int32_t& A, int32_t& B) {
+  const int wy = ai + kB - 1, wx = aj + kB - 1;
+  int32_t bs = 0;
+  int64_t as = 0;
+  for (int dy = -r; dy <= r; dy++)
+    for (int dx = -r; dx <= r; dx++) {
+      const int v = W.at(wy + dy, wx + dx);
+      bs += v;
+      as += int64_t(v) * v;
+    }
+  const int64_t a = round2_64(as, 2 * (bd - 8));
+  const int64_t dd = round2(bs, bd - 8);
+  const int64_t p = max(a * n - dd * dd, int64_t(0));
+  const int64_t z = round2_64(p * s, 20);  // SGRPROJ_MTABLE_BITS
+  const int zc = int(min(z, int64_t(255)));
+  const int32_t a2 = zc >= 255 ? 256 : (zc == 0 ? 1 : ((zc << 8) + zc / 2) / (zc + 1));
+  const int64_t b2 = int64_t(256 - a2) * int64_t(bs) * int64_t(one_over_n);
+  A = a2;
+  B = int32_t(round2_64(b2, 12));  // SGRPROJ_RECIP_BITS
+}
+
+struct SgrPass {
+  int r, n, s, one_over_n;
+};
+
+__device__ __forceinline__ SgrPass sgr_pass(int set, int pass) {
+  SgrPass q;
+  q.r = kSgrParams[set][pass * 2];
+  const int eps = kSgrParams[set][pass * 2 + 1];
+  q.n = (2 * q.r + 1) * (2 * q.r + 1);
+  const int n2e = q.n * q.n * eps;
+  q.s = q.r ? ((1 << 20) + n2e / 2) / n2e : 0;
+  q.one_over_n = ((1 << 12) + q.n / 2) / q.n;
+  return q;
+}
+
+// A self-guided filter output (postfilter.rs:950-988) at (i, j) from A/B
+// rows held in shared memory (`ab`: rows ai0.., stride aw; A then B).
+__device__ __forceinline__ int32_t sgr_flt(int pass, int yabs, int i_rel, int j, const int32_t* Ab, const int32_t* Bb,
+                                           int aw, int cval) {
+  int32_t a = 0, b = 0;
+#pragma unroll
+  for (int dy = -1; dy <= 1; dy++) {
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++) {
+      int wgt;
+      if (pass == 0)
+        wgt = ((yabs + dy) & 1) ? (dx == 0 ? 6 : 5) : 0;
+      else
+        wgt = (dx == 0 || dy == 0) ? 4 : 3;
+      if (wgt) {
+        const int k = (i_rel + 1 + dy) * aw + (j + 1 + dx);
+        a += wgt * Ab[k];
+        b += wgt * Bb[k];
+      }
+    }
+  }
+  const int shift = (pass == 0 && (yabs & 1)) ? 4 : 5;
+  return round2(a * cval + b, 8 + shift - 4);
+}
+
+// The same output with A/B computed on the spot (the in-order fallback).
+__device__ int32_t sgr_flt_direct(const Win& W, int pass, const SgrPass& q, int bd, int yabs, int i, int j, int cval) {
+  int32_t a = 0, b = 0;
+  for (int dy = -1; dy <= 1; dy++)
+    for (int dx = -1; dx <= 1; dx++) {
+      int wgt;
+      if (pass == 0)
+        wgt = ((yabs + dy) & 1) ? (dx == 0 ? 6 : 5) : 0;
+      else
+        wgt = (dx == 0 || dy == 0) ? 4 : 3;
+      if (wgt) {
+        int32_t A, B;
+        sgr_ab(W, i + 1 + dy, j + 1 + dx, q.r, q.n, q.s, q.one_over_n, bd, A, B);
+        a += wgt * A;
+        b += wgt * B;
+      }
+    }
+  const int shift = (pass == 0 && (yabs & 1)) ? 4 : 5;
+  return round2(a * cval + b, 8 + shift - 4);
+}
+
+// Fills A/B rows for output rows [i0, i0 + rows) of a rectangle (A/B rows
+// i0 .. i0 + rows + 1) for one pass. Pass 0 computes odd absolute rows only
+// (the others have weight 0).
+__device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
+                            int32_t* Ab, int32_t* Bb, int aw) {
+  const int n = (rows + 2) * (w + 2);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int ir = k / (w + 2), j = k - ir * (w + 2);
+    const int ai = i0 + ir;
+    if (pass == 0 && ((y0 + ai - 1) & 1) == 0) continue;
+    int32_t A, B;
+    sgr_ab(W, ai, j, q.r, q.n, q.s, q.one_over_n, bd, A, B);
+    Ab[ir * aw + j] = A;
+    Bb[ir * aw + j] = B;
+  }
+}
+
+}  // namespace
+
+// Shared memory of the search kernel: the window, then a region used as the
+// Wiener pass's term rows or the self-guided A/B bands.
+size_t lr_search_smem(int wmax, int hmax) {
+  const size_t ws = size_t(wmax + 2 * kB + 1) & ~size_t(1);
+  const size_t win = ((size_t(hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15);
+  const size_t terms = size_t(2) * 4 * size_t(wmax) * sizeof(double);
+  const size_t ab = size_t(4) * (kBand + 2) * size_t(wmax + 2) * sizeof(int32_t);
+  return win + (terms > ab ? terms : ab);
+}
+
+__global__ void __launch_bounds__(kThreads) lr_search_kernel(const LrSearchDesc d) {
+  extern __shared__ __align__(16) uint8_t lrs_smem[];
+  __shared__ int64_t red[kThreads / 32];
+  __shared__ double s_m[3][3], s_v[3], s_hc[3], s_vc[3];
+  __shared__ int s_coef[2][3];
+  __shared__ int s_xqd[2];
+  __shared__ double s_best_cost;
+  __shared__ av1pf_lr_unit s_best;
+  const LrSearchJob job = d.jobs[blockIdx.x];
+  const int p = job.plane, x0 = job.x0, w = job.w;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ws = (d.wmax + 2 * kB + 1) & ~1;
+  int16_t* win = reinterpret_cast<int16_t*>(lrs_smem);
+  uint8_t* region = lrs_smem + (((size_t(d.hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15));
+  const Win W{win, ws};
+  const int bd = d.bd, sb = d.sb, maxv = (1 << bd) - 1;
+  const int first = p == 0 ? 0 : 1;
+  const LrSearchRect* rects = d.rects + job.r0;
+  const int step = d.step;
+
+  // --- no filter: the CDEF output's error (encoder/lr.rs:134-146) ---
+  int64_t acc = 0;
+  for (int ri = 0; ri < job.nr; ri++) {
+    const LrSearchRect rc = rects[ri];
+    for (int k = tid; k < rc.h * w; k += blockDim.x) {
+      const int i = k / w, j = k - i * w;
+      const int e = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+      acc += int64_t(e) * e;
+    }
+  }
+  const uint64_t none = uint64_t(block_sum_i64(acc, red));
+  if (tid == 0) {
+    s_best_cost = __dadd_rn(__ull2double_rn(none), d.lambda);
+    s_best = av1pf_lr_unit{};
+    for (int k = 0; k < 3; k++) s_hc[k] = s_vc[k] = 0.0;
+  }
+  __syncthreads();
+
+  // --- Wiener fit (encoder/lr.rs:235-328) ---
+  for (int iter = 0; iter < 3; iter++) {
+    const bool vertical = (iter & 1) == 0;
+    const double* other = vertical ? s_hc : s_vc;
+    const int nci = (w + step - 1) / step;
+    if (iter == 0) {
+      // lines of plain samples: integer terms, summed exactly in any order
+      int64_t m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
+      for (int ri = 0; ri < job.nr; ri++) {
+        const LrSearchRect rc = rects[ri];
+        __syncthreads();
+        stage_window(d, p, rc, x0, w, win, ws);
+        __syncthreads();
+        const int nri = (rc.h + step - 1) / step;
+        for (int k = tid; k < nri * nci; k += blockDim.x) {
+          const int i = (k / nci) * step, j = (k % nci) * step;
+          int ln[7];
+#pragma unroll
+          for (int t = 0; t < 7; t++) ln[t] = vertical ? W.at(i + t, j + kB) : W.at(i + kB, j + t);
+          const int64_t tg = ld(d.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
+          const int64_t d0 = ln[0] + ln[6] - 2 * ln[3], d1 = ln[1] + ln[5] - 2 * ln[3], d2 = ln[2] + ln[4] - 2 * ln[3];
+          m00 += d0 * d0;
+          m01 += d0 * d1;
+          m02 += d0 * d2;
+          m11 += d1 * d1;
+          m12 += d1 * d2;
+          m22 += d2 * d2;
+          v0 += d0 * tg;
+          v1 += d1 * tg;
+          v2 += d2 * tg;
+        }
+      }
+      const int64_t sums[9] = {m00, m01, m02, m11, m12, m22, v0, v1, v2};
+      double tot[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) tot[q] = double(block_sum_i64(sums[q], red));
+      if (tid == 0) {
+        s_m[0][0] = tot[0];
+        s_m[0][1] = s_m[1][0] = tot[1];
+        s_m[0][2] = s_m[2][0] = tot[2];
+        s_m[1][1] = tot[3];
+        s_m[1][2] = s_m[2][1] = tot[4];
+        s_m[2][2] = tot[5];
+        s_v[0] = tot[6];
+        s_v[1] = tot[7];
+        s_v[2] = tot[8];
+      }
+    } else {
+      // real-valued terms: each accumulator adds its terms in sample order
+      // (lane q of warp 0 owns accumulator q: m00 m01 m02 m11 m12 m22 v0 v1 v2)
+      double* terms = reinterpret_cast<double*>(region);  // [2 buffers][4][wmax]: d0 d1 d2 t
+      double macc = 0.0;
+      const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
+      const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
+      const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
+      for (int ri = 0; ri < job.nr; ri++) {
+        const LrSearchRect rc = rects[ri];
+        __syncthreads();
+        stage_window(d, p, rc, x0, w, win, ws);
+        __syncthreads();
+        const int nri = (rc.h + step - 1) / step;
+        // rows in turn, two buffers: warps 1.. fill row r + 1 while warp 0 adds row r
+        for (int rr = 0; rr <= nri; rr++) {
+          if (rr < nri && warp > 0) {
+            double* tb = terms + (rr & 1) * 4 * d.wmax;
+            const int i = rr * step;
+            for (int jj = tid - 32; jj < nci; jj += blockDim.x - 32) {
+              const int j = jj * step;
+              double line[7];
+              wiener_line(W, vertical, i, j, other, line);
+              const double two3 = __dmul_rn(2.0, line[3]);
+              tb[0 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
+              tb[1 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
+              tb[2 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
+              tb[3 * d.wmax + jj] =
+                  __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
+            }
+          }
+          if (rr > 0 && owner) {
+            const double* tb = terms + ((rr - 1) & 1) * 4 * d.wmax;
+            for (int jj = 0; jj < nci; jj++)
+              macc = __dadd_rn(macc, __dmul_rn(tb[qa * d.wmax + jj], tb[qb * d.wmax + jj]));
+          }
+          __syncthreads();
+        }
+      }
+      if (owner) {
+        if (qb == 3)
+          s_v[qa] = macc;
+        else
+          s_m[qa][qb] = s_m[qb][qa] = macc;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double sol[3] = {0.0, 0.0, 0.0};
+      if (first == 0) {
+        double m[3][3], v[3];
+        for (int a = 0; a < 3; a++) {
+          v[a] = s_v[a];
+          for (int b = 0; b < 3; b++) m[a][b] = s_m[a][b];
+        }
+        solve<3>(m, v, sol);
+      } else {
+        double m[2][2] = {{s_m[1][1], s_m[1][2]}, {s_m[2][1], s_m[2][2]}}, v[2] = {s_v[1], s_v[2]}, x2[2];
+        solve<2>(m, v, x2);
+        sol[1] = x2[0];
+        sol[2] = x2[1];
+      }
+      for (int k = 0; k < 3; k++) (vertical ? s_vc : s_hc)[k] = sol[k];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    for (int k = 0; k < 3; k++) {
+      s_coef[0][k] = k < first ? 0 : min(max(f64_to_i32(round(s_vc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
+      s_coef[1][k] = k < first ? 0 : min(max(f64_to_i32(round(s_hc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
+    }
+  }
+  __syncthreads();
+  // --- the Wiener filter's error (postfilter.rs:781-822 restoration) ---
+  {
+    int vf[7], hf[7];
+    vf[3] = hf[3] = 128;
+    for (int k = 0; k < 3; k++) {
+      vf[k] = vf[6 - k] = s_coef[0][k];
+      hf[k] = hf[6 - k] = s_coef[1][k];
+      vf[3] -= 2 * s_coef[0][k];
+      hf[3] -= 2 * s_coef[1][k];
+    }
+    const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
+    const int off = 1 << (bd + 7 - round0 - 1), lim = (1 << (bd + 1 + 7 - round0)) - 1;
+    acc = 0;
+    for (int ri = 0; ri < job.nr; ri++) {
+      const LrSearchRect rc = rects[ri];
+      __syncthreads();
+      stage_window(d, p, rc, x0, w, win, ws);
+      __syncthreads();
+      for (int k = tid; k < rc.h * w; k += blockDim.x) {
+        const int i = k / w, j = k - i * w;
+        const int e = wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) -
+                      ld(d.src[p], sb, x0 + j, rc.y0 + i);
+        acc += int64_t(e) * e;
+      }
+    }
+    const uint64_t e = uint64_t(block_sum_i64(acc, red));
+    if (tid == 0) {
+      const double cost = __dadd_rn(__ull2double_rn(e), __dmul_rn(d.lambda, p == 0 ? 40.0 : 28.0));
+      if (cost < s_best_cost) {
+        s_best_cost = cost;
+        s_best = av1pf_lr_unit{};
+        s_best.type = AV1PF_RESTORE_WIENER;
+        for (int a = 0; a < 2; a++)
+          for (int b = 0; b < 3; b++) s_best.wiener[a][b] = int8_t(s_coef[a][b]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // --- self-guided fits (encoder/lr.rs:330-430), one parameter set at a time ---
+  int32_t* Ab[2];
+  int32_t* Bb[2];
+  const int aw = d.wmax + 2;
+  for (int q = 0; q < 2; q++) {
+    Ab[q] = reinterpret_cast<int32_t*>(region) + (2 * q) * (kBand + 2) * aw;
+    Bb[q] = reinterpret_cast<int32_t*>(region) + (2 * q + 1) * (kBand + 2) * aw;
+  }
+  for (int si = 0; si < d.nsets; si++) {
+    const int set = d.sets[si];
+    const SgrPass q0 = sgr_pass(set, 0), q1 = sgr_pass(set, 1);
+    const int r0 = q0.r, r1 = q1.r;
+    // fit sums, exact in int64, with the magnitudes' sums to check exactness
+    int64_t f00 = 0, f01 = 0, f11 = 0, g0 = 0, g1 = 0;
+    uint64_t b01 = 0, bg0 = 0, bg1 = 0;
+    for (int pass_sse = 0; pass_sse < 2; pass_sse++) {
+      // pass_sse 0: the fit; 1: the error with the quantised weights
+      int pw0 = 0, pw1 = 0, pw2 = 0;
+      if (pass_sse == 1) {
+        pw0 = s_xqd[0];
+        pw1 = s_xqd[1];
+        pw2 = (1 << 7) - pw0 - pw1;
+      }
+      acc = 0;
+      for (int ri = 0; ri < job.nr; ri++) {
+        const LrSearchRect rc = rects[ri];
+        __syncthreads();
+        stage_window(d, p, rc, x0, w, win, ws);
+        for (int i0 = 0; i0 < rc.h; i0 += kBand) {
+          const int rows = min(kBand, rc.h - i0);
+          __syncthreads();
+          if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw);
+          if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw);
+          __syncthreads();
+          for (int k = tid; k < rows * w; k += blockDim.x) {
+            const int ir = k / w, j = k - ir * w;
+            const int i = i0 + ir, yabs = rc.y0 + i;
+            if (pass_sse == 0 && ((i % step) != 0 || (j % step) != 0)) continue;
+            const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
+            const int u = cval << 4;  // SGRPROJ_RST_BITS
+            const int fl0 = r0 ? sgr_flt(0, yabs, ir, j, Ab[0], Bb[0], aw, cval) : 0;
+            const int fl1 = r1 ? sgr_flt(1, yabs, ir, j, Ab[1], Bb[1], aw, cval) : 0;
+            const int sv = ld(d.src[p], sb, x0 + j, yabs);
+            if (pass_sse == 0) {
+              const int64_t a = r0 ? int64_t(fl0 - u) : 0, b = r1 ? int64_t(fl1 - u) : 0;
+              const int64_t t = 128 * (int64_t(sv << 4) - u);
+              f00 += a * a;
+              f01 += a * b;
+              f11 += b * b;
+              g0 += a * t;
+              g1 += b * t;
+              b01 += uint64_t(llabs(a * b));
+              bg0 += uint64_t(llabs(a * t));
+              bg1 += uint64_t(llabs(b * t));
+            } else {
+              int32_t val = pw1 * u;
+              val += r0 ? pw0 * fl0 : pw0 * u;
+              val += r1 ? pw2 * fl1 : pw2 * u;
+              const int out = min(max(round2(val, 4 + 7), 0), maxv);
+              const int e = out - sv;
+              acc += int64_t(e) * e;
+            }
+          }
+        }
+      }
+      if (pass_sse == 0) {
+        const int64_t t00 = block_sum_i64(f00, red), t01 = block_sum_i64(f01, red), t11 = block_sum_i64(f11, red);
+        const int64_t tg0 = block_sum_i64(g0, red), tg1 = block_sum_i64(g1, red);
+        // each f64 partial sum is exact (so any order gives the reference's
+        // sums) while the terms' magnitudes sum below 2^53
+        const uint64_t m00abs = uint64_t(t00), m11abs = uint64_t(t11);
+        const uint64_t sb01 = uint64_t(block_sum_i64(int64_t(b01), red));
+        const uint64_t sbg0 = uint64_t(block_sum_i64(int64_t(bg0), red));
+        const uint64_t sbg1 = uint64_t(block_sum_i64(int64_t(bg1), red));
+        const bool exact = m00abs < kExact && m11abs < kExact && sb01 < kExact && sbg0 < kExact && sbg1 < kExact;
+        if (tid == 0) {
+          double m00, m01, m11, v0, v1;
+          if (exact) {
+            m00 = double(t00);
+            m01 = double(t01);
+            m11 = double(t11);
+            v0 = double(tg0);
+            v1 = double(tg1);
+          } else {
+            // the reference's f64 sums in sample order (rare: very large units
+            // with large errors at 12 bits)
+            m00 = m01 = m11 = v0 = v1 = 0.0;
+            for (int ri = 0; ri < job.nr; ri++) {
+              const LrSearchRect rc = rects[ri];
+              // the window of this rectangle is rebuilt by this thread alone
+              const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
+              for (int k = 0; k < ww * wh; k++) {
+                const int rr = k / ww, c = k - rr * ww;
+                const int x = max(min(x0 + c - kB, d.pex[p]), 0), y = max(min(rc.y0 + rr - kB, d.pey[p]), 0);
+                win[rr * ws + c] = int16_t(y < rc.ss   ? ld(d.cur[p], sb, x, max(rc.ss - 2, y))
+                                           : y > rc.se ? ld(d.cur[p], sb, x, min(rc.se + 2, y))
+                                                       : ld(d.cdef[p], sb, x, y));
+              }
+              for (int i = 0; i < rc.h; i += step)
+                for (int j = 0; j < w; j += step) {
+                  const int yabs = rc.y0 + i;
+                  const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
+                  const double u = double(cval << 4);
+                  const double a = r0 ? __dsub_rn(double(sgr_flt_direct(W, 0, q0, bd, yabs, i, j, cval)), u) : 0.0;
+                  const double b = r1 ? __dsub_rn(double(sgr_flt_direct(W, 1, q1, bd, yabs, i, j, cval)), u) : 0.0;
+                  const double t = __dmul_rn(128.0, __dsub_rn(double(ld(d.src[p], sb, x0 + j, yabs) << 4), u));
+                  m00 = __dadd_rn(m00, __dmul_rn(a, a));
+                  m01 = __dadd_rn(m01, __dmul_rn(a, b));
+                  m11 = __dadd_rn(m11, __dmul_rn(b, b));
+                  v0 = __dadd_rn(v0, __dmul_rn(a, t));
+                  v1 = __dadd_rn(v1, __dmul_rn(b, t));
+                }
+            }
+          }
+          double w0, w2;
+          if (r0 && r1) {
+            double m[2][2] = {{m00, m01}, {m01, m11}}, v[2] = {v0, v1}, x2[2];
+            solve<2>(m, v, x2);
+            w0 = x2[0];
+            w2 = x2[1];
+          } else if (r0) {
+            w0 = m00 > 0.0 ? __ddiv_rn(v0, m00) : 0.0;
+            w2 = 0.0;
+          } else {
+            w0 = 0.0;
+            w2 = m11 > 0.0 ? __ddiv_rn(v1, m11) : 0.0;
+          }
+          const int x0q = r0 ? min(max(f64_to_i32(round(w0)), kXqdMin[0]), kXqdMax[0]) : 0;
+          int x1q;
+          if (r1) {
+            // i32 arithmetic wraps as the reference's release build does
+            const int diff = int(uint32_t(1 << 7) - uint32_t(x0q) - uint32_t(f64_to_i32(round(w2))));
+            x1q = min(max(diff, kXqdMin[1]), kXqdMax[1]);
+          } else {
+            x1q = min(max((1 << 7) - x0q, kXqdMin[1]), kXqdMax[1]);
+          }
+          s_xqd[0] = x0q;
+          s_xqd[1] = x1q;
+        }
+        __syncthreads();
+      } else {
+        const uint64_t e = uint64_t(block_sum_i64(acc, red));
+        if (tid == 0) {
+          const double cost = __dadd_rn(__ull2double_rn(e), __dmul_rn(d.lambda, 20.0));
+          if (cost < s_best_cost) {
+            s_best_cost = cost;
+            s_best = av1pf_lr_unit{};
+            s_best.type = AV1PF_RESTORE_SGRPROJ;
+            s_best.sgr_set = uint8_t(set);
+            s_best.sgr_xqd[0] = int8_t(s_xqd[0]);
+            s_best.sgr_xqd[1] = int8_t(s_xqd[1]);
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (tid == 0) d.out[blockIdx.x] = s_best;
+}
+
+cudaError_t lr_search_init(size_t smem) {
+  return cudaFuncSetAttribute(lr_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+}
+
+void launch_lr_search(const LrSearchDesc& d, int njobs, size_t smem, cudaStream_t s) {
+  if (njobs <= 0) return;
+  lr_search_kernel<<<njobs, kThreads, smem, s>>>(d);
+  note_launch();
+}
+
+}  // namespace av1pf

@@ -76,6 +76,21 @@ void cdef_candidates(bool thorough, std::vector<std::pair<int, int>>& y, std::ve
   }
 }
 
+// Planes covering each plane's visible (upscaled) area, 16-byte aligned rows.
+int check_visible(const av1pf_frame_info* i, const av1pf_plane* pl, const char* what) {
+  if (!pl) return fail_input(what);
+  for (int p = 0; p < i->num_planes; p++) {
+    const int sx = p ? i->subsampling_x : 0, sy = p ? i->subsampling_y : 0;
+    if (!pl[p].data) return fail_input(what);
+    if ((reinterpret_cast<uintptr_t>(pl[p].data) & 15) || ((pl[p].stride * i->sample_bytes) & 15))
+      return fail_input("planes and rows must be 16-byte aligned");
+    if (pl[p].stride < pl[p].width || pl[p].width < ((i->upscaled_width + sx) >> sx) ||
+        pl[p].height < ((i->frame_height + sy) >> sy))
+      return fail_input("plane smaller than the visible frame");
+  }
+  return AV1PF_OK;
+}
+
 int coded_sec(int coded) { return coded == 3 ? 4 : coded; }  // encoder/cdef.rs:43-46
 int damping_for(int qidx) { return std::min(qidx >> 6, 3); }  // encoder/cdef.rs:255-258
 
@@ -294,6 +309,131 @@ int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
     levels_out[0] = levels_out[1] = best_l[0];
     levels_out[2] = best_l[1];
     levels_out[3] = best_l[2];
+  }
+  return AV1PF_OK;
+}
+
+int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                    const av1pf_plane* cur, const av1pf_plane* cdef, const av1pf_plane* src, double lambda,
+                    int32_t effort, av1pf_lr_unit* const units_out[3], int32_t frame_type_out[3], void* stream) {
+  int rc = enter(ctx);
+  if (rc) return rc;
+  if (!params) return fail_input("null params");
+  // the unit grid as a frame whose planes all use switchable restoration
+  av1pf_params q = *params;
+  q.uses_lr = 1;
+  for (int k = 0; k < 3; k++) q.frame_restoration_type[k] = 3;
+  q.cdef_enabled = 0;
+  std::string why;
+  if ((rc = validate_frame(info, &q, nullptr, &why)) != AV1PF_OK) return set_error(why), rc;
+  if ((rc = check_visible(info, cur, "null deblocked planes")) != AV1PF_OK ||
+      (rc = check_visible(info, cdef, "null CDEF planes")) != AV1PF_OK ||
+      (rc = check_visible(info, src, "null source planes")) != AV1PF_OK)
+    return rc;
+  if (effort < 0 || effort > 2) return fail_input("effort must be 0 (fast), 1 (normal) or 2 (thorough)");
+  if (!std::isfinite(lambda)) return fail_input("lambda must be finite");
+  if (!units_out || !frame_type_out) return fail_input("null outputs");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int np = info->num_planes;
+
+  LrSearchDesc d{};
+  d.bd = info->bit_depth;
+  d.sb = info->sample_bytes;
+  // encoder/lr.rs:74-81: parameter sets and the fit's sampling step
+  static const int kNormal[6] = {0, 3, 6, 10, 13, 14}, kFast[2] = {3, 10};
+  if (effort == 2) {
+    d.nsets = 16;
+    for (int k = 0; k < 16; k++) d.sets[k] = k;
+  } else if (effort == 1) {
+    d.nsets = 6;
+    for (int k = 0; k < 6; k++) d.sets[k] = kNormal[k];
+  } else {
+    d.nsets = 2;
+    for (int k = 0; k < 2; k++) d.sets[k] = kFast[k];
+  }
+  d.step = effort == 0 ? 2 : 1;
+  d.lambda = lambda;
+  // jobs: every unit with a stripe and columns inside the plane (encoder/lr.rs:84-122)
+  std::vector<LrSearchJob> jobs;
+  std::vector<LrSearchRect> rects;
+  std::vector<std::array<int, 3>> where;  // (plane, unit row, unit column) of each job
+  const int stripes = (info->frame_height + 8 + 63) / 64;
+  for (int p = 0; p < np; p++) {
+    const int sx = p ? info->subsampling_x : 0, sy = p ? info->subsampling_y : 0;
+    d.cur[p] = dplane(cur[p]);
+    d.cdef[p] = dplane(cdef[p]);
+    d.src[p] = dplane(src[p]);
+    d.pex[p] = ((info->upscaled_width + sx) >> sx) - 1;
+    d.pey[p] = ((info->frame_height + sy) >> sy) - 1;
+    const int us = q.loop_restoration_size[p], urows = q.lr_unit_rows[p], ucols = q.lr_unit_cols[p];
+    // lr_stripe (postfilter.rs:640-661): each stripe's unit row
+    std::vector<std::vector<LrSearchRect>> by_row(static_cast<size_t>(urows));
+    for (int st = 0; st < stripes; st++) {
+      const int ss = (-8 + st * 64) >> sy, se = ss + (64 >> sy) - 1;
+      const int y0 = std::max(ss, 0), y1 = std::min(se, d.pey[p]);
+      if (y0 > y1) continue;
+      const int luma_row = st * 64 >= 8 ? st * 64 - 8 : 0;
+      const int ur = std::min(urows - 1, ((luma_row + 8) >> sy) / us);
+      by_row[size_t(ur)].push_back(LrSearchRect{ss, se, y0, y1 - y0 + 1});
+    }
+    for (int ur = 0; ur < urows; ur++)
+      for (int uc = 0; uc < ucols; uc++) {
+        // lr_unit_cols (postfilter.rs:664-675)
+        const int x0 = uc * us;
+        const int x1 = uc + 1 == ucols ? d.pex[p] : std::min((uc + 1) * us - 1, d.pex[p]);
+        if (x0 > d.pex[p] || by_row[size_t(ur)].empty()) continue;
+        LrSearchJob jb{p, x0, x1 - x0 + 1, int32_t(rects.size()), int32_t(by_row[size_t(ur)].size())};
+        for (const LrSearchRect& r : by_row[size_t(ur)]) {
+          rects.push_back(r);
+          d.hmax = std::max(d.hmax, r.h);
+        }
+        d.wmax = std::max(d.wmax, jb.w);
+        jobs.push_back(jb);
+        where.push_back({p, ur, uc});
+      }
+  }
+  std::vector<av1pf_lr_unit> chosen(jobs.size());
+  if (!jobs.empty()) {
+    const size_t smem = lr_search_smem(d.wmax, d.hmax);
+    cudaError_t e = lr_search_init(smem);
+    if (e != cudaSuccess) return cuda_status(e, "loop-restoration search attributes");
+    const size_t jb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);
+    const size_t ob = jobs.size() * sizeof(av1pf_lr_unit);
+    const size_t o_rects = align256(jb), o_out = o_rects + align256(rb), total = o_out + align256(ob);
+    if ((rc = ctx->ensure(ctx->search_dev, total)) != AV1PF_OK) return rc;
+    if ((rc = ctx->ensure_host(ctx->search_host, total)) != AV1PF_OK) return rc;
+    uint8_t* dv = static_cast<uint8_t*>(ctx->search_dev.ptr);
+    uint8_t* hs = static_cast<uint8_t*>(ctx->search_host.ptr);
+    std::memcpy(hs, jobs.data(), jb);
+    std::memcpy(hs + o_rects, rects.data(), rb);
+    d.jobs = reinterpret_cast<const LrSearchJob*>(dv);
+    d.rects = reinterpret_cast<const LrSearchRect*>(dv + o_rects);
+    d.out = reinterpret_cast<av1pf_lr_unit*>(dv + o_out);
+    e = cudaMemcpyAsync(dv, hs, o_out, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_status(e, "loop-restoration search upload");
+    launch_lr_search(d, int(jobs.size()), smem, s);
+    e = cudaMemcpyAsync(hs + o_out, dv + o_out, ob, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "loop-restoration search");
+    std::memcpy(chosen.data(), hs + o_out, ob);
+  }
+  // the plan: units without a job keep no filter (encoder/lr.rs:188-208)
+  for (int p = 0; p < 3; p++) {
+    frame_type_out[p] = 0;
+    if (p >= np || !units_out[p]) continue;
+    const size_t n = size_t(q.lr_unit_rows[p]) * size_t(q.lr_unit_cols[p]);
+    for (size_t k = 0; k < n; k++) units_out[p][k] = av1pf_lr_unit{};
+  }
+  bool used[3][3] = {};
+  for (size_t k = 0; k < jobs.size(); k++) {
+    const int p = where[k][0];
+    used[p][chosen[k].type] = true;
+    if (units_out[p]) units_out[p][size_t(where[k][1]) * size_t(q.lr_unit_cols[p]) + size_t(where[k][2])] = chosen[k];
+  }
+  for (int p = 0; p < np; p++) {
+    const bool wu = used[p][AV1PF_RESTORE_WIENER], su = used[p][AV1PF_RESTORE_SGRPROJ];
+    frame_type_out[p] = wu ? (su ? 3 : AV1PF_RESTORE_WIENER) : (su ? AV1PF_RESTORE_SGRPROJ : AV1PF_RESTORE_NONE);
   }
   return AV1PF_OK;
 }

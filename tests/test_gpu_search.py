@@ -1,7 +1,9 @@
 """The encoder's filter searches on the GPU (av1pf_cdef_search,
-av1pf_lf_search) against the oracle, bit for bit: the chosen CDEF strengths,
-bits and damping, the per-block index table and every candidate's per-block
-error; the loop-filter levels and every scale's plane errors. Shapes cover
+av1pf_lf_search, av1pf_lr_search) against the oracle, bit for bit: the
+chosen CDEF strengths, bits and damping, the per-block index table and every
+candidate's per-block error; the loop-filter levels and every scale's plane
+errors; every restoration unit's choice (type, Wiener coefficients,
+self-guided set and weights) and each plane's restoration type. Shapes cover
 8/10/12-bit, one- and two-byte samples, 4:2:0, 4:2:2, 4:4:4 and monochrome,
 ragged frame edges, full HD, frames with no coding block, and both
 candidate lists."""
@@ -152,3 +154,65 @@ def test_lf_search_picks_levels_on_blocky_reconstruction(ctx):
     lv_g, sse_g = gpu_lf_search(ctx, sf, cur, src, params=p)
     assert np.array_equal(sse_g, sse_o) and lv_g == lv_o
     assert lv_o[0] > 0
+
+
+LR_CASES = {
+    "256x144_10b": dict(width=256, height=144, bit_depth=10, seed=41, enable_lr=1),
+    "200x120_8b_u8": dict(width=200, height=120, bit_depth=8, sample_bytes=1, seed=42, enable_lr=1, lr_unit_shift=1),
+    "136x72_12b_444": dict(width=136, height=72, bit_depth=12, subsampling_x=0, subsampling_y=0, seed=43,
+                           enable_lr=1),
+    "160x96_10b_422": dict(width=160, height=96, bit_depth=10, subsampling_x=1, subsampling_y=0, seed=44,
+                           enable_lr=1, lr_unit_shift=2),
+    "120x80_10b_mono": dict(width=120, height=80, bit_depth=10, mono=1, seed=45, enable_lr=1),
+    "600x300_12b_256units": dict(width=600, height=300, bit_depth=12, seed=46, enable_lr=1, lr_unit_shift=2,
+                                 lr_uv_shift=0),
+    "1920x1080_10b": dict(width=1920, height=1080, bit_depth=10, seed=47, enable_lr=1),
+}
+
+
+def gpu_lr_search(ctx, sf, cur, cdef, src, lam, effort):
+    info, params = sf.f.info, sf.f.params
+    dcur, dcdef, dsrc = (G.DevPlanes.from_host(info, x) for x in (cur, cdef, src))
+    arrs = O.lr_unit_arrays(params, info.num_planes)
+    ptrs = (C.POINTER(A.LrUnit) * 3)(*[C.cast(a, C.POINTER(A.LrUnit)) if a is not None else None for a in arrs])
+    ft = (C.c_int32 * 3)()
+    A.check(A.lib().av1pf_lr_search(ctx.p, C.byref(info), C.byref(params), dcur.c, dcdef.c, dsrc.c, lam, effort,
+                                    ptrs, ft, None), "av1pf_lr_search")
+    units = [[O.lr_unit_tuple(u) for u in arrs[p][:params.lr_unit_rows[p] * params.lr_unit_cols[p]]]
+             if arrs[p] is not None else [] for p in range(3)]
+    return list(ft), units
+
+
+@pytest.mark.parametrize("effort", [0, 1, 2], ids=["fast", "normal", "thorough"])
+@pytest.mark.parametrize("name", sorted(LR_CASES))
+def test_lr_search_matches_oracle(ctx, name, effort):
+    sf = A.SynthHandle(**LR_CASES[name])
+    cur, cdef, src = O.lr_search_inputs(sf, 51)
+    # lambda -1e12 makes every unit take its Wiener filter (every fitted
+    # coefficient compared); 0 takes the least error (self-guided fits compared)
+    for lam in (0.0, 150.0, -1e12):
+        o = O.lr_search(sf, cur, cdef, src, lam, effort)
+        g = gpu_lr_search(ctx, sf, cur, cdef, src, lam, effort)
+        assert g[0] == o[0], f"{name} lambda {lam}: frame types"
+        for p in range(3):
+            bad = [k for k, (a, b) in enumerate(zip(g[1][p], o[1][p])) if a != b]
+            assert not bad, f"{name} lambda {lam} plane {p}: units {bad[:4]} gpu {[g[1][p][k] for k in bad[:2]]} " \
+                            f"oracle {[o[1][p][k] for k in bad[:2]]}"
+
+
+def test_lr_search_identity_and_rejection(ctx):
+    sf = A.SynthHandle(**LR_CASES["256x144_10b"])
+    cur, cdef, src = O.lr_search_inputs(sf, 52)
+    ft, units = gpu_lr_search(ctx, sf, cur, src, src, 5.0, 1)
+    assert ft == [0, 0, 0] and all(u[0] == 0 for pl in units for u in pl)
+    info, params = sf.f.info, sf.f.params
+    d = G.DevPlanes.from_host(info, src)
+    arrs = O.lr_unit_arrays(params, info.num_planes)
+    ptrs = (C.POINTER(A.LrUnit) * 3)(*[C.cast(a, C.POINTER(A.LrUnit)) for a in arrs])
+    ft = (C.c_int32 * 3)()
+    L = A.lib()
+    for lam, eff in ((float("nan"), 1), (1.0, 3), (1.0, -1)):
+        assert L.av1pf_lr_search(ctx.p, C.byref(info), C.byref(params), d.c, d.c, d.c, lam, eff, ptrs, ft,
+                                 None) == A.ERR_INVALID_INPUT
+    assert L.av1pf_lr_search(ctx.p, C.byref(info), C.byref(params), d.c, None, d.c, 1.0, 1, ptrs, ft,
+                             None) == A.ERR_INVALID_INPUT

@@ -2,8 +2,9 @@
 encoder/mod.rs:1457-1506) against independent numpy restatements of their
 parts: the unfiltered candidate's block errors (skip flags, the frame crop,
 the 64x64 blocks that code an index), the greedy choice recomputed in Python
-from the error table, and the loop-filter search's per-scale plane errors.
-CPU only."""
+from the error table, and the loop-filter search's per-scale plane errors;
+and the loop-restoration search's Wiener fit (encoder/lr.rs:212-328) against
+a pure-Python restatement, window construction included. CPU only."""
 import ctypes as C
 
 import numpy as np
@@ -194,3 +195,147 @@ def test_searches_thread_count_invariant():
     b = O.cdef_search(sf, cur, src, 90, 20.0, True, threads=0)
     assert a[0].pairs() == b[0].pairs() and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
     assert O.lf_search(sf, cur, src, threads=1)[0] == O.lf_search(sf, cur, src, threads=0)[0]
+
+
+# ---------------------------------------------------------------------------
+# Loop-restoration search (encoder/lr.rs)
+# ---------------------------------------------------------------------------
+WIENER_MIN, WIENER_MAX = (-5, -23, -17), (10, 8, 46)
+
+
+def py_solve(m, v):
+    """encoder/lr.rs:212-233 in Python floats (f64, same operation order)."""
+    n = len(v)
+    m = [list(r) for r in m]
+    v = list(v)
+    for i in range(n):
+        piv = i
+        for a in range(i + 1, n):
+            if abs(m[a][i]) >= abs(m[piv][i]):
+                piv = a
+        m[i], m[piv] = m[piv], m[i]
+        v[i], v[piv] = v[piv], v[i]
+        if abs(m[i][i]) < 1e-9:
+            return [0.0] * n
+        for r in range(n):
+            if r != i:
+                f = m[r][i] / m[i][i]
+                for c in range(i, n):
+                    m[r][c] -= f * m[i][c]
+                v[r] -= f * v[i]
+    return [v[i] / m[i][i] for i in range(n)]
+
+
+def rust_round(x):
+    return int(np.floor(x + 0.5)) if x >= 0 else -int(np.floor(-x + 0.5))
+
+
+def py_fit_wiener(plane, rects, src, step):
+    """encoder/lr.rs:235-328 on pre-built windows: rects = [(win, y0, h)]."""
+    first = 0 if plane == 0 else 1
+    hc, vc = [0.0] * 3, [0.0] * 3
+    for it in range(3):
+        vertical = it % 2 == 0
+        m = [[0.0] * 3 for _ in range(3)]
+        v = [0.0] * 3
+        for win, y0, h, x0, w in rects:
+            at = lambda r, c: float(win[r][c])  # noqa: E731
+            for i in range(0, h, step):
+                for j in range(0, w, step):
+                    line = []
+                    for t in range(7):
+                        r, c = (i + t, j + 3) if vertical else (i + 3, j + t)
+                        other = hc if vertical else vc
+                        center = at(r, c)
+                        s = center
+                        for k in range(3):
+                            d = 3 - k
+                            a, b = (at(r, c - d), at(r, c + d)) if vertical else (at(r - d, c), at(r + d, c))
+                            s += other[k] * (a + b - 2.0 * center)
+                        line.append(s)
+                    target = float(src[y0 + i][x0 + j]) - line[3]
+                    d = [line[k] + line[6 - k] - 2.0 * line[3] for k in range(3)]
+                    for a in range(first, 3):
+                        for b in range(first, 3):
+                            m[a][b] += d[a] * d[b]
+                        v[a] += d[a] * target
+        if first == 0:
+            sol = py_solve(m, v)
+        else:
+            s2 = py_solve([[m[1][1], m[1][2]], [m[2][1], m[2][2]]], [v[1], v[2]])
+            sol = [0.0, s2[0], s2[1]]
+        if vertical:
+            vc = sol
+        else:
+            hc = sol
+    q = lambda c: tuple(0 if k < first else min(max(rust_round(c[k] * 128.0), WIENER_MIN[k]), WIENER_MAX[k])  # noqa
+                        for k in range(3))
+    return (q(vc), q(hc))
+
+
+def py_lr_rects(sf, plane, cur, cdef, ur, uc):
+    """The unit's stripes as (window, y0, h, x0, w) (postfilter.rs:640-675, 765-777)."""
+    info, p = sf.f.info, sf.f.params
+    sx = info.subsampling_x if plane else 0
+    sy = info.subsampling_y if plane else 0
+    pex = ((info.upscaled_width + sx) >> sx) - 1
+    pey = ((info.frame_height + sy) >> sy) - 1
+    us = p.loop_restoration_size[plane]
+    x0 = uc * us
+    x1 = pex if uc + 1 == p.lr_unit_cols[plane] else min((uc + 1) * us - 1, pex)
+    w = x1 - x0 + 1
+    rects = []
+    for s in range((info.frame_height + 8 + 63) // 64):
+        ss = (-8 + s * 64) >> sy
+        se = ss + (64 >> sy) - 1
+        y0, y1 = max(ss, 0), min(se, pey)
+        if y0 > y1:
+            continue
+        luma_row = s * 64 - 8 if s * 64 >= 8 else 0
+        if min(p.lr_unit_rows[plane] - 1, ((luma_row + 8) >> sy) // us) != ur:
+            continue
+        h = y1 - y0 + 1
+        win = [[0] * (w + 6) for _ in range(h + 6)]
+        for r in range(h + 6):
+            y = min(max(y0 + r - 3, 0), pey)
+            for c in range(w + 6):
+                xx = max(min(x0 + c - 3, pex), 0)
+                if y < ss:
+                    win[r][c] = int(cur.arrays[plane][max(ss - 2, y)][xx])
+                elif y > se:
+                    win[r][c] = int(cur.arrays[plane][min(se + 2, y)][xx])
+                else:
+                    win[r][c] = int(cdef.arrays[plane][y][xx])
+        rects.append((win, y0, h, x0, w))
+    return rects
+
+
+@pytest.mark.parametrize("effort", [0, 1])
+def test_lr_wiener_fit_matches_python_restatement(effort):
+    """lambda -1e12 makes every unit take its Wiener filter, exposing each
+    fitted coefficient set."""
+    sf = A.SynthHandle(width=72, height=40, bit_depth=10, seed=8, enable_lr=1, lr_unit_shift=0, lr_uv_shift=1)
+    cur, cdef, src = O.lr_search_inputs(sf, 21)
+    ft, units = O.lr_search(sf, cur, cdef, src, -1e12, effort)
+    p = sf.f.params
+    assert ft == [1, 1, 1]
+    for plane in range(3):
+        for ur in range(p.lr_unit_rows[plane]):
+            for uc in range(p.lr_unit_cols[plane]):
+                rects = py_lr_rects(sf, plane, cur, cdef, ur, uc)
+                want = py_fit_wiener(plane, rects, src.arrays[plane], 2 if effort == 0 else 1)
+                got = units[plane][ur * p.lr_unit_cols[plane] + uc]
+                assert got[0] == 1 and got[1] == want, (plane, ur, uc)
+
+
+def test_lr_search_identity_chooses_none():
+    sf = A.SynthHandle(width=256, height=144, bit_depth=10, seed=9, enable_lr=1)
+    cur, cdef, src = O.lr_search_inputs(sf, 22)
+    ft, units = O.lr_search(sf, cur, src, src, 5.0, 2)
+    assert ft == [0, 0, 0] and all(u[0] == 0 for pl in units for u in pl)
+
+
+def test_lr_search_thread_count_invariant():
+    sf = A.SynthHandle(width=200, height=120, bit_depth=12, subsampling_x=0, subsampling_y=0, seed=10, enable_lr=1)
+    cur, cdef, src = O.lr_search_inputs(sf, 23)
+    assert O.lr_search(sf, cur, cdef, src, 50.0, 1, threads=1) == O.lr_search(sf, cur, cdef, src, 50.0, 1, threads=0)
