@@ -639,9 +639,58 @@ def bench_search(args, ctx, rank, world):
             out["speedup_vs_oracle"] = {k: round(out["cpu_oracle_ms"][k] / out[k + "_ms"], 1)
                                         for k in ("cdef_fast", "cdef_thorough", "lf")}
         res[name] = out
+    res["lr_1080p_10bit"] = bench_lr_search(args, ctx, rank, world)
     res["inputs"] = (f"seeded synthetic frames; reconstruction = source + seeded 4x4-block noise (+-24) and "
                      f"per-sample noise; base_q_idx {q}, lambda {lam}")
     return res
+
+
+def bench_lr_search(args, ctx, rank, world, lam=150.0):
+    """The loop-restoration search (encoder/lr.rs:64-210) on a 1080p 10-bit
+    frame with 64x64 luma / 32x32 chroma units, each effort (fast: 2
+    self-guided sets on every other sample; normal: 6; thorough: 16), one
+    synchronous call per frame; the oracle's time beside it (rank 0, N = 1)."""
+    import gpu_util as G
+    import torch
+    L = A.lib()
+    sf = A.SynthHandle(width=1920, height=1080, bit_depth=10, seed=503, enable_lr=1)
+    info, params = sf.f.info, sf.f.params
+    cdef, src = A.synth_search_planes(sf, 8)
+    cur, _ = A.synth_search_planes(sf, 1008)
+    dev = []
+    for planes in (cur, cdef, src):
+        d = G.DevPlanes(info, [(a.shape[1], a.shape[0]) for a in planes], [a.shape[1] for a in planes])
+        for p in range(info.num_planes):
+            d.t[p].copy_(torch.from_numpy(planes[p].view(np.uint8).reshape(-1)))
+        dev.append(d)
+    arrs = [(A.LrUnit * (params.lr_unit_rows[p] * params.lr_unit_cols[p]))() for p in range(info.num_planes)]
+    ptrs = (C.POINTER(A.LrUnit) * 3)(*[C.cast(a, C.POINTER(A.LrUnit)) for a in arrs])
+    ft = (C.c_int32 * 3)()
+    out = {"units": [params.lr_unit_rows[p] * params.lr_unit_cols[p] for p in range(info.num_planes)]}
+    for eff, name in enumerate(("fast", "normal", "thorough")):
+        def run():
+            A.check(L.av1pf_lr_search(ctx.p, C.byref(info), C.byref(params), dev[0].c, dev[1].c, dev[2].c, lam, eff,
+                                      ptrs, ft, None), "av1pf_lr_search")
+        for _ in range(max(2, args.warmup)):
+            run()
+        reps = 10
+        t = time.perf_counter()
+        for _ in range(reps):
+            run()
+        out[name + "_ms"] = round((time.perf_counter() - t) / reps * 1e3, 3)
+        if rank == 0 and world == 1 and args.cpu_seconds > 0:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            t = time.perf_counter()
+            ft_o, units_o = O.lr_search(sf, O.HostPlanes(cur), O.HostPlanes(cdef), O.HostPlanes(src), lam, eff)
+            cms = (time.perf_counter() - t) * 1e3
+            same = ft_o == list(ft) and all(O.lr_unit_tuple(u) == units_o[p][k] for p in range(info.num_planes)
+                                            for k, u in enumerate(arrs[p]))
+            out.setdefault("cpu_oracle_ms", {})[name] = round(cms, 1)
+            out.setdefault("same_choice_as_oracle", {})[name] = bool(same)
+            out.setdefault("speedup_vs_oracle", {})[name] = round(cms / out[name + "_ms"], 1)
+    out["frame_types"] = list(ft)[:info.num_planes]
+    return out
 
 
 SERVE_MIX = [(8, dict(width=640, height=360, bit_depth=8, sample_bytes=1)),

@@ -114,16 +114,31 @@ struct LrSearchRect {
   int32_t ss, se;  // StripeStartY, StripeEndY
   int32_t y0, h;   // rows restored
 };
+// Per unit: the unfiltered error, the first Wiener pass's vertical
+// solution, the quantised Wiener coefficients and their error.
+struct LrJobState {
+  uint64_t none, wiener;
+  double vc[3];
+  int32_t coef[2][3];
+};
+// Per (unit, self-guided set): the projection weights and their error.
+struct LrSgrResult {
+  int32_t xqd[2];
+  uint64_t sse;
+};
 struct LrSearchDesc {
   DPlane cur[3], cdef[3], src[3];  // deblocked frame, CDEF output, source
   int32_t bd, sb;
   int32_t pex[3], pey[3];  // last column / row of each plane
   int32_t wmax, hmax;      // the widest unit and tallest rectangle
   int32_t step;            // fit on every step-th row and column
+  int32_t band, cache_px;  // self-guided rows per band; filter outputs kept per unit
   int32_t nsets, sets[16];
   double lambda;
   const LrSearchJob* jobs;
   const LrSearchRect* rects;
+  LrJobState* state;   // one per job
+  LrSgrResult* sgr;    // one per (job, set), set-minor
   av1pf_lr_unit* out;  // one per job
 };
 

@@ -85,10 +85,16 @@ struct SsePlane {
   int64_t sa, sb_;  // strides in samples
   int32_t w, h;
 };
-// The loop-restoration search (lr_search.cu): one CTA per unit job.
-size_t lr_search_smem(int wmax, int hmax);
-cudaError_t lr_search_init(size_t smem);  // raises the kernel's shared-memory limit
-void launch_lr_search(const LrSearchDesc& d, int njobs, size_t smem, cudaStream_t s);
+// The loop-restoration search (lr_search.cu): per unit job, a prep kernel
+// and the in-order Wiener passes on `s`, the self-guided fits (one CTA per
+// job and set) on `side` beside them, then the choice.
+size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px);
+// The self-guided band height and filter-output cache that fit shared memory.
+void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px);
+// Raises the kernels' shared-memory limits for that shape.
+cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px);
+void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                      cudaEvent_t join);
 void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s);
 
 // Super-resolution (superres.cu)

@@ -33,7 +33,7 @@ namespace av1pf {
 namespace {
 
 constexpr int kB = 3;            // window border (postfilter.rs:744 LRB)
-constexpr int kBand = 8;         // self-guided output rows per band
+constexpr int kSgrCachePx = 6144;  // filter outputs kept between the fit and its error (units up to 96 x 64)
 constexpr int kThreads = 256;
 __constant__ int32_t kSgrParams[16][4] = AV1T_SGR_PARAMS;
 __constant__ int32_t kWienerMin[3] = AV1T_WIENER_TAPS_MIN, kWienerMax[3] = AV1T_WIENER_TAPS_MAX;
@@ -57,22 +57,35 @@ struct Win {
 };
 
 // lr_window (postfilter.rs:765-777) of rectangle `rc` into shared memory.
+__device__ __forceinline__ int window_sample(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int ww,
+                                             int k) {
+  const int r = k / ww, c = k - r * ww;
+  const int x = max(min(x0 + c - kB, d.pex[p]), 0);
+  const int y = max(min(rc.y0 + r - kB, d.pey[p]), 0);
+  if (y < rc.ss) return ld(d.cur[p], d.sb, x, max(rc.ss - 2, y));
+  if (y > rc.se) return ld(d.cur[p], d.sb, x, min(rc.se + 2, y));
+  return ld(d.cdef[p], d.sb, x, y);
+}
+
 __device__ void stage_window(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int w, int16_t* win,
                              int ws) {
-  const int pex = d.pex[p], pey = d.pey[p];
-  const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
-  for (int k = threadIdx.x; k < ww * wh; k += blockDim.x) {
-    const int r = k / ww, c = k - r * ww;
-    const int x = max(min(x0 + c - kB, pex), 0);
-    const int y = max(min(rc.y0 + r - kB, pey), 0);
-    int v;
-    if (y < rc.ss)
-      v = ld(d.cur[p], d.sb, x, max(rc.ss - 2, y));
-    else if (y > rc.se)
-      v = ld(d.cur[p], d.sb, x, min(rc.se + 2, y));
-    else
-      v = ld(d.cdef[p], d.sb, x, y);
-    win[r * ws + c] = int16_t(v);
+  const int ww = w + 2 * kB, wh = rc.h + 2 * kB, n = ww * wh, nt = blockDim.x;
+  // four loads in flight per thread before their stores
+  for (int k0 = threadIdx.x; k0 < n; k0 += 4 * nt) {
+    int v[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = k0 + m * nt;
+      v[m] = k < n ? window_sample(d, p, rc, x0, ww, k) : 0;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = k0 + m * nt;
+      if (k < n) {
+        const int r = k / ww, c = k - r * ww;
+        win[r * ws + c] = int16_t(v[m]);
+      }
+    }
   }
 }
 
@@ -93,7 +106,7 @@ __device__ int64_t block_sum_i64(int64_t v, int64_t* red) {
 // last row of largest magnitude is the pivot (Iterator::max_by); zeros when
 // singular.
 template <int N>
-__device__ void solve(double (&m)[N][N], double (&v)[N], double (&x)[N]) {
+__device__ __noinline__ void solve(double (&m)[N][N], double (&v)[N], double (&x)[N]) {
   for (int i = 0; i < N; i++) {
     int piv = i;
     for (int a = i + 1; a < N; a++)
@@ -241,56 +254,122 @@ __device__ int32_t sgr_flt_direct(const Win& W, int pass, const SgrPass& q, int 
   return round2(a * cval + b, 8 + shift - 4);
 }
 
+// SGR_A2 (postfilter.rs:884-898), built at compile time.
+struct LrsA2 {
+  int32_t v[256];
+};
+constexpr LrsA2 make_lrs_a2() {
+  LrsA2 t{};
+  for (int z = 0; z < 256; z++) t.v[z] = z >= 255 ? 256 : (z == 0 ? 1 : ((z << 8) + z / 2) / (z + 1));
+  return t;
+}
+__device__ const LrsA2 g_lrs_a2 = make_lrs_a2();
+
 // Fills A/B rows for output rows [i0, i0 + rows) of a rectangle (A/B rows
-// i0 .. i0 + rows + 1) for one pass. Pass 0 computes odd absolute rows only
-// (the others have weight 0).
+// i0 .. i0 + rows + 1) for one pass (postfilter.rs:918-948), with separable
+// box sums: first each window row's horizontal sums of the samples and of
+// their squares (int32: 25 squares of 12-bit samples fit), then the
+// vertical sums. Pass 0 computes odd absolute rows only (the others have
+// weight 0). `hs`/`hq` hold (rows + 2 + 2r) x (w + 2) sums.
 __device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
-                            int32_t* Ab, int32_t* Bb, int aw) {
-  const int n = (rows + 2) * (w + 2);
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const int ir = k / (w + 2), j = k - ir * (w + 2);
-    const int ai = i0 + ir;
-    if (pass == 0 && ((y0 + ai - 1) & 1) == 0) continue;
-    int32_t A, B;
-    sgr_ab(W, ai, j, q.r, q.n, q.s, q.one_over_n, bd, A, B);
-    Ab[ir * aw + j] = A;
-    Bb[ir * aw + j] = B;
+                            int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+  const int r = q.r, cw = w + 2;
+  const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
+  __syncthreads();  // the previous users of hs / hq are done
+  for (int k = threadIdx.x; k < nrow * cw; k += blockDim.x) {
+    const int rr = k / cw, aj = k - rr * cw;
+    const int wy = wy0 + rr, wx = aj + kB - 1;
+    int32_t sum = 0, sq = 0;
+    for (int dx = -r; dx <= r; dx++) {
+      const int v = W.at(wy, wx + dx);
+      sum += v;
+      sq += v * v;
+    }
+    hs[k] = sum;
+    hq[k] = sq;
+  }
+  __syncthreads();
+  const int sh = 2 * (bd - 8);
+  for (int k = threadIdx.x; k < (rows + 2) * cw; k += blockDim.x) {
+    const int ir = k / cw, aj = k - ir * cw;
+    if (pass == 0 && ((y0 + i0 + ir - 1) & 1) == 0) continue;
+    int32_t bs = 0, as = 0;
+    for (int dy = 0; dy <= 2 * r; dy++) {
+      bs += hs[(ir + dy) * cw + aj];
+      as += hq[(ir + dy) * cw + aj];
+    }
+    const int32_t a = round2(as, sh);
+    const int32_t dd = round2(bs, bd - 8);
+    const int64_t p = max(int64_t(a) * q.n - int64_t(dd) * dd, int64_t(0));
+    const int64_t z = round2_64(p * q.s, 20);  // SGRPROJ_MTABLE_BITS
+    const int32_t a2 = g_lrs_a2.v[int(min(z, int64_t(255)))];
+    const int64_t b2 = int64_t((256 - a2) * bs) * int64_t(q.one_over_n);
+    Ab[ir * aw + aj] = a2;
+    Bb[ir * aw + aj] = int32_t(round2_64(b2, 12));  // SGRPROJ_RECIP_BITS
   }
 }
 
 }  // namespace
 
-// Shared memory of the search kernel: the window, then a region used as the
+// Shared memory of a search kernel: the window, then a region used as the
 // Wiener pass's term rows or the self-guided A/B bands.
-size_t lr_search_smem(int wmax, int hmax) {
+size_t lr_window_bytes(int wmax, int hmax) {
   const size_t ws = size_t(wmax + 2 * kB + 1) & ~size_t(1);
-  const size_t win = ((size_t(hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15);
-  const size_t terms = size_t(2) * 4 * size_t(wmax) * sizeof(double);
-  const size_t ab = size_t(4) * (kBand + 2) * size_t(wmax + 2) * sizeof(int32_t);
-  return win + (terms > ab ? terms : ab);
+  return ((size_t(hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15);
+}
+size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px) {
+  const size_t win = lr_window_bytes(wmax, hmax);
+  if (kind == 0) return win;                                                   // prep
+  if (kind == 1) return win + size_t(2) * 4 * size_t(wmax) * sizeof(double);  // Wiener passes
+  // self-guided: A/B of both passes, the band's box sums, the filter-output cache
+  return win + size_t(4) * (band + 2) * size_t(wmax + 2) * sizeof(int32_t) +
+         size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) + size_t(cache_px) * 2 * sizeof(int32_t);
 }
 
-__global__ void __launch_bounds__(kThreads) lr_search_kernel(const LrSearchDesc d) {
+void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px) {
+  // Filter outputs are kept when every unit's fit fits the cache; then the
+  // tallest band that leaves room for two CTAs per SM, else the tallest that
+  // fits at all.
+  constexpr size_t kTwo = 113 * 1024, kLimit = 220 * 1024;
+  cache_px = upx_max <= kSgrCachePx ? upx_max : 0;
+  for (size_t lim : {kTwo, kLimit})
+    for (band = 16; band >= 4; band /= 2)
+      if (lr_search_smem(wmax, hmax, 2, band, cache_px) <= lim) return;
+  band = 4;
+  cache_px = 0;
+}
+
+namespace {
+
+// Window stride and the region after the window.
+struct Smem {
+  int16_t* win;
+  int ws;
+  uint8_t* region;
+};
+__device__ __forceinline__ Smem smem_of(uint8_t* base, const LrSearchDesc& d) {
+  Smem m;
+  m.ws = (d.wmax + 2 * kB + 1) & ~1;
+  m.win = reinterpret_cast<int16_t*>(base);
+  m.region = base + ((((size_t(d.hmax + 2 * kB) * m.ws * 2) + 15) & ~size_t(15)));
+  return m;
+}
+
+}  // namespace
+
+// Phase 1, one CTA per unit (256 threads): the error without a filter
+// (encoder/lr.rs:134-146), and the first Wiener pass (vertical, the other
+// direction's filter still zero: its lines are plain samples, so its sums
+// are exact integer sums in any order) and its solve.
+__global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSearchDesc d) {
   extern __shared__ __align__(16) uint8_t lrs_smem[];
   __shared__ int64_t red[kThreads / 32];
-  __shared__ double s_m[3][3], s_v[3], s_hc[3], s_vc[3];
-  __shared__ int s_coef[2][3];
-  __shared__ int s_xqd[2];
-  __shared__ double s_best_cost;
-  __shared__ av1pf_lr_unit s_best;
   const LrSearchJob job = d.jobs[blockIdx.x];
-  const int p = job.plane, x0 = job.x0, w = job.w;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int ws = (d.wmax + 2 * kB + 1) & ~1;
-  int16_t* win = reinterpret_cast<int16_t*>(lrs_smem);
-  uint8_t* region = lrs_smem + (((size_t(d.hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15));
-  const Win W{win, ws};
-  const int bd = d.bd, sb = d.sb, maxv = (1 << bd) - 1;
-  const int first = p == 0 ? 0 : 1;
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const Smem sm = smem_of(lrs_smem, d);
+  const Win W{sm.win, sm.ws};
   const LrSearchRect* rects = d.rects + job.r0;
-  const int step = d.step;
-
-  // --- no filter: the CDEF output's error (encoder/lr.rs:134-146) ---
+  LrJobState& st = d.state[blockIdx.x];
   int64_t acc = 0;
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
@@ -300,106 +379,119 @@ __global__ void __launch_bounds__(kThreads) lr_search_kernel(const LrSearchDesc 
       acc += int64_t(e) * e;
     }
   }
-  const uint64_t none = uint64_t(block_sum_i64(acc, red));
-  if (tid == 0) {
-    s_best_cost = __dadd_rn(__ull2double_rn(none), d.lambda);
-    s_best = av1pf_lr_unit{};
-    for (int k = 0; k < 3; k++) s_hc[k] = s_vc[k] = 0.0;
+  const int64_t none = block_sum_i64(acc, red);
+  int64_t m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
+  const int nci = (w + step - 1) / step;
+  for (int ri = 0; ri < job.nr; ri++) {
+    const LrSearchRect rc = rects[ri];
+    __syncthreads();
+    stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+    __syncthreads();
+    const int nri = (rc.h + step - 1) / step;
+    for (int k = tid; k < nri * nci; k += blockDim.x) {
+      const int i = (k / nci) * step, j = (k % nci) * step;
+      int ln[7];
+#pragma unroll
+      for (int t = 0; t < 7; t++) ln[t] = W.at(i + t, j + kB);
+      const int64_t tg = ld(d.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
+      const int64_t d0 = ln[0] + ln[6] - 2 * ln[3], d1 = ln[1] + ln[5] - 2 * ln[3], d2 = ln[2] + ln[4] - 2 * ln[3];
+      m00 += d0 * d0;
+      m01 += d0 * d1;
+      m02 += d0 * d2;
+      m11 += d1 * d1;
+      m12 += d1 * d2;
+      m22 += d2 * d2;
+      v0 += d0 * tg;
+      v1 += d1 * tg;
+      v2 += d2 * tg;
+    }
   }
-  __syncthreads();
-
-  // --- Wiener fit (encoder/lr.rs:235-328) ---
-  for (int iter = 0; iter < 3; iter++) {
-    const bool vertical = (iter & 1) == 0;
-    const double* other = vertical ? s_hc : s_vc;
-    const int nci = (w + step - 1) / step;
-    if (iter == 0) {
-      // lines of plain samples: integer terms, summed exactly in any order
-      int64_t m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
-      for (int ri = 0; ri < job.nr; ri++) {
-        const LrSearchRect rc = rects[ri];
-        __syncthreads();
-        stage_window(d, p, rc, x0, w, win, ws);
-        __syncthreads();
-        const int nri = (rc.h + step - 1) / step;
-        for (int k = tid; k < nri * nci; k += blockDim.x) {
-          const int i = (k / nci) * step, j = (k % nci) * step;
-          int ln[7];
+  const int64_t sums[9] = {m00, m01, m02, m11, m12, m22, v0, v1, v2};
+  double tot[9];
 #pragma unroll
-          for (int t = 0; t < 7; t++) ln[t] = vertical ? W.at(i + t, j + kB) : W.at(i + kB, j + t);
-          const int64_t tg = ld(d.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
-          const int64_t d0 = ln[0] + ln[6] - 2 * ln[3], d1 = ln[1] + ln[5] - 2 * ln[3], d2 = ln[2] + ln[4] - 2 * ln[3];
-          m00 += d0 * d0;
-          m01 += d0 * d1;
-          m02 += d0 * d2;
-          m11 += d1 * d1;
-          m12 += d1 * d2;
-          m22 += d2 * d2;
-          v0 += d0 * tg;
-          v1 += d1 * tg;
-          v2 += d2 * tg;
-        }
-      }
-      const int64_t sums[9] = {m00, m01, m02, m11, m12, m22, v0, v1, v2};
-      double tot[9];
-#pragma unroll
-      for (int q = 0; q < 9; q++) tot[q] = double(block_sum_i64(sums[q], red));
-      if (tid == 0) {
-        s_m[0][0] = tot[0];
-        s_m[0][1] = s_m[1][0] = tot[1];
-        s_m[0][2] = s_m[2][0] = tot[2];
-        s_m[1][1] = tot[3];
-        s_m[1][2] = s_m[2][1] = tot[4];
-        s_m[2][2] = tot[5];
-        s_v[0] = tot[6];
-        s_v[1] = tot[7];
-        s_v[2] = tot[8];
-      }
+  for (int q = 0; q < 9; q++) tot[q] = double(block_sum_i64(sums[q], red));
+  if (tid == 0) {
+    st.none = uint64_t(none);
+    double sol[3] = {0.0, 0.0, 0.0};
+    if (p == 0) {
+      double m[3][3] = {{tot[0], tot[1], tot[2]}, {tot[1], tot[3], tot[4]}, {tot[2], tot[4], tot[5]}};
+      double v[3] = {tot[6], tot[7], tot[8]};
+      solve<3>(m, v, sol);
     } else {
-      // real-valued terms: each accumulator adds its terms in sample order
-      // (lane q of warp 0 owns accumulator q: m00 m01 m02 m11 m12 m22 v0 v1 v2)
-      double* terms = reinterpret_cast<double*>(region);  // [2 buffers][4][wmax]: d0 d1 d2 t
-      double macc = 0.0;
-      const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
-      const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
-      const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
-      for (int ri = 0; ri < job.nr; ri++) {
-        const LrSearchRect rc = rects[ri];
-        __syncthreads();
-        stage_window(d, p, rc, x0, w, win, ws);
-        __syncthreads();
-        const int nri = (rc.h + step - 1) / step;
-        // rows in turn, two buffers: warps 1.. fill row r + 1 while warp 0 adds row r
-        for (int rr = 0; rr <= nri; rr++) {
-          if (rr < nri && warp > 0) {
-            double* tb = terms + (rr & 1) * 4 * d.wmax;
-            const int i = rr * step;
-            for (int jj = tid - 32; jj < nci; jj += blockDim.x - 32) {
-              const int j = jj * step;
-              double line[7];
-              wiener_line(W, vertical, i, j, other, line);
-              const double two3 = __dmul_rn(2.0, line[3]);
-              tb[0 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
-              tb[1 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
-              tb[2 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
-              tb[3 * d.wmax + jj] =
-                  __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
-            }
+      double m[2][2] = {{tot[3], tot[4]}, {tot[4], tot[5]}}, v[2] = {tot[7], tot[8]}, x2[2];
+      solve<2>(m, v, x2);
+      sol[1] = x2[0];
+      sol[2] = x2[1];
+    }
+    for (int k = 0; k < 3; k++) st.vc[k] = sol[k];
+  }
+}
+
+// Phase 2, one CTA per unit (128 threads): the second (horizontal) and
+// third (vertical) Wiener passes, whose terms are real-valued, so each of
+// their sums runs in the reference's sample order: warps 1-3 produce a row's
+// terms into shared memory (two buffers) while lane q of warp 0 adds
+// accumulator q's terms (m00 m01 m02 m11 m12 m22 v0 v1 v2). Then the solves,
+// the quantised coefficients (encoder/lr.rs:316-327) and the filter's error.
+__global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearchDesc d) {
+  extern __shared__ __align__(16) uint8_t lrs_smem[];
+  __shared__ int64_t red[4];
+  __shared__ double s_m[3][3], s_v[3], s_other[3];
+  __shared__ int s_coef[2][3];
+  const LrSearchJob job = d.jobs[blockIdx.x];
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const int lane = tid & 31, warp = tid >> 5;
+  const Smem sm = smem_of(lrs_smem, d);
+  const Win W{sm.win, sm.ws};
+  const LrSearchRect* rects = d.rects + job.r0;
+  LrJobState& st = d.state[blockIdx.x];
+  const int first = p == 0 ? 0 : 1;
+  const int bd = d.bd, maxv = (1 << bd) - 1;
+  double vc[3] = {st.vc[0], st.vc[1], st.vc[2]}, hc[3] = {0.0, 0.0, 0.0};
+  const int nci = (w + step - 1) / step;
+  const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
+  const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
+  const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
+  double* terms = reinterpret_cast<double*>(sm.region);  // [2][4][wmax]: d0 d1 d2 t
+  for (int iter = 1; iter < 3; iter++) {
+    const bool vertical = iter == 2;
+    if (tid < 3) s_other[tid] = vertical ? hc[tid] : vc[tid];
+    double macc = 0.0;
+    for (int ri = 0; ri < job.nr; ri++) {
+      const LrSearchRect rc = rects[ri];
+      __syncthreads();
+      stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+      __syncthreads();
+      const int nri = (rc.h + step - 1) / step;
+      for (int rr = 0; rr <= nri; rr++) {
+        if (rr < nri && warp > 0) {
+          double* tb = terms + (rr & 1) * 4 * d.wmax;
+          const int i = rr * step;
+          for (int jj = tid - 32; jj < nci; jj += blockDim.x - 32) {
+            const int j = jj * step;
+            double line[7];
+            wiener_line(W, vertical, i, j, s_other, line);
+            const double two3 = __dmul_rn(2.0, line[3]);
+            tb[0 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
+            tb[1 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
+            tb[2 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
+            tb[3 * d.wmax + jj] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
           }
-          if (rr > 0 && owner) {
-            const double* tb = terms + ((rr - 1) & 1) * 4 * d.wmax;
-            for (int jj = 0; jj < nci; jj++)
-              macc = __dadd_rn(macc, __dmul_rn(tb[qa * d.wmax + jj], tb[qb * d.wmax + jj]));
-          }
-          __syncthreads();
         }
+        if (rr > 0 && owner) {
+          const double* tb = terms + ((rr - 1) & 1) * 4 * d.wmax;
+          const double* ta = tb + qa * d.wmax;
+          const double* tq = tb + qb * d.wmax;
+          for (int jj = 0; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
+        }
+        __syncthreads();
       }
-      if (owner) {
-        if (qb == 3)
-          s_v[qa] = macc;
-        else
-          s_m[qa][qb] = s_m[qb][qa] = macc;
-      }
+    }
+    if (owner) {
+      if (qb == 3)
+        s_v[qa] = macc;
+      else
+        s_m[qa][qb] = s_m[qb][qa] = macc;
     }
     __syncthreads();
     if (tid == 0) {
@@ -417,224 +509,318 @@ __global__ void __launch_bounds__(kThreads) lr_search_kernel(const LrSearchDesc 
         sol[1] = x2[0];
         sol[2] = x2[1];
       }
-      for (int k = 0; k < 3; k++) (vertical ? s_vc : s_hc)[k] = sol[k];
+      for (int k = 0; k < 3; k++) s_other[k] = sol[k];  // the pass's solution
     }
+    __syncthreads();
+    for (int k = 0; k < 3; k++) (vertical ? vc : hc)[k] = s_other[k];
     __syncthreads();
   }
   if (tid == 0) {
     for (int k = 0; k < 3; k++) {
-      s_coef[0][k] = k < first ? 0 : min(max(f64_to_i32(round(s_vc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
-      s_coef[1][k] = k < first ? 0 : min(max(f64_to_i32(round(s_hc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
+      s_coef[0][k] = k < first ? 0 : min(max(f64_to_i32(round(vc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
+      s_coef[1][k] = k < first ? 0 : min(max(f64_to_i32(round(hc[k] * 128.0)), kWienerMin[k]), kWienerMax[k]);
     }
   }
   __syncthreads();
-  // --- the Wiener filter's error (postfilter.rs:781-822 restoration) ---
-  {
-    int vf[7], hf[7];
-    vf[3] = hf[3] = 128;
-    for (int k = 0; k < 3; k++) {
-      vf[k] = vf[6 - k] = s_coef[0][k];
-      hf[k] = hf[6 - k] = s_coef[1][k];
-      vf[3] -= 2 * s_coef[0][k];
-      hf[3] -= 2 * s_coef[1][k];
+  // the Wiener filter's error (postfilter.rs:781-822 restoration)
+  int vf[7], hf[7];
+  vf[3] = hf[3] = 128;
+  for (int k = 0; k < 3; k++) {
+    vf[k] = vf[6 - k] = s_coef[0][k];
+    hf[k] = hf[6 - k] = s_coef[1][k];
+    vf[3] -= 2 * s_coef[0][k];
+    hf[3] -= 2 * s_coef[1][k];
+  }
+  const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
+  const int off = 1 << (bd + 7 - round0 - 1), lim = (1 << (bd + 1 + 7 - round0)) - 1;
+  int64_t acc = 0;
+  for (int ri = 0; ri < job.nr; ri++) {
+    const LrSearchRect rc = rects[ri];
+    __syncthreads();
+    stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+    __syncthreads();
+    for (int k = tid; k < rc.h * w; k += blockDim.x) {
+      const int i = k / w, j = k - i * w;
+      const int e = wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+      acc += int64_t(e) * e;
     }
-    const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
-    const int off = 1 << (bd + 7 - round0 - 1), lim = (1 << (bd + 1 + 7 - round0)) - 1;
-    acc = 0;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    st.wiener = uint64_t(red[0] + red[1] + red[2] + red[3]);
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 3; b++) st.coef[a][b] = s_coef[a][b];
+  }
+}
+
+// The self-guided fit's f64 sums in the reference's sample order, on one
+// thread (rare: very large units with large errors at 12 bits, where the
+// exact integer sums could round differently); the thread rebuilds each
+// rectangle's window itself.
+__device__ __noinline__ void sgr_fit_in_order(const LrSearchDesc& d, const LrSearchJob& job, const LrSearchRect* rects,
+                                              const Win& W, const Smem& sm, const SgrPass& q0, const SgrPass& q1,
+                                              double& m00, double& m01, double& m11, double& v0, double& v1) {
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, step = d.step, bd = d.bd;
+  const int r0 = q0.r, r1 = q1.r;
+  m00 = m01 = m11 = v0 = v1 = 0.0;
+  for (int ri = 0; ri < job.nr; ri++) {
+    const LrSearchRect rc = rects[ri];
+    const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
+    for (int k = 0; k < ww * wh; k++) {
+      const int rr = k / ww, c = k - rr * ww;
+      const int x = max(min(x0 + c - kB, d.pex[p]), 0), y = max(min(rc.y0 + rr - kB, d.pey[p]), 0);
+      sm.win[rr * sm.ws + c] = int16_t(y < rc.ss   ? ld(d.cur[p], sb, x, max(rc.ss - 2, y))
+                                       : y > rc.se ? ld(d.cur[p], sb, x, min(rc.se + 2, y))
+                                                   : ld(d.cdef[p], sb, x, y));
+    }
+    for (int i = 0; i < rc.h; i += step)
+      for (int j = 0; j < w; j += step) {
+        const int yabs = rc.y0 + i;
+        const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
+        const double u = double(cval << 4);
+        const double a = r0 ? __dsub_rn(double(sgr_flt_direct(W, 0, q0, bd, yabs, i, j, cval)), u) : 0.0;
+        const double b = r1 ? __dsub_rn(double(sgr_flt_direct(W, 1, q1, bd, yabs, i, j, cval)), u) : 0.0;
+        const double t = __dmul_rn(128.0, __dsub_rn(double(ld(d.src[p], sb, x0 + j, yabs) << 4), u));
+        m00 = __dadd_rn(m00, __dmul_rn(a, a));
+        m01 = __dadd_rn(m01, __dmul_rn(a, b));
+        m11 = __dadd_rn(m11, __dmul_rn(b, b));
+        v0 = __dadd_rn(v0, __dmul_rn(a, t));
+        v1 = __dadd_rn(v1, __dmul_rn(b, t));
+      }
+  }
+}
+
+// Phase 3, one CTA per (unit, parameter set) (256 threads): the self-guided
+// fit (encoder/lr.rs:330-430) — the two box filters in bands of rows, the
+// fit's sums exact in int64 under the 2^53 magnitude bound (else in order
+// on one thread), the projection weights — and the restoration's error.
+__global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSearchDesc d) {
+  extern __shared__ __align__(16) uint8_t lrs_smem[];
+  __shared__ int64_t red[kThreads / 32];
+  __shared__ int s_xqd[2];
+  const int ji = blockIdx.x / d.nsets, si = blockIdx.x - ji * d.nsets;
+  const LrSearchJob job = d.jobs[ji];
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const Smem sm = smem_of(lrs_smem, d);
+  const Win W{sm.win, sm.ws};
+  const LrSearchRect* rects = d.rects + job.r0;
+  const int bd = d.bd, maxv = (1 << bd) - 1;
+  const int set = d.sets[si];
+  const SgrPass q0 = sgr_pass(set, 0), q1 = sgr_pass(set, 1);
+  const int r0 = q0.r, r1 = q1.r;
+  const int aw = d.wmax + 2, band = d.band;
+  int32_t* Ab[2];
+  int32_t* Bb[2];
+  int32_t* reg = reinterpret_cast<int32_t*>(sm.region);
+  for (int q = 0; q < 2; q++) {
+    Ab[q] = reg + (2 * q) * (band + 2) * aw;
+    Bb[q] = reg + (2 * q + 1) * (band + 2) * aw;
+  }
+  int32_t* hs = reg + 4 * (band + 2) * aw;
+  int32_t* hq = hs + (band + 6) * aw;
+  int32_t* cache = hq + (band + 6) * aw;  // [px][2] filter outputs of the unit
+  int upx = 0;
+  for (int ri = 0; ri < job.nr; ri++) upx += rects[ri].h * w;
+  const bool cached = upx <= d.cache_px;
+  int64_t f00 = 0, f01 = 0, f11 = 0, g0 = 0, g1 = 0, acc = 0;
+  uint64_t b01 = 0, bg0 = 0, bg1 = 0;
+  for (int pass_sse = 0; pass_sse < 2; pass_sse++) {
+    // pass_sse 0: the fit; 1: the error with the quantised weights
+    int pw0 = 0, pw1 = 0, pw2 = 0;
+    if (pass_sse == 1) {
+      pw0 = s_xqd[0];
+      pw1 = s_xqd[1];
+      pw2 = (1 << 7) - pw0 - pw1;
+    }
+    if (pass_sse == 1 && cached) {
+      // the fit pass kept every filter output
+      int off = 0;
+      for (int ri = 0; ri < job.nr; ri++) {
+        const LrSearchRect rc = rects[ri];
+        for (int k = tid; k < rc.h * w; k += blockDim.x) {
+          const int i = k / w, j = k - i * w;
+          const int u = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) << 4;
+          const int fl0 = cache[2 * (off + k)], fl1 = cache[2 * (off + k) + 1];
+          int32_t val = pw1 * u;
+          val += r0 ? pw0 * fl0 : pw0 * u;
+          val += r1 ? pw2 * fl1 : pw2 * u;
+          const int out = min(max(round2(val, 4 + 7), 0), maxv);
+          const int e = out - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+          acc += int64_t(e) * e;
+        }
+        off += rc.h * w;
+      }
+      break;
+    }
+    int off = 0;
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      stage_window(d, p, rc, x0, w, win, ws);
-      __syncthreads();
-      for (int k = tid; k < rc.h * w; k += blockDim.x) {
-        const int i = k / w, j = k - i * w;
-        const int e = wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) -
-                      ld(d.src[p], sb, x0 + j, rc.y0 + i);
-        acc += int64_t(e) * e;
+      stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+      for (int i0 = 0; i0 < rc.h; i0 += band) {
+        const int rows = min(band, rc.h - i0);
+        __syncthreads();
+        if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw, hs, hq);
+        if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw, hs, hq);
+        __syncthreads();
+        for (int k = tid; k < rows * w; k += blockDim.x) {
+          const int ir = k / w, j = k - ir * w;
+          const int i = i0 + ir, yabs = rc.y0 + i;
+          const bool fit_px = (i % step) == 0 && (j % step) == 0;
+          if (pass_sse == 0 && !fit_px && !cached) continue;
+          const int cval = W.at(i + kB, j + kB);  // the rectangle's rows lie in its stripe: CDEF output
+          const int u = cval << 4;  // SGRPROJ_RST_BITS
+          const int fl0 = r0 ? sgr_flt(0, yabs, ir, j, Ab[0], Bb[0], aw, cval) : 0;
+          const int fl1 = r1 ? sgr_flt(1, yabs, ir, j, Ab[1], Bb[1], aw, cval) : 0;
+          if (pass_sse == 0 && cached) {
+            cache[2 * (off + i * w + j)] = fl0;
+            cache[2 * (off + i * w + j) + 1] = fl1;
+          }
+          if (pass_sse == 0 && !fit_px) continue;
+          const int sv = ld(d.src[p], sb, x0 + j, yabs);
+          if (pass_sse == 0) {
+            const int64_t a = r0 ? int64_t(fl0 - u) : 0, b = r1 ? int64_t(fl1 - u) : 0;
+            const int64_t t = 128 * (int64_t(sv << 4) - u);
+            f00 += a * a;
+            f01 += a * b;
+            f11 += b * b;
+            g0 += a * t;
+            g1 += b * t;
+            b01 += uint64_t(llabs(a * b));
+            bg0 += uint64_t(llabs(a * t));
+            bg1 += uint64_t(llabs(b * t));
+          } else {
+            int32_t val = pw1 * u;
+            val += r0 ? pw0 * fl0 : pw0 * u;
+            val += r1 ? pw2 * fl1 : pw2 * u;
+            const int out = min(max(round2(val, 4 + 7), 0), maxv);
+            const int e = out - sv;
+            acc += int64_t(e) * e;
+          }
+        }
       }
+      off += rc.h * w;
     }
-    const uint64_t e = uint64_t(block_sum_i64(acc, red));
+    if (pass_sse == 1) break;
+    const int64_t t00 = block_sum_i64(f00, red), t01 = block_sum_i64(f01, red), t11 = block_sum_i64(f11, red);
+    const int64_t tg0 = block_sum_i64(g0, red), tg1 = block_sum_i64(g1, red);
+    // each f64 partial sum is exact (so any order gives the reference's sums)
+    // while the terms' magnitudes sum below 2^53
+    const uint64_t sb01 = uint64_t(block_sum_i64(int64_t(b01), red));
+    const uint64_t sbg0 = uint64_t(block_sum_i64(int64_t(bg0), red));
+    const uint64_t sbg1 = uint64_t(block_sum_i64(int64_t(bg1), red));
+    const bool exact = uint64_t(t00) < kExact && uint64_t(t11) < kExact && sb01 < kExact && sbg0 < kExact &&
+                       sbg1 < kExact;
     if (tid == 0) {
-      const double cost = __dadd_rn(__ull2double_rn(e), __dmul_rn(d.lambda, p == 0 ? 40.0 : 28.0));
-      if (cost < s_best_cost) {
-        s_best_cost = cost;
-        s_best = av1pf_lr_unit{};
-        s_best.type = AV1PF_RESTORE_WIENER;
-        for (int a = 0; a < 2; a++)
-          for (int b = 0; b < 3; b++) s_best.wiener[a][b] = int8_t(s_coef[a][b]);
+      double m00, m01, m11, v0, v1;
+      if (exact) {
+        m00 = double(t00);
+        m01 = double(t01);
+        m11 = double(t11);
+        v0 = double(tg0);
+        v1 = double(tg1);
+      } else {
+        sgr_fit_in_order(d, job, rects, W, sm, q0, q1, m00, m01, m11, v0, v1);
       }
+      double w0, w2;
+      if (r0 && r1) {
+        double m[2][2] = {{m00, m01}, {m01, m11}}, v[2] = {v0, v1}, x2[2];
+        solve<2>(m, v, x2);
+        w0 = x2[0];
+        w2 = x2[1];
+      } else if (r0) {
+        w0 = m00 > 0.0 ? __ddiv_rn(v0, m00) : 0.0;
+        w2 = 0.0;
+      } else {
+        w0 = 0.0;
+        w2 = m11 > 0.0 ? __ddiv_rn(v1, m11) : 0.0;
+      }
+      const int x0q = r0 ? min(max(f64_to_i32(round(w0)), kXqdMin[0]), kXqdMax[0]) : 0;
+      int x1q;
+      if (r1) {
+        // i32 arithmetic wraps as the reference's release build does
+        const int diff = int(uint32_t(1 << 7) - uint32_t(x0q) - uint32_t(f64_to_i32(round(w2))));
+        x1q = min(max(diff, kXqdMin[1]), kXqdMax[1]);
+      } else {
+        x1q = min(max((1 << 7) - x0q, kXqdMin[1]), kXqdMax[1]);
+      }
+      s_xqd[0] = x0q;
+      s_xqd[1] = x1q;
     }
     __syncthreads();
   }
+  const int64_t e = block_sum_i64(acc, red);
+  if (tid == 0) {
+    LrSgrResult& r = d.sgr[blockIdx.x];
+    r.xqd[0] = s_xqd[0];
+    r.xqd[1] = s_xqd[1];
+    r.sse = uint64_t(e);
+  }
+}
 
-  // --- self-guided fits (encoder/lr.rs:330-430), one parameter set at a time ---
-  int32_t* Ab[2];
-  int32_t* Bb[2];
-  const int aw = d.wmax + 2;
-  for (int q = 0; q < 2; q++) {
-    Ab[q] = reinterpret_cast<int32_t*>(region) + (2 * q) * (kBand + 2) * aw;
-    Bb[q] = reinterpret_cast<int32_t*>(region) + (2 * q + 1) * (kBand + 2) * aw;
+// Phase 4, one thread per unit: the cheapest of no filter (error + lambda),
+// the Wiener filter (+ 40 or 28 lambda) and each self-guided set in order
+// (+ 20 lambda), the first on ties (encoder/lr.rs:147-186).
+__global__ void lr_search_choose_kernel(const LrSearchDesc d, int njobs) {
+  const int ji = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ji >= njobs) return;
+  const LrJobState& st = d.state[ji];
+  const int p = d.jobs[ji].plane;
+  av1pf_lr_unit best{};
+  double best_cost = __dadd_rn(__ull2double_rn(st.none), d.lambda);
+  double cost = __dadd_rn(__ull2double_rn(st.wiener), __dmul_rn(d.lambda, p == 0 ? 40.0 : 28.0));
+  if (cost < best_cost) {
+    best_cost = cost;
+    best.type = AV1PF_RESTORE_WIENER;
+    for (int a = 0; a < 2; a++)
+      for (int b = 0; b < 3; b++) best.wiener[a][b] = int8_t(st.coef[a][b]);
   }
   for (int si = 0; si < d.nsets; si++) {
-    const int set = d.sets[si];
-    const SgrPass q0 = sgr_pass(set, 0), q1 = sgr_pass(set, 1);
-    const int r0 = q0.r, r1 = q1.r;
-    // fit sums, exact in int64, with the magnitudes' sums to check exactness
-    int64_t f00 = 0, f01 = 0, f11 = 0, g0 = 0, g1 = 0;
-    uint64_t b01 = 0, bg0 = 0, bg1 = 0;
-    for (int pass_sse = 0; pass_sse < 2; pass_sse++) {
-      // pass_sse 0: the fit; 1: the error with the quantised weights
-      int pw0 = 0, pw1 = 0, pw2 = 0;
-      if (pass_sse == 1) {
-        pw0 = s_xqd[0];
-        pw1 = s_xqd[1];
-        pw2 = (1 << 7) - pw0 - pw1;
-      }
-      acc = 0;
-      for (int ri = 0; ri < job.nr; ri++) {
-        const LrSearchRect rc = rects[ri];
-        __syncthreads();
-        stage_window(d, p, rc, x0, w, win, ws);
-        for (int i0 = 0; i0 < rc.h; i0 += kBand) {
-          const int rows = min(kBand, rc.h - i0);
-          __syncthreads();
-          if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw);
-          if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw);
-          __syncthreads();
-          for (int k = tid; k < rows * w; k += blockDim.x) {
-            const int ir = k / w, j = k - ir * w;
-            const int i = i0 + ir, yabs = rc.y0 + i;
-            if (pass_sse == 0 && ((i % step) != 0 || (j % step) != 0)) continue;
-            const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
-            const int u = cval << 4;  // SGRPROJ_RST_BITS
-            const int fl0 = r0 ? sgr_flt(0, yabs, ir, j, Ab[0], Bb[0], aw, cval) : 0;
-            const int fl1 = r1 ? sgr_flt(1, yabs, ir, j, Ab[1], Bb[1], aw, cval) : 0;
-            const int sv = ld(d.src[p], sb, x0 + j, yabs);
-            if (pass_sse == 0) {
-              const int64_t a = r0 ? int64_t(fl0 - u) : 0, b = r1 ? int64_t(fl1 - u) : 0;
-              const int64_t t = 128 * (int64_t(sv << 4) - u);
-              f00 += a * a;
-              f01 += a * b;
-              f11 += b * b;
-              g0 += a * t;
-              g1 += b * t;
-              b01 += uint64_t(llabs(a * b));
-              bg0 += uint64_t(llabs(a * t));
-              bg1 += uint64_t(llabs(b * t));
-            } else {
-              int32_t val = pw1 * u;
-              val += r0 ? pw0 * fl0 : pw0 * u;
-              val += r1 ? pw2 * fl1 : pw2 * u;
-              const int out = min(max(round2(val, 4 + 7), 0), maxv);
-              const int e = out - sv;
-              acc += int64_t(e) * e;
-            }
-          }
-        }
-      }
-      if (pass_sse == 0) {
-        const int64_t t00 = block_sum_i64(f00, red), t01 = block_sum_i64(f01, red), t11 = block_sum_i64(f11, red);
-        const int64_t tg0 = block_sum_i64(g0, red), tg1 = block_sum_i64(g1, red);
-        // each f64 partial sum is exact (so any order gives the reference's
-        // sums) while the terms' magnitudes sum below 2^53
-        const uint64_t m00abs = uint64_t(t00), m11abs = uint64_t(t11);
-        const uint64_t sb01 = uint64_t(block_sum_i64(int64_t(b01), red));
-        const uint64_t sbg0 = uint64_t(block_sum_i64(int64_t(bg0), red));
-        const uint64_t sbg1 = uint64_t(block_sum_i64(int64_t(bg1), red));
-        const bool exact = m00abs < kExact && m11abs < kExact && sb01 < kExact && sbg0 < kExact && sbg1 < kExact;
-        if (tid == 0) {
-          double m00, m01, m11, v0, v1;
-          if (exact) {
-            m00 = double(t00);
-            m01 = double(t01);
-            m11 = double(t11);
-            v0 = double(tg0);
-            v1 = double(tg1);
-          } else {
-            // the reference's f64 sums in sample order (rare: very large units
-            // with large errors at 12 bits)
-            m00 = m01 = m11 = v0 = v1 = 0.0;
-            for (int ri = 0; ri < job.nr; ri++) {
-              const LrSearchRect rc = rects[ri];
-              // the window of this rectangle is rebuilt by this thread alone
-              const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
-              for (int k = 0; k < ww * wh; k++) {
-                const int rr = k / ww, c = k - rr * ww;
-                const int x = max(min(x0 + c - kB, d.pex[p]), 0), y = max(min(rc.y0 + rr - kB, d.pey[p]), 0);
-                win[rr * ws + c] = int16_t(y < rc.ss   ? ld(d.cur[p], sb, x, max(rc.ss - 2, y))
-                                           : y > rc.se ? ld(d.cur[p], sb, x, min(rc.se + 2, y))
-                                                       : ld(d.cdef[p], sb, x, y));
-              }
-              for (int i = 0; i < rc.h; i += step)
-                for (int j = 0; j < w; j += step) {
-                  const int yabs = rc.y0 + i;
-                  const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
-                  const double u = double(cval << 4);
-                  const double a = r0 ? __dsub_rn(double(sgr_flt_direct(W, 0, q0, bd, yabs, i, j, cval)), u) : 0.0;
-                  const double b = r1 ? __dsub_rn(double(sgr_flt_direct(W, 1, q1, bd, yabs, i, j, cval)), u) : 0.0;
-                  const double t = __dmul_rn(128.0, __dsub_rn(double(ld(d.src[p], sb, x0 + j, yabs) << 4), u));
-                  m00 = __dadd_rn(m00, __dmul_rn(a, a));
-                  m01 = __dadd_rn(m01, __dmul_rn(a, b));
-                  m11 = __dadd_rn(m11, __dmul_rn(b, b));
-                  v0 = __dadd_rn(v0, __dmul_rn(a, t));
-                  v1 = __dadd_rn(v1, __dmul_rn(b, t));
-                }
-            }
-          }
-          double w0, w2;
-          if (r0 && r1) {
-            double m[2][2] = {{m00, m01}, {m01, m11}}, v[2] = {v0, v1}, x2[2];
-            solve<2>(m, v, x2);
-            w0 = x2[0];
-            w2 = x2[1];
-          } else if (r0) {
-            w0 = m00 > 0.0 ? __ddiv_rn(v0, m00) : 0.0;
-            w2 = 0.0;
-          } else {
-            w0 = 0.0;
-            w2 = m11 > 0.0 ? __ddiv_rn(v1, m11) : 0.0;
-          }
-          const int x0q = r0 ? min(max(f64_to_i32(round(w0)), kXqdMin[0]), kXqdMax[0]) : 0;
-          int x1q;
-          if (r1) {
-            // i32 arithmetic wraps as the reference's release build does
-            const int diff = int(uint32_t(1 << 7) - uint32_t(x0q) - uint32_t(f64_to_i32(round(w2))));
-            x1q = min(max(diff, kXqdMin[1]), kXqdMax[1]);
-          } else {
-            x1q = min(max((1 << 7) - x0q, kXqdMin[1]), kXqdMax[1]);
-          }
-          s_xqd[0] = x0q;
-          s_xqd[1] = x1q;
-        }
-        __syncthreads();
-      } else {
-        const uint64_t e = uint64_t(block_sum_i64(acc, red));
-        if (tid == 0) {
-          const double cost = __dadd_rn(__ull2double_rn(e), __dmul_rn(d.lambda, 20.0));
-          if (cost < s_best_cost) {
-            s_best_cost = cost;
-            s_best = av1pf_lr_unit{};
-            s_best.type = AV1PF_RESTORE_SGRPROJ;
-            s_best.sgr_set = uint8_t(set);
-            s_best.sgr_xqd[0] = int8_t(s_xqd[0]);
-            s_best.sgr_xqd[1] = int8_t(s_xqd[1]);
-          }
-        }
-        __syncthreads();
-      }
+    const LrSgrResult& r = d.sgr[ji * d.nsets + si];
+    cost = __dadd_rn(__ull2double_rn(r.sse), __dmul_rn(d.lambda, 20.0));
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = av1pf_lr_unit{};
+      best.type = AV1PF_RESTORE_SGRPROJ;
+      best.sgr_set = uint8_t(d.sets[si]);
+      best.sgr_xqd[0] = int8_t(r.xqd[0]);
+      best.sgr_xqd[1] = int8_t(r.xqd[1]);
     }
   }
-  if (tid == 0) d.out[blockIdx.x] = s_best;
+  d.out[ji] = best;
 }
 
-cudaError_t lr_search_init(size_t smem) {
-  return cudaFuncSetAttribute(lr_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px) {
+  cudaError_t e = cudaFuncSetAttribute(lr_search_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(lr_search_smem(wmax, hmax, 0, band, cache_px)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(lr_search_wiener_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(lr_search_smem(wmax, hmax, 1, band, cache_px)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(lr_search_sgr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(lr_search_smem(wmax, hmax, 2, band, cache_px)));
+  return e;
 }
 
-void launch_lr_search(const LrSearchDesc& d, int njobs, size_t smem, cudaStream_t s) {
+void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
+                      cudaEvent_t join) {
   if (njobs <= 0) return;
-  lr_search_kernel<<<njobs, kThreads, smem, s>>>(d);
-  note_launch();
+  const size_t s0 = lr_search_smem(d.wmax, d.hmax, 0, d.band, d.cache_px);
+  const size_t s1 = lr_search_smem(d.wmax, d.hmax, 1, d.band, d.cache_px);
+  const size_t s2 = lr_search_smem(d.wmax, d.hmax, 2, d.band, d.cache_px);
+  // the self-guided fits depend on nothing else: they run beside the Wiener passes
+  cudaEventRecord(fork, s);
+  cudaStreamWaitEvent(side, fork, 0);
+  lr_search_sgr_kernel<<<njobs * d.nsets, kThreads, s2, side>>>(d);
+  lr_search_prep_kernel<<<njobs, kThreads, s0, s>>>(d);
+  lr_search_wiener_kernel<<<njobs, 128, s1, s>>>(d);
+  cudaEventRecord(join, side);
+  cudaStreamWaitEvent(s, join, 0);
+  lr_search_choose_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(d, njobs);
+  note_launch(4);
 }
 
 }  // namespace av1pf

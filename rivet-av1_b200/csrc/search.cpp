@@ -394,14 +394,22 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
   }
   std::vector<av1pf_lr_unit> chosen(jobs.size());
   if (!jobs.empty()) {
-    const size_t smem = lr_search_smem(d.wmax, d.hmax);
-    cudaError_t e = lr_search_init(smem);
+    int upx_max = 0;
+    for (const LrSearchJob& jb : jobs) {
+      int px = 0;
+      for (int r = 0; r < jb.nr; r++) px += rects[size_t(jb.r0 + r)].h * jb.w;
+      upx_max = std::max(upx_max, px);
+    }
+    lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px);
+    cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px);
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search attributes");
     const size_t jb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);
     const size_t ob = jobs.size() * sizeof(av1pf_lr_unit);
-    const size_t o_rects = align256(jb), o_out = o_rects + align256(rb), total = o_out + align256(ob);
+    const size_t stb = jobs.size() * sizeof(LrJobState), sgb = jobs.size() * size_t(d.nsets) * sizeof(LrSgrResult);
+    const size_t o_rects = align256(jb), o_out = o_rects + align256(rb), o_state = o_out + align256(ob);
+    const size_t o_sgr = o_state + align256(stb), total = o_sgr + align256(sgb);
     if ((rc = ctx->ensure(ctx->search_dev, total)) != AV1PF_OK) return rc;
-    if ((rc = ctx->ensure_host(ctx->search_host, total)) != AV1PF_OK) return rc;
+    if ((rc = ctx->ensure_host(ctx->search_host, o_state)) != AV1PF_OK) return rc;
     uint8_t* dv = static_cast<uint8_t*>(ctx->search_dev.ptr);
     uint8_t* hs = static_cast<uint8_t*>(ctx->search_host.ptr);
     std::memcpy(hs, jobs.data(), jb);
@@ -409,9 +417,11 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
     d.jobs = reinterpret_cast<const LrSearchJob*>(dv);
     d.rects = reinterpret_cast<const LrSearchRect*>(dv + o_rects);
     d.out = reinterpret_cast<av1pf_lr_unit*>(dv + o_out);
+    d.state = reinterpret_cast<LrJobState*>(dv + o_state);
+    d.sgr = reinterpret_cast<LrSgrResult*>(dv + o_sgr);
     e = cudaMemcpyAsync(dv, hs, o_out, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search upload");
-    launch_lr_search(d, int(jobs.size()), smem, s);
+    launch_lr_search(d, int(jobs.size()), s, ctx->side, ctx->fork, ctx->join);
     e = cudaMemcpyAsync(hs + o_out, dv + o_out, ob, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
