@@ -57,33 +57,38 @@ struct Win {
 };
 
 // lr_window (postfilter.rs:765-777) of rectangle `rc` into shared memory.
-__device__ __forceinline__ int window_sample(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int ww,
-                                             int k) {
-  const int r = k / ww, c = k - r * ww;
-  const int x = max(min(x0 + c - kB, d.pex[p]), 0);
-  const int y = max(min(rc.y0 + r - kB, d.pey[p]), 0);
-  if (y < rc.ss) return ld(d.cur[p], d.sb, x, max(rc.ss - 2, y));
-  if (y > rc.se) return ld(d.cur[p], d.sb, x, min(rc.se + 2, y));
-  return ld(d.cdef[p], d.sb, x, y);
-}
-
 __device__ void stage_window(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int w, int16_t* win,
-                             int ws) {
-  const int ww = w + 2 * kB, wh = rc.h + 2 * kB, n = ww * wh, nt = blockDim.x;
-  // four loads in flight per thread before their stores
-  for (int k0 = threadIdx.x; k0 < n; k0 += 4 * nt) {
-    int v[4];
+                             int ws, int16_t* srcw = nullptr) {
+  // a warp per window row, lanes along it (no index division), eight rows'
+  // loads in flight before their stores; with `srcw`, the rectangle's source
+  // samples too (row stride w)
+  constexpr int kR = 8;
+  const int ww = w + 2 * kB, wh = rc.h + 2 * kB, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  const int pex = d.pex[p], pey = d.pey[p];
+  const int rows_all = wh + (srcw ? rc.h : 0);
+  for (int r0 = threadIdx.x >> 5; r0 < rows_all; r0 += kR * nw) {
+    for (int c = lane; c < ww; c += 32) {
+      int v[kR];
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int k = k0 + m * nt;
-      v[m] = k < n ? window_sample(d, p, rc, x0, ww, k) : 0;
-    }
+      for (int m = 0; m < kR; m++) {
+        const int r = r0 + m * nw;
+        v[m] = 0;
+        if (r < wh) {
+          const int y = max(min(rc.y0 + r - kB, pey), 0);
+          const DPlane& pl = y < rc.ss || y > rc.se ? d.cur[p] : d.cdef[p];
+          const int yy = y < rc.ss ? max(rc.ss - 2, y) : (y > rc.se ? min(rc.se + 2, y) : y);
+          v[m] = ld(pl, d.sb, max(min(x0 + c - kB, pex), 0), yy);
+        } else if (r < rows_all && c < w) {
+          v[m] = ld(d.src[p], d.sb, x0 + c, rc.y0 + r - wh);
+        }
+      }
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int k = k0 + m * nt;
-      if (k < n) {
-        const int r = k / ww, c = k - r * ww;
-        win[r * ws + c] = int16_t(v[m]);
+      for (int m = 0; m < kR; m++) {
+        const int r = r0 + m * nw;
+        if (r < wh)
+          win[r * ws + c] = int16_t(v[m]);
+        else if (r < rows_all && c < w)
+          srcw[(r - wh) * w + c] = int16_t(v[m]);
       }
     }
   }
@@ -275,37 +280,42 @@ __device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, in
                             int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
   const int r = q.r, cw = w + 2;
   const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();  // the previous users of hs / hq are done
-  for (int k = threadIdx.x; k < nrow * cw; k += blockDim.x) {
-    const int rr = k / cw, aj = k - rr * cw;
-    const int wy = wy0 + rr, wx = aj + kB - 1;
-    int32_t sum = 0, sq = 0;
-    for (int dx = -r; dx <= r; dx++) {
-      const int v = W.at(wy, wx + dx);
-      sum += v;
-      sq += v * v;
+  for (int rr = warp; rr < nrow; rr += nw) {
+    const int wy = wy0 + rr;
+    for (int aj = lane; aj < cw; aj += 32) {
+      const int wx = aj + kB - 1;
+      int32_t sum = 0, sq = 0;
+      for (int dx = -r; dx <= r; dx++) {
+        const int v = W.at(wy, wx + dx);
+        sum += v;
+        sq += v * v;
+      }
+      hs[rr * cw + aj] = sum;
+      hq[rr * cw + aj] = sq;
     }
-    hs[k] = sum;
-    hq[k] = sq;
   }
   __syncthreads();
   const int sh = 2 * (bd - 8);
-  for (int k = threadIdx.x; k < (rows + 2) * cw; k += blockDim.x) {
-    const int ir = k / cw, aj = k - ir * cw;
+  for (int ir = warp; ir < rows + 2; ir += nw) {
     if (pass == 0 && ((y0 + i0 + ir - 1) & 1) == 0) continue;
-    int32_t bs = 0, as = 0;
-    for (int dy = 0; dy <= 2 * r; dy++) {
-      bs += hs[(ir + dy) * cw + aj];
-      as += hq[(ir + dy) * cw + aj];
+    for (int aj = lane; aj < cw; aj += 32) {
+      int32_t bs = 0, as = 0;
+      for (int dy = 0; dy <= 2 * r; dy++) {
+        bs += hs[(ir + dy) * cw + aj];
+        as += hq[(ir + dy) * cw + aj];
+      }
+      // a * n and dd^2 stay below 2^31 (25 * 25 * 255^2); p * s needs 64 bits
+      const int32_t a = round2(as, sh);
+      const int32_t dd = round2(bs, bd - 8);
+      const int32_t p = max(a * q.n - dd * dd, 0);
+      const int64_t z = (int64_t(p) * q.s + (int64_t(1) << 19)) >> 20;  // SGRPROJ_MTABLE_BITS
+      const int32_t a2 = g_lrs_a2.v[z < 255 ? int(z) : 255];
+      const int64_t b2 = int64_t((256 - a2) * bs) * q.one_over_n;
+      Ab[ir * aw + aj] = a2;
+      Bb[ir * aw + aj] = int32_t((b2 + (1 << 11)) >> 12);  // SGRPROJ_RECIP_BITS
     }
-    const int32_t a = round2(as, sh);
-    const int32_t dd = round2(bs, bd - 8);
-    const int64_t p = max(int64_t(a) * q.n - int64_t(dd) * dd, int64_t(0));
-    const int64_t z = round2_64(p * q.s, 20);  // SGRPROJ_MTABLE_BITS
-    const int32_t a2 = g_lrs_a2.v[int(min(z, int64_t(255)))];
-    const int64_t b2 = int64_t((256 - a2) * bs) * int64_t(q.one_over_n);
-    Ab[ir * aw + aj] = a2;
-    Bb[ir * aw + aj] = int32_t(round2_64(b2, 12));  // SGRPROJ_RECIP_BITS
   }
 }
 
@@ -320,10 +330,11 @@ size_t lr_window_bytes(int wmax, int hmax) {
 size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px) {
   const size_t win = lr_window_bytes(wmax, hmax);
   if (kind == 0) return win;                                                   // prep
-  if (kind == 1) return win + size_t(2) * 4 * size_t(wmax) * sizeof(double);  // Wiener passes
+  if (kind == 1) return win + size_t(2) * 4 * size_t(wmax + 1) * sizeof(double);  // Wiener passes
   // self-guided: A/B of both passes, the band's box sums, the filter-output cache
   return win + size_t(4) * (band + 2) * size_t(wmax + 2) * sizeof(int32_t) +
-         size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) + size_t(cache_px) * 2 * sizeof(int32_t);
+         size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) + size_t(cache_px) * 2 * sizeof(int32_t) +
+         ((size_t(hmax) * size_t(wmax) * sizeof(int16_t) + 15) & ~size_t(15));
 }
 
 void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px) {
@@ -373,11 +384,11 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
   int64_t acc = 0;
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
-    for (int k = tid; k < rc.h * w; k += blockDim.x) {
-      const int i = k / w, j = k - i * w;
-      const int e = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
-      acc += int64_t(e) * e;
-    }
+    for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
+      for (int j = tid & 31; j < w; j += 32) {
+        const int e = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+        acc += int64_t(e) * e;
+      }
   }
   const int64_t none = block_sum_i64(acc, red);
   int64_t m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
@@ -452,7 +463,10 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
   const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
   const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
-  double* terms = reinterpret_cast<double*>(sm.region);  // [2][4][wmax]: d0 d1 d2 t
+  // [2][4][wmax + 1]: d0 d1 d2 t (the odd row stride puts the four terms of
+  // a sample on different banks for the accumulating lanes)
+  double* terms = reinterpret_cast<double*>(sm.region);
+  const int ts = d.wmax + 1;
   for (int iter = 1; iter < 3; iter++) {
     const bool vertical = iter == 2;
     if (tid < 3) s_other[tid] = vertical ? hc[tid] : vc[tid];
@@ -465,23 +479,23 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
       const int nri = (rc.h + step - 1) / step;
       for (int rr = 0; rr <= nri; rr++) {
         if (rr < nri && warp > 0) {
-          double* tb = terms + (rr & 1) * 4 * d.wmax;
+          double* tb = terms + (rr & 1) * 4 * ts;
           const int i = rr * step;
           for (int jj = tid - 32; jj < nci; jj += blockDim.x - 32) {
             const int j = jj * step;
             double line[7];
             wiener_line(W, vertical, i, j, s_other, line);
             const double two3 = __dmul_rn(2.0, line[3]);
-            tb[0 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
-            tb[1 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
-            tb[2 * d.wmax + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
-            tb[3 * d.wmax + jj] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
+            tb[0 * ts + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
+            tb[1 * ts + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
+            tb[2 * ts + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
+            tb[3 * ts + jj] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
           }
         }
         if (rr > 0 && owner) {
-          const double* tb = terms + ((rr - 1) & 1) * 4 * d.wmax;
-          const double* ta = tb + qa * d.wmax;
-          const double* tq = tb + qb * d.wmax;
+          const double* tb = terms + ((rr - 1) & 1) * 4 * ts;
+          const double* ta = tb + qa * ts;
+          const double* tq = tb + qb * ts;
           for (int jj = 0; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
         }
         __syncthreads();
@@ -539,11 +553,12 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
     __syncthreads();
     stage_window(d, p, rc, x0, w, sm.win, sm.ws);
     __syncthreads();
-    for (int k = tid; k < rc.h * w; k += blockDim.x) {
-      const int i = k / w, j = k - i * w;
-      const int e = wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
-      acc += int64_t(e) * e;
-    }
+    for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
+      for (int j = tid & 31; j < w; j += 32) {
+        const int e =
+            wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+        acc += int64_t(e) * e;
+      }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -622,6 +637,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
   int32_t* hs = reg + 4 * (band + 2) * aw;
   int32_t* hq = hs + (band + 6) * aw;
   int32_t* cache = hq + (band + 6) * aw;  // [px][2] filter outputs of the unit
+  int16_t* srcw = reinterpret_cast<int16_t*>(cache + 2 * d.cache_px);  // the rectangle's source samples
   int upx = 0;
   for (int ri = 0; ri < job.nr; ri++) upx += rects[ri].h * w;
   const bool cached = upx <= d.cache_px;
@@ -640,17 +656,19 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
       int off = 0;
       for (int ri = 0; ri < job.nr; ri++) {
         const LrSearchRect rc = rects[ri];
-        for (int k = tid; k < rc.h * w; k += blockDim.x) {
-          const int i = k / w, j = k - i * w;
-          const int u = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) << 4;
+        for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
+          for (int j = tid & 31; j < w; j += 32) {
+          const int k = i * w + j;
+          // one rectangle: its window and source are still staged
+          const int u = (job.nr == 1 ? W.at(i + kB, j + kB) : ld(d.cdef[p], sb, x0 + j, rc.y0 + i)) << 4;
           const int fl0 = cache[2 * (off + k)], fl1 = cache[2 * (off + k) + 1];
           int32_t val = pw1 * u;
           val += r0 ? pw0 * fl0 : pw0 * u;
           val += r1 ? pw2 * fl1 : pw2 * u;
           const int out = min(max(round2(val, 4 + 7), 0), maxv);
-          const int e = out - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+          const int e = out - (job.nr == 1 ? srcw[k] : ld(d.src[p], sb, x0 + j, rc.y0 + i));
           acc += int64_t(e) * e;
-        }
+          }
         off += rc.h * w;
       }
       break;
@@ -659,15 +677,15 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+      stage_window(d, p, rc, x0, w, sm.win, sm.ws, srcw);
       for (int i0 = 0; i0 < rc.h; i0 += band) {
         const int rows = min(band, rc.h - i0);
         __syncthreads();
         if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw, hs, hq);
         if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw, hs, hq);
         __syncthreads();
-        for (int k = tid; k < rows * w; k += blockDim.x) {
-          const int ir = k / w, j = k - ir * w;
+        for (int ir = tid >> 5; ir < rows; ir += blockDim.x >> 5)
+          for (int j = tid & 31; j < w; j += 32) {
           const int i = i0 + ir, yabs = rc.y0 + i;
           const bool fit_px = (i % step) == 0 && (j % step) == 0;
           if (pass_sse == 0 && !fit_px && !cached) continue;
@@ -680,18 +698,20 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
             cache[2 * (off + i * w + j) + 1] = fl1;
           }
           if (pass_sse == 0 && !fit_px) continue;
-          const int sv = ld(d.src[p], sb, x0 + j, yabs);
+          const int sv = srcw[i * w + j];
           if (pass_sse == 0) {
-            const int64_t a = r0 ? int64_t(fl0 - u) : 0, b = r1 ? int64_t(fl1 - u) : 0;
-            const int64_t t = 128 * (int64_t(sv << 4) - u);
-            f00 += a * a;
-            f01 += a * b;
-            f11 += b * b;
-            g0 += a * t;
-            g1 += b * t;
-            b01 += uint64_t(llabs(a * b));
-            bg0 += uint64_t(llabs(a * t));
-            bg1 += uint64_t(llabs(b * t));
+            // |a|, |b| < 2^17 and |t| < 2^23: 32-bit operands, 64-bit products
+            const int32_t a = r0 ? fl0 - u : 0, b = r1 ? fl1 - u : 0;
+            const int32_t t = 128 * ((sv << 4) - u);
+            f00 += int64_t(a) * a;
+            f01 += int64_t(a) * b;
+            f11 += int64_t(b) * b;
+            g0 += int64_t(a) * t;
+            g1 += int64_t(b) * t;
+            const uint32_t ua = uint32_t(abs(a)), ub = uint32_t(abs(b)), ut = uint32_t(abs(t));
+            b01 += uint64_t(ua) * ub;
+            bg0 += uint64_t(ua) * ut;
+            bg1 += uint64_t(ub) * ut;
           } else {
             int32_t val = pw1 * u;
             val += r0 ? pw0 * fl0 : pw0 * u;
