@@ -254,6 +254,18 @@ int av1pf_output(av1pf_ctx* ctx, const av1pf_frame_info* info,
 /* Bytes av1pf_output writes for `info`. */
 size_t av1pf_frame_bytes(const av1pf_frame_info* info);
 
+/* The MD5 a conformance vector's .md5 file holds for a decoded frame
+ * (tests/common/mod.rs:101-119 `frame_md5`): MD5 (RFC 1321) of the packed
+ * frame as av1pf_output writes it (HOST memory, av1pf_frame_bytes bytes),
+ * followed for a monochrome frame by two neutral chroma planes
+ * (ceil(w/2) x ceil(h/2) samples of 1 << (bit_depth - 1), as a 4:2:0 file
+ * carries it). Writes 32 lowercase hex digits and a NUL. Runs on the host:
+ * MD5 is one serial chain of 64-byte blocks. */
+int av1pf_frame_md5(const av1pf_frame_info* info, const uint8_t* frame,
+                    char md5_hex[33]);
+/* MD5 (RFC 1321) of n host bytes, as 32 hex digits and a NUL. */
+int av1pf_md5(const uint8_t* data, size_t n, char md5_hex[33]);
+
 /* av1pf_output for callers that cannot allocate device memory — a decoder
  * embedded in a host whose device memory belongs to another allocator, or a
  * real-time output path that cannot take an allocation's latency or an

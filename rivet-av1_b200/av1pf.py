@@ -189,6 +189,8 @@ def lib():
              P(Plane), vp)
         _sig(L, "av1pf_output", C.c_int, vp, P(FrameInfo), P(Params), P(Plane), vp, vp)
         _sig(L, "av1pf_frame_bytes", C.c_size_t, P(FrameInfo))
+        _sig(L, "av1pf_frame_md5", C.c_int, P(FrameInfo), vp, C.c_char_p)
+        _sig(L, "av1pf_md5", C.c_int, vp, C.c_size_t, C.c_char_p)
         _sig(L, "av1pf_output_noalloc", C.c_int, P(FrameInfo), P(Params), P(Plane), vp, vp)
         _sig(L, "av1pf_chain", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp, vp)
         _sig(L, "av1pf_chain_host", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp)
@@ -313,6 +315,13 @@ def synth_search_planes(sf, seed, amp=None):
         noise = np.kron(blk, np.ones((4, 4), np.int64))[:h, :w] + fine
         cur.append(np.clip(arr.astype(np.int64) + noise, 0, hi).astype(arr.dtype))
     return cur, src
+
+
+def frame_md5(info, frame):
+    """av1pf_frame_md5 of a packed frame (numpy uint8 array)."""
+    out = C.create_string_buffer(33)
+    check(lib().av1pf_frame_md5(C.byref(info), frame.ctypes.data, out), "av1pf_frame_md5")
+    return out.value.decode()
 
 
 def frame_bytes(info):
