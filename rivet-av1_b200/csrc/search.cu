@@ -29,13 +29,16 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
   return v;
 }
 
-// The reference's f64 total of per-block minima, in block order (blocks that
-// code no index hold 0 everywhere and add nothing); Y == nullptr: of best[]
-// alone.
-__device__ double ordered_total(const uint64_t* best, const uint64_t* Y, const uint64_t* U, int nfb) {
+// The reference's f64 total, in block order, of min(best[b], last pair,
+// pair (Y, U)) over the blocks (blocks that code no index hold 0 everywhere
+// and add nothing). L / Y may be null (no last pair / no candidate).
+__device__ double ordered_total(const uint64_t* best, const uint64_t* YL, const uint64_t* UL, const uint64_t* Y,
+                                const uint64_t* U, int nfb) {
   double t = 0.0;
   for (int b = 0; b < nfb; b++) {
-    const uint64_t v = Y ? min(__ldcg(&best[b]), Y[b] + U[b]) : __ldcg(&best[b]);
+    uint64_t v = __ldcg(&best[b]);
+    if (YL) v = min(v, YL[b] + UL[b]);
+    if (Y) v = min(v, Y[b] + U[b]);
     t = __dadd_rn(t, double(v));
   }
   return t;
@@ -50,21 +53,29 @@ __device__ __forceinline__ void argmin_pair(double& t, int& c, double t2, int c2
   }
 }
 
-// Step k of the greedy (encoder/cdef.rs:215-232): a warp per candidate pair
-// scores sum_b min(best[b], Y[yk][b] + UV[uk][b]) — the reference's
-// best_for(set + pair), since best[b] is the minimum over the set so far —
-// lanes striding over the blocks (candidate-major table: coalesced, four
-// blocks in flight per lane). The last CTA to finish (a fenced arrival
-// count; no CTA waits) takes the smallest total, first in (yk, uk) order
-// on ties, adds it to the set, lowers best[], and at set sizes 1, 2, 4 and
-// 8 prices the set. Launched with programmatic dependent launch: the state
-// is read after pdl_wait().
+// Step k of the greedy (encoder/cdef.rs:215-232). A warp per candidate pair
+// scores sum_b min(best[b], last[b], Y[yk][b] + UV[uk][b]) — the reference's
+// best_for(set + pair): best[b] holds the minimum over the set but for its
+// newest pair `last`, which every scorer folds in (and CTA 0 writes back;
+// the min is idempotent, so readers that see either value agree). Lanes
+// stride over the blocks (candidate-major table: coalesced, four blocks in
+// flight per lane). The last CTA to finish (a fenced arrival count; no CTA
+// waits) takes the smallest total, first in (yk, uk) order on ties, and adds
+// its pair to the set. Its total is the new set's total, so at set sizes 1,
+// 2, 4 and 8 it prices the set from it (encoder/cdef.rs:233-239). The
+// candidate lists hold at least 420 pairs, so a pair always remains.
+// Launched with programmatic dependent launch: the state is read after
+// pdl_wait().
 __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchDesc d, CdefGreedy* g, double lambda,
                                                              uint64_t* __restrict__ tot) {
   const int nfb = d.fb_rows * d.fb_cols, ncand = d.ny * d.nuv;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   pdl_wait();
   const int n = g->n;
+  const uint64_t* YL = n ? d.sse + int64_t(g->set_y[n - 1]) * nfb : nullptr;
+  const uint64_t* UL = n ? d.sse + int64_t(d.ny + g->set_uv[n - 1]) * nfb : nullptr;
+  if (n && blockIdx.x == 0)
+    for (int b = tid; b < nfb; b += blockDim.x) d.best[b] = min(d.best[b], YL[b] + UL[b]);
   const int c = blockIdx.x * 8 + warp;
   if (c < ncand) {
     const int yk = c / d.nuv, uk = c - yk * d.nuv;
@@ -77,13 +88,23 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
       const uint64_t* B = d.best;
       uint64_t a1 = 0, a2 = 0, a3 = 0;
       int b = lane;
-      for (; b + 96 < nfb; b += 128) {
-        acc += min(B[b], Y[b] + U[b]);
-        a1 += min(B[b + 32], Y[b + 32] + U[b + 32]);
-        a2 += min(B[b + 64], Y[b + 64] + U[b + 64]);
-        a3 += min(B[b + 96], Y[b + 96] + U[b + 96]);
+      if (n) {
+        for (; b + 96 < nfb; b += 128) {
+          acc += min(min(B[b], YL[b] + UL[b]), Y[b] + U[b]);
+          a1 += min(min(B[b + 32], YL[b + 32] + UL[b + 32]), Y[b + 32] + U[b + 32]);
+          a2 += min(min(B[b + 64], YL[b + 64] + UL[b + 64]), Y[b + 64] + U[b + 64]);
+          a3 += min(min(B[b + 96], YL[b + 96] + UL[b + 96]), Y[b + 96] + U[b + 96]);
+        }
+        for (; b < nfb; b += 32) acc += min(min(B[b], YL[b] + UL[b]), Y[b] + U[b]);
+      } else {
+        for (; b + 96 < nfb; b += 128) {
+          acc += min(B[b], Y[b] + U[b]);
+          a1 += min(B[b + 32], Y[b + 32] + U[b + 32]);
+          a2 += min(B[b + 64], Y[b + 64] + U[b + 64]);
+          a3 += min(B[b + 96], Y[b + 96] + U[b + 96]);
+        }
+        for (; b < nfb; b += 32) acc += min(B[b], Y[b] + U[b]);
       }
-      for (; b < nfb; b += 32) acc += min(B[b], Y[b] + U[b]);
       acc = warp_sum_u64(acc + a1 + a2 + a3);
     }
     if (lane == 0) tot[c] = in_set ? ~uint64_t(0) : acc;
@@ -97,7 +118,7 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  // --- argmin over (total, candidate): per thread, per warp, then warp 0 ---
+  // --- argmin over (total, candidate): per thread, per warp, then all ---
   __shared__ double s_t[8];
   __shared__ int s_c[8];
   double bt = DBL_MAX;
@@ -106,7 +127,7 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
     const uint64_t u = __ldcg(&tot[k]);
     if (u == ~uint64_t(0)) continue;  // in the set
     const double t = u < kExact ? double(u)
-                                 : ordered_total(d.best, d.sse + int64_t(k / d.nuv) * nfb,
+                                 : ordered_total(d.best, YL, UL, d.sse + int64_t(k / d.nuv) * nfb,
                                                  d.sse + int64_t(d.ny + k % d.nuv) * nfb, nfb);
     argmin_pair(bt, bc, t, k);
   }
@@ -121,55 +142,25 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
     s_c[warp] = bc;
   }
   __syncthreads();
+  if (tid != 0) return;
   bt = s_t[0];
   bc = s_c[0];
   for (int w = 1; w < 8; w++) argmin_pair(bt, bc, s_t[w], s_c[w]);
-  // no pair left (fewer than 8 candidates): the reference adds (0, 0)
-  const int pick = bc < 0 ? 0 : bc;
-  const int py = pick / d.nuv, pu = pick - py * d.nuv;
-  if (tid == 0) {
-    g->set_y[n] = py;
-    g->set_uv[n] = pu;
-    g->n = n + 1;
-    g->arrived = 0;
-  }
-  // --- lower the per-block minima by the new pair ---
-  __shared__ uint64_t s_sum[8];
-  uint64_t part = 0;
-  {
-    const uint64_t* Y = d.sse + int64_t(py) * nfb;
-    const uint64_t* U = d.sse + int64_t(d.ny + pu) * nfb;
-    for (int b = tid; b < nfb; b += blockDim.x) {
-      const uint64_t m = min(__ldcg(&d.best[b]), Y[b] + U[b]);
-      d.best[b] = m;
-      part += m;
-    }
-  }
+  g->set_y[n] = bc / d.nuv;
+  g->set_uv[n] = bc % d.nuv;
+  g->n = n + 1;
+  g->arrived = 0;
   const int size = n + 1;
   if ((size & (size - 1)) != 0) return;  // not a power of two: the level is not complete
-  // --- price the set of 1 << bits pairs (encoder/cdef.rs:233-239) ---
-  part = warp_sum_u64(part);
-  if (lane == 0) s_sum[warp] = part;
-  __syncthreads();
-  if (tid == 0) {
-    uint64_t total = 0;
-    for (int w = 0; w < 8; w++) total += s_sum[w];
-    const int bits = __ffs(size) - 1;
-    double t;
-    if (total < kExact) {
-      t = double(total);
-    } else {
-      t = ordered_total(d.best, nullptr, nullptr, nfb);
-    }
-    const double pen = __dmul_rn(__dmul_rn(lambda, double(bits)), double(g->nb));
-    const double cost = __dadd_rn(t, pen);
-    const double prev = bits == 0 ? DBL_MAX : g->best_cost;
-    if (cost < prev) {
-      g->best_cost = cost;
-      g->best_bits = bits;
-    } else if (bits == 0) {
-      g->best_cost = DBL_MAX;
-    }
+  const int bits = __ffs(size) - 1;
+  const double pen = __dmul_rn(__dmul_rn(lambda, double(bits)), double(g->nb));
+  const double cost = __dadd_rn(bt, pen);
+  const double prev = bits == 0 ? DBL_MAX : g->best_cost;
+  if (cost < prev) {
+    g->best_cost = cost;
+    g->best_bits = bits;
+  } else if (bits == 0) {
+    g->best_cost = DBL_MAX;
   }
 }
 
