@@ -216,3 +216,35 @@ def test_lr_search_identity_and_rejection(ctx):
                                  None) == A.ERR_INVALID_INPUT
     assert L.av1pf_lr_search(ctx.p, C.byref(info), C.byref(params), d.c, None, d.c, 1.0, 1, ptrs, ft,
                              None) == A.ERR_INVALID_INPUT
+
+
+def test_searches_interleaved_with_chains_on_one_context(ctx):
+    """The searches share the context with the chain (its streams, events,
+    descriptor buffers and the loop-filter search's planning): chains run
+    before, between and after them stay bit-exact, and each search repeats
+    its result."""
+    sf_chain = A.SynthHandle(width=640, height=360, bit_depth=10, superres_denom=12, enable_grain=1, seed=61)
+    ref_cpu, fb_cpu = O.chain(sf_chain, threads=0)
+    df_chain = G.DevFrame(sf_chain)
+
+    def chain_ok():
+        ref_gpu, fb_gpu = G.gpu_chain(ctx, df_chain)
+        assert all(np.array_equal(g, c) for g, c in zip(ref_gpu, ref_cpu.arrays))
+        assert np.array_equal(fb_gpu, fb_cpu)
+
+    sf = A.SynthHandle(width=320, height=192, bit_depth=10, seed=62, enable_lr=1)
+    cur, src = O.search_inputs(sf, 63)
+    lcur, lcdef, lsrc = O.lr_search_inputs(sf, 64)
+    df = G.DevFrame(sf)
+    want_cdef = O.cdef_search(sf, cur, src, 100, 20.0, False)
+    want_lf = O.lf_search(sf, cur, src)
+    want_lr = O.lr_search(sf, lcur, lcdef, lsrc, 80.0, 1)
+    chain_ok()
+    for _ in range(2):
+        assert_cdef_same(gpu_cdef_search(ctx, sf, df, cur, src, 100, 20.0, False), want_cdef, "interleaved")
+        chain_ok()
+        lv, sse = gpu_lf_search(ctx, sf, cur, src)
+        assert lv == want_lf[0] and np.array_equal(sse, want_lf[1])
+        chain_ok()
+        assert gpu_lr_search(ctx, sf, lcur, lcdef, lsrc, 80.0, 1) == want_lr
+        chain_ok()
