@@ -248,3 +248,36 @@ def test_searches_interleaved_with_chains_on_one_context(ctx):
         chain_ok()
         assert gpu_lr_search(ctx, sf, lcur, lcdef, lsrc, 80.0, 1) == want_lr
         chain_ok()
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_searches_random_configurations(ctx, seed):
+    """Seeded random frame shapes and parameters through all three searches,
+    GPU against oracle: 8/10/12-bit, u8/u16, every subsampling, sizes from
+    8 samples up, both CDEF lists, every LR effort and unit size, lambdas of
+    both signs (LR) and zero."""
+    rng = np.random.default_rng(1000 + seed)
+    bd = int(rng.choice([8, 10, 12]))
+    sub = [(1, 1), (1, 0), (0, 0)][int(rng.integers(0, 3))]
+    cfg = dict(width=int(rng.integers(8, 400)), height=int(rng.integers(8, 260)), bit_depth=bd,
+               subsampling_x=sub[0], subsampling_y=sub[1], seed=2000 + seed, enable_lr=1,
+               lr_unit_shift=int(rng.integers(0, 3)), lr_uv_shift=int(rng.integers(0, 2)),
+               skip_pct=int(rng.integers(0, 100)))
+    if bd == 8 and rng.random() < 0.5:
+        cfg["sample_bytes"] = 1
+    if rng.random() < 0.15:
+        cfg["mono"] = 1
+    sf = A.SynthHandle(**cfg)
+    amp = int(rng.integers(1, 40)) << (bd - 8)
+    cur, src = O.search_inputs(sf, 3000 + seed, amp=amp)
+    df = G.DevFrame(sf)
+    q, lam, thorough = int(rng.integers(0, 256)), float(rng.choice([0.0, 3.0, 50.0, 2000.0])), bool(rng.random() < 0.5)
+    assert_cdef_same(gpu_cdef_search(ctx, sf, df, cur, src, q, lam, thorough),
+                     O.cdef_search(sf, cur, src, q, lam, thorough), f"cdef {cfg}")
+    lv, sse = gpu_lf_search(ctx, sf, cur, src)
+    lv_o, sse_o = O.lf_search(sf, cur, src)
+    assert lv == lv_o and np.array_equal(sse, sse_o), f"lf {cfg}"
+    lcur, lcdef, lsrc = O.lr_search_inputs(sf, 4000 + seed, amp=amp)
+    eff, llam = int(rng.integers(0, 3)), float(rng.choice([0.0, 40.0, 500.0, -1e9]))
+    assert gpu_lr_search(ctx, sf, lcur, lcdef, lsrc, llam, eff) == O.lr_search(sf, lcur, lcdef, lsrc, llam, eff), \
+        f"lr {cfg} effort {eff} lambda {llam}"
