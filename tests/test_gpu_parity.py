@@ -364,3 +364,36 @@ def test_invalid_inputs_rejected(ctx):
     assert L.av1pf_chain(ctx.p, C.byref(df.info), C.byref(df.params), C.byref(df.maps), small, ref.c, None,
                          None) == A.ERR_INVALID_INPUT
     assert L.av1pf_last_error()
+
+
+def random_chain_config(seed):
+    """A seeded random frame: size, bit depth and storage, subsampling,
+    superres, film grain, segmentation and delta-lf, block sizes and skip
+    rate, LR unit sizes, each stage on or off."""
+    rng = np.random.default_rng(5000 + seed)
+    bd = int(rng.choice([8, 10, 12]))
+    sub = [(1, 1), (1, 0), (0, 0)][int(rng.integers(0, 3))]
+    cfg = dict(width=int(rng.integers(8, 520)), height=int(rng.integers(8, 300)), bit_depth=bd,
+               subsampling_x=sub[0], subsampling_y=sub[1], seed=6000 + seed, frame_index=int(rng.integers(0, 8)),
+               content=int(rng.integers(0, 2)), noise_sigma=int(rng.integers(0, 12)),
+               enable_lf=int(rng.random() < 0.9), enable_cdef=int(rng.random() < 0.9),
+               enable_lr=int(rng.random() < 0.9), enable_grain=int(rng.random() < 0.4),
+               segmentation=int(rng.random() < 0.3), delta_lf=int(rng.integers(0, 3)),
+               min_block_log2=int(rng.integers(2, 6)), skip_pct=int(rng.integers(0, 101)),
+               lr_unit_shift=int(rng.integers(0, 3)), lr_uv_shift=int(rng.integers(0, 2)))
+    if bd == 8 and rng.random() < 0.5:
+        cfg["sample_bytes"] = 1
+    if rng.random() < 0.15:
+        cfg["mono"] = 1
+    if rng.random() < 0.3:
+        cfg["superres_denom"] = int(rng.integers(9, 17))
+    return cfg
+
+
+@pytest.mark.parametrize("seed", range(30))
+def test_chain_random_configurations(ctx, seed):
+    cfg = random_chain_config(seed)
+    sf = A.SynthHandle(**cfg)
+    ref_cpu, fb_cpu = O.chain(sf, threads=0)
+    ref_gpu, fb_gpu = G.gpu_chain(ctx, G.DevFrame(sf))
+    assert_same(ref_gpu, fb_gpu, ref_cpu, fb_cpu, f"random {seed}: {cfg}")
