@@ -640,9 +640,60 @@ def bench_search(args, ctx, rank, world):
                                         for k in ("cdef_fast", "cdef_thorough", "lf")}
         res[name] = out
     res["lr_1080p_10bit"] = bench_lr_search(args, ctx, rank, world)
+    res["cdef_batch_640x360_x16"] = bench_cdef_search_batch(args, ctx)
     res["inputs"] = (f"seeded synthetic frames; reconstruction = source + seeded 4x4-block noise (+-24) and "
                      f"per-sample noise; base_q_idx {q}, lambda {lam}")
     return res
+
+
+def bench_cdef_search_batch(args, ctx, n=16, w=640, h=360):
+    """The CDEF search (fast lists) over n small frames: n per-frame calls
+    against one av1pf_cdef_search_many call (host clock around each
+    synchronous call; the results are the same by construction and by the
+    parity tests)."""
+    import gpu_util as G
+    import torch
+    L = A.lib()
+    keep = []
+    jobs = (A.CdefSearchJob * n)()
+    for i in range(n):
+        sf = A.SynthHandle(width=w, height=h, bit_depth=10, seed=600 + i)
+        cur, src = A.synth_search_planes(sf, 700 + i, amp=24)
+        info = sf.f.info
+        df = G.DevFrame(sf)
+        planes = []
+        for arrs in (cur, src):
+            d = G.DevPlanes(info, [(a.shape[1], a.shape[0]) for a in arrs], [a.shape[1] for a in arrs])
+            for p in range(info.num_planes):
+                d.t[p].copy_(torch.from_numpy(arrs[p].view(np.uint8).reshape(-1)))
+            planes.append(d)
+        res = A.CdefSearchResult()
+        keep.append((sf, df, planes, res))
+        jobs[i].info = C.pointer(sf.f.info)
+        jobs[i].maps = C.pointer(df.maps)
+        jobs[i].cur = C.cast(planes[0].c, C.POINTER(A.Plane))
+        jobs[i].src = C.cast(planes[1].c, C.POINTER(A.Plane))
+        jobs[i].base_q_idx = 120
+        jobs[i].lam = 40.0
+        jobs[i].result = C.pointer(res)
+
+    def per_frame():
+        for k in range(n):
+            A.check(L.av1pf_cdef_search_many(ctx.p, 1, C.byref(jobs[k]), 0, None), "cdef_search_many")
+
+    def batched():
+        A.check(L.av1pf_cdef_search_many(ctx.p, n, jobs, 0, None), "cdef_search_many")
+    out = {}
+    for name, fn in (("per_frame_ms", per_frame), ("batched_ms", batched)):
+        for _ in range(max(2, args.warmup)):
+            fn()
+        reps = 10
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        out[name] = round((time.perf_counter() - t) / reps * 1e3, 3)
+    out["batched_vs_per_frame"] = round(out["per_frame_ms"] / out["batched_ms"], 2)
+    return out
 
 
 def bench_lr_search(args, ctx, rank, world, lam=150.0):

@@ -516,6 +516,27 @@ int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
                       av1pf_cdef_search_result* result, int8_t* cdef_idx_out,
                       uint64_t* block_sse, void* stream);
 
+/* One frame of av1pf_cdef_search_many: the arguments of av1pf_cdef_search. */
+typedef struct av1pf_cdef_search_job {
+  const av1pf_frame_info* info;
+  const av1pf_maps* maps;    /* device */
+  const av1pf_plane* cur;    /* device */
+  const av1pf_plane* src;    /* device */
+  int32_t base_q_idx;
+  double lambda;
+  av1pf_cdef_search_result* result; /* host */
+  int8_t* cdef_idx_out;      /* host, or NULL */
+  uint64_t* block_sse;       /* host, or NULL */
+} av1pf_cdef_search_job;
+
+/* av1pf_cdef_search for n frames (shapes may differ) in one call: one launch
+ * scores every frame's blocks and each greedy step advances every frame, so
+ * small frames share the device and the per-call costs (an encoder's
+ * lookahead or the rungs of a resolution ladder). Each result equals that of
+ * av1pf_cdef_search on its frame. n <= 4096. */
+int av1pf_cdef_search_many(av1pf_ctx* ctx, int n, const av1pf_cdef_search_job* jobs,
+                           int32_t thorough, void* stream);
+
 /* Effort of the loop-restoration search (encoder/lr.rs:47-58): fast fits
  * on every other row and column and tries 2 self-guided parameter sets,
  * normal 6, thorough all 16. */

@@ -126,6 +126,12 @@ class CdefSearchResult(C.Structure):
 CDEF_SEARCH_N = {False: (28, 15), True: (44, 24)}  # (luma, chroma) candidate pairs
 
 
+class CdefSearchJob(C.Structure):
+    _fields_ = [("info", C.POINTER(FrameInfo)), ("maps", C.POINTER(Maps)), ("cur", C.POINTER(Plane)),
+                ("src", C.POINTER(Plane)), ("base_q_idx", C.c_int32), ("lam", C.c_double),
+                ("result", C.POINTER(CdefSearchResult)), ("cdef_idx_out", C.c_void_p), ("block_sse", C.c_void_p)]
+
+
 class LfEdgeParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("limit", "blimit", "thresh", "filter_size", "chroma", "bit_depth")]
 
@@ -212,6 +218,7 @@ def lib():
         _sig(L, "av1pf_serve_close", C.c_int, vp)
         _sig(L, "av1pf_cdef_search", C.c_int, vp, P(FrameInfo), P(Maps), P(Plane), P(Plane), C.c_int32, C.c_double,
              C.c_int32, P(CdefSearchResult), vp, vp, vp)
+        _sig(L, "av1pf_cdef_search_many", C.c_int, vp, C.c_int, P(CdefSearchJob), C.c_int32, vp)
         _sig(L, "av1pf_lr_search", C.c_int, vp, P(FrameInfo), P(Params), P(Plane), P(Plane), P(Plane), C.c_double,
              C.c_int32, P(P(LrUnit)), P(C.c_int32), vp)
         _sig(L, "av1pf_lf_search", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane),

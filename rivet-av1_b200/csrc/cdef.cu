@@ -717,10 +717,11 @@ __device__ __forceinline__ void warp_reduce_pairs(const uint32_t (&acc)[N], uint
 // the decoder's. Then each thread takes 16 luma samples of one 8x8 block
 // (rows r and r + 4; a warp per row of blocks) and scores every pair on
 // each (sample_pairs), the errors of each pair accumulating in a register;
-// the chroma samples of the same block follow. TH: the thorough lists.
+// the chroma samples of the same block follow. TH: the thorough lists. The
+// grid covers every block of n frames: frame i's blocks start at CTA
+// ds[i].block0.
 template <bool TH>
-__global__ void __launch_bounds__(256, 2) cdef_search_kernel(const FrameDesc* __restrict__ frames,
-                                                                    const CdefSearchDesc d, CdefGreedy* __restrict__ g) {
+__global__ void __launch_bounds__(256, 2) cdef_search_kernel(const CdefSearchDesc* __restrict__ ds, int n) {
   constexpr int NYP = TH ? 11 : 7, NUVP = TH ? 8 : 5, NYS = 4, NUVS = 3;
   constexpr int NY = NYP * NYS, NUV = NUVP * NUVS;
   constexpr int R = 64, top = 2, wrows = R + 2 * top;
@@ -735,9 +736,19 @@ __global__ void __launch_bounds__(256, 2) cdef_search_kernel(const FrameDesc* __
   __shared__ uint8_t uvdir[2][2][8];
   __shared__ int s_one;
   __shared__ uint64_t red[8][kSearchMaxY + kSearchMaxUV];
-  const FrameDesc& f = frames[0];
+  int fi = 0;
+  for (int hi = n - 1; fi < hi;) {  // the last frame whose first block is at or before this CTA
+    const int mid = (fi + hi + 1) >> 1;
+    if (ds[mid].block0 <= int(blockIdx.x))
+      fi = mid;
+    else
+      hi = mid - 1;
+  }
+  const CdefSearchDesc& d = ds[fi];
+  const FrameDesc& f = *d.frame;
+  CdefGreedy* g = d.g;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int fb = blockIdx.x, nfb = d.fb_rows * d.fb_cols;
+  const int fb = int(blockIdx.x) - d.block0, nfb = d.fb_rows * d.fb_cols;
   const int fr = fb / d.fb_cols, fc = fb - fr * d.fb_cols;
   const int idx = f.cdef_idx[int64_t(fr) * f.cdef_stride + fc];
   if (idx < 0) {  // codes no index: zero errors, and no part in the greedy's sums
@@ -877,7 +888,6 @@ __global__ void __launch_bounds__(256, 2) cdef_search_kernel(const FrameDesc* __
 }
 
 constexpr int kSearchSmem = 3 * (64 + 4) * kS * 2 + 3 * 64 * kS * 2;
-constexpr int search_lists_ny(bool th) { return th ? 44 : 28; }
 
 // dsp::cdef::filter (cdef.rs:29) on independent 12x12 windows: one CTA per
 // window, one thread per output sample.
@@ -954,13 +964,12 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
                wrows);
 }
 
-void launch_cdef_search(const FrameDesc* frames, const CdefSearchDesc& d, CdefGreedy* g, cudaStream_t s) {
-  const int nfb = d.fb_rows * d.fb_cols;
-  if (nfb <= 0) return;
-  if (d.ny == search_lists_ny(true))
-    cdef_search_kernel<true><<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
+void launch_cdef_search(const CdefSearchDesc* ds, int n, int blocks, bool thorough, cudaStream_t s) {
+  if (blocks <= 0) return;
+  if (thorough)
+    cdef_search_kernel<true><<<blocks, 256, kSearchSmem, s>>>(ds, n);
   else
-    cdef_search_kernel<false><<<nfb, 256, kSearchSmem, s>>>(frames, d, g);
+    cdef_search_kernel<false><<<blocks, 256, kSearchSmem, s>>>(ds, n);
   note_launch();
 }
 

@@ -102,6 +102,17 @@ struct CdefSearchDesc {
   int8_t uv_pri[kSearchMaxUV], uv_sec[kSearchMaxUV];
   uint64_t* sse;           // [ny + nuv][fb_rows * fb_cols], candidate-major
   uint64_t* best;          // [fb_rows * fb_cols]: the greedy's per-block minimum
+  // one frame of a batched search: its descriptor, greedy state, candidate
+  // totals, input table and outputs, and its first CTA in each grid
+  const FrameDesc* frame;
+  struct CdefGreedy* g;
+  uint64_t* tot;           // [ny * nuv]
+  const int8_t* cdef_idx;
+  int32_t cdef_stride;
+  int8_t* table;           // [fb_rows * cdef_stride]
+  int32_t* res;            // [18]: nb, bits, the chosen pairs' indices
+  double lambda;
+  int32_t block0, table0;  // first CTA in the table kernel, first entry in the finish kernel
 };
 
 // The encoder's loop-restoration search (encoder/lr.rs:64-430): one job

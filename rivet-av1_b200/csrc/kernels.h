@@ -65,18 +65,19 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
 cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
 // The encoder's CDEF search: per-block squared errors of every candidate
-// (one CTA per 64x64 block of frames[0]); counts the coding blocks into g->nb.
-void launch_cdef_search(const FrameDesc* frames, const CdefSearchDesc& d, CdefGreedy* g, cudaStream_t s);
+// (one CTA per 64x64 block of n frames, `blocks` in all); counts each
+// frame's coding blocks into its greedy state.
+void launch_cdef_search(const CdefSearchDesc* ds, int n, int blocks, bool thorough, cudaStream_t s);
 
 // Encoder searches (search.cu)
-// One greedy step of the CDEF search: every pair not yet chosen is scored
-// and the best is added (the last CTA to finish picks); `tot` holds
-// ny * nuv totals.
-void launch_cdef_greedy_step(const CdefSearchDesc& d, CdefGreedy* g, uint64_t* tot, double lambda, cudaStream_t s);
-// The CDEF search's outcome: each coding block's index into `table` (a copy
-// of cdef_idx, rows x stride) and the chosen pairs into `res`.
-void launch_cdef_greedy_finish(const CdefSearchDesc& d, const CdefGreedy* g, const int8_t* cdef_idx, int stride,
-                               int8_t* table, int32_t* res, cudaStream_t s);
+// One greedy step of the CDEF search for n frames side by side: every pair
+// not yet chosen is scored and the best is added (the last CTA of a frame
+// to finish picks).
+void launch_cdef_greedy_step(const CdefSearchDesc* ds, int n, int ncand, cudaStream_t s);
+// The CDEF search's outcome: each coding block's index into each frame's
+// table (a copy of its cdef_idx) and the chosen pairs into its result
+// (`total` table entries over all frames).
+void launch_cdef_greedy_finish(const CdefSearchDesc* ds, int n, int total, cudaStream_t s);
 // Squared error of planes against the source over each plane's frame area:
 // sse[i] += sum over plane job i (a[i], b[i]: plane pointers, strides).
 struct SsePlane {

@@ -98,111 +98,172 @@ int damping_for(int qidx) { return std::min(qidx >> 6, 3); }  // encoder/cdef.rs
 
 extern "C" {
 
-int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_maps* maps, const av1pf_plane* cur,
-                      const av1pf_plane* src, int32_t base_q_idx, double lambda, int32_t thorough,
-                      av1pf_cdef_search_result* result, int8_t* cdef_idx_out, uint64_t* block_sse, void* stream) {
+int av1pf_cdef_search_many(av1pf_ctx* ctx, int n, const av1pf_cdef_search_job* jobs, int32_t thorough,
+                           void* stream) {
   int rc = enter(ctx);
   if (rc) return rc;
-  std::string why;
-  if ((rc = validate_frame(info, nullptr, cur, &why)) != AV1PF_OK) return set_error(why), rc;
-  if ((rc = check_src(info, src)) != AV1PF_OK) return rc;
-  const int fb_rows = (info->mi_rows + 15) / 16, fb_cols = (info->mi_cols + 15) / 16;
-  if (!maps || !maps->mi || maps->mi_stride < info->mi_cols) return fail_input("mi map missing or mi_stride < mi_cols");
-  if (!maps->cdef_idx || maps->cdef_stride < fb_cols) return fail_input("cdef_idx missing or cdef_stride too small");
-  if (base_q_idx < 0 || base_q_idx > 255) return fail_input("base_q_idx out of range");
-  if (!std::isfinite(lambda) || lambda < 0) return fail_input("lambda must be finite and >= 0");
-  if (!result) return fail_input("null result");
+  if (n <= 0 || n > 4096 || !jobs) return fail_input("bad job count");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-
   std::vector<std::pair<int, int>> yc, uvc;
   cdef_candidates(thorough != 0, yc, uvc);
-  FrameDesc f{};
-  f.bd = info->bit_depth;
-  f.sb = info->sample_bytes;
-  f.ssx = info->subsampling_x;
-  f.ssy = info->subsampling_y;
-  f.np = info->num_planes;
-  f.fw = info->frame_width;
-  f.fh = info->frame_height;
-  f.uw = info->upscaled_width;
-  f.mi_rows = info->mi_rows;
-  f.mi_cols = info->mi_cols;
-  f.mc = info->matrix_coefficients;
-  for (int p = 0; p < f.np; p++) f.cur[p] = dplane(cur[p]);
-  f.mi = maps->mi;
-  f.mi_stride = maps->mi_stride;
-  f.cdef_idx = maps->cdef_idx;
-  f.cdef_stride = maps->cdef_stride;
-
-  CdefSearchDesc d{};
-  for (int p = 0; p < f.np; p++) d.src[p] = dplane(src[p]);
-  d.ny = int32_t(yc.size());
-  d.nuv = int32_t(uvc.size());
-  d.damping = damping_for(base_q_idx) + 3;
-  d.fb_rows = fb_rows;
-  d.fb_cols = fb_cols;
-  for (size_t k = 0; k < yc.size(); k++) {
-    d.y_pri[k] = int8_t(yc[k].first);
-    d.y_sec[k] = int8_t(coded_sec(yc[k].second));
+  const int ny = int(yc.size()), nuv = int(uvc.size()), nc = ny + nuv, ncand = ny * nuv;
+  // layout: descriptors and greedy states, then per frame its totals, error
+  // table and minima; the results (pairs and index table) of every frame
+  // sit together so that one copy brings them back
+  struct Geo {
+    int fb_rows, fb_cols, nfb;
+    size_t table_bytes, o_tot, o_sse, o_best, o_res;
+  };
+  std::vector<Geo> geo(static_cast<size_t>(n));
+  std::string why;
+  const size_t o_descs = align256(size_t(n) * sizeof(FrameDesc));
+  const size_t o_g = o_descs + align256(size_t(n) * sizeof(CdefSearchDesc));
+  size_t off = o_g + align256(size_t(n) * sizeof(CdefGreedy));
+  size_t res_bytes = 0;
+  int blocks = 0, entries = 0;
+  for (int i = 0; i < n; i++) {
+    const av1pf_cdef_search_job& jb = jobs[i];
+    const av1pf_frame_info* info = jb.info;
+    if ((rc = validate_frame(info, nullptr, jb.cur, &why)) != AV1PF_OK) return set_error(why), rc;
+    if ((rc = check_src(info, jb.src)) != AV1PF_OK) return rc;
+    Geo& G = geo[size_t(i)];
+    G.fb_rows = (info->mi_rows + 15) / 16;
+    G.fb_cols = (info->mi_cols + 15) / 16;
+    G.nfb = G.fb_rows * G.fb_cols;
+    const av1pf_maps* maps = jb.maps;
+    if (!maps || !maps->mi || maps->mi_stride < info->mi_cols) return fail_input("mi map missing or mi_stride < mi_cols");
+    if (!maps->cdef_idx || maps->cdef_stride < G.fb_cols) return fail_input("cdef_idx missing or cdef_stride too small");
+    if (jb.base_q_idx < 0 || jb.base_q_idx > 255) return fail_input("base_q_idx out of range");
+    if (!std::isfinite(jb.lambda) || jb.lambda < 0) return fail_input("lambda must be finite and >= 0");
+    if (!jb.result) return fail_input("null result");
+    G.table_bytes = size_t(G.fb_rows) * size_t(maps->cdef_stride);
+    G.o_tot = off;
+    G.o_sse = G.o_tot + align256(size_t(ncand) * 8);
+    G.o_best = G.o_sse + align256(size_t(nc) * size_t(G.nfb) * 8);
+    off = G.o_best + align256(size_t(G.nfb) * 8);
+    G.o_res = res_bytes;  // within the results region: 18 ints, then the index table
+    res_bytes += align256(18 * sizeof(int32_t) + G.table_bytes);
+    blocks += G.nfb;
+    entries += int(G.table_bytes);
   }
-  for (size_t k = 0; k < uvc.size(); k++) {
-    d.uv_pri[k] = int8_t(uvc[k].first);
-    d.uv_sec[k] = int8_t(coded_sec(uvc[k].second));
-  }
-  const size_t nfb = size_t(fb_rows) * size_t(fb_cols), nc = size_t(d.ny + d.nuv), ncand = size_t(d.ny * d.nuv);
-  const size_t table_bytes = size_t(fb_rows) * size_t(maps->cdef_stride);
-  // device: descriptor | greedy state | candidate totals | error table | minima | table | result
-  const size_t o_desc = 0, o_g = align256(sizeof(FrameDesc)), o_tot = o_g + align256(sizeof(CdefGreedy));
-  const size_t o_sse = o_tot + align256(ncand * 8), o_best = o_sse + align256(nc * nfb * 8);
-  const size_t o_table = o_best + align256(nfb * 8), o_res = o_table + align256(table_bytes);
-  const size_t dev_bytes = o_res + 256;
-  // host staging: descriptor | result | table | error table
-  const size_t h_res = align256(sizeof(FrameDesc)), h_table = h_res + 256, h_sse = h_table + align256(table_bytes);
-  const size_t host_bytes = h_sse + (block_sse ? nc * nfb * 8 : 0);
+  const size_t o_results = off, dev_bytes = o_results + res_bytes;
+  size_t sse_bytes = 0;
+  for (int i = 0; i < n; i++)
+    if (jobs[i].block_sse) sse_bytes += size_t(nc) * size_t(geo[size_t(i)].nfb) * 8;
+  const size_t host_bytes = o_g + res_bytes + sse_bytes;
   if ((rc = ctx->ensure(ctx->search_dev, dev_bytes)) != AV1PF_OK) return rc;
   if ((rc = ctx->ensure_host(ctx->search_host, host_bytes)) != AV1PF_OK) return rc;
   uint8_t* dv = static_cast<uint8_t*>(ctx->search_dev.ptr);
   uint8_t* hs = static_cast<uint8_t*>(ctx->search_host.ptr);
-  d.sse = reinterpret_cast<uint64_t*>(dv + o_sse);
-  d.best = reinterpret_cast<uint64_t*>(dv + o_best);
-  auto* g = reinterpret_cast<CdefGreedy*>(dv + o_g);
-  std::memcpy(hs, &f, sizeof(FrameDesc));
-  cudaError_t e = cudaMemcpyAsync(dv + o_desc, hs, sizeof(FrameDesc), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(g, 0, sizeof(CdefGreedy), s);
+  auto* hframes = reinterpret_cast<FrameDesc*>(hs);
+  auto* hdescs = reinterpret_cast<CdefSearchDesc*>(hs + o_descs);
+  const auto* dframes = reinterpret_cast<const FrameDesc*>(dv);
+  auto* dg = reinterpret_cast<CdefGreedy*>(dv + o_g);
+  int block0 = 0, table0 = 0;
+  for (int i = 0; i < n; i++) {
+    const av1pf_cdef_search_job& jb = jobs[i];
+    const av1pf_frame_info* info = jb.info;
+    const Geo& G = geo[size_t(i)];
+    FrameDesc f{};
+    f.bd = info->bit_depth;
+    f.sb = info->sample_bytes;
+    f.ssx = info->subsampling_x;
+    f.ssy = info->subsampling_y;
+    f.np = info->num_planes;
+    f.fw = info->frame_width;
+    f.fh = info->frame_height;
+    f.uw = info->upscaled_width;
+    f.mi_rows = info->mi_rows;
+    f.mi_cols = info->mi_cols;
+    f.mc = info->matrix_coefficients;
+    for (int p = 0; p < f.np; p++) f.cur[p] = dplane(jb.cur[p]);
+    f.mi = jb.maps->mi;
+    f.mi_stride = jb.maps->mi_stride;
+    f.cdef_idx = jb.maps->cdef_idx;
+    f.cdef_stride = jb.maps->cdef_stride;
+    hframes[i] = f;
+    CdefSearchDesc d{};
+    for (int p = 0; p < f.np; p++) d.src[p] = dplane(jb.src[p]);
+    d.ny = ny;
+    d.nuv = nuv;
+    d.damping = damping_for(jb.base_q_idx) + 3;
+    d.fb_rows = G.fb_rows;
+    d.fb_cols = G.fb_cols;
+    for (int k = 0; k < ny; k++) {
+      d.y_pri[k] = int8_t(yc[size_t(k)].first);
+      d.y_sec[k] = int8_t(coded_sec(yc[size_t(k)].second));
+    }
+    for (int k = 0; k < nuv; k++) {
+      d.uv_pri[k] = int8_t(uvc[size_t(k)].first);
+      d.uv_sec[k] = int8_t(coded_sec(uvc[size_t(k)].second));
+    }
+    d.sse = reinterpret_cast<uint64_t*>(dv + G.o_sse);
+    d.best = reinterpret_cast<uint64_t*>(dv + G.o_best);
+    d.frame = dframes + i;
+    d.g = dg + i;
+    d.tot = reinterpret_cast<uint64_t*>(dv + G.o_tot);
+    d.cdef_idx = jb.maps->cdef_idx;
+    d.cdef_stride = jb.maps->cdef_stride;
+    d.res = reinterpret_cast<int32_t*>(dv + o_results + G.o_res);
+    d.table = reinterpret_cast<int8_t*>(dv + o_results + G.o_res + 18 * sizeof(int32_t));
+    d.lambda = jb.lambda;
+    d.block0 = block0;
+    d.table0 = table0;
+    block0 += G.nfb;
+    table0 += int(G.table_bytes);
+    hdescs[i] = d;
+  }
+  const auto* ddescs = reinterpret_cast<const CdefSearchDesc*>(dv + o_descs);
+  cudaError_t e = cudaMemcpyAsync(dv, hs, o_g, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, size_t(n) * sizeof(CdefGreedy), s);
   if (e != cudaSuccess) return cuda_status(e, "search upload");
-  launch_cdef_search(reinterpret_cast<const FrameDesc*>(dv + o_desc), d, g, s);
-  for (int step = 0; step < 8; step++)
-    launch_cdef_greedy_step(d, g, reinterpret_cast<uint64_t*>(dv + o_tot), lambda, s);
-  launch_cdef_greedy_finish(d, g, maps->cdef_idx, maps->cdef_stride, reinterpret_cast<int8_t*>(dv + o_table),
-                            reinterpret_cast<int32_t*>(dv + o_res), s);
-  e = cudaMemcpyAsync(hs + h_res, dv + o_res, 18 * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(hs + h_table, dv + o_table, table_bytes, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && block_sse)
-    e = cudaMemcpyAsync(hs + h_sse, dv + o_sse, nc * nfb * 8, cudaMemcpyDeviceToHost, s);
+  launch_cdef_search(ddescs, n, blocks, thorough != 0, s);
+  for (int step = 0; step < 8; step++) launch_cdef_greedy_step(ddescs, n, ncand, s);
+  launch_cdef_greedy_finish(ddescs, n, entries, s);
+  e = cudaMemcpyAsync(hs + o_g, dv + o_results, res_bytes, cudaMemcpyDeviceToHost, s);
+  size_t so = o_g + res_bytes;
+  for (int i = 0; i < n && e == cudaSuccess; i++) {
+    if (!jobs[i].block_sse) continue;
+    const size_t bytes = size_t(nc) * size_t(geo[size_t(i)].nfb) * 8;
+    e = cudaMemcpyAsync(hs + so, dv + geo[size_t(i)].o_sse, bytes, cudaMemcpyDeviceToHost, s);
+    so += bytes;
+  }
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_status(e, "CDEF search");
-
-  const int32_t* res = reinterpret_cast<const int32_t*>(hs + h_res);
-  std::memset(result, 0, sizeof(*result));
-  if (res[0] > 0) {  // else CdefParams::off(): one all-zero entry, damping_minus_3 0
-    result->damping_minus_3 = damping_for(base_q_idx);
-    result->bits = res[1];
-    for (int i = 0; i < (1 << res[1]); i++) {
-      result->y_pri[i] = yc[size_t(res[2 + i])].first;
-      result->y_sec[i] = yc[size_t(res[2 + i])].second;
-      result->uv_pri[i] = uvc[size_t(res[10 + i])].first;
-      result->uv_sec[i] = uvc[size_t(res[10 + i])].second;
+  so = o_g + res_bytes;
+  for (int i = 0; i < n; i++) {
+    const av1pf_cdef_search_job& jb = jobs[i];
+    const Geo& G = geo[size_t(i)];
+    const int32_t* res = reinterpret_cast<const int32_t*>(hs + o_g + G.o_res);
+    av1pf_cdef_search_result* result = jb.result;
+    std::memset(result, 0, sizeof(*result));
+    if (res[0] > 0) {  // else CdefParams::off(): one all-zero entry, damping_minus_3 0
+      result->damping_minus_3 = damping_for(jb.base_q_idx);
+      result->bits = res[1];
+      for (int k = 0; k < (1 << res[1]); k++) {
+        result->y_pri[k] = yc[size_t(res[2 + k])].first;
+        result->y_sec[k] = yc[size_t(res[2 + k])].second;
+        result->uv_pri[k] = uvc[size_t(res[10 + k])].first;
+        result->uv_sec[k] = uvc[size_t(res[10 + k])].second;
+      }
+    }
+    if (jb.cdef_idx_out) std::memcpy(jb.cdef_idx_out, hs + o_g + G.o_res + 18 * sizeof(int32_t), G.table_bytes);
+    if (jb.block_sse) {  // candidate-major on the device, block-major for the caller
+      const uint64_t* t = reinterpret_cast<const uint64_t*>(hs + so);
+      for (int k = 0; k < nc; k++)
+        for (int b = 0; b < G.nfb; b++) jb.block_sse[size_t(b) * size_t(nc) + size_t(k)] = t[size_t(k) * size_t(G.nfb) + size_t(b)];
+      so += size_t(nc) * size_t(G.nfb) * 8;
     }
   }
-  if (cdef_idx_out) std::memcpy(cdef_idx_out, hs + h_table, table_bytes);
-  if (block_sse) {  // candidate-major on the device, block-major for the caller
-    const uint64_t* t = reinterpret_cast<const uint64_t*>(hs + h_sse);
-    for (size_t k = 0; k < nc; k++)
-      for (size_t b = 0; b < nfb; b++) block_sse[b * nc + k] = t[k * nfb + b];
-  }
   return AV1PF_OK;
+}
+
+int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_maps* maps, const av1pf_plane* cur,
+                      const av1pf_plane* src, int32_t base_q_idx, double lambda, int32_t thorough,
+                      av1pf_cdef_search_result* result, int8_t* cdef_idx_out, uint64_t* block_sse, void* stream) {
+  const av1pf_cdef_search_job job{info, maps, cur, src, base_q_idx, lambda, result, cdef_idx_out, block_sse};
+  return av1pf_cdef_search_many(ctx, 1, &job, thorough, stream);
 }
 
 int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,

@@ -65,18 +65,23 @@ __device__ __forceinline__ void argmin_pair(double& t, int& c, double t2, int c2
 // 2, 4 and 8 it prices the set from it (encoder/cdef.rs:233-239). The
 // candidate lists hold at least 420 pairs, so a pair always remains.
 // Launched with programmatic dependent launch: the state is read after
-// pdl_wait().
-__global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchDesc d, CdefGreedy* g, double lambda,
-                                                             uint64_t* __restrict__ tot) {
+// pdl_wait(). A batch of frames runs side by side: `cpf` CTAs per frame,
+// each frame with its own state and arrival count.
+__global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchDesc* __restrict__ ds, int cpf) {
+  const int fi = blockIdx.x / cpf, lb = blockIdx.x - fi * cpf;
+  const CdefSearchDesc& d = ds[fi];
+  CdefGreedy* g = d.g;
+  uint64_t* tot = d.tot;
+  const double lambda = d.lambda;
   const int nfb = d.fb_rows * d.fb_cols, ncand = d.ny * d.nuv;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   pdl_wait();
   const int n = g->n;
   const uint64_t* YL = n ? d.sse + int64_t(g->set_y[n - 1]) * nfb : nullptr;
   const uint64_t* UL = n ? d.sse + int64_t(d.ny + g->set_uv[n - 1]) * nfb : nullptr;
-  if (n && blockIdx.x == 0)
+  if (n && lb == 0)
     for (int b = tid; b < nfb; b += blockDim.x) d.best[b] = min(d.best[b], YL[b] + UL[b]);
-  const int c = blockIdx.x * 8 + warp;
+  const int c = lb * 8 + warp;
   if (c < ncand) {
     const int yk = c / d.nuv, uk = c - yk * d.nuv;
     bool in_set = false;
@@ -113,7 +118,7 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
   __syncthreads();
   if (tid == 0) {
     __threadfence();
-    s_last = atomicAdd(&g->arrived, 1u) == gridDim.x - 1;
+    s_last = atomicAdd(&g->arrived, 1u) == unsigned(cpf) - 1;
   }
   __syncthreads();
   if (!s_last) return;
@@ -167,24 +172,33 @@ __global__ void __launch_bounds__(256) cdef_greedy_step_kernel(const CdefSearchD
 // The outcome (encoder/cdef.rs:241-250): each coding block's index is the
 // first of the chosen 1 << best_bits pairs with its least error; the other
 // table entries are copied.
-__global__ void cdef_greedy_finish_kernel(const CdefSearchDesc d, const CdefGreedy* __restrict__ g,
-                                          const int8_t* __restrict__ cdef_idx, int stride, int8_t* __restrict__ table,
-                                          int32_t* __restrict__ res) {
-  const int nfb = d.fb_rows * d.fb_cols;
+__global__ void cdef_greedy_finish_kernel(const CdefSearchDesc* __restrict__ ds, int n, int total) {
+  const int eg = blockIdx.x * blockDim.x + threadIdx.x;
   pdl_wait();
+  if (eg >= total) return;
+  int fi = 0;
+  for (int hi = n - 1; fi < hi;) {  // the last frame whose table starts at or before eg
+    const int mid = (fi + hi + 1) >> 1;
+    if (ds[mid].table0 <= eg)
+      fi = mid;
+    else
+      hi = mid - 1;
+  }
+  const CdefSearchDesc& d = ds[fi];
+  const CdefGreedy* g = d.g;
+  const int nfb = d.fb_rows * d.fb_cols, stride = d.cdef_stride;
   const int m = 1 << g->best_bits;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = eg - d.table0;
   if (e == 0) {
-    res[0] = int32_t(g->nb);
-    res[1] = g->best_bits;
+    d.res[0] = int32_t(g->nb);
+    d.res[1] = g->best_bits;
     for (int i = 0; i < 8; i++) {
-      res[2 + i] = i < m ? g->set_y[i] : 0;
-      res[10 + i] = i < m ? g->set_uv[i] : 0;
+      d.res[2 + i] = i < m ? g->set_y[i] : 0;
+      d.res[10 + i] = i < m ? g->set_uv[i] : 0;
     }
   }
-  if (e >= d.fb_rows * stride) return;
   const int r = e / stride, c = e - r * stride;
-  int8_t v = cdef_idx[e];
+  int8_t v = d.cdef_idx[e];
   if (c < d.fb_cols && v >= 0) {
     const int b = r * d.fb_cols + c;
     uint64_t best = ~uint64_t(0);
@@ -198,7 +212,7 @@ __global__ void cdef_greedy_finish_kernel(const CdefSearchDesc d, const CdefGree
     }
     v = int8_t(pick);
   }
-  table[e] = v;
+  d.table[e] = v;
 }
 
 // Squared error of one plane pair over rows [4*blockIdx.x, +4) of job
@@ -262,15 +276,13 @@ __global__ void __launch_bounds__(256) plane_sse_kernel(const SseJobs jobs, int 
 
 }  // namespace
 
-void launch_cdef_greedy_step(const CdefSearchDesc& d, CdefGreedy* g, uint64_t* tot, double lambda, cudaStream_t s) {
-  const int ncand = d.ny * d.nuv;
-  launch_pdl(cdef_greedy_step_kernel, (ncand + 7) / 8, 256, 0, s, d, g, lambda, tot);
+void launch_cdef_greedy_step(const CdefSearchDesc* ds, int n, int ncand, cudaStream_t s) {
+  const int cpf = (ncand + 7) / 8;
+  launch_pdl(cdef_greedy_step_kernel, n * cpf, 256, 0, s, ds, cpf);
 }
 
-void launch_cdef_greedy_finish(const CdefSearchDesc& d, const CdefGreedy* g, const int8_t* cdef_idx, int stride,
-                               int8_t* table, int32_t* res, cudaStream_t s) {
-  const int n = d.fb_rows * stride;
-  launch_pdl(cdef_greedy_finish_kernel, (n + 255) / 256, 256, 0, s, d, g, cdef_idx, stride, table, res);
+void launch_cdef_greedy_finish(const CdefSearchDesc* ds, int n, int total, cudaStream_t s) {
+  launch_pdl(cdef_greedy_finish_kernel, (total + 255) / 256, 256, 0, s, ds, n, total);
 }
 
 void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s) {

@@ -281,3 +281,45 @@ def test_searches_random_configurations(ctx, seed):
     eff, llam = int(rng.integers(0, 3)), float(rng.choice([0.0, 40.0, 500.0, -1e9]))
     assert gpu_lr_search(ctx, sf, lcur, lcdef, lsrc, llam, eff) == O.lr_search(sf, lcur, lcdef, lsrc, llam, eff), \
         f"lr {cfg} effort {eff} lambda {llam}"
+
+
+@pytest.mark.parametrize("thorough", [False, True], ids=["fast", "thorough"])
+def test_cdef_search_many_matches_per_frame_oracle(ctx, thorough):
+    """A batch of frames of different shapes, formats, q and lambda in one
+    call: each frame's result, table and block errors equal the oracle's
+    per-frame search."""
+    cfgs = [dict(width=640, height=360, bit_depth=10, seed=71), dict(width=200, height=120, bit_depth=8,
+                                                                      sample_bytes=1, seed=72),
+            dict(width=136, height=72, bit_depth=12, subsampling_x=0, subsampling_y=0, seed=73),
+            dict(width=120, height=80, bit_depth=10, mono=1, seed=74),
+            dict(width=72, height=40, bit_depth=10, subsampling_x=1, subsampling_y=0, seed=75),
+            dict(width=1920, height=1080, bit_depth=10, seed=76)]
+    sfs = [A.SynthHandle(**c) for c in cfgs]
+    idx, _, _ = coding_blocks(sfs[4])
+    idx[:] = -1  # one frame without coding blocks
+    keep, jobs, want = [], (A.CdefSearchJob * len(sfs))(), []
+    ny, nuv = A.CDEF_SEARCH_N[thorough]
+    for i, sf in enumerate(sfs):
+        cur, src = O.search_inputs(sf, 80 + i, amp=8 << (sf.f.info.bit_depth - 8))
+        q, lam = 40 * i + 10, [0.0, 5.0, 60.0, 900.0, 2.0, 40.0][i]
+        want.append(O.cdef_search(sf, cur, src, q, lam, thorough))
+        info = sf.f.info
+        df = G.DevFrame(sf)
+        dcur, dsrc = G.DevPlanes.from_host(info, cur), G.DevPlanes.from_host(info, src)
+        fbr, fbc = (info.mi_rows + 15) // 16, (info.mi_cols + 15) // 16
+        res = A.CdefSearchResult()
+        table = np.zeros(fbr * df.maps.cdef_stride, np.int8)
+        sse = np.zeros((fbr * fbc, ny + nuv), np.uint64)
+        keep.append((sf, df, dcur, dsrc, res, table, sse))
+        jobs[i].info = C.pointer(info)
+        jobs[i].maps = C.pointer(df.maps)
+        jobs[i].cur = C.cast(dcur.c, C.POINTER(A.Plane))
+        jobs[i].src = C.cast(dsrc.c, C.POINTER(A.Plane))
+        jobs[i].base_q_idx = q
+        jobs[i].lam = lam
+        jobs[i].result = C.pointer(res)
+        jobs[i].cdef_idx_out = table.ctypes.data
+        jobs[i].block_sse = sse.ctypes.data
+    A.check(A.lib().av1pf_cdef_search_many(ctx.p, len(sfs), jobs, int(thorough), None), "av1pf_cdef_search_many")
+    for i, (sf, df, dcur, dsrc, res, table, sse) in enumerate(keep):
+        assert_cdef_same((res, table, sse), want[i], f"batch frame {i}")
