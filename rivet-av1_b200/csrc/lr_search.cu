@@ -35,6 +35,7 @@ namespace {
 constexpr int kB = 3;            // window border (postfilter.rs:744 LRB)
 constexpr int kSgrCachePx = 6144;  // filter outputs kept between the fit and its error (units up to 96 x 64)
 constexpr int kThreads = 256;
+constexpr int kWienerChunk = 4;  // rows of Wiener terms handed from the producing warps to the adding lanes at a time
 __constant__ int32_t kSgrParams[16][4] = AV1T_SGR_PARAMS;
 __constant__ int32_t kWienerMin[3] = AV1T_WIENER_TAPS_MIN, kWienerMax[3] = AV1T_WIENER_TAPS_MAX;
 __constant__ int32_t kXqdMin[2] = AV1T_SGRPROJ_XQD_MIN, kXqdMax[2] = AV1T_SGRPROJ_XQD_MAX;
@@ -330,7 +331,7 @@ size_t lr_window_bytes(int wmax, int hmax) {
 size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px) {
   const size_t win = lr_window_bytes(wmax, hmax);
   if (kind == 0) return win;                                                   // prep
-  if (kind == 1) return win + size_t(2) * 4 * size_t(wmax + 1) * sizeof(double);  // Wiener passes
+  if (kind == 1) return win + size_t(2) * 4 * kWienerChunk * size_t(wmax + 1) * sizeof(double);  // Wiener passes
   // self-guided: A/B of both passes, the band's box sums, the filter-output cache
   return win + size_t(4) * (band + 2) * size_t(wmax + 2) * sizeof(int32_t) +
          size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) + size_t(cache_px) * 2 * sizeof(int32_t) +
@@ -463,10 +464,11 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
   const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
   const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
-  // [2][4][wmax + 1]: d0 d1 d2 t (the odd row stride puts the four terms of
-  // a sample on different banks for the accumulating lanes)
+  // [2 buffers][4 terms: d0 d1 d2 t][kWienerChunk rows][wmax + 1]: the odd
+  // row stride puts the four terms of a sample on different banks for the
+  // accumulating lanes
   double* terms = reinterpret_cast<double*>(sm.region);
-  const int ts = d.wmax + 1;
+  const int ts = d.wmax + 1, tq_stride = kWienerChunk * ts;
   for (int iter = 1; iter < 3; iter++) {
     const bool vertical = iter == 2;
     if (tid < 3) s_other[tid] = vertical ? hc[tid] : vc[tid];
@@ -476,27 +478,34 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
       __syncthreads();
       stage_window(d, p, rc, x0, w, sm.win, sm.ws);
       __syncthreads();
-      const int nri = (rc.h + step - 1) / step;
-      for (int rr = 0; rr <= nri; rr++) {
-        if (rr < nri && warp > 0) {
-          double* tb = terms + (rr & 1) * 4 * ts;
-          const int i = rr * step;
-          for (int jj = tid - 32; jj < nci; jj += blockDim.x - 32) {
-            const int j = jj * step;
+      const int nri = (rc.h + step - 1) / step, nch = (nri + kWienerChunk - 1) / kWienerChunk;
+      // chunks of rows in turn, two buffers: warps 1.. fill chunk c + 1 while
+      // warp 0 adds chunk c, row by row in sample order
+      for (int ch = 0; ch <= nch; ch++) {
+        if (ch < nch && warp > 0) {
+          double* tb = terms + (ch & 1) * 4 * tq_stride;
+          const int rows = min(kWienerChunk, nri - ch * kWienerChunk);
+          for (int k = tid - 32; k < rows * nci; k += blockDim.x - 32) {
+            const int r = k / nci, jj = k - r * nci;
+            const int i = (ch * kWienerChunk + r) * step, j = jj * step;
             double line[7];
             wiener_line(W, vertical, i, j, s_other, line);
             const double two3 = __dmul_rn(2.0, line[3]);
-            tb[0 * ts + jj] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
-            tb[1 * ts + jj] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
-            tb[2 * ts + jj] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
-            tb[3 * ts + jj] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
+            double* tr = tb + r * ts + jj;
+            tr[0 * tq_stride] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
+            tr[1 * tq_stride] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
+            tr[2 * tq_stride] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
+            tr[3 * tq_stride] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
           }
         }
-        if (rr > 0 && owner) {
-          const double* tb = terms + ((rr - 1) & 1) * 4 * ts;
-          const double* ta = tb + qa * ts;
-          const double* tq = tb + qb * ts;
-          for (int jj = 0; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
+        if (ch > 0 && owner) {
+          const double* tb = terms + ((ch - 1) & 1) * 4 * tq_stride;
+          const int rows = min(kWienerChunk, nri - (ch - 1) * kWienerChunk);
+          for (int r = 0; r < rows; r++) {
+            const double* ta = tb + qa * tq_stride + r * ts;
+            const double* tq = tb + qb * tq_stride + r * ts;
+            for (int jj = 0; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
+          }
         }
         __syncthreads();
       }
