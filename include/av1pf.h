@@ -562,6 +562,25 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info,
                     av1pf_lr_unit* const units_out[3],
                     int32_t frame_type_out[3], void* stream);
 
+/* One frame of av1pf_lr_search_many: the arguments of av1pf_lr_search, with
+ * its outputs inside. */
+typedef struct av1pf_lr_search_job {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_plane* cur;   /* device */
+  const av1pf_plane* cdef;  /* device */
+  const av1pf_plane* src;   /* device */
+  double lambda;
+  av1pf_lr_unit* units_out[3];  /* host, or NULL per plane */
+  int32_t frame_type_out[3];    /* written */
+} av1pf_lr_search_job;
+
+/* av1pf_lr_search for n frames (shapes may differ, one effort) in one call:
+ * every frame's units run in the same launches. Each frame's result equals
+ * that of av1pf_lr_search on it. n <= 4096. */
+int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs,
+                         int32_t effort, void* stream);
+
 /* search_lf (encoder/mod.rs:1457-1506): the loop-filter levels with the
  * least error. `params` carries the starting levels (loop_filter_level) and
  * the other loop-filter fields the filter reads; `cur` (device, left

@@ -118,8 +118,15 @@ struct CdefSearchDesc {
 // The encoder's loop-restoration search (encoder/lr.rs:64-430): one job
 // per restoration unit, its stripe rectangles, and the chosen filter.
 struct LrSearchJob {
-  int32_t plane, x0, w;  // unit columns x0 .. x0 + w - 1
-  int32_t r0, nr;        // rectangles r0 .. r0 + nr - 1 (one per stripe)
+  int32_t frame, plane, x0, w;  // unit columns x0 .. x0 + w - 1
+  int32_t r0, nr;               // rectangles r0 .. r0 + nr - 1 (one per stripe)
+};
+// One frame of a (batched) loop-restoration search.
+struct LrSearchFrame {
+  DPlane cur[3], cdef[3], src[3];  // deblocked frame, CDEF output, source
+  int32_t bd, sb;
+  int32_t pex[3], pey[3];  // last column / row of each plane
+  double lambda;
 };
 struct LrSearchRect {
   int32_t ss, se;  // StripeStartY, StripeEndY
@@ -138,14 +145,11 @@ struct LrSgrResult {
   uint64_t sse;
 };
 struct LrSearchDesc {
-  DPlane cur[3], cdef[3], src[3];  // deblocked frame, CDEF output, source
-  int32_t bd, sb;
-  int32_t pex[3], pey[3];  // last column / row of each plane
+  const LrSearchFrame* frames;
   int32_t wmax, hmax;      // the widest unit and tallest rectangle
   int32_t step;            // fit on every step-th row and column
   int32_t band, cache_px;  // self-guided rows per band; filter outputs kept per unit
   int32_t nsets, sets[16];
-  double lambda;
   const LrSearchJob* jobs;
   const LrSearchRect* rects;
   LrJobState* state;   // one per job

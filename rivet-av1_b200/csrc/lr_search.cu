@@ -58,7 +58,7 @@ struct Win {
 };
 
 // lr_window (postfilter.rs:765-777) of rectangle `rc` into shared memory.
-__device__ void stage_window(const LrSearchDesc& d, int p, const LrSearchRect& rc, int x0, int w, int16_t* win,
+__device__ void stage_window(const LrSearchFrame& d, int p, const LrSearchRect& rc, int x0, int w, int16_t* win,
                              int ws, int16_t* srcw = nullptr) {
   // a warp per window row, lanes along it (no index division), eight rows'
   // loads in flight before their stores; with `srcw`, the rectangle's source
@@ -377,7 +377,8 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
   extern __shared__ __align__(16) uint8_t lrs_smem[];
   __shared__ int64_t red[kThreads / 32];
   const LrSearchJob job = d.jobs[blockIdx.x];
-  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const LrSearchFrame& F = d.frames[job.frame];
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, tid = threadIdx.x, step = d.step;
   const Smem sm = smem_of(lrs_smem, d);
   const Win W{sm.win, sm.ws};
   const LrSearchRect* rects = d.rects + job.r0;
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
     const LrSearchRect rc = rects[ri];
     for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
       for (int j = tid & 31; j < w; j += 32) {
-        const int e = ld(d.cdef[p], sb, x0 + j, rc.y0 + i) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+        const int e = ld(F.cdef[p], sb, x0 + j, rc.y0 + i) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
         acc += int64_t(e) * e;
       }
   }
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
     __syncthreads();
-    stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+    stage_window(F, p, rc, x0, w, sm.win, sm.ws);
     __syncthreads();
     const int nri = (rc.h + step - 1) / step;
     for (int k = tid; k < nri * nci; k += blockDim.x) {
@@ -405,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
       int ln[7];
 #pragma unroll
       for (int t = 0; t < 7; t++) ln[t] = W.at(i + t, j + kB);
-      const int64_t tg = ld(d.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
+      const int64_t tg = ld(F.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
       const int64_t d0 = ln[0] + ln[6] - 2 * ln[3], d1 = ln[1] + ln[5] - 2 * ln[3], d2 = ln[2] + ln[4] - 2 * ln[3];
       m00 += d0 * d0;
       m01 += d0 * d1;
@@ -451,14 +452,15 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   __shared__ double s_m[3][3], s_v[3], s_other[3];
   __shared__ int s_coef[2][3];
   const LrSearchJob job = d.jobs[blockIdx.x];
-  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const LrSearchFrame& F = d.frames[job.frame];
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, tid = threadIdx.x, step = d.step;
   const int lane = tid & 31, warp = tid >> 5;
   const Smem sm = smem_of(lrs_smem, d);
   const Win W{sm.win, sm.ws};
   const LrSearchRect* rects = d.rects + job.r0;
   LrJobState& st = d.state[blockIdx.x];
   const int first = p == 0 ? 0 : 1;
-  const int bd = d.bd, maxv = (1 << bd) - 1;
+  const int bd = F.bd, maxv = (1 << bd) - 1;
   double vc[3] = {st.vc[0], st.vc[1], st.vc[2]}, hc[3] = {0.0, 0.0, 0.0};
   const int nci = (w + step - 1) / step;
   const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
@@ -476,7 +478,7 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+      stage_window(F, p, rc, x0, w, sm.win, sm.ws);
       __syncthreads();
       const int nri = (rc.h + step - 1) / step, nch = (nri + kWienerChunk - 1) / kWienerChunk;
       // chunks of rows in turn, two buffers: warps 1.. fill chunk c + 1 while
@@ -495,7 +497,7 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
             tr[0 * tq_stride] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
             tr[1 * tq_stride] = __dsub_rn(__dadd_rn(line[1], line[5]), two3);
             tr[2 * tq_stride] = __dsub_rn(__dadd_rn(line[2], line[4]), two3);
-            tr[3 * tq_stride] = __dsub_rn(double(ld(d.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
+            tr[3 * tq_stride] = __dsub_rn(double(ld(F.src[p], sb, x0 + j, rc.y0 + i)), line[3]);
           }
         }
         if (ch > 0 && owner) {
@@ -560,12 +562,12 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
     __syncthreads();
-    stage_window(d, p, rc, x0, w, sm.win, sm.ws);
+    stage_window(F, p, rc, x0, w, sm.win, sm.ws);
     __syncthreads();
     for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
       for (int j = tid & 31; j < w; j += 32) {
         const int e =
-            wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(d.src[p], sb, x0 + j, rc.y0 + i);
+            wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
         acc += int64_t(e) * e;
       }
   }
@@ -584,10 +586,11 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
 // thread (rare: very large units with large errors at 12 bits, where the
 // exact integer sums could round differently); the thread rebuilds each
 // rectangle's window itself.
-__device__ __noinline__ void sgr_fit_in_order(const LrSearchDesc& d, const LrSearchJob& job, const LrSearchRect* rects,
+__device__ __noinline__ void sgr_fit_in_order(const LrSearchDesc& d, const LrSearchFrame& F, const LrSearchJob& job,
+                                              const LrSearchRect* rects,
                                               const Win& W, const Smem& sm, const SgrPass& q0, const SgrPass& q1,
                                               double& m00, double& m01, double& m11, double& v0, double& v1) {
-  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, step = d.step, bd = d.bd;
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, step = d.step, bd = F.bd;
   const int r0 = q0.r, r1 = q1.r;
   m00 = m01 = m11 = v0 = v1 = 0.0;
   for (int ri = 0; ri < job.nr; ri++) {
@@ -595,19 +598,19 @@ __device__ __noinline__ void sgr_fit_in_order(const LrSearchDesc& d, const LrSea
     const int ww = w + 2 * kB, wh = rc.h + 2 * kB;
     for (int k = 0; k < ww * wh; k++) {
       const int rr = k / ww, c = k - rr * ww;
-      const int x = max(min(x0 + c - kB, d.pex[p]), 0), y = max(min(rc.y0 + rr - kB, d.pey[p]), 0);
-      sm.win[rr * sm.ws + c] = int16_t(y < rc.ss   ? ld(d.cur[p], sb, x, max(rc.ss - 2, y))
-                                       : y > rc.se ? ld(d.cur[p], sb, x, min(rc.se + 2, y))
-                                                   : ld(d.cdef[p], sb, x, y));
+      const int x = max(min(x0 + c - kB, F.pex[p]), 0), y = max(min(rc.y0 + rr - kB, F.pey[p]), 0);
+      sm.win[rr * sm.ws + c] = int16_t(y < rc.ss   ? ld(F.cur[p], sb, x, max(rc.ss - 2, y))
+                                       : y > rc.se ? ld(F.cur[p], sb, x, min(rc.se + 2, y))
+                                                   : ld(F.cdef[p], sb, x, y));
     }
     for (int i = 0; i < rc.h; i += step)
       for (int j = 0; j < w; j += step) {
         const int yabs = rc.y0 + i;
-        const int cval = ld(d.cdef[p], sb, x0 + j, yabs);
+        const int cval = ld(F.cdef[p], sb, x0 + j, yabs);
         const double u = double(cval << 4);
         const double a = r0 ? __dsub_rn(double(sgr_flt_direct(W, 0, q0, bd, yabs, i, j, cval)), u) : 0.0;
         const double b = r1 ? __dsub_rn(double(sgr_flt_direct(W, 1, q1, bd, yabs, i, j, cval)), u) : 0.0;
-        const double t = __dmul_rn(128.0, __dsub_rn(double(ld(d.src[p], sb, x0 + j, yabs) << 4), u));
+        const double t = __dmul_rn(128.0, __dsub_rn(double(ld(F.src[p], sb, x0 + j, yabs) << 4), u));
         m00 = __dadd_rn(m00, __dmul_rn(a, a));
         m01 = __dadd_rn(m01, __dmul_rn(a, b));
         m11 = __dadd_rn(m11, __dmul_rn(b, b));
@@ -627,11 +630,12 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
   __shared__ int s_xqd[2];
   const int ji = blockIdx.x / d.nsets, si = blockIdx.x - ji * d.nsets;
   const LrSearchJob job = d.jobs[ji];
-  const int p = job.plane, x0 = job.x0, w = job.w, sb = d.sb, tid = threadIdx.x, step = d.step;
+  const LrSearchFrame& F = d.frames[job.frame];
+  const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, tid = threadIdx.x, step = d.step;
   const Smem sm = smem_of(lrs_smem, d);
   const Win W{sm.win, sm.ws};
   const LrSearchRect* rects = d.rects + job.r0;
-  const int bd = d.bd, maxv = (1 << bd) - 1;
+  const int bd = F.bd, maxv = (1 << bd) - 1;
   const int set = d.sets[si];
   const SgrPass q0 = sgr_pass(set, 0), q1 = sgr_pass(set, 1);
   const int r0 = q0.r, r1 = q1.r;
@@ -669,13 +673,13 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
           for (int j = tid & 31; j < w; j += 32) {
           const int k = i * w + j;
           // one rectangle: its window and source are still staged
-          const int u = (job.nr == 1 ? W.at(i + kB, j + kB) : ld(d.cdef[p], sb, x0 + j, rc.y0 + i)) << 4;
+          const int u = (job.nr == 1 ? W.at(i + kB, j + kB) : ld(F.cdef[p], sb, x0 + j, rc.y0 + i)) << 4;
           const int fl0 = cache[2 * (off + k)], fl1 = cache[2 * (off + k) + 1];
           int32_t val = pw1 * u;
           val += r0 ? pw0 * fl0 : pw0 * u;
           val += r1 ? pw2 * fl1 : pw2 * u;
           const int out = min(max(round2(val, 4 + 7), 0), maxv);
-          const int e = out - (job.nr == 1 ? srcw[k] : ld(d.src[p], sb, x0 + j, rc.y0 + i));
+          const int e = out - (job.nr == 1 ? srcw[k] : ld(F.src[p], sb, x0 + j, rc.y0 + i));
           acc += int64_t(e) * e;
           }
         off += rc.h * w;
@@ -686,7 +690,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      stage_window(d, p, rc, x0, w, sm.win, sm.ws, srcw);
+      stage_window(F, p, rc, x0, w, sm.win, sm.ws, srcw);
       for (int i0 = 0; i0 < rc.h; i0 += band) {
         const int rows = min(band, rc.h - i0);
         __syncthreads();
@@ -752,7 +756,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
         v0 = double(tg0);
         v1 = double(tg1);
       } else {
-        sgr_fit_in_order(d, job, rects, W, sm, q0, q1, m00, m01, m11, v0, v1);
+        sgr_fit_in_order(d, F, job, rects, W, sm, q0, q1, m00, m01, m11, v0, v1);
       }
       double w0, w2;
       if (r0 && r1) {
@@ -798,9 +802,10 @@ __global__ void lr_search_choose_kernel(const LrSearchDesc d, int njobs) {
   if (ji >= njobs) return;
   const LrJobState& st = d.state[ji];
   const int p = d.jobs[ji].plane;
+  const LrSearchFrame& F = d.frames[d.jobs[ji].frame];
   av1pf_lr_unit best{};
-  double best_cost = __dadd_rn(__ull2double_rn(st.none), d.lambda);
-  double cost = __dadd_rn(__ull2double_rn(st.wiener), __dmul_rn(d.lambda, p == 0 ? 40.0 : 28.0));
+  double best_cost = __dadd_rn(__ull2double_rn(st.none), F.lambda);
+  double cost = __dadd_rn(__ull2double_rn(st.wiener), __dmul_rn(F.lambda, p == 0 ? 40.0 : 28.0));
   if (cost < best_cost) {
     best_cost = cost;
     best.type = AV1PF_RESTORE_WIENER;
@@ -809,7 +814,7 @@ __global__ void lr_search_choose_kernel(const LrSearchDesc d, int njobs) {
   }
   for (int si = 0; si < d.nsets; si++) {
     const LrSgrResult& r = d.sgr[ji * d.nsets + si];
-    cost = __dadd_rn(__ull2double_rn(r.sse), __dmul_rn(d.lambda, 20.0));
+    cost = __dadd_rn(__ull2double_rn(r.sse), __dmul_rn(F.lambda, 20.0));
     if (cost < best_cost) {
       best_cost = cost;
       best = av1pf_lr_unit{};

@@ -374,32 +374,13 @@ int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
   return AV1PF_OK;
 }
 
-int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
-                    const av1pf_plane* cur, const av1pf_plane* cdef, const av1pf_plane* src, double lambda,
-                    int32_t effort, av1pf_lr_unit* const units_out[3], int32_t frame_type_out[3], void* stream) {
+int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs_in, int32_t effort, void* stream) {
   int rc = enter(ctx);
   if (rc) return rc;
-  if (!params) return fail_input("null params");
-  // the unit grid as a frame whose planes all use switchable restoration
-  av1pf_params q = *params;
-  q.uses_lr = 1;
-  for (int k = 0; k < 3; k++) q.frame_restoration_type[k] = 3;
-  q.cdef_enabled = 0;
-  std::string why;
-  if ((rc = validate_frame(info, &q, nullptr, &why)) != AV1PF_OK) return set_error(why), rc;
-  if ((rc = check_visible(info, cur, "null deblocked planes")) != AV1PF_OK ||
-      (rc = check_visible(info, cdef, "null CDEF planes")) != AV1PF_OK ||
-      (rc = check_visible(info, src, "null source planes")) != AV1PF_OK)
-    return rc;
+  if (n <= 0 || n > 4096 || !jobs_in) return fail_input("bad job count");
   if (effort < 0 || effort > 2) return fail_input("effort must be 0 (fast), 1 (normal) or 2 (thorough)");
-  if (!std::isfinite(lambda)) return fail_input("lambda must be finite");
-  if (!units_out || !frame_type_out) return fail_input("null outputs");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int np = info->num_planes;
-
   LrSearchDesc d{};
-  d.bd = info->bit_depth;
-  d.sb = info->sample_bytes;
   // encoder/lr.rs:74-81: parameter sets and the fit's sampling step
   static const int kNormal[6] = {0, 3, 6, 10, 13, 14}, kFast[2] = {3, 10};
   if (effort == 2) {
@@ -413,45 +394,70 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
     for (int k = 0; k < 2; k++) d.sets[k] = kFast[k];
   }
   d.step = effort == 0 ? 2 : 1;
-  d.lambda = lambda;
-  // jobs: every unit with a stripe and columns inside the plane (encoder/lr.rs:84-122)
+  std::vector<LrSearchFrame> frames(static_cast<size_t>(n));
+  std::vector<av1pf_params> grids(static_cast<size_t>(n));
   std::vector<LrSearchJob> jobs;
   std::vector<LrSearchRect> rects;
-  std::vector<std::array<int, 3>> where;  // (plane, unit row, unit column) of each job
-  const int stripes = (info->frame_height + 8 + 63) / 64;
-  for (int p = 0; p < np; p++) {
-    const int sx = p ? info->subsampling_x : 0, sy = p ? info->subsampling_y : 0;
-    d.cur[p] = dplane(cur[p]);
-    d.cdef[p] = dplane(cdef[p]);
-    d.src[p] = dplane(src[p]);
-    d.pex[p] = ((info->upscaled_width + sx) >> sx) - 1;
-    d.pey[p] = ((info->frame_height + sy) >> sy) - 1;
-    const int us = q.loop_restoration_size[p], urows = q.lr_unit_rows[p], ucols = q.lr_unit_cols[p];
-    // lr_stripe (postfilter.rs:640-661): each stripe's unit row
-    std::vector<std::vector<LrSearchRect>> by_row(static_cast<size_t>(urows));
-    for (int st = 0; st < stripes; st++) {
-      const int ss = (-8 + st * 64) >> sy, se = ss + (64 >> sy) - 1;
-      const int y0 = std::max(ss, 0), y1 = std::min(se, d.pey[p]);
-      if (y0 > y1) continue;
-      const int luma_row = st * 64 >= 8 ? st * 64 - 8 : 0;
-      const int ur = std::min(urows - 1, ((luma_row + 8) >> sy) / us);
-      by_row[size_t(ur)].push_back(LrSearchRect{ss, se, y0, y1 - y0 + 1});
-    }
-    for (int ur = 0; ur < urows; ur++)
-      for (int uc = 0; uc < ucols; uc++) {
-        // lr_unit_cols (postfilter.rs:664-675)
-        const int x0 = uc * us;
-        const int x1 = uc + 1 == ucols ? d.pex[p] : std::min((uc + 1) * us - 1, d.pex[p]);
-        if (x0 > d.pex[p] || by_row[size_t(ur)].empty()) continue;
-        LrSearchJob jb{p, x0, x1 - x0 + 1, int32_t(rects.size()), int32_t(by_row[size_t(ur)].size())};
-        for (const LrSearchRect& r : by_row[size_t(ur)]) {
-          rects.push_back(r);
-          d.hmax = std::max(d.hmax, r.h);
-        }
-        d.wmax = std::max(d.wmax, jb.w);
-        jobs.push_back(jb);
-        where.push_back({p, ur, uc});
+  std::vector<std::array<int, 4>> where;  // (frame, plane, unit row, unit column) of each job
+  std::string why;
+  for (int fi = 0; fi < n; fi++) {
+    const av1pf_lr_search_job& jb = jobs_in[fi];
+    const av1pf_frame_info* info = jb.info;
+    if (!jb.params) return fail_input("null params");
+    // the unit grid as a frame whose planes all use switchable restoration
+    av1pf_params& q = grids[size_t(fi)];
+    q = *jb.params;
+    q.uses_lr = 1;
+    for (int k = 0; k < 3; k++) q.frame_restoration_type[k] = 3;
+    q.cdef_enabled = 0;
+    if ((rc = validate_frame(info, &q, nullptr, &why)) != AV1PF_OK) return set_error(why), rc;
+    if ((rc = check_visible(info, jb.cur, "null deblocked planes")) != AV1PF_OK ||
+        (rc = check_visible(info, jb.cdef, "null CDEF planes")) != AV1PF_OK ||
+        (rc = check_visible(info, jb.src, "null source planes")) != AV1PF_OK)
+      return rc;
+    if (!std::isfinite(jb.lambda)) return fail_input("lambda must be finite");
+    LrSearchFrame& F = frames[size_t(fi)];
+    F = LrSearchFrame{};
+    F.bd = info->bit_depth;
+    F.sb = info->sample_bytes;
+    F.lambda = jb.lambda;
+    const int np = info->num_planes;
+    const int stripes = (info->frame_height + 8 + 63) / 64;
+    for (int p = 0; p < np; p++) {
+      const int sx = p ? info->subsampling_x : 0, sy = p ? info->subsampling_y : 0;
+      F.cur[p] = dplane(jb.cur[p]);
+      F.cdef[p] = dplane(jb.cdef[p]);
+      F.src[p] = dplane(jb.src[p]);
+      F.pex[p] = ((info->upscaled_width + sx) >> sx) - 1;
+      F.pey[p] = ((info->frame_height + sy) >> sy) - 1;
+      const int us = q.loop_restoration_size[p], urows = q.lr_unit_rows[p], ucols = q.lr_unit_cols[p];
+      // lr_stripe (postfilter.rs:640-661): each stripe's unit row
+      std::vector<std::vector<LrSearchRect>> by_row(static_cast<size_t>(urows));
+      for (int st = 0; st < stripes; st++) {
+        const int ss = (-8 + st * 64) >> sy, se = ss + (64 >> sy) - 1;
+        const int y0 = std::max(ss, 0), y1 = std::min(se, F.pey[p]);
+        if (y0 > y1) continue;
+        const int luma_row = st * 64 >= 8 ? st * 64 - 8 : 0;
+        const int ur = std::min(urows - 1, ((luma_row + 8) >> sy) / us);
+        by_row[size_t(ur)].push_back(LrSearchRect{ss, se, y0, y1 - y0 + 1});
       }
+      // jobs: every unit with a stripe and columns inside the plane (encoder/lr.rs:84-122)
+      for (int ur = 0; ur < urows; ur++)
+        for (int uc = 0; uc < ucols; uc++) {
+          // lr_unit_cols (postfilter.rs:664-675)
+          const int x0 = uc * us;
+          const int x1 = uc + 1 == ucols ? F.pex[p] : std::min((uc + 1) * us - 1, F.pex[p]);
+          if (x0 > F.pex[p] || by_row[size_t(ur)].empty()) continue;
+          LrSearchJob job{fi, p, x0, x1 - x0 + 1, int32_t(rects.size()), int32_t(by_row[size_t(ur)].size())};
+          for (const LrSearchRect& r : by_row[size_t(ur)]) {
+            rects.push_back(r);
+            d.hmax = std::max(d.hmax, r.h);
+          }
+          d.wmax = std::max(d.wmax, job.w);
+          jobs.push_back(job);
+          where.push_back({fi, p, ur, uc});
+        }
+    }
   }
   std::vector<av1pf_lr_unit> chosen(jobs.size());
   if (!jobs.empty()) {
@@ -464,18 +470,21 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
     lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px);
     cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px);
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search attributes");
-    const size_t jb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);
+    const size_t fb = frames.size() * sizeof(LrSearchFrame);
+    const size_t jbb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);
     const size_t ob = jobs.size() * sizeof(av1pf_lr_unit);
     const size_t stb = jobs.size() * sizeof(LrJobState), sgb = jobs.size() * size_t(d.nsets) * sizeof(LrSgrResult);
-    const size_t o_rects = align256(jb), o_out = o_rects + align256(rb), o_state = o_out + align256(ob);
-    const size_t o_sgr = o_state + align256(stb), total = o_sgr + align256(sgb);
+    const size_t o_jobs = align256(fb), o_rects = o_jobs + align256(jbb), o_out = o_rects + align256(rb);
+    const size_t o_state = o_out + align256(ob), o_sgr = o_state + align256(stb), total = o_sgr + align256(sgb);
     if ((rc = ctx->ensure(ctx->search_dev, total)) != AV1PF_OK) return rc;
     if ((rc = ctx->ensure_host(ctx->search_host, o_state)) != AV1PF_OK) return rc;
     uint8_t* dv = static_cast<uint8_t*>(ctx->search_dev.ptr);
     uint8_t* hs = static_cast<uint8_t*>(ctx->search_host.ptr);
-    std::memcpy(hs, jobs.data(), jb);
+    std::memcpy(hs, frames.data(), fb);
+    std::memcpy(hs + o_jobs, jobs.data(), jbb);
     std::memcpy(hs + o_rects, rects.data(), rb);
-    d.jobs = reinterpret_cast<const LrSearchJob*>(dv);
+    d.frames = reinterpret_cast<const LrSearchFrame*>(dv);
+    d.jobs = reinterpret_cast<const LrSearchJob*>(dv + o_jobs);
     d.rects = reinterpret_cast<const LrSearchRect*>(dv + o_rects);
     d.out = reinterpret_cast<av1pf_lr_unit*>(dv + o_out);
     d.state = reinterpret_cast<LrJobState*>(dv + o_state);
@@ -489,24 +498,56 @@ int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_pa
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search");
     std::memcpy(chosen.data(), hs + o_out, ob);
   }
-  // the plan: units without a job keep no filter (encoder/lr.rs:188-208)
-  for (int p = 0; p < 3; p++) {
-    frame_type_out[p] = 0;
-    if (p >= np || !units_out[p]) continue;
-    const size_t n = size_t(q.lr_unit_rows[p]) * size_t(q.lr_unit_cols[p]);
-    for (size_t k = 0; k < n; k++) units_out[p][k] = av1pf_lr_unit{};
+  // the plans: units without a job keep no filter (encoder/lr.rs:188-208)
+  for (int fi = 0; fi < n; fi++) {
+    av1pf_lr_search_job& jb = jobs_in[fi];
+    const av1pf_params& q = grids[size_t(fi)];
+    for (int p = 0; p < 3; p++) {
+      jb.frame_type_out[p] = 0;
+      if (p >= jb.info->num_planes || !jb.units_out[p]) continue;
+      const size_t cnt = size_t(q.lr_unit_rows[p]) * size_t(q.lr_unit_cols[p]);
+      for (size_t k = 0; k < cnt; k++) jb.units_out[p][k] = av1pf_lr_unit{};
+    }
   }
-  bool used[3][3] = {};
+  std::vector<std::array<std::array<bool, 3>, 3>> used(static_cast<size_t>(n));
+  for (auto& u : used)
+    for (auto& pl : u) pl = {false, false, false};
   for (size_t k = 0; k < jobs.size(); k++) {
-    const int p = where[k][0];
-    used[p][chosen[k].type] = true;
-    if (units_out[p]) units_out[p][size_t(where[k][1]) * size_t(q.lr_unit_cols[p]) + size_t(where[k][2])] = chosen[k];
+    const int fi = where[k][0], p = where[k][1];
+    av1pf_lr_search_job& jb = jobs_in[fi];
+    used[size_t(fi)][size_t(p)][chosen[k].type] = true;
+    if (jb.units_out[p])
+      jb.units_out[p][size_t(where[k][2]) * size_t(grids[size_t(fi)].lr_unit_cols[p]) + size_t(where[k][3])] =
+          chosen[k];
   }
-  for (int p = 0; p < np; p++) {
-    const bool wu = used[p][AV1PF_RESTORE_WIENER], su = used[p][AV1PF_RESTORE_SGRPROJ];
-    frame_type_out[p] = wu ? (su ? 3 : AV1PF_RESTORE_WIENER) : (su ? AV1PF_RESTORE_SGRPROJ : AV1PF_RESTORE_NONE);
+  for (int fi = 0; fi < n; fi++) {
+    av1pf_lr_search_job& jb = jobs_in[fi];
+    for (int p = 0; p < jb.info->num_planes; p++) {
+      const bool wu = used[size_t(fi)][size_t(p)][AV1PF_RESTORE_WIENER];
+      const bool su = used[size_t(fi)][size_t(p)][AV1PF_RESTORE_SGRPROJ];
+      jb.frame_type_out[p] = wu ? (su ? 3 : AV1PF_RESTORE_WIENER) : (su ? AV1PF_RESTORE_SGRPROJ : AV1PF_RESTORE_NONE);
+    }
   }
   return AV1PF_OK;
+}
+
+int av1pf_lr_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                    const av1pf_plane* cur, const av1pf_plane* cdef, const av1pf_plane* src, double lambda,
+                    int32_t effort, av1pf_lr_unit* const units_out[3], int32_t frame_type_out[3], void* stream) {
+  if (!units_out || !frame_type_out) return fail_input("null outputs");
+  av1pf_lr_search_job job{};
+  job.info = info;
+  job.params = params;
+  job.cur = cur;
+  job.cdef = cdef;
+  job.src = src;
+  job.lambda = lambda;
+  for (int p = 0; p < 3; p++) job.units_out[p] = units_out[p];
+  if (!info) return fail_input("null frame info");
+  const int rc = av1pf_lr_search_many(ctx, 1, &job, effort, stream);
+  if (rc == AV1PF_OK)
+    for (int p = 0; p < 3; p++) frame_type_out[p] = job.frame_type_out[p];
+  return rc;
 }
 
 }  // extern "C"

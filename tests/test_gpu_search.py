@@ -323,3 +323,40 @@ def test_cdef_search_many_matches_per_frame_oracle(ctx, thorough):
     A.check(A.lib().av1pf_cdef_search_many(ctx.p, len(sfs), jobs, int(thorough), None), "av1pf_cdef_search_many")
     for i, (sf, df, dcur, dsrc, res, table, sse) in enumerate(keep):
         assert_cdef_same((res, table, sse), want[i], f"batch frame {i}")
+
+
+@pytest.mark.parametrize("effort", [0, 1, 2], ids=["fast", "normal", "thorough"])
+def test_lr_search_many_matches_per_frame_oracle(ctx, effort):
+    """A batch of frames of different shapes, formats, unit sizes and lambdas
+    in one call: each frame's units and restoration types equal the oracle's
+    per-frame search."""
+    cfgs = [dict(width=256, height=144, bit_depth=10, seed=141, enable_lr=1),
+            dict(width=200, height=120, bit_depth=8, sample_bytes=1, seed=142, enable_lr=1, lr_unit_shift=1),
+            dict(width=136, height=72, bit_depth=12, subsampling_x=0, subsampling_y=0, seed=143, enable_lr=1),
+            dict(width=120, height=80, bit_depth=10, mono=1, seed=144, enable_lr=1),
+            dict(width=600, height=300, bit_depth=12, seed=145, enable_lr=1, lr_unit_shift=2, lr_uv_shift=0)]
+    lams = [0.0, 150.0, -1e12, 40.0, 300.0]
+    keep, want = [], []
+    jobs = (A.LrSearchJob * len(cfgs))()
+    for i, cfg in enumerate(cfgs):
+        sf = A.SynthHandle(**cfg)
+        cur, cdef, src = O.lr_search_inputs(sf, 150 + i)
+        want.append(O.lr_search(sf, cur, cdef, src, lams[i], effort))
+        info, params = sf.f.info, sf.f.params
+        dev = [G.DevPlanes.from_host(info, x) for x in (cur, cdef, src)]
+        arrs = O.lr_unit_arrays(params, info.num_planes)
+        keep.append((sf, dev, arrs))
+        jobs[i].info = C.pointer(info)
+        jobs[i].params = C.pointer(params)
+        jobs[i].cur = C.cast(dev[0].c, C.POINTER(A.Plane))
+        jobs[i].cdef = C.cast(dev[1].c, C.POINTER(A.Plane))
+        jobs[i].src = C.cast(dev[2].c, C.POINTER(A.Plane))
+        jobs[i].lam = lams[i]
+        for p in range(3):
+            jobs[i].units_out[p] = C.cast(arrs[p], C.POINTER(A.LrUnit)) if arrs[p] is not None else None
+    A.check(A.lib().av1pf_lr_search_many(ctx.p, len(cfgs), jobs, effort, None), "av1pf_lr_search_many")
+    for i, (sf, dev, arrs) in enumerate(keep):
+        params = sf.f.params
+        units = [[O.lr_unit_tuple(u) for u in arrs[p][:params.lr_unit_rows[p] * params.lr_unit_cols[p]]]
+                 if arrs[p] is not None else [] for p in range(3)]
+        assert (list(jobs[i].frame_type_out), units) == want[i], f"batch frame {i}"
