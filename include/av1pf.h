@@ -537,6 +537,23 @@ typedef struct av1pf_cdef_search_job {
 int av1pf_cdef_search_many(av1pf_ctx* ctx, int n, const av1pf_cdef_search_job* jobs,
                            int32_t thorough, void* stream);
 
+/* One frame of av1pf_lf_search_many: the arguments of av1pf_lf_search, the
+ * chosen levels written into it. */
+typedef struct av1pf_lf_search_job {
+  const av1pf_frame_info* info;
+  const av1pf_params* params;
+  const av1pf_maps* maps;    /* device */
+  const av1pf_plane* cur;    /* device */
+  const av1pf_plane* src;    /* device */
+  int32_t levels_out[4];     /* written */
+  uint64_t* sse_out;         /* host 6 x 3, or NULL */
+} av1pf_lf_search_job;
+
+/* av1pf_lf_search for n frames in one call: every frame's filtered scales
+ * run as one batch and every error in one launch. Each frame's result
+ * equals that of av1pf_lf_search on it. n <= 1024. */
+int av1pf_lf_search_many(av1pf_ctx* ctx, int n, av1pf_lf_search_job* jobs, void* stream);
+
 /* Effort of the loop-restoration search (encoder/lr.rs:47-58): fast fits
  * on every other row and column and tries 2 self-guided parameter sets,
  * normal 6, thorough all 16. */

@@ -132,6 +132,12 @@ class CdefSearchJob(C.Structure):
                 ("result", C.POINTER(CdefSearchResult)), ("cdef_idx_out", C.c_void_p), ("block_sse", C.c_void_p)]
 
 
+class LfSearchJob(C.Structure):
+    _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("maps", C.POINTER(Maps)),
+                ("cur", C.POINTER(Plane)), ("src", C.POINTER(Plane)), ("levels_out", C.c_int32 * 4),
+                ("sse_out", C.c_void_p)]
+
+
 class LrSearchJob(C.Structure):
     _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("cur", C.POINTER(Plane)),
                 ("cdef", C.POINTER(Plane)), ("src", C.POINTER(Plane)), ("lam", C.c_double),
@@ -227,6 +233,7 @@ def lib():
         _sig(L, "av1pf_cdef_search_many", C.c_int, vp, C.c_int, P(CdefSearchJob), C.c_int32, vp)
         _sig(L, "av1pf_lr_search", C.c_int, vp, P(FrameInfo), P(Params), P(Plane), P(Plane), P(Plane), C.c_double,
              C.c_int32, P(P(LrUnit)), P(C.c_int32), vp)
+        _sig(L, "av1pf_lf_search_many", C.c_int, vp, C.c_int, P(LfSearchJob), vp)
         _sig(L, "av1pf_lr_search_many", C.c_int, vp, C.c_int, P(LrSearchJob), C.c_int32, vp)
         _sig(L, "av1pf_lf_search", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane),
              P(C.c_int32), vp, vp)

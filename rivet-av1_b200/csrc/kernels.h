@@ -79,12 +79,14 @@ void launch_cdef_greedy_step(const CdefSearchDesc* ds, int n, int ncand, cudaStr
 // (`total` table entries over all frames).
 void launch_cdef_greedy_finish(const CdefSearchDesc* ds, int n, int total, cudaStream_t s);
 // Squared error of planes against the source over each plane's frame area:
-// sse[i] += sum over plane job i (a[i], b[i]: plane pointers, strides).
+// sse[i] += sum over plane job i (a, b: plane pointers and strides; `jobs`
+// in device memory, at most 65535).
 struct SsePlane {
   const uint8_t* a;
   const uint8_t* b;
   int64_t sa, sb_;  // strides in samples
   int32_t w, h;
+  int32_t sb;       // bytes per sample
 };
 // The loop-restoration search (lr_search.cu): per unit job, a prep kernel
 // and the in-order Wiener passes on `s`, the self-guided fits (one CTA per
@@ -96,7 +98,7 @@ void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px);
 cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px);
 void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                       cudaEvent_t join);
-void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s);
+void launch_plane_sse(const SsePlane* jobs, int n, int rows_max, uint64_t* sse, cudaStream_t s);
 
 // Super-resolution (superres.cu)
 // `row_max`: the most source samples in a row among the launch's frames.

@@ -266,112 +266,164 @@ int av1pf_cdef_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_
   return av1pf_cdef_search_many(ctx, 1, &job, thorough, stream);
 }
 
-int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
-                    const av1pf_maps* maps, const av1pf_plane* cur, const av1pf_plane* src, int32_t levels_out[4],
-                    uint64_t* sse_out, void* stream) {
+int av1pf_lf_search_many(av1pf_ctx* ctx, int n, av1pf_lf_search_job* jobs, void* stream) {
   int rc = enter(ctx);
   if (rc) return rc;
-  std::string why;
-  if (!params) return fail_input("null params");
-  if ((rc = validate_frame(info, params, cur, &why)) != AV1PF_OK) return set_error(why), rc;
-  if ((rc = check_src(info, src)) != AV1PF_OK) return rc;
-  if (!maps || !maps->mi || maps->mi_stride < info->mi_cols) return fail_input("mi map missing or mi_stride < mi_cols");
-  for (int p = 0; p < info->num_planes; p++)
-    if (!maps->lf_tx_size[p]) return fail_input("lf_tx_size map missing");
-  if (!levels_out) return fail_input("null levels_out");
+  if (n <= 0 || n > 1024 || !jobs) return fail_input("bad job count");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int np = info->num_planes, sb = info->sample_bytes;
-
+  std::string why;
   // the six scales of the starting levels (encoder/mod.rs:1470-1472)
   static const double kScales[6] = {0.0, 0.5, 0.75, 1.0, 1.25, 1.5};
-  int32_t levels[6][4];
-  for (int si = 0; si < 6; si++)
-    for (int k = 0; k < 4; k++)
-      levels[si][k] = std::min(int32_t(std::round(double(params->loop_filter_level[k]) * kScales[si])), 63);
-  // a filtered copy of `cur` for each scale that filters
-  size_t frame_bytes = 0;
-  size_t plane_off[3] = {0, 0, 0};
-  for (int p = 0; p < np; p++) {
-    plane_off[p] = frame_bytes;
-    frame_bytes += align256(size_t(cur[p].height) * size_t(cur[p].stride) * size_t(sb));
-  }
-  std::vector<int> filtered;
-  for (int si = 0; si < 6; si++)
-    if (levels[si][0] || levels[si][1]) filtered.push_back(si);
-  if ((rc = ctx->ensure(ctx->search_planes, std::max<size_t>(1, filtered.size()) * frame_bytes)) != AV1PF_OK) return rc;
-  if ((rc = ctx->ensure(ctx->search_dev, 256)) != AV1PF_OK) return rc;
-  if ((rc = ctx->ensure_host(ctx->search_host, 256)) != AV1PF_OK) return rc;
-  uint8_t* base = static_cast<uint8_t*>(ctx->search_planes.ptr);
-  std::vector<av1pf_params> prm(filtered.size(), *params);
-  std::vector<std::array<av1pf_plane, 3>> planes(filtered.size());
-  std::vector<FrameJob> jobs;
-  cudaError_t e = cudaSuccess;
-  for (size_t i = 0; i < filtered.size(); i++) {
-    for (int k = 0; k < 4; k++) prm[i].loop_filter_level[k] = levels[filtered[i]][k];
-    for (int p = 0; p < np; p++) {
-      uint8_t* dst = base + i * frame_bytes + plane_off[p];
-      const size_t bytes = size_t(cur[p].height) * size_t(cur[p].stride) * size_t(sb);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(dst, cur[p].data, bytes, cudaMemcpyDeviceToDevice, s);
-      planes[i][size_t(p)] = cur[p];
-      planes[i][size_t(p)].data = dst;
+  struct Frame {
+    int32_t levels[6][4];
+    size_t bytes, plane_off[3];
+    int filtered[6];  // index of the filtered copy of each scale, or -1
+  };
+  std::vector<Frame> fr(static_cast<size_t>(n));
+  size_t copy_bytes = 0;
+  int copies = 0;
+  for (int fi = 0; fi < n; fi++) {
+    const av1pf_lf_search_job& jb = jobs[fi];
+    const av1pf_frame_info* info = jb.info;
+    if (!jb.params) return fail_input("null params");
+    if ((rc = validate_frame(info, jb.params, jb.cur, &why)) != AV1PF_OK) return set_error(why), rc;
+    if ((rc = check_src(info, jb.src)) != AV1PF_OK) return rc;
+    const av1pf_maps* maps = jb.maps;
+    if (!maps || !maps->mi || maps->mi_stride < info->mi_cols) return fail_input("mi map missing or mi_stride < mi_cols");
+    for (int p = 0; p < info->num_planes; p++)
+      if (!maps->lf_tx_size[p]) return fail_input("lf_tx_size map missing");
+    Frame& F = fr[size_t(fi)];
+    F.bytes = 0;
+    for (int p = 0; p < info->num_planes; p++) {
+      F.plane_off[p] = F.bytes;
+      F.bytes += align256(size_t(jb.cur[p].height) * size_t(jb.cur[p].stride) * size_t(info->sample_bytes));
     }
-    jobs.push_back(FrameJob{info, &prm[i], maps, planes[i].data(), nullptr, planes[i].data(), nullptr, ST_LF, true});
+    for (int si = 0; si < 6; si++) {
+      for (int k = 0; k < 4; k++)
+        F.levels[si][k] = std::min(int32_t(std::round(double(jb.params->loop_filter_level[k]) * kScales[si])), 63);
+      F.filtered[si] = (F.levels[si][0] || F.levels[si][1]) ? copies++ : -1;
+      if (F.filtered[si] >= 0) copy_bytes += F.bytes;
+    }
+  }
+  // filtered copies, one per (frame, scale that filters), filtered in place as one batch
+  if ((rc = ctx->ensure(ctx->search_planes, std::max<size_t>(1, copy_bytes))) != AV1PF_OK) return rc;
+  uint8_t* base = static_cast<uint8_t*>(ctx->search_planes.ptr);
+  std::vector<uint8_t*> copy_at(static_cast<size_t>(copies));
+  std::vector<av1pf_params> prm(static_cast<size_t>(copies));
+  std::vector<std::array<av1pf_plane, 3>> planes(static_cast<size_t>(copies));
+  std::vector<FrameJob> fjobs;
+  cudaError_t e = cudaSuccess;
+  size_t at = 0;
+  for (int fi = 0; fi < n; fi++) {
+    const av1pf_lf_search_job& jb = jobs[fi];
+    const Frame& F = fr[size_t(fi)];
+    for (int si = 0; si < 6; si++) {
+      const int ci = F.filtered[si];
+      if (ci < 0) continue;
+      copy_at[size_t(ci)] = base + at;
+      prm[size_t(ci)] = *jb.params;
+      for (int k = 0; k < 4; k++) prm[size_t(ci)].loop_filter_level[k] = F.levels[si][k];
+      for (int p = 0; p < jb.info->num_planes; p++) {
+        uint8_t* dst = base + at + F.plane_off[p];
+        const size_t bytes = size_t(jb.cur[p].height) * size_t(jb.cur[p].stride) * size_t(jb.info->sample_bytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dst, jb.cur[p].data, bytes, cudaMemcpyDeviceToDevice, s);
+        planes[size_t(ci)][size_t(p)] = jb.cur[p];
+        planes[size_t(ci)][size_t(p)].data = dst;
+      }
+      fjobs.push_back(FrameJob{jb.info, &prm[size_t(ci)], jb.maps, planes[size_t(ci)].data(), nullptr,
+                               planes[size_t(ci)].data(), nullptr, ST_LF, true});
+      at += F.bytes;
+    }
   }
   if (e != cudaSuccess) return cuda_status(e, "loop-filter search copies");
-  if (!jobs.empty() && (rc = ctx->run(jobs.data(), int(jobs.size()), s)) != AV1PF_OK) return rc;
-  // the errors of every (scale, plane) in one launch
+  if (!fjobs.empty() && (rc = ctx->run(fjobs.data(), int(fjobs.size()), s)) != AV1PF_OK) return rc;
+  // the errors of every (frame, scale, plane) in one launch
   std::vector<SsePlane> sj;
   int rows_max = 0;
-  for (int si = 0; si < 6; si++) {
-    const auto it = std::find(filtered.begin(), filtered.end(), si);
-    for (int p = 0; p < np; p++) {
-      const int sx = p ? info->subsampling_x : 0, sy = p ? info->subsampling_y : 0;
-      SsePlane j{};
-      j.a = it == filtered.end() ? static_cast<const uint8_t*>(cur[p].data)
-                                 : base + size_t(it - filtered.begin()) * frame_bytes + plane_off[p];
-      j.b = static_cast<const uint8_t*>(src[p].data);
-      j.sa = cur[p].stride;
-      j.sb_ = src[p].stride;
-      j.w = (info->frame_width + sx) >> sx;
-      j.h = (info->frame_height + sy) >> sy;
-      rows_max = std::max(rows_max, j.h);
-      sj.push_back(j);
-    }
+  for (int fi = 0; fi < n; fi++) {
+    const av1pf_lf_search_job& jb = jobs[fi];
+    const av1pf_frame_info* info = jb.info;
+    const Frame& F = fr[size_t(fi)];
+    for (int si = 0; si < 6; si++)
+      for (int p = 0; p < info->num_planes; p++) {
+        const int sx = p ? info->subsampling_x : 0, sy = p ? info->subsampling_y : 0;
+        SsePlane j{};
+        j.a = F.filtered[si] < 0 ? static_cast<const uint8_t*>(jb.cur[p].data)
+                                 : copy_at[size_t(F.filtered[si])] + F.plane_off[p];
+        j.b = static_cast<const uint8_t*>(jb.src[p].data);
+        j.sa = jb.cur[p].stride;
+        j.sb_ = jb.src[p].stride;
+        j.w = (info->frame_width + sx) >> sx;
+        j.h = (info->frame_height + sy) >> sy;
+        j.sb = info->sample_bytes;
+        rows_max = std::max(rows_max, j.h);
+        sj.push_back(j);
+      }
   }
-  uint64_t* dsse = static_cast<uint64_t*>(ctx->search_dev.ptr);
-  uint64_t* hsse = static_cast<uint64_t*>(ctx->search_host.ptr);
-  e = cudaMemsetAsync(dsse, 0, 18 * sizeof(uint64_t), s);
+  const size_t jb_bytes = sj.size() * sizeof(SsePlane), o_sse = align256(jb_bytes);
+  const size_t total = o_sse + align256(sj.size() * sizeof(uint64_t));
+  if ((rc = ctx->ensure(ctx->search_dev, total)) != AV1PF_OK) return rc;
+  if ((rc = ctx->ensure_host(ctx->search_host, total)) != AV1PF_OK) return rc;
+  uint8_t* dv = static_cast<uint8_t*>(ctx->search_dev.ptr);
+  uint8_t* hs = static_cast<uint8_t*>(ctx->search_host.ptr);
+  std::memcpy(hs, sj.data(), jb_bytes);
+  e = cudaMemcpyAsync(dv, hs, jb_bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dv + o_sse, 0, sj.size() * sizeof(uint64_t), s);
   if (e != cudaSuccess) return cuda_status(e, "loop-filter search");
-  launch_plane_sse(sj.data(), int(sj.size()), sb, rows_max, dsse, s);
-  e = cudaMemcpyAsync(hsse, dsse, 18 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+  launch_plane_sse(reinterpret_cast<const SsePlane*>(dv), int(sj.size()), rows_max,
+                   reinterpret_cast<uint64_t*>(dv + o_sse), s);
+  e = cudaMemcpyAsync(hs + o_sse, dv + o_sse, sj.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_status(e, "loop-filter search");
-
   // each plane's level with the least error, the first scale on ties
   // (encoder/mod.rs:1477-1492)
-  uint64_t best_e[3] = {UINT64_MAX, UINT64_MAX, UINT64_MAX};
-  int32_t best_l[3] = {0, 0, 0};
-  for (int si = 0; si < 6; si++)
-    for (int p = 0; p < np; p++) {
-      const uint64_t err = hsse[si * np + p];
-      if (sse_out) sse_out[si * 3 + p] = err;
-      if (err < best_e[p]) {
-        best_e[p] = err;
-        best_l[p] = p == 0 ? levels[si][0] : levels[si][1 + p];
-      }
-    }
-  if (sse_out)
+  const uint64_t* hsse = reinterpret_cast<const uint64_t*>(hs + o_sse);
+  size_t k = 0;
+  for (int fi = 0; fi < n; fi++) {
+    av1pf_lf_search_job& jb = jobs[fi];
+    const int np = jb.info->num_planes;
+    const Frame& F = fr[size_t(fi)];
+    uint64_t best_e[3] = {UINT64_MAX, UINT64_MAX, UINT64_MAX};
+    int32_t best_l[3] = {0, 0, 0};
+    if (jb.sse_out)
+      for (int q = 0; q < 18; q++) jb.sse_out[q] = 0;
     for (int si = 0; si < 6; si++)
-      for (int p = np; p < 3; p++) sse_out[si * 3 + p] = 0;
-  if (best_l[0] == 0) {
-    for (int k = 0; k < 4; k++) levels_out[k] = 0;
-  } else {
-    levels_out[0] = levels_out[1] = best_l[0];
-    levels_out[2] = best_l[1];
-    levels_out[3] = best_l[2];
+      for (int p = 0; p < np; p++) {
+        const uint64_t err = hsse[k++];
+        if (jb.sse_out) jb.sse_out[si * 3 + p] = err;
+        if (err < best_e[p]) {
+          best_e[p] = err;
+          best_l[p] = p == 0 ? F.levels[si][0] : F.levels[si][1 + p];
+        }
+      }
+    if (best_l[0] == 0) {
+      for (int q = 0; q < 4; q++) jb.levels_out[q] = 0;
+    } else {
+      jb.levels_out[0] = jb.levels_out[1] = best_l[0];
+      jb.levels_out[2] = best_l[1];
+      jb.levels_out[3] = best_l[2];
+    }
   }
   return AV1PF_OK;
+}
+
+int av1pf_lf_search(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_params* params,
+                    const av1pf_maps* maps, const av1pf_plane* cur, const av1pf_plane* src, int32_t levels_out[4],
+                    uint64_t* sse_out, void* stream) {
+  if (!levels_out) return fail_input("null levels_out");
+  av1pf_lf_search_job job{};
+  job.info = info;
+  job.params = params;
+  job.maps = maps;
+  job.cur = cur;
+  job.src = src;
+  job.sse_out = sse_out;
+  if (!info) return fail_input("null frame info");
+  const int rc = av1pf_lf_search_many(ctx, 1, &job, stream);
+  if (rc == AV1PF_OK)
+    for (int q = 0; q < 4; q++) levels_out[q] = job.levels_out[q];
+  return rc;
 }
 
 int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs_in, int32_t effort, void* stream) {

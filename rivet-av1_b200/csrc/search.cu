@@ -218,12 +218,9 @@ __global__ void cdef_greedy_finish_kernel(const CdefSearchDesc* __restrict__ ds,
 // Squared error of one plane pair over rows [4*blockIdx.x, +4) of job
 // blockIdx.y: 16-byte loads (planes and rows are 16-byte aligned), the
 // ragged end of a row sample by sample.
-struct SseJobs {
-  SsePlane p[18];
-};
-
-__global__ void __launch_bounds__(256) plane_sse_kernel(const SseJobs jobs, int sb, uint64_t* __restrict__ sse) {
-  const SsePlane j = jobs.p[blockIdx.y];
+__global__ void __launch_bounds__(256) plane_sse_kernel(const SsePlane* __restrict__ jobs, uint64_t* __restrict__ sse) {
+  const SsePlane j = jobs[blockIdx.y];
+  const int sb = j.sb;
   const int y0 = blockIdx.x * 4;
   uint64_t acc = 0;
   if (y0 < j.h) {
@@ -285,11 +282,9 @@ void launch_cdef_greedy_finish(const CdefSearchDesc* ds, int n, int total, cudaS
   launch_pdl(cdef_greedy_finish_kernel, (total + 255) / 256, 256, 0, s, ds, n, total);
 }
 
-void launch_plane_sse(const SsePlane* jobs, int n, int sample_bytes, int rows_max, uint64_t* sse, cudaStream_t s) {
+void launch_plane_sse(const SsePlane* jobs, int n, int rows_max, uint64_t* sse, cudaStream_t s) {
   if (n <= 0 || rows_max <= 0) return;
-  SseJobs j{};
-  for (int i = 0; i < n && i < 18; i++) j.p[i] = jobs[i];
-  plane_sse_kernel<<<dim3(unsigned((rows_max + 3) / 4), unsigned(n)), 256, 0, s>>>(j, sample_bytes, sse);
+  plane_sse_kernel<<<dim3(unsigned((rows_max + 3) / 4), unsigned(n)), 256, 0, s>>>(jobs, sse);
   note_launch();
 }
 

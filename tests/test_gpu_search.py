@@ -360,3 +360,37 @@ def test_lr_search_many_matches_per_frame_oracle(ctx, effort):
         units = [[O.lr_unit_tuple(u) for u in arrs[p][:params.lr_unit_rows[p] * params.lr_unit_cols[p]]]
                  if arrs[p] is not None else [] for p in range(3)]
         assert (list(jobs[i].frame_type_out), units) == want[i], f"batch frame {i}"
+
+
+def test_lf_search_many_matches_per_frame_oracle(ctx):
+    """A batch of frames of different shapes, formats and starting levels in
+    one call: each frame's levels and errors equal the oracle's search."""
+    cfgs = [dict(width=256, height=144, bit_depth=10, seed=171), dict(width=200, height=120, bit_depth=8,
+                                                                       sample_bytes=1, seed=172),
+            dict(width=136, height=72, bit_depth=12, subsampling_x=0, subsampling_y=0, seed=173),
+            dict(width=120, height=80, bit_depth=10, mono=1, seed=174),
+            dict(width=640, height=360, bit_depth=10, subsampling_x=1, subsampling_y=0, seed=175)]
+    keep, want = [], []
+    jobs = (A.LfSearchJob * len(cfgs))()
+    for i, cfg in enumerate(cfgs):
+        sf = A.SynthHandle(**cfg)
+        cur, src = O.search_inputs(sf, 180 + i, amp=(10 + 8 * i) << (sf.f.info.bit_depth - 8))
+        p = A.Params.from_buffer_copy(sf.f.params)
+        for k, v in enumerate(((8, 8, 4, 4), (30, 30, 20, 20), (63, 50, 63, 0), (12, 0, 5, 5), (0, 0, 9, 9))[i]):
+            p.loop_filter_level[k] = v
+        want.append(O.lf_search(sf, cur, src, params=p))
+        info = sf.f.info
+        df = G.DevFrame(sf)
+        dcur, dsrc = G.DevPlanes.from_host(info, cur), G.DevPlanes.from_host(info, src)
+        sse = np.zeros((6, 3), np.uint64)
+        keep.append((sf, p, df, dcur, dsrc, sse))
+        jobs[i].info = C.pointer(info)
+        jobs[i].params = C.pointer(p)
+        jobs[i].maps = C.pointer(df.maps)
+        jobs[i].cur = C.cast(dcur.c, C.POINTER(A.Plane))
+        jobs[i].src = C.cast(dsrc.c, C.POINTER(A.Plane))
+        jobs[i].sse_out = sse.ctypes.data
+    A.check(A.lib().av1pf_lf_search_many(ctx.p, len(cfgs), jobs, None), "av1pf_lf_search_many")
+    for i, (sf, p, df, dcur, dsrc, sse) in enumerate(keep):
+        assert list(jobs[i].levels_out) == want[i][0], f"batch frame {i}"
+        assert np.array_equal(sse, want[i][1]), f"batch frame {i}"
