@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
         for (int ir = tid >> 5; ir < rows; ir += blockDim.x >> 5)
           for (int j = tid & 31; j < w; j += 32) {
           const int i = i0 + ir, yabs = rc.y0 + i;
-          const bool fit_px = (i % step) == 0 && (j % step) == 0;
+          const bool fit_px = ((i | j) & (step - 1)) == 0;  // step is 1 or 2
           if (pass_sse == 0 && !fit_px && !cached) continue;
           const int cval = W.at(i + kB, j + kB);  // the rectangle's rows lie in its stripe: CDEF output
           const int u = cval << 4;  // SGRPROJ_RST_BITS
