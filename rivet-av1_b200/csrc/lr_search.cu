@@ -401,8 +401,9 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
     stage_window(F, p, rc, x0, w, sm.win, sm.ws);
     __syncthreads();
     const int nri = (rc.h + step - 1) / step;
-    for (int k = tid; k < nri * nci; k += blockDim.x) {
-      const int i = (k / nci) * step, j = (k % nci) * step;
+    for (int ii = tid >> 5; ii < nri; ii += blockDim.x >> 5)
+      for (int jj = tid & 31; jj < nci; jj += 32) {
+      const int i = ii * step, j = jj * step;
       int ln[7];
 #pragma unroll
       for (int t = 0; t < 7; t++) ln[t] = W.at(i + t, j + kB);
@@ -417,7 +418,7 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
       v0 += d0 * tg;
       v1 += d1 * tg;
       v2 += d2 * tg;
-    }
+      }
   }
   const int64_t sums[9] = {m00, m01, m02, m11, m12, m22, v0, v1, v2};
   double tot[9];
