@@ -277,9 +277,10 @@ __device__ const LrsA2 g_lrs_a2 = make_lrs_a2();
 // their squares (int32: 25 squares of 12-bit samples fit), then the
 // vertical sums. Pass 0 computes odd absolute rows only (the others have
 // weight 0). `hs`/`hq` hold (rows + 2 + 2r) x (w + 2) sums.
-__device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
-                            int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
-  const int r = q.r, cw = w + 2;
+template <int r>
+__device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
+                              int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+  const int cw = w + 2;
   const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
   const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();  // the previous users of hs / hq are done
@@ -288,6 +289,7 @@ __device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, in
     for (int aj = lane; aj < cw; aj += 32) {
       const int wx = aj + kB - 1;
       int32_t sum = 0, sq = 0;
+#pragma unroll
       for (int dx = -r; dx <= r; dx++) {
         const int v = W.at(wy, wx + dx);
         sum += v;
@@ -303,6 +305,7 @@ __device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, in
     if (pass == 0 && ((y0 + i0 + ir - 1) & 1) == 0) continue;
     for (int aj = lane; aj < cw; aj += 32) {
       int32_t bs = 0, as = 0;
+#pragma unroll
       for (int dy = 0; dy <= 2 * r; dy++) {
         bs += hs[(ir + dy) * cw + aj];
         as += hq[(ir + dy) * cw + aj];
@@ -318,6 +321,15 @@ __device__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, in
       Bb[ir * aw + aj] = int32_t((b2 + (1 << 11)) >> 12);  // SGRPROJ_RECIP_BITS
     }
   }
+}
+
+// The band's A/B for the pass's radius (1 or 2): the box sums' loops unrolled.
+__device__ __forceinline__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows,
+                                            int w, int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+  if (q.r == 2)
+    sgr_band_ab_r<2>(W, q, pass, bd, y0, i0, rows, w, Ab, Bb, aw, hs, hq);
+  else
+    sgr_band_ab_r<1>(W, q, pass, bd, y0, i0, rows, w, Ab, Bb, aw, hs, hq);
 }
 
 }  // namespace
