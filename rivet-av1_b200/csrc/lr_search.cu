@@ -280,6 +280,8 @@ __device__ const LrsA2 g_lrs_a2 = make_lrs_a2();
 template <int r>
 __device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
                               int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+  // n and 1/n follow from the radius (sgr_pass computes the same values)
+  constexpr int n = (2 * r + 1) * (2 * r + 1), one_over_n = ((1 << 12) + n / 2) / n;
   const int cw = w + 2;
   const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
   const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -313,10 +315,10 @@ __device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, 
       // a * n and dd^2 stay below 2^31 (25 * 25 * 255^2); p * s needs 64 bits
       const int32_t a = round2(as, sh);
       const int32_t dd = round2(bs, bd - 8);
-      const int32_t p = max(a * q.n - dd * dd, 0);
+      const int32_t p = max(a * n - dd * dd, 0);
       const int64_t z = (int64_t(p) * q.s + (int64_t(1) << 19)) >> 20;  // SGRPROJ_MTABLE_BITS
       const int32_t a2 = g_lrs_a2.v[z < 255 ? int(z) : 255];
-      const int64_t b2 = int64_t((256 - a2) * bs) * q.one_over_n;
+      const int64_t b2 = int64_t((256 - a2) * bs) * one_over_n;
       Ab[ir * aw + aj] = a2;
       Bb[ir * aw + aj] = int32_t((b2 + (1 << 11)) >> 12);  // SGRPROJ_RECIP_BITS
     }
