@@ -16,9 +16,9 @@
 // sum of the terms' magnitudes stays below 2^53: they are summed in int64
 // in parallel (the self-guided sums check that bound and otherwise redo the
 // sum in order on one thread). The second and third Wiener passes have
-// real-valued terms, so their sums run in the reference's order: warps 1-7
-// produce a row's terms into shared memory while lanes of warp 0 each add
-// one accumulator's terms in sample order. Every f64 operation is a
+// real-valued terms, so their sums run in the reference's order: warps 1-3
+// produce four rows of terms at a time into shared memory while lanes of
+// warp 0 each add one accumulator's terms in sample order. Every f64 operation is a
 // round-to-nearest multiply, add or divide in the reference's order (this
 // file is compiled without floating-point contraction, and the sums use
 // the explicit _rn intrinsics).
@@ -148,14 +148,16 @@ __device__ __forceinline__ void wiener_line(const Win& W, bool vertical, int i, 
 #pragma unroll
   for (int t = 0; t < 7; t++) {
     const int r = vertical ? i + t : i + kB, c = vertical ? j + kB : j + t;
-    const double center = double(W.at(r, c));
-    double s = center;
+    const int center = W.at(r, c);
+    double s = double(center);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const int dd = 3 - k;
-      const double a = double(vertical ? W.at(r, c - dd) : W.at(r - dd, c));
-      const double b = double(vertical ? W.at(r, c + dd) : W.at(r + dd, c));
-      s = __dadd_rn(s, __dmul_rn(other[k], __dsub_rn(__dadd_rn(a, b), __dmul_rn(2.0, center))));
+      const int a = vertical ? W.at(r, c - dd) : W.at(r - dd, c);
+      const int b = vertical ? W.at(r, c + dd) : W.at(r + dd, c);
+      // a + b - 2 * center is an integer below 2^17: the f64 expression of
+      // encoder/lr.rs is exact, so integer arithmetic gives the same value
+      s = __dadd_rn(s, __dmul_rn(other[k], double(a + b - 2 * center)));
     }
     line[t] = s;
   }
@@ -502,11 +504,12 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
         if (ch < nch && warp > 0) {
           double* tb = terms + (ch & 1) * 4 * tq_stride;
           const int rows = min(kWienerChunk, nri - ch * kWienerChunk);
+          const double oth[3] = {s_other[0], s_other[1], s_other[2]};
           for (int k = tid - 32; k < rows * nci; k += blockDim.x - 32) {
             const int r = k / nci, jj = k - r * nci;
             const int i = (ch * kWienerChunk + r) * step, j = jj * step;
             double line[7];
-            wiener_line(W, vertical, i, j, s_other, line);
+            wiener_line(W, vertical, i, j, oth, line);
             const double two3 = __dmul_rn(2.0, line[3]);
             double* tr = tb + r * ts + jj;
             tr[0 * tq_stride] = __dsub_rn(__dadd_rn(line[0], line[6]), two3);
