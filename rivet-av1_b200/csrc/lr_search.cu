@@ -36,6 +36,7 @@ constexpr int kB = 3;            // window border (postfilter.rs:744 LRB)
 constexpr int kSgrCachePx = 6144;  // filter outputs kept between the fit and its error (units up to 96 x 64)
 constexpr int kThreads = 256;
 constexpr int kWienerChunk = 4;  // rows of Wiener terms handed from the producing warps to the adding lanes at a time
+constexpr int kWienerErrBand = 32;  // output rows per band of the Wiener error pass (its int16 rows fit the term region)
 __constant__ int32_t kSgrParams[16][4] = AV1T_SGR_PARAMS;
 __constant__ int32_t kWienerMin[3] = AV1T_WIENER_TAPS_MIN, kWienerMax[3] = AV1T_WIENER_TAPS_MAX;
 __constant__ int32_t kXqdMin[2] = AV1T_SGRPROJ_XQD_MIN, kXqdMax[2] = AV1T_SGRPROJ_XQD_MAX;
@@ -161,20 +162,6 @@ __device__ __forceinline__ void wiener_line(const Win& W, bool vertical, int i, 
     }
     line[t] = s;
   }
-}
-
-// One restored Wiener sample (postfilter.rs:781-822) at (i, j) of the window.
-__device__ __forceinline__ int wiener_px(const Win& W, int i, int j, const int (&hf)[7], const int (&vf)[7], int round0,
-                                         int round1, int off, int lim, int maxv) {
-  int s = 0;
-#pragma unroll
-  for (int t = 0; t < 7; t++) {
-    int h = 0;
-#pragma unroll
-    for (int u = 0; u < 7; u++) h += hf[u] * W.at(i + t, j + u);
-    s += vf[t] * clip3(-off, lim - off, round2(h, round0));
-  }
-  return min(max(round2(s, round1), 0), maxv);
 }
 
 // One self-guided A/B pair (postfilter.rs:918-948) at A/B position (ai, aj)
@@ -576,18 +563,36 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   }
   const int round0 = bd == 12 ? 5 : 3, round1 = bd == 12 ? 9 : 11;
   const int off = 1 << (bd + 7 - round0 - 1), lim = (1 << (bd + 1 + 7 - round0)) - 1;
+  // separable: each band's horizontally filtered window rows go to the term
+  // region as int16 (clipped to [-off, lim - off], within [-2^13, 2^15)),
+  // then the vertical taps run over them
+  int16_t* hrow = reinterpret_cast<int16_t*>(sm.region);
+  const int nw = blockDim.x >> 5;
   int64_t acc = 0;
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
     __syncthreads();
     stage_window(F, p, rc, x0, w, sm.win, sm.ws);
-    __syncthreads();
-    for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
-      for (int j = tid & 31; j < w; j += 32) {
-        const int e =
-            wiener_px(W, i, j, hf, vf, round0, round1, off, lim, maxv) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
-        acc += int64_t(e) * e;
-      }
+    for (int i0 = 0; i0 < rc.h; i0 += kWienerErrBand) {
+      const int rows = min(kWienerErrBand, rc.h - i0);
+      __syncthreads();  // the window is staged; the previous band's rows are read
+      for (int r = warp; r < rows + 2 * kB; r += nw)
+        for (int j = lane; j < w; j += 32) {
+          int h = 0;
+#pragma unroll
+          for (int u = 0; u < 7; u++) h += hf[u] * W.at(i0 + r, j + u);
+          hrow[r * w + j] = int16_t(clip3(-off, lim - off, round2(h, round0)));
+        }
+      __syncthreads();
+      for (int ir = warp; ir < rows; ir += nw)
+        for (int j = lane; j < w; j += 32) {
+          int sv = 0;
+#pragma unroll
+          for (int t = 0; t < 7; t++) sv += vf[t] * hrow[(ir + t) * w + j];
+          const int e = min(max(round2(sv, round1), 0), maxv) - ld(F.src[p], sb, x0 + j, rc.y0 + i0 + ir);
+          acc += int64_t(e) * e;
+        }
+    }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
