@@ -109,6 +109,25 @@ __device__ int64_t block_sum_i64(int64_t v, int64_t* red) {
   return t;
 }
 
+// Block sums of N 64-bit values in one round (every thread gets the totals).
+template <int N>
+__device__ void block_sums_i64(int64_t (&v)[N], int64_t (*red)[kThreads / 32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    if (lane == 0) red[q][warp] = v[q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+    int64_t t = 0;
+    for (int k = 0; k < nw; k++) t += red[q][k];
+    v[q] = t;
+  }
+}
+
 // Gaussian elimination with partial pivoting (encoder/lr.rs:212-233): the
 // last row of largest magnitude is the pivot (Iterator::max_by); zeros when
 // singular.
@@ -378,7 +397,7 @@ __device__ __forceinline__ Smem smem_of(uint8_t* base, const LrSearchDesc& d) {
 // are exact integer sums in any order) and its solve.
 __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSearchDesc d) {
   extern __shared__ __align__(16) uint8_t lrs_smem[];
-  __shared__ int64_t red[kThreads / 32];
+  __shared__ int64_t red10[10][kThreads / 32];
   const LrSearchJob job = d.jobs[blockIdx.x];
   const LrSearchFrame& F = d.frames[job.frame];
   const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, tid = threadIdx.x, step = d.step;
@@ -386,23 +405,20 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
   const Win W{sm.win, sm.ws};
   const LrSearchRect* rects = d.rects + job.r0;
   LrJobState& st = d.state[blockIdx.x];
-  int64_t acc = 0;
-  for (int ri = 0; ri < job.nr; ri++) {
-    const LrSearchRect rc = rects[ri];
-    for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
-      for (int j = tid & 31; j < w; j += 32) {
-        const int e = ld(F.cdef[p], sb, x0 + j, rc.y0 + i) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
-        acc += int64_t(e) * e;
-      }
-  }
-  const int64_t none = block_sum_i64(acc, red);
-  int64_t m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
+  int64_t acc = 0, m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
   const int nci = (w + step - 1) / step;
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
     __syncthreads();
     stage_window(F, p, rc, x0, w, sm.win, sm.ws);
     __syncthreads();
+    // no filter: the window's interior is the rectangle's CDEF output (its
+    // rows lie in its stripe, its columns in the plane)
+    for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
+      for (int j = tid & 31; j < w; j += 32) {
+        const int e = W.at(i + kB, j + kB) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
+        acc += int64_t(e) * e;
+      }
     const int nri = (rc.h + step - 1) / step;
     for (int ii = tid >> 5; ii < nri; ii += blockDim.x >> 5)
       for (int jj = tid & 31; jj < nci; jj += 32) {
@@ -423,12 +439,13 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
       v2 += d2 * tg;
       }
   }
-  const int64_t sums[9] = {m00, m01, m02, m11, m12, m22, v0, v1, v2};
+  int64_t sums[10] = {m00, m01, m02, m11, m12, m22, v0, v1, v2, acc};
+  block_sums_i64(sums, red10);
   double tot[9];
 #pragma unroll
-  for (int q = 0; q < 9; q++) tot[q] = double(block_sum_i64(sums[q], red));
+  for (int q = 0; q < 9; q++) tot[q] = double(sums[q]);
   if (tid == 0) {
-    st.none = uint64_t(none);
+    st.none = uint64_t(sums[9]);
     double sol[3] = {0.0, 0.0, 0.0};
     if (p == 0) {
       double m[3][3] = {{tot[0], tot[1], tot[2]}, {tot[1], tot[3], tot[4]}, {tot[2], tot[4], tot[5]}};
