@@ -528,7 +528,17 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
           for (int r = 0; r < rows; r++) {
             const double* ta = tb + qa * tq_stride + r * ts;
             const double* tq = tb + qb * tq_stride + r * ts;
-            for (int jj = 0; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
+            // the products of 8 terms are independent of the sum: form them
+            // first, then add them one after another in sample order
+            int jj = 0;
+            for (; jj + 8 <= nci; jj += 8) {
+              double pr[8];
+#pragma unroll
+              for (int u = 0; u < 8; u++) pr[u] = __dmul_rn(ta[jj + u], tq[jj + u]);
+#pragma unroll
+              for (int u = 0; u < 8; u++) macc = __dadd_rn(macc, pr[u]);
+            }
+            for (; jj < nci; jj++) macc = __dadd_rn(macc, __dmul_rn(ta[jj], tq[jj]));
           }
         }
         __syncthreads();
