@@ -149,6 +149,7 @@ struct LrSearchDesc {
   int32_t wmax, hmax;      // the widest unit and tallest rectangle
   int32_t step;            // fit on every step-th row and column
   int32_t band, cache_px;  // self-guided rows per band; filter outputs kept per unit
+  int32_t both;            // 1: radius-2 and radius-1 box sums from one sweep (their buffers fit)
   int32_t nsets, sets[16];
   const LrSearchJob* jobs;
   const LrSearchRect* rects;

@@ -285,31 +285,15 @@ __device__ const LrsA2 g_lrs_a2 = make_lrs_a2();
 // their squares (int32: 25 squares of 12-bit samples fit), then the
 // vertical sums. Pass 0 computes odd absolute rows only (the others have
 // weight 0). `hs`/`hq` hold (rows + 2 + 2r) x (w + 2) sums.
+// The vertical half: A/B rows 0 .. rows + 1 of the band from the window
+// rows' horizontal sums `hs`/`hq` (rows + 2 + 2r rows of stride w + 2).
 template <int r>
-__device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
-                              int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+__device__ __forceinline__ void sgr_vert_ab(const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
+                                            int32_t* Ab, int32_t* Bb, int aw, const int32_t* hs, const int32_t* hq) {
   // n and 1/n follow from the radius (sgr_pass computes the same values)
   constexpr int n = (2 * r + 1) * (2 * r + 1), one_over_n = ((1 << 12) + n / 2) / n;
   const int cw = w + 2;
-  const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
   const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();  // the previous users of hs / hq are done
-  for (int rr = warp; rr < nrow; rr += nw) {
-    const int wy = wy0 + rr;
-    for (int aj = lane; aj < cw; aj += 32) {
-      const int wx = aj + kB - 1;
-      int32_t sum = 0, sq = 0;
-#pragma unroll
-      for (int dx = -r; dx <= r; dx++) {
-        const int v = W.at(wy, wx + dx);
-        sum += v;
-        sq += v * v;
-      }
-      hs[rr * cw + aj] = sum;
-      hq[rr * cw + aj] = sq;
-    }
-  }
-  __syncthreads();
   const int sh = 2 * (bd - 8);
   for (int ir = warp; ir < rows + 2; ir += nw) {
     if (pass == 0 && ((y0 + i0 + ir - 1) & 1) == 0) continue;
@@ -333,6 +317,70 @@ __device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, 
   }
 }
 
+// Fills A/B rows for output rows [i0, i0 + rows) of a rectangle (A/B rows
+// i0 .. i0 + rows + 1) for one pass (postfilter.rs:918-948), with separable
+// box sums: first each window row's horizontal sums of the samples and of
+// their squares (int32: 25 squares of 12-bit samples fit), then the
+// vertical sums. Pass 0 computes odd absolute rows only (the others have
+// weight 0). `hs`/`hq` hold (rows + 2 + 2r) x (w + 2) sums.
+template <int r>
+__device__ void sgr_band_ab_r(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows, int w,
+                              int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
+  const int cw = w + 2;
+  const int nrow = rows + 2 + 2 * r, wy0 = i0 + kB - 1 - r;
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // the previous users of hs / hq are done
+  for (int rr = warp; rr < nrow; rr += nw) {
+    const int wy = wy0 + rr;
+    for (int aj = lane; aj < cw; aj += 32) {
+      const int wx = aj + kB - 1;
+      int32_t sum = 0, sq = 0;
+#pragma unroll
+      for (int dx = -r; dx <= r; dx++) {
+        const int v = W.at(wy, wx + dx);
+        sum += v;
+        sq += v * v;
+      }
+      hs[rr * cw + aj] = sum;
+      hq[rr * cw + aj] = sq;
+    }
+  }
+  __syncthreads();
+  sgr_vert_ab<r>(q, pass, bd, y0, i0, rows, w, Ab, Bb, aw, hs, hq);
+}
+
+// Both passes of a band (pass 0 of radius 2, pass 1 of radius 1) from one
+// horizontal sweep: a row's 3-wide sums are the middle of its 5-wide ones.
+// `hs5`/`hq5` hold rows + 6 rows, `hs3`/`hq3` rows + 4 (window rows one
+// lower).
+__device__ void sgr_band_ab_both(const Win& W, const SgrPass& q0, const SgrPass& q1, int bd, int y0, int i0, int rows,
+                                 int w, int32_t* Ab0, int32_t* Bb0, int32_t* Ab1, int32_t* Bb1, int aw, int32_t* hs5,
+                                 int32_t* hq5, int32_t* hs3, int32_t* hq3) {
+  const int cw = w + 2;
+  const int nrow = rows + 6, wy0 = i0 + kB - 3;
+  const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();  // the previous users of the sums are done
+  for (int rr = warp; rr < nrow; rr += nw) {
+    const int wy = wy0 + rr;
+    const bool mid = rr >= 1 && rr < nrow - 1;  // also a row of the radius-1 sums (row rr - 1)
+    for (int aj = lane; aj < cw; aj += 32) {
+      const int wx = aj + kB - 1;
+      const int v0 = W.at(wy, wx - 2), v1 = W.at(wy, wx - 1), v2 = W.at(wy, wx), v3 = W.at(wy, wx + 1),
+                v4 = W.at(wy, wx + 2);
+      const int32_t s3 = v1 + v2 + v3, q3 = v1 * v1 + v2 * v2 + v3 * v3;
+      hs5[rr * cw + aj] = s3 + v0 + v4;
+      hq5[rr * cw + aj] = q3 + v0 * v0 + v4 * v4;
+      if (mid) {
+        hs3[(rr - 1) * cw + aj] = s3;
+        hq3[(rr - 1) * cw + aj] = q3;
+      }
+    }
+  }
+  __syncthreads();
+  sgr_vert_ab<2>(q0, 0, bd, y0, i0, rows, w, Ab0, Bb0, aw, hs5, hq5);
+  sgr_vert_ab<1>(q1, 1, bd, y0, i0, rows, w, Ab1, Bb1, aw, hs3, hq3);
+}
+
 // The band's A/B for the pass's radius (1 or 2): the box sums' loops unrolled.
 __device__ __forceinline__ void sgr_band_ab(const Win& W, const SgrPass& q, int pass, int bd, int y0, int i0, int rows,
                                             int w, int32_t* Ab, int32_t* Bb, int aw, int32_t* hs, int32_t* hq) {
@@ -350,27 +398,32 @@ size_t lr_window_bytes(int wmax, int hmax) {
   const size_t ws = size_t(wmax + 2 * kB + 1) & ~size_t(1);
   return ((size_t(hmax + 2 * kB) * ws * 2) + 15) & ~size_t(15);
 }
-size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px) {
+size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px, int both) {
   const size_t win = lr_window_bytes(wmax, hmax);
   if (kind == 0) return win;                                                   // prep
   if (kind == 1) return win + size_t(2) * 4 * kWienerChunk * size_t(wmax + 1) * sizeof(double);  // Wiener passes
   // self-guided: A/B of both passes, the band's box sums, the filter-output cache
   return win + size_t(4) * (band + 2) * size_t(wmax + 2) * sizeof(int32_t) +
-         size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) + size_t(cache_px) * 2 * sizeof(int32_t) +
+         size_t(2) * (band + 6) * size_t(wmax + 2) * sizeof(int32_t) +
+         size_t(both ? 2 : 0) * (band + 4) * size_t(wmax + 2) * sizeof(int32_t) +
+         size_t(cache_px) * 2 * sizeof(int32_t) +
          ((size_t(hmax) * size_t(wmax) * sizeof(int16_t) + 15) & ~size_t(15));
 }
 
-void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px) {
+void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px, int& both) {
   // Filter outputs are kept when every unit's fit fits the cache; then the
   // tallest band that leaves room for two CTAs per SM, else the tallest that
-  // fits at all.
+  // fits at all; the one-sweep box sums where their buffers fit beside that
+  // band.
   constexpr size_t kTwo = 113 * 1024, kLimit = 220 * 1024;
   cache_px = upx_max <= kSgrCachePx ? upx_max : 0;
   for (size_t lim : {kTwo, kLimit})
     for (band = 16; band >= 4; band /= 2)
-      if (lr_search_smem(wmax, hmax, 2, band, cache_px) <= lim) return;
+      for (both = 1; both >= 0; both--)
+        if (lr_search_smem(wmax, hmax, 2, band, cache_px, both) <= lim) return;
   band = 4;
   cache_px = 0;
+  both = 0;
 }
 
 namespace {
@@ -699,7 +752,9 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
   }
   int32_t* hs = reg + 4 * (band + 2) * aw;
   int32_t* hq = hs + (band + 6) * aw;
-  int32_t* cache = hq + (band + 6) * aw;  // [px][2] filter outputs of the unit
+  int32_t* hs3 = hq + (band + 6) * aw;  // the radius-1 sums of the one-sweep box sums
+  int32_t* hq3 = hs3 + (band + 4) * aw;
+  int32_t* cache = d.both ? hq3 + (band + 4) * aw : hs3;  // [px][2] filter outputs of the unit
   int16_t* srcw = reinterpret_cast<int16_t*>(cache + 2 * d.cache_px);  // the rectangle's source samples
   int upx = 0;
   for (int ri = 0; ri < job.nr; ri++) upx += rects[ri].h * w;
@@ -744,8 +799,12 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_sgr_kernel(const LrSear
       for (int i0 = 0; i0 < rc.h; i0 += band) {
         const int rows = min(band, rc.h - i0);
         __syncthreads();
-        if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw, hs, hq);
-        if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw, hs, hq);
+        if (d.both && r0 == 2 && r1 == 1) {
+          sgr_band_ab_both(W, q0, q1, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], Ab[1], Bb[1], aw, hs, hq, hs3, hq3);
+        } else {
+          if (r0) sgr_band_ab(W, q0, 0, bd, rc.y0, i0, rows, w, Ab[0], Bb[0], aw, hs, hq);
+          if (r1) sgr_band_ab(W, q1, 1, bd, rc.y0, i0, rows, w, Ab[1], Bb[1], aw, hs, hq);
+        }
         __syncthreads();
         for (int ir = tid >> 5; ir < rows; ir += blockDim.x >> 5)
           for (int j = tid & 31; j < w; j += 32) {
@@ -877,24 +936,24 @@ __global__ void lr_search_choose_kernel(const LrSearchDesc d, int njobs) {
   d.out[ji] = best;
 }
 
-cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px) {
+cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px, int both) {
   cudaError_t e = cudaFuncSetAttribute(lr_search_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(lr_search_smem(wmax, hmax, 0, band, cache_px)));
+                                       int(lr_search_smem(wmax, hmax, 0, band, cache_px, both)));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(lr_search_wiener_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(lr_search_smem(wmax, hmax, 1, band, cache_px)));
+                             int(lr_search_smem(wmax, hmax, 1, band, cache_px, both)));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(lr_search_sgr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(lr_search_smem(wmax, hmax, 2, band, cache_px)));
+                             int(lr_search_smem(wmax, hmax, 2, band, cache_px, both)));
   return e;
 }
 
 void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                       cudaEvent_t join) {
   if (njobs <= 0) return;
-  const size_t s0 = lr_search_smem(d.wmax, d.hmax, 0, d.band, d.cache_px);
-  const size_t s1 = lr_search_smem(d.wmax, d.hmax, 1, d.band, d.cache_px);
-  const size_t s2 = lr_search_smem(d.wmax, d.hmax, 2, d.band, d.cache_px);
+  const size_t s0 = lr_search_smem(d.wmax, d.hmax, 0, d.band, d.cache_px, d.both);
+  const size_t s1 = lr_search_smem(d.wmax, d.hmax, 1, d.band, d.cache_px, d.both);
+  const size_t s2 = lr_search_smem(d.wmax, d.hmax, 2, d.band, d.cache_px, d.both);
   // the self-guided fits depend on nothing else: they run beside the Wiener passes
   cudaEventRecord(fork, s);
   cudaStreamWaitEvent(side, fork, 0);

@@ -519,8 +519,8 @@ int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs_in, in
       for (int r = 0; r < jb.nr; r++) px += rects[size_t(jb.r0 + r)].h * jb.w;
       upx_max = std::max(upx_max, px);
     }
-    lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px);
-    cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px);
+    lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px, d.both);
+    cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px, d.both);
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search attributes");
     const size_t fb = frames.size() * sizeof(LrSearchFrame);
     const size_t jbb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);
