@@ -552,7 +552,9 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      stage_window(F, p, rc, x0, w, sm.win, sm.ws);
+      // one rectangle: its window, staged for the horizontal pass, stays in
+      // place (the term rows and band rows lie outside it)
+      if (job.nr > 1 || iter == 1) stage_window(F, p, rc, x0, w, sm.win, sm.ws);
       __syncthreads();
       const int nri = (rc.h + step - 1) / step, nch = (nri + kWienerChunk - 1) / kWienerChunk;
       // chunks of rows in turn, two buffers: warps 1.. fill chunk c + 1 while
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   for (int ri = 0; ri < job.nr; ri++) {
     const LrSearchRect rc = rects[ri];
     __syncthreads();
-    stage_window(F, p, rc, x0, w, sm.win, sm.ws);
+    if (job.nr > 1) stage_window(F, p, rc, x0, w, sm.win, sm.ws);  // else still staged
     for (int i0 = 0; i0 < rc.h; i0 += kWienerErrBand) {
       const int rows = min(kWienerErrBand, rc.h - i0);
       __syncthreads();  // the window is staged; the previous band's rows are read
