@@ -136,7 +136,7 @@ struct LrSearchRect {
 // solution, the quantised Wiener coefficients and their error.
 struct LrJobState {
   uint64_t none, wiener;
-  double vc[3];
+  double vc[3];  // first-pass solution of a unit of several rectangles
   int32_t coef[2][3];
 };
 // Per (unit, self-guided set): the projection weights and their error.
@@ -150,6 +150,7 @@ struct LrSearchDesc {
   int32_t step;            // fit on every step-th row and column
   int32_t band, cache_px;  // self-guided rows per band; filter outputs kept per unit
   int32_t both;            // 1: radius-2 and radius-1 box sums from one sweep (their buffers fit)
+  int32_t multi_rect;      // 1: some job has several stripe rectangles (the first-pass kernel runs)
   int32_t nsets, sets[16];
   const LrSearchJob* jobs;
   const LrSearchRect* rects;

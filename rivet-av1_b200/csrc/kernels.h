@@ -88,9 +88,11 @@ struct SsePlane {
   int32_t w, h;
   int32_t sb;       // bytes per sample
 };
-// The loop-restoration search (lr_search.cu): per unit job, a prep kernel
-// and the in-order Wiener passes on `s`, the self-guided fits (one CTA per
-// job and set) on `side` beside them, then the choice.
+// The loop-restoration search (lr_search.cu): per unit job, the no-filter
+// error and the Wiener passes on `s` (the first pass in a kernel of its own
+// for jobs of several rectangles), the self-guided fits (one CTA per job
+// and set) on `side` beside them, then the choice. Shared memory per kind:
+// 0 the first-pass kernel, 1 the Wiener kernel, 2 the self-guided kernel.
 size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px, int both);
 // The self-guided band height and filter-output cache that fit shared memory.
 void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px, int& both);

@@ -400,7 +400,7 @@ size_t lr_window_bytes(int wmax, int hmax) {
 }
 size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px, int both) {
   const size_t win = lr_window_bytes(wmax, hmax);
-  if (kind == 0) return win;                                                   // prep
+  if (kind == 0) return win;  // the first-pass kernel
   if (kind == 1) return win + size_t(2) * 4 * kWienerChunk * size_t(wmax + 1) * sizeof(double);  // Wiener passes
   // self-guided: A/B of both passes, the band's box sums, the filter-output cache
   return win + size_t(4) * (band + 2) * size_t(wmax + 2) * sizeof(int32_t) +
@@ -444,14 +444,17 @@ __device__ __forceinline__ Smem smem_of(uint8_t* base, const LrSearchDesc& d) {
 
 }  // namespace
 
-// Phase 1, one CTA per unit (256 threads): the error without a filter
-// (encoder/lr.rs:134-146), and the first Wiener pass (vertical, the other
-// direction's filter still zero: its lines are plain samples, so its sums
-// are exact integer sums in any order) and its solve.
+// For units of several stripe rectangles, one CTA per unit (256 threads):
+// the error without a filter (encoder/lr.rs:134-146), and the first Wiener
+// pass (vertical, the other direction's filter still zero: its lines are
+// plain samples, so its sums are exact integer sums in any order) and its
+// solve. A one-rectangle unit's Wiener CTA does this itself, on the window
+// it keeps for its other passes.
 __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSearchDesc d) {
   extern __shared__ __align__(16) uint8_t lrs_smem[];
   __shared__ int64_t red10[10][kThreads / 32];
   const LrSearchJob job = d.jobs[blockIdx.x];
+  if (job.nr == 1) return;
   const LrSearchFrame& F = d.frames[job.frame];
   const int p = job.plane, x0 = job.x0, w = job.w, sb = F.sb, tid = threadIdx.x, step = d.step;
   const Smem sm = smem_of(lrs_smem, d);
@@ -514,16 +517,20 @@ __global__ void __launch_bounds__(kThreads, 2) lr_search_prep_kernel(const LrSea
   }
 }
 
-// Phase 2, one CTA per unit (128 threads): the second (horizontal) and
-// third (vertical) Wiener passes, whose terms are real-valued, so each of
-// their sums runs in the reference's sample order: warps 1-3 produce a row's
-// terms into shared memory (two buffers) while lane q of warp 0 adds
-// accumulator q's terms (m00 m01 m02 m11 m12 m22 v0 v1 v2). Then the solves,
-// the quantised coefficients (encoder/lr.rs:316-327) and the filter's error.
+// One CTA per unit (128 threads). For a one-rectangle unit, first the error
+// without a filter and the first Wiener pass and its solve, as the kernel
+// above does for the others. Then the second
+// (horizontal) and third (vertical) Wiener passes, whose terms are
+// real-valued, so each of their sums runs in the reference's sample order:
+// warps 1-3 produce four rows of terms into shared memory (two buffers)
+// while lane q of warp 0 adds accumulator q's terms (m00 m01 m02 m11 m12 m22
+// v0 v1 v2). Then the solves, the quantised coefficients
+// (encoder/lr.rs:316-327) and the filter's error.
 __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearchDesc d) {
   extern __shared__ __align__(16) uint8_t lrs_smem[];
   __shared__ int64_t red[4];
-  __shared__ double s_m[3][3], s_v[3], s_other[3];
+  __shared__ int64_t red10[10][kThreads / 32];
+  __shared__ double s_m[3][3], s_v[3], s_other[3], s_vc[3];
   __shared__ int s_coef[2][3];
   const LrSearchJob job = d.jobs[blockIdx.x];
   const LrSearchFrame& F = d.frames[job.frame];
@@ -535,8 +542,65 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
   LrJobState& st = d.state[blockIdx.x];
   const int first = p == 0 ? 0 : 1;
   const int bd = F.bd, maxv = (1 << bd) - 1;
-  double vc[3] = {st.vc[0], st.vc[1], st.vc[2]}, hc[3] = {0.0, 0.0, 0.0};
   const int nci = (w + step - 1) / step;
+  if (job.nr == 1) {  // the no-filter error and the first pass (CTA-uniform)
+    int64_t acc = 0, m00 = 0, m01 = 0, m02 = 0, m11 = 0, m12 = 0, m22 = 0, v0 = 0, v1 = 0, v2 = 0;
+    for (int ri = 0; ri < job.nr; ri++) {
+      const LrSearchRect rc = rects[ri];
+      __syncthreads();
+      stage_window(F, p, rc, x0, w, sm.win, sm.ws);
+      __syncthreads();
+      // no filter: the window's interior is the rectangle's CDEF output (its
+      // rows lie in its stripe, its columns in the plane)
+      for (int i = tid >> 5; i < rc.h; i += blockDim.x >> 5)
+        for (int j = tid & 31; j < w; j += 32) {
+          const int e = W.at(i + kB, j + kB) - ld(F.src[p], sb, x0 + j, rc.y0 + i);
+          acc += int64_t(e) * e;
+        }
+      const int nri = (rc.h + step - 1) / step;
+      for (int ii = tid >> 5; ii < nri; ii += blockDim.x >> 5)
+        for (int jj = tid & 31; jj < nci; jj += 32) {
+        const int i = ii * step, j = jj * step;
+        int ln[7];
+#pragma unroll
+        for (int t = 0; t < 7; t++) ln[t] = W.at(i + t, j + kB);
+        const int64_t tg = ld(F.src[p], sb, x0 + j, rc.y0 + i) - ln[3];
+        const int64_t d0 = ln[0] + ln[6] - 2 * ln[3], d1 = ln[1] + ln[5] - 2 * ln[3], d2 = ln[2] + ln[4] - 2 * ln[3];
+        m00 += d0 * d0;
+        m01 += d0 * d1;
+        m02 += d0 * d2;
+        m11 += d1 * d1;
+        m12 += d1 * d2;
+        m22 += d2 * d2;
+        v0 += d0 * tg;
+        v1 += d1 * tg;
+        v2 += d2 * tg;
+        }
+    }
+    int64_t sums[10] = {m00, m01, m02, m11, m12, m22, v0, v1, v2, acc};
+    block_sums_i64(sums, red10);
+    if (tid == 0) {
+      st.none = uint64_t(sums[9]);
+      double sol[3] = {0.0, 0.0, 0.0};
+      const double tot[9] = {double(sums[0]), double(sums[1]), double(sums[2]), double(sums[3]), double(sums[4]),
+                             double(sums[5]), double(sums[6]), double(sums[7]), double(sums[8])};
+      if (p == 0) {
+        double m[3][3] = {{tot[0], tot[1], tot[2]}, {tot[1], tot[3], tot[4]}, {tot[2], tot[4], tot[5]}};
+        double v[3] = {tot[6], tot[7], tot[8]};
+        solve<3>(m, v, sol);
+      } else {
+        double m[2][2] = {{tot[3], tot[4]}, {tot[4], tot[5]}}, v[2] = {tot[7], tot[8]}, x2[2];
+        solve<2>(m, v, x2);
+        sol[1] = x2[0];
+        sol[2] = x2[1];
+      }
+      for (int k = 0; k < 3; k++) s_vc[k] = sol[k];
+    }
+  } else if (tid < 3) {
+    s_vc[tid] = st.vc[tid];  // from the kernel above
+  }
+  __syncthreads();
+  double vc[3] = {s_vc[0], s_vc[1], s_vc[2]}, hc[3] = {0.0, 0.0, 0.0};
   const int qa = lane < 6 ? (lane < 3 ? 0 : (lane < 5 ? 1 : 2)) : lane - 6;
   const int qb = lane < 6 ? (lane < 3 ? lane : (lane < 5 ? lane - 2 : 2)) : 3;  // 3: the target
   const bool owner = warp == 0 && lane < 9 && qa >= first && (qb == 3 || qb >= first);
@@ -552,9 +616,9 @@ __global__ void __launch_bounds__(128, 4) lr_search_wiener_kernel(const LrSearch
     for (int ri = 0; ri < job.nr; ri++) {
       const LrSearchRect rc = rects[ri];
       __syncthreads();
-      // one rectangle: its window, staged for the horizontal pass, stays in
-      // place (the term rows and band rows lie outside it)
-      if (job.nr > 1 || iter == 1) stage_window(F, p, rc, x0, w, sm.win, sm.ws);
+      // one rectangle: its window, staged for the first pass, stays in place
+      // (the term rows and band rows lie outside it)
+      if (job.nr > 1) stage_window(F, p, rc, x0, w, sm.win, sm.ws);
       __syncthreads();
       const int nri = (rc.h + step - 1) / step, nch = (nri + kWienerChunk - 1) / kWienerChunk;
       // chunks of rows in turn, two buffers: warps 1.. fill chunk c + 1 while
@@ -960,12 +1024,12 @@ void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStre
   cudaEventRecord(fork, s);
   cudaStreamWaitEvent(side, fork, 0);
   lr_search_sgr_kernel<<<njobs * d.nsets, kThreads, s2, side>>>(d);
-  lr_search_prep_kernel<<<njobs, kThreads, s0, s>>>(d);
+  if (d.multi_rect) lr_search_prep_kernel<<<njobs, kThreads, s0, s>>>(d);
   lr_search_wiener_kernel<<<njobs, 128, s1, s>>>(d);
   cudaEventRecord(join, side);
   cudaStreamWaitEvent(s, join, 0);
   lr_search_choose_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(d, njobs);
-  note_launch(4);
+  note_launch(d.multi_rect ? 4 : 3);
 }
 
 }  // namespace av1pf

@@ -518,6 +518,7 @@ int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs_in, in
       int px = 0;
       for (int r = 0; r < jb.nr; r++) px += rects[size_t(jb.r0 + r)].h * jb.w;
       upx_max = std::max(upx_max, px);
+      if (jb.nr > 1) d.multi_rect = 1;
     }
     lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px, d.both);
     cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px, d.both);
