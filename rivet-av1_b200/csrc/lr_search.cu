@@ -418,7 +418,7 @@ void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px, 
   constexpr size_t kTwo = 113 * 1024, kLimit = 220 * 1024;
   cache_px = upx_max <= kSgrCachePx ? upx_max : 0;
   for (size_t lim : {kTwo, kLimit})
-    for (band = 16; band >= 4; band /= 2)
+    for (band = 32; band >= 4; band /= 2)
       for (both = 1; both >= 0; both--)
         if (lr_search_smem(wmax, hmax, 2, band, cache_px, both) <= lim) return;
   band = 4;
