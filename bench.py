@@ -59,7 +59,6 @@ METRIC = "bit-exact post-filtered Mpx/s"
 HEADLINE = dict(width=1920, height=1080, bit_depth=10)
 L2_BYTES = 126 * 2**20
 HEADLINE_WORKLOAD = "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+CDEF+LR+pack)"
-REF_ARM_BUDGET_S = 120.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each stage's kernels on the
 # headline workload, from one `ncu --set full` capture (cold cache; the outputs stay in the 126 MB
 # L2, so the writes read 0). The loop filter's is its three kernels together. The headline frames
@@ -166,37 +165,45 @@ def cpu_rate(cfgs, budget_s, threads=0):
     return px / el / 1e6, n, el, cores
 
 
+CPU_SEEDS = [1000 + i for i in range(4)]  # the CPU legs' frames (both arms time the same sample)
+
+
+def headline_config(world):
+    """The workload's `config`, identical in both arms' lines."""
+    probe = A.SynthHandle(**HEADLINE, seed=1)
+    in_bytes = sum(probe.f.plane_bytes[p] for p in range(3))
+    pool_n = max(8, int(2 * L2_BYTES / in_bytes) + 1)
+    return {"workload": HEADLINE_WORKLOAD, "frames_per_step": 1, "pool_frames": pool_n,
+            "l2": f"inputs rotate over {pool_n} distinct frames ({pool_n * in_bytes / 2**20:.0f} MiB > 2x L2)",
+            "parallelism": f"replicas x{world}"}, pool_n, in_bytes
+
+
 def reference_arm(args):
-    # rank 0 alone times the CPU path; other ranks exit without work (no process group)
+    """The reference's CPU implementation of the path (the oracle port, all
+    host threads) on the headline workload: rank 0 alone; the other ranks
+    exit without work. The sample is time-bounded like the cpu_baseline leg
+    of the GPU arm (at least args.cpu_seconds of frames, rotating over the
+    same 4 seeded frames), after the warm-up frames."""
     rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    cfg = dict(HEADLINE, seed=1)
-    steps, warm = args.steps, args.warmup
+    config, _, _ = headline_config(world)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    sf = A.SynthHandle(**cfg)
-    for _ in range(warm):
-        O.chain(sf, threads=0)
-    times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        O.chain(sf, threads=0)
-        times.append(time.perf_counter() - t0)
-        if sum(times) > REF_ARM_BUDGET_S:  # bounded sample: the run ends within a few minutes
-            break
-    total = sum(times)
-    timed = len(times)
-    mpx = 1920 * 1080 * timed / total / 1e6
+    sfs = [A.SynthHandle(**HEADLINE, seed=s) for s in CPU_SEEDS]
+    for i in range(args.warmup):
+        O.chain(sfs[i % len(sfs)], threads=0)
+    budget = max(args.cpu_seconds, 1.0)
+    rate, n, el, cores = cpu_rate([dict(HEADLINE, seed=s) for s in CPU_SEEDS], budget)
+    ms_frame = 1e3 * el / n
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(mpx, 3), "unit": "Mpx/s", "n_gpus": world,
-        "steps": steps, "warmup": warm, "ms_per_step": round(1e3 * total / timed, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": HEADLINE_WORKLOAD, "frames_per_step": 1},
-        "cpu_baseline": {"value": round(mpx, 3), "unit": "Mpx/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"{timed} timed frames of the workload (of {steps} asked; at most "
-                                   f"{REF_ARM_BUDGET_S:.0f} s) after {warm} warm-up, all host threads"},
-        "e2e": {"value": round(mpx, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "impl": "reference", "metric": METRIC, "value": round(rate, 3), "unit": "Mpx/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_frame, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config,
+        "cpu_baseline": {"value": round(rate, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} frames of the workload in {el:.1f} s (4 seeded frames in turn) after "
+                                   f"{args.warmup} warm-up frames, CPU oracle on all host threads"},
+        "e2e": {"value": round(rate, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -216,6 +223,7 @@ def main_gpu(args):
         ctx = G.Ctx(local)
         fn = {"mix": lambda: bench_mix(args, ctx, rank, torch.cuda.synchronize, lambda v: v),
               "c3": lambda: bench_4k(args, ctx, torch.cuda.synchronize, lambda v: v),
+              "grain": lambda: bench_4k(args, ctx, torch.cuda.synchronize, lambda v: v, GRAIN_CASES),
               "serve": lambda: bench_serve(args, ctx, rank),
               "search": lambda: bench_search(args, ctx, rank, world)}[args.only]
         print(json.dumps({args.only: fn()}), flush=True)
@@ -228,10 +236,7 @@ def main_gpu(args):
     max_over_ranks = ranks.max
 
     # ---- headline pool: distinct frames whose inputs exceed 2x L2 ----
-    probe = A.SynthHandle(**HEADLINE, seed=1)
-    in_bytes = sum(probe.f.plane_bytes[p] for p in range(3))
-    pool_n = max(8, int(2 * L2_BYTES / in_bytes) + 1)
-    del probe
+    config, pool_n, in_bytes = headline_config(world)
     sfs = [A.SynthHandle(**HEADLINE, seed=R.frame_seed(rank, i)) for i in range(pool_n)]
     dfs = [G.DevFrame(s) for s in sfs]
     outs = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
@@ -303,10 +308,7 @@ def main_gpu(args):
         "metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": HEADLINE_WORKLOAD,
-                   "frames_per_step": 1, "pool_frames": pool_n,
-                   "l2": f"inputs rotate over {pool_n} distinct frames ({pool_n * in_bytes / 2**20:.0f} MiB > 2x L2)",
-                   "parallelism": f"replicas x{world}"},
+        "config": config,
         "bit_exact_vs_oracle": exact,
         "gpu_launches": int(launches),
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
@@ -408,15 +410,19 @@ def main_gpu(args):
     if not args.skip_extras:
         result["mix"] = bench_mix(args, ctx, rank, barrier, max_over_ranks)
         result["c3_4k"] = bench_4k(args, ctx, barrier, max_over_ranks)
+        grain = bench_4k(args, ctx, barrier, max_over_ranks, GRAIN_CASES)
+        for v in grain.values():
+            v["vs_grain_free_headline"] = round(v["ms_per_frame"] / (ms_max / args.steps), 3)
+        result["grain_1080p"] = grain
         result["serve"] = bench_serve(args, ctx, rank)
         result["search"] = bench_search(args, ctx, rank, world)
 
     # ---- CPU baseline (rank 0, N = 1) ----
     if rank == 0 and world == 1:
-        rate, n, el, cores = cpu_rate([dict(HEADLINE, seed=1000 + i) for i in range(4)], args.cpu_seconds)
+        rate, n, el, cores = cpu_rate([dict(HEADLINE, seed=s) for s in CPU_SEEDS], args.cpu_seconds)
         result["cpu_baseline"] = {"value": round(rate, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
-                                  "sample": f"{n} frames of the headline workload in {el:.1f} s, "
-                                            f"CPU oracle on all host threads"}
+                                  "sample": f"{n} frames of the headline workload in {el:.1f} s (4 seeded frames "
+                                            f"in turn), CPU oracle on all host threads"}
     ctx.close()
     ranks.close()
     if rank == 0:
@@ -504,24 +510,34 @@ def bench_mix(args, ctx, rank, barrier, max_over_ranks):
             "bit_exact_batched_vs_per_frame": bool(exact), "autotune": tuned}
 
 
-def bench_4k(args, ctx, barrier, max_over_ranks):
-    """4K chains with superres (denominator 13 / 10) and film grain."""
+C3_CASES = [("10bit_420_superres_grain", 3, dict(width=3840, height=2160, bit_depth=10, superres_denom=13,
+                                                  enable_grain=1, seed=77, frame_index=3)),
+            ("12bit_444_superres_grain", 3, dict(width=3840, height=2160, bit_depth=12, subsampling_x=0,
+                                                  subsampling_y=0, superres_denom=10, enable_grain=1, seed=78,
+                                                  frame_index=4))]
+# the headline's shape with film grain: its inputs rotate over 20 frames (124 MB of input, plus outputs), so
+# the comparison with the grain-free headline is not flattered by L2
+GRAIN_CASES = [("1080p_10bit_420_grain", 20, dict(width=1920, height=1080, bit_depth=10, enable_grain=1, seed=79,
+                                                  frame_index=5))]
+
+
+def bench_4k(args, ctx, barrier, max_over_ranks, cases=C3_CASES):
+    """Per-frame chains of `cases` (name, distinct frames, synthesis
+    arguments): by default config 3's 4K chains with superres (denominator
+    13 / 10) and film grain."""
     import torch
     import gpu_util as G
     L = A.lib()
     res = {}
-    for name, cfg in [("10bit_420_superres_grain", dict(width=3840, height=2160, bit_depth=10, superres_denom=13,
-                                                         enable_grain=1, seed=77, frame_index=3)),
-                      ("12bit_444_superres_grain", dict(width=3840, height=2160, bit_depth=12, subsampling_x=0,
-                                                         subsampling_y=0, superres_denom=10, enable_grain=1,
-                                                         seed=78, frame_index=4))]:
-        sfs = [A.SynthHandle(**dict(cfg, seed=cfg["seed"] + i)) for i in range(3)]
+    for name, pool, cfg in cases:
+        sfs = [A.SynthHandle(**dict(cfg, seed=cfg["seed"] + i, frame_index=cfg["frame_index"] + i))
+               for i in range(pool)]
         dfs = [G.DevFrame(s) for s in sfs]
         outs = [(G.DevPlanes.visible(d.info), G.dev_bytes(A.frame_bytes(d.info))) for d in dfs]
 
         def run(i):
-            d = dfs[i % 3]
-            r, fb = outs[i % 3]
+            d = dfs[i % pool]
+            r, fb = outs[i % pool]
             A.check(L.av1pf_chain(ctx.p, C.byref(d.info), C.byref(d.params), C.byref(d.maps), d.inp.c, r.c,
                                   fb.data_ptr(), None))
         for i in range(args.warmup):
@@ -548,7 +564,8 @@ def bench_4k(args, ctx, barrier, max_over_ranks):
         info = dfs[0].info
         chain_bytes = plane_set_bytes(info, upscaled=False) + 2 * plane_set_bytes(info)
         peak, _ = peaks()
-        res[name] = {"ms_per_frame": round(ms, 4), "mpx_s": round(3840 * 2160 / (ms / 1e3) / 1e6, 1),
+        res[name] = {"ms_per_frame": round(ms, 4), "frames": pool,
+                     "mpx_s": round(info.upscaled_width * info.frame_height / (ms / 1e3) / 1e6, 1),
                      "chain_hbm_frac": round(chain_bytes / (ms / 1e3) / 1e9 / peak, 4),
                      "stages_ms": {n: round(float(ms5[k]) / max(1, calls.value), 4)
                                    for k, n in enumerate(["loop_filter", "cdef", "superres", "loop_restoration",
@@ -933,7 +950,7 @@ def main():
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-extras", action="store_true")
-    ap.add_argument("--only", choices=["mix", "c3", "serve", "search"], default=None,
+    ap.add_argument("--only", choices=["mix", "c3", "grain", "serve", "search"], default=None,
                     help="run one extra section alone (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:

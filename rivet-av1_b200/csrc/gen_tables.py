@@ -10,7 +10,7 @@ is read. Each table becomes an initializer macro ``AV1T_<NAME>`` plus its
 dimensions, so host code (``static const``) and device code (``__constant__``)
 build from the same data.
 
-Usage: python gen_tables.py [path/to/tables.rs]
+Usage: python gen_tables.py <path of the reference's src/tables.rs>
 """
 import os
 import re
@@ -60,7 +60,9 @@ def dims_of(rust_type):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/tables.rs"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: gen_tables.py <path of the reference's src/tables.rs>")
+    src = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     out_path = os.path.join(here, "av1_tables.h")
     found = {}
