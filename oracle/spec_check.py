@@ -1,26 +1,31 @@
-"""A second CPU restatement of two post-filter processes, written from the AV1
-Bitstream & Decoding Process Specification's pseudo-code rather than from the
-reference's Rust code or from oracle.cpp:
+"""A second CPU restatement of the post-filter processes, written from the
+AV1 Bitstream & Decoding Process Specification's pseudo-code rather than from
+the reference's Rust code or from oracle.cpp:
 
+  - 7.14 loop filter (edge loop filter, filter size, adaptive filter
+    strength and its level selection, filter masks, narrow and wide filters);
   - 7.15 CDEF process (cdef_block, 7.15.1 cdef_direction, 7.15.2
     cdef_filter with cdef_get_at / is_inside_filter_region / constrain);
+  - 7.16 super-resolution (upscaling of the CDEF and the pre-CDEF frames);
+  - 7.17 loop restoration (per 4x4 block: stripes, units and the source
+    sample rule, the Wiener filter with its rounding variables, the
+    self-guided box filters and projection);
   - 7.18.3 film grain synthesis (7.18.3.2 random numbers, 7.18.3.3 grain
     generation, 7.18.3.4 scaling lookup, 7.18.3.5 noise stripes, noise image
-    and blending), followed by the packing of the output frame.
+    and blending), followed by the packing of the output frame;
+  - the chain in decode_frame_wrapup's order.
 
 TEST INFRASTRUCTURE ONLY: tests/test_spec_check.py compares it with the
-oracle's cdef and output processes on small synthetic frames. The oracle and
-the CUDA kernels were both written from the reference's Rust code; this file
-was written from the specification alone, so a misreading of the reference
-that the oracle and the kernels share would show up here as a difference.
-It does not pin parity to the reference's binary.
+oracle's per-stage and whole-chain processes on small synthetic frames. The
+oracle and the CUDA kernels were both written from the reference's Rust
+code; this file was written from the specification alone, so a misreading of
+the reference that the oracle and the kernels share would show up here as a
+difference. It does not pin parity to the reference's binary.
 
-Plain Python and numpy: the per-sample loops are vectorised over 8x8 blocks
-(CDEF) and whole planes (grain blending), and the grain templates run as
-the specification's scalar loops, so a 352x288 frame takes a few seconds.
-Only the specification's constant tables are taken from the library's table
-header (av1_tables.h: Cdef_Uv_Dir, Div_Table, Cdef_Directions,
-Gaussian_Sequence).
+Plain Python and numpy, at the specification's granularity (per edge lane,
+per 8x8 CDEF block, per 4x4 restoration block), so frames of a few hundred
+samples a side take seconds. Only the specification's constant tables are
+taken from the library's table header (av1_tables.h).
 """
 import ctypes as C
 import os
@@ -454,3 +459,421 @@ def output_frame(info, params, ref_planes):
                            info.subsampling_y, w, h, info.matrix_coefficients)
     dt = np.uint8 if info.bit_depth == 8 else np.dtype("<u2")
     return np.concatenate([p.astype(dt).reshape(-1).view(np.uint8) for p in planes])
+
+
+# ---------------------------------------------------------------------------
+# Inputs of the other processes: the ABI's maps and parameters as arrays
+# ---------------------------------------------------------------------------
+# YMode numbering of av1pf_mi.y_mode (the reference's: UV_CFL_PRED 13 shares
+# the intra range, NEARESTMV 14 .. NEW_NEWMV 25)
+NEARESTMV, GLOBALMV, GLOBAL_GLOBALMV = 14, 16, 24
+RESTORE_NONE, RESTORE_WIENER, RESTORE_SGRPROJ = 0, 1, 2
+
+
+class Frame:
+    """The frame-level inputs of the post-filter processes, read from an
+    av1pf_frame_info / av1pf_params / av1pf_maps triple of host pointers."""
+
+    def __init__(self, info, params, maps, f_counts):
+        self.info, self.p = info, params
+        self.bd = info.bit_depth
+        self.ssx, self.ssy = info.subsampling_x, info.subsampling_y
+        self.np = info.num_planes
+        self.mi_rows, self.mi_cols = info.mi_rows, info.mi_cols
+        self.fw, self.fh, self.uw = info.frame_width, info.frame_height, info.upscaled_width
+        ms = maps.mi_stride
+        self.ms = ms
+        mi_count, tx_count, cdef_count, lr_count = f_counts
+        raw = np.frombuffer((C.c_uint8 * (mi_count * 8)).from_address(maps.mi), np.uint8).reshape(-1, ms, 8)
+        self.mi_size = raw[:, :, 0].astype(np.int64)
+        self.y_mode = raw[:, :, 1].astype(np.int64)
+        self.ref0 = raw[:, :, 2].view(np.int8).astype(np.int64)
+        self.skip = (raw[:, :, 3] & 0x80) != 0
+        self.seg = (raw[:, :, 3] & 7).astype(np.int64)
+        self.delta_lf = raw[:, :, 4:8].view(np.int8).astype(np.int64)
+        self.tx = []
+        for k in range(3):
+            if maps.lf_tx_size[k] and tx_count[k]:
+                a = np.frombuffer((C.c_uint8 * tx_count[k]).from_address(maps.lf_tx_size[k]), np.uint8)
+                self.tx.append(a.reshape(-1, ms).astype(np.int64))
+            else:
+                self.tx.append(None)
+        self.cdef_idx = np.frombuffer((C.c_int8 * cdef_count).from_address(maps.cdef_idx),
+                                      np.int8).reshape(-1, maps.cdef_stride)
+        self.lru = []
+        for k in range(3):
+            if maps.lr_units[k] and lr_count[k]:
+                u = np.frombuffer((C.c_uint8 * (lr_count[k] * 12)).from_address(maps.lr_units[k]),
+                                  np.uint8).reshape(-1, 12)
+                self.lru.append(u)
+            else:
+                self.lru.append(None)
+
+
+def frame_of(sf):
+    f = sf.f
+    return Frame(f.info, f.params, f.maps, (f.mi_count, list(f.tx_count), f.cdef_count, list(f.lr_count)))
+
+
+# ---------------------------------------------------------------------------
+# 7.14 loop filter
+# ---------------------------------------------------------------------------
+def filter_strength(fr, row, col, plane, pass_):
+    """7.14.4 adaptive_filter_strength with 7.14.5's level selection:
+    (lvl, limit, blimit, thresh) of mode-info position (row, col)."""
+    p = fr.p
+    segment = int(fr.seg[row][col])
+    ref = int(fr.ref0[row][col])
+    mode = int(fr.y_mode[row][col])
+    mode_type = 1 if (mode >= NEARESTMV and mode != GLOBALMV and mode != GLOBAL_GLOBALMV) else 0
+    i = pass_ if plane == 0 else plane + 1
+    delta_lf = int(fr.delta_lf[row][col][0 if not p.delta_lf_multi else i])
+    lvl = min(63, max(0, delta_lf + p.loop_filter_level[i]))
+    feature = 1 + i  # SEG_LVL_ALT_LF_Y_V + i
+    if p.segmentation_enabled and p.feature_enabled[segment][feature]:
+        lvl = min(63, max(0, p.feature_data[segment][feature] + lvl))
+    if p.loop_filter_delta_enabled:
+        n_shift = lvl >> 5
+        if ref <= 0:  # INTRA_FRAME
+            lvl += p.loop_filter_ref_deltas[0] << n_shift
+        else:
+            lvl += (p.loop_filter_ref_deltas[ref] << n_shift) + (p.loop_filter_mode_deltas[mode_type] << n_shift)
+        lvl = min(63, max(0, lvl))
+    sharp = p.loop_filter_sharpness
+    shift = 2 if sharp > 4 else (1 if sharp > 0 else 0)
+    limit = min(9 - sharp, max(1, lvl >> shift)) if sharp > 0 else max(1, lvl >> shift)
+    blimit = 2 * (lvl + 2) + limit
+    thresh = lvl >> 4
+    return lvl, limit, blimit, thresh
+
+
+def sample_filtering(pl, x, y, plane, limit, blimit, thresh, dx, dy, filter_size, bd):
+    """7.14.6 on the sample (x, y) of plane array `pl` (int64, in place)."""
+    def at(k):
+        return int(pl[y + k * dy][x + k * dx])
+    shift = bd - 8
+    q = [at(k) for k in range(7)] if filter_size >= 16 else [at(k) for k in range(4)]
+    pp = [at(-1 - k) for k in range(7)] if filter_size >= 16 else [at(-1 - k) for k in range(4)]
+    # 7.14.6.2 filter mask process
+    hev = abs(pp[1] - pp[0]) > (thresh << shift) or abs(q[1] - q[0]) > (thresh << shift)
+    flen = 4 if filter_size == 4 else (6 if plane else (8 if filter_size == 8 else 16))
+    lim, blim = limit << shift, blimit << shift
+    mask = abs(pp[1] - pp[0]) <= lim and abs(q[1] - q[0]) <= lim and abs(pp[0] - q[0]) * 2 + abs(pp[1] - q[1]) // 2 <= blim
+    if flen >= 6:
+        mask = mask and abs(pp[2] - pp[1]) <= lim and abs(q[2] - q[1]) <= lim
+    if flen >= 8:
+        mask = mask and abs(pp[3] - pp[2]) <= lim and abs(q[3] - q[2]) <= lim
+    t = 1 << shift
+    flat = False
+    if filter_size >= 8:
+        flat = abs(pp[1] - pp[0]) <= t and abs(q[1] - q[0]) <= t and abs(pp[2] - pp[0]) <= t and abs(q[2] - q[0]) <= t
+        if flen >= 8:
+            flat = flat and abs(pp[3] - pp[0]) <= t and abs(q[3] - q[0]) <= t
+    flat2 = False
+    if filter_size >= 16:
+        flat2 = all(abs(pp[k] - pp[0]) <= t and abs(q[k] - q[0]) <= t for k in (6, 5, 4))
+    if not mask:
+        return
+    if filter_size == 4 or not flat:
+        # 7.14.6.3 narrow filter
+        lo, hi = -(1 << (bd - 1)), (1 << (bd - 1)) - 1
+
+        def c4(v):
+            return min(hi, max(lo, v))
+        off = 0x80 << shift
+        ps1, ps0, qs0, qs1 = pp[1] - off, pp[0] - off, q[0] - off, q[1] - off
+        fl = c4(ps1 - qs1) if hev else 0
+        fl = c4(fl + 3 * (qs0 - ps0))
+        f1 = c4(fl + 4) >> 3
+        f2 = c4(fl + 3) >> 3
+        pl[y][x] = c4(qs0 - f1) + off
+        pl[y - dy][x - dx] = c4(ps0 + f2) + off
+        if not hev:
+            fr_ = round2(f1, 1)
+            pl[y + dy][x + dx] = c4(qs1 - fr_) + off
+            pl[y - 2 * dy][x - 2 * dx] = c4(ps1 + fr_) + off
+        return
+    # 7.14.6.4 wide filter
+    log2 = 3 if (filter_size == 8 or not flat2) else 4
+    n = 6 if log2 == 4 else (3 if plane == 0 else 2)
+    n2 = 0 if (log2 == 3 and plane == 0) else 1
+    src = {k: at(k) for k in range(-(n + 1), n + 1)}
+    out = {}
+    for i in range(-n, n):
+        tot = 0
+        for j in range(-n, n + 1):
+            pos = min(n, max(-(n + 1), i + j))
+            tot += src[pos] * (2 if abs(j) <= n2 else 1)
+        out[i] = round2(tot, log2)
+    for i, v in out.items():
+        pl[y + i * dy][x + i * dx] = v
+
+
+def loop_filter(planes, fr):
+    """7.14.1: both passes over every plane whose level is set, in place,
+    in raster order (vertical edges of the plane first)."""
+    sub = table("SUBSAMPLED_SIZE")
+    n4w, n4h = table("NUM_4X4_BLOCKS_WIDE"), table("NUM_4X4_BLOCKS_HIGH")
+    txw, txh = table("TX_WIDTH"), table("TX_HEIGHT")
+    p = fr.p
+    if not (p.loop_filter_level[0] or p.loop_filter_level[1]):
+        return planes
+    for plane in range(fr.np):
+        if plane and not p.loop_filter_level[1 + plane]:
+            continue
+        sx = fr.ssx if plane else 0
+        sy = fr.ssy if plane else 0
+        pl = planes[plane]
+        for pass_ in range(2):
+            dx, dy = (1, 0) if pass_ == 0 else (0, 1)
+            for row0 in range(0, fr.mi_rows, 1 << sy):
+                for col0 in range(0, fr.mi_cols, 1 << sx):
+                    x, y = col0 * 4, row0 * 4
+                    if x >= fr.fw or y >= fr.fh or (pass_ == 0 and x == 0) or (pass_ == 1 and y == 0):
+                        continue
+                    xp, yp = x >> sx, y >> sy
+                    row, col = row0 | sy, col0 | sx
+                    prev_row, prev_col = row - (dy << sy), col - (dx << sx)
+                    plane_size = int(sub[fr.mi_size[row][col]][sx][sy])
+                    tx_sz = int(fr.tx[plane][row >> sy][col >> sx])
+                    prev_tx = int(fr.tx[plane][prev_row >> sy][prev_col >> sx])
+                    skip = bool(fr.skip[row][col])
+                    is_intra = fr.ref0[row][col] <= 0
+                    if pass_ == 0:
+                        block_edge = xp % (4 * int(n4w[plane_size])) == 0
+                        tx_edge = xp % int(txw[tx_sz]) == 0
+                        base = min(int(txw[prev_tx]), int(txw[tx_sz]))
+                    else:
+                        block_edge = yp % (4 * int(n4h[plane_size])) == 0
+                        tx_edge = yp % int(txh[tx_sz]) == 0
+                        base = min(int(txh[prev_tx]), int(txh[tx_sz]))
+                    apply = tx_edge and (block_edge or not skip or is_intra)
+                    size = min(16 if plane == 0 else 8, base)
+                    lvl, limit, blimit, thresh = filter_strength(fr, row, col, plane, pass_)
+                    if lvl == 0:
+                        lvl, limit, blimit, thresh = filter_strength(fr, prev_row, prev_col, plane, pass_)
+                    if not apply or lvl == 0:
+                        continue
+                    for i in range(4):
+                        sample_filtering(pl, xp + dy * i, yp + dx * i, plane, limit, blimit, thresh, dx, dy, size,
+                                         fr.bd)
+    return planes
+
+
+# ---------------------------------------------------------------------------
+# 7.16 super-resolution
+# ---------------------------------------------------------------------------
+def _div_trunc(a, b):
+    """Integer division truncating toward zero (the specification's /)."""
+    q = abs(a) // abs(b)
+    return q if (a >= 0) == (b > 0) else -q
+
+
+def upscale(planes, fr):
+    """7.16: the upscaled planes (frame_width -> upscaled_width)."""
+    flt = table("UPSCALE_FILTER")
+    out = []
+    for plane in range(fr.np):
+        sx = fr.ssx if plane else 0
+        sy = fr.ssy if plane else 0
+        down_w = round2(fr.fw, sx)
+        up_w = round2(fr.uw, sx)
+        ph = round2(fr.fh, sy)
+        step = _div_trunc((down_w << 14) + up_w // 2, up_w)
+        err = up_w * step - (down_w << 14)
+        init = _div_trunc(-((up_w - down_w) << 13) + up_w // 2, up_w) + (1 << 7) - _div_trunc(err, 2)
+        init &= (1 << 14) - 1
+        max_x = (fr.mi_cols >> sx) * 4 - 1
+        src = planes[plane]
+        xs = np.arange(up_w, dtype=np.int64)
+        src_x = -(1 << 14) + init + xs * step
+        px = src_x >> 14
+        phase = (src_x & ((1 << 14) - 1)) >> 8
+        res = np.zeros((ph, up_w), np.int64)
+        for k in range(8):
+            sxk = np.clip(px + k - 3, 0, max_x)
+            res += src[:ph, sxk] * flt[phase, k][None, :]
+        dst = np.zeros((src.shape[0], max(up_w, src.shape[1])), np.int64)
+        dst[:ph, :up_w] = np.clip(round2(res, 7), 0, (1 << fr.bd) - 1)
+        out.append(dst)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# 7.17 loop restoration
+# ---------------------------------------------------------------------------
+def count_units(unit_size, frame_size):
+    return max((frame_size + (unit_size >> 1)) // unit_size, 1)
+
+
+def loop_restoration(cdef_up, cur_up, fr):
+    """7.17: LrFrame from UpscaledCdefFrame (`cdef_up`) with the stripe
+    boundary rows taken from UpscaledCurrFrame (`cur_up`), block by block."""
+    p = fr.p
+    lr = [a.copy() for a in cdef_up]
+    if not p.uses_lr:
+        return lr
+    sgr = table("SGR_PARAMS")
+    bd = fr.bd
+    maxv = (1 << bd) - 1
+    for plane in range(fr.np):
+        if p.frame_restoration_type[plane] == RESTORE_NONE:
+            continue
+        sx = fr.ssx if plane else 0
+        sy = fr.ssy if plane else 0
+        unit_size = p.loop_restoration_size[plane]
+        unit_rows = count_units(unit_size, round2(fr.fh, sy))
+        unit_cols = count_units(unit_size, round2(fr.uw, sx))
+        pex, pey = round2(fr.uw, sx) - 1, round2(fr.fh, sy) - 1
+        units = fr.lru[plane]
+        cd, cu = cdef_up[plane], cur_up[plane]
+        for y_l in range(0, fr.fh, 4):
+            row = y_l >> 2
+            stripe = (row * 4 + 8) // 64
+            ss = (-8 + stripe * 64) >> sy
+            se = ss + (64 >> sy) - 1
+            unit_row = min(unit_rows - 1, ((row * 4 + 8) >> sy) // unit_size)
+            y = (row * 4) >> sy
+            h = min(4 >> sy, pey - y + 1)
+            if h <= 0:
+                continue
+            # the rows this block reads (3 above and below, the stripe rule per row)
+            src_rows = {}
+            for yy in range(y - 4, y + h + 4):
+                yc = min(pey, max(0, yy))
+                if yc < ss:
+                    src_rows[yy] = cu[max(ss - 2, yc)]
+                elif yc > se:
+                    src_rows[yy] = cu[min(se + 2, yc)]
+                else:
+                    src_rows[yy] = cd[yc]
+            for x_l in range(0, fr.uw, 4):
+                col = x_l >> 2
+                unit_col = min(unit_cols - 1, ((col * 4) >> sx) // unit_size)
+                x = (col * 4) >> sx
+                w = min(4 >> sx, pex - x + 1)
+                if w <= 0:
+                    continue
+                u = units[unit_row * unit_cols + unit_col]
+                rtype = int(u[0])
+                cols = np.clip(np.arange(x - 4, x + w + 4), 0, pex)
+
+                def window(r0, r1):
+                    """Source samples of rows y+r0 .. y+r1-1, columns x-4 .. x+w+3."""
+                    return np.array([src_rows[y + r][cols] for r in range(r0, r1)], np.int64)
+                if rtype == RESTORE_WIENER:
+                    coef = u[4:10].view(np.int8).astype(np.int64).reshape(2, 3)  # [0] vertical, [1] horizontal
+
+                    def filt(c3):
+                        f = np.zeros(7, np.int64)
+                        f[3] = 128
+                        for i in range(3):
+                            f[i] = f[6 - i] = c3[i]
+                            f[3] -= 2 * c3[i]
+                        return f
+                    vf, hf = filt(coef[0]), filt(coef[1])
+                    r0 = 5 if bd == 12 else 3
+                    r1 = 9 if bd == 12 else 11
+                    offset = 1 << (bd + 7 - r0 - 1)
+                    limit = (1 << (bd + 1 + 7 - r0)) - 1
+                    win = window(-3, h + 3)  # h + 6 rows
+                    inter = np.zeros((h + 6, w), np.int64)
+                    for c in range(w):
+                        s = sum(hf[t] * win[:, c + 4 + t - 3] for t in range(7))
+                        inter[:, c] = np.clip(round2(s, r0), -offset, limit - offset)
+                    out = np.zeros((h, w), np.int64)
+                    for r in range(h):
+                        s = sum(vf[t] * inter[r + t] for t in range(7))
+                        out[r] = np.clip(round2(s, r1), 0, maxv)
+                    lr[plane][y:y + h, x:x + w] = out
+                elif rtype == RESTORE_SGRPROJ:
+                    st = int(u[1]) & 15
+                    xqd = u[2:4].view(np.int8).astype(np.int64)
+                    win = window(-4, h + 4)  # rows y-4 .. y+h+3, cols x-4 .. x+w+3
+
+                    def box_filter(pass_):
+                        r = int(sgr[st][2 * pass_])
+                        eps = int(sgr[st][2 * pass_ + 1])
+                        n = (2 * r + 1) ** 2
+                        n2e = n * n * eps
+                        s = ((1 << 20) + n2e // 2) // n2e
+                        one_over_n = ((1 << 12) + n // 2) // n
+                        A = np.zeros((h + 2, w + 2), np.int64)
+                        B = np.zeros((h + 2, w + 2), np.int64)
+                        for i in range(-1, h + 1):
+                            for j in range(-1, w + 1):
+                                blk = win[4 + i - r:4 + i + r + 1, 4 + j - r:4 + j + r + 1]
+                                a = round2(int((blk * blk).sum()), 2 * (bd - 8))
+                                b = int(blk.sum())
+                                d = round2(b, bd - 8)
+                                pp = max(0, a * n - d * d)
+                                z = round2(pp * s, 20)
+                                if z >= 255:
+                                    a2 = 256
+                                elif z == 0:
+                                    a2 = 1
+                                else:
+                                    a2 = ((z << 8) + z // 2) // (z + 1)
+                                A[i + 1][j + 1] = a2
+                                B[i + 1][j + 1] = round2((256 - a2) * b * one_over_n, 12)
+                        F = np.zeros((h, w), np.int64)
+                        for i in range(h):
+                            shift = 4 if (pass_ == 0 and (i & 1)) else 5
+                            for j in range(w):
+                                a = b = 0
+                                for ddy in (-1, 0, 1):
+                                    for ddx in (-1, 0, 1):
+                                        if pass_ == 0:
+                                            wt = (6 if ddx == 0 else 5) if ((i + ddy) & 1) else 0
+                                        else:
+                                            wt = 4 if (ddx == 0 or ddy == 0) else 3
+                                        a += wt * int(A[i + 1 + ddy][j + 1 + ddx])
+                                        b += wt * int(B[i + 1 + ddy][j + 1 + ddx])
+                                v = a * int(cd[y + i][x + j]) + b
+                                F[i][j] = round2(v, 8 + shift - 4)
+                        return F
+                    rr0, rr1 = int(sgr[st][0]), int(sgr[st][2])
+                    flt0 = box_filter(0) if rr0 else None
+                    flt1 = box_filter(1) if rr1 else None
+                    w0, w1 = int(xqd[0]), int(xqd[1])
+                    w2 = (1 << 7) - w0 - w1
+                    uu = cd[y:y + h, x:x + w] << 4
+                    v = w1 * uu
+                    v = v + (w0 * flt0 if rr0 else w0 * uu)
+                    v = v + (w2 * flt1 if rr1 else w2 * uu)
+                    lr[plane][y:y + h, x:x + w] = np.clip(round2(v, 11), 0, maxv)
+    return lr
+
+
+# ---------------------------------------------------------------------------
+# The whole chain (decode_frame_wrapup's order) and the output process
+# ---------------------------------------------------------------------------
+def chain(sf, in_planes):
+    """The chain from the pre-filter planes (int64 arrays in the frame's
+    allocated layout): loop filter, CDEF, upscaling of the CDEF and the
+    pre-CDEF frames, loop restoration; returns (LR frame planes cropped to
+    the visible area, packed output frame)."""
+    fr = frame_of(sf)
+    p = fr.p
+    cur = loop_filter([a.astype(np.int64).copy() for a in in_planes], fr)
+    if p.cdef_enabled:
+        skip = fr.skip[: fr.mi_rows, : fr.mi_cols]
+        strengths = dict(damping=p.cdef_damping, y_pri=list(p.cdef_y_pri_strength),
+                         y_sec=list(p.cdef_y_sec_strength), uv_pri=list(p.cdef_uv_pri_strength),
+                         uv_sec=list(p.cdef_uv_sec_strength))
+        frd = dict(bit_depth=fr.bd, ss_x=fr.ssx, ss_y=fr.ssy, mi_rows=fr.mi_rows, mi_cols=fr.mi_cols,
+                   num_planes=fr.np)
+        cdef = cdef_frame(cur, frd, skip, fr.cdef_idx, strengths)
+    else:
+        cdef = cur
+    if p.use_superres and fr.uw != fr.fw:
+        cdef_up, cur_up = upscale(cdef, fr), upscale(cur, fr)
+    else:
+        cdef_up, cur_up = cdef, cur
+    lr = loop_restoration(cdef_up, cur_up, fr)
+    vis = []
+    for plane in range(fr.np):
+        sx = fr.ssx if plane else 0
+        sy = fr.ssy if plane else 0
+        vis.append(lr[plane][: round2(fr.fh, sy), : round2(fr.uw, sx)].copy())
+    return vis, output_frame(sf.f.info, p, vis)
