@@ -576,6 +576,10 @@ int check_error_flags(cudaStream_t s) {
   uint32_t flags = 0;
   cudaError_t e = read_error_flags(&flags, s);
   if (e != cudaSuccess) return cuda_status(e, "error flags");
+  if (flags & kErrfStall) {
+    set_error("a kernel's bounded wait gave up; the output is not valid");
+    return AV1PF_ERR_TIMEOUT;
+  }
   if (flags) {
     set_error("the maps broke a conformance requirement (bad block / transform size or edge position)");
     return AV1PF_ERR_INVALID_INPUT;

@@ -36,7 +36,9 @@ extern __device__ uint16_t g_rng_jump82[73][16];
 extern __device__ uint16_t g_rng_jump44[73][16];
 // Sticky device-side error bits (bad map values met by a kernel).
 extern __device__ uint32_t g_error_flags;
-enum : uint32_t { ERRF_BAD_MAP = 1u, ERRF_BAD_ITEM = 2u };
+// ERRF_STALL (kErrfStall on the host): a bounded wait inside a kernel gave
+// up, so its result is not valid.
+enum : uint32_t { ERRF_BAD_MAP = 1u, ERRF_BAD_ITEM = 2u, ERRF_STALL = 4u };
 
 // ---------------------------------------------------------------------------
 // Integer helpers (consts.rs:328-368, bits.rs:112)

@@ -13,8 +13,9 @@
 //     template row) and each thread starts its row from there.
 //   - The auto-regressive filter is a raster recurrence whose reach is at
 //     most 3 columns left and 3 rows up (3 columns right on earlier rows),
-//     so cells with equal (x - 3) + 4 (y - 3) are independent: one thread
-//     per template row walks the anti-diagonal wavefront.
+//     so cells with equal (x - 3) + 4 (y - 3) are independent: one warp per
+//     template walks that wavefront, a lane per row on it, with warp-level
+//     synchronisation only; the chroma warps trail the luma warp.
 // output_kernel: per 256-column tile of a plane's visible area, reads the reference
 // frame, adds grain (noise assembled from the templates, the 32x32 block
 // offsets and the overlap blends of grain.rs:179-283, evaluated per sample
@@ -45,83 +46,133 @@ constexpr int kTH = 73, kTW = 82;
 constexpr int kOutOffs = 18;
 }  // namespace
 
-// Luma auto-regression (grain.rs:55-73) with lag LAG: thread `rr` owns
-// template row 3 + rr and walks the wavefront (x - 3) + 4 * rr = t, so every
-// cell's earlier neighbours (left in its row, up to LAG right in the rows
-// above) are done one step earlier. Coefficients live in registers.
-template <int LAG>
-__device__ __forceinline__ void ar_luma(int16_t (*T)[kTW], const int32_t* coef_s, int ar_shift, int gmin, int gmax) {
-  constexpr int NC = 2 * LAG * (LAG + 1);
-  int c[NC > 0 ? NC : 1];
-#pragma unroll
-  for (int k = 0; k < NC; k++) c[k] = coef_s[k];
-  const int rr = threadIdx.x;
-  const int y = 3 + rr;
-  const int steps = (kTW - 3 - 3 - 1) + 4 * (kTH - 3 - 1) + 1;
-  for (int t = 0; t < steps; t++) {
-    const int x = 3 + t - 4 * rr;
-    if (y < kTH && x >= 3 && x < kTW - 3) {
-      int s = 0, pos = 0;
-#pragma unroll
-      for (int dr = -LAG; dr <= 0; dr++)
-#pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++) {
-          if (dr == 0 && dc >= 0) continue;
-          s += T[y + dr][x + dc] * c[pos];
-          pos++;
-        }
-      T[y][x] = int16_t(clip3(gmin, gmax, T[y][x] + round2(s, ar_shift)));
-    }
-    __syncthreads();
-  }
+// Auto-regression of one template (grain.rs:55-73 for luma, :101-134 for
+// chroma with its luma term) by one warp. Template row 3 + rr belongs to lane
+// rr % 32 and is walked left to right along the wavefront (x - 3) + 4 rr = t:
+// a cell's left neighbours in its row were done at steps t-1..t-LAG by the
+// same lane (kept in registers), and its neighbours in the rows above, at
+// most LAG columns to the right, at step t-1 or earlier by the lanes before
+// it. At most 20 rows are on the wavefront at once, so no two of a lane's
+// rows are. The luma warp publishes its completed step count in `progress`;
+// a chroma warp waits, before each step, for the luma cells its luma term
+// reads (a bounded wait: after kSpinLimit polls it flags ERRF_STALL and
+// goes on).
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];"
+               : "=r"(v)
+               : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p)))
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "r"(v)
+               : "memory");
 }
 
-// Chroma auto-regression with the luma term (grain.rs:101-134): threads
-// 0..127 take Cb rows, 128..255 Cr rows, same wavefront as the luma one.
-template <int LAG>
-__device__ __forceinline__ void ar_chroma(int16_t (*T)[kTH][kTW], const int32_t (*coef_s)[25], int ar_shift, int gmin,
-                                          int gmax, int chroma_w, int chroma_h, int sub_x, int sub_y, bool luma_on) {
+template <int LAG, bool CHROMA>
+__device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kTW], const int32_t* coef_s, int H,
+                                        int W, int ar_shift, int gmin, int gmax, int sub_x, int sub_y, bool luma_on,
+                                        uint32_t* progress) {
   constexpr int NC = 2 * LAG * (LAG + 1);
-  const int plane = threadIdx.x < 128 ? 1 : 2;
   int c[NC + 1];
 #pragma unroll
-  for (int k = 0; k <= NC; k++) c[k] = coef_s[plane][k];
-  const int rr = threadIdx.x & 127;
-  const int y = 3 + rr;
-  const int steps = (chroma_w - 3 - 3 - 1) + 4 * (chroma_h - 3 - 1) + 1;
+  for (int k = 0; k <= NC; k++) c[k] = coef_s[k];
+  const int lane = threadIdx.x & 31;
+  const int rows = H - 3, cols = W - 6;
+  const int steps = (cols - 1) + 4 * (rows - 1) + 1;
+  int l1 = 0, l2 = 0, l3 = 0;  // the lane's row at x-1, x-2, x-3
+  uint32_t seen = 0;           // luma steps known complete
   for (int t = 0; t < steps; t++) {
+    const int q = t >> 2;
+    const int rr = q - ((q - lane) & 31);  // the lane's row on this step's wavefront
     const int x = 3 + t - 4 * rr;
-    if (y < chroma_h && x >= 3 && x < chroma_w - 3) {
-      int s = 0, pos = 0;
-#pragma unroll
-      for (int dr = -LAG; dr <= 0; dr++)
-#pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++) {
-          if (dr == 0 && dc >= 0) continue;
-          s += T[plane][y + dr][x + dc] * c[pos];
-          pos++;
+    const bool active = rr >= 0 && rr < rows && x < W - 3;
+    const int y = 3 + rr;
+    if (CHROMA && luma_on) {
+      // the last luma step whose cell this step's luma terms read
+      const int need = active ? ((x - 3) << sub_x) + sub_x + 4 * (((y - 3) << sub_y) + sub_y) : -1;
+      const int wneed = __reduce_max_sync(0xffffffffu, need);
+      if (wneed >= int(seen)) {
+        int spins = 0;
+        while ((seen = ld_acquire_cta(progress)) <= uint32_t(wneed)) {
+          if (++spins > kSpinLimit) {
+            if (lane == 0) atomicOr(&g_error_flags, ERRF_STALL);
+            break;
+          }
         }
-      if (luma_on) {
-        int luma = 0;
-        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
-        for (int i = 0; i <= sub_y; i++)
-          for (int j = 0; j <= sub_x; j++) luma += T[0][ly + i][lx + j];
-        luma = round2(luma, sub_x + sub_y);
-        s += luma * c[NC];
       }
-      T[plane][y][x] = int16_t(clip3(gmin, gmax, T[plane][y][x] + round2(s, ar_shift)));
     }
-    __syncthreads();
+    if (active) {
+      if (x == 3) {  // a new row: its first three columns are not filtered
+        l1 = T[y][2];
+        l2 = T[y][1];
+        l3 = T[y][0];
+      }
+      int s[LAG + 2] = {};
+#pragma unroll
+      for (int dr = -LAG; dr < 0; dr++)
+#pragma unroll
+        for (int dc = -LAG; dc <= LAG; dc++) s[LAG + dr] += T[y + dr][x + dc] * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
+      const int lp = LAG * (2 * LAG + 1);
+      if (LAG >= 1) s[LAG] += l1 * c[lp + LAG - 1];
+      if (LAG >= 2) s[LAG] += l2 * c[lp + LAG - 2];
+      if (LAG >= 3) s[LAG] += l3 * c[lp + LAG - 3];
+      if (CHROMA && luma_on) {
+        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
+        int luma = Y[ly][lx];
+        if (sub_x) luma += Y[ly][lx + 1];
+        if (sub_y) luma += Y[ly + 1][lx];
+        if (sub_x && sub_y) luma += Y[ly + 1][lx + 1];
+        s[LAG + 1] = round2(luma, sub_x + sub_y) * c[NC];
+      }
+      int sum = 0;
+#pragma unroll
+      for (int k = 0; k < LAG + 2; k++) sum += s[k];
+      const int v = clip3(gmin, gmax, T[y][x] + round2(sum, ar_shift));
+      T[y][x] = int16_t(v);
+      l3 = l2;
+      l2 = l1;
+      l1 = v;
+    }
+    if (!CHROMA) {
+      __threadfence_block();
+      __syncwarp();
+      if (lane == 0) st_release_cta(progress, uint32_t(t + 1));
+    } else {
+      __syncwarp();
+    }
   }
 }
 
+template <bool CHROMA>
+__device__ __forceinline__ void ar_plane(int lag, int16_t (*T)[kTW], const int16_t (*Y)[kTW], const int32_t* coef,
+                                         int H, int W, int ar_shift, int gmin, int gmax, int sub_x, int sub_y,
+                                         bool luma_on, uint32_t* progress) {
+  switch (lag) {
+    case 0: ar_warp<0, CHROMA>(T, Y, coef, H, W, ar_shift, gmin, gmax, sub_x, sub_y, luma_on, progress); break;
+    case 1: ar_warp<1, CHROMA>(T, Y, coef, H, W, ar_shift, gmin, gmax, sub_x, sub_y, luma_on, progress); break;
+    case 2: ar_warp<2, CHROMA>(T, Y, coef, H, W, ar_shift, gmin, gmax, sub_x, sub_y, luma_on, progress); break;
+    default: ar_warp<3, CHROMA>(T, Y, coef, H, W, ar_shift, gmin, gmax, sub_x, sub_y, luma_on, progress); break;
+  }
+}
+
+// One CTA of 256 threads per frame. All threads fill the templates with
+// Gaussian values (one template row each). Then warps 0, 1 and 2 run the
+// luma, Cb and Cr auto-regressions side by side, chroma trailing luma,
+// while warps 3-7 build the scaling tables (one entry per thread) and the
+// per-stripe block offsets (one stripe per thread).
 __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __restrict__ frames,
                                                          const Item* __restrict__ items, int n_items) {
-  __shared__ int16_t T[3][kTH][kTW];
+  __shared__ __align__(16) int16_t T[3][kTH][kTW];
   __shared__ int32_t coef[3][25];
-  __shared__ int32_t lut[3][256];
+  __shared__ uint8_t lut[3][256];
   __shared__ int16_t gauss[2048];
+  __shared__ uint32_t progress;
   const int tid = threadIdx.x;
+  const int warp = tid >> 5;
   for (int k = tid; k < 2048; k += 256) gauss[k] = g_gaussian[k];
   pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
@@ -137,24 +188,22 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
     const int chroma_w = sub_x ? 44 : 82, chroma_h = sub_y ? 38 : 73;
     const uint32_t seed = uint32_t(g.grain_seed) & 0xffffu;
     // --- Gaussian fill (grain.rs:43-54, 78-100) ---
-    for (int k = tid; k < 3 * kTH * kTW; k += 256) (&T[0][0][0])[k] = 0;
+    for (int k = tid; k < 3 * kTH * kTW / 2; k += 256) reinterpret_cast<uint32_t*>(&T[0][0][0])[k] = 0u;
     if (tid < 25) {
       coef[0][tid] = tid < 24 ? g.ar_coeffs_y_plus_128[tid] - 128 : 0;
       coef[1][tid] = g.ar_coeffs_cb_plus_128[tid] - 128;
       coef[2][tid] = g.ar_coeffs_cr_plus_128[tid] - 128;
     }
+    if (tid == 0) progress = 0u;
     __syncthreads();
     {
-      int plane = -1, row = 0;
-      if (tid < kTH) {
+      int plane = -1, row = tid;
+      if (row < kTH) {
         plane = 0;
-        row = tid;
-      } else if (tid >= 80 && tid < 80 + chroma_h && !mono) {
+      } else if (!mono && (row -= kTH) < chroma_h) {
         plane = 1;
-        row = tid - 80;
-      } else if (tid >= 160 && tid < 160 + chroma_h && !mono) {
+      } else if (!mono && (row -= chroma_h) < chroma_h) {
         plane = 2;
-        row = tid - 160;
       }
       if (plane >= 0) {
         const bool on = plane == 0 ? g.num_y_points > 0
@@ -171,65 +220,60 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
       }
     }
     __syncthreads();
-    // --- auto-regression (grain.rs:55-134) ---
     const int lag = g.ar_coeff_lag;
     const int ar_shift = g.ar_coeff_shift_minus_6 + 6;
-    switch (lag) {
-      case 0: ar_luma<0>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
-      case 1: ar_luma<1>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
-      case 2: ar_luma<2>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
-      default: ar_luma<3>(T[0], coef[0], ar_shift, grain_min, grain_max); break;
-    }
-    if (!mono) {
-      const bool luma_on = g.num_y_points > 0;
-      switch (lag) {
-        case 0: ar_chroma<0>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
-        case 1: ar_chroma<1>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
-        case 2: ar_chroma<2>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
-        default: ar_chroma<3>(T, coef, ar_shift, grain_min, grain_max, chroma_w, chroma_h, sub_x, sub_y, luma_on); break;
-      }
-    }
-    // --- scaling lookup (grain.rs:137-165): one thread per plane, as written ---
-    if (tid < 3) {
-      const int plane = tid;
-      int np = 0;
-      const int32_t *xs = nullptr, *ys = nullptr;
-      if (plane == 0 || g.chroma_scaling_from_luma) {
-        np = g.num_y_points; xs = g.point_y_value; ys = g.point_y_scaling;
-      } else if (plane == 1) {
-        np = g.num_cb_points; xs = g.point_cb_value; ys = g.point_cb_scaling;
-      } else {
-        np = g.num_cr_points; xs = g.point_cr_value; ys = g.point_cr_scaling;
-      }
-      for (int x = 0; x < 256; x++) lut[plane][x] = 0;
-      if (np > 0 && !(mono && plane > 0)) {
-        for (int x = 0; x < min(xs[0], 256); x++) lut[plane][x] = ys[0];
-        for (int i = 0; i < np - 1; i++) {
-          const int dy = ys[i + 1] - ys[i], dx = xs[i + 1] - xs[i];
-          if (dx <= 0) continue;  // the format requires increasing points
-          const int delta = dy * ((65536 + (dx >> 1)) / dx);
-          for (int x = 0; x < dx; x++) {
-            const int idx = xs[i] + x;
-            if (idx >= 0 && idx < 256) lut[plane][idx] = ys[i] + ((x * delta + 32768) >> 16);
-          }
+    if (warp == 0) {
+      // --- luma auto-regression (grain.rs:55-73) ---
+      ar_plane<false>(lag, T[0], T[0], coef[0], kTH, kTW, ar_shift, grain_min, grain_max, 0, 0, false, &progress);
+    } else if (warp <= 2) {
+      // --- chroma auto-regression with the luma term (grain.rs:101-134) ---
+      if (!mono)
+        ar_plane<true>(lag, T[warp], T[0], coef[warp], chroma_h, chroma_w, ar_shift, grain_min, grain_max, sub_x,
+                       sub_y, g.num_y_points > 0, &progress);
+    } else {
+      // --- scaling lookup (grain.rs:137-165), one entry per thread: the
+      // later of the reference's writes to an entry is the one kept ---
+      for (int k = tid - 96; k < 3 * 256; k += 160) {
+        const int plane = k >> 8, x = k & 255;
+        int np = 0;
+        const int32_t *xs = nullptr, *ys = nullptr;
+        if (plane == 0 || g.chroma_scaling_from_luma) {
+          np = g.num_y_points; xs = g.point_y_value; ys = g.point_y_scaling;
+        } else if (plane == 1) {
+          np = g.num_cb_points; xs = g.point_cb_value; ys = g.point_cb_scaling;
+        } else {
+          np = g.num_cr_points; xs = g.point_cr_value; ys = g.point_cr_scaling;
         }
-        for (int x = max(xs[np - 1], 0); x < 256; x++) lut[plane][x] = ys[np - 1];
+        int v = 0;
+        if (np > 0 && !(mono && plane > 0)) {
+          if (x < xs[0]) v = ys[0];
+          for (int i = 0; i < np - 1; i++) {
+            const int dy = ys[i + 1] - ys[i], dx = xs[i + 1] - xs[i];
+            if (dx <= 0 || x < xs[i] || x >= xs[i] + dx) continue;  // the format requires increasing points
+            const int delta = dy * ((65536 + (dx >> 1)) / dx);
+            v = ys[i] + (((x - xs[i]) * delta + 32768) >> 16);
+          }
+          if (x >= xs[np - 1]) v = ys[np - 1];
+        }
+        lut[plane][x] = uint8_t(v);
       }
-    }
-    // --- per-stripe block offsets (grain.rs:192-199) ---
-    for (int s = tid; s < f.grain_ns; s += 256) {
-      uint32_t r = seed;
-      r ^= uint32_t(((s * 37 + 178) & 255) << 8);
-      r ^= uint32_t((s * 173 + 105) & 255);
-      for (int b = 0; b < f.grain_nb; b++) {
-        r = rng_step(r);
-        f.grain_off[int64_t(s) * f.grain_nb + b] = uint8_t((r >> 8) & 255u);
+      // --- per-stripe block offsets (grain.rs:192-199) ---
+      for (int s = tid - 96; s < f.grain_ns; s += 160) {
+        uint32_t r = seed;
+        r ^= uint32_t(((s * 37 + 178) & 255) << 8);
+        r ^= uint32_t((s * 173 + 105) & 255);
+        for (int b = 0; b < f.grain_nb; b++) {
+          r = rng_step(r);
+          f.grain_off[int64_t(s) * f.grain_nb + b] = uint8_t((r >> 8) & 255u);
+        }
       }
     }
     __syncthreads();
     GrainScratch* gs = f.grain;
-    for (int k = tid; k < 3 * kTH * kTW; k += 256) (&gs->tmpl[0][0][0])[k] = (&T[0][0][0])[k];
-    for (int k = tid; k < 3 * 256; k += 256) (&gs->lut[0][0])[k] = uint8_t(lut[k >> 8][k & 255]);
+    for (int k = tid; k < 3 * kTH * kTW / 2; k += 256)
+      reinterpret_cast<uint32_t*>(&gs->tmpl[0][0][0])[k] = reinterpret_cast<const uint32_t*>(&T[0][0][0])[k];
+    for (int k = tid; k < 3 * 256 / 4; k += 256)
+      reinterpret_cast<uint32_t*>(&gs->lut[0][0])[k] = reinterpret_cast<const uint32_t*>(&lut[0][0])[k];
     __syncthreads();
   }
 }

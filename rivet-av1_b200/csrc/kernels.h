@@ -119,7 +119,9 @@ void launch_output(const FrameDesc* frames, const Item* items, int n_items, cuda
 // Uploads the LFSR jump-ahead tables (once per device).
 cudaError_t upload_grain_tables();
 
-// Device error flags (g_error_flags): read and clear.
+// Device error flags (g_error_flags): read and clear. This bit of them
+// means a kernel's bounded wait gave up (ERRF_STALL in common.cuh).
+constexpr uint32_t kErrfStall = 4u;
 cudaError_t read_error_flags(uint32_t* flags, cudaStream_t s);
 
 }  // namespace av1pf
