@@ -380,7 +380,10 @@ typedef struct av1pf_tuning {
    *    staged with 16 columns of halo), horizontal edges from a list;
    * 2: as 1, with the horizontal edges filtered inside the CDEF kernel on
    *    its staged superblock window (frames with CDEF enabled; others use
-   *    mode 1). */
+   *    mode 1);
+   * 3: one kernel per 64x64 tile stages the tile and 8 samples of halo on
+   *    every side once, filters the vertical edges (halo rows included) and
+   *    then the horizontal edges in shared memory, and writes the tile. */
   int32_t lf_mode;
   /* 0: per frame shape, as measured (64 while unmeasured); 32 or 64: the
    *    width of the loop-restoration rectangles one CTA restores. */
@@ -399,7 +402,7 @@ int av1pf_get_tuning(av1pf_ctx* ctx, av1pf_tuning* tuning);
  * recorded are measured again. *n_shapes (may be NULL) = shapes measured. */
 int av1pf_autotune(av1pf_ctx* ctx, const av1pf_job* jobs, int n_jobs, int32_t reps, int32_t* n_shapes);
 
-/* The recorded choice for the shape of `info` (lf_mode 0-2 and
+/* The recorded choice for the shape of `info` (lf_mode 0-3 and
  * lr_rect_cols) and its measured device time per frame in ms;
  * AV1PF_ERR_NOT_FOUND when the shape has not been measured. */
 int av1pf_tuned_choice(av1pf_ctx* ctx, const av1pf_frame_info* info, av1pf_tuning* choice, float* ms);

@@ -53,6 +53,8 @@ void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uin
 // included); horizontal decisions appended to list_h when item kind bit 2.
 void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_h, uint32_t* counts,
                      uint32_t cap, cudaStream_t s);
+// Both directions per 64x64 tile in shared memory (copy in -> cur included).
+void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,
                      cudaStream_t s);
 void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s);

@@ -390,6 +390,200 @@ __global__ void __launch_bounds__(256, 4) lf_tile_kernel(const FrameDesc* __rest
   }
 }
 
+namespace {
+constexpr int kFT = 64;             // fused tile side (samples)
+constexpr int kFH = 8;              // halo on each side: the widest filter reads 7 samples past its edge
+constexpr int kFW = kFT + 2 * kFH;  // window side (80)
+constexpr int kFS = 88;             // window row stride (u16): rows 16-byte aligned
+constexpr int kFCR = kFW / 4;       // 4x4 rows of the window (20): vertical edges of every staged row
+constexpr int kFCC = kFT / 4 + 1;   // 4x4 columns with vertical edges (17): the tile's 16 + the right neighbour's first
+constexpr int kFCells = kFCR * kFCC;
+constexpr int kFChunks = kFW / 8 * kFW;  // 8-sample chunks of the window (800)
+}  // namespace
+
+// Loop filter, both passes, one 64x64 tile per CTA (kind bit 0: the tile is
+// copied in -> cur; bit 1: it overlaps the mode-info area and is filtered).
+// The tile and 8 samples on every side are staged once from the unfiltered
+// input. Every vertical edge that changes a staged row at the tile's columns
+// (edges at x0 .. x0 + 64) is filtered in shared memory, including the 8
+// halo rows above and below, which the horizontal edges at y0 .. y0 + 64
+// read; then those horizontal edges are filtered, and only the tile's own
+// samples are written to cur. Neighbouring tiles recompute the halo rows'
+// vertical edges and the shared horizontal edge at their boundary from the
+// same input, so no tile reads what another writes. This is exact by the
+// same property as the in-place passes: for conformant maps no edge of a
+// pass reads a sample another edge of that pass changes. The active edges of
+// each pass are listed in shared memory grouped by filter size, so a warp's
+// lanes mostly take one filter path. 256 threads.
+__global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __restrict__ frames,
+                                                       const Item* __restrict__ items, int n_items) {
+  const LfTables& tb = g_lf_tables;
+  __shared__ __align__(16) uint16_t W[kFW * kFS];
+  __shared__ uint32_t list_v[kFCells], list_h[kFCells];
+  __shared__ uint32_t cnt[2][4], base[2][4];
+  const int tid = threadIdx.x;
+  pdl_wait();  // the previous stage's output is complete past this point
+  FOR_EACH_ITEM(it, n_items) {
+    const Item item = items[it];
+    const FrameDesc& f = frames[item.frame];
+    const int plane = item.plane;
+    const DPlane src = f.in[plane], dst = f.cur[plane];
+    const int sb = f.sb;
+    const int x0 = item.x0, y0 = item.y0;
+    const int x1 = min(int(item.x1), src.w), y1 = min(int(item.y1), src.h);
+    const int rows = y1 - y0;
+    const bool filt = (item.kind & 2) != 0;
+    const int wx0 = x0 - kFH, wy0 = y0 - kFH;
+    if (tid < 8) (&cnt[0][0])[tid] = 0u;  // every thread read the previous item's counts
+    __syncthreads();  // the previous item's window is written out
+    // --- stage the window: a filtered tile takes all of it, a copied one its own samples ---
+    const int r_lo = filt ? 0 : kFH, r_hi = filt ? kFW : kFH + rows;
+    const int c_lo = filt ? 0 : 1, c_hi = filt ? kFW / 8 : 1 + kFT / 8;
+    uint2 q8[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = tid + m * 256;
+      const int r = k / 10, ch = k - r * 10;
+      q8[m] = make_uint2(0u, 0u);
+      if (k >= kFChunks || r < r_lo || r >= r_hi || ch < c_lo || ch >= c_hi) continue;
+      const int gy = wy0 + r, gx = wx0 + ch * 8;
+      uint16_t* wp = &W[r * kFS + ch * 8];
+      if (gy < 0 || gy >= src.h) {
+        *reinterpret_cast<uint4*>(wp) = make_uint4(0u, 0u, 0u, 0u);
+        continue;
+      }
+      const uint8_t* rp = src.p + int64_t(gy) * src.stride * sb;
+      if (gx >= 0 && gx + 8 <= src.w) {
+        if (sb == 2)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(
+                           __cvta_generic_to_shared(wp))),
+                       "l"(rp + int64_t(gx) * 2)
+                       : "memory");
+        else
+          q8[m] = *reinterpret_cast<const uint2*>(rp + gx);
+      } else {
+        for (int e = 0; e < 8; e++) {
+          const int x = gx + e;
+          wp[e] = (x >= 0 && x < src.w) ? uint16_t(sb == 1 ? rp[x] : reinterpret_cast<const uint16_t*>(rp)[x]) : 0;
+        }
+      }
+    }
+    // --- decisions: vertical edges of the window's 20 x 17 cells, horizontal
+    // edges of the tile's 17 x 16 (postfilter.rs:107-264) ---
+    int dv[2] = {0, 0}, dh[2] = {0, 0};
+    const int cx0 = x0 >> 2, cy0 = (y0 >> 2) - 2;
+    if (filt) {
+      const int sx = plane_ssx(f, plane), sy = plane_ssy(f, plane);
+      const int gw = f.mi_cols >> sx, gh = f.mi_rows >> sy;
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        const int k = tid + m * 256;
+        if (k >= kFCells) break;
+        const int i = k / kFCC, j = k - i * kFCC;
+        const int cx = cx0 + j, cy = cy0 + i;
+        if (cx < 0 || cy < 0 || cx >= gw || cy >= gh) continue;
+        int v = 0, h = 0;
+        lf_decide2(f, tb, plane, cx, cy, v, h);
+        // a conformant map keeps wide edges off the plane start
+        if (v && cx * 4 < ((v >> 6) == 3 ? 8 : 4)) {
+          atomicOr(&g_error_flags, ERRF_BAD_MAP);
+          v = 0;
+        }
+        if (h && cy * 4 < ((h >> 6) == 3 ? 8 : 4)) {
+          atomicOr(&g_error_flags, ERRF_BAD_MAP);
+          h = 0;
+        }
+        dv[m] = v;
+        if (i >= 2 && i <= 2 + kFT / 4 && j < kFT / 4) dh[m] = h;
+      }
+    }
+    // u8 samples widen to the u16 window
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = tid + m * 256;
+      const int r = k / 10, ch = k - r * 10;
+      if (sb != 1 || k >= kFChunks || r < r_lo || r >= r_hi || ch < c_lo || ch >= c_hi) continue;
+      const int gy = wy0 + r, gx = wx0 + ch * 8;
+      if (gy < 0 || gy >= src.h || gx < 0 || gx + 8 > src.w) continue;
+      uint16_t* wp = &W[r * kFS + ch * 8];
+      *reinterpret_cast<uint4*>(wp) =
+          make_uint4(__byte_perm(q8[m].x, 0, 0x4140), __byte_perm(q8[m].x, 0, 0x4342),
+                     __byte_perm(q8[m].y, 0, 0x4140), __byte_perm(q8[m].y, 0, 0x4342));
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (filt) {
+      // --- the active edges of each pass, grouped by filter size ---
+      uint32_t iv[2], ih[2];
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        iv[m] = dv[m] ? atomicAdd(&cnt[0][dv[m] >> 6], 1u) : 0u;
+        ih[m] = dh[m] ? atomicAdd(&cnt[1][dh[m] >> 6], 1u) : 0u;
+      }
+      __syncthreads();
+      if (tid < 2) {
+        uint32_t run = 0;
+        for (int c = 3; c >= 1; c--) {
+          base[tid][c] = run;
+          run += cnt[tid][c];
+        }
+        cnt[tid][0] = run;  // the pass's edge count
+      }
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        const int k = tid + m * 256;
+        const int i = k / kFCC, j = k - i * kFCC;
+        if (dv[m]) list_v[base[0][dv[m] >> 6] + iv[m]] = uint32_t(j) | (uint32_t(i) << 5) | (uint32_t(dv[m]) << 10);
+        if (dh[m]) list_h[base[1][dh[m] >> 6] + ih[m]] = uint32_t(j) | (uint32_t(i - 2) << 5) | (uint32_t(dh[m]) << 10);
+      }
+      __syncthreads();
+      const int bd = f.bd, sharp = f.sharpness;
+      const bool chroma = plane != 0;
+      // --- vertical edges: (edge, row lane) per thread ---
+      const int nv = int(cnt[0][0]) * 4;
+      for (int t = tid; t < nv; t += 256) {
+        const uint32_t e = list_v[t >> 2];
+        const int j = int(e & 31u), i = int((e >> 5) & 31u), d = int(e >> 10);
+        lf_filter_smem(&W[(i * 4 + (t & 3)) * kFS + kFH + j * 4], 1, d >> 6, chroma, bd, d & 63, sharp);
+      }
+      __syncthreads();
+      // --- horizontal edges: (edge, column lane) per thread ---
+      const int nh = int(cnt[1][0]) * 4;
+      for (int t = tid; t < nh; t += 256) {
+        const uint32_t e = list_h[t >> 2];
+        const int j = int(e & 31u), i = int((e >> 5) & 31u), d = int(e >> 10);
+        lf_filter_smem(&W[(kFH + i * 4) * kFS + kFH + j * 4 + (t & 3)], kFS, d >> 6, chroma, bd, d & 63, sharp);
+      }
+    }
+    __syncthreads();
+    // --- write the tile's own samples [x0, x1) x [y0, y1) ---
+    {
+      const int w = x1 - x0;
+      const int nvec = w >> 3;  // 8-sample groups
+      for (int k = tid; k < rows * 8; k += 256) {
+        const int r = k >> 3, g = k & 7;
+        uint8_t* rp = dst.p + int64_t(y0 + r) * dst.stride * sb;
+        const uint16_t* wp = &W[(kFH + r) * kFS + kFH + g * 8];
+        if (g < nvec) {
+          const uint4 q = *reinterpret_cast<const uint4*>(wp);
+          if (sb == 2)
+            *reinterpret_cast<uint4*>(rp + int64_t(x0 + g * 8) * 2) = q;
+          else
+            *reinterpret_cast<uint2*>(rp + x0 + g * 8) =
+                make_uint2(__byte_perm(q.x, q.y, 0x6420), __byte_perm(q.z, q.w, 0x6420));
+        } else if (g == nvec) {
+          for (int e = 0; e < w - nvec * 8; e++) {
+            if (sb == 2)
+              reinterpret_cast<uint16_t*>(rp)[x0 + g * 8 + e] = wp[e];
+            else
+              rp[x0 + g * 8 + e] = uint8_t(wp[e]);
+          }
+        }
+      }
+    }
+  }
+}
+
 // dsp::lf::filter (lf.rs:25) on independent edges: one thread per lane.
 __global__ void dsp_lf_kernel(int32_t* __restrict__ edges, const av1pf_lf_edge_params* __restrict__ prm, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -420,6 +614,11 @@ void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, ui
                      uint32_t cap, cudaStream_t s) {
   if (n_items <= 0) return;
   launch_pdl(lf_tile_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items, list_h, counts, cap);
+}
+
+void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
+  if (n_items <= 0) return;
+  launch_pdl(lf_fused_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items);
 }
 
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,

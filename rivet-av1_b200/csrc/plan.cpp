@@ -174,8 +174,8 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   if (items) {
     // the lists keep their capacity from call to call (a chain call plans
     // one frame of the same shape again and again)
-    for (auto* v : {&plan.lf_items, &plan.lft_items, &plan.cdef_items, &plan.sr_items, &plan.lr_items,
-                    &plan.grain_items, &plan.out_items, &plan.copy_items})
+    for (auto* v : {&plan.lf_items, &plan.lft_items, &plan.lff_items, &plan.cdef_items, &plan.sr_items,
+                    &plan.lr_items, &plan.grain_items, &plan.out_items, &plan.copy_items})
       v->clear();
     plan.edge_cap = 0;
     plan.any_hlist = false;
@@ -183,7 +183,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     plan.cdef_half = false;
     plan.sr_row_max = 0;
     plan.any_lf = plan.any_cdef = plan.any_sr = plan.any_lr = plan.any_grain = plan.any_out = false;
-    plan.off_frames = plan.off_lf = plan.off_lft = plan.off_cdef = plan.off_sr = plan.off_lr = plan.off_grain =
+    plan.off_frames = plan.off_lf = plan.off_lft = plan.off_lff = plan.off_cdef = plan.off_sr = plan.off_lr = plan.off_grain =
         plan.off_out = plan.off_copy = plan.off_edges_v = plan.off_edges_h = plan.off_counts = plan.meta_bytes =
             plan.upload_bytes = 0;
   }
@@ -253,7 +253,8 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
     const bool lf_frame = (j.stages & ST_LF) && (p->loop_filter_level[0] || p->loop_filter_level[1]);
     // horizontal edges inside the CDEF kernel: needs the chain's copy of the
     // input (cur is not the caller's) and a CDEF pass to carry them
-    const bool tiles = !j.in_place_lf && j.lf_mode >= 1;
+    const bool tiles = !j.in_place_lf && (j.lf_mode == 1 || j.lf_mode == 2);
+    const bool fused = !j.in_place_lf && j.lf_mode == 3;
     const bool fuse_h = lf_frame && chain && tiles && j.lf_mode == 2 && (j.stages & ST_CDEF) && p->cdef_enabled;
     for (int k = 0; k < np; k++) {
       d.in[k] = from_abi(j.in[k]);
@@ -268,6 +269,22 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       if (j.in_place_lf) {
         d.cur[k] = d.in[k];
         if (items) add_tiles(plan.lf_items, fi, k, 2, gw * 4, gh * 4, kTile, kTile);
+      } else if (fused) {
+        // copy in -> cur with both passes filtered per tile
+        d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
+        const int W = d.in[k].w, H = d.in[k].h;
+        for (int y = 0; items && y < H; y += kTile)
+          for (int x = 0; x < W; x += kTile) {
+            Item it{};
+            it.frame = uint16_t(fi);
+            it.plane = uint8_t(k);
+            it.kind = uint8_t(1 | ((x < gw * 4 && y < gh * 4) ? 2 : 0));
+            it.x0 = uint16_t(x);
+            it.y0 = uint16_t(y);
+            it.x1 = uint16_t(std::min(x + kTile, W));
+            it.y1 = uint16_t(std::min(y + kTile, H));
+            plan.lff_items.push_back(it);
+          }
       } else if (!tiles) {
         // copy in -> cur and decide every 4x4 edge into the two edge lists
         d.cur[k] = bump.plane(d.in[k].w, d.in[k].h, sb);
@@ -486,6 +503,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   plan.off_frames = place(plan.frames.size() * sizeof(FrameDesc));
   plan.off_lf = place(plan.lf_items.size() * sizeof(Item));
   plan.off_lft = place(plan.lft_items.size() * sizeof(Item));
+  plan.off_lff = place(plan.lff_items.size() * sizeof(Item));
   plan.off_cdef = place(plan.cdef_items.size() * sizeof(Item));
   plan.off_sr = place(plan.sr_items.size() * sizeof(Item));
   plan.off_lr = place(plan.lr_items.size() * sizeof(Item));
@@ -530,6 +548,7 @@ void pack_meta(const Plan& plan, uint8_t* host) {
   put(plan.off_frames, plan.frames.data(), plan.frames.size() * sizeof(FrameDesc));
   put(plan.off_lf, plan.lf_items.data(), plan.lf_items.size() * sizeof(Item));
   put(plan.off_lft, plan.lft_items.data(), plan.lft_items.size() * sizeof(Item));
+  put(plan.off_lff, plan.lff_items.data(), plan.lff_items.size() * sizeof(Item));
   put(plan.off_cdef, plan.cdef_items.data(), plan.cdef_items.size() * sizeof(Item));
   put(plan.off_sr, plan.sr_items.data(), plan.sr_items.size() * sizeof(Item));
   put(plan.off_lr, plan.lr_items.data(), plan.lr_items.size() * sizeof(Item));
@@ -576,6 +595,8 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     launch_lf_tiles(frames, items(plan.off_lft), int(plan.lft_items.size()), eh, counts, plan.edge_cap, s);
     if (plan.any_hlist) launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
+  if (plan.any_lf && !plan.lff_items.empty())
+    launch_lf_fused(frames, items(plan.off_lff), int(plan.lff_items.size()), s);
   mark(1);
   if (plan.any_cdef)
     launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), plan.any_lfh, plan.cdef_half, s);

@@ -37,7 +37,8 @@ struct FrameJob {
   uint32_t stages;          // StageMask
   bool in_place_lf;         // av1pf_loop_filter: filter `in` in place
   // chain only (av1pf_tuning.lf_mode): 0 decisions + edge lists, 1 vertical
-  // edges per tile, 2 as 1 with the horizontal edges inside the CDEF kernel
+  // edges per tile, 2 as 1 with the horizontal edges inside the CDEF kernel,
+  // 3 both directions per tile in one kernel
   int lf_mode = 0;
   int lr_cols = 64;  // loop-restoration rectangle width (<= 64)
 };
@@ -45,7 +46,8 @@ struct FrameJob {
 // Work lists of every stage for a set of frames.
 struct Plan {
   std::vector<FrameDesc> frames;
-  std::vector<Item> lf_items, lft_items, cdef_items, sr_items, lr_items, grain_items, out_items, copy_items;
+  std::vector<Item> lf_items, lft_items, lff_items, cdef_items, sr_items, lr_items, grain_items, out_items,
+      copy_items;
   uint32_t edge_cap = 0;
   size_t scratch_bytes = 0;   // bytes of per-frame scratch (planes, grain)
   bool any_hlist = false;  // some plane's horizontal loop-filter edges run as their own pass
@@ -54,7 +56,7 @@ struct Plan {
   int sr_row_max = 0;      // superres: the most source samples in a row (sr_maxx + 1)
   bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
   // byte offsets of each list in the device meta buffer
-  size_t off_frames = 0, off_lf = 0, off_lft = 0, off_cdef = 0, off_sr = 0, off_lr = 0, off_grain = 0, off_out = 0,
+  size_t off_frames = 0, off_lf = 0, off_lft = 0, off_lff = 0, off_cdef = 0, off_sr = 0, off_lr = 0, off_grain = 0, off_out = 0,
          off_copy = 0, off_edges_v = 0, off_edges_h = 0, off_counts = 0, meta_bytes = 0, upload_bytes = 0;
 };
 

@@ -3,9 +3,10 @@
 // Two knobs change how the chain's work is cut, never what it computes:
 //   - lf_mode: the loop filter as a decision kernel plus one edge-list pass
 //     per direction (0); vertical edges per 64x64 tile in shared memory plus
-//     the horizontal edge list (1); or as 1 with the horizontal edges inside
+//     the horizontal edge list (1); as 1 with the horizontal edges inside
 //     the CDEF kernel on the superblock window it stages anyway, 11 rows of
-//     halo instead of 2 (2);
+//     halo instead of 2 (2); or both directions per 64x64 tile in shared
+//     memory, one kernel (3);
 //   - lr_rect_cols: loop-restoration rectangles of 64 or 32 columns (more,
 //     smaller CTAs balance better on small frames; wider ones re-read less
 //     halo).
@@ -102,13 +103,18 @@ int tune_shapes(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, bool only
     const av1pf_params* p = j.params;
     const bool lf_on = p->loop_filter_level[0] || p->loop_filter_level[1];
     // modes that differ for this frame: none without the loop filter, no
-    // fused pass without CDEF
-    const int modes = !lf_on ? 1 : (p->cdef_enabled ? 3 : 2);
+    // horizontal pass inside CDEF without CDEF
+    std::vector<int> modes{0};
+    if (lf_on) {
+      modes.push_back(1);
+      if (p->cdef_enabled) modes.push_back(2);
+      modes.push_back(3);
+    }
     const bool lr_on = p->uses_lr && (p->frame_restoration_type[0] || p->frame_restoration_type[1] ||
                                       p->frame_restoration_type[2]);
     ShapeChoice best{0, 64, 0.f};
     bool have = false;
-    for (int mode = 0; mode < modes; mode++)
+    for (int mode : modes)
       for (int cols : {64, 32}) {
         if (cols == 32 && !lr_on) continue;
         FrameJob fj{j.info, j.params, j.maps, j.in, nullptr, j.ref_out, j.frame_out, ST_CHAIN, false};
@@ -142,8 +148,9 @@ int tune_batch(Ctx* ctx, const av1pf_job* jobs, int n_jobs, int reps, std::vecto
   for (int i = 0; i < n_jobs; i++) any_cdef = any_cdef || jobs[i].params->cdef_enabled;
   // candidates: each variant for every frame, and the per-shape record
   std::vector<std::vector<FrameJob>> cands;
-  for (int mode = 0; mode < (any_cdef ? 3 : 2); mode++)
+  for (int mode : {0, 1, 2, 3})
     for (int cols : {64, 32}) {
+      if (mode == 2 && !any_cdef) continue;
       std::vector<FrameJob> v;
       for (int i = 0; i < n_jobs; i++) {
         FrameJob fj = base(i);
@@ -188,9 +195,9 @@ extern "C" {
 
 int av1pf_set_tuning(av1pf_ctx* ctx, const av1pf_tuning* t) {
   if (!ctx || !t) return AV1PF_ERR_INVALID_INPUT;
-  if (t->lf_mode < -1 || t->lf_mode > 2 ||
+  if (t->lf_mode < -1 || t->lf_mode > 3 ||
       (t->lr_rect_cols != 0 && t->lr_rect_cols != 32 && t->lr_rect_cols != 64)) {
-    set_error("av1pf_set_tuning: lf_mode must be -1, 0, 1 or 2 and lr_rect_cols 0, 32 or 64");
+    set_error("av1pf_set_tuning: lf_mode must be -1, 0, 1, 2 or 3 and lr_rect_cols 0, 32 or 64");
     return AV1PF_ERR_INVALID_INPUT;
   }
   std::lock_guard<std::mutex> lk(ctx->tune_mu);

@@ -1,8 +1,9 @@
 """Kernel variants and the autotuner: every variant computes the same samples.
 
-The chain runs its loop filter in three ways (edge lists for both
+The chain runs its loop filter in four ways (edge lists for both
 directions; vertical edges per shared-memory tile with a horizontal edge
-list; or the horizontal edges inside the CDEF kernel) and restores 64- or
+list; the horizontal edges inside the CDEF kernel; or both directions per
+shared-memory tile in one kernel) and restores 64- or
 32-column loop-restoration rectangles; each combination is compared with the
 CPU oracle bit for bit on the same synthetic frames as the chain tests (the
 default, mode 0 with 64-column rectangles, is what test_gpu_parity runs). The autotuner is
@@ -25,7 +26,7 @@ if cuda_available():
     import gpu_util as G
     import torch
 
-VARIANTS = [(1, 64), (2, 64), (0, 32), (2, 32)]
+VARIANTS = [(1, 64), (2, 64), (3, 64), (0, 32), (2, 32), (3, 32)]
 
 
 @pytest.fixture(scope="module")
@@ -53,7 +54,7 @@ def test_chain_variant_matches_oracle(ctx, name, variant):
         set_tuning(ctx, -1, 0)
 
 
-@pytest.mark.parametrize("variant", [(1, 64), (2, 64)])
+@pytest.mark.parametrize("variant", [(1, 64), (2, 64), (3, 64)])
 def test_full_hd_variant(ctx, variant):
     set_tuning(ctx, *variant)
     try:
@@ -81,7 +82,7 @@ def test_full_superblock_ctas_with_fused_lf(ctx):
 
 
 def test_tuning_rejects_bad_values(ctx):
-    for bad in [(3, 0), (-2, 0), (0, 48), (1, 128)]:
+    for bad in [(4, 0), (-2, 0), (0, 48), (1, 128)]:
         t = A.Tuning(*bad)
         assert A.lib().av1pf_set_tuning(ctx.p, C.byref(t)) == A.ERR_INVALID_INPUT
     t = A.Tuning()
@@ -118,10 +119,10 @@ def test_autotune_records_shapes_and_keeps_results():
         assert n.value == 3  # the two b10_420 frames share a shape
         for d in dfs:
             A.check(A.lib().av1pf_tuned_choice(c.p, C.byref(d.info), C.byref(t), C.byref(ms)))
-            assert t.lf_mode in (0, 1, 2) and t.lr_rect_cols in (32, 64) and ms.value > 0
-        # CDEF off: the fused mode does not apply, so it is never chosen
+            assert t.lf_mode in (0, 1, 2, 3) and t.lr_rect_cols in (32, 64) and ms.value > 0
+        # CDEF off: the horizontal pass inside CDEF does not apply, so mode 2 is never chosen
         A.check(A.lib().av1pf_tuned_choice(c.p, C.byref(dfs[2].info), C.byref(t), C.byref(ms)))
-        assert t.lf_mode in (0, 1)
+        assert t.lf_mode in (0, 1, 3)
         # the chain and a batch on the recorded choices still match the oracle
         for sf, d in zip(sfs, dfs):
             ref_cpu, fb_cpu = O.chain(sf, threads=0)
