@@ -35,9 +35,17 @@ constexpr int kS = 82;
 constexpr int kTopLfh = 11;     // rows above (and below) with the horizontal LF pass fused
 constexpr int kColOff = 8;       // window column of plane x = px0
 constexpr int16_t kNA = -32768;  // unavailable sample
-// dynamic shared memory of the three windows: R + 2*2 rows, or R + 2*11 with
-// the horizontal loop-filter pass fused in
-constexpr int cdef_smem(int R, bool lfh) { return 3 * (R + 2 * (lfh ? kTopLfh : 2)) * kS * 2; }
+// The direction search reads the R luma rows of the superblock's 64 columns
+// from a copy with 16-byte aligned rows (kDS int16 each): one 16-byte load
+// per block row, and the 8 lanes of a load phase (8 blocks side by side)
+// read 32 consecutive words. (From the filter window, whose odd row stride
+// keeps the filter's loads apart, blocks 8 rows apart would share banks: a
+// 4-way conflict on every load.)
+constexpr int kDS = 72;
+// dynamic shared memory: the direction-search copy, then the three windows
+// of R + 2*2 rows, or R + 2*11 with the horizontal loop-filter pass fused in
+constexpr int cdef_dir_bytes(int R) { return R * kDS * 2; }
+constexpr int cdef_smem(int R, bool lfh) { return cdef_dir_bytes(R) + 3 * (R + 2 * (lfh ? kTopLfh : 2)) * kS * 2; }
 
 // Per 8x8 block and plane: strengths, tap weights and window offsets.
 struct BlkTaps {
@@ -184,15 +192,26 @@ __device__ __forceinline__ int32_t cdef_cost_of(const int32_t* p) {
 }
 
 // Costs of directions P and P + 4 of the 8x8 block whose top-left sample is
-// window word `w0` (4-byte aligned); samples are >> sh then - 128.
-template <int P>
+// `s`, rows ST samples apart; samples are >> sh then - 128. With ST = kDS the
+// rows are 16-byte aligned and each is one 16-byte load, else 4-byte words.
+template <int P, int ST = kS>
 __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int one, int32_t& c1, int32_t& c2) {
   int32_t a[15], b[15];
 #pragma unroll
   for (int k = 0; k < 15; k++) a[k] = b[k] = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    const uint32_t* row = reinterpret_cast<const uint32_t*>(s + i * kS);
+    uint32_t row[4];
+    if (ST == kDS) {
+      const uint4 v = *reinterpret_cast<const uint4*>(s + i * ST);
+      row[0] = v.x;
+      row[1] = v.y;
+      row[2] = v.z;
+      row[3] = v.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; q++) row[q] = reinterpret_cast<const uint32_t*>(s + i * ST)[q];
+    }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const uint32_t w = row[q];
@@ -216,8 +235,11 @@ __device__ __forceinline__ void cdef_cost_pair(const int16_t* s, int sh, int one
 // samples outside the mode-info area as kNA. Window rows are NCH chunks of 8
 // samples (the first chunk starts 8 samples left of the superblock, so loads
 // stay 8-sample aligned); loads issue two at a time before their stores.
+// With `dw` (luma only) the superblock's R rows x 64 columns also go to the
+// direction-search copy (rows kDS apart).
 template <int R, int SX>
-__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int y0, int top, int16_t* wp, int tid) {
+__device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, int y0, int top, int16_t* wp, int tid,
+                                            int16_t* dw = nullptr) {
   constexpr int NT = 4 * R;
   constexpr int NCH = ((64 >> SX) + 16) / 8;
   constexpr int kSlots = ((R + 2 * kTopLfh) * NCH + NT - 1) / NT;
@@ -281,6 +303,8 @@ __device__ __forceinline__ void stage_plane(const FrameDesc& f, int p, int sc, i
       uint32_t* dst = reinterpret_cast<uint32_t*>(wp + r * kS + ch * 8);
 #pragma unroll
       for (int e = 0; e < 4; e++) dst[e] = o[e];
+      if (dw && r >= top && r < top + R && ch >= 1 && ch <= 8)
+        *reinterpret_cast<uint4*>(dw + (r - top) * kDS + (ch - 1) * 8) = make_uint4(o[0], o[1], o[2], o[3]);
     }
   }
 }
@@ -365,10 +389,15 @@ __device__ __forceinline__ void write_prelf(const FrameDesc& f, int p, int sc, i
 // horizontal loop-filter edges (planes in f.lfh_mask) are filtered here, on
 // the staged window, before CDEF. `wrows` is the rows of one plane's window
 // (R + 22 when the launch has kind-1 items, else R + 4).
-template <int R>
+// LFH: the launch has kind-1 items (the fused horizontal loop-filter pass);
+// without it the kernel carries none of that pass's code, which keeps the
+// default kernel's instruction footprint small.
+template <int R, bool LFH>
 __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* __restrict__ frames,
                                                            const Item* __restrict__ items, int n_items, int wrows) {
-  extern __shared__ __align__(16) int16_t cdef_win[];  // [3][wrows * kS]
+  extern __shared__ __align__(16) int16_t cdef_smem_base[];  // [R][kDS] direction copy, then [3][wrows * kS]
+  int16_t* const dwin = cdef_smem_base;
+  int16_t* const cdef_win = cdef_smem_base + cdef_dir_bytes(R) / 2;
   auto win = [&](int p) { return cdef_win + p * wrows * kS; };  // plane p's window
   __shared__ int32_t cost[R][8];
   __shared__ BlkTaps taps[3][R];
@@ -391,7 +420,7 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
     const int np = f.np, sb = f.sb;
     const int cs = f.bd - 8;
     const int idx = f.cdef_idx[int64_t(sr) * f.cdef_stride + sc];  // postfilter.rs:285
-    const bool lfh = item.kind != 0;
+    const bool lfh = LFH && item.kind != 0;
     const int top = lfh ? kTopLfh : 2;  // window row of the superblock's first row
     // --- per 8x8: inside the MI area? skipped? (postfilter.rs:281-287, 306-310) ---
     // (the maps are inputs of the chain: read before waiting for the loop filter)
@@ -418,7 +447,7 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
       if (plane_ssx(f, p))
         stage_plane<R, 1>(f, p, sc, y0, top, win(p), tid);
       else
-        stage_plane<R, 0>(f, p, sc, y0, top, win(p), tid);
+        stage_plane<R, 0>(f, p, sc, y0, top, win(p), tid, p == 0 && !lfh ? dwin : nullptr);
     }
     if (lfh) {
       __syncthreads();
@@ -427,6 +456,12 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
       if (y0 + R == sr * 64 + 64)  // the rows that end the superblock row
         for (int p = 0; p < np; p++)
           if ((f.lfh_mask >> p) & 1) write_prelf<R>(f, p, sc, sr, win(p), tid);
+      // the direction search reads the loop-filtered luma
+      for (int k = tid; k < R * 8; k += 4 * R) {
+        const int r = k >> 3, ch = k & 7;
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(win(0) + (top + r) * kS + kColOff + ch * 8);
+        *reinterpret_cast<uint4*>(dwin + r * kDS + ch * 8) = make_uint4(src[0], src[1], src[2], src[3]);
+      }
     }
     __syncthreads();
     // --- direction search (postfilter.rs:345-401): each thread two directions of one block ---
@@ -435,13 +470,13 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
       const int b = (warp >> 2) * 32 + lane;
       if (bstate[b] == 2) {
         const int by = b >> 3, bx = b & 7;
-        const int16_t* s = &win(0)[(top + by * 8) * kS + kColOff + bx * 8];
+        const int16_t* s = &dwin[by * 8 * kDS + bx * 8];
         int32_t c1, c2;
         switch (pair) {
-          case 0: cdef_cost_pair<0>(s, cs, s_one, c1, c2); break;
-          case 1: cdef_cost_pair<1>(s, cs, s_one, c1, c2); break;
-          case 2: cdef_cost_pair<2>(s, cs, s_one, c1, c2); break;
-          default: cdef_cost_pair<3>(s, cs, s_one, c1, c2); break;
+          case 0: cdef_cost_pair<0, kDS>(s, cs, s_one, c1, c2); break;
+          case 1: cdef_cost_pair<1, kDS>(s, cs, s_one, c1, c2); break;
+          case 2: cdef_cost_pair<2, kDS>(s, cs, s_one, c1, c2); break;
+          default: cdef_cost_pair<3, kDS>(s, cs, s_one, c1, c2); break;
         }
         cost[b][pair] = c1;
         cost[b][pair + 4] = c2;
@@ -939,10 +974,17 @@ __global__ void dsp_cdef_kernel(const int32_t* __restrict__ win, const av1pf_cde
 }
 
 cudaError_t cdef_init() {
-  cudaError_t e = cudaFuncSetAttribute(cdef_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(cdef_kernel<64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        cdef_smem(64, true));
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(cdef_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, cdef_smem(32, true));
+    e = cudaFuncSetAttribute(cdef_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             cdef_smem(32, true));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cdef_kernel<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             cdef_smem(64, false));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cdef_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             cdef_smem(32, false));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(cdef_search_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSearchSmem);
   if (e == cudaSuccess)
@@ -956,12 +998,15 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
   // side: smaller windows, more CTAs per SM
   const int R = half ? 32 : 64;
   const int wrows = R + 2 * (lfh ? kTopLfh : 2);
-  if (half)
-    launch_pdl(cdef_kernel<32>, min(n_items, kItemGrid), 128, size_t(cdef_smem(32, lfh)), s, frames, items, n_items,
-               wrows);
+  const int grid = min(n_items, kItemGrid);
+  if (half && lfh)
+    launch_pdl(cdef_kernel<32, true>, grid, 128, size_t(cdef_smem(32, true)), s, frames, items, n_items, wrows);
+  else if (half)
+    launch_pdl(cdef_kernel<32, false>, grid, 128, size_t(cdef_smem(32, false)), s, frames, items, n_items, wrows);
+  else if (lfh)
+    launch_pdl(cdef_kernel<64, true>, grid, 256, size_t(cdef_smem(64, true)), s, frames, items, n_items, wrows);
   else
-    launch_pdl(cdef_kernel<64>, min(n_items, kItemGrid), 256, size_t(cdef_smem(64, lfh)), s, frames, items, n_items,
-               wrows);
+    launch_pdl(cdef_kernel<64, false>, grid, 256, size_t(cdef_smem(64, false)), s, frames, items, n_items, wrows);
 }
 
 void launch_cdef_search(const CdefSearchDesc* ds, int n, int blocks, bool thorough, cudaStream_t s) {

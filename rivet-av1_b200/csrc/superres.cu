@@ -8,11 +8,13 @@
 // frame is upscaled only at those rows, into a small line buffer.
 // Item kind 0: rows [y0, y1) of cdef -> up. Kind 1: line rows [y0, y1) of the
 // line buffer (4 per stripe boundary: rows B-2 .. B+1 of the boundary at B).
-// Each source row is staged once in shared memory (16-byte loads), then every
-// output sample reads its 8 taps from there and its filter phase's 8
-// coefficients with one 16-byte load from global memory (through the L1),
-// so CTAs start without staging the filter table. The row buffer is sized
-// per launch to the widest source row among the launch's frames.
+// An item's (at most 4) source rows are staged together in shared memory
+// (16-byte loads), behind one barrier; then each thread makes 8 consecutive
+// output samples of a row, each reading its 8 taps from shared memory and
+// its filter phase's 8 coefficients with one 16-byte load from global memory
+// (through the L1), and stores them as one 16-byte (8-byte at u8) vector.
+// The row buffers are sized per launch to the widest source row among the
+// launch's frames.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -20,12 +22,15 @@ namespace av1pf {
 
 namespace {
 constexpr int kMaxRow = 16384 + 16;  // source samples staged per row, at most
-}
+constexpr int kRows = 4;             // rows per item
+// row stride of the staged rows (u16): 16-byte aligned
+__host__ __device__ constexpr int sr_stride(int n) { return (n + 7) & ~7; }
+}  // namespace
 
 __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restrict__ frames,
-                                                       const Item* __restrict__ items, int n_items) {
+                                                       const Item* __restrict__ items, int n_items, int rs) {
   extern __shared__ __align__(16) uint8_t sr_smem[];
-  uint16_t* row = reinterpret_cast<uint16_t*>(sr_smem);  // staged source row
+  uint16_t* rows = reinterpret_cast<uint16_t*>(sr_smem);  // kRows staged source rows, rs apart
   pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
@@ -51,71 +56,109 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
       dst = kind == 0 ? f.up[p] : f.lines[p];
     }
     const int n_src = max_x + 1;
-    for (int r = item.y0; r < item.y1; r++) {
-      int src_row = r;
+    const int nr = min(int(item.y1) - int(item.y0), kRows);
+    // the source row of output row y0 + k, or -1 outside the plane (uniform across the CTA)
+    auto src_row_of = [&](int k) {
+      const int r = item.y0 + k;
+      int sr = r;
       if (kind == 1) {
         const int s = r / 4 + 1, j = r % 4;
-        const int B = (64 * s - 8) >> sy;
-        src_row = B - 2 + j;
+        sr = ((64 * s - 8) >> sy) - 2 + j;
       }
-      const bool live = src_row >= 0 && src_row < plane_h;  // uniform across the CTA
-      if (live) {
-        const uint8_t* sp = src.p + int64_t(prelf ? r : src_row) * src.stride * sb;
-        if (sb == 2) {
-          const int nv = n_src >> 3;
-          for (int k = threadIdx.x; k < nv; k += blockDim.x)
-            reinterpret_cast<uint4*>(row)[k] = reinterpret_cast<const uint4*>(sp)[k];
-          for (int k = nv * 8 + threadIdx.x; k < n_src; k += blockDim.x)
-            row[k] = reinterpret_cast<const uint16_t*>(sp)[k];
-        } else {
-          for (int k = threadIdx.x; k < n_src; k += blockDim.x) row[k] = sp[k];
+      return sr >= 0 && sr < plane_h ? (prelf ? r : sr) : -1;
+    };
+    // --- stage the rows ---
+    for (int k = 0; k < nr; k++) {
+      const int sr = src_row_of(k);
+      if (sr < 0) continue;
+      const uint8_t* sp = src.p + int64_t(sr) * src.stride * sb;
+      uint16_t* rp = rows + k * rs;
+      if (sb == 2) {
+        const int nv = n_src >> 3;
+        for (int q = threadIdx.x; q < nv; q += blockDim.x)
+          reinterpret_cast<uint4*>(rp)[q] = reinterpret_cast<const uint4*>(sp)[q];
+        for (int q = nv * 8 + threadIdx.x; q < n_src; q += blockDim.x) rp[q] = reinterpret_cast<const uint16_t*>(sp)[q];
+      } else {
+        const int nv = n_src >> 4;
+        for (int q = threadIdx.x; q < nv; q += blockDim.x) {
+          const uint4 v = reinterpret_cast<const uint4*>(sp)[q];
+          uint4* d = reinterpret_cast<uint4*>(rp + q * 16);
+          d[0] = make_uint4(__byte_perm(v.x, 0, 0x4140), __byte_perm(v.x, 0, 0x4342), __byte_perm(v.y, 0, 0x4140),
+                            __byte_perm(v.y, 0, 0x4342));
+          d[1] = make_uint4(__byte_perm(v.z, 0, 0x4140), __byte_perm(v.z, 0, 0x4342), __byte_perm(v.w, 0, 0x4140),
+                            __byte_perm(v.w, 0, 0x4342));
         }
+        for (int q = nv * 16 + threadIdx.x; q < n_src; q += blockDim.x) rp[q] = sp[q];
       }
-      __syncthreads();
-      if (live) {
-        uint8_t* dp = dst.p + int64_t(r) * dst.stride * sb;
-        for (int x = threadIdx.x; x < w; x += blockDim.x) {
-          // postfilter.rs:547-561
-          const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
-          const int px = int(src_x >> 14);
-          const int phase = int((src_x & 0x3fff) >> 8);
-          const int4 fq = __ldg(reinterpret_cast<const int4*>(g_upscale_filter[phase]));
-          const uint32_t fw[4] = {uint32_t(fq.x), uint32_t(fq.y), uint32_t(fq.z), uint32_t(fq.w)};
-          int fk[8];
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            fk[2 * k] = int(int16_t(uint16_t(fw[k] & 0xffffu)));
-            fk[2 * k + 1] = int(int16_t(uint16_t(fw[k] >> 16)));
-          }
-          int sum = 0;
-          if (px - 3 >= 0 && px + 4 <= max_x) {
-#pragma unroll
-            for (int k = 0; k < 8; k++) sum += int(row[px - 3 + k]) * fk[k];
-          } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) sum += int(row[min(max(px + k - 3, 0), max_x)]) * fk[k];
-          }
-          const int v = min(max(round2(sum, 7), 0), maxv);
-          if (sb == 2)
-            reinterpret_cast<uint16_t*>(dp)[x] = uint16_t(v);
-          else
-            dp[x] = uint8_t(v);
-        }
-      }
-      __syncthreads();
     }
+    __syncthreads();
+    // --- 8 outputs per thread (postfilter.rs:547-561) ---
+    const int ng = (w + 7) >> 3;
+    for (int u = threadIdx.x; u < nr * ng; u += blockDim.x) {
+      const int k = u / ng, g = u - k * ng;
+      if (src_row_of(k) < 0) continue;
+      const uint16_t* rp = rows + k * rs;
+      const int x0 = g * 8;
+      int v[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int x = min(x0 + e, w - 1);
+        const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
+        const int px = int(src_x >> 14);
+        const int phase = int((src_x & 0x3fff) >> 8);
+        const int4 fq = __ldg(reinterpret_cast<const int4*>(g_upscale_filter[phase]));
+        const uint32_t fw[4] = {uint32_t(fq.x), uint32_t(fq.y), uint32_t(fq.z), uint32_t(fq.w)};
+        int sum = 0;
+        if (px - 3 >= 0 && px + 4 <= max_x) {
+#pragma unroll
+          for (int t = 0; t < 4; t++) {
+            sum += int(rp[px - 3 + 2 * t]) * int(int16_t(uint16_t(fw[t] & 0xffffu)));
+            sum += int(rp[px - 2 + 2 * t]) * int(int16_t(uint16_t(fw[t] >> 16)));
+          }
+        } else {
+#pragma unroll
+          for (int t = 0; t < 4; t++) {
+            sum += int(rp[min(max(px - 3 + 2 * t, 0), max_x)]) * int(int16_t(uint16_t(fw[t] & 0xffffu)));
+            sum += int(rp[min(max(px - 2 + 2 * t, 0), max_x)]) * int(int16_t(uint16_t(fw[t] >> 16)));
+          }
+        }
+        v[e] = min(max(round2(sum, 7), 0), maxv);
+      }
+      uint8_t* dp = dst.p + int64_t(item.y0 + k) * dst.stride * sb;
+      const int n = min(8, w - x0);
+      if (sb == 2) {
+        uint16_t* op = reinterpret_cast<uint16_t*>(dp) + x0;
+        if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 15) == 0) {
+          *reinterpret_cast<uint4*>(op) =
+              make_uint4(uint32_t(v[0]) | (uint32_t(v[1]) << 16), uint32_t(v[2]) | (uint32_t(v[3]) << 16),
+                         uint32_t(v[4]) | (uint32_t(v[5]) << 16), uint32_t(v[6]) | (uint32_t(v[7]) << 16));
+        } else {
+          for (int e = 0; e < n; e++) op[e] = uint16_t(v[e]);
+        }
+      } else {
+        uint8_t* op = dp + x0;
+        if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 7) == 0) {
+          *reinterpret_cast<uint2*>(op) =
+              make_uint2(uint32_t(v[0]) | (uint32_t(v[1]) << 8) | (uint32_t(v[2]) << 16) | (uint32_t(v[3]) << 24),
+                         uint32_t(v[4]) | (uint32_t(v[5]) << 8) | (uint32_t(v[6]) << 16) | (uint32_t(v[7]) << 24));
+        } else {
+          for (int e = 0; e < n; e++) op[e] = uint8_t(v[e]);
+        }
+      }
+    }
+    __syncthreads();  // the rows are free for the next item
   }
 }
 
 cudaError_t superres_init() {
-  return cudaFuncSetAttribute(superres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxRow * 2);
+  return cudaFuncSetAttribute(superres_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kRows * sr_stride(kMaxRow) * 2);
 }
 
 void launch_superres(const FrameDesc* frames, const Item* items, int n_items, int row_max, cudaStream_t s) {
   if (n_items <= 0) return;
-  const int row = min(max(row_max, 8), kMaxRow);
-  launch_pdl(superres_kernel, min(n_items, kItemGrid), 256, size_t((row * 2 + 15) / 16 * 16), s, frames, items,
-             n_items);
+  const int rs = sr_stride(min(max(row_max, 8), kMaxRow));
+  launch_pdl(superres_kernel, min(n_items, kItemGrid), 256, size_t(kRows * rs * 2), s, frames, items, n_items, rs);
 }
 
 }  // namespace av1pf
