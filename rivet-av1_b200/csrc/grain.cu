@@ -324,7 +324,8 @@ __device__ __forceinline__ int noise_at(const int16_t* T, int psx, int psy, int 
 }
 
 // Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
-// 256 (so of the grain block width). The rows are taken one noise stripe
+// 256 (so of the grain block width). A CTA works through a contiguous run of
+// items. The rows are taken one noise stripe
 // (32 rows, 16 for vertically subsampled chroma) at a time, with the
 // stripe's block offsets staged in shared memory; 256 threads, 8 consecutive
 // samples (one grain block) per thread per step.
@@ -336,7 +337,11 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
   __shared__ uint8_t offs_cur[kOutOffs], offs_prev[kOutOffs];
   int loaded = -1;  // frame * 4 + plane whose template is in T
   pdl_wait();  // the previous stage's output is complete past this point
-  FOR_EACH_ITEM(it, n_items) {
+  // a CTA takes a contiguous run of items: the items of a plane are
+  // consecutive, so it stages that plane's template once for its whole run
+  const int per = (n_items + int(gridDim.x) - 1) / int(gridDim.x);
+  const int it_end = min(n_items, (int(blockIdx.x) + 1) * per);
+  for (int it = int(blockIdx.x) * per; it < it_end; it++) {
     const Item item = items[it];
     OutParams P;
     {
@@ -453,14 +458,37 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
             // un-grained luma under each chroma sample (grain.rs:303-314)
             const int ly = yy << P.ssy;
             const uint8_t* lrow = P.luma + int64_t(ly) * P.luma_pitch;
+            const int lx0 = xs << P.ssx;
+            const uint8_t* lp = lrow + int64_t(lx0) * P.sb;
+            // the group's whole luma span (8 or 16 samples, no edge clamp
+            // inside it) in 8-byte loads
+            if (n == 8 && lx0 + (8 << P.ssx) <= P.w && (reinterpret_cast<uintptr_t>(lp) & 7) == 0) {
+              uint32_t wv[8];
+              const int nw = (8 << P.ssx) * P.sb / 4;  // 32-bit words: 2, 4 or 8
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-              if (e < n) {
-                const int lx = (xs + e) << P.ssx;
-                const int lnx = min(lx + 1, P.w - 1);
-                const int l0 = P.sb == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
-                const int l1 = P.sb == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
-                lum[e] = P.ssx ? round2(l0 + l1, 1) : l0;
+              for (int q = 0; q < 4; q++)
+                if (2 * q < nw) {
+                  const uint2 v2 = reinterpret_cast<const uint2*>(lp)[q];
+                  wv[2 * q] = v2.x;
+                  wv[2 * q + 1] = v2.y;
+                }
+              auto lsamp = [&](int k) {  // luma sample k of the span
+                return P.sb == 2 ? int((wv[k >> 1] >> (16 * (k & 1))) & 0xffffu)
+                                 : int((wv[k >> 2] >> (8 * (k & 3))) & 0xffu);
+              };
+#pragma unroll
+              for (int e = 0; e < 8; e++)
+                lum[e] = P.ssx ? round2(lsamp(2 * e) + lsamp(2 * e + 1), 1) : lsamp(e);
+            } else {
+#pragma unroll
+              for (int e = 0; e < 8; e++) {
+                if (e < n) {
+                  const int lx = (xs + e) << P.ssx;
+                  const int lnx = min(lx + 1, P.w - 1);
+                  const int l0 = P.sb == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
+                  const int l1 = P.sb == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
+                  lum[e] = P.ssx ? round2(l0 + l1, 1) : l0;
+                }
               }
             }
           }
@@ -533,7 +561,8 @@ void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, 
 
 void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  launch_pdl(output_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items);
+  // one resident wave (3 CTAs per SM), each CTA a contiguous run of items
+  launch_pdl(output_kernel, min(n_items, kNumSMs * 3), 256, 0, s, frames, items, n_items);
 }
 
 }  // namespace av1pf

@@ -292,6 +292,62 @@ __device__ __forceinline__ void sgr_flt_col(const int32_t* A, const int32_t* B, 
   }
 }
 
+// A rectangle without restoration: its samples of the upscaled CDEF frame
+// go straight to the reference frame and (frames without film grain) the
+// packed frame, 8 samples per thread and step, with no shared-memory round
+// trip and no barrier.
+__device__ __noinline__ void pass_through(const FrameDesc& f, int p, int x0, int y0, int w, int h, int tid) {
+  const int sb = f.sb, bps = f.bd > 8 ? 2 : 1;
+  const DPlane src = f.up[p], dst = f.ref[p];
+  const int pw = ((f.uw + plane_ssx(f, p)) >> plane_ssx(f, p));
+  uint8_t* out = f.lr_pack ? f.frame_out + f.out_off[p] : nullptr;
+  const int ng = (w + 7) >> 3;
+  for (int k = tid; k < h * ng; k += kThreads) {
+    const int r = k / ng, c = (k - r * ng) * 8;
+    const int n = min(8, w - c);
+    const int y = y0 + r, x = x0 + c;
+    const uint8_t* sp = src.p + (int64_t(y) * src.stride + x) * sb;
+    uint8_t* dp = dst.p + (int64_t(y) * dst.stride + x) * sb;
+    uint8_t* op = out ? out + (int64_t(y) * pw + x) * bps : nullptr;
+    uint32_t v[8];
+    const bool sv = n == 8 && (reinterpret_cast<uintptr_t>(sp) & (8 * sb - 1)) == 0;
+    if (sv && sb == 2) {
+      const uint4 q = *reinterpret_cast<const uint4*>(sp);
+      v[0] = q.x & 0xffffu; v[1] = q.x >> 16; v[2] = q.y & 0xffffu; v[3] = q.y >> 16;
+      v[4] = q.z & 0xffffu; v[5] = q.z >> 16; v[6] = q.w & 0xffffu; v[7] = q.w >> 16;
+    } else if (sv) {
+      const uint2 q = *reinterpret_cast<const uint2*>(sp);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        v[e] = (q.x >> (8 * e)) & 0xffu;
+        v[4 + e] = (q.y >> (8 * e)) & 0xffu;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; e++) v[e] = e < n ? uint32_t(ld_row(sp, sb, e)) : 0u;
+    }
+    auto put = [&](uint8_t* base, int width) {
+      if (n == 8 && (reinterpret_cast<uintptr_t>(base) & (8 * width - 1)) == 0) {
+        if (width == 2)
+          *reinterpret_cast<uint4*>(base) =
+              make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
+        else
+          *reinterpret_cast<uint2*>(base) = make_uint2(v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24),
+                                                       v[4] | (v[5] << 8) | (v[6] << 16) | (v[7] << 24));
+      } else {
+        for (int e = 0; e < n; e++) {
+          if (width == 2)
+            reinterpret_cast<uint16_t*>(base)[e] = uint16_t(v[e]);
+          else
+            base[e] = uint8_t(v[e]);
+        }
+      }
+    };
+    put(dp, sb);
+    if (op) put(op, bps);
+  }
+}
+
 // The shared-memory areas of one CTA.
 struct LrSmem {
   uint16_t* win;    // the window, rows kWS apart
@@ -492,6 +548,10 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     // the descriptor and the unit are inputs of the chain; the planes below
     // are the previous stage's output
     pdl_wait();
+    if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
+      pass_through(f, p, x0, geo.y0, w, h, tid);  // uniform across the CTA: no barrier needed
+      continue;
+    }
     if (w > 32)
       restore_rect<72>(f, sm, geo, p, s, x0, w, h, type, unit_p, tid);
     else
