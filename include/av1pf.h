@@ -194,8 +194,11 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx);
 
 /* Mirrors Decoder::set_threads (decoder/mod.rs:323-329): the reference's
  * worker-thread count for the post-filter bands. On the device the bands all
- * run at once; here `n` is the number of frames the per-frame host entry
- * points keep in flight on separate CUDA streams (0 = default of 2). */
+ * run at once; here `n` is the number of frames av1pf_chain_host_many keeps
+ * in flight, each in a device frame slot of its own (its upload, chain and
+ * download overlap those of the other slots' frames): 0 = the default of 3,
+ * values above 8 mean 8. Each slot holds one frame's input planes, maps,
+ * reference frame and packed frame, allocated on first use. */
 int av1pf_set_threads(av1pf_ctx* ctx, int n);
 
 /* Bytes of device memory the context currently holds. */
@@ -278,9 +281,11 @@ int av1pf_md5(const uint8_t* data, size_t n, char md5_hex[33]);
  * until the process exits. Limit: with film grain on, frames up to
  * ceil(upscaled_width/32) * ceil(frame_height/32) <= 65536 (e.g. 8192x8192);
  * larger frames are refused with AV1PF_ERR_UNSUPPORTED. Runs on the current
- * device. The first call on a device does a one-time set-up there (looks up
- * the array's device address, uploads the grain RNG tables); make that first
- * call before any stream capture. Every call shares the one array, and each
+ * device. The first call in a device's context does a one-time set-up there
+ * (looks up the array's device address, uploads the grain RNG tables); make
+ * that first call before any stream capture. After a cudaDeviceReset the
+ * device's next context gets the same set-up on its first call. Every call
+ * shares the one array, and each
  * call rewrites all of it that it reads, so nothing depends on earlier
  * contents; calls that overlap on the GPU (different streams, or several
  * host threads at once) race on it — issue them on one stream. */
@@ -323,8 +328,8 @@ typedef struct av1pf_host_job {
 
 /* n av1pf_chain_host calls in one, for a decoder that holds several decoded
  * frames (a sequence's frames, or several streams'): the frames' uploads,
- * filter chains and downloads overlap on separate streams, over 3 device
- * frame slots used in turn, so the copies in both directions and the
+ * filter chains and downloads overlap on separate streams, over device frame
+ * slots used in turn (3, or as av1pf_set_threads sets), so the copies in both directions and the
  * kernels run at the same time. Returns when every job's outputs are on the
  * host; the results equal n av1pf_chain_host calls. Every job is validated
  * before anything is queued. Host buffers should be pinned (page-locked),

@@ -123,7 +123,8 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
     rc = build_plan(jobs, n, nullptr, plan, &why);
     if (rc != AV1PF_OK) return set_error(why), rc;
     if ((rc = ensure(scratch, plan.scratch_bytes + 256)) != AV1PF_OK) return rc;
-    rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why);
+    // the lists are built; with the scratch in place only the descriptors change
+    rc = build_plan(jobs, n, static_cast<uint8_t*>(scratch.ptr), plan, &why, false);
     if (rc != AV1PF_OK) return set_error(why), rc;
     host_key = key_scratch;
     host_ready = true;
@@ -337,7 +338,7 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
 
 int av1pf_set_threads(av1pf_ctx* ctx, int n) {
   if (!ctx || n < 0) return AV1PF_ERR_INVALID_INPUT;
-  ctx->threads = n == 0 ? 2 : n;
+  ctx->threads = n == 0 ? 3 : std::min(n, Ctx::kPipeSlots);
   return AV1PF_OK;
 }
 
@@ -646,7 +647,7 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     need_maps = std::max(need_maps, lay[size_t(k)].total_maps);
     need_frame = std::max(need_frame, lay[size_t(k)].fbytes + 16);
   }
-  const int slots = std::min(n, Ctx::kPipeSlots);
+  const int slots = std::min(n, ctx->threads);
   for (int q = 0; q < slots; q++) {
     Ctx::PipeSlot& ps = ctx->pipe[q];
     if ((rc = ctx->ensure(ps.in, need_in)) || (rc = ctx->ensure(ps.ref, need_ref)) ||

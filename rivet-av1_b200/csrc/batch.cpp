@@ -147,7 +147,7 @@ int create_batch(Ctx* ctx, const FrameJob* fj, int n_jobs, uint32_t flags, av1pf
     const int n = int(jobs.size());
     rc = build_plan(jobs.data(), n, nullptr, G.plan, &why);
     if (rc == AV1PF_OK) rc = ctx->ensure(G.scratch, G.plan.scratch_bytes + 256);
-    if (rc == AV1PF_OK) rc = build_plan(jobs.data(), n, static_cast<uint8_t*>(G.scratch.ptr), G.plan, &why);
+    if (rc == AV1PF_OK) rc = build_plan(jobs.data(), n, static_cast<uint8_t*>(G.scratch.ptr), G.plan, &why, false);
     if (rc == AV1PF_OK) rc = ctx->ensure(G.meta, G.plan.meta_bytes + 256);
     if (rc == AV1PF_OK) {
       // the work lists and descriptors are uploaded once

@@ -53,7 +53,7 @@ struct Ctx {
   int device = 0;
   uint64_t cap = 0;   // 0 = no cap
   uint64_t held = 0;  // device bytes held by this context
-  int threads = 2;
+  int threads = 3;  // av1pf_set_threads: device frame slots of av1pf_chain_host_many
   cudaStream_t side = nullptr;  // grain templates beside the chain
   cudaStream_t own = nullptr;   // the host-buffer entry points
   cudaEvent_t fork = nullptr, join = nullptr;
@@ -63,10 +63,10 @@ struct Ctx {
   // loop-filter search's filtered copies; pinned staging of both
   DevBuf search_dev, search_planes;
   HostBuf search_host;
-  // av1pf_chain_host_many: device frame slots used in turn, with the events
-  // that order a slot's upload (pipe_up), chain (own) and download
-  // (pipe_down) against its next use
-  static constexpr int kPipeSlots = 3;
+  // av1pf_chain_host_many: device frame slots used in turn (`threads` of
+  // them), with the events that order a slot's upload (pipe_up), chain
+  // (own) and download (pipe_down) against its next use
+  static constexpr int kPipeSlots = 8;
   struct PipeSlot {
     DevBuf in, ref, maps, frame;
     cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;

@@ -98,8 +98,9 @@ struct SsePlane {
 size_t lr_search_smem(int wmax, int hmax, int kind, int band, int cache_px, int both);
 // The self-guided band height and filter-output cache that fit shared memory.
 void lr_search_shape(int wmax, int hmax, int upx_max, int& band, int& cache_px, int& both);
-// Raises the kernels' shared-memory limits for that shape.
-cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px, int both);
+// Raises the kernels' dynamic shared-memory limits to the device's maximum
+// (the same value on every call) on the current device.
+cudaError_t lr_search_init();
 void launch_lr_search(const LrSearchDesc& d, int njobs, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                       cudaEvent_t join);
 void launch_plane_sse(const SsePlane* jobs, int n, int rows_max, uint64_t* sse, cudaStream_t s);

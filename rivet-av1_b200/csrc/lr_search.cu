@@ -1002,15 +1002,27 @@ __global__ void lr_search_choose_kernel(const LrSearchDesc d, int njobs) {
   d.out[ji] = best;
 }
 
-cudaError_t lr_search_init(int wmax, int hmax, int band, int cache_px, int both) {
-  cudaError_t e = cudaFuncSetAttribute(lr_search_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(lr_search_smem(wmax, hmax, 0, band, cache_px, both)));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(lr_search_wiener_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(lr_search_smem(wmax, hmax, 1, band, cache_px, both)));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(lr_search_sgr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(lr_search_smem(wmax, hmax, 2, band, cache_px, both)));
+namespace {
+// Raises a kernel's dynamic shared-memory limit to all the device allows
+// beside its static shared memory. The attribute is process-wide, so every
+// call sets the same value: searches on several contexts and host threads
+// cannot lower it under one another's launches.
+template <typename K>
+cudaError_t allow_max_smem(K kernel, int optin) {
+  cudaFuncAttributes a{};
+  cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(a.sharedSizeBytes));
+}
+}  // namespace
+
+cudaError_t lr_search_init() {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = allow_max_smem(lr_search_prep_kernel, optin);
+  if (e == cudaSuccess) e = allow_max_smem(lr_search_wiener_kernel, optin);
+  if (e == cudaSuccess) e = allow_max_smem(lr_search_sgr_kernel, optin);
   return e;
 }
 

@@ -15,6 +15,7 @@
 // device array of kNoAllocBytes, reserved when the library is loaded and
 // kept by every GPU that loads it until the process exits. The kernels are
 // the ones av1pf_output launches; only where their scratch lives differs.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -44,23 +45,54 @@ static_assert(sizeof(FrameDesc) <= kDescBytes, "descriptor slot too small");
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_setup_mu;
-uint8_t* g_scratch_ptr[64] = {};  // per device: address of g_noalloc_scratch
+uint8_t* g_scratch_ptr[64] = {};     // per device: address of g_noalloc_scratch
+unsigned long long g_ctx_id[64] = {};  // per device: the context the address and tables belong to
 
-// Once per device, with that device current: look up the scratch's device
-// address and upload the film-grain RNG jump tables.
+// The unique ID of the calling thread's current CUDA context (cuCtxGetId,
+// reached through the runtime's driver entry points, so the library needs
+// no link against the driver library); false if unavailable.
+bool current_context_id(unsigned long long* id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  CUcontext c = nullptr;
+  return get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, id) == CUDA_SUCCESS;
+}
+
+// With the device current: look up the scratch's device address and upload
+// the film-grain RNG jump tables, once per device context. After a
+// cudaDeviceReset the device's next context loads the module again (the
+// array at a possibly new address, the tables zeroed): that context has a
+// new ID, so the lookup and upload run again.
 int setup(int device, uint8_t** out) {
   if (device < 0 || device >= 64) {
     set_error("av1pf_output_noalloc: device index out of range");
     return AV1PF_ERR_UNSUPPORTED;
   }
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_status(e, "av1pf_output_noalloc: cudaGetSymbolAddress");
+  void* p = nullptr;
+  // (also makes the device's context current in this thread)
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_status(e, "av1pf_output_noalloc: cudaGetSymbolAddress");
+  unsigned long long id = 0;
+  const bool have_id = current_context_id(&id);
+  if (g_scratch_ptr[device] != p || (have_id && g_ctx_id[device] != id)) {
     e = upload_grain_tables();
     if (e != cudaSuccess) return cuda_status(e, "av1pf_output_noalloc: grain tables");
     g_scratch_ptr[device] = static_cast<uint8_t*>(p);
+    g_ctx_id[device] = have_id ? id : 0;
   }
   *out = g_scratch_ptr[device];
   return AV1PF_OK;

@@ -521,7 +521,7 @@ int av1pf_lr_search_many(av1pf_ctx* ctx, int n, av1pf_lr_search_job* jobs_in, in
       if (jb.nr > 1) d.multi_rect = 1;
     }
     lr_search_shape(d.wmax, d.hmax, upx_max, d.band, d.cache_px, d.both);
-    cudaError_t e = lr_search_init(d.wmax, d.hmax, d.band, d.cache_px, d.both);
+    cudaError_t e = lr_search_init();
     if (e != cudaSuccess) return cuda_status(e, "loop-restoration search attributes");
     const size_t fb = frames.size() * sizeof(LrSearchFrame);
     const size_t jbb = jobs.size() * sizeof(LrSearchJob), rb = rects.size() * sizeof(LrSearchRect);

@@ -279,7 +279,8 @@ int Server::start_batch(InFlight& b, std::vector<Request*>& reqs) {
   int rc = build_plan(jobs.data(), int(jobs.size()), nullptr, b.plan, &why);
   if (rc == AV1PF_OK) rc = ensure_dev(*this, &b.scratch, &b.scratch_size, b.plan.scratch_bytes + 256);
   if (rc == AV1PF_OK)
-    rc = build_plan(jobs.data(), int(jobs.size()), static_cast<uint8_t*>(b.scratch), b.plan, &why);
+    // the lists are built; with the scratch in place only the descriptors change
+    rc = build_plan(jobs.data(), int(jobs.size()), static_cast<uint8_t*>(b.scratch), b.plan, &why, false);
   if (rc == AV1PF_OK) rc = ensure_dev(*this, &b.meta, &b.meta_size, b.plan.meta_bytes + 256);
   if (rc != AV1PF_OK) return rc;
   if (b.meta_host_size < b.plan.upload_bytes) {
