@@ -337,6 +337,58 @@ typedef struct av1pf_host_job {
 int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs);
 
 /* ------------------------------------------------------------------------ */
+/* Reference frames on the device: the reference frame update process (7.20, */
+/* decoder/mod.rs:797-806) over frames the chain leaves on the device. Each  */
+/* of the 8 slots holds a frame (RefData.frame, state.rs:79-101: the LR      */
+/* frame) by reference count, several slots sharing one, as the reference's  */
+/* Arc<RefData> does; a GPU decoder upstream reads a slot's planes for inter */
+/* prediction without a copy.                                                */
+/* ------------------------------------------------------------------------ */
+typedef struct av1pf_refs av1pf_refs;
+
+/* What a slot holds. */
+typedef struct av1pf_ref_frame {
+  int32_t valid;              /* 0: the slot is empty (the rest is zero) */
+  av1pf_frame_info info;      /* the frame's geometry */
+  uint32_t order_hint;        /* as given to av1pf_refs_chain */
+  uint64_t frame_id;          /* 1, 2, ...: the av1pf_refs_chain call that made it */
+  av1pf_plane planes[AV1PF_MAX_PLANES]; /* device: the LR frame over the visible area */
+} av1pf_ref_frame;
+
+/* An empty table (no device memory until the first frame). The table uses
+ * the context's device, scratch and HBM cap. */
+int av1pf_refs_create(av1pf_ctx* ctx, av1pf_refs** out);
+/* Synchronises the device, then frees the table's frames. */
+int av1pf_refs_destroy(av1pf_refs* refs);
+
+/* decode_frame_wrapup (decoder/mod.rs:747-806) for a frame kept on the
+ * device: av1pf_chain with its reference frame written into a frame of the
+ * table, then the reference frame update process: every slot i whose bit i
+ * of refresh_frame_flags is set now holds that frame. A frame no slot holds
+ * any longer returns to the table's pool, and a later call writes into it in
+ * stream order: use one stream per table (or order the streams that read
+ * slot planes before the next call). frame_out as for av1pf_chain (may be
+ * NULL). */
+int av1pf_refs_chain(av1pf_refs* refs, const av1pf_frame_info* info,
+                     const av1pf_params* params, const av1pf_maps* maps,
+                     const av1pf_plane* in, uint32_t refresh_frame_flags,
+                     uint32_t order_hint, uint8_t* frame_out, void* stream);
+
+/* The frame slot `slot` (0..7) holds. Its planes stay valid until calls have
+ * replaced it in every slot that holds it. */
+int av1pf_refs_get(const av1pf_refs* refs, int slot, av1pf_ref_frame* out);
+
+/* show_existing_frame (decoder/mod.rs:819-842): the output process on the
+ * frame in `slot` with the film grain of `params` into `frame_out` (device),
+ * then the update with refresh_frame_flags (a shown key frame passes all
+ * slots; otherwise 0). AV1PF_ERR_INVALID_INPUT for an empty slot. */
+int av1pf_refs_show(av1pf_refs* refs, int slot, const av1pf_params* params,
+                    uint32_t refresh_frame_flags, uint8_t* frame_out, void* stream);
+
+/* Device bytes the table's frames hold, and how many frames it has made. */
+int av1pf_refs_memory(const av1pf_refs* refs, uint64_t* bytes, int32_t* frames);
+
+/* ------------------------------------------------------------------------ */
 /* Batched path: many frames of mixed shape / bit depth / subsampling, one   */
 /* persistent launch per stage, replayed from a captured CUDA graph.         */
 /* ------------------------------------------------------------------------ */

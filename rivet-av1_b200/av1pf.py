@@ -82,6 +82,12 @@ class Params(C.Structure):
         ("film_grain", FilmGrain)]
 
 
+class RefFrame(C.Structure):
+    """av1pf_ref_frame: what a device reference slot holds."""
+    _fields_ = [("valid", C.c_int32), ("info", FrameInfo), ("order_hint", C.c_uint32), ("frame_id", C.c_uint64),
+                ("planes", Plane * 3)]
+
+
 class Job(C.Structure):
     _fields_ = [("info", C.POINTER(FrameInfo)), ("params", C.POINTER(Params)), ("maps", C.POINTER(Maps)),
                 ("inp", C.POINTER(Plane)), ("ref_out", C.POINTER(Plane)), ("frame_out", C.c_void_p)]
@@ -213,6 +219,13 @@ def lib():
         _sig(L, "av1pf_chain", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp, vp)
         _sig(L, "av1pf_chain_host", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), P(Plane), vp)
         _sig(L, "av1pf_chain_host_many", C.c_int, vp, C.c_int, P(HostJob))
+        _sig(L, "av1pf_refs_create", C.c_int, vp, P(vp))
+        _sig(L, "av1pf_refs_destroy", C.c_int, vp)
+        _sig(L, "av1pf_refs_chain", C.c_int, vp, P(FrameInfo), P(Params), P(Maps), P(Plane), C.c_uint32, C.c_uint32,
+             vp, vp)
+        _sig(L, "av1pf_refs_get", C.c_int, vp, C.c_int, P(RefFrame))
+        _sig(L, "av1pf_refs_show", C.c_int, vp, C.c_int, P(Params), C.c_uint32, vp, vp)
+        _sig(L, "av1pf_refs_memory", C.c_int, vp, P(C.c_uint64), P(C.c_int32))
         _sig(L, "av1pf_batch_create", C.c_int, vp, P(Job), C.c_int, C.c_uint32, P(vp))
         _sig(L, "av1pf_batch_run", C.c_int, vp, vp)
         _sig(L, "av1pf_batch_destroy", C.c_int, vp)

@@ -44,6 +44,32 @@ def test_struct_sizes_match_header():
     assert C.sizeof(A.Plane) == 24
 
 
+def test_struct_layouts_match_the_compiled_header(tmp_path):
+    """sizeof and field offsets of the ABI structs, as gcc lays them out
+    from include/av1pf.h, equal the Python bindings'."""
+    structs = {"av1pf_frame_info": (A.FrameInfo, []), "av1pf_params": (A.Params, ["film_grain"]),
+               "av1pf_film_grain": (A.FilmGrain, ["ar_coeff_shift_minus_6", "clip_to_restricted_range"]),
+               "av1pf_maps": (A.Maps, ["cdef_idx", "lr_units"]), "av1pf_plane": (A.Plane, ["height"]),
+               "av1pf_host_job": (A.HostJob, ["frame_out"]), "av1pf_job": (A.Job, ["frame_out"]),
+               "av1pf_ref_frame": (A.RefFrame, ["info", "order_hint", "frame_id", "planes"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "av1pf.h"', "int main(void) {"]
+    for name, (_, fields) in structs.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for fld in fields:
+            lines.append(f'  printf("{name}.{fld} %zu\\n", offsetof({name}, {fld}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for name, (cls, fields) in structs.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for fld in fields:
+            assert int(got[f"{name}.{fld}"]) == getattr(cls, fld).offset, f"{name}.{fld}"
+
+
 def test_validate_accepts_synthetic_frames():
     for kw in [dict(width=1920, height=1080, bit_depth=10), dict(width=352, height=288, bit_depth=8, sample_bytes=1),
                dict(width=640, height=360, bit_depth=12, subsampling_x=0, subsampling_y=0, superres_denom=12,
