@@ -59,11 +59,41 @@ METRIC = "bit-exact post-filtered Mpx/s"
 HEADLINE = dict(width=1920, height=1080, bit_depth=10)
 L2_BYTES = 126 * 2**20
 HEADLINE_WORKLOAD = "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+CDEF+LR+pack)"
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each stage's kernels on the
-# headline workload, from one `ncu --set full` capture (cold cache; the outputs stay in the 126 MB
-# L2, so the writes read 0). The loop filter's is its three kernels together. The headline frames
-# have no film grain, so the loop-restoration kernel packs them and no output kernel runs.
-NCU_TRAFFIC_HEADLINE = {"loop_filter": 8308480 + 6636800 + 4791552, "cdef": 7033856, "loop_restoration": 6830336}
+# Per launch of each stage's kernels on the headline workload, from one ncu capture of the headline
+# bench (profiles/metrics_1080p10_chain.md gives the command): DRAM bytes read and written
+# (dram__bytes_read.sum, dram__bytes_write.sum) and warp-instructions executed
+# (smsp__inst_executed.sum). ncu flushes the caches before a captured launch, so the reads are cold;
+# a frame's 6-19 MB of writes stay in the 126 MB L2 when the launch ends, so the writes read near 0
+# (they reach DRAM later, during the next launches). The headline frames have no film grain: the
+# loop-restoration kernel packs them and no output kernel runs.
+NCU_HEADLINE = {
+    "loop_filter": {"dram_read": 8308480 + 6636800 + 4791552, "dram_write": 0, "warp_inst": 7500000},
+    "cdef": {"dram_read": 7033856, "dram_write": 0, "warp_inst": 17600000},
+    "loop_restoration": {"dram_read": 6830336, "dram_write": 0, "warp_inst": 16200000},
+}
+B200_SMS, ISSUE_PER_SM_CLK = 148, 4  # four schedulers per SM, one warp-instruction each per clock
+
+
+def traffic_of(stage):
+    n = NCU_HEADLINE.get(stage)
+    return None if n is None else n["dram_read"] + n["dram_write"]
+
+
+def issue_fractions(stage_ms, frame_ms, clocks):
+    """The bound that binds this path: warp-instructions issued per stage
+    (ncu, per launch) over what the SMs can issue in the stage's measured
+    time at the sampled SM clock (148 SMs x 4 per clock)."""
+    mhz = clocks.get("sm_mhz") or 1965.0
+    per_ms = B200_SMS * ISSUE_PER_SM_CLK * mhz * 1e3  # warp-instructions per ms
+    out = {"sm_mhz": mhz, "source": "smsp__inst_executed.sum per launch (ncu) / (148 x 4 x SM clock x time)"}
+    total = 0
+    for stage, n in NCU_HEADLINE.items():
+        total += n["warp_inst"]
+        if stage_ms.get(stage):
+            out[stage] = round(n["warp_inst"] / (per_ms * stage_ms[stage]), 4)
+    out["chain"] = round(total / (per_ms * frame_ms), 4)
+    out["warp_inst_per_frame"] = total
+    return out
 
 
 def peaks():
@@ -314,8 +344,11 @@ def main_gpu(args):
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "algorithmic_bytes": int(algo[dom]), "traffic": NCU_TRAFFIC_HEADLINE.get(dom),
-                     "chain_frac": round(chain_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak, 4)},
+                     "algorithmic_bytes": int(algo[dom]), "traffic": traffic_of(dom),
+                     "traffic_note": "ncu dram read+write of one cold-cache launch; the launch's writes are "
+                                     "still in L2 when it ends, so they are not counted",
+                     "chain_frac": round(chain_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak, 4),
+                     "issue": issue_fractions(stage_ms, ms_max / args.steps, clocks)},
         "clocks": clocks,
     }
 

@@ -20,6 +20,7 @@ import pytest
 import av1pf as A
 import oracle as O
 import spec_check as S
+from conftest import cuda_available
 
 CDEF_CASES = {
     "352x288_8bit_u8": dict(width=352, height=288, bit_depth=8, sample_bytes=1, content=1, seed=1, frame_index=2),
@@ -168,3 +169,22 @@ def test_chain_matches_specification(name):
         bad = np.argwhere(g != c)
         assert not len(bad), f"{name} plane {p}: {len(bad)} samples differ, first at {tuple(bad[0])}"
     assert np.array_equal(fb, fb_cpu), f"{name}: packed frame differs"
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not cuda_available(), reason="needs a CUDA device")
+@pytest.mark.parametrize("name", ["10bit_420_seg_dlf", "superres_d16_grain", "12bit_444", "8bit_u8_420"])
+def test_gpu_chain_matches_specification(name):
+    """The CUDA chain through the C ABI against the specification's
+    restatement directly (no oracle in between)."""
+    import gpu_util as G
+    sf = A.SynthHandle(**CHAIN_CASES[name])
+    vis, fb = S.chain(sf, O.HostPlanes.like_synth(sf).arrays)
+    ctx = G.Ctx()
+    try:
+        ref_gpu, fb_gpu = G.gpu_chain(ctx, G.DevFrame(sf))
+    finally:
+        ctx.close()
+    for p, (g, c) in enumerate(zip(ref_gpu, vis)):
+        assert np.array_equal(g, c), f"{name} plane {p}"
+    assert np.array_equal(fb_gpu, fb), f"{name}: packed frame"
