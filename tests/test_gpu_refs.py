@@ -73,7 +73,9 @@ def test_refresh_sequence_matches_the_update_process(ctx):
         sfs = [A.SynthHandle(**c) for c in cfgs]
         want = [oracle_ref_packed(sf) for sf in sfs]
         held = [None] * 8  # frame index per slot, as the update process leaves it
+        peak = 0  # frames the pool needs: the most held at once when a frame is made, plus that one
         for k, (sf, fl) in enumerate(zip(sfs, flags)):
+            peak = max(peak, len({h for h in held if h is not None}) + 1)
             df = G.DevFrame(sf)
             fb = G.dev_bytes(A.frame_bytes(sf.info))
             A.check(L.av1pf_refs_chain(refs, C.byref(sf.f.info), C.byref(sf.f.params), C.byref(df.maps), df.inp.c, fl,
@@ -99,11 +101,12 @@ def test_refresh_sequence_matches_the_update_process(ctx):
                 ptrs.setdefault(j, set()).add(r.planes[0].data)
             # slots holding one frame share its planes
             assert all(len(v) == 1 for v in ptrs.values())
-            # a frame no slot holds goes back to the pool: the table never
-            # holds more frames than are in slots plus the one being made
+            # a frame no slot holds goes back to the pool and is reused: the
+            # table has never made more frames than were held at once plus
+            # the one being made
             b, n = C.c_uint64(), C.c_int32()
             A.check(L.av1pf_refs_memory(refs, C.byref(b), C.byref(n)), "refs_memory")
-            assert n.value <= len({h for h in held if h is not None}) + 1
+            assert n.value <= peak, f"after frame {k}: {n.value} frames made, {peak} needed"
         # show_existing_frame of slot 1 with film grain: the output process on that frame
         r1 = get(refs, 1)
         sf = sfs[held[1]]
