@@ -430,7 +430,7 @@ int av1pf_batch_destroy(av1pf_batch* batch);
 /* ------------------------------------------------------------------------ */
 typedef struct av1pf_tuning {
   /* How the loop filter runs in chain calls. -1: per frame shape, the mode
-   * av1pf_autotune measured fastest (mode 0 while a shape is unmeasured).
+   * av1pf_autotune measured fastest (mode 3 while a shape is unmeasured).
    * 0: one kernel decides every 4x4 edge into a compact list per direction,
    *    then one kernel per direction filters the listed edges in place;
    * 1: vertical edges filtered per 64x64 tile in shared memory (the tile

@@ -15,7 +15,8 @@
 //     most 3 columns left and 3 rows up (3 columns right on earlier rows),
 //     so cells with equal (x - 3) + 4 (y - 3) are independent: one warp per
 //     template walks that wavefront, a lane per row on it, with warp-level
-//     synchronisation only; the chroma warps trail the luma warp.
+//     synchronisation only (the value each step needs from the previous one
+//     comes by shuffle); the chroma warps trail the luma warp.
 // output_kernel: per 256-column tile of a plane's visible area, reads the reference
 // frame, adds grain (noise assembled from the templates, the 32x32 block
 // offsets and the overlap blends of grain.rs:179-283, evaluated per sample
@@ -53,11 +54,15 @@ constexpr int kOutOffs = 18;
 // same lane (kept in registers), and its neighbours in the rows above, at
 // most LAG columns to the right, at step t-1 or earlier by the lanes before
 // it. At most 20 rows are on the wavefront at once, so no two of a lane's
-// rows are. The luma warp publishes its completed step count in `progress`;
-// a chroma warp waits, before each step, for the luma cells its luma term
-// reads (a bounded wait: after kSpinLimit polls it flags ERRF_STALL and
-// goes on).
+// rows are. The one value a step needs from the step just before it — the
+// cell up and LAG = 3 to the right, made by the lane above — comes by a warp
+// shuffle; every other neighbour was stored to shared memory at least two
+// steps earlier and is visible after the warp's barrier. The luma warp
+// publishes its completed step count in `progress` every kPublish steps; a
+// chroma warp waits, before a step, for the luma cells its luma term reads
+// (a bounded wait: after kSpinLimit polls it flags ERRF_STALL and goes on).
 constexpr int kSpinLimit = 1 << 22;
+constexpr int kPublish = 8;
 
 __device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t* p) {
   uint32_t v;
@@ -81,9 +86,11 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
 #pragma unroll
   for (int k = 0; k <= NC; k++) c[k] = coef_s[k];
   const int lane = threadIdx.x & 31;
+  const int above = (lane + 31) & 31;  // the lane of the row above
   const int rows = H - 3, cols = W - 6;
   const int steps = (cols - 1) + 4 * (rows - 1) + 1;
   int l1 = 0, l2 = 0, l3 = 0;  // the lane's row at x-1, x-2, x-3
+  int v = 0;                   // the lane's latest output
   uint32_t seen = 0;           // luma steps known complete
   for (int t = 0; t < steps; t++) {
     const int q = t >> 2;
@@ -91,6 +98,8 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
     const int x = 3 + t - 4 * rr;
     const bool active = rr >= 0 && rr < rows && x < W - 3;
     const int y = 3 + rr;
+    // the cell (y - 1, x + 3) the lane above made on the previous step
+    const int up = __shfl_sync(0xffffffffu, v, above);
     if (CHROMA && luma_on) {
       // the last luma step whose cell this step's luma terms read
       const int need = active ? ((x - 3) << sub_x) + sub_x + 4 * (((y - 3) << sub_y) + sub_y) : -1;
@@ -111,11 +120,17 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
         l2 = T[y][1];
         l3 = T[y][0];
       }
+      // (y - 1, x + 3) is an AR cell of the previous step when the row above
+      // is filtered and x + 3 is inside the filtered columns
+      const bool up_fresh = LAG == 3 && rr >= 1 && x + 3 < W - 3;
       int s[LAG + 2] = {};
 #pragma unroll
       for (int dr = -LAG; dr < 0; dr++)
 #pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++) s[LAG + dr] += T[y + dr][x + dc] * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
+        for (int dc = -LAG; dc <= LAG; dc++) {
+          const int cv = (dr == -1 && dc == LAG && up_fresh) ? up : int(T[y + dr][x + dc]);
+          s[LAG + dr] += cv * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
+        }
       const int lp = LAG * (2 * LAG + 1);
       if (LAG >= 1) s[LAG] += l1 * c[lp + LAG - 1];
       if (LAG >= 2) s[LAG] += l2 * c[lp + LAG - 2];
@@ -131,19 +146,17 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
       int sum = 0;
 #pragma unroll
       for (int k = 0; k < LAG + 2; k++) sum += s[k];
-      const int v = clip3(gmin, gmax, T[y][x] + round2(sum, ar_shift));
+      v = clip3(gmin, gmax, T[y][x] + round2(sum, ar_shift));
       T[y][x] = int16_t(v);
       l3 = l2;
       l2 = l1;
       l1 = v;
     }
-    if (!CHROMA) {
-      __threadfence_block();
-      __syncwarp();
-      if (lane == 0) st_release_cta(progress, uint32_t(t + 1));
-    } else {
-      __syncwarp();
-    }
+    // the step's stores are visible to the whole warp past this barrier
+    __syncwarp();
+    // (the barrier orders every lane's stores before lane 0's release)
+    if (!CHROMA && lane == 0 && ((t % kPublish) == kPublish - 1 || t == steps - 1))
+      st_release_cta(progress, uint32_t(t + 1));
   }
 }
 

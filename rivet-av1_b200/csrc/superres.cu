@@ -9,10 +9,12 @@
 // Item kind 0: rows [y0, y1) of cdef -> up. Kind 1: line rows [y0, y1) of the
 // line buffer (4 per stripe boundary: rows B-2 .. B+1 of the boundary at B).
 // An item's (at most 4) source rows are staged together in shared memory
-// (16-byte loads), behind one barrier; then each thread makes 8 consecutive
-// output samples of a row, each reading its 8 taps from shared memory and
+// (16-byte loads), behind one barrier; then the lanes of a warp make
+// consecutive output samples, each reading its 8 taps from shared memory and
 // its filter phase's 8 coefficients with one 16-byte load from global memory
-// (through the L1), and stores them as one 16-byte (8-byte at u8) vector.
+// (through the L1). (Eight consecutive outputs per thread, stored as one
+// vector, measured slower: a warp's lanes then read taps about 5 samples
+// apart, and the bank conflicts cost more than the wider stores saved.)
 // The row buffers are sized per launch to the widest source row among the
 // launch's frames.
 #include "common.cuh"
@@ -92,17 +94,14 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
       }
     }
     __syncthreads();
-    // --- 8 outputs per thread (postfilter.rs:547-561) ---
-    const int ng = (w + 7) >> 3;
-    for (int u = threadIdx.x; u < nr * ng; u += blockDim.x) {
-      const int k = u / ng, g = u - k * ng;
+    // --- one output per thread and step (postfilter.rs:547-561): the lanes
+    // of a warp make consecutive outputs, so their taps read neighbouring
+    // (often the same) shared-memory words and their stores coalesce ---
+    for (int k = 0; k < nr; k++) {
       if (src_row_of(k) < 0) continue;
       const uint16_t* rp = rows + k * rs;
-      const int x0 = g * 8;
-      int v[8];
-#pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int x = min(x0 + e, w - 1);
+      uint8_t* dp = dst.p + int64_t(item.y0 + k) * dst.stride * sb;
+      for (int x = threadIdx.x; x < w; x += blockDim.x) {
         const int64_t src_x = -(int64_t(1) << 14) + init + int64_t(x) * step;
         const int px = int(src_x >> 14);
         const int phase = int((src_x & 0x3fff) >> 8);
@@ -122,28 +121,11 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
             sum += int(rp[min(max(px - 2 + 2 * t, 0), max_x)]) * int(int16_t(uint16_t(fw[t] >> 16)));
           }
         }
-        v[e] = min(max(round2(sum, 7), 0), maxv);
-      }
-      uint8_t* dp = dst.p + int64_t(item.y0 + k) * dst.stride * sb;
-      const int n = min(8, w - x0);
-      if (sb == 2) {
-        uint16_t* op = reinterpret_cast<uint16_t*>(dp) + x0;
-        if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 15) == 0) {
-          *reinterpret_cast<uint4*>(op) =
-              make_uint4(uint32_t(v[0]) | (uint32_t(v[1]) << 16), uint32_t(v[2]) | (uint32_t(v[3]) << 16),
-                         uint32_t(v[4]) | (uint32_t(v[5]) << 16), uint32_t(v[6]) | (uint32_t(v[7]) << 16));
-        } else {
-          for (int e = 0; e < n; e++) op[e] = uint16_t(v[e]);
-        }
-      } else {
-        uint8_t* op = dp + x0;
-        if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 7) == 0) {
-          *reinterpret_cast<uint2*>(op) =
-              make_uint2(uint32_t(v[0]) | (uint32_t(v[1]) << 8) | (uint32_t(v[2]) << 16) | (uint32_t(v[3]) << 24),
-                         uint32_t(v[4]) | (uint32_t(v[5]) << 8) | (uint32_t(v[6]) << 16) | (uint32_t(v[7]) << 24));
-        } else {
-          for (int e = 0; e < n; e++) op[e] = uint8_t(v[e]);
-        }
+        const int v = min(max(round2(sum, 7), 0), maxv);
+        if (sb == 2)
+          reinterpret_cast<uint16_t*>(dp)[x] = uint16_t(v);
+        else
+          dp[x] = uint8_t(v);
       }
     }
     __syncthreads();  // the rows are free for the next item

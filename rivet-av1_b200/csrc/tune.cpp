@@ -38,7 +38,7 @@ ShapeKey shape_of(const av1pf_frame_info* i) {
 
 void Ctx::apply_tuning(FrameJob& j) const {
   std::lock_guard<std::mutex> lk(tune_mu);
-  int mode = 0;
+  int mode = 3;  // unmeasured shapes: both loop-filter passes in one kernel
   int cols = 64;
   const auto it = tuned.find(shape_of(j.info));
   if (it != tuned.end()) {
