@@ -316,24 +316,21 @@ struct OutParams {
   int mult, lmult, offs;
 };
 
-// One noise sample from the template in shared memory (grain.rs:200-243 for
-// the horizontal overlap): stripe offsets `rnd` (this block) and `rnd_prev`
-// (the block to its left).
-__device__ __forceinline__ int noise_at(const int16_t* T, int psx, int psy, int row, int j, int rnd, int rnd_prev,
-                                        bool blend, int gmin, int gmax) {
+// Template positions (grain.rs:200-243): the sample of block column j and
+// noise-stripe row `row` of a block with offsets `rnd` is at
+// tmpl_at(...)[j], and the column of the block to its left that overlaps it
+// at left_at(...)[j].
+__device__ __forceinline__ const int16_t* tmpl_at(const int16_t* T, int psx, int psy, int row, int rnd) {
   const int ox = rnd >> 4, oy = rnd & 15;
-  const int pox = psx ? 6 + ox : 9 + 2 * ox;
-  const int poy = psy ? 6 + oy : 9 + 2 * oy;
-  int gv = T[(poy + row) * kTW + pox + j];
-  if (blend) {
-    const int oxp = rnd_prev >> 4, oyp = rnd_prev & 15;
-    const int poxp = psx ? 6 + oxp : 9 + 2 * oxp;
-    const int poyp = psy ? 6 + oyp : 9 + 2 * oyp;
-    const int old = T[(poyp + row) * kTW + poxp + j + (32 >> psx)];
-    gv = psx ? old * 23 + gv * 22 : (j == 0 ? old * 27 + gv * 17 : old * 17 + gv * 27);
-    gv = clip3(gmin, gmax, round2(gv, 5));
-  }
-  return gv;
+  return T + ((psy ? 6 + oy : 9 + 2 * oy) + row) * kTW + (psx ? 6 + ox : 9 + 2 * ox);
+}
+__device__ __forceinline__ const int16_t* left_at(const int16_t* T, int psx, int psy, int row, int rnd_prev) {
+  return tmpl_at(T, psx, psy, row, rnd_prev) + (32 >> psx);
+}
+// The horizontal overlap blend of column j (0 or 1) of a block.
+__device__ __forceinline__ int hblend(int old, int g, int j, int psx, int gmin, int gmax) {
+  const int gv = psx ? old * 23 + g * 22 : (j == 0 ? old * 27 + g * 17 : old * 17 + g * 27);
+  return clip3(gmin, gmax, round2(gv, 5));
 }
 
 // Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
@@ -342,7 +339,7 @@ __device__ __forceinline__ int noise_at(const int16_t* T, int psx, int psy, int 
 // (32 rows, 16 for vertically subsampled chroma) at a time, with the
 // stripe's block offsets staged in shared memory; 256 threads, 8 consecutive
 // samples (one grain block) per thread per step.
-__global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restrict__ frames,
+__global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restrict__ frames,
                                                      const Item* __restrict__ items, int n_items) {
   __shared__ __align__(16) int16_t T[kTH * kTW];
   __shared__ int16_t lut[256];
@@ -350,11 +347,12 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
   __shared__ uint8_t offs_cur[kOutOffs], offs_prev[kOutOffs];
   int loaded = -1;  // frame * 4 + plane whose template is in T
   pdl_wait();  // the previous stage's output is complete past this point
-  // a CTA takes a contiguous run of items: the items of a plane are
-  // consecutive, so it stages that plane's template once for its whole run
-  const int per = (n_items + int(gridDim.x) - 1) / int(gridDim.x);
-  const int it_end = min(n_items, (int(blockIdx.x) + 1) * per);
-  for (int it = int(blockIdx.x) * per; it < it_end; it++) {
+  // a CTA takes a contiguous run of items, the runs split as evenly as the
+  // count allows: the items of a plane are consecutive, so a CTA stages that
+  // plane's template once for its whole run
+  const int it_begin = int(int64_t(blockIdx.x) * n_items / gridDim.x);
+  const int it_end = int(int64_t(blockIdx.x + 1) * n_items / gridDim.x);
+  for (int it = it_begin; it < it_end; it++) {
     const Item item = items[it];
     OutParams P;
     {
@@ -505,17 +503,26 @@ __global__ void __launch_bounds__(256, 3) output_kernel(const FrameDesc* __restr
               }
             }
           }
+          // the group's noise (grain.rs:200-283): its 8 samples lie in one
+          // grain block, so the template positions are found once; only a
+          // block's first 1-2 columns blend with the block to the left, and
+          // only a stripe's first 1-2 rows with the stripe above
+          const int nh = (P.overlap && b > 0 && jb == 0) ? (P.psx ? 1 : 2) : 0;
+          const int16_t* tp = tmpl_at(T, P.psx, P.psy, i, offs_cur[li]) + jb;
+          const int16_t* tl = left_at(T, P.psx, P.psy, i, offs_cur[li - 1]);
+          const int vrow = i + (32 >> P.psy);
+          const int16_t* vp = tmpl_at(T, P.psx, P.psy, vrow, offs_prev[li]) + jb;
+          const int16_t* vl = left_at(T, P.psx, P.psy, vrow, offs_prev[li - 1]);
 #pragma unroll
           for (int e = 0; e < 8; e++) {
             if (e >= n) continue;
-            const int j = jb + e;
-            const bool hblend = P.overlap && b > 0 && j < (P.psx ? 1 : 2);
-            int noise = noise_at(T, P.psx, P.psy, i, j, offs_cur[li], offs_cur[li - 1], hblend, P.gmin, P.gmax);
+            int noise = tp[e];
+            if (e < nh) noise = hblend(tl[e], noise, e, P.psx, P.gmin, P.gmax);
             if (vblend) {
-              const int old = noise_at(T, P.psx, P.psy, i + (32 >> P.psy), j, offs_prev[li], offs_prev[li - 1],
-                                       hblend, P.gmin, P.gmax);
-              noise = P.psy ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
-              noise = clip3(P.gmin, P.gmax, round2(noise, 5));
+              int old = vp[e];
+              if (e < nh) old = hblend(vl[e], old, e, P.psx, P.gmin, P.gmax);
+              const int g2 = P.psy ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
+              noise = clip3(P.gmin, P.gmax, round2(g2, 5));
             }
             const int orig = v[e];
             int idx = orig;
@@ -574,8 +581,8 @@ void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, 
 
 void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
-  // one resident wave (3 CTAs per SM), each CTA a contiguous run of items
-  launch_pdl(output_kernel, min(n_items, kNumSMs * 3), 256, 0, s, frames, items, n_items);
+  // one resident wave (2 CTAs per SM), each CTA a contiguous run of items
+  launch_pdl(output_kernel, min(n_items, kNumSMs * 2), 256, 0, s, frames, items, n_items);
 }
 
 }  // namespace av1pf
