@@ -60,8 +60,9 @@ constexpr int kOutOffs = 18;
 // steps earlier and is visible after the warp's barrier. The luma warp
 // publishes its completed step count in `progress` every kPublish steps; a
 // chroma warp waits, before a step, for the luma cells its luma term reads
-// (a bounded wait: after kSpinLimit polls it flags ERRF_STALL and goes on).
-constexpr int kSpinLimit = 1 << 22;
+// (a bounded wait, polling with a short sleep: after kSpinLimit polls it
+// flags ERRF_STALL and goes on).
+constexpr int kSpinLimit = 1 << 20;
 constexpr int kPublish = 8;
 
 __device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t* p) {
@@ -111,6 +112,9 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
             if (lane == 0) atomicOr(&g_error_flags, ERRF_STALL);
             break;
           }
+          // back off: a tight poll would crowd the shared-memory pipe the
+          // luma warp's loads go through
+          __nanosleep(64);
         }
       }
     }
@@ -333,6 +337,157 @@ __device__ __forceinline__ int hblend(int old, int g, int j, int psx, int gmin, 
   return clip3(gmin, gmax, round2(gv, 5));
 }
 
+// The 8-sample groups of noise-stripe rows [ys, ye) of an item (columns
+// x0 .. x1): load, film grain (grain.rs:186-354), pack. Specialised on the
+// plane kind — CHROMA with its subsampling PSX / PSY (a chroma plane's
+// luma sits at x << PSX, y << PSY), and the sample width — so the per-sample
+// work has no run-time plane selects.
+template <bool CHROMA, int PSX, int PSY, int SB>
+__device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T, const int16_t* lut,
+                                           const uint8_t* offs_cur, const uint8_t* offs_prev, int x0, int x1,
+                                           int ys, int ye, int stripe, int b0, bool grain) {
+  const int ngroups = (x1 - x0 + 7) >> 3;  // 8-sample groups per row (<= 32)
+  const int sh = P.bd - 8;
+  constexpr int bshift = 5 - PSX;  // grain block width 32 >> psx
+  constexpr int sshift = 5 - PSY;  // noise stripe height 32 >> psy
+      for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
+    const int gx = k & 31, r = k >> 5;
+    if (gx >= ngroups) continue;
+    const int yy = ys + r;
+    const int xs = x0 + gx * 8;
+    const int n = min(8, x1 - xs);
+    int v[8];
+    const uint8_t* sp = P.src + int64_t(yy) * P.src_pitch + int64_t(xs) * SB;
+    const bool vec = n == 8 && (reinterpret_cast<uintptr_t>(sp) & (8 * SB - 1)) == 0;
+    if (vec && SB == 2) {
+      const uint4 q = *reinterpret_cast<const uint4*>(sp);
+      v[0] = q.x & 0xffff; v[1] = q.x >> 16; v[2] = q.y & 0xffff; v[3] = q.y >> 16;
+      v[4] = q.z & 0xffff; v[5] = q.z >> 16; v[6] = q.w & 0xffff; v[7] = q.w >> 16;
+    } else if (vec) {
+      const uint2 q = *reinterpret_cast<const uint2*>(sp);
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        v[e] = (q.x >> (8 * e)) & 0xff;
+        v[4 + e] = (q.y >> (8 * e)) & 0xff;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 8; e++)
+        v[e] = e < n ? (SB == 1 ? int(sp[e]) : int(reinterpret_cast<const uint16_t*>(sp)[e])) : 0;
+    }
+    if (grain) {
+      // noise image (grain.rs:251-283); the 8 samples share one grain block
+      const int i = yy - (stripe << sshift);
+      const int b = xs >> bshift;
+      const int jb = xs - (b << bshift);
+      const int li = b - b0 + 1;  // index into the staged offsets
+      const bool vblend = P.overlap && stripe > 0 && i < (PSY ? 1 : 2);
+      int lum[8];
+      if (CHROMA) {
+        // un-grained luma under each chroma sample (grain.rs:303-314)
+        const int ly = yy << PSY;
+        const uint8_t* lrow = P.luma + int64_t(ly) * P.luma_pitch;
+        const int lx0 = xs << PSX;
+        const uint8_t* lp = lrow + int64_t(lx0) * SB;
+        // the group's whole luma span (8 or 16 samples, no edge clamp
+        // inside it) in 8-byte loads
+        if (n == 8 && lx0 + (8 << PSX) <= P.w && (reinterpret_cast<uintptr_t>(lp) & 7) == 0) {
+          uint32_t wv[8];
+          const int nw = (8 << PSX) * SB / 4;  // 32-bit words: 2, 4 or 8
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (2 * q < nw) {
+              const uint2 v2 = reinterpret_cast<const uint2*>(lp)[q];
+              wv[2 * q] = v2.x;
+              wv[2 * q + 1] = v2.y;
+            }
+          auto lsamp = [&](int k) {  // luma sample k of the span
+            return SB == 2 ? int((wv[k >> 1] >> (16 * (k & 1))) & 0xffffu)
+                             : int((wv[k >> 2] >> (8 * (k & 3))) & 0xffu);
+          };
+#pragma unroll
+          for (int e = 0; e < 8; e++)
+            lum[e] = PSX ? round2(lsamp(2 * e) + lsamp(2 * e + 1), 1) : lsamp(e);
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            if (e < n) {
+              const int lx = (xs + e) << PSX;
+              const int lnx = min(lx + 1, P.w - 1);
+              const int l0 = SB == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
+              const int l1 = SB == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
+              lum[e] = PSX ? round2(l0 + l1, 1) : l0;
+            }
+          }
+        }
+      }
+      // the group's noise (grain.rs:200-283): its 8 samples lie in one
+      // grain block, so the template positions are found once; only a
+      // block's first 1-2 columns blend with the block to the left, and
+      // only a stripe's first 1-2 rows with the stripe above
+      const int nh = (P.overlap && b > 0 && jb == 0) ? (PSX ? 1 : 2) : 0;
+      const int16_t* tp = tmpl_at(T, PSX, PSY, i, offs_cur[li]) + jb;
+      const int16_t* tl = left_at(T, PSX, PSY, i, offs_cur[li - 1]);
+      const int vrow = i + (32 >> PSY);
+      const int16_t* vp = tmpl_at(T, PSX, PSY, vrow, offs_prev[li]) + jb;
+      const int16_t* vl = left_at(T, PSX, PSY, vrow, offs_prev[li - 1]);
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        if (e >= n) continue;
+        int noise = tp[e];
+        if (e < nh) noise = hblend(tl[e], noise, e, PSX, P.gmin, P.gmax);
+        if (vblend) {
+          int old = vp[e];
+          if (e < nh) old = hblend(vl[e], old, e, PSX, P.gmin, P.gmax);
+          const int g2 = PSY ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
+          noise = clip3(P.gmin, P.gmax, round2(g2, 5));
+        }
+        const int orig = v[e];
+        int idx = orig;
+        if (CHROMA) {
+          if (P.csfl) {
+            idx = lum[e];
+          } else {
+            const int combined = lum[e] * (P.lmult - 128) + orig * (P.mult - 128);
+            idx = clip3(0, P.maxpix, (combined >> 6) + ((P.offs - 256) * (1 << sh)));
+          }
+        }
+        noise = round2(grain_scale(lut, idx, sh) * noise, P.scaling_shift);
+        v[e] = clip3(P.min_value, P.max_v, orig + noise);
+      }
+    }
+    // pack (frame.rs:153-158): u8 at 8-bit, little-endian u16 above
+    const int64_t o = int64_t(yy) * P.pw + xs;
+    if (P.wide) {
+      uint16_t* op = reinterpret_cast<uint16_t*>(P.out) + o;
+      if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 15) == 0) {
+        uint4 q;
+        q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 16);
+        q.y = uint32_t(v[2]) | (uint32_t(v[3]) << 16);
+        q.z = uint32_t(v[4]) | (uint32_t(v[5]) << 16);
+        q.w = uint32_t(v[6]) | (uint32_t(v[7]) << 16);
+        *reinterpret_cast<uint4*>(op) = q;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 8; e++)
+          if (e < n) op[e] = uint16_t(v[e]);
+      }
+    } else {
+      uint8_t* op = P.out + o;
+      if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 7) == 0) {
+        uint2 q;
+        q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 8) | (uint32_t(v[2]) << 16) | (uint32_t(v[3]) << 24);
+        q.y = uint32_t(v[4]) | (uint32_t(v[5]) << 8) | (uint32_t(v[6]) << 16) | (uint32_t(v[7]) << 24);
+        *reinterpret_cast<uint2*>(op) = q;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 8; e++)
+          if (e < n) op[e] = uint8_t(v[e]);
+      }
+    }
+  }
+}
+
 // Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
 // 256 (so of the grain block width). A CTA works through a contiguous run of
 // items. The rows are taken one noise stripe
@@ -417,8 +572,6 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
       }
     }
     const int x0 = item.x0, x1 = item.x1;
-    const int ngroups = (x1 - x0 + 7) >> 3;  // 8-sample groups per row (<= 32)
-    const int sh = P.bd - 8;
     const int bshift = 5 - P.psx;  // grain block width 32 >> psx
     const int sshift = 5 - P.psy;  // noise stripe height 32 >> psy
     const int b0 = x0 >> bshift;
@@ -432,140 +585,20 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
         offs_prev[threadIdx.x] = ok && stripe > 0 ? P.off[int64_t(stripe - 1) * P.nb + b] : 0;
       }
       __syncthreads();
-      for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
-        const int gx = k & 31, r = k >> 5;
-        if (gx >= ngroups) continue;
-        const int yy = ys + r;
-        const int xs = x0 + gx * 8;
-        const int n = min(8, x1 - xs);
-        int v[8];
-        const uint8_t* sp = P.src + int64_t(yy) * P.src_pitch + int64_t(xs) * P.sb;
-        const bool vec = n == 8 && (reinterpret_cast<uintptr_t>(sp) & (8 * P.sb - 1)) == 0;
-        if (vec && P.sb == 2) {
-          const uint4 q = *reinterpret_cast<const uint4*>(sp);
-          v[0] = q.x & 0xffff; v[1] = q.x >> 16; v[2] = q.y & 0xffff; v[3] = q.y >> 16;
-          v[4] = q.z & 0xffff; v[5] = q.z >> 16; v[6] = q.w & 0xffff; v[7] = q.w >> 16;
-        } else if (vec) {
-          const uint2 q = *reinterpret_cast<const uint2*>(sp);
-#pragma unroll
-          for (int e = 0; e < 4; e++) {
-            v[e] = (q.x >> (8 * e)) & 0xff;
-            v[4 + e] = (q.y >> (8 * e)) & 0xff;
-          }
-        } else {
-#pragma unroll
-          for (int e = 0; e < 8; e++)
-            v[e] = e < n ? (P.sb == 1 ? int(sp[e]) : int(reinterpret_cast<const uint16_t*>(sp)[e])) : 0;
-        }
-        if (P.grain) {
-          // noise image (grain.rs:251-283); the 8 samples share one grain block
-          const int i = yy - (stripe << sshift);
-          const int b = xs >> bshift;
-          const int jb = xs - (b << bshift);
-          const int li = b - b0 + 1;  // index into the staged offsets
-          const bool vblend = P.overlap && stripe > 0 && i < (P.psy ? 1 : 2);
-          int lum[8];
-          if (item.plane != 0) {
-            // un-grained luma under each chroma sample (grain.rs:303-314)
-            const int ly = yy << P.ssy;
-            const uint8_t* lrow = P.luma + int64_t(ly) * P.luma_pitch;
-            const int lx0 = xs << P.ssx;
-            const uint8_t* lp = lrow + int64_t(lx0) * P.sb;
-            // the group's whole luma span (8 or 16 samples, no edge clamp
-            // inside it) in 8-byte loads
-            if (n == 8 && lx0 + (8 << P.ssx) <= P.w && (reinterpret_cast<uintptr_t>(lp) & 7) == 0) {
-              uint32_t wv[8];
-              const int nw = (8 << P.ssx) * P.sb / 4;  // 32-bit words: 2, 4 or 8
-#pragma unroll
-              for (int q = 0; q < 4; q++)
-                if (2 * q < nw) {
-                  const uint2 v2 = reinterpret_cast<const uint2*>(lp)[q];
-                  wv[2 * q] = v2.x;
-                  wv[2 * q + 1] = v2.y;
-                }
-              auto lsamp = [&](int k) {  // luma sample k of the span
-                return P.sb == 2 ? int((wv[k >> 1] >> (16 * (k & 1))) & 0xffffu)
-                                 : int((wv[k >> 2] >> (8 * (k & 3))) & 0xffu);
-              };
-#pragma unroll
-              for (int e = 0; e < 8; e++)
-                lum[e] = P.ssx ? round2(lsamp(2 * e) + lsamp(2 * e + 1), 1) : lsamp(e);
-            } else {
-#pragma unroll
-              for (int e = 0; e < 8; e++) {
-                if (e < n) {
-                  const int lx = (xs + e) << P.ssx;
-                  const int lnx = min(lx + 1, P.w - 1);
-                  const int l0 = P.sb == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
-                  const int l1 = P.sb == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
-                  lum[e] = P.ssx ? round2(l0 + l1, 1) : l0;
-                }
-              }
-            }
-          }
-          // the group's noise (grain.rs:200-283): its 8 samples lie in one
-          // grain block, so the template positions are found once; only a
-          // block's first 1-2 columns blend with the block to the left, and
-          // only a stripe's first 1-2 rows with the stripe above
-          const int nh = (P.overlap && b > 0 && jb == 0) ? (P.psx ? 1 : 2) : 0;
-          const int16_t* tp = tmpl_at(T, P.psx, P.psy, i, offs_cur[li]) + jb;
-          const int16_t* tl = left_at(T, P.psx, P.psy, i, offs_cur[li - 1]);
-          const int vrow = i + (32 >> P.psy);
-          const int16_t* vp = tmpl_at(T, P.psx, P.psy, vrow, offs_prev[li]) + jb;
-          const int16_t* vl = left_at(T, P.psx, P.psy, vrow, offs_prev[li - 1]);
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            if (e >= n) continue;
-            int noise = tp[e];
-            if (e < nh) noise = hblend(tl[e], noise, e, P.psx, P.gmin, P.gmax);
-            if (vblend) {
-              int old = vp[e];
-              if (e < nh) old = hblend(vl[e], old, e, P.psx, P.gmin, P.gmax);
-              const int g2 = P.psy ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
-              noise = clip3(P.gmin, P.gmax, round2(g2, 5));
-            }
-            const int orig = v[e];
-            int idx = orig;
-            if (item.plane != 0) {
-              if (P.csfl) {
-                idx = lum[e];
-              } else {
-                const int combined = lum[e] * (P.lmult - 128) + orig * (P.mult - 128);
-                idx = clip3(0, P.maxpix, (combined >> 6) + ((P.offs - 256) * (1 << sh)));
-              }
-            }
-            noise = round2(grain_scale(lut, idx, sh) * noise, P.scaling_shift);
-            v[e] = clip3(P.min_value, P.max_v, orig + noise);
-          }
-        }
-        // pack (frame.rs:153-158): u8 at 8-bit, little-endian u16 above
-        const int64_t o = int64_t(yy) * P.pw + xs;
-        if (P.wide) {
-          uint16_t* op = reinterpret_cast<uint16_t*>(P.out) + o;
-          if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 15) == 0) {
-            uint4 q;
-            q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 16);
-            q.y = uint32_t(v[2]) | (uint32_t(v[3]) << 16);
-            q.z = uint32_t(v[4]) | (uint32_t(v[5]) << 16);
-            q.w = uint32_t(v[6]) | (uint32_t(v[7]) << 16);
-            *reinterpret_cast<uint4*>(op) = q;
-          } else {
-#pragma unroll
-            for (int e = 0; e < 8; e++)
-              if (e < n) op[e] = uint16_t(v[e]);
-          }
-        } else {
-          uint8_t* op = P.out + o;
-          if (n == 8 && (reinterpret_cast<uintptr_t>(op) & 7) == 0) {
-            uint2 q;
-            q.x = uint32_t(v[0]) | (uint32_t(v[1]) << 8) | (uint32_t(v[2]) << 16) | (uint32_t(v[3]) << 24);
-            q.y = uint32_t(v[4]) | (uint32_t(v[5]) << 8) | (uint32_t(v[6]) << 16) | (uint32_t(v[7]) << 24);
-            *reinterpret_cast<uint2*>(op) = q;
-          } else {
-#pragma unroll
-            for (int e = 0; e < 8; e++)
-              if (e < n) op[e] = uint8_t(v[e]);
-          }
+      if (item.plane == 0) {
+        if (P.sb == 2)
+          out_stripe<false, 0, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain);
+        else
+          out_stripe<false, 0, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain);
+      } else {
+        const int k3 = (P.psx ? 2 : 0) + (P.psy ? 1 : 0) + (P.sb == 2 ? 4 : 0);
+        switch (k3) {
+          case 0: out_stripe<true, 0, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 2: out_stripe<true, 1, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 3: out_stripe<true, 1, 1, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 4: out_stripe<true, 0, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 6: out_stripe<true, 1, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          default: out_stripe<true, 1, 1, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
         }
       }
       __syncthreads();

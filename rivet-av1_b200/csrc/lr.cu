@@ -396,22 +396,72 @@ __device__ __forceinline__ void restore_rect(const FrameDesc& f, const LrSmem& s
     src.cur_pitch = int32_t(f.cur[p].stride * sb);
     src.lines_pitch = int32_t(lines.stride * sb);
     src.sr = f.sr_on != 0 || f.prelf[p].p != nullptr;
-    const int sg = tid / SW, sc = tid - sg * SW;
-    const int x = max(min(x0 + sc - 3, geo.pex), 0);
-    constexpr int kWinRows = (kMaxH + 6 + SG - 1) / SG;  // window rows per thread
-    constexpr int kBatch = (kWinRows + 1) / 2;               // loads in flight per thread
+    // Window row r, columns 8q .. 8q+7 (samples x0-3+8q ..) per task. Where
+    // the two aligned 8-sample chunks that hold them lie inside the plane
+    // row (and the row is 16-byte aligned) they come as two vector loads
+    // and are shifted into place; other chunks (the plane's left and right
+    // edges) take one clamped scalar load per sample. The loads of two tasks
+    // issue before their stores.
+    const int nq = (ww + 7) >> 3;  // chunks per window row (<= 9)
+    constexpr int kTasks = ((kMaxH + 6) * 9 + kThreads - 1) / kThreads;
+    const int ntask = wh * nq;
+    constexpr int kBatch = 2;  // tasks whose loads are in flight together
 #pragma unroll
-    for (int m0 = 0; m0 < kWinRows; m0 += kBatch) {
-      int v[kBatch];
+    for (int m0 = 0; m0 < kTasks; m0 += kBatch) {
+      uint32_t wv[kBatch][5];  // the loaded words a window chunk is cut from
+      bool vec[kBatch];
 #pragma unroll
       for (int m = 0; m < kBatch; m++) {
-        const int r = sg + SG * (m0 + m);
-        if (r < wh && sc < ww) v[m] = ld_row(lr_row(src, geo, s, geo.y0 + r - 3), sb, x);
+        const int k = tid + (m0 + m) * kThreads;
+        vec[m] = false;
+        if (m0 + m >= kTasks || k >= ntask) continue;
+        const int r = k / nq, q = k - r * nq;
+        const uint8_t* row = lr_row(src, geo, s, geo.y0 + r - 3);
+        const int gx = x0 - 8 + 8 * q;  // first sample of the left chunk
+        if (gx < 0 || gx + 16 > geo.pex + 1 || (reinterpret_cast<uintptr_t>(row) & 15) != 0) continue;
+        vec[m] = true;
+        if (sb == 2) {
+          // samples 4..7 of the left chunk and 0..5 of the right one
+          const uint2 a = *reinterpret_cast<const uint2*>(row + int64_t(gx) * 2 + 8);
+          const uint4 b = *reinterpret_cast<const uint4*>(row + int64_t(gx) * 2 + 16);
+          wv[m][0] = a.x; wv[m][1] = a.y; wv[m][2] = b.x; wv[m][3] = b.y; wv[m][4] = b.z;
+        } else {
+          // bytes 4..15 of the 16 samples
+          const uint4 a = *reinterpret_cast<const uint4*>(row + gx);
+          wv[m][0] = a.y; wv[m][1] = a.z; wv[m][2] = a.w;
+        }
       }
 #pragma unroll
       for (int m = 0; m < kBatch; m++) {
-        const int r = sg + SG * (m0 + m);
-        if (r < wh && sc < ww) win[r * kWS + sc] = uint16_t(v[m]);
+        const int k = tid + (m0 + m) * kThreads;
+        if (m0 + m >= kTasks || k >= ntask) continue;
+        const int r = k / nq, q = k - r * nq;
+        uint16_t* wp = &win[r * kWS + 8 * q];
+        if (vec[m]) {
+          uint4 o;
+          if (sb == 2) {
+            // window sample 2j of the chunk is sample 5 + 2j of the 16 from gx
+            o.x = __funnelshift_r(wv[m][0], wv[m][1], 16);
+            o.y = __funnelshift_r(wv[m][1], wv[m][2], 16);
+            o.z = __funnelshift_r(wv[m][2], wv[m][3], 16);
+            o.w = __funnelshift_r(wv[m][3], wv[m][4], 16);
+          } else {
+            const uint32_t lo = __funnelshift_r(wv[m][0], wv[m][1], 8);  // bytes 5..8
+            const uint32_t hi = __funnelshift_r(wv[m][1], wv[m][2], 8);  // bytes 9..12
+            o.x = __byte_perm(lo, 0, 0x4140);
+            o.y = __byte_perm(lo, 0, 0x4342);
+            o.z = __byte_perm(hi, 0, 0x4140);
+            o.w = __byte_perm(hi, 0, 0x4342);
+          }
+          *reinterpret_cast<uint4*>(wp) = o;
+        } else {
+          const uint8_t* row = lr_row(src, geo, s, geo.y0 + r - 3);
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            const int c = 8 * q + e;
+            if (c < ww) wp[e] = uint16_t(ld_row(row, sb, max(min(x0 - 3 + c, geo.pex), 0)));
+          }
+        }
       }
     }
   }
