@@ -78,6 +78,16 @@ __device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
                : "memory");
 }
 
+// A signed 16-bit shared-memory load at byte offset `off` from the shared
+// address `a`. Volatile, so a step's loads issue in order, back to back,
+// before the first of them is used, and stay after the warp barrier that
+// makes them visible.
+__device__ __forceinline__ int ld_shared_s16(uint32_t a, int off) {
+  short v;
+  asm volatile("ld.shared.s16 %0, [%1];" : "=h"(v) : "r"(a + uint32_t(off)));
+  return int(v);
+}
+
 template <int LAG, bool CHROMA>
 __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kTW], const int32_t* coef_s, int H,
                                         int W, int ar_shift, int gmin, int gmax, int sub_x, int sub_y, bool luma_on,
@@ -127,30 +137,42 @@ __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kT
       // (y - 1, x + 3) is an AR cell of the previous step when the row above
       // is filtered and x + 3 is inside the filtered columns
       const bool up_fresh = LAG == 3 && rr >= 1 && x + 3 < W - 3;
+      // every neighbour of the rows above, and the cell itself, loaded
+      // before any is used (one shared-memory round trip per step)
+      const uint32_t at = static_cast<uint32_t>(__cvta_generic_to_shared(&T[y][x]));
+      int nb[LAG > 0 ? LAG : 1][2 * LAG + 1];
+#pragma unroll
+      for (int dr = -LAG; dr < 0; dr++)
+#pragma unroll
+        for (int dc = -LAG; dc <= LAG; dc++) nb[dr + LAG][dc + LAG] = ld_shared_s16(at, 2 * (dr * kTW + dc));
+      const int own = ld_shared_s16(at, 0);
+      int luma = 0;
+      if (CHROMA && luma_on) {
+        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
+        const uint32_t la = static_cast<uint32_t>(__cvta_generic_to_shared(&Y[ly][lx]));
+        luma = ld_shared_s16(la, 0);
+        if (sub_x) luma += ld_shared_s16(la, 2);
+        if (sub_y) luma += ld_shared_s16(la, 2 * kTW);
+        if (sub_x && sub_y) luma += ld_shared_s16(la, 2 * kTW + 2);
+      }
+      if constexpr (LAG == 3) {
+        if (up_fresh) nb[2][6] = up;
+      }
       int s[LAG + 2] = {};
 #pragma unroll
       for (int dr = -LAG; dr < 0; dr++)
 #pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++) {
-          const int cv = (dr == -1 && dc == LAG && up_fresh) ? up : int(T[y + dr][x + dc]);
-          s[LAG + dr] += cv * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
-        }
+        for (int dc = -LAG; dc <= LAG; dc++)
+          s[LAG + dr] += nb[dr + LAG][dc + LAG] * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
       const int lp = LAG * (2 * LAG + 1);
       if (LAG >= 1) s[LAG] += l1 * c[lp + LAG - 1];
       if (LAG >= 2) s[LAG] += l2 * c[lp + LAG - 2];
       if (LAG >= 3) s[LAG] += l3 * c[lp + LAG - 3];
-      if (CHROMA && luma_on) {
-        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
-        int luma = Y[ly][lx];
-        if (sub_x) luma += Y[ly][lx + 1];
-        if (sub_y) luma += Y[ly + 1][lx];
-        if (sub_x && sub_y) luma += Y[ly + 1][lx + 1];
-        s[LAG + 1] = round2(luma, sub_x + sub_y) * c[NC];
-      }
+      if (CHROMA && luma_on) s[LAG + 1] = round2(luma, sub_x + sub_y) * c[NC];
       int sum = 0;
 #pragma unroll
       for (int k = 0; k < LAG + 2; k++) sum += s[k];
-      v = clip3(gmin, gmax, T[y][x] + round2(sum, ar_shift));
+      v = clip3(gmin, gmax, own + round2(sum, ar_shift));
       T[y][x] = int16_t(v);
       l3 = l2;
       l2 = l1;
