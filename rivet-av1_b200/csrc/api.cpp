@@ -286,6 +286,7 @@ int av1pf_ctx_create(int device, uint64_t hbm_cap_bytes, av1pf_ctx** out) {
       if ((e = lr_init()) != cudaSuccess) return cuda_status(e, "loop restoration kernel attributes");
       if ((e = superres_init()) != cudaSuccess) return cuda_status(e, "superres kernel attributes");
       if ((e = cdef_init()) != cudaSuccess) return cuda_status(e, "CDEF kernel attributes");
+      if ((e = output_init()) != cudaSuccess) return cuda_status(e, "output kernel attributes");
       g_tables_ready[device] = true;
     }
   }

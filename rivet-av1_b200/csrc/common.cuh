@@ -43,8 +43,8 @@ enum : uint32_t { ERRF_BAD_MAP = 1u, ERRF_BAD_ITEM = 2u, ERRF_STALL = 4u };
 // ---------------------------------------------------------------------------
 // Integer helpers (consts.rs:328-368, bits.rs:112)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int32_t round2(int32_t x, int n) {
-  return n == 0 ? x : (x + (1 << (n - 1))) >> n;
+__device__ __forceinline__ int32_t round2(int32_t x, int n) {  // 0 <= n <= 30
+  return (x + ((1 << n) >> 1)) >> n;
 }
 __device__ __forceinline__ int64_t round2_64(int64_t x, int n) {
   return n == 0 ? x : (x + (int64_t(1) << (n - 1))) >> n;

@@ -19,7 +19,9 @@ struct DPlane {
 // Film-grain scratch of one frame (filled by the template kernel).
 struct GrainScratch {
   int16_t tmpl[3][73][82];  // luma, cb, cr grain templates (7.18.3.3)
-  uint8_t lut[3][256];      // scaling lookup (7.18.3.4)
+  // the scaling function (7.18.3.4) at every sample value 0 .. 2^bitdepth - 1:
+  // the 256-entry lookup, interpolated between entries above 8 bits
+  alignas(16) uint8_t scale[3][4096];
 };
 
 // Everything a stage kernel needs about one frame. Built on the host,

@@ -14,9 +14,11 @@
 //   - The auto-regressive filter is a raster recurrence whose reach is at
 //     most 3 columns left and 3 rows up (3 columns right on earlier rows),
 //     so cells with equal (x - 3) + 4 (y - 3) are independent: one warp per
-//     template walks that wavefront, a lane per row on it, with warp-level
-//     synchronisation only (the value each step needs from the previous one
-//     comes by shuffle); the chroma warps trail the luma warp.
+//     template walks that wavefront, a lane per row on it. Every neighbour a
+//     cell reads reaches its lane by warp shuffles from the lanes of the rows
+//     above and is kept in register rings, so the recurrence runs without
+//     shared-memory round trips or barriers; the chroma warps trail the luma
+//     warp.
 // output_kernel: per 256-column tile of a plane's visible area, reads the reference
 // frame, adds grain (noise assembled from the templates, the 32x32 block
 // offsets and the overlap blends of grain.rs:179-283, evaluated per sample
@@ -33,6 +35,19 @@ __device__ __forceinline__ uint32_t rng_step(uint32_t r) {  // grain.rs:12-18 (s
   return (r >> 1) | (bit << 15);
 }
 
+// Four steps of rng_step at once, the states after each into st[0..3]. The
+// feedback bit of step j (1..4) is bit j - 1 of r ^ r>>1 ^ r>>3 ^ r>>12: its
+// taps read bits j-1, j, j+2 and j+11 of the starting state, all below the
+// bits the earlier steps shifted in (those reach bit 12 of the state only
+// at step 5).
+__device__ __forceinline__ void rng_step4(uint32_t r, uint32_t st[4]) {
+  const uint32_t f = r ^ (r >> 1) ^ (r >> 3) ^ (r >> 12);
+  st[0] = (r >> 1) | ((f & 1u) << 15);
+  st[1] = (r >> 2) | ((f & 3u) << 14);
+  st[2] = (r >> 3) | ((f & 7u) << 13);
+  st[3] = (r >> 4) | ((f & 15u) << 12);
+}
+
 __device__ __forceinline__ uint32_t rng_jump(uint32_t seed, const uint16_t* cols) {
   uint32_t s = 0;
 #pragma unroll
@@ -45,25 +60,48 @@ constexpr int kTH = 73, kTW = 82;
 // Staged block offsets per output item: 256 columns span at most 16 grain
 // blocks (16 columns wide in subsampled chroma), plus the block to the left.
 constexpr int kOutOffs = 18;
+// Staged row strides of the output kernel: 256 samples of up to 2 bytes, and
+// the luma under 256 chroma columns (512 samples at 2:1).
+constexpr int kStageSrc = 512, kStageLuma = 1024;
 }  // namespace
 
 // Auto-regression of one template (grain.rs:55-73 for luma, :101-134 for
-// chroma with its luma term) by one warp. Template row 3 + rr belongs to lane
-// rr % 32 and is walked left to right along the wavefront (x - 3) + 4 rr = t:
-// a cell's left neighbours in its row were done at steps t-1..t-LAG by the
-// same lane (kept in registers), and its neighbours in the rows above, at
-// most LAG columns to the right, at step t-1 or earlier by the lanes before
-// it. At most 20 rows are on the wavefront at once, so no two of a lane's
-// rows are. The one value a step needs from the step just before it — the
-// cell up and LAG = 3 to the right, made by the lane above — comes by a warp
-// shuffle; every other neighbour was stored to shared memory at least two
-// steps earlier and is visible after the warp's barrier. The luma warp
-// publishes its completed step count in `progress` every kPublish steps; a
-// chroma warp waits, before a step, for the luma cells its luma term reads
-// (a bounded wait, polling with a short sleep: after kSpinLimit polls it
-// flags ERRF_STALL and goes on).
+// chroma with its luma term) by one warp, on a wavefront: the cell (y, x) is
+// filtered at step t = (x - 3) + S (y - 3). Its neighbours reach LAG rows up
+// and LAG columns to either side (left only in its own row), so with a slope
+// S >= LAG + 1 each of them comes at an earlier step; S is at least 3 so
+// that no more rows are on the wavefront at once than a warp has lanes.
+// Template row 3 + rr belongs to lane rr % 32, which walks it left to right,
+// one column per step, from column 0 (three steps before its first filtered
+// cell) to the last column.
+//
+// At every step every lane emits the value of its cell: the filtered value,
+// or the Gaussian value for the unfiltered border columns and the three top
+// rows (rows -3 .. -1 of the wavefront, walked by lanes 29 .. 31). The lane
+// k rows below receives the emission one step later by a warp shuffle: the
+// emission of lane (l - k) at step t - 1 is the cell (y - k, x + kS - 1) of
+// lane l at step t. Each lane keeps what it received from the lanes 1 .. LAG
+// above in register rings (slot t % 16; the oldest value read is 3S + LAG - 1
+// <= 14 steps old) and its own last LAG emissions: the filter reads no
+// shared memory except the cell's own Gaussian value, and the warp needs no
+// barrier between steps. The steps run in groups of 8 without branches
+// (cells outside the filter compute and store their own value back), so the
+// scheduler overlaps each step's sums over older values with the step
+// before; the step-to-step chain is the shuffle, one multiply-add, the
+// rounding and the clip.
+//
+// The luma warp publishes its completed step count in `progress` after every
+// group of 8 steps (past a warp barrier that orders its lanes' template
+// stores before the release); a chroma warp waits, before a group, for the
+// luma cells the group's luma terms read (a bounded wait, polling with a
+// short sleep: after kSpinLimit polls it flags ERRF_STALL and goes on).
 constexpr int kSpinLimit = 1 << 20;
-constexpr int kPublish = 8;
+constexpr int kProgressBias = 64;  // progress holds (last luma step done) + 1 + bias; 0 is "none"
+
+template <int LAG>
+__device__ __forceinline__ constexpr int ar_slope() {
+  return LAG + 1 > 3 ? LAG + 1 : 3;
+}
 
 __device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t* p) {
   uint32_t v;
@@ -78,111 +116,132 @@ __device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
                : "memory");
 }
 
-// A signed 16-bit shared-memory load at byte offset `off` from the shared
-// address `a`. Volatile, so a step's loads issue in order, back to back,
-// before the first of them is used, and stay after the warp barrier that
-// makes them visible.
-__device__ __forceinline__ int ld_shared_s16(uint32_t a, int off) {
-  short v;
-  asm volatile("ld.shared.s16 %0, [%1];" : "=h"(v) : "r"(a + uint32_t(off)));
-  return int(v);
+// The cell lane `lane` holds at step t: row y, column x, whether the filter
+// runs there, and a template offset that is always inside the template —
+// the cell itself, or for a cell outside the template, a border cell (row 0,
+// or the first or last column) that no step filters.
+struct ArCell {
+  int y, x, off;
+  bool ar;
+};
+template <int S>
+__device__ __forceinline__ ArCell ar_cell(int t, int lane, int H, int W) {
+  const int q = (t + 3 + 16 * S) / S - 16;  // floor((t + 3) / S): rows change lanes at column 0
+  const int rr = q - ((q - lane) & 31);
+  ArCell c;
+  c.y = 3 + rr;
+  c.x = 3 + t - S * rr;
+  c.ar = rr >= 0 && c.y < H && c.x >= 3 && c.x < W - 3;
+  const int yc = c.y >= 0 && c.y < H ? c.y : 0;
+  const int xc = min(max(c.x, 0), W - 1);
+  c.off = yc * kTW + xc;
+  return c;
 }
 
 template <int LAG, bool CHROMA>
 __device__ __forceinline__ void ar_warp(int16_t (*T)[kTW], const int16_t (*Y)[kTW], const int32_t* coef_s, int H,
                                         int W, int ar_shift, int gmin, int gmax, int sub_x, int sub_y, bool luma_on,
                                         uint32_t* progress) {
+  constexpr int S = ar_slope<LAG>();
   constexpr int NC = 2 * LAG * (LAG + 1);
+  constexpr int RW = 2 * LAG + 1;  // coefficients per row above
   int c[NC + 1];
 #pragma unroll
   for (int k = 0; k <= NC; k++) c[k] = coef_s[k];
   const int lane = threadIdx.x & 31;
-  const int above = (lane + 31) & 31;  // the lane of the row above
-  const int rows = H - 3, cols = W - 6;
-  const int steps = (cols - 1) + 4 * (rows - 1) + 1;
-  int l1 = 0, l2 = 0, l3 = 0;  // the lane's row at x-1, x-2, x-3
-  int v = 0;                   // the lane's latest output
-  uint32_t seen = 0;           // luma steps known complete
-  for (int t = 0; t < steps; t++) {
-    const int q = t >> 2;
-    const int rr = q - ((q - lane) & 31);  // the lane's row on this step's wavefront
-    const int x = 3 + t - 4 * rr;
-    const bool active = rr >= 0 && rr < rows && x < W - 3;
-    const int y = 3 + rr;
-    // the cell (y - 1, x + 3) the lane above made on the previous step
-    const int up = __shfl_sync(0xffffffffu, v, above);
-    if (CHROMA && luma_on) {
-      // the last luma step whose cell this step's luma terms read
-      const int need = active ? ((x - 3) << sub_x) + sub_x + 4 * (((y - 3) << sub_y) + sub_y) : -1;
-      const int wneed = __reduce_max_sync(0xffffffffu, need);
-      if (wneed >= int(seen)) {
-        int spins = 0;
-        while ((seen = ld_acquire_cta(progress)) <= uint32_t(wneed)) {
-          if (++spins > kSpinLimit) {
-            if (lane == 0) atomicOr(&g_error_flags, ERRF_STALL);
-            break;
+  const int rows = H - 3;
+  const int t_last = (W - 7) + S * (rows - 1);  // the last row's last filtered cell
+  const bool luma_term = CHROMA && luma_on;
+  int16_t* Tf = &T[0][0];
+  const int16_t* Yf = &Y[0][0];
+  int own[16];                   // the lane's emission of step t in slot t % 16
+  int w[LAG > 0 ? LAG : 1][16];  // w[k - 1]: emissions of the lane k rows above, one step late
+#pragma unroll
+  for (int u = 0; u < 16; u++) {
+    own[u] = 0;
+#pragma unroll
+    for (int k = 0; k < (LAG > 0 ? LAG : 1); k++) w[k][u] = 0;
+  }
+  uint32_t seen = 0;  // the luma progress last read
+  // steps from -16 (the top row -3 starts at -S * 3 - 3 >= -15), in blocks of
+  // 16 so that every ring slot is a constant, and groups of 8 whose steps
+  // have no branches
+  for (int tb = -16; tb <= t_last; tb += 16) {
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const int t0 = tb + 8 * half;
+      if (luma_term) {
+        // the last luma step whose cell the group's luma terms read
+        int need = -(1 << 20);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const ArCell e = ar_cell<S>(t0 + j, lane, H, W);
+          if (e.ar) need = max(need, ((e.x - 3) << sub_x) + sub_x + S * (((e.y - 3) << sub_y) + sub_y));
+        }
+        const int wneed = __reduce_max_sync(0xffffffffu, need) + kProgressBias;
+        if (wneed >= int(seen)) {
+          int spins = 0;
+          while ((seen = ld_acquire_cta(progress)) <= uint32_t(wneed)) {
+            if (++spins > kSpinLimit) {
+              if (lane == 0) atomicOr(&g_error_flags, ERRF_STALL);
+              break;
+            }
+            __nanosleep(32);
           }
-          // back off: a tight poll would crowd the shared-memory pipe the
-          // luma warp's loads go through
-          __nanosleep(64);
         }
       }
+      // the group's cells, their Gaussian values and luma terms, loaded
+      // ahead: a cell is written by its own lane only
+      int off[8], g[8], lum[8];
+      uint32_t arm = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const ArCell e = ar_cell<S>(t0 + j, lane, H, W);
+        off[j] = e.off;
+        arm |= uint32_t(e.ar) << j;
+        g[j] = Tf[e.off];
+        lum[j] = 0;
+        if (luma_term) {
+          const int lo = e.ar ? (((e.y - 3) << sub_y) + 3) * kTW + ((e.x - 3) << sub_x) + 3 : 3 * kTW + 3;
+          int l = Yf[lo];
+          if (sub_x) l += Yf[lo + 1];
+          if (sub_y) l += Yf[lo + kTW];
+          if (sub_x && sub_y) l += Yf[lo + kTW + 1];
+          lum[j] = round2(l, sub_x + sub_y) * c[NC];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int u = 8 * half + j;
+        const int vprev = own[(u + 15) & 15];
+#pragma unroll
+        for (int k = 1; k <= LAG; k++) w[k - 1][u] = __shfl_sync(0xffffffffu, vprev, (lane - k) & 31);
+        // four partial sums over the values from earlier steps; (y - k, x +
+        // dc) came at step t + dc - kS + 1, and (y, x + dc) is the lane's
+        // own emission of step t + dc
+        int acc[4] = {lum[j], 0, 0, 0};
+        int n = 0;
+#pragma unroll
+        for (int k = LAG; k >= 1; k--)
+#pragma unroll
+          for (int dc = -LAG; dc <= LAG; dc++)
+            if (!(k == 1 && dc == LAG)) acc[n++ & 3] += w[k - 1][(u + dc - k * S + 1 + 32) & 15] * c[(LAG - k) * RW + dc + LAG];
+#pragma unroll
+        for (int dc = -LAG; dc <= -2; dc++) acc[n++ & 3] += own[(u + dc + 16) & 15] * c[LAG * RW + LAG + dc];
+        int sum = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        // the two values of the step before: the cell up and LAG to the
+        // right (just received) and the cell to the left
+        if (LAG > 0) sum += w[0][u] * c[(LAG - 1) * RW + 2 * LAG] + vprev * c[LAG * RW + LAG - 1];
+        const int v = (arm >> j) & 1u ? clip3(gmin, gmax, g[j] + round2(sum, ar_shift)) : g[j];
+        Tf[off[j]] = int16_t(v);  // a cell outside the filter gets its own value back
+        own[u] = v;
+      }
+      if (!CHROMA) {
+        // the warp barrier orders every lane's stores before the releases
+        __syncwarp();
+        st_release_cta(progress, uint32_t(t0 + 8 + kProgressBias));
+      }
     }
-    if (active) {
-      if (x == 3) {  // a new row: its first three columns are not filtered
-        l1 = T[y][2];
-        l2 = T[y][1];
-        l3 = T[y][0];
-      }
-      // (y - 1, x + 3) is an AR cell of the previous step when the row above
-      // is filtered and x + 3 is inside the filtered columns
-      const bool up_fresh = LAG == 3 && rr >= 1 && x + 3 < W - 3;
-      // every neighbour of the rows above, and the cell itself, loaded
-      // before any is used (one shared-memory round trip per step)
-      const uint32_t at = static_cast<uint32_t>(__cvta_generic_to_shared(&T[y][x]));
-      int nb[LAG > 0 ? LAG : 1][2 * LAG + 1];
-#pragma unroll
-      for (int dr = -LAG; dr < 0; dr++)
-#pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++) nb[dr + LAG][dc + LAG] = ld_shared_s16(at, 2 * (dr * kTW + dc));
-      const int own = ld_shared_s16(at, 0);
-      int luma = 0;
-      if (CHROMA && luma_on) {
-        const int lx = ((x - 3) << sub_x) + 3, ly = ((y - 3) << sub_y) + 3;
-        const uint32_t la = static_cast<uint32_t>(__cvta_generic_to_shared(&Y[ly][lx]));
-        luma = ld_shared_s16(la, 0);
-        if (sub_x) luma += ld_shared_s16(la, 2);
-        if (sub_y) luma += ld_shared_s16(la, 2 * kTW);
-        if (sub_x && sub_y) luma += ld_shared_s16(la, 2 * kTW + 2);
-      }
-      if constexpr (LAG == 3) {
-        if (up_fresh) nb[2][6] = up;
-      }
-      int s[LAG + 2] = {};
-#pragma unroll
-      for (int dr = -LAG; dr < 0; dr++)
-#pragma unroll
-        for (int dc = -LAG; dc <= LAG; dc++)
-          s[LAG + dr] += nb[dr + LAG][dc + LAG] * c[(dr + LAG) * (2 * LAG + 1) + dc + LAG];
-      const int lp = LAG * (2 * LAG + 1);
-      if (LAG >= 1) s[LAG] += l1 * c[lp + LAG - 1];
-      if (LAG >= 2) s[LAG] += l2 * c[lp + LAG - 2];
-      if (LAG >= 3) s[LAG] += l3 * c[lp + LAG - 3];
-      if (CHROMA && luma_on) s[LAG + 1] = round2(luma, sub_x + sub_y) * c[NC];
-      int sum = 0;
-#pragma unroll
-      for (int k = 0; k < LAG + 2; k++) sum += s[k];
-      v = clip3(gmin, gmax, own + round2(sum, ar_shift));
-      T[y][x] = int16_t(v);
-      l3 = l2;
-      l2 = l1;
-      l1 = v;
-    }
-    // the step's stores are visible to the whole warp past this barrier
-    __syncwarp();
-    // (the barrier orders every lane's stores before lane 0's release)
-    if (!CHROMA && lane == 0 && ((t % kPublish) == kPublish - 1 || t == steps - 1))
-      st_release_cta(progress, uint32_t(t + 1));
   }
 }
 
@@ -251,9 +310,17 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
         if (on) {
           const uint32_t s0 = plane == 0 ? seed : (plane == 1 ? seed ^ 0xb524u : seed ^ 0x49d8u);
           uint32_t r = rng_jump(s0, width == 82 ? g_rng_jump82[row] : g_rng_jump44[row]);
-          for (int c = 0; c < width; c++) {
-            r = rng_step(r);
-            T[plane][row][c] = int16_t(round2(gauss[(r >> 5) & 2047u], shift));
+          // four states per pass (rng_step4); the widths are even, so pairs
+          // of values go out as 32-bit stores (a row is 164 bytes)
+          uint32_t* dst = reinterpret_cast<uint32_t*>(&T[plane][row][0]);
+          for (int c = 0; c < width; c += 4) {
+            uint32_t st[4];
+            rng_step4(r, st);
+            r = st[3];
+            const int v0 = round2(gauss[(st[0] >> 5) & 2047u], shift), v1 = round2(gauss[(st[1] >> 5) & 2047u], shift);
+            const int v2 = round2(gauss[(st[2] >> 5) & 2047u], shift), v3 = round2(gauss[(st[3] >> 5) & 2047u], shift);
+            dst[c >> 1] = uint32_t(uint16_t(v0)) | (uint32_t(uint16_t(v1)) << 16);
+            if (c + 2 < width) dst[(c >> 1) + 1] = uint32_t(uint16_t(v2)) | (uint32_t(uint16_t(v3)) << 16);
           }
         }
       }
@@ -311,19 +378,28 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
     GrainScratch* gs = f.grain;
     for (int k = tid; k < 3 * kTH * kTW / 2; k += 256)
       reinterpret_cast<uint32_t*>(&gs->tmpl[0][0][0])[k] = reinterpret_cast<const uint32_t*>(&T[0][0][0])[k];
-    for (int k = tid; k < 3 * 256 / 4; k += 256)
-      reinterpret_cast<uint32_t*>(&gs->lut[0][0])[k] = reinterpret_cast<const uint32_t*>(&lut[0][0])[k];
+    // the scaling function at every sample value (scale_lut of
+    // grain.rs:166-177: above 8 bits, interpolated between the two entries
+    // around index >> (bitdepth - 8)), four values per 32-bit store
+    {
+      const int sh = bd - 8;
+      const int wshift = bd - 2;  // log2 of the words per plane
+      for (int k = tid; k < (3 << wshift); k += 256) {
+        const int plane = k >> wshift, i0 = (k - (plane << wshift)) * 4;
+        uint32_t word = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int index = i0 + e;
+          const int x = index >> sh, rem = index - (x << sh);
+          int v = lut[plane][x];
+          if (sh > 0 && x < 255) v += round2((int(lut[plane][x + 1]) - v) * rem, sh);
+          word |= uint32_t(v) << (8 * e);
+        }
+        reinterpret_cast<uint32_t*>(&gs->scale[plane][0])[k - (plane << wshift)] = word;
+      }
+    }
     __syncthreads();
   }
-}
-
-// scale_lut of grain.rs:166-177 (`lut` in shared memory).
-__device__ __forceinline__ int grain_scale(const int16_t* lut, int index, int sh) {
-  const int x = index >> sh;
-  const int rem = index - (x << sh);
-  if (sh == 0 || x == 255) return lut[x];
-  const int start = lut[x], end = lut[x + 1];
-  return start + round2((end - start) * rem, sh);
 }
 
 // Per-item constants of the output stage, held in registers: the stores to
@@ -365,22 +441,25 @@ __device__ __forceinline__ int hblend(int old, int g, int j, int psx, int gmin, 
 // luma sits at x << PSX, y << PSY), and the sample width — so the per-sample
 // work has no run-time plane selects.
 template <bool CHROMA, int PSX, int PSY, int SB>
-__device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T, const int16_t* lut,
-                                           const uint8_t* offs_cur, const uint8_t* offs_prev, int x0, int x1,
-                                           int ys, int ye, int stripe, int b0, bool grain) {
+__device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T, const uint8_t* scale,
+                                           const uint8_t* offs_cur, const uint8_t* offs_prev, const uint8_t* ssrc,
+                                           const uint8_t* sluma, int x0, int x1, int ys, int ye, int stripe, int b0,
+                                           bool grain) {
   const int ngroups = (x1 - x0 + 7) >> 3;  // 8-sample groups per row (<= 32)
   const int sh = P.bd - 8;
   constexpr int bshift = 5 - PSX;  // grain block width 32 >> psx
   constexpr int sshift = 5 - PSY;  // noise stripe height 32 >> psy
-      for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
+  for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
     const int gx = k & 31, r = k >> 5;
     if (gx >= ngroups) continue;
     const int yy = ys + r;
     const int xs = x0 + gx * 8;
     const int n = min(8, x1 - xs);
     int v[8];
-    const uint8_t* sp = P.src + int64_t(yy) * P.src_pitch + int64_t(xs) * SB;
-    const bool vec = n == 8 && (reinterpret_cast<uintptr_t>(sp) & (8 * SB - 1)) == 0;
+    // the stripe's rows are staged (kStageSrc bytes a row, from column x0):
+    // the group's 8 samples start 8 * SB-aligned
+    const uint8_t* sp = ssrc + r * kStageSrc + gx * 8 * SB;
+    const bool vec = n == 8;
     if (vec && SB == 2) {
       const uint4 q = *reinterpret_cast<const uint4*>(sp);
       v[0] = q.x & 0xffff; v[1] = q.x >> 16; v[2] = q.y & 0xffff; v[3] = q.y >> 16;
@@ -406,14 +485,14 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
       const bool vblend = P.overlap && stripe > 0 && i < (PSY ? 1 : 2);
       int lum[8];
       if (CHROMA) {
-        // un-grained luma under each chroma sample (grain.rs:303-314)
-        const int ly = yy << PSY;
-        const uint8_t* lrow = P.luma + int64_t(ly) * P.luma_pitch;
-        const int lx0 = xs << PSX;
-        const uint8_t* lp = lrow + int64_t(lx0) * SB;
+        // un-grained luma under each chroma sample (grain.rs:303-314), from
+        // the staged luma row (kStageLuma bytes, from luma column x0 << PSX)
+        const uint8_t* lrow = sluma + r * kStageLuma;
+        const int lx0 = xs << PSX, lbase = x0 << PSX;
+        const uint8_t* lp = lrow + (lx0 - lbase) * SB;
         // the group's whole luma span (8 or 16 samples, no edge clamp
         // inside it) in 8-byte loads
-        if (n == 8 && lx0 + (8 << PSX) <= P.w && (reinterpret_cast<uintptr_t>(lp) & 7) == 0) {
+        if (n == 8 && lx0 + (8 << PSX) <= P.w) {
           uint32_t wv[8];
           const int nw = (8 << PSX) * SB / 4;  // 32-bit words: 2, 4 or 8
 #pragma unroll
@@ -433,9 +512,10 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
         } else {
 #pragma unroll
           for (int e = 0; e < 8; e++) {
+            lum[e] = 0;  // (samples past the row's end: a valid table index, not stored)
             if (e < n) {
-              const int lx = (xs + e) << PSX;
-              const int lnx = min(lx + 1, P.w - 1);
+              const int lx = ((xs + e) << PSX) - lbase;
+              const int lnx = min(lx + 1, P.w - 1 - lbase);
               const int l0 = SB == 1 ? int(lrow[lx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lx]);
               const int l1 = SB == 1 ? int(lrow[lnx]) : int(reinterpret_cast<const uint16_t*>(lrow)[lnx]);
               lum[e] = PSX ? round2(l0 + l1, 1) : l0;
@@ -447,35 +527,40 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
       // grain block, so the template positions are found once; only a
       // block's first 1-2 columns blend with the block to the left, and
       // only a stripe's first 1-2 rows with the stripe above
-      const int nh = (P.overlap && b > 0 && jb == 0) ? (PSX ? 1 : 2) : 0;
+      const bool hb = P.overlap && b > 0 && jb == 0;
       const int16_t* tp = tmpl_at(T, PSX, PSY, i, offs_cur[li]) + jb;
-      const int16_t* tl = left_at(T, PSX, PSY, i, offs_cur[li - 1]);
-      const int vrow = i + (32 >> PSY);
-      const int16_t* vp = tmpl_at(T, PSX, PSY, vrow, offs_prev[li]) + jb;
-      const int16_t* vl = left_at(T, PSX, PSY, vrow, offs_prev[li - 1]);
+      int noise[8];
+#pragma unroll
+      for (int e = 0; e < 8; e++) noise[e] = tp[e];  // (all 8 inside the template row)
+      if (hb) {
+        const int16_t* tl = left_at(T, PSX, PSY, i, offs_cur[li - 1]);
+        noise[0] = hblend(tl[0], noise[0], 0, PSX, P.gmin, P.gmax);
+        if (!PSX) noise[1] = hblend(tl[1], noise[1], 1, PSX, P.gmin, P.gmax);
+      }
+      if (vblend) {
+        const int vrow = i + (32 >> PSY);
+        const int16_t* vp = tmpl_at(T, PSX, PSY, vrow, offs_prev[li]) + jb;
+        int old[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) old[e] = vp[e];
+        if (hb) {
+          const int16_t* vl = left_at(T, PSX, PSY, vrow, offs_prev[li - 1]);
+          old[0] = hblend(vl[0], old[0], 0, PSX, P.gmin, P.gmax);
+          if (!PSX) old[1] = hblend(vl[1], old[1], 1, PSX, P.gmin, P.gmax);
+        }
+        const int wo = PSY ? 23 : (i == 0 ? 27 : 17), wn = PSY ? 22 : (i == 0 ? 17 : 27);
+#pragma unroll
+        for (int e = 0; e < 8; e++) noise[e] = clip3(P.gmin, P.gmax, round2(old[e] * wo + noise[e] * wn, 5));
+      }
+      // scaling (grain.rs:166-177 through the full-resolution table), then
+      // the sample plus scaled noise, clipped (grain.rs:316-350)
+      const int lm = P.lmult - 128, m = P.mult - 128, ov = (P.offs - 256) * (1 << sh);
 #pragma unroll
       for (int e = 0; e < 8; e++) {
-        if (e >= n) continue;
-        int noise = tp[e];
-        if (e < nh) noise = hblend(tl[e], noise, e, PSX, P.gmin, P.gmax);
-        if (vblend) {
-          int old = vp[e];
-          if (e < nh) old = hblend(vl[e], old, e, PSX, P.gmin, P.gmax);
-          const int g2 = PSY ? old * 23 + noise * 22 : (i == 0 ? old * 27 + noise * 17 : old * 17 + noise * 27);
-          noise = clip3(P.gmin, P.gmax, round2(g2, 5));
-        }
         const int orig = v[e];
         int idx = orig;
-        if (CHROMA) {
-          if (P.csfl) {
-            idx = lum[e];
-          } else {
-            const int combined = lum[e] * (P.lmult - 128) + orig * (P.mult - 128);
-            idx = clip3(0, P.maxpix, (combined >> 6) + ((P.offs - 256) * (1 << sh)));
-          }
-        }
-        noise = round2(grain_scale(lut, idx, sh) * noise, P.scaling_shift);
-        v[e] = clip3(P.min_value, P.max_v, orig + noise);
+        if (CHROMA) idx = P.csfl ? lum[e] : clip3(0, P.maxpix, ((lum[e] * lm + orig * m) >> 6) + ov);
+        v[e] = clip3(P.min_value, P.max_v, orig + round2(int(scale[idx]) * noise[e], P.scaling_shift));
       }
     }
     // pack (frame.rs:153-158): u8 at 8-bit, little-endian u16 above
@@ -510,18 +595,57 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
   }
 }
 
+// Copies `rows` rows of `len` bytes, `pitch` bytes apart in global memory,
+// to shared memory at `dst` (rows `stride` bytes apart, 16-byte aligned):
+// 16-byte asynchronous copies where the source is 16-byte aligned, byte
+// copies for the rest (a row's ragged end, or rows of an unaligned pitch).
+// The caller waits for the copies (cp.async.wait_all) and then the CTA's
+// barrier.
+__device__ __forceinline__ void stage_rows(uint8_t* dst, int stride, const uint8_t* src, int64_t pitch, int rows,
+                                           int len) {
+  const int chunks = (len + 15) >> 4;
+  const uint32_t d0 = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  for (int k = threadIdx.x; k < rows * chunks; k += blockDim.x) {
+    const int r = k / chunks, j = k - r * chunks;
+    const uint8_t* g = src + int64_t(r) * pitch + 16 * j;
+    const int nb = min(16, len - 16 * j);
+    if (nb == 16 && (reinterpret_cast<uintptr_t>(g) & 15) == 0) {
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + uint32_t(r * stride + 16 * j)), "l"(g)
+                   : "memory");
+    } else {
+      for (int b = 0; b < nb; b++) dst[r * stride + 16 * j + b] = g[b];
+    }
+  }
+}
+
+// Dynamic shared memory of the output kernel: the plane's template and
+// scaling table, the stripe's block offsets, and the stripe's source rows
+// (up to 32 rows of 256 samples) with, for chroma, the luma row under each
+// (up to 512 luma samples: 256 chroma columns at 2:1).
+struct OutSmem {
+  int16_t T[kTH * kTW + 2];  // (+2: the staged rows below start 16-byte aligned)
+  __align__(16) uint8_t scale[4096];
+  uint8_t offs_cur[kOutOffs + 6], offs_prev[kOutOffs + 6];  // block offsets of stripes s and s-1, blocks b0-1 ..
+  __align__(16) uint8_t src[32 * kStageSrc];
+  __align__(16) uint8_t luma[32 * kStageLuma];
+};
+constexpr int kOutSmem = int(sizeof(OutSmem));
+
 // Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
 // 256 (so of the grain block width). A CTA works through a contiguous run of
-// items. The rows are taken one noise stripe
-// (32 rows, 16 for vertically subsampled chroma) at a time, with the
-// stripe's block offsets staged in shared memory; 256 threads, 8 consecutive
-// samples (one grain block) per thread per step.
+// items. The rows are taken one noise stripe (32 rows, 16 for vertically
+// subsampled chroma) at a time: the stripe's source rows, the luma rows a
+// chroma stripe reads and the stripe's block offsets are brought into
+// shared memory together (all in flight at once), then 256 threads take 8
+// consecutive samples (one grain block) each per step.
 __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restrict__ frames,
                                                      const Item* __restrict__ items, int n_items) {
-  __shared__ __align__(16) int16_t T[kTH * kTW];
-  __shared__ int16_t lut[256];
-  // block offsets of stripes s and s-1, blocks b0-1 .. b0+16
-  __shared__ uint8_t offs_cur[kOutOffs], offs_prev[kOutOffs];
+  extern __shared__ __align__(16) uint8_t out_smem[];
+  OutSmem& sm = *reinterpret_cast<OutSmem*>(out_smem);
+  int16_t* T = sm.T;
+  uint8_t* scale = sm.scale;
+  uint8_t* offs_cur = sm.offs_cur;
+  uint8_t* offs_prev = sm.offs_prev;
   int loaded = -1;  // frame * 4 + plane whose template is in T
   pdl_wait();  // the previous stage's output is complete past this point
   // a CTA takes a contiguous run of items, the runs split as evenly as the
@@ -578,17 +702,17 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
         const int key = int(item.frame) * 4 + p;
         if (key != loaded) {  // the plane's template and scaling table
           __syncthreads();
-          // the template goes to shared memory as asynchronous copies, all
-          // in flight at once (a thread's 12 words would otherwise wait
-          // for each other's loads); the barrier before the stripe's
-          // samples follows the wait
+          // asynchronous copies, waited for with the stripe's rows below
           const uint32_t* tg = reinterpret_cast<const uint32_t*>(&f.grain->tmpl[p][0][0]);
           const uint32_t tbase = static_cast<uint32_t>(__cvta_generic_to_shared(T));
           for (int k = threadIdx.x; k < kTH * kTW / 2; k += 256)
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tbase + 4u * uint32_t(k)), "l"(tg + k)
                          : "memory");
-          for (int k = threadIdx.x; k < 256; k += 256) lut[k] = f.grain->lut[p][k];
-          asm volatile("cp.async.wait_all;" ::: "memory");
+          const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(scale));
+          for (int k = threadIdx.x; k < (1 << bd) / 16; k += 256)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sbase + 16u * uint32_t(k)),
+                         "l"(&f.grain->scale[p][16 * k])
+                         : "memory");
           loaded = key;
         }
       }
@@ -597,36 +721,51 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
     const int bshift = 5 - P.psx;  // grain block width 32 >> psx
     const int sshift = 5 - P.psy;  // noise stripe height 32 >> psy
     const int b0 = x0 >> bshift;
+    const bool luma_rows = item.plane != 0 && P.grain;
     for (int ys = item.y0; ys < int(item.y1);) {
       const int stripe = ys >> sshift;
       const int ye = min(int(item.y1), (stripe + 1) << sshift);
+      // the stripe's source rows; for chroma the luma row under each chroma
+      // row, columns x0 << psx up to the luma width
+      stage_rows(sm.src, kStageSrc, P.src + int64_t(ys) * P.src_pitch + int64_t(x0) * P.sb, P.src_pitch, ye - ys,
+                 (x1 - x0) * P.sb);
+      if (luma_rows)
+        stage_rows(sm.luma, kStageLuma, P.luma + (int64_t(ys) << P.psy) * P.luma_pitch + (int64_t(x0) << P.psx) * P.sb,
+                   P.luma_pitch << P.psy, ye - ys, (min(x1 << P.psx, P.w) - (x0 << P.psx)) * P.sb);
       if (P.grain && threadIdx.x < kOutOffs) {
         const int b = b0 - 1 + int(threadIdx.x);
         const bool ok = b >= 0 && b < P.nb;
         offs_cur[threadIdx.x] = ok ? P.off[int64_t(stripe) * P.nb + b] : 0;
         offs_prev[threadIdx.x] = ok && stripe > 0 ? P.off[int64_t(stripe - 1) * P.nb + b] : 0;
       }
+      asm volatile("cp.async.wait_all;" ::: "memory");
       __syncthreads();
+      const uint8_t* ss = sm.src;
+      const uint8_t* sl = sm.luma;
       if (item.plane == 0) {
         if (P.sb == 2)
-          out_stripe<false, 0, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain);
+          out_stripe<false, 0, 0, 2>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain);
         else
-          out_stripe<false, 0, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain);
+          out_stripe<false, 0, 0, 1>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain);
       } else {
         const int k3 = (P.psx ? 2 : 0) + (P.psy ? 1 : 0) + (P.sb == 2 ? 4 : 0);
         switch (k3) {
-          case 0: out_stripe<true, 0, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
-          case 2: out_stripe<true, 1, 0, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
-          case 3: out_stripe<true, 1, 1, 1>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
-          case 4: out_stripe<true, 0, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
-          case 6: out_stripe<true, 1, 0, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
-          default: out_stripe<true, 1, 1, 2>(P, T, lut, offs_cur, offs_prev, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 0: out_stripe<true, 0, 0, 1>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 2: out_stripe<true, 1, 0, 1>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 3: out_stripe<true, 1, 1, 1>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 4: out_stripe<true, 0, 0, 2>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          case 6: out_stripe<true, 1, 0, 2>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
+          default: out_stripe<true, 1, 1, 2>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain); break;
         }
       }
       __syncthreads();
       ys = ye;
     }
   }
+}
+
+cudaError_t output_init() {
+  return cudaFuncSetAttribute(output_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kOutSmem);
 }
 
 void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
@@ -637,7 +776,7 @@ void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, 
 void launch_output(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
   if (n_items <= 0) return;
   // one resident wave (2 CTAs per SM), each CTA a contiguous run of items
-  launch_pdl(output_kernel, min(n_items, kNumSMs * 2), 256, 0, s, frames, items, n_items);
+  launch_pdl(output_kernel, min(n_items, kNumSMs * 2), 256, size_t(kOutSmem), s, frames, items, n_items);
 }
 
 }  // namespace av1pf

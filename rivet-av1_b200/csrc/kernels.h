@@ -115,6 +115,8 @@ cudaError_t superres_init();
 void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
 // Sets lr_kernel's dynamic shared-memory limit on the current device.
 cudaError_t lr_init();
+// Opts the output kernel into its dynamic shared memory (once per device).
+cudaError_t output_init();
 
 // Film grain + output packing (grain.cu)
 void launch_grain_prep(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);

@@ -71,11 +71,12 @@ bool current_context_id(unsigned long long* id) {
   return get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, id) == CUDA_SUCCESS;
 }
 
-// With the device current: look up the scratch's device address and upload
-// the film-grain RNG jump tables, once per device context. After a
-// cudaDeviceReset the device's next context loads the module again (the
-// array at a possibly new address, the tables zeroed): that context has a
-// new ID, so the lookup and upload run again.
+// With the device current: look up the scratch's device address, upload
+// the film-grain RNG jump tables and give the output kernel its shared
+// memory, once per device context. After a cudaDeviceReset the device's
+// next context loads the module again (the array at a possibly new address,
+// the tables zeroed, the kernel attribute unset): that context has a new ID,
+// so the lookup, upload and attribute run again.
 int setup(int device, uint8_t** out) {
   if (device < 0 || device >= 64) {
     set_error("av1pf_output_noalloc: device index out of range");
@@ -91,6 +92,8 @@ int setup(int device, uint8_t** out) {
   if (g_scratch_ptr[device] != p || (have_id && g_ctx_id[device] != id)) {
     e = upload_grain_tables();
     if (e != cudaSuccess) return cuda_status(e, "av1pf_output_noalloc: grain tables");
+    e = output_init();
+    if (e != cudaSuccess) return cuda_status(e, "av1pf_output_noalloc: output kernel attributes");
     g_scratch_ptr[device] = static_cast<uint8_t*>(p);
     g_ctx_id[device] = have_id ? id : 0;
   }
