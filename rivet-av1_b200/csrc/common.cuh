@@ -41,6 +41,46 @@ extern __device__ uint32_t g_error_flags;
 enum : uint32_t { ERRF_BAD_MAP = 1u, ERRF_BAD_ITEM = 2u, ERRF_STALL = 4u };
 
 // ---------------------------------------------------------------------------
+// One-dimensional bulk copies (TMA) into this CTA's shared memory, completing
+// on an mbarrier. Source and destination 16-byte aligned, size a multiple of
+// 16. No multicast.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  // the initialisation is visible to the bulk copies' completions
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// One arrival that also expects `bytes` of copies on the current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Waits for the phase of parity `phase` to complete: each try suspends the
+// thread for up to about a microsecond; after `limit` tries the wait gives up
+// and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int limit) {
+  for (int k = 0; k < limit; k++) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(1000u)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
 // Integer helpers (consts.rs:328-368, bits.rs:112)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int32_t round2(int32_t x, int n) {  // 0 <= n <= 30

@@ -17,8 +17,11 @@ struct DPlane {
 };
 
 // Film-grain scratch of one frame (filled by the template kernel).
+constexpr int kTmplStride = 5992;  // 73 * 82 = 5986 samples, padded
 struct GrainScratch {
-  int16_t tmpl[3][73][82];  // luma, cb, cr grain templates (7.18.3.3)
+  // luma, cb, cr grain templates (7.18.3.3): 73 rows of 82, each plane
+  // padded to a multiple of 16 bytes so that it moves as one bulk copy
+  alignas(16) int16_t tmpl[3][kTmplStride];
   // the scaling function (7.18.3.4) at every sample value 0 .. 2^bitdepth - 1:
   // the 256-entry lookup, interpolated between entries above 8 bits
   alignas(16) uint8_t scale[3][4096];

@@ -376,8 +376,15 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
     }
     __syncthreads();
     GrainScratch* gs = f.grain;
-    for (int k = tid; k < 3 * kTH * kTW / 2; k += 256)
-      reinterpret_cast<uint32_t*>(&gs->tmpl[0][0][0])[k] = reinterpret_cast<const uint32_t*>(&T[0][0][0])[k];
+    {
+      // each plane's template, its padding zeroed
+      constexpr int kPlaneWords = kTmplStride / 2, kTmplWords = kTH * kTW / 2;
+      for (int k = tid; k < 3 * kPlaneWords; k += 256) {
+        const int p = k / kPlaneWords, w = k - p * kPlaneWords;
+        reinterpret_cast<uint32_t*>(&gs->tmpl[p][0])[w] =
+            w < kTmplWords ? reinterpret_cast<const uint32_t*>(&T[p][0][0])[w] : 0u;
+      }
+    }
     // the scaling function at every sample value (scale_lut of
     // grain.rs:166-177: above 8 bits, interpolated between the two entries
     // around index >> (bitdepth - 8)), four values per 32-bit store
@@ -445,16 +452,28 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
                                            const uint8_t* offs_cur, const uint8_t* offs_prev, const uint8_t* ssrc,
                                            const uint8_t* sluma, int x0, int x1, int ys, int ye, int stripe, int b0,
                                            bool grain) {
+  // a lane keeps one 8-sample column group (one grain block's) on every
+  // row it takes: the block, its template columns and the luma span are
+  // found once
   const int ngroups = (x1 - x0 + 7) >> 3;  // 8-sample groups per row (<= 32)
+  const int gx = threadIdx.x & 31;
+  if (gx >= ngroups) return;
   const int sh = P.bd - 8;
   constexpr int bshift = 5 - PSX;  // grain block width 32 >> psx
   constexpr int sshift = 5 - PSY;  // noise stripe height 32 >> psy
-  for (int k = threadIdx.x; k < (ye - ys) * 32; k += 256) {
-    const int gx = k & 31, r = k >> 5;
-    if (gx >= ngroups) continue;
+  const int xs = x0 + gx * 8;
+  const int n = min(8, x1 - xs);
+  const int b = xs >> bshift;
+  const int jb = xs - (b << bshift);
+  const int li = b - b0 + 1;  // index into the staged offsets
+  const bool hb = P.overlap && b > 0 && jb == 0;  // the block's first columns blend with the one to its left
+  const int16_t* tp0 = tmpl_at(T, PSX, PSY, 0, offs_cur[li]) + jb;
+  const int16_t* tl0 = left_at(T, PSX, PSY, 0, offs_cur[li - 1]);
+  const int lx0 = xs << PSX, lbase = x0 << PSX;
+  const bool lvec = n == 8 && lx0 + (8 << PSX) <= P.w;  // the luma span needs no edge clamp
+  const int lm = P.lmult - 128, m = P.mult - 128, ov = (P.offs - 256) * (1 << sh);
+  for (int r = threadIdx.x >> 5; r < ye - ys; r += 8) {
     const int yy = ys + r;
-    const int xs = x0 + gx * 8;
-    const int n = min(8, x1 - xs);
     int v[8];
     // the stripe's rows are staged (kStageSrc bytes a row, from column x0):
     // the group's 8 samples start 8 * SB-aligned
@@ -479,20 +498,15 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
     if (grain) {
       // noise image (grain.rs:251-283); the 8 samples share one grain block
       const int i = yy - (stripe << sshift);
-      const int b = xs >> bshift;
-      const int jb = xs - (b << bshift);
-      const int li = b - b0 + 1;  // index into the staged offsets
       const bool vblend = P.overlap && stripe > 0 && i < (PSY ? 1 : 2);
       int lum[8];
       if (CHROMA) {
         // un-grained luma under each chroma sample (grain.rs:303-314), from
         // the staged luma row (kStageLuma bytes, from luma column x0 << PSX)
         const uint8_t* lrow = sluma + r * kStageLuma;
-        const int lx0 = xs << PSX, lbase = x0 << PSX;
         const uint8_t* lp = lrow + (lx0 - lbase) * SB;
-        // the group's whole luma span (8 or 16 samples, no edge clamp
-        // inside it) in 8-byte loads
-        if (n == 8 && lx0 + (8 << PSX) <= P.w) {
+        // the group's whole luma span (8 or 16 samples) in 8-byte loads
+        if (lvec) {
           uint32_t wv[8];
           const int nw = (8 << PSX) * SB / 4;  // 32-bit words: 2, 4 or 8
 #pragma unroll
@@ -523,43 +537,41 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
           }
         }
       }
-      // the group's noise (grain.rs:200-283): its 8 samples lie in one
-      // grain block, so the template positions are found once; only a
-      // block's first 1-2 columns blend with the block to the left, and
-      // only a stripe's first 1-2 rows with the stripe above
-      const bool hb = P.overlap && b > 0 && jb == 0;
-      const int16_t* tp = tmpl_at(T, PSX, PSY, i, offs_cur[li]) + jb;
+      // the group's noise (grain.rs:200-283): only a block's first 1-2
+      // columns blend with the block to the left, and only a stripe's first
+      // 1-2 rows with the stripe above
+      const int16_t* tp = tp0 + i * kTW;
       int noise[8];
 #pragma unroll
       for (int e = 0; e < 8; e++) noise[e] = tp[e];  // (all 8 inside the template row)
-      if (hb) {
-        const int16_t* tl = left_at(T, PSX, PSY, i, offs_cur[li - 1]);
-        noise[0] = hblend(tl[0], noise[0], 0, PSX, P.gmin, P.gmax);
-        if (!PSX) noise[1] = hblend(tl[1], noise[1], 1, PSX, P.gmin, P.gmax);
-      }
+      // (the blend is computed for every group and kept where it applies:
+      // the block to the left's columns are inside the template)
+      const int16_t* tl = tl0 + i * kTW;
+      noise[0] = hb ? hblend(tl[0], noise[0], 0, PSX, P.gmin, P.gmax) : noise[0];
+      if (!PSX) noise[1] = hb ? hblend(tl[1], noise[1], 1, PSX, P.gmin, P.gmax) : noise[1];
       if (vblend) {
         const int vrow = i + (32 >> PSY);
         const int16_t* vp = tmpl_at(T, PSX, PSY, vrow, offs_prev[li]) + jb;
         int old[8];
 #pragma unroll
         for (int e = 0; e < 8; e++) old[e] = vp[e];
-        if (hb) {
-          const int16_t* vl = left_at(T, PSX, PSY, vrow, offs_prev[li - 1]);
-          old[0] = hblend(vl[0], old[0], 0, PSX, P.gmin, P.gmax);
-          if (!PSX) old[1] = hblend(vl[1], old[1], 1, PSX, P.gmin, P.gmax);
-        }
+        const int16_t* vl = left_at(T, PSX, PSY, vrow, offs_prev[li - 1]);
+        old[0] = hb ? hblend(vl[0], old[0], 0, PSX, P.gmin, P.gmax) : old[0];
+        if (!PSX) old[1] = hb ? hblend(vl[1], old[1], 1, PSX, P.gmin, P.gmax) : old[1];
         const int wo = PSY ? 23 : (i == 0 ? 27 : 17), wn = PSY ? 22 : (i == 0 ? 17 : 27);
 #pragma unroll
         for (int e = 0; e < 8; e++) noise[e] = clip3(P.gmin, P.gmax, round2(old[e] * wo + noise[e] * wn, 5));
       }
       // scaling (grain.rs:166-177 through the full-resolution table), then
       // the sample plus scaled noise, clipped (grain.rs:316-350)
-      const int lm = P.lmult - 128, m = P.mult - 128, ov = (P.offs - 256) * (1 << sh);
 #pragma unroll
       for (int e = 0; e < 8; e++) {
         const int orig = v[e];
         int idx = orig;
-        if (CHROMA) idx = P.csfl ? lum[e] : clip3(0, P.maxpix, ((lum[e] * lm + orig * m) >> 6) + ov);
+        if (CHROMA) {
+          const int mixed = clip3(0, P.maxpix, ((lum[e] * lm + orig * m) >> 6) + ov);
+          idx = P.csfl ? lum[e] : mixed;
+        }
         v[e] = clip3(P.min_value, P.max_v, orig + round2(int(scale[idx]) * noise[e], P.scaling_shift));
       }
     }
@@ -595,49 +607,45 @@ __device__ __forceinline__ void out_stripe(const OutParams& P, const int16_t* T,
   }
 }
 
-// Copies `rows` rows of `len` bytes, `pitch` bytes apart in global memory,
-// to shared memory at `dst` (rows `stride` bytes apart, 16-byte aligned):
-// 16-byte asynchronous copies where the source is 16-byte aligned, byte
-// copies for the rest (a row's ragged end, or rows of an unaligned pitch).
-// The caller waits for the copies (cp.async.wait_all) and then the CTA's
-// barrier.
-__device__ __forceinline__ void stage_rows(uint8_t* dst, int stride, const uint8_t* src, int64_t pitch, int rows,
-                                           int len) {
-  const int chunks = (len + 15) >> 4;
-  const uint32_t d0 = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-  for (int k = threadIdx.x; k < rows * chunks; k += blockDim.x) {
-    const int r = k / chunks, j = k - r * chunks;
-    const uint8_t* g = src + int64_t(r) * pitch + 16 * j;
-    const int nb = min(16, len - 16 * j);
-    if (nb == 16 && (reinterpret_cast<uintptr_t>(g) & 15) == 0) {
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + uint32_t(r * stride + 16 * j)), "l"(g)
-                   : "memory");
-    } else {
-      for (int b = 0; b < nb; b++) dst[r * stride + 16 * j + b] = g[b];
-    }
+// Copies bytes [from, len) of `rows` rows, `pitch` bytes apart in global
+// memory, to shared memory at `dst` (rows `stride` bytes apart), a warp per
+// row: the part of a stripe's rows that the bulk copies do not move (a
+// row's last len % 16 bytes, or whole rows of an unaligned plane).
+__device__ __forceinline__ void copy_rows(uint8_t* dst, int stride, const uint8_t* src, int64_t pitch, int rows,
+                                          int from, int len) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = warp; r < rows; r += 8) {
+    const uint8_t* g = src + int64_t(r) * pitch;
+    uint8_t* d = dst + r * stride;
+    for (int b = from + lane; b < len; b += 32) d[b] = g[b];
   }
 }
 
-// Dynamic shared memory of the output kernel: the plane's template and
-// scaling table, the stripe's block offsets, and the stripe's source rows
-// (up to 32 rows of 256 samples) with, for chroma, the luma row under each
-// (up to 512 luma samples: 256 chroma columns at 2:1).
+// Dynamic shared memory of the output kernel: the bulk copies' barrier, the
+// frame's descriptor, the plane's template and scaling table, the stripe's
+// block offsets, and the stripe's source rows (up to 32 rows of 256
+// samples) with, for chroma, the luma row under each (up to 512 luma
+// samples: 256 chroma columns at 2:1).
 struct OutSmem {
-  int16_t T[kTH * kTW + 2];  // (+2: the staged rows below start 16-byte aligned)
-  __align__(16) uint8_t scale[4096];
+  uint64_t bar;
+  FrameDesc fd;
+  alignas(16) int16_t T[kTmplStride];
+  alignas(16) uint8_t scale[4096];
   uint8_t offs_cur[kOutOffs + 6], offs_prev[kOutOffs + 6];  // block offsets of stripes s and s-1, blocks b0-1 ..
-  __align__(16) uint8_t src[32 * kStageSrc];
-  __align__(16) uint8_t luma[32 * kStageLuma];
+  alignas(16) uint8_t src[32 * kStageSrc];
+  alignas(16) uint8_t luma[32 * kStageLuma];
 };
 constexpr int kOutSmem = int(sizeof(OutSmem));
+constexpr int kOutWaitLimit = 1 << 16;  // bulk-copy waits of about 1 us each before ERRF_STALL
 
 // Item: rows y0..y1 of a plane by up to 256 columns from x0, a multiple of
 // 256 (so of the grain block width). A CTA works through a contiguous run of
 // items. The rows are taken one noise stripe (32 rows, 16 for vertically
-// subsampled chroma) at a time: the stripe's source rows, the luma rows a
-// chroma stripe reads and the stripe's block offsets are brought into
-// shared memory together (all in flight at once), then 256 threads take 8
-// consecutive samples (one grain block) each per step.
+// subsampled chroma) at a time: the stripe's source rows and the luma rows a
+// chroma stripe reads come into shared memory as one bulk copy per row (and
+// a new plane's template and scaling table as two more), all completing on
+// one barrier, while 18 threads fetch the stripe's block offsets; then 256
+// threads take 8 consecutive samples (one grain block) each per row.
 __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restrict__ frames,
                                                      const Item* __restrict__ items, int n_items) {
   extern __shared__ __align__(16) uint8_t out_smem[];
@@ -646,19 +654,44 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
   uint8_t* scale = sm.scale;
   uint8_t* offs_cur = sm.offs_cur;
   uint8_t* offs_prev = sm.offs_prev;
-  int loaded = -1;  // frame * 4 + plane whose template is in T
-  pdl_wait();  // the previous stage's output is complete past this point
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) mbar_init(&sm.bar, 1);
+  uint32_t phase = 0;     // parity of the barrier's current phase
+  int loaded = -1;        // frame * 4 + plane whose template is in T
+  int loaded_frame = -1;  // the frame whose descriptor is in sm.fd
   // a CTA takes a contiguous run of items, the runs split as evenly as the
   // count allows: the items of a plane are consecutive, so a CTA stages that
   // plane's template once for its whole run
   const int it_begin = int(int64_t(blockIdx.x) * n_items / gridDim.x);
   const int it_end = int(int64_t(blockIdx.x + 1) * n_items / gridDim.x);
+  if (it_begin < it_end) {
+    // the first item's descriptor: copied from the host before any kernel
+    // of the call ran, so it is fetched before waiting for the previous
+    // stage (whose output, and the film-grain tables, are read only after)
+    const Item first = items[it_begin];
+    const uint2* fs = reinterpret_cast<const uint2*>(&frames[first.frame]);
+    uint2* fdst = reinterpret_cast<uint2*>(&sm.fd);
+    for (int k = tid; k < int(sizeof(FrameDesc) / 8); k += 256) fdst[k] = fs[k];
+    loaded_frame = first.frame;
+  }
+  __syncthreads();  // (also publishes the barrier's initialisation)
+  pdl_wait();  // the previous stage's output is complete past this point
   for (int it = it_begin; it < it_end; it++) {
     const Item item = items[it];
+    if (int(item.frame) != loaded_frame) {
+      // the descriptor's fields are read by every thread: from shared memory
+      // (the previous stripe ended with a barrier, so no thread reads it now)
+      const uint2* fs = reinterpret_cast<const uint2*>(&frames[item.frame]);
+      uint2* fdst = reinterpret_cast<uint2*>(&sm.fd);
+      for (int k = tid; k < int(sizeof(FrameDesc) / 8); k += 256) fdst[k] = fs[k];
+      __syncthreads();
+      loaded_frame = item.frame;
+    }
     OutParams P;
+    bool new_tables = false;  // the plane's template and table to fetch with the first stripe
+    const FrameDesc& f = sm.fd;
+    const int p = item.plane;
     {
-      const FrameDesc& f = frames[item.frame];
-      const int p = item.plane;
       P.bd = f.bd;
       P.sb = f.sb;
       P.psx = plane_ssx(f, p);
@@ -700,49 +733,62 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
         P.lmult = p == 1 ? g.cb_luma_mult : g.cr_luma_mult;
         P.offs = p == 1 ? g.cb_offset : g.cr_offset;
         const int key = int(item.frame) * 4 + p;
-        if (key != loaded) {  // the plane's template and scaling table
-          __syncthreads();
-          // asynchronous copies, waited for with the stripe's rows below
-          const uint32_t* tg = reinterpret_cast<const uint32_t*>(&f.grain->tmpl[p][0][0]);
-          const uint32_t tbase = static_cast<uint32_t>(__cvta_generic_to_shared(T));
-          for (int k = threadIdx.x; k < kTH * kTW / 2; k += 256)
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tbase + 4u * uint32_t(k)), "l"(tg + k)
-                         : "memory");
-          const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(scale));
-          for (int k = threadIdx.x; k < (1 << bd) / 16; k += 256)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sbase + 16u * uint32_t(k)),
-                         "l"(&f.grain->scale[p][16 * k])
-                         : "memory");
-          loaded = key;
-        }
+        new_tables = key != loaded;
+        loaded = key;
       }
     }
     const int x0 = item.x0, x1 = item.x1;
     const int bshift = 5 - P.psx;  // grain block width 32 >> psx
     const int sshift = 5 - P.psy;  // noise stripe height 32 >> psy
     const int b0 = x0 >> bshift;
-    const bool luma_rows = item.plane != 0 && P.grain;
+    const bool luma_rows = p != 0 && P.grain;
+    // the stripe's rows in global memory, and how much of each a bulk copy
+    // moves (whole 16-byte units, when the plane's rows are 16-byte aligned)
+    const uint8_t* s_src = P.src + int64_t(x0) * P.sb;
+    const int s_len = (x1 - x0) * P.sb;
+    const int s_bulk = ((reinterpret_cast<uintptr_t>(s_src) | uintptr_t(P.src_pitch)) & 15) == 0 ? s_len & ~15 : 0;
+    const int64_t l_pitch = P.luma_pitch << P.psy;
+    const uint8_t* l_src = P.luma + (int64_t(x0) << P.psx) * P.sb;
+    const int l_len = (min(x1 << P.psx, P.w) - (x0 << P.psx)) * P.sb;
+    const int l_bulk =
+        luma_rows && ((reinterpret_cast<uintptr_t>(l_src) | uintptr_t(l_pitch)) & 15) == 0 ? l_len & ~15 : 0;
     for (int ys = item.y0; ys < int(item.y1);) {
       const int stripe = ys >> sshift;
       const int ye = min(int(item.y1), (stripe + 1) << sshift);
-      // the stripe's source rows; for chroma the luma row under each chroma
-      // row, columns x0 << psx up to the luma width
-      stage_rows(sm.src, kStageSrc, P.src + int64_t(ys) * P.src_pitch + int64_t(x0) * P.sb, P.src_pitch, ye - ys,
-                 (x1 - x0) * P.sb);
-      if (luma_rows)
-        stage_rows(sm.luma, kStageLuma, P.luma + (int64_t(ys) << P.psy) * P.luma_pitch + (int64_t(x0) << P.psx) * P.sb,
-                   P.luma_pitch << P.psy, ye - ys, (min(x1 << P.psx, P.w) - (x0 << P.psx)) * P.sb);
-      if (P.grain && threadIdx.x < kOutOffs) {
-        const int b = b0 - 1 + int(threadIdx.x);
-        const bool ok = b >= 0 && b < P.nb;
-        offs_cur[threadIdx.x] = ok ? P.off[int64_t(stripe) * P.nb + b] : 0;
-        offs_prev[threadIdx.x] = ok && stripe > 0 ? P.off[int64_t(stripe - 1) * P.nb + b] : 0;
+      const int rows = ye - ys;
+      const uint8_t* srow = s_src + int64_t(ys) * P.src_pitch;
+      const uint8_t* lrow = l_src + int64_t(ys) * l_pitch;
+      const uint32_t tx = uint32_t(rows * (s_bulk + l_bulk)) +
+                          (new_tables ? uint32_t(kTmplStride * 2 + (1 << P.bd)) : 0u);
+      if (tx) {
+        if (tid == 0) mbar_arrive_expect_tx(&sm.bar, tx);
+        if (warp == 0 && lane < rows && s_bulk)
+          bulk_g2s(sm.src + lane * kStageSrc, srow + int64_t(lane) * P.src_pitch, uint32_t(s_bulk), &sm.bar);
+        if (warp == 1 && lane < rows && l_bulk)
+          bulk_g2s(sm.luma + lane * kStageLuma, lrow + int64_t(lane) * l_pitch, uint32_t(l_bulk), &sm.bar);
+        if (warp == 2 && new_tables) {
+          if (lane == 0) bulk_g2s(T, &f.grain->tmpl[p][0], uint32_t(kTmplStride * 2), &sm.bar);
+          if (lane == 1) bulk_g2s(scale, &f.grain->scale[p][0], uint32_t(1 << P.bd), &sm.bar);
+        }
       }
-      asm volatile("cp.async.wait_all;" ::: "memory");
+      new_tables = false;
+      // the rest of each row, by plain copies
+      if (s_bulk < s_len) copy_rows(sm.src, kStageSrc, srow, P.src_pitch, rows, s_bulk, s_len);
+      if (luma_rows && l_bulk < l_len) copy_rows(sm.luma, kStageLuma, lrow, l_pitch, rows, l_bulk, l_len);
+      if (P.grain && tid < kOutOffs) {
+        const int b = b0 - 1 + tid;
+        const bool ok = b >= 0 && b < P.nb;
+        offs_cur[tid] = ok ? P.off[int64_t(stripe) * P.nb + b] : 0;
+        offs_prev[tid] = ok && stripe > 0 ? P.off[int64_t(stripe - 1) * P.nb + b] : 0;
+      }
+      if (tx) {
+        if (!mbar_wait(&sm.bar, phase, kOutWaitLimit) && tid == 0) atomicOr(&g_error_flags, ERRF_STALL);
+        phase ^= 1u;
+      }
       __syncthreads();
       const uint8_t* ss = sm.src;
       const uint8_t* sl = sm.luma;
-      if (item.plane == 0) {
+      if (p == 0) {
         if (P.sb == 2)
           out_stripe<false, 0, 0, 2>(P, T, scale, offs_cur, offs_prev, ss, sl, x0, x1, ys, ye, stripe, b0, P.grain);
         else
