@@ -142,21 +142,27 @@ __device__ __forceinline__ void lf_decide2(const FrameDesc& f, const LfTables& t
 }
 
 // The wide filter of 7.14.6.4 with N taps each side (inner weight-2 taps
-// |j| <= N2), output positions 7-N .. 7+N-1, all indices compile-time.
+// |j| <= N2), output positions 7-N .. 7+N-1, all indices compile-time. Each
+// output's tap sum is the previous one's with the tap that leaves the
+// window taken out and the one that enters added (taps past the ends repeat
+// the end samples), so an output costs four adds instead of 2N + 1.
 template <int N, int N2, int LOG2>
 __device__ __forceinline__ void lf_wide(int32_t v[14]) {
   int32_t o[14];
 #pragma unroll
   for (int k = 0; k < 14; k++) o[k] = v[k];
+  // the sample at offset k from q0, with the clamp to the filter's ends
+  auto at = [&](int k) { return o[7 + (k < -(N + 1) ? -(N + 1) : (k > N ? N : k))]; };
+  int32_t all = 0, inner = 0;  // the window sums of the first output (i = -N)
+#pragma unroll
+  for (int j = -N; j <= N; j++) all += at(-N + j);
+#pragma unroll
+  for (int j = -N2; j <= N2; j++) inner += at(-N + j);
 #pragma unroll
   for (int i = -N; i < N; i++) {
-    int32_t acc = 0;
-#pragma unroll
-    for (int j = -N; j <= N; j++) {
-      const int pp = (i + j) < -(N + 1) ? -(N + 1) : ((i + j) > N ? N : (i + j));
-      acc += o[7 + pp] * ((j <= N2 && j >= -N2) ? 2 : 1);
-    }
-    v[7 + i] = (acc + (1 << (LOG2 - 1))) >> LOG2;
+    v[7 + i] = (all + inner + (1 << (LOG2 - 1))) >> LOG2;
+    all += at(i + N + 1) - at(i - N);
+    inner += at(i + N2 + 1) - at(i - N2);
   }
 }
 
@@ -173,7 +179,7 @@ __device__ __forceinline__ void lf_filter_one(int32_t v[14], int filter_size, bo
   const int32_t thresh_bd = thresh << sh, limit_bd = limit << sh, blimit_bd = blimit << sh;
   const bool hev = abs(p1 - p0) > thresh_bd || abs(q1 - q0) > thresh_bd;
   const int filter_len = filter_size == 4 ? 4 : (chroma ? 6 : (filter_size == 8 ? 8 : 16));
-  bool mask = abs(p1 - p0) > limit_bd || abs(q1 - q0) > limit_bd || abs(p0 - q0) * 2 + abs(p1 - q1) / 2 > blimit_bd;
+  bool mask = abs(p1 - p0) > limit_bd || abs(q1 - q0) > limit_bd || abs(p0 - q0) * 2 + (abs(p1 - q1) >> 1) > blimit_bd;
   if (filter_len >= 6) mask = mask || abs(p2 - p1) > limit_bd || abs(q2 - q1) > limit_bd;
   if (filter_len >= 8) mask = mask || abs(p3 - p2) > limit_bd || abs(q3 - q2) > limit_bd;
   if (mask) return;
