@@ -170,6 +170,8 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // the loop filter's edge-list counters start at zero: cleared here, in the
   // upload's stream order, so the chain's stream holds kernels only
   if (e == cudaSuccess) e = cudaMemsetAsync(dmeta + plan.off_counts, 0, 16, upload);
+  // and the stages' readiness flags start cleared
+  if (e == cudaSuccess && plan.n_flags) e = cudaMemsetAsync(dmeta + plan.off_flags, 0, plan.n_flags * 4, upload);
   if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, upload);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(s, m.uploaded, 0);
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
@@ -195,7 +197,7 @@ int Ctx::launch_on(uint8_t* dmeta, cudaStream_t s) {
     prof_used[slot] = true;
     ev = prof_ev[slot];
   }
-  launch_plan(plan, dmeta, s, side, fork, join, ev, true);
+  launch_plan(plan, dmeta, s, side, fork, join, ev, true, true);
   return cuda_status(cudaGetLastError(), "kernel launch");
 }
 

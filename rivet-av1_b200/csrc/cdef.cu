@@ -392,9 +392,28 @@ __device__ __forceinline__ void write_prelf(const FrameDesc& f, int p, int sc, i
 // LFH: the launch has kind-1 items (the fused horizontal loop-filter pass);
 // without it the kernel carries none of that pass's code, which keeps the
 // default kernel's instruction footprint small.
+// With readiness flags: waits (threads 0..47, one flag each) for the
+// loop-filter tiles under the CTA's windows, the rows and columns
+// stage_plane reads: plane rows (y0 >> sy) - 2 .. ((y0 + R) >> sy) + 1 and
+// 8 columns past the superblock on either side, within the plane.
+template <int R>
+__device__ __forceinline__ void cdef_wait_lf(const FrameDesc& f, const uint32_t* flags, int sc, int y0, int tid) {
+  if (tid >= 48) return;
+  const int p = tid >> 4, dy = (tid >> 2) & 3, dx = tid & 3;
+  if (p >= f.np || f.lf_tiles_x[p] == 0) return;
+  const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+  const int W = f.cur[p].w, H = f.cur[p].h;
+  const int r0 = max((y0 >> sy) - 2, 0), r1 = min(((y0 + R) >> sy) + 1, H - 1);
+  const int c0 = max(((sc * 64) >> sx) - 8, 0), c1 = min(((sc * 64 + 64) >> sx) + 7, W - 1);
+  const int ty = (r0 >> 6) + dy, tx = (c0 >> 6) + dx;
+  if (r0 > r1 || c0 > c1 || ty > (r1 >> 6) || tx > (c1 >> 6)) return;
+  flag_wait(flags + f.lf_flag_base[p] + ty * f.lf_tiles_x[p] + tx);
+}
+
 template <int R, bool LFH>
 __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* __restrict__ frames,
-                                                           const Item* __restrict__ items, int n_items, int wrows) {
+                                                           const Item* __restrict__ items, int n_items, int wrows,
+                                                           uint32_t* __restrict__ flags) {
   extern __shared__ __align__(16) int16_t cdef_smem_base[];  // [R][kDS] direction copy, then [3][wrows * kS]
   int16_t* const dwin = cdef_smem_base;
   int16_t* const cdef_win = cdef_smem_base + cdef_dir_bytes(R) / 2;
@@ -439,7 +458,13 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
         }
       }
     }
-    pdl_wait();       // the loop filter's output is complete past this point
+    if (flags) {
+      // only the loop-filter tiles this CTA reads
+      pdl_trigger();
+      cdef_wait_lf<R>(f, flags, sc, y0, tid);
+    } else {
+      pdl_wait();  // the loop filter's output is complete past this point
+    }
     __syncthreads();  // the previous item is done with the windows and block states
     if (tid < R) bstate[tid] = st;
     // --- stage the windows (postfilter.rs:464-488): 8-sample chunks ---
@@ -566,6 +591,16 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
       }
     }
     __syncthreads();
+    if (flags && tid == 0) {
+      // the rows are in the CDEF planes: the half superblocks' flags
+      uint32_t* fl = flags + f.cdef_flag_base + 2 * sr * f.cdef_sbc + sc;
+      if (R == 64) {
+        flag_set(fl);
+        flag_set(fl + f.cdef_sbc);
+      } else {
+        flag_set(fl + item.a * f.cdef_sbc);
+      }
+    }
   }
 }
 
@@ -992,7 +1027,8 @@ cudaError_t cdef_init() {
   return e;
 }
 
-void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, cudaStream_t s) {
+void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, uint32_t* flags,
+                 cudaStream_t s) {
   if (n_items <= 0) return;
   // without the fused horizontal pass the windows hold 2 border rows each
   // side: smaller windows, more CTAs per SM
@@ -1000,13 +1036,13 @@ void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool l
   const int wrows = R + 2 * (lfh ? kTopLfh : 2);
   const int grid = min(n_items, kItemGrid);
   if (half && lfh)
-    launch_pdl(cdef_kernel<32, true>, grid, 128, size_t(cdef_smem(32, true)), s, frames, items, n_items, wrows);
+    launch_pdl(cdef_kernel<32, true>, grid, 128, size_t(cdef_smem(32, true)), s, frames, items, n_items, wrows, flags);
   else if (half)
-    launch_pdl(cdef_kernel<32, false>, grid, 128, size_t(cdef_smem(32, false)), s, frames, items, n_items, wrows);
+    launch_pdl(cdef_kernel<32, false>, grid, 128, size_t(cdef_smem(32, false)), s, frames, items, n_items, wrows, flags);
   else if (lfh)
-    launch_pdl(cdef_kernel<64, true>, grid, 256, size_t(cdef_smem(64, true)), s, frames, items, n_items, wrows);
+    launch_pdl(cdef_kernel<64, true>, grid, 256, size_t(cdef_smem(64, true)), s, frames, items, n_items, wrows, flags);
   else
-    launch_pdl(cdef_kernel<64, false>, grid, 256, size_t(cdef_smem(64, false)), s, frames, items, n_items, wrows);
+    launch_pdl(cdef_kernel<64, false>, grid, 256, size_t(cdef_smem(64, false)), s, frames, items, n_items, wrows, flags);
 }
 
 void launch_cdef_search(const CdefSearchDesc* ds, int n, int blocks, bool thorough, cudaStream_t s) {

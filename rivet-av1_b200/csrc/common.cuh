@@ -121,6 +121,33 @@ __device__ __forceinline__ void pdl_wait() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+// For the stages that wait on readiness flags (FrameDesc::lf_flag_base ...)
+// instead of pdl_wait: such a kernel lets its successor launch at once (all
+// of its own CTAs have then started, so none waits for a place on an SM
+// that a CTA of the successor holds) and waits per item for the flags of
+// the data it reads. The chain's last stage (loop restoration) waits for
+// flags that every CDEF item sets after its last read of the loop filter's
+// output, so when that stage's grid is complete no kernel of the chain
+// reads or writes the chain's buffers any more.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// A readiness flag: set with release semantics at GPU scope after the CTA's
+// barrier (so every thread's writes before the barrier are visible to a
+// thread that sees the flag), waited for with acquire semantics. The wait is
+// bounded: after kFlagSpins polls it flags ERRF_STALL and returns.
+constexpr int kFlagSpins = 1 << 21;
+__device__ __forceinline__ void flag_set(uint32_t* p) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(1u) : "memory");
+}
+__device__ __forceinline__ void flag_wait(const uint32_t* p) {
+  for (int k = 0; k < kFlagSpins; k++) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    if (v) return;
+    __nanosleep(100);
+  }
+  atomicOr(&g_error_flags, ERRF_STALL);
+}
 
 // Grid-stride loop over the items of a launch.
 #define FOR_EACH_ITEM(it, n)                                   \

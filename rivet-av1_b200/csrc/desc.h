@@ -82,6 +82,17 @@ struct FrameDesc {
   int32_t grain_nb;        // blocks per stripe
   int32_t grain_ns;        // stripes
   av1pf_film_grain g;
+  // Readiness flags between the stages, when a launch is given a flag array
+  // (else each stage waits for the whole previous stage): the loop-filter
+  // kernel sets one flag per 64x64 tile (plane p's tiles from
+  // lf_flag_base[p], lf_tiles_x[p] a row; lf_tiles_x[p] = 0 where the plane
+  // is not loop filtered), and the CDEF kernel one per half superblock (from
+  // cdef_flag_base, cdef_sbc a row of halves, two rows per superblock row).
+  // A CDEF CTA waits for the tiles under its window and a loop-restoration
+  // CTA for the half superblocks under its rectangle, instead of for the
+  // whole previous stage.
+  int32_t lf_flag_base[3], lf_tiles_x[3];
+  int32_t cdef_flag_base, cdef_sbc;
 };
 
 // One unit of work of a stage: a tile of one plane of one frame.

@@ -54,7 +54,8 @@ void launch_lf_prep(const FrameDesc* frames, const Item* items, int n_items, uin
 void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, uint64_t* list_h, uint32_t* counts,
                      uint32_t cap, cudaStream_t s);
 // Both directions per 64x64 tile in shared memory (copy in -> cur included).
-void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// `flags`: the readiness flags the kernel sets (see FrameDesc), or null.
+void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, uint32_t* flags, cudaStream_t s);
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,
                      cudaStream_t s);
 void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaStream_t s);
@@ -62,7 +63,9 @@ void launch_dsp_lf(int32_t* edges, const av1pf_lf_edge_params* prm, int n, cudaS
 // CDEF (cdef.cu)
 // `lfh`: some item has the horizontal loop-filter pass fused (item kind 1).
 // `half`: the items are half superblocks (Item::a = 0 top, 1 bottom).
-void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, cudaStream_t s);
+// `flags`: the readiness flags the kernel waits for and sets, or null.
+void launch_cdef(const FrameDesc* frames, const Item* items, int n_items, bool lfh, bool half, uint32_t* flags,
+                 cudaStream_t s);
 // Sets cdef_kernel's dynamic shared-memory limit on the current device.
 cudaError_t cdef_init();
 void launch_dsp_cdef(const int32_t* win, const av1pf_cdef_taps* taps, uint16_t* res, int n, cudaStream_t s);
@@ -112,7 +115,8 @@ void launch_superres(const FrameDesc* frames, const Item* items, int n_items, in
 cudaError_t superres_init();
 
 // Loop restoration (lr.cu)
-void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s);
+// `flags`: the readiness flags the kernel waits for, or null.
+void launch_lr(const FrameDesc* frames, const Item* items, int n_items, uint32_t* flags, cudaStream_t s);
 // Sets lr_kernel's dynamic shared-memory limit on the current device.
 cudaError_t lr_init();
 // Opts the output kernel into its dynamic shared memory (once per device).

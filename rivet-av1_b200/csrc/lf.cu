@@ -416,7 +416,8 @@ constexpr int kFChunks = kFW / 8 * kFW;  // 8-sample chunks of the window (800)
 // each pass are listed in shared memory grouped by filter size, so a warp's
 // lanes mostly take one filter path. 256 threads.
 __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __restrict__ frames,
-                                                       const Item* __restrict__ items, int n_items) {
+                                                       const Item* __restrict__ items, int n_items,
+                                                       uint32_t* __restrict__ flags) {
   const LfTables& tb = g_lf_tables;
   __shared__ __align__(16) uint16_t W[kFW * kFS];
   __shared__ uint32_t list_v[kFCells], list_h[kFCells];
@@ -581,6 +582,12 @@ __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __res
         }
       }
     }
+    if (flags) {
+      // the tile is in cur: its readiness flag (the barrier orders every
+      // thread's stores before the release)
+      __syncthreads();
+      if (tid == 0) flag_set(flags + f.lf_flag_base[plane] + (y0 / kFT) * f.lf_tiles_x[plane] + x0 / kFT);
+    }
   }
 }
 
@@ -616,9 +623,9 @@ void launch_lf_tiles(const FrameDesc* frames, const Item* items, int n_items, ui
   launch_pdl(lf_tile_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items, list_h, counts, cap);
 }
 
-void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
+void launch_lf_fused(const FrameDesc* frames, const Item* items, int n_items, uint32_t* flags, cudaStream_t s) {
   if (n_items <= 0) return;
-  launch_pdl(lf_fused_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items);
+  launch_pdl(lf_fused_kernel, min(n_items, kItemGrid), 256, 0, s, frames, items, n_items, flags);
 }
 
 void launch_lf_edges(int pass, const FrameDesc* frames, const uint64_t* list, const uint32_t* count, uint32_t cap,

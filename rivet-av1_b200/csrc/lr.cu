@@ -553,8 +553,27 @@ __device__ __forceinline__ void restore_rect(const FrameDesc& f, const LrSmem& s
   }
 }
 
+// With readiness flags: waits (threads 0..15, one flag each) for the CDEF
+// half superblocks under a rectangle: the stripe's rows y0 .. y1, which it
+// reads from the CDEF planes, over its columns and 3 on either side. (The
+// rows past the stripe come from the loop filter's output: the half
+// superblocks at the stripe's first and last rows waited for the tiles
+// under their windows, which reach 2 rows further.)
+__device__ __forceinline__ void lr_wait_cdef(const FrameDesc& f, const uint32_t* flags, int p, const LrGeom& geo, int x0,
+                                             int w, int tid) {
+  if (tid >= 16) return;
+  const int sx = plane_ssx(f, p), sy = plane_ssy(f, p);
+  const int xa = max(x0 - 3, 0), xb = min(x0 + w + 2, geo.pex);
+  const int h0 = (geo.y0 << sy) >> 5, h1 = ((geo.y1 << sy) + sy) >> 5;
+  const int c0 = (xa << sx) >> 6, c1 = min(((xb << sx) + sx) >> 6, f.cdef_sbc - 1);
+  const int hr = h0 + (tid >> 2), c = c0 + (tid & 3);
+  if (hr > h1 || c > c1) return;
+  flag_wait(flags + f.cdef_flag_base + hr * f.cdef_sbc + c);
+}
+
 __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __restrict__ frames,
-                                                         const Item* __restrict__ items, int n_items) {
+                                                         const Item* __restrict__ items, int n_items,
+                                                         const uint32_t* __restrict__ flags) {
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ av1pf_lr_unit s_unit;
   LrSmem sm;
@@ -583,7 +602,12 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     const int x0 = item.x0, w = int(item.x1) - int(item.x0);
     const int h = geo.y1 - geo.y0 + 1;
     if (h <= 0 || w <= 0) {
-      pdl_wait();  // every CTA waits, so the kernel never completes before its predecessor
+      // without flags every CTA waits, so the kernel never completes before
+      // its predecessor
+      if (flags)
+        pdl_trigger();
+      else
+        pdl_wait();
       continue;
     }
     int type = AV1PF_RESTORE_NONE;
@@ -596,8 +620,15 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
       type = unit_p->type;
     }
     // the descriptor and the unit are inputs of the chain; the planes below
-    // are the previous stage's output
-    pdl_wait();
+    // are the previous stage's output: all of it, or with readiness flags
+    // the half superblocks under the rectangle
+    if (flags) {
+      pdl_trigger();
+      lr_wait_cdef(f, flags, p, geo, x0, w, tid);
+      __syncthreads();
+    } else {
+      pdl_wait();
+    }
     if (type != AV1PF_RESTORE_WIENER && type != AV1PF_RESTORE_SGRPROJ) {
       pass_through(f, p, x0, geo.y0, w, h, tid);  // uniform across the CTA: no barrier needed
       continue;
@@ -637,11 +668,12 @@ cudaError_t lr_init() {
   return cudaFuncSetAttribute(lr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
 }
 
-void launch_lr(const FrameDesc* frames, const Item* items, int n_items, cudaStream_t s) {
+void launch_lr(const FrameDesc* frames, const Item* items, int n_items, uint32_t* flags, cudaStream_t s) {
   if (n_items <= 0) return;
   // one CTA per rectangle: the block scheduler hands rectangles of uneven
   // cost (copy, Wiener, self-guided) to SMs as they free up
-  launch_pdl(lr_kernel, min(n_items, kItemGrid), kThreads, size_t(kSmemBytes), s, frames, items, n_items);
+  launch_pdl(lr_kernel, min(n_items, kItemGrid), kThreads, size_t(kSmemBytes), s, frames, items, n_items,
+             static_cast<const uint32_t*>(flags));
 }
 
 }  // namespace av1pf

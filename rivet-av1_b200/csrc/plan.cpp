@@ -190,6 +190,10 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   if (n <= 0 || n > 65535) return fail(why, "bad job count"), AV1PF_ERR_INVALID_INPUT;
   Bump bump{scratch_base};
   uint32_t cap = 0;
+  // readiness flags (FrameDesc::lf_flag_base ...): their count, and whether every
+  // frame's stages fit them
+  size_t nflags = 0;
+  bool flags_fit = true;
   for (int fi = 0; fi < n; fi++) {
     const FrameJob& j = jobs[fi];
     const av1pf_frame_info* i = j.info;
@@ -262,6 +266,15 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       if (!lf_plane) {
         d.cur[k] = d.in[k];
         continue;
+      }
+      if (fused) {
+        // one flag per 64x64 tile of the fused kernel
+        const int tx = (d.in[k].w + kTile - 1) / kTile, ty = (d.in[k].h + kTile - 1) / kTile;
+        d.lf_flag_base[k] = int32_t(nflags);
+        d.lf_tiles_x[k] = tx;
+        nflags += size_t(tx) * size_t(ty);
+      } else {
+        flags_fit = false;
       }
       plan.any_lf = true;
       const int sx = k ? d.ssx : 0, sy = k ? d.ssy : 0;
@@ -336,6 +349,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       for (int k = 0; k < np; k++) d.cur[k] = from_abi(j.in[k]);
     }
     const bool cdef_on = cdef_stage && p->cdef_enabled;
+    if (!cdef_on) flags_fit = false;  // loop restoration would read the loop filter's output unflagged
     for (int k = 0; k < np; k++) {
       if (cdef_on)
         d.cdef[k] = chain ? bump.plane(d.cur[k].w, d.cur[k].h, sb) : from_abi(j.out[k]);
@@ -346,6 +360,11 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
       plan.any_cdef = true;
       const int sbr = (i->mi_rows + 15) / 16, sbc = (i->mi_cols + 15) / 16;
       if (d.lfh_mask) plan.any_lfh = true;
+      // one flag per half superblock
+      d.cdef_flag_base = int32_t(nflags);
+      d.cdef_sbc = sbc;
+      nflags += size_t(2 * sbr) * size_t(sbc);
+      if (d.lfh_mask || !chain) flags_fit = false;
       for (int r = 0; items && r < sbr; r++)
         for (int c = 0; c < sbc; c++) {
           Item it{};
@@ -474,6 +493,9 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   }
   plan.scratch_bytes = align_up(bump.used, 256);
   if (!items) return AV1PF_OK;  // the lists and their layout are the previous call's
+  plan.flag_sync = flags_fit && plan.any_lf && plan.any_cdef && plan.any_lr && !plan.any_sr && !plan.any_hlist &&
+                   plan.lf_items.empty() && plan.lft_items.empty() && plan.copy_items.empty();
+  plan.n_flags = plan.flag_sync ? nflags : 0;
   // At most one wave of superblocks (4 CTAs on each SM): CDEF runs a CTA per
   // half superblock instead, so the SMs end up with equal shares.
   plan.cdef_half = !plan.cdef_items.empty() && plan.cdef_items.size() <= size_t(kNumSMs) * 4;
@@ -514,6 +536,7 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   plan.off_edges_v = place(size_t(cap) * 8);
   plan.off_edges_h = place(size_t(cap) * 8);
   plan.off_counts = place(16);
+  plan.off_flags = place(plan.n_flags * 4);
   plan.meta_bytes = align_up(off, 256);
   return AV1PF_OK;
 }
@@ -558,7 +581,8 @@ void pack_meta(const Plan& plan, uint8_t* host) {
 }
 
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join, const cudaEvent_t* stage_ev, bool counts_zeroed) {
+                 cudaEvent_t join, const cudaEvent_t* stage_ev, bool counts_zeroed, bool flags) {
+  uint32_t* sync = flags && plan.flag_sync ? reinterpret_cast<uint32_t*>(meta + plan.off_flags) : nullptr;
   auto mark = [&](int k) {
     if (stage_ev) cudaEventRecord(stage_ev[k], s);
   };
@@ -596,14 +620,14 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
     if (plan.any_hlist) launch_lf_edges(1, frames, eh, counts + 1, plan.edge_cap, s);
   }
   if (plan.any_lf && !plan.lff_items.empty())
-    launch_lf_fused(frames, items(plan.off_lff), int(plan.lff_items.size()), s);
+    launch_lf_fused(frames, items(plan.off_lff), int(plan.lff_items.size()), sync, s);
   mark(1);
   if (plan.any_cdef)
-    launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), plan.any_lfh, plan.cdef_half, s);
+    launch_cdef(frames, items(plan.off_cdef), int(plan.cdef_items.size()), plan.any_lfh, plan.cdef_half, sync, s);
   mark(2);
   if (plan.any_sr) launch_superres(frames, items(plan.off_sr), int(plan.sr_items.size()), plan.sr_row_max, s);
   mark(3);
-  if (plan.any_lr) launch_lr(frames, items(plan.off_lr), int(plan.lr_items.size()), s);
+  if (plan.any_lr) launch_lr(frames, items(plan.off_lr), int(plan.lr_items.size()), sync, s);
   mark(4);
   if (plan.any_out) {
     if (plan.any_grain) cudaStreamWaitEvent(s, join, 0);

@@ -53,6 +53,13 @@ struct Plan {
   bool any_hlist = false;  // some plane's horizontal loop-filter edges run as their own pass
   bool any_lfh = false;    // some frame's horizontal loop-filter edges run inside the CDEF kernel
   bool cdef_half = false;  // CDEF items are half superblocks (Item::a: 0 top, 1 bottom)
+  // the stages can wait on readiness flags (FrameDesc::lf_flag_base ...)
+  // instead of on the whole previous stage: every frame runs the fused loop filter,
+  // CDEF and loop restoration, without superres or the horizontal
+  // loop-filter pass inside CDEF; n_flags flags at off_flags in the meta
+  // buffer, cleared before every call
+  bool flag_sync = false;
+  size_t n_flags = 0, off_flags = 0;
   int sr_row_max = 0;      // superres: the most source samples in a row (sr_maxx + 1)
   bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
   // byte offsets of each list in the device meta buffer
@@ -86,9 +93,12 @@ void pack_meta(const Plan& plan, uint8_t* host);
 // filter and after each of the 5 stages (for av1pf_stage_times).
 // `counts_zeroed`: the edge-list counters in `meta` are already zero (the
 // caller cleared them in stream order), so the first loop-filter pass needs
-// no memset on `s`.
+// no memset on `s`. `flags`: the stages wait on the readiness flags at
+// plan.off_flags in `meta` (plan.flag_sync; the caller cleared them in
+// stream order) instead of on the whole previous stage.
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr, bool counts_zeroed = false);
+                 cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr, bool counts_zeroed = false,
+                 bool flags = false);
 
 // Plane helpers.
 inline int plane_w(const av1pf_frame_info* i, int p, int width) {
