@@ -423,7 +423,6 @@ __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __res
   __shared__ uint32_t list_v[kFCells], list_h[kFCells];
   __shared__ uint32_t cnt[2][4], base[2][4];
   const int tid = threadIdx.x;
-  pdl_wait();  // the previous stage's output is complete past this point
   FOR_EACH_ITEM(it, n_items) {
     const Item item = items[it];
     const FrameDesc& f = frames[item.frame];
@@ -557,6 +556,11 @@ __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __res
       }
     }
     __syncthreads();
+    // Up to here the tile read only this call's inputs (the unfiltered
+    // planes, the maps, the descriptor) and worked in shared memory, so it
+    // ran while the previous call's stages drained; cur, which they read,
+    // is written only past this wait.
+    pdl_wait();
     // --- write the tile's own samples [x0, x1) x [y0, y1) ---
     {
       const int w = x1 - x0;
