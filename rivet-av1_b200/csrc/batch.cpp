@@ -71,7 +71,11 @@ void launch_groups(Batch& b, cudaStream_t s) {
   for (size_t g = 1; g < n; g++) cudaStreamWaitEvent(b.groups[g].stream, b.start, 0);
   for (size_t g = 0; g < n; g++) {
     BatchGroup& G = b.groups[g];
-    launch_plan(G.plan, static_cast<uint8_t*>(G.meta.ptr), g ? G.stream : s, G.side, G.fork, G.join);
+    uint8_t* meta = static_cast<uint8_t*>(G.meta.ptr);
+    cudaStream_t gs = g ? G.stream : s;
+    // the stages' readiness flags start cleared on every run
+    if (G.plan.n_flags) cudaMemsetAsync(meta + G.plan.off_flags, 0, G.plan.n_flags * 4, gs);
+    launch_plan(G.plan, meta, gs, G.side, G.fork, G.join, nullptr, false, true);
   }
   for (size_t g = 1; g < n; g++) {
     cudaEventRecord(b.groups[g].done, b.groups[g].stream);

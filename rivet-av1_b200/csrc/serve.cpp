@@ -292,7 +292,10 @@ int Server::start_batch(InFlight& b, std::vector<Request*>& reqs) {
   }
   pack_meta(b.plan, static_cast<uint8_t*>(b.meta_host));
   cudaMemcpyAsync(b.meta, b.meta_host, b.plan.upload_bytes, cudaMemcpyHostToDevice, b.s);
-  launch_plan(b.plan, static_cast<uint8_t*>(b.meta), b.s, b.side, b.fork, b.join);
+  // the stages' readiness flags start cleared
+  if (b.plan.n_flags)
+    cudaMemsetAsync(static_cast<uint8_t*>(b.meta) + b.plan.off_flags, 0, b.plan.n_flags * 4, b.s);
+  launch_plan(b.plan, static_cast<uint8_t*>(b.meta), b.s, b.side, b.fork, b.join, nullptr, false, true);
   for (Request* r : reqs)
     if (!r->device)
       cudaMemcpyAsync(r->hres, r->dframe_out, r->st->lay.frame_bytes, cudaMemcpyDeviceToHost, b.s);
