@@ -173,7 +173,13 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // and the stages' readiness flags start cleared
   if (e == cudaSuccess && plan.n_flags) e = cudaMemsetAsync(dmeta + plan.off_flags, 0, plan.n_flags * 4, upload);
   if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, upload);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, m.uploaded, 0);
+  // The kernels read the upload: the host waits for it rather than the
+  // chain's stream. It waited only for the chain that used this buffer two
+  // calls ago, so it has usually landed already; and with nothing between
+  // the previous call's last kernel and this call's first on the stream,
+  // programmatic dependent launch chains them (a stream-side wait here made
+  // every call boundary a full one: 9 us per 1080p frame).
+  if (e == cudaSuccess) e = cudaEventSynchronize(m.uploaded);
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
   m.used = true;
   rc = launch_on(dmeta, s);
