@@ -154,6 +154,13 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   if (m.used) cudaStreamWaitEvent(upload, m.done, 0);
   uint8_t* dmeta = static_cast<uint8_t*>(m.dev.ptr);
   uint8_t* hmeta = static_cast<uint8_t*>(m.host.ptr);
+  // film grain: this buffer's own scratch (the previous call's output kernel
+  // reads the other buffer's), so the template kernel can start at once
+  for (size_t fi = 0; fi < plan.frames.size() && fi < plan.grain_meta.size(); fi++) {
+    if (plan.grain_meta[fi].first == SIZE_MAX) continue;
+    plan.frames[fi].grain = reinterpret_cast<GrainScratch*>(dmeta + plan.off_grain_meta + plan.grain_meta[fi].first);
+    plan.frames[fi].grain_off = dmeta + plan.off_grain_meta + plan.grain_meta[fi].second;
+  }
   if (m.ready && m.key == key_scratch) {
     const size_t fbytes = plan.frames.size() * sizeof(FrameDesc);
     std::memcpy(hmeta + plan.off_frames, plan.frames.data(), fbytes);
@@ -203,7 +210,7 @@ int Ctx::launch_on(uint8_t* dmeta, cudaStream_t s) {
     prof_used[slot] = true;
     ev = prof_ev[slot];
   }
-  launch_plan(plan, dmeta, s, side, fork, join, ev, true, true);
+  launch_plan(plan, dmeta, s, side, fork, join, ev, true, true, true);
   return cuda_status(cudaGetLastError(), "kernel launch");
 }
 

@@ -414,6 +414,7 @@ template <int R, bool LFH>
 __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* __restrict__ frames,
                                                            const Item* __restrict__ items, int n_items, int wrows,
                                                            uint32_t* __restrict__ flags) {
+  AV1PF_TRACE_BEGIN();
   extern __shared__ __align__(16) int16_t cdef_smem_base[];  // [R][kDS] direction copy, then [3][wrows * kS]
   int16_t* const dwin = cdef_smem_base;
   int16_t* const cdef_win = cdef_smem_base + cdef_dir_bytes(R) / 2;
@@ -602,6 +603,7 @@ __global__ void __launch_bounds__(4 * R, 256 / R) cdef_kernel(const FrameDesc* _
       }
     }
   }
+  AV1PF_TRACE_END(2);
 }
 
 // Sum of a u32 over the warp, exactly (two 16-bit halves, so no lane sum

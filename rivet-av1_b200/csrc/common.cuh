@@ -131,6 +131,44 @@ __device__ __forceinline__ void pdl_wait() {
 // reads or writes the chain's buffers any more.
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Per-CTA timeline, in the AV1PF_TRACE build only (libav1pf_trace.so, read
+// by timeline.py): each stage kernel's CTAs record their start and end
+// (%globaltimer, ns), their SM and block, and the kernel's id into g_trace.
+// In the product build the two macros are empty.
+#ifdef AV1PF_TRACE
+constexpr int kTraceCap = 65536;
+extern __device__ unsigned long long g_trace[3 * kTraceCap];
+extern __device__ unsigned int g_trace_n;
+__device__ __forceinline__ unsigned long long trace_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void trace_end(int kid, unsigned long long t0) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    const unsigned i = atomicAdd(&g_trace_n, 1u);
+    if (i < unsigned(kTraceCap)) {
+      g_trace[3 * i] = t0;
+      g_trace[3 * i + 1] = trace_clock();
+      g_trace[3 * i + 2] = (static_cast<unsigned long long>(kid) << 40) | (static_cast<unsigned long long>(sm) << 24) |
+                           blockIdx.x;
+    }
+  }
+}
+#define AV1PF_TRACE_BEGIN() const unsigned long long av1pf_trace_t0 = ::av1pf::trace_clock()
+#define AV1PF_TRACE_END(kid) ::av1pf::trace_end((kid), av1pf_trace_t0)
+#else
+#define AV1PF_TRACE_BEGIN() \
+  do {                      \
+  } while (0)
+#define AV1PF_TRACE_END(kid) \
+  do {                       \
+  } while (0)
+#endif
+
 // A readiness flag: set with release semantics at GPU scope after the CTA's
 // barrier (so every thread's writes before the barrier are visible to a
 // thread that sees the flag), waited for with acquire semantics. The wait is

@@ -264,6 +264,7 @@ __device__ __forceinline__ void ar_plane(int lag, int16_t (*T)[kTW], const int16
 // per-stripe block offsets (one stripe per thread).
 __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __restrict__ frames,
                                                          const Item* __restrict__ items, int n_items) {
+  AV1PF_TRACE_BEGIN();
   __shared__ __align__(16) int16_t T[3][kTH][kTW];
   __shared__ int32_t coef[3][25];
   __shared__ uint8_t lut[3][256];
@@ -407,6 +408,7 @@ __global__ void __launch_bounds__(256) grain_prep_kernel(const FrameDesc* __rest
     }
     __syncthreads();
   }
+  AV1PF_TRACE_END(6);
 }
 
 // Per-item constants of the output stage, held in registers: the stores to
@@ -648,6 +650,7 @@ constexpr int kOutWaitLimit = 1 << 16;  // bulk-copy waits of about 1 us each be
 // threads take 8 consecutive samples (one grain block) each per row.
 __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restrict__ frames,
                                                      const Item* __restrict__ items, int n_items) {
+  AV1PF_TRACE_BEGIN();
   extern __shared__ __align__(16) uint8_t out_smem[];
   OutSmem& sm = *reinterpret_cast<OutSmem*>(out_smem);
   int16_t* T = sm.T;
@@ -808,6 +811,7 @@ __global__ void __launch_bounds__(256, 2) output_kernel(const FrameDesc* __restr
       ys = ye;
     }
   }
+  AV1PF_TRACE_END(4);
 }
 
 cudaError_t output_init() {

@@ -418,6 +418,7 @@ constexpr int kFChunks = kFW / 8 * kFW;  // 8-sample chunks of the window (800)
 __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __restrict__ frames,
                                                        const Item* __restrict__ items, int n_items,
                                                        uint32_t* __restrict__ flags) {
+  AV1PF_TRACE_BEGIN();
   const LfTables& tb = g_lf_tables;
   __shared__ __align__(16) uint16_t W[kFW * kFS];
   __shared__ uint32_t list_v[kFCells], list_h[kFCells];
@@ -593,6 +594,7 @@ __global__ void __launch_bounds__(256, 4) lf_fused_kernel(const FrameDesc* __res
       if (tid == 0) flag_set(flags + f.lf_flag_base[plane] + (y0 / kFT) * f.lf_tiles_x[plane] + x0 / kFT);
     }
   }
+  AV1PF_TRACE_END(1);
 }
 
 // dsp::lf::filter (lf.rs:25) on independent edges: one thread per lane.

@@ -574,6 +574,7 @@ __device__ __forceinline__ void lr_wait_cdef(const FrameDesc& f, const uint32_t*
 __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __restrict__ frames,
                                                          const Item* __restrict__ items, int n_items,
                                                          const uint32_t* __restrict__ flags) {
+  AV1PF_TRACE_BEGIN();
   extern __shared__ __align__(16) uint8_t smem[];
   __shared__ av1pf_lr_unit s_unit;
   LrSmem sm;
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(kThreads, 3) lr_kernel(const FrameDesc* __rest
     }
     __syncthreads();
   }
+  AV1PF_TRACE_END(3);
 }
 
 cudaError_t lr_init() {

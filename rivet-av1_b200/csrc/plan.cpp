@@ -537,6 +537,19 @@ int build_plan(const FrameJob* jobs, int n, uint8_t* scratch_base, Plan& plan, s
   plan.off_edges_h = place(size_t(cap) * 8);
   plan.off_counts = place(16);
   plan.off_flags = place(plan.n_flags * 4);
+  {
+    plan.grain_meta.assign(plan.frames.size(), {SIZE_MAX, SIZE_MAX});
+    size_t g = 0;
+    for (size_t fi = 0; fi < plan.frames.size(); fi++) {
+      const FrameDesc& d = plan.frames[fi];
+      if (!d.grain_on) continue;
+      plan.grain_meta[fi].first = g;
+      g = align_up(g + sizeof(GrainScratch), 256);
+      plan.grain_meta[fi].second = g;
+      g = align_up(g + size_t(d.grain_ns) * size_t(d.grain_nb), 256);
+    }
+    plan.off_grain_meta = place(g);
+  }
   plan.meta_bytes = align_up(off, 256);
   return AV1PF_OK;
 }
@@ -581,7 +594,8 @@ void pack_meta(const Plan& plan, uint8_t* host) {
 }
 
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
-                 cudaEvent_t join, const cudaEvent_t* stage_ev, bool counts_zeroed, bool flags) {
+                 cudaEvent_t join, const cudaEvent_t* stage_ev, bool counts_zeroed, bool flags,
+                 bool grain_private) {
   uint32_t* sync = flags && plan.flag_sync ? reinterpret_cast<uint32_t*>(meta + plan.off_flags) : nullptr;
   auto mark = [&](int k) {
     if (stage_ev) cudaEventRecord(stage_ev[k], s);
@@ -592,9 +606,13 @@ void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t s
   uint64_t* eh = reinterpret_cast<uint64_t*>(meta + plan.off_edges_h);
   uint32_t* counts = reinterpret_cast<uint32_t*>(meta + plan.off_counts);
   if (plan.any_grain) {
-    // the grain templates depend only on the parameters: run them beside the chain
-    cudaEventRecord(fork, s);
-    cudaStreamWaitEvent(side, fork, 0);
+    // the grain templates depend only on the parameters: run them beside the
+    // chain; into a scratch that the previous call's output kernel may still
+    // read, only once `s` has got this far
+    if (!grain_private) {
+      cudaEventRecord(fork, s);
+      cudaStreamWaitEvent(side, fork, 0);
+    }
     launch_grain_prep(frames, items(plan.off_grain), int(plan.grain_items.size()), side);
     cudaEventRecord(join, side);
   }

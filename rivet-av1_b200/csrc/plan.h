@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "av1pf.h"
@@ -60,6 +61,14 @@ struct Plan {
   // buffer, cleared before every call
   bool flag_sync = false;
   size_t n_flags = 0, off_flags = 0;
+  // A call's own film-grain scratch (templates, scaling tables, block
+  // offsets) in the descriptor buffer, one per frame with grain:
+  // grain_meta[frame] = {scratch offset, block-offsets offset} from
+  // off_grain_meta (SIZE_MAX: no grain). Single calls point their
+  // descriptors here, so a call's template kernel never writes what the
+  // previous call's output kernel reads.
+  size_t off_grain_meta = 0;
+  std::vector<std::pair<size_t, size_t>> grain_meta;
   int sr_row_max = 0;      // superres: the most source samples in a row (sr_maxx + 1)
   bool any_lf = false, any_cdef = false, any_sr = false, any_lr = false, any_grain = false, any_out = false;
   // byte offsets of each list in the device meta buffer
@@ -95,10 +104,13 @@ void pack_meta(const Plan& plan, uint8_t* host);
 // caller cleared them in stream order), so the first loop-filter pass needs
 // no memset on `s`. `flags`: the stages wait on the readiness flags at
 // plan.off_flags in `meta` (plan.flag_sync; the caller cleared them in
-// stream order) instead of on the whole previous stage.
+// stream order) instead of on the whole previous stage. `grain_private`:
+// the frames' film-grain scratch is this call's own (plan.grain_meta, no
+// earlier kernel still reads it), so the template kernel starts on the side
+// stream without waiting for `s`.
 void launch_plan(const Plan& plan, uint8_t* meta, cudaStream_t s, cudaStream_t side, cudaEvent_t fork,
                  cudaEvent_t join, const cudaEvent_t* stage_ev = nullptr, bool counts_zeroed = false,
-                 bool flags = false);
+                 bool flags = false, bool grain_private = false);
 
 // Plane helpers.
 inline int plane_w(const av1pf_frame_info* i, int p, int width) {

@@ -31,6 +31,7 @@ __host__ __device__ constexpr int sr_stride(int n) { return (n + 7) & ~7; }
 
 __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restrict__ frames,
                                                        const Item* __restrict__ items, int n_items, int rs) {
+  AV1PF_TRACE_BEGIN();
   extern __shared__ __align__(16) uint8_t sr_smem[];
   uint16_t* rows = reinterpret_cast<uint16_t*>(sr_smem);  // kRows staged source rows, rs apart
   pdl_wait();  // the previous stage's output is complete past this point
@@ -130,6 +131,7 @@ __global__ void __launch_bounds__(256) superres_kernel(const FrameDesc* __restri
     }
     __syncthreads();  // the rows are free for the next item
   }
+  AV1PF_TRACE_END(5);
 }
 
 cudaError_t superres_init() {

@@ -56,3 +56,22 @@ cudaError_t read_error_flags(uint32_t* flags, cudaStream_t s) {
 }
 
 }  // namespace av1pf
+
+#ifdef AV1PF_TRACE
+namespace av1pf {
+__device__ unsigned long long g_trace[3 * kTraceCap];
+__device__ unsigned int g_trace_n;
+}  // namespace av1pf
+
+// The trace build's read-out: copies the records (3 words each: start,
+// end, kernel << 40 | SM << 24 | block) and their count, then clears the
+// count. Returns a cudaError_t.
+extern "C" int av1pf_trace_read(unsigned long long* out, unsigned* n) {
+  cudaError_t e = cudaMemcpyFromSymbol(n, av1pf::g_trace_n, sizeof(unsigned));
+  const unsigned m = *n < unsigned(av1pf::kTraceCap) ? *n : unsigned(av1pf::kTraceCap);
+  if (e == cudaSuccess && m) e = cudaMemcpyFromSymbol(out, av1pf::g_trace, m * 3 * sizeof(unsigned long long));
+  const unsigned z = 0;
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(av1pf::g_trace_n, &z, sizeof(unsigned));
+  return int(e);
+}
+#endif
