@@ -300,7 +300,11 @@ int av1pf_output_noalloc(const av1pf_frame_info* info, const av1pf_params* param
  * output process: reads the pre-filter planes `in` (left unchanged), writes
  * the LR frame (the reference frame, RefData.frame) into `ref_out` over the
  * visible area, and — when `frame_out` is not NULL — the packed output frame
- * as av1pf_output does. Scratch comes from the context. */
+ * as av1pf_output does. Scratch comes from the context. The kernels are
+ * queued on `stream`; the call returns once the frame's descriptors are on
+ * the device. The context keeps two descriptor buffers in turn, so the call
+ * may first wait on the host for the chain it queued two calls earlier:
+ * a caller runs at most about two calls ahead of the GPU per context. */
 int av1pf_chain(av1pf_ctx* ctx, const av1pf_frame_info* info,
                 const av1pf_params* params, const av1pf_maps* maps,
                 const av1pf_plane* in, av1pf_plane* ref_out,
