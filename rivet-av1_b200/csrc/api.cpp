@@ -186,7 +186,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // the previous call's last kernel and this call's first on the stream,
   // programmatic dependent launch chains them (a stream-side wait here made
   // every call boundary a full one: 9 us per 1080p frame).
-  if (e == cudaSuccess) e = cudaEventSynchronize(m.uploaded);
+  if (e == cudaSuccess) e = stream_upload_wait ? cudaStreamWaitEvent(s, m.uploaded, 0) : cudaEventSynchronize(m.uploaded);
   if (e != cudaSuccess) return cuda_status(e, "descriptor upload");
   m.used = true;
   rc = launch_on(dmeta, s);
@@ -334,8 +334,10 @@ int av1pf_ctx_destroy(av1pf_ctx* ctx) {
   for (auto* b : {&ctx->h_in, &ctx->h_ref, &ctx->h_maps, &ctx->h_frame, &ctx->search_dev, &ctx->search_planes})
     ctx->release(*b);
   if (ctx->search_host.ptr) cudaFreeHost(ctx->search_host.ptr);
+  if (ctx->h_maps_stage.ptr) cudaFreeHost(ctx->h_maps_stage.ptr);
   for (Ctx::PipeSlot& ps : ctx->pipe) {
     for (auto* b : {&ps.in, &ps.ref, &ps.maps, &ps.frame}) ctx->release(*b);
+    if (ps.maps_stage.ptr) cudaFreeHost(ps.maps_stage.ptr);
     for (cudaEvent_t ev : {ps.uploaded, ps.computed, ps.downloaded})
       if (ev) cudaEventDestroy(ev);
   }
@@ -519,7 +521,7 @@ void host_layout(const av1pf_frame_info* info, const av1pf_params* params, const
 // out by `L`; fills din / dref / dm with the device-side descriptions.
 cudaError_t upload_job(const HostLayout& L, const av1pf_frame_info* info, const av1pf_maps* maps,
                        const av1pf_plane* in, uint8_t* bin, uint8_t* bref, uint8_t* bmap, av1pf_plane* din,
-                       av1pf_plane* dref, av1pf_maps& dm, cudaStream_t s) {
+                       av1pf_plane* dref, av1pf_maps& dm, uint8_t* stage, cudaStream_t s) {
   const int np = info->num_planes, sb = info->sample_bytes;
   cudaError_t e = cudaSuccess;
   for (int k = 0; k < np && e == cudaSuccess; k++) {
@@ -539,27 +541,37 @@ cudaError_t upload_job(const HostLayout& L, const av1pf_frame_info* info, const 
   dm.mi = reinterpret_cast<const av1pf_mi*>(bmap + L.map_off[0]);
   if (e == cudaSuccess && L.mi_n && maps->mi)
     e = cudaMemcpyAsync(bmap + L.map_off[0], maps->mi, L.mi_n * sizeof(av1pf_mi), cudaMemcpyHostToDevice, s);
-  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+  // the maps after the mode info (transform sizes, CDEF indices, LR units):
+  // with `stage`, packed on the host in their device layout and uploaded as
+  // one copy (each copy costs the copy engine a few microseconds, and small
+  // ones also slow the concurrent download), else one copy each
+  const size_t s0 = L.map_off[1];
+  auto put = [&](size_t off, const void* src, size_t bytes) {
+    if (!bytes || e != cudaSuccess) return;
+    if (stage) std::memcpy(stage + (off - s0), src, bytes);
+    else e = cudaMemcpyAsync(bmap + off, src, bytes, cudaMemcpyHostToDevice, s);
+  };
+  for (int k = 0; k < 3; k++) {
     dm.lf_tx_size[k] = nullptr;
     if (k < np && maps->lf_tx_size[k]) {
       dm.lf_tx_size[k] = bmap + L.map_off[1 + k];
-      e = cudaMemcpyAsync(bmap + L.map_off[1 + k], maps->lf_tx_size[k], L.tx_rows[k] * size_t(maps->mi_stride),
-                          cudaMemcpyHostToDevice, s);
+      put(L.map_off[1 + k], maps->lf_tx_size[k], L.tx_rows[k] * size_t(maps->mi_stride));
     }
   }
   dm.cdef_idx = nullptr;
-  if (e == cudaSuccess && maps->cdef_idx) {
+  if (maps->cdef_idx) {
     dm.cdef_idx = reinterpret_cast<const int8_t*>(bmap + L.map_off[4]);
-    e = cudaMemcpyAsync(bmap + L.map_off[4], maps->cdef_idx, L.cdef_n, cudaMemcpyHostToDevice, s);
+    put(L.map_off[4], maps->cdef_idx, L.cdef_n);
   }
-  for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+  for (int k = 0; k < 3; k++) {
     dm.lr_units[k] = nullptr;
     if (L.lr_n[k]) {
       dm.lr_units[k] = reinterpret_cast<const av1pf_lr_unit*>(bmap + L.map_off[5 + k]);
-      e = cudaMemcpyAsync(bmap + L.map_off[5 + k], maps->lr_units[k], L.lr_n[k] * sizeof(av1pf_lr_unit),
-                          cudaMemcpyHostToDevice, s);
+      put(L.map_off[5 + k], maps->lr_units[k], L.lr_n[k] * sizeof(av1pf_lr_unit));
     }
   }
+  if (stage && e == cudaSuccess && L.total_maps > s0)
+    e = cudaMemcpyAsync(bmap + s0, stage, L.total_maps - s0, cudaMemcpyHostToDevice, s);
   return e;
 }
 
@@ -620,13 +632,14 @@ int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_p
   HostLayout L;
   host_layout(info, params, maps, in, L);
   if ((rc = ctx->ensure(ctx->h_in, L.total_in)) || (rc = ctx->ensure(ctx->h_ref, L.total_ref)) ||
-      (rc = ctx->ensure(ctx->h_maps, L.total_maps)) || (rc = ctx->ensure(ctx->h_frame, L.fbytes + 16)))
+      (rc = ctx->ensure(ctx->h_maps, L.total_maps)) || (rc = ctx->ensure(ctx->h_frame, L.fbytes + 16)) ||
+      (rc = ctx->ensure_host(ctx->h_maps_stage, L.total_maps - L.map_off[1] + 16)))
     return rc;
   av1pf_plane din[3], dref[3];
   av1pf_maps dm;
   cudaError_t e = upload_job(L, info, maps, in, static_cast<uint8_t*>(ctx->h_in.ptr),
                              static_cast<uint8_t*>(ctx->h_ref.ptr), static_cast<uint8_t*>(ctx->h_maps.ptr), din, dref,
-                             dm, s);
+                             dm, static_cast<uint8_t*>(ctx->h_maps_stage.ptr), s);
   if (e != cudaSuccess) return cuda_status(e, "host-to-device copy");
   uint8_t* dframe = frame_out ? static_cast<uint8_t*>(ctx->h_frame.ptr) : nullptr;
   rc = av1pf_chain(ctx, info, params, &dm, din, dref, dframe, s);
@@ -648,7 +661,7 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
   // every job is checked, and the slots sized for the largest, before
   // anything is queued
   std::vector<HostLayout> lay(static_cast<size_t>(n));
-  size_t need_in = 0, need_ref = 0, need_maps = 0, need_frame = 0;
+  size_t need_in = 0, need_ref = 0, need_maps = 0, need_frame = 0, need_stage = 0;
   for (int k = 0; k < n; k++) {
     const av1pf_host_job& j = jobs[k];
     if ((rc = validate_all(j.info, j.params, nullptr))) return rc;
@@ -662,6 +675,7 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     need_ref = std::max(need_ref, lay[size_t(k)].total_ref);
     need_maps = std::max(need_maps, lay[size_t(k)].total_maps);
     need_frame = std::max(need_frame, lay[size_t(k)].fbytes + 16);
+    need_stage = std::max(need_stage, lay[size_t(k)].total_maps - lay[size_t(k)].map_off[1] + 16);
   }
   const int slots = std::min(n, ctx->threads);
   for (int q = 0; q < slots; q++) {
@@ -669,10 +683,20 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     if ((rc = ctx->ensure(ps.in, need_in)) || (rc = ctx->ensure(ps.ref, need_ref)) ||
         (rc = ctx->ensure(ps.maps, need_maps)) || (rc = ctx->ensure(ps.frame, need_frame)))
       return rc;
+    // (the staging is rewritten only after the upload that read it: at the
+    // start of a call every earlier call's uploads are done)
+    if ((rc = ctx->ensure_host(ps.maps_stage, need_stage))) return rc;
   }
   cudaError_t e = ctx->pipe_streams();
   if (e != cudaSuccess) return cuda_status(e, "pipeline streams");
   cudaStream_t up = ctx->pipe_up, comp = ctx->own, down = ctx->pipe_down;
+  // each chain already waits for its planes on `comp`: its descriptor upload
+  // is waited for there too, and the host goes on queueing uploads
+  struct StreamWait {
+    Ctx* c;
+    explicit StreamWait(Ctx* c_) : c(c_) { c->stream_upload_wait = true; }
+    ~StreamWait() { c->stream_upload_wait = false; }
+  } stream_wait(ctx);
   // frame k uses slot k % slots: its upload waits for the chain that last
   // read the slot's inputs, its chain for its upload and for the download
   // that last read the slot's outputs
@@ -681,11 +705,14 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     Ctx::PipeSlot& ps = ctx->pipe[k % slots];
     const bool reused = k >= slots;
     if (reused) e = cudaStreamWaitEvent(up, ps.computed, 0);
+    // the slot's map staging is read by its previous upload
+    if (e == cudaSuccess && reused) e = cudaEventSynchronize(ps.uploaded);
     av1pf_plane din[3], dref[3];
     av1pf_maps dm;
     if (e == cudaSuccess)
       e = upload_job(lay[size_t(k)], j.info, j.maps, j.in, static_cast<uint8_t*>(ps.in.ptr),
-                     static_cast<uint8_t*>(ps.ref.ptr), static_cast<uint8_t*>(ps.maps.ptr), din, dref, dm, up);
+                     static_cast<uint8_t*>(ps.ref.ptr), static_cast<uint8_t*>(ps.maps.ptr), din, dref, dm,
+                     static_cast<uint8_t*>(ps.maps_stage.ptr), up);
     if (e == cudaSuccess) e = cudaEventRecord(ps.uploaded, up);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ps.uploaded, 0);
     if (e == cudaSuccess && reused) e = cudaStreamWaitEvent(comp, ps.downloaded, 0);

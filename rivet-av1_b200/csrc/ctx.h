@@ -59,6 +59,7 @@ struct Ctx {
   cudaEvent_t fork = nullptr, join = nullptr;
   DevBuf scratch;
   DevBuf h_in, h_ref, h_maps, h_frame;  // av1pf_chain_host
+  HostBuf h_maps_stage;                  // its small maps, packed for one upload
   // encoder searches: descriptors, error tables and greedy state; the
   // loop-filter search's filtered copies; pinned staging of both
   DevBuf search_dev, search_planes;
@@ -69,6 +70,7 @@ struct Ctx {
   static constexpr int kPipeSlots = 8;
   struct PipeSlot {
     DevBuf in, ref, maps, frame;
+    HostBuf maps_stage;  // the frame's small maps, packed for one upload
     cudaEvent_t uploaded = nullptr, computed = nullptr, downloaded = nullptr;
   };
   PipeSlot pipe[kPipeSlots];
@@ -91,6 +93,11 @@ struct Ctx {
   MetaSlot metas[2];
   int meta_next = 0;
   cudaStream_t upload = nullptr;  // descriptor uploads
+  // the chain's stream, not the host, waits for the descriptor upload: set
+  // by callers whose chains begin with a stream wait anyway (the host-buffer
+  // pipeline waits for each frame's planes), so that the host keeps queueing
+  // uploads instead of waiting behind them
+  bool stream_upload_wait = false;
   // profiling: a ring of event sets, one per profiled call
   static constexpr int kProfSlots = 64;
   bool prof = false;
