@@ -67,9 +67,9 @@ HEADLINE_WORKLOAD = "1920x1080 10-bit 4:2:0 single-frame post-filter chain (LF+C
 # (they reach DRAM later, during the next launches). The headline frames have no film grain: the
 # loop-restoration kernel packs them and no output kernel runs.
 NCU_HEADLINE = {
-    "loop_filter": {"dram_read": 8344064, "dram_write": 0, "warp_inst": 9694327},  # lf_fused_kernel (mode 3)
-    "cdef": {"dram_read": 7012864, "dram_write": 0, "warp_inst": 16999918},
-    "loop_restoration": {"dram_read": 8341760, "dram_write": 18176, "warp_inst": 15006469},
+    "loop_filter": {"dram_read": 8345344, "dram_write": 0, "warp_inst": 10128792},  # lf_fused_kernel (mode 3)
+    "cdef": {"dram_read": 6999808, "dram_write": 0, "warp_inst": 16245271},
+    "loop_restoration": {"dram_read": 8367872, "dram_write": 13312, "warp_inst": 14475086},
 }
 B200_SMS, ISSUE_PER_SM_CLK = 148, 4  # four schedulers per SM, one warp-instruction each per clock
 
