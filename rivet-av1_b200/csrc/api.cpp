@@ -151,7 +151,8 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // overwritten
   if (m.used && (e = cudaEventSynchronize(m.uploaded)) != cudaSuccess) return cuda_status(e, "staging wait");
   if ((rc = ensure_host(m.host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
-  if (m.used) cudaStreamWaitEvent(upload, m.done, 0);
+  cudaStream_t ups = upload_override ? upload_override : upload;
+  if (m.used) cudaStreamWaitEvent(ups, m.done, 0);
   uint8_t* dmeta = static_cast<uint8_t*>(m.dev.ptr);
   uint8_t* hmeta = static_cast<uint8_t*>(m.host.ptr);
   // film grain: this buffer's own scratch (the previous call's output kernel
@@ -164,11 +165,11 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   if (m.ready && m.key == key_scratch) {
     const size_t fbytes = plan.frames.size() * sizeof(FrameDesc);
     std::memcpy(hmeta + plan.off_frames, plan.frames.data(), fbytes);
-    e = cudaMemcpyAsync(dmeta + plan.off_frames, hmeta + plan.off_frames, fbytes, cudaMemcpyHostToDevice, upload);
+    e = cudaMemcpyAsync(dmeta + plan.off_frames, hmeta + plan.off_frames, fbytes, cudaMemcpyHostToDevice, ups);
   } else {
     m.ready = false;
     pack_meta(plan, hmeta);
-    e = cudaMemcpyAsync(dmeta, hmeta, plan.upload_bytes, cudaMemcpyHostToDevice, upload);
+    e = cudaMemcpyAsync(dmeta, hmeta, plan.upload_bytes, cudaMemcpyHostToDevice, ups);
     if (e == cudaSuccess) {
       m.key = key_scratch;
       m.ready = true;
@@ -176,10 +177,10 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   }
   // the loop filter's edge-list counters start at zero: cleared here, in the
   // upload's stream order, so the chain's stream holds kernels only
-  if (e == cudaSuccess) e = cudaMemsetAsync(dmeta + plan.off_counts, 0, 16, upload);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dmeta + plan.off_counts, 0, 16, ups);
   // and the stages' readiness flags start cleared
-  if (e == cudaSuccess && plan.n_flags) e = cudaMemsetAsync(dmeta + plan.off_flags, 0, plan.n_flags * 4, upload);
-  if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, upload);
+  if (e == cudaSuccess && plan.n_flags) e = cudaMemsetAsync(dmeta + plan.off_flags, 0, plan.n_flags * 4, ups);
+  if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, ups);
   // The kernels read the upload: the host waits for it rather than the
   // chain's stream. It waited only for the chain that used this buffer two
   // calls ago, so it has usually landed already; and with nothing between
@@ -691,12 +692,19 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
   if (e != cudaSuccess) return cuda_status(e, "pipeline streams");
   cudaStream_t up = ctx->pipe_up, comp = ctx->own, down = ctx->pipe_down;
   // each chain already waits for its planes on `comp`: its descriptor upload
-  // is waited for there too, and the host goes on queueing uploads
+  // goes on `up` right after them and is waited for on `comp` too, and the
+  // host goes on queueing uploads
   struct StreamWait {
     Ctx* c;
-    explicit StreamWait(Ctx* c_) : c(c_) { c->stream_upload_wait = true; }
-    ~StreamWait() { c->stream_upload_wait = false; }
-  } stream_wait(ctx);
+    StreamWait(Ctx* c_, cudaStream_t up_) : c(c_) {
+      c->stream_upload_wait = true;
+      c->upload_override = up_;
+    }
+    ~StreamWait() {
+      c->stream_upload_wait = false;
+      c->upload_override = nullptr;
+    }
+  } stream_wait(ctx, up);
   // frame k uses slot k % slots: its upload waits for the chain that last
   // read the slot's inputs, its chain for its upload and for the download
   // that last read the slot's outputs

@@ -98,6 +98,11 @@ struct Ctx {
   // pipeline waits for each frame's planes), so that the host keeps queueing
   // uploads instead of waiting behind them
   bool stream_upload_wait = false;
+  // the stream the descriptor uploads go on instead of `upload` (null: that
+  // one): the host-buffer pipeline puts each frame's descriptors right after
+  // its planes, in the same stream, since a small copy on a stream of its own
+  // was measured landing 0.5 ms late behind the frames' large copies
+  cudaStream_t upload_override = nullptr;
   // profiling: a ring of event sets, one per profiled call
   static constexpr int kProfSlots = 64;
   bool prof = false;
