@@ -602,6 +602,21 @@ int check_host_planes(const av1pf_frame_info* info, const av1pf_plane* in) {
   return AV1PF_OK;
 }
 
+// While alive, the context's descriptor uploads go on `up` (the stream that
+// uploads the frames' planes, so each lands right after its frame's planes)
+// and its chains wait for them on their own stream, not on the host.
+struct UploadsAfterPlanes {
+  Ctx* c;
+  UploadsAfterPlanes(Ctx* c_, cudaStream_t up) : c(c_) {
+    c->stream_upload_wait = true;
+    c->upload_override = up;
+  }
+  ~UploadsAfterPlanes() {
+    c->stream_upload_wait = false;
+    c->upload_override = nullptr;
+  }
+};
+
 int check_error_flags(cudaStream_t s) {
   uint32_t flags = 0;
   cudaError_t e = read_error_flags(&flags, s);
@@ -643,7 +658,11 @@ int av1pf_chain_host(av1pf_ctx* ctx, const av1pf_frame_info* info, const av1pf_p
                              dm, static_cast<uint8_t*>(ctx->h_maps_stage.ptr), s);
   if (e != cudaSuccess) return cuda_status(e, "host-to-device copy");
   uint8_t* dframe = frame_out ? static_cast<uint8_t*>(ctx->h_frame.ptr) : nullptr;
-  rc = av1pf_chain(ctx, info, params, &dm, din, dref, dframe, s);
+  {
+    // the descriptors follow the planes on `s`: the chain is queued at once
+    UploadsAfterPlanes uploads_after_planes(ctx, s);
+    rc = av1pf_chain(ctx, info, params, &dm, din, dref, dframe, s);
+  }
   if (rc != AV1PF_OK) return rc;
   e = download_job(L, info, dref, ref_out, dframe, frame_out, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -694,17 +713,7 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
   // each chain already waits for its planes on `comp`: its descriptor upload
   // goes on `up` right after them and is waited for on `comp` too, and the
   // host goes on queueing uploads
-  struct StreamWait {
-    Ctx* c;
-    StreamWait(Ctx* c_, cudaStream_t up_) : c(c_) {
-      c->stream_upload_wait = true;
-      c->upload_override = up_;
-    }
-    ~StreamWait() {
-      c->stream_upload_wait = false;
-      c->upload_override = nullptr;
-    }
-  } stream_wait(ctx, up);
+  UploadsAfterPlanes uploads_after_planes(ctx, up);
   // frame k uses slot k % slots: its upload waits for the chain that last
   // read the slot's inputs, its chain for its upload and for the download
   // that last read the slot's outputs
