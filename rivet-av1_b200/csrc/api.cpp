@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -105,6 +106,43 @@ void Ctx::release(DevBuf& b) {
   b.size = 0;
 }
 
+// Pipeline trace of av1pf_chain_host_many, in the tracing build only
+// (AV1PF_TRACE; av1pf_trace_pipeline reads it): per frame of the last call,
+// CUDA events at the start and end of its upload, chain, download and
+// descriptor upload on their streams, and host timestamps of its enqueue
+// steps. Elsewhere the calls are empty.
+namespace pipe_trace {
+#ifdef AV1PF_TRACE
+constexpr int kCap = 256;
+cudaEvent_t g_ev[kCap][8] = {};
+double g_host[kCap][4] = {};
+int g_n = 0, g_cur = -1;
+std::chrono::steady_clock::time_point g_t0;
+void begin(int frames) {
+  if (!g_ev[0][0])
+    for (auto& row : g_ev)
+      for (cudaEvent_t& e : row) cudaEventCreate(&e);
+  g_n = frames < kCap ? frames : kCap;
+  g_t0 = std::chrono::steady_clock::now();
+}
+void frame(int k) { g_cur = k < kCap ? k : -1; }
+void mark(int j, cudaStream_t s) {
+  if (g_cur >= 0) cudaEventRecord(g_ev[g_cur][j], s);
+}
+void stamp(int j) {
+  if (g_cur >= 0)
+    g_host[g_cur][j] = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - g_t0).count();
+}
+void end() { g_cur = -1; }
+#else
+inline void begin(int) {}
+inline void frame(int) {}
+inline void mark(int, cudaStream_t) {}
+inline void stamp(int) {}
+inline void end() {}
+#endif
+}  // namespace pipe_trace
+
 // Plans `jobs`, sizes scratch and a descriptor buffer, uploads and launches
 // on `s`.
 int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
@@ -153,6 +191,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   if ((rc = ensure_host(m.host, plan.upload_bytes + 256)) != AV1PF_OK) return rc;
   cudaStream_t ups = upload_override ? upload_override : upload;
   if (m.used) cudaStreamWaitEvent(ups, m.done, 0);
+  pipe_trace::mark(6, ups);
   uint8_t* dmeta = static_cast<uint8_t*>(m.dev.ptr);
   uint8_t* hmeta = static_cast<uint8_t*>(m.host.ptr);
   // film grain: this buffer's own scratch (the previous call's output kernel
@@ -181,6 +220,7 @@ int Ctx::run(const FrameJob* jobs, int n, cudaStream_t s) {
   // and the stages' readiness flags start cleared
   if (e == cudaSuccess && plan.n_flags) e = cudaMemsetAsync(dmeta + plan.off_flags, 0, plan.n_flags * 4, ups);
   if (e == cudaSuccess) e = cudaEventRecord(m.uploaded, ups);
+  pipe_trace::mark(7, ups);
   // The kernels read the upload: the host waits for it rather than the
   // chain's stream. It waited only for the chain that used this buffer two
   // calls ago, so it has usually landed already; and with nothing between
@@ -714,6 +754,7 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
   // goes on `up` right after them and is waited for on `comp` too, and the
   // host goes on queueing uploads
   UploadsAfterPlanes uploads_after_planes(ctx, up);
+  pipe_trace::begin(n);
   // frame k uses slot k % slots: its upload waits for the chain that last
   // read the slot's inputs, its chain for its upload and for the download
   // that last read the slot's outputs
@@ -721,22 +762,31 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     const av1pf_host_job& j = jobs[k];
     Ctx::PipeSlot& ps = ctx->pipe[k % slots];
     const bool reused = k >= slots;
+    pipe_trace::frame(k);
+    pipe_trace::stamp(0);
     if (reused) e = cudaStreamWaitEvent(up, ps.computed, 0);
     // the slot's map staging is read by its previous upload
     if (e == cudaSuccess && reused) e = cudaEventSynchronize(ps.uploaded);
     av1pf_plane din[3], dref[3];
     av1pf_maps dm;
+    pipe_trace::mark(0, up);
     if (e == cudaSuccess)
       e = upload_job(lay[size_t(k)], j.info, j.maps, j.in, static_cast<uint8_t*>(ps.in.ptr),
                      static_cast<uint8_t*>(ps.ref.ptr), static_cast<uint8_t*>(ps.maps.ptr), din, dref, dm,
                      static_cast<uint8_t*>(ps.maps_stage.ptr), up);
+    pipe_trace::mark(1, up);
+    pipe_trace::stamp(1);
     if (e == cudaSuccess) e = cudaEventRecord(ps.uploaded, up);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(comp, ps.uploaded, 0);
     if (e == cudaSuccess && reused) e = cudaStreamWaitEvent(comp, ps.downloaded, 0);
     if (e != cudaSuccess) break;
     uint8_t* dframe = j.frame_out ? static_cast<uint8_t*>(ps.frame.ptr) : nullptr;
+    pipe_trace::mark(2, comp);
     rc = av1pf_chain(ctx, j.info, j.params, &dm, din, dref, dframe, comp);
+    pipe_trace::mark(3, comp);
+    pipe_trace::stamp(2);
     if (rc != AV1PF_OK) {
+      pipe_trace::end();
       cudaStreamSynchronize(up);
       cudaStreamSynchronize(comp);
       cudaStreamSynchronize(down);
@@ -744,9 +794,13 @@ int av1pf_chain_host_many(av1pf_ctx* ctx, int n, const av1pf_host_job* jobs) {
     }
     e = cudaEventRecord(ps.computed, comp);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(down, ps.computed, 0);
+    pipe_trace::mark(4, down);
     if (e == cudaSuccess) e = download_job(lay[size_t(k)], j.info, dref, j.ref_out, dframe, j.frame_out, down);
+    pipe_trace::mark(5, down);
+    pipe_trace::stamp(3);
     if (e == cudaSuccess) e = cudaEventRecord(ps.downloaded, down);
   }
+  pipe_trace::end();
   // every download waits for its chain, which waits for its upload
   const cudaError_t e_up = cudaStreamSynchronize(up);
   const cudaError_t e_comp = cudaStreamSynchronize(comp);
@@ -798,3 +852,25 @@ const char* av1pf_last_error(void) { return t_last_error.c_str(); }
 uint64_t av1pf_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 }  // extern "C"
+
+#ifdef AV1PF_TRACE
+// The tracing build's read-out of the last av1pf_chain_host_many call: per
+// frame (at most `max`), 8 device times in us from frame 0's upload start
+// (upload start, end; chain start, end; download start, end; descriptor
+// upload start, end; -1 where not recorded) and 4 host times in us from the
+// call's start (frame begun, upload queued, chain queued, download queued).
+// Returns the frame count.
+extern "C" int av1pf_trace_pipeline(float* dev_us, double* host_us, int max) {
+  using namespace av1pf::pipe_trace;
+  const int n = g_n < max ? g_n : max;
+  for (int k = 0; k < n; k++) {
+    for (int j = 0; j < 8; j++) {
+      float ms = -1.f;
+      if (cudaEventElapsedTime(&ms, g_ev[0][0], g_ev[k][j]) != cudaSuccess) ms = -1e-3f;
+      dev_us[k * 8 + j] = ms * 1e3f;
+    }
+    for (int j = 0; j < 4; j++) host_us[k * 4 + j] = g_host[k][j];
+  }
+  return n;
+}
+#endif
