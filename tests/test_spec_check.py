@@ -152,6 +152,14 @@ CHAIN_CASES = {
     "lr_unit128": dict(width=200, height=140, bit_depth=10, lr_unit_shift=1, seed=14),
     "big_blocks": dict(width=128, height=128, bit_depth=10, min_block_log2=5, skip_pct=10, seed=17),
     "odd_67x45_grain": dict(width=67, height=45, bit_depth=10, enable_grain=1, seed=25, frame_index=1),
+    "12bit_422_sr11_grain": dict(width=112, height=64, bit_depth=12, subsampling_x=1, subsampling_y=0,
+                                 superres_denom=11, enable_grain=1, seed=41, frame_index=6),
+    "8bit_u8_444_grain": dict(width=96, height=64, bit_depth=8, sample_bytes=1, subsampling_x=0, subsampling_y=0,
+                              enable_grain=1, seed=42, frame_index=2),
+    "lr_unit256_uv_half": dict(width=180, height=104, bit_depth=10, lr_unit_shift=2, lr_uv_shift=1, seed=43),
+    "no_cdef": dict(width=120, height=72, bit_depth=10, enable_cdef=0, seed=44),
+    "no_lf": dict(width=120, height=72, bit_depth=10, enable_lf=0, seed=45),
+    "8bit_u16_samples": dict(width=104, height=64, bit_depth=8, sample_bytes=2, seed=46),
 }
 
 
